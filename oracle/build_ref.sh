@@ -1,0 +1,81 @@
+#!/usr/bin/env bash
+# Builds the oracle (test infrastructure only):
+#   oracle/_ref/liboracle.so               CPU restatement of the transient solve + CPU Cholesky
+#   oracle/_ref/CalcNonstat3DLine_{A2,A3,E2,E3}
+#                                          the reference's own 3D transient solver, compiled
+#                                          unmodified from its sources with the shim headers in
+#                                          oracle/shim and the pardiso_64 stand-in
+#   oracle/_ref/CalcStat3D_3T_A            the reference's stationary A0 / V solver, same way
+#
+# The reference sources are read in place (default /root/reference, override with
+# TDEM_REFERENCE_ROOT); nothing is copied into the repository.  When the reference
+# tree is absent (for example on a machine that only runs the prebuilt files) the
+# reference binaries are skipped and only liboracle.so is built.
+set -euo pipefail
+HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
+OUT="$HERE/_ref"
+REF="${TDEM_REFERENCE_ROOT:-/root/reference}"
+MOD="$REF/CODE/programs to folder Modules"
+JOBS="${JOBS:-$(nproc)}"
+CXX="${TDEM_CXX:-g++}"
+mkdir -p "$OUT"
+
+OPT="-O2 -g0"
+CXXFLAGS_OR="-std=c++17 $OPT -fPIC -pthread -Wall -Wno-unused-function"
+
+# --- oracle library (own code only) -------------------------------------------
+build_oracle() {
+  local objs=()
+  for f in cpu_cholesky pardiso_shim tdem_oracle; do
+    if [ -f "$HERE/$f.cpp" ]; then
+      if [ ! -f "$OUT/$f.o" ] || [ "$HERE/$f.cpp" -nt "$OUT/$f.o" ] || [ "$HERE/cpu_cholesky.h" -nt "$OUT/$f.o" ]; then
+        $CXX $CXXFLAGS_OR -c "$HERE/$f.cpp" -o "$OUT/$f.o"
+      fi
+      objs+=("$OUT/$f.o")
+    fi
+  done
+  $CXX -shared -pthread -o "$OUT/liboracle.so" "${objs[@]}" -ldl
+}
+build_oracle
+
+if [ ! -d "$MOD" ]; then
+  echo "reference tree not found at $REF: skipping the reference binaries"
+  exit 0
+fi
+
+# flags that let the MSVC sources compile with g++ (no source edits)
+REFFLAGS="-std=c++17 $OPT -fpermissive -w -D__forceinline=inline -include cmath -include cfloat \
+ -include cstring -include ctime -include algorithm -include iterator -include $HERE/shim/llp64_stdio.h \
+ -I$HERE/shim"
+
+build_variant() {  # name, source dir, extra compiler flags
+  local name="$1" src="$2" extra="${3:-}"
+  local obj="$OUT/obj_$name" inc="$OUT/inc_$name"
+  mkdir -p "$obj" "$inc"
+  # case aliases: the sources include headers with a different capitalisation
+  # (forwarding headers, so the real header's own includes resolve next to it)
+  rm -f "$inc/Vec_Prep_Data.h" "$inc/Give_out_vec_loop.h"
+  [ -f "$src/vec_prep_data.h" ] && printf '#include "%s/vec_prep_data.h"\n' "$src" > "$inc/Vec_Prep_Data.h"
+  [ -f "$src/give_out_vec_loop.h" ] && printf '#include "%s/give_out_vec_loop.h"\n' "$src" > "$inc/Give_out_vec_loop.h"
+  local objs=()
+  local pids=()
+  while IFS= read -r -d '' f; do
+    local b
+    b="$(basename "$f" .cpp)"
+    objs+=("$obj/$b.o")
+    if [ ! -f "$obj/$b.o" ] || [ "$f" -nt "$obj/$b.o" ]; then
+      $CXX $REFFLAGS $extra -I"$inc" -c "$f" -o "$obj/$b.o" &
+      pids+=($!)
+      if [ "${#pids[@]}" -ge "$JOBS" ]; then wait "${pids[0]}"; pids=("${pids[@]:1}"); fi
+    fi
+  done < <(find "$src" -maxdepth 1 -name '*.cpp' -print0 | sort -z)
+  for p in "${pids[@]}"; do wait "$p"; done
+  $CXX -pthread -o "$OUT/$name" "${objs[@]}" "$OUT/pardiso_shim.o" "$OUT/cpu_cholesky.o" -ldl
+  echo "built $OUT/$name"
+}
+
+build_variant CalcNonstat3DLine_A2 "$MOD/!programs for 2-point implicit scheme/!programs for A-formulation/CalcNonstat3DLine"
+build_variant CalcNonstat3DLine_A3 "$MOD/!programs for 3-point implicit scheme/!programs for A-formulation/CalcNonstat3DLine"
+build_variant CalcNonstat3DLine_E2 "$MOD/!programs for 2-point implicit scheme/!programs for E-formulation/CalcNonstat3DLine"
+build_variant CalcNonstat3DLine_E3 "$MOD/!programs for 3-point implicit scheme/!programs for E-formulation/CalcNonstat3DLine"
+build_variant CalcStat3D_3T_A "$MOD/CalcStat3D_3T_A" "-Dsprintf_s=sprintf"
