@@ -1,1 +1,233 @@
-"""B200-native 3D time-domain EM edge-FEM forward solve (grounded-wire source)."""
+"""B200-native 3D time-domain EM edge-FEM forward solve (horizontal grounded-wire source).
+
+Python mirror of the C-ABI in include/tdem.h.  The product path is the native
+library lib/libtdem_b200.so (CUDA kernels for sm_100a + C++ host code); this
+module only loads it with ctypes.  There is no CPU fallback: every entry point
+raises RuntimeError when the library is missing or no CUDA device is usable.
+
+Reference interfaces mirrored:
+  * run_directory(workdir, "A"|"E", 2|3)  ~ running CalcNonstat3DLine in the
+    Calculations directory (GeoCalculatorSP.cpp:1656-1662 -> CalcSP, TaskSP.cpp:445);
+  * Solver                               ~ Read_data / Prepare_To_Schema /
+    the decade loop / Gather_edsall of CalcNonstat3DLine;
+  * pardiso_64(...)                      ~ MKL's pardiso_64 as called by
+    pardiso_solver (pardiso.cpp:69-126), backed by the GPU factorization.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libtdem_b200.so")
+EXE_PATH = os.path.join(_HERE, "lib", "tdem_calcnonstat3dline")
+
+FORMULATIONS = {"A": 0, "E": 1, 0: 0, 1: 1}
+
+STATUS = {
+    0: "TDEM_OK",
+    1: "TDEM_ERR_ARGUMENT",
+    2: "TDEM_ERR_INPUT",
+    3: "TDEM_ERR_CUDA",
+    4: "TDEM_ERR_NUMERIC",
+    5: "TDEM_ERR_CANCELLED",
+    6: "TDEM_ERR_STATE",
+}
+
+
+class TdemError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__("%s: %s" % (STATUS.get(status, status), message))
+        self.status = status
+
+
+class TdemInfo(ctypes.Structure):
+    _fields_ = [
+        ("n_edges", ctypes.c_int64),
+        ("n_interior", ctypes.c_int64),
+        ("nnz_matrix", ctypes.c_int64),
+        ("nnz_factor", ctypes.c_int64),
+        ("factor_flops", ctypes.c_double),
+        ("device_bytes", ctypes.c_int64),
+        ("n_sources", ctypes.c_int),
+        ("n_times", ctypes.c_int),
+        ("first_layer", ctypes.c_int),
+        ("last_layer", ctypes.c_int),
+        ("n_rec_b", ctypes.c_int),
+        ("n_rec_e", ctypes.c_int),
+        ("factorizations", ctypes.c_int),
+        ("steps", ctypes.c_int),
+        ("kernel_launches", ctypes.c_int),
+        ("t_setup_s", ctypes.c_double),
+        ("t_assemble_s", ctypes.c_double),
+        ("t_factor_s", ctypes.c_double),
+        ("t_steps_s", ctypes.c_double),
+        ("t_output_s", ctypes.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+_lib: Optional[ctypes.CDLL] = None
+
+EXPORTED = [
+    "tdem_run_directory",
+    "tdem_solver_create",
+    "tdem_solver_run",
+    "tdem_solver_write_outputs",
+    "tdem_solver_results",
+    "tdem_solver_info",
+    "tdem_solver_cancel",
+    "tdem_solver_error",
+    "tdem_solver_destroy",
+    "tdem_pardiso_64",
+    "pardiso_64",
+    "mkl_set_num_threads",
+    "tdem_version",
+]
+
+
+def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Loads libtdem_b200.so (fails loudly when it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError("native library %s not found: run __graft_entry__.build() "
+                           "(or python -m <package>.build) first" % path)
+    lib = ctypes.CDLL(path)
+    P = ctypes.c_void_p
+    lib.tdem_run_directory.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_char_p, ctypes.c_size_t]
+    lib.tdem_run_directory.restype = ctypes.c_int
+    lib.tdem_solver_create.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                       ctypes.POINTER(P)]
+    lib.tdem_solver_create.restype = ctypes.c_int
+    for name in ("tdem_solver_run", "tdem_solver_write_outputs", "tdem_solver_cancel"):
+        getattr(lib, name).argtypes = [P]
+        getattr(lib, name).restype = ctypes.c_int
+    lib.tdem_solver_results.argtypes = [P, P, P, P]
+    lib.tdem_solver_results.restype = ctypes.c_int
+    lib.tdem_solver_info.argtypes = [P, ctypes.POINTER(TdemInfo)]
+    lib.tdem_solver_info.restype = ctypes.c_int
+    lib.tdem_solver_error.argtypes = [P]
+    lib.tdem_solver_error.restype = ctypes.c_char_p
+    lib.tdem_solver_destroy.argtypes = [P]
+    lib.tdem_solver_destroy.restype = None
+    lib.tdem_version.restype = ctypes.c_char_p
+    pi = ctypes.POINTER(ctypes.c_longlong)
+    for name in ("tdem_pardiso_64", "pardiso_64"):
+        f = getattr(lib, name)
+        f.argtypes = [P, pi, pi, pi, pi, pi, P, pi, pi, pi, pi, pi, pi, P, P, pi]
+        f.restype = None
+    _lib = lib
+    return lib
+
+
+def _form(formulation) -> int:
+    if formulation not in FORMULATIONS:
+        raise ValueError("formulation must be 'A' or 'E'")
+    return FORMULATIONS[formulation]
+
+
+def run_directory(workdir: str, formulation="A", scheme: int = 2, device: int = 0) -> None:
+    """One drop-in run of CalcNonstat3DLine in workdir (writes edsall/ball/eall_anom.N)."""
+    lib = load_library()
+    buf = ctypes.create_string_buffer(2048)
+    st = lib.tdem_run_directory(os.fsencode(workdir), _form(formulation), int(scheme), int(device), buf,
+                                len(buf))
+    if st != 0:
+        raise TdemError(st, buf.value.decode(errors="replace"))
+
+
+class Solver:
+    """A transient forward solve held on one GPU: create -> run -> results / write_outputs."""
+
+    def __init__(self, workdir: str, formulation="A", scheme: int = 2, device: int = 0):
+        self._lib = load_library()
+        self._h = ctypes.c_void_p()
+        st = self._lib.tdem_solver_create(os.fsencode(workdir), _form(formulation), int(scheme), int(device),
+                                          ctypes.byref(self._h))
+        if st != 0:
+            msg = self.error()
+            self.close()
+            raise TdemError(st, msg)
+
+    def error(self) -> str:
+        if not self._h:
+            return "no solver"
+        return (self._lib.tdem_solver_error(self._h) or b"").decode(errors="replace")
+
+    def _check(self, st: int) -> None:
+        if st != 0:
+            raise TdemError(st, self.error())
+
+    def run(self) -> "Solver":
+        self._check(self._lib.tdem_solver_run(self._h))
+        return self
+
+    def cancel(self) -> None:
+        self._check(self._lib.tdem_solver_cancel(self._h))
+
+    def write_outputs(self) -> None:
+        self._check(self._lib.tdem_solver_write_outputs(self._h))
+
+    def info(self) -> dict:
+        inf = TdemInfo()
+        self._check(self._lib.tdem_solver_info(self._h, ctypes.byref(inf)))
+        return inf.as_dict()
+
+    def results(self):
+        """(eall, emf, ball): arrays [layer][component][receiver] in mV, mV, mTl."""
+        inf = self.info()
+        nl = inf["last_layer"] - inf["first_layer"] + 1
+        e = np.zeros((nl, 3, inf["n_rec_e"]))
+        m = np.zeros((nl, 3, inf["n_rec_b"]))
+        b = np.zeros((nl, 3, inf["n_rec_b"]))
+        self._check(self._lib.tdem_solver_results(self._h, e.ctypes.data, m.ctypes.data, b.ctypes.data))
+        return e, m, b
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.tdem_solver_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def pardiso_64(handle: np.ndarray, phase: int, a, ia, ja, nrhs: int = 1, b=None, x=None) -> int:
+    """Calls the GPU-backed pardiso_64 with MKL's argument conventions (mtype 2,
+    1-based upper CSR with int64 indices).  handle is a 64-entry int64 array
+    (MKL's pt); returns MKL's error code."""
+    lib = load_library()
+    pi = ctypes.POINTER(ctypes.c_longlong)
+
+    def ll(v):
+        return ctypes.byref(ctypes.c_longlong(v))
+
+    n = len(ia) - 1
+    err = ctypes.c_longlong(0)
+    iparm = np.zeros(64, dtype=np.int64)
+    perm = np.zeros(max(n, 1), dtype=np.int64)
+    ia = np.ascontiguousarray(ia, dtype=np.int64)
+    ja = np.ascontiguousarray(ja, dtype=np.int64)
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    lib.pardiso_64(handle.ctypes.data, ll(1), ll(1), ll(2), ll(phase), ll(n), a.ctypes.data,
+                   ia.ctypes.data_as(pi), ja.ctypes.data_as(pi), perm.ctypes.data_as(pi), ll(nrhs),
+                   iparm.ctypes.data_as(pi), ll(0), None if b is None else b.ctypes.data,
+                   None if x is None else x.ctypes.data, ctypes.byref(err))
+    return int(err.value)

@@ -1,0 +1,316 @@
+// C-ABI entry points (include/tdem.h).
+#include "../../include/tdem.h"
+
+#include <cuda_runtime.h>
+
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "driver.h"
+#include "gpu_cholesky.h"
+#include "symbolic.h"
+
+struct tdem_solver {
+  tdem::TransientSolve solve;
+  cudaStream_t stream = nullptr;
+  int device = 0;
+  std::string error;
+  volatile int cancel = 0;
+  bool ran = false;
+};
+
+namespace {
+
+tdem_status classify(const std::string& e) {
+  if (e.empty()) return TDEM_OK;
+  if (e == "cancelled") return TDEM_ERR_CANCELLED;
+  if (e.find("cuda") != std::string::npos || e.find("CUDA") != std::string::npos) return TDEM_ERR_CUDA;
+  if (e.find("non-positive pivot") != std::string::npos) return TDEM_ERR_NUMERIC;
+  return TDEM_ERR_INPUT;
+}
+
+void put_err(char* buf, size_t len, const std::string& e) {
+  if (!buf || !len) return;
+  std::strncpy(buf, e.c_str(), len - 1);
+  buf[len - 1] = 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* tdem_version(void) { return "tdem-b200 0.1 (sm_100a, FP64 multifrontal)"; }
+
+tdem_status tdem_solver_create(const char* workdir, int formulation, int scheme, int device,
+                               tdem_solver** out) {
+  if (!workdir || !out) return TDEM_ERR_ARGUMENT;
+  *out = nullptr;
+  if ((formulation != 0 && formulation != 1) || (scheme != 2 && scheme != 3)) return TDEM_ERR_ARGUMENT;
+  auto s = std::make_unique<tdem_solver>();
+  s->device = device;
+  if (cudaSetDevice(device) != cudaSuccess) return TDEM_ERR_CUDA;
+  if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) return TDEM_ERR_CUDA;
+  tdem::RunOptions opt;
+  opt.formulation = formulation;
+  opt.scheme = scheme;
+  opt.cancel = &s->cancel;
+  s->error = s->solve.prepare(workdir, opt, s->stream);
+  const tdem_status st = classify(s->error);
+  *out = s.release();
+  return st;
+}
+
+tdem_status tdem_solver_run(tdem_solver* s) {
+  if (!s) return TDEM_ERR_ARGUMENT;
+  if (!s->error.empty() && !s->ran) return TDEM_ERR_STATE;
+  cudaSetDevice(s->device);
+  s->error = s->solve.run();
+  s->ran = s->error.empty();
+  return classify(s->error);
+}
+
+tdem_status tdem_solver_write_outputs(tdem_solver* s) {
+  if (!s) return TDEM_ERR_ARGUMENT;
+  if (!s->ran) return TDEM_ERR_STATE;
+  cudaSetDevice(s->device);
+  s->error = s->solve.write_outputs();
+  return classify(s->error);
+}
+
+tdem_status tdem_solver_results(tdem_solver* s, double* eall, double* emf, double* ball) {
+  if (!s) return TDEM_ERR_ARGUMENT;
+  if (!s->ran) return TDEM_ERR_STATE;
+  cudaSetDevice(s->device);
+  std::vector<double> e, m, b;
+  s->error = s->solve.results(e, m, b);
+  if (!s->error.empty()) return classify(s->error);
+  // units and signs as written to the files (Gather_edsall)
+  if (eall)
+    for (size_t i = 0; i < e.size(); ++i) eall[i] = e[i] * 1000;
+  if (emf)
+    for (size_t i = 0; i < m.size(); ++i) emf[i] = m[i] * (-1000);
+  if (ball)
+    for (size_t i = 0; i < b.size(); ++i) ball[i] = b[i] * 1000;
+  return TDEM_OK;
+}
+
+tdem_status tdem_solver_info(const tdem_solver* s, tdem_info* info) {
+  if (!s || !info) return TDEM_ERR_ARGUMENT;
+  std::memset(info, 0, sizeof(*info));
+  const tdem::Model& m = s->solve.model();
+  info->n_edges = m.n_edges;
+  info->n_sources = m.npls;
+  info->n_times = (int)m.time.size();
+  info->n_rec_b = (int)m.rec_b.size();
+  info->n_rec_e = (int)m.rec_e.size();
+  info->first_layer = s->solve.first_layer();
+  info->last_layer = s->solve.last_layer();
+  info->n_interior = s->solve.n_interior();
+  info->nnz_matrix = s->solve.nnz_full();
+  const tdem::PhaseTimes& pt = s->solve.times();
+  info->factorizations = pt.factorizations;
+  info->steps = pt.steps;
+  info->t_setup_s = pt.setup_s;
+  info->t_assemble_s = pt.assemble_s;
+  info->t_factor_s = pt.factor_s;
+  info->t_steps_s = pt.steps_s;
+  info->t_output_s = pt.output_s;
+  info->kernel_launches = s->solve.kernel_launches();
+  if (m.n_edges > 0 && s->solve.n_interior() > 0) {
+    const tdem::GpuCholesky& c = s->solve.cholesky();
+    info->nnz_factor = c.symbolic().nnz_l;
+    info->factor_flops = c.symbolic().flops;
+    info->device_bytes = (int64_t)c.device_bytes();
+  }
+  return TDEM_OK;
+}
+
+tdem_status tdem_solver_cancel(tdem_solver* s) {
+  if (!s) return TDEM_ERR_ARGUMENT;
+  s->cancel = 1;
+  return TDEM_OK;
+}
+
+const char* tdem_solver_error(const tdem_solver* s) { return s ? s->error.c_str() : "null solver"; }
+
+void tdem_solver_destroy(tdem_solver* s) {
+  if (!s) return;
+  cudaSetDevice(s->device);
+  cudaStream_t st = s->stream;
+  delete s;
+  if (st) cudaStreamDestroy(st);
+}
+
+tdem_status tdem_run_directory(const char* workdir, int formulation, int scheme, int device, char* errbuf,
+                               size_t errlen) {
+  tdem_solver* s = nullptr;
+  tdem_status st = tdem_solver_create(workdir, formulation, scheme, device, &s);
+  if (st == TDEM_OK) st = tdem_solver_run(s);
+  if (st == TDEM_OK) st = tdem_solver_write_outputs(s);
+  put_err(errbuf, errlen, s ? s->error : std::string("invalid arguments"));
+  tdem_solver_destroy(s);
+  return st;
+}
+
+// ---------------------------------------------------------------------------
+// pardiso_64 on the GPU
+// ---------------------------------------------------------------------------
+namespace {
+struct PardisoHandle {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::unique_ptr<tdem::GpuCholesky> chol;
+  int64_t n = 0, nnz = 0;
+  uint64_t hash = 0;
+  std::vector<int64_t> upper_to_lower;  // upper-CSR entry -> lower-CSR entry
+  double* d_vals = nullptr;
+  double* d_x = nullptr;
+  int nrhs_cap = 0;
+};
+
+uint64_t pattern_hash(int64_t n, const long long* ia, const long long* ja) {
+  uint64_t h = 1469598103934665603ull ^ (uint64_t)n;
+  for (int64_t i = 0; i <= n; ++i) h = (h ^ (uint64_t)ia[i]) * 1099511628211ull;
+  for (int64_t q = 0; q < ia[n] - 1; ++q) h = (h ^ (uint64_t)ja[q]) * 1099511628211ull;
+  return h;
+}
+
+int pardiso_analyse(PardisoHandle* h, int64_t n, const long long* ia, const long long* ja, int nrhs) {
+  // upper 1-based CSR (row i: columns j >= i) -> lower 0-based CSR (row j: columns i <= j)
+  const int64_t nnz = ia[n] - 1;
+  std::vector<int64_t> cnt(n + 1, 0);
+  for (int64_t i = 0; i < n; ++i)
+    for (int64_t q = ia[i] - 1; q < ia[i + 1] - 1; ++q) {
+      const int64_t j = ja[q] - 1;
+      if (j < i || j >= n) return -1;
+      ++cnt[j + 1];
+    }
+  for (int64_t j = 0; j < n; ++j) cnt[j + 1] += cnt[j];
+  std::vector<int> col(nnz);
+  h->upper_to_lower.assign(nnz, 0);
+  std::vector<int64_t> fill(cnt.begin(), cnt.end() - 1);
+  for (int64_t i = 0; i < n; ++i)
+    for (int64_t q = ia[i] - 1; q < ia[i + 1] - 1; ++q) {
+      const int64_t j = ja[q] - 1;
+      const int64_t p = fill[j]++;
+      col[p] = (int)i;
+      h->upper_to_lower[q] = p;
+    }
+  tdem::Symbolic sy;
+  if (!tdem::analyse((int)n, cnt.data(), col.data(), nullptr, sy).empty()) return -1;
+  std::vector<int> p2v(n);
+  for (int64_t p = 0; p < n; ++p) p2v[p] = sy.iperm[p];
+  h->chol.reset(new tdem::GpuCholesky());
+  if (!h->chol->setup(std::move(sy), p2v, std::max(1, nrhs), h->stream).empty()) return -2;
+  if (h->d_vals) cudaFree(h->d_vals);
+  if (cudaMalloc(&h->d_vals, sizeof(double) * std::max<int64_t>(nnz, 1)) != cudaSuccess) return -2;
+  h->n = n;
+  h->nnz = nnz;
+  h->hash = pattern_hash(n, ia, ja);
+  return 0;
+}
+}  // namespace
+
+void tdem_pardiso_64(void* pt, const long long* /*maxfct*/, const long long* /*mnum*/, const long long* mtype,
+                     const long long* phase, const long long* n, const void* a, const long long* ia,
+                     const long long* ja, long long* /*perm*/, const long long* nrhs, long long* /*iparm*/,
+                     const long long* /*msglvl*/, void* b, void* x, long long* error) {
+  void** ptv = (void**)pt;
+  PardisoHandle* h = (PardisoHandle*)ptv[0];
+  *error = 0;
+  if (*phase == -1) {
+    if (h) {
+      cudaSetDevice(h->device);
+      h->chol.reset();
+      if (h->d_vals) cudaFree(h->d_vals);
+      if (h->d_x) cudaFree(h->d_x);
+      if (h->stream) cudaStreamDestroy(h->stream);
+      delete h;
+    }
+    ptv[0] = nullptr;
+    return;
+  }
+  if (*mtype != 2) {
+    *error = -1;
+    return;
+  }
+  if (*phase == 12) {
+    if (!h) {
+      h = new PardisoHandle();
+      const char* dv = getenv("TDEM_PARDISO_DEVICE");
+      h->device = dv ? atoi(dv) : 0;
+      if (cudaSetDevice(h->device) != cudaSuccess ||
+          cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete h;
+        *error = -2;
+        return;
+      }
+      ptv[0] = h;
+    }
+    cudaSetDevice(h->device);
+    if (!h->chol || h->n != *n || h->nnz != ia[*n] - 1 || h->hash != pattern_hash(*n, ia, ja)) {
+      const int r = pardiso_analyse(h, *n, ia, ja, 1);
+      if (r) {
+        *error = r;
+        return;
+      }
+    }
+    // values: upper CSR order -> lower CSR order
+    std::vector<double> lv(h->nnz);
+    const double* av = (const double*)a;
+    for (int64_t q = 0; q < h->nnz; ++q) lv[h->upper_to_lower[q]] = av[q];
+    cudaMemcpyAsync(h->d_vals, lv.data(), sizeof(double) * h->nnz, cudaMemcpyHostToDevice, h->stream);
+    h->chol->factor(h->d_vals, h->stream);
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
+      *error = -2;
+      return;
+    }
+    if (h->chol->status(h->stream)) *error = -4;
+    return;
+  }
+  if (*phase == 33) {
+    if (!h || !h->chol) {
+      *error = -1;
+      return;
+    }
+    cudaSetDevice(h->device);
+    const int nr = (int)*nrhs;
+    if (nr < 1) {
+      *error = -1;
+      return;
+    }
+    if (nr > h->nrhs_cap) {
+      if (h->d_x) cudaFree(h->d_x);
+      h->d_x = nullptr;
+      if (cudaMalloc(&h->d_x, sizeof(double) * h->n * nr) != cudaSuccess) {
+        *error = -2;
+        return;
+      }
+      h->nrhs_cap = nr;
+    }
+    // the solve workspace was sized for one column: solve column by column
+    for (int r = 0; r < nr; ++r) {
+      cudaMemcpyAsync(h->d_x + h->n * r, (const double*)b + h->n * r, sizeof(double) * h->n,
+                      cudaMemcpyHostToDevice, h->stream);
+      h->chol->solve(h->d_x + h->n * r, h->d_x + h->n * r, h->n, 1, h->stream);
+    }
+    cudaMemcpyAsync(x, h->d_x, sizeof(double) * h->n * nr, cudaMemcpyDeviceToHost, h->stream);
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) *error = -2;
+    return;
+  }
+  *error = -1;
+}
+
+void pardiso_64(void* pt, const long long* maxfct, const long long* mnum, const long long* mtype,
+                const long long* phase, const long long* n, const void* a, const long long* ia,
+                const long long* ja, long long* perm, const long long* nrhs, long long* iparm,
+                const long long* msglvl, void* b, void* x, long long* error) {
+  tdem_pardiso_64(pt, maxfct, mnum, mtype, phase, n, a, ia, ja, perm, nrhs, iparm, msglvl, b, x, error);
+}
+
+void mkl_set_num_threads(int) {}
+
+}  // extern "C"

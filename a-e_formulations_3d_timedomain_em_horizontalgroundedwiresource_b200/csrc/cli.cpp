@@ -1,0 +1,46 @@
+// Drop-in executable for the reference's CalcNonstat3DLine (run in the
+// Calculations directory by GeoCalculatorSP, GeoCalculatorSP.cpp:1656-1662).
+//
+//   tdem_calcnonstat3dline [--form A|E] [--scheme 2|3] [--device N] [workdir]
+//
+// Without flags the variant is taken from the program name when it ends in
+// _A2, _A3, _E2 or _E3 (one name per reference build), else A-form, two-point.
+// Unlike the reference, which always exits 0, the exit code is the tdem_status.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+
+#include "../../include/tdem.h"
+
+int main(int argc, char** argv) {
+  int form = 0, scheme = 2, device = 0;
+  std::string dir = ".";
+  const std::string prog = argv[0];
+  if (prog.size() >= 3) {
+    const std::string tail = prog.substr(prog.size() - 3);
+    if (tail == "_A2") { form = 0; scheme = 2; }
+    if (tail == "_A3") { form = 0; scheme = 3; }
+    if (tail == "_E2") { form = 1; scheme = 2; }
+    if (tail == "_E3") { form = 1; scheme = 3; }
+  }
+  for (int i = 1; i < argc; ++i) {
+    if (!strcmp(argv[i], "--form") && i + 1 < argc) {
+      const char* v = argv[++i];
+      form = (v[0] == 'E' || v[0] == 'e' || v[0] == '1') ? 1 : 0;
+    } else if (!strcmp(argv[i], "--scheme") && i + 1 < argc) {
+      scheme = atoi(argv[++i]);
+    } else if (!strcmp(argv[i], "--device") && i + 1 < argc) {
+      device = atoi(argv[++i]);
+    } else if (argv[i][0] == '-') {
+      fprintf(stderr, "usage: %s [--form A|E] [--scheme 2|3] [--device N] [workdir]\n", argv[0]);
+      return (int)TDEM_ERR_ARGUMENT;
+    } else {
+      dir = argv[i];
+    }
+  }
+  char err[1024] = {0};
+  const tdem_status st = tdem_run_directory(dir.c_str(), form, scheme, device, err, sizeof err);
+  if (st != TDEM_OK) fprintf(stderr, "CalcNonstat3DLine (B200): %s\n", err);
+  return (int)st;
+}

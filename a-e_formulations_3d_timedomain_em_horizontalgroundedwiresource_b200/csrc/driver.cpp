@@ -1,0 +1,575 @@
+// Transient driver (see driver.h).
+#include "driver.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "fem_kernels.h"
+#include "symbolic.h"
+
+namespace tdem {
+namespace {
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+#define TRY_CUDA(x)                                                              \
+  do {                                                                           \
+    cudaError_t e_ = (x);                                                        \
+    if (e_ != cudaSuccess) return std::string(#x ": ") + cudaGetErrorString(e_); \
+  } while (0)
+
+// Reference-cube edge basis at `in` (each coordinate in [-1, 1]) dotted with d
+// (T_Brick::Basis_func_on_reference_vec_par, T_Brick.cpp:741-811).
+double basis_dot(int j, const double in[3], const double d[3]) {
+  auto l0 = [](double t) { return (1.0 - t) * 0.5; };
+  auto l1 = [](double t) { return (t + 1.0) * 0.5; };
+  const int dir = j >> 2, a = j & 1, b = (j >> 1) & 1;
+  const int u = (dir + 1) % 3, v = (dir + 2) % 3;
+  const double fa = a ? l1(in[u]) : l0(in[u]);
+  const double fb = b ? l1(in[v]) : l0(in[v]);
+  return fa * fb * d[dir];
+}
+
+// dA_dt of the reference with its argument order (time_approx.cpp:1361-1374).
+double ref_dA_dt(double t, double u_j, double u_j1, double u_j2, double dt, double dt0, double dt1,
+                 double t_j, double t_j1, double t_j2) {
+  if (t < t_j2) t = t_j2;
+  if (t > t_j) t = t_j;
+  return u_j2 * (2.0 * t - t_j - t_j1) / (dt1 * dt) - u_j1 * (2.0 * t - t_j - t_j2) / (dt1 * dt0) +
+         u_j * (2.0 * t - t_j1 - t_j2) / (dt * dt0);
+}
+
+}  // namespace
+
+std::vector<int> decade_starts(const std::vector<double>& time) {
+  std::vector<int> ig{0};
+  const int nt = (int)time.size();
+  double hpre = time[1] - time[0];
+  for (int i = 2; i < nt; ++i) {
+    const double hcur = time[i] - time[i - 1];
+    if (std::fabs(1.0 - hpre / hcur) > 1e-3) {
+      ig.push_back(i);
+      hpre = hcur;
+    }
+  }
+  ig.push_back(nt);
+  return ig;
+}
+
+int find_time_layer(const std::vector<double>& time, double val) {
+  const int nt = (int)time.size();
+  if (nt < 1) return -1;
+  if (std::fabs(val) < 1e-14 && std::fabs(time[0]) < 1e-14) return 0;
+  for (int it = 1; it < nt; ++it)
+    if (std::fabs(1.0 - time[it] / val) < 1e-6) return it;
+  return -1;
+}
+
+TransientSolve::TransientSolve() = default;
+TransientSolve::~TransientSolve() {
+  chol_.reset();
+  for (void* p : allocs_) cudaFree(p);
+}
+
+std::string TransientSolve::alloc(void** p, size_t bytes) {
+  *p = nullptr;
+  cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
+  if (e != cudaSuccess) return std::string("cudaMalloc: ") + cudaGetErrorString(e);
+  allocs_.push_back(*p);
+  return "";
+}
+
+template <class T>
+std::string TransientSolve::upload(T** d, const std::vector<T>& h) {
+  std::string e = alloc((void**)d, h.size() * sizeof(T));
+  if (!e.empty()) return e;
+  if (!h.empty()) TRY_CUDA(cudaMemcpyAsync(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s_));
+  return "";
+}
+
+double TransientSolve::source_coef(int itime, bool two_layer, double dt) const {
+  if (!have_source_) return 0.0;
+  const auto& cf = m_.currentfunction;
+  const auto& t = m_.time;
+  if (opt_.formulation == 0) return cf[itime] != 0.0 ? cf[itime] : 0.0;
+  // E-form: -dJ/dt (time_approx.cpp E-form 1085-1102; Two_Layers_Schema 756-773)
+  double djdt;
+  if (itime + 1 < ntime_) {
+    if (cf[itime] == 0.0) {
+      const double den = two_layer ? dt : (t[itime] - t[itime - 1]);
+      djdt = ((cf[itime] - cf[itime - 1]) / den) * 1.0;
+    } else {
+      const double tm2 = t[std::max(0, itime - 2)];
+      djdt = ref_dA_dt(t[itime], cf[itime - 1], cf[itime], cf[itime + 1], t[itime + 1] - t[itime - 1],
+                       t[itime + 1] - t[itime], t[itime] - t[itime - 1], t[itime], t[itime - 1], tm2);
+    }
+  } else {
+    const double den = two_layer ? dt : (t[itime] - t[itime - 1]);
+    djdt = (cf[itime] - cf[itime - 1]) / den;
+  }
+  return -djdt;
+}
+
+std::string TransientSolve::prepare(const std::string& dir, const RunOptions& opt, cudaStream_t stream) {
+  const double t0 = now_s();
+  opt_ = opt;
+  s_ = stream;
+  if (opt.formulation != 0 && opt.formulation != 1) return "formulation must be 0 (A) or 1 (E)";
+  if (opt.scheme != 2 && opt.scheme != 3) return "scheme must be 2 or 3";
+  std::string e = load_model(dir, m_);
+  if (!e.empty()) return e;
+  n_ = m_.n_edges;
+  npls_ = m_.npls;
+  ntime_ = (int)m_.time.size();
+
+  // printed layers (give_out_vec_loop.cpp:52-73)
+  tlf_ = tll_ = 2;
+  for (int i = 0; i < ntime_; ++i)
+    if (m_.time[i] >= m_.print_left) { tlf_ = i; break; }
+  if (tlf_ > ntime_ - 1) tlf_ = ntime_ - 1;
+  for (int i = 0; i < ntime_; ++i)
+    if (m_.time[i] >= m_.print_right - 1e-6) { tll_ = i; break; }
+  if (m_.print_right > m_.time[ntime_ - 1] - 1e-6) tll_ = ntime_ - 1;
+  if (tll_ - tlf_ < 2) return "fewer than three printed time layers";
+
+  // source
+  if (m_.fdirect) {
+    bool any = false;
+    for (int i = 1; i < ntime_; ++i) any = any || m_.currentfunction[i] != 0.0;
+    have_source_ = (opt.formulation == 1 || any) && m_.n_srs_razb > 0;
+    if (have_source_) {
+      e = locate_dipoles(m_);
+      if (!e.empty()) return e;
+    }
+  }
+  e = load_initial_field(m_, opt.formulation == 1, u0_);
+  if (!e.empty()) return e;
+
+  // patterns: full symmetric CSR over all edges, lower triangle of the interior system
+  edge_pattern(m_, rowptr_, col_);
+  std::vector<int> int_id(n_, -1), int_edge;
+  for (int i = 0; i < n_; ++i)
+    if (!m_.edge_bound[i]) {
+      int_id[i] = (int)int_edge.size();
+      int_edge.push_back(i);
+    }
+  n_int_ = (int64_t)int_edge.size();
+  if (n_int_ == 0) return "no interior edges";
+  std::vector<int64_t> lptr(n_int_ + 1, 0), src;
+  std::vector<int> lcol;
+  std::vector<uint8_t> diag;
+  std::vector<double> xyz((size_t)n_int_ * 3);
+  for (int64_t r = 0; r < n_int_; ++r) {
+    const int i = int_edge[r];
+    for (int64_t q = rowptr_[i]; q < rowptr_[i + 1]; ++q) {
+      const int j = col_[q];
+      if (int_id[j] >= 0 && int_id[j] <= r) {
+        lcol.push_back(int_id[j]);
+        src.push_back(q);
+        diag.push_back(int_id[j] == r);
+      }
+    }
+    lptr[r + 1] = (int64_t)lcol.size();
+    for (int a = 0; a < 3; ++a)
+      xyz[3 * r + a] = 0.5 * (m_.xyz[m_.edge_nodes[i][0]][a] + m_.xyz[m_.edge_nodes[i][1]][a]);
+  }
+  Symbolic sy;
+  e = analyse((int)n_int_, lptr.data(), lcol.data(), xyz.data(), sy, opt.leaf_size);
+  if (!e.empty()) return "analysis: " + e;
+  std::vector<int> p2v(n_int_);
+  for (int64_t p = 0; p < n_int_; ++p) p2v[p] = int_edge[sy.iperm[p]];
+  chol_.reset(new GpuCholesky());
+  e = chol_->setup(std::move(sy), p2v, npls_, s_);
+  if (!e.empty()) return e;
+
+  // device buffers
+  if (!(e = upload(&d_rowptr_, rowptr_)).empty()) return e;
+  if (!(e = upload(&d_col_, col_)).empty()) return e;
+  if (!(e = alloc((void**)&d_C_, sizeof(double) * col_.size())).empty()) return e;
+  if (!(e = alloc((void**)&d_B_, sizeof(double) * col_.size())).empty()) return e;
+  if (!(e = upload(&d_src_, src)).empty()) return e;
+  if (!(e = upload(&d_diag_, diag)).empty()) return e;
+  if (!(e = alloc((void**)&d_avals_, sizeof(double) * src.size())).empty()) return e;
+  {
+    std::vector<uint8_t> b(m_.edge_bound.begin(), m_.edge_bound.end());
+    if (!(e = upload(&d_bound_, b)).empty()) return e;
+  }
+  // source vectors S[e, p] = sum over dipoles of basis . dl * 2 / edge length
+  {
+    std::vector<double> S((size_t)n_ * npls_, 0.0);
+    if (have_source_) {
+      for (int p = 0; p < npls_; ++p)
+        for (const Dipole& d : m_.dipoles[p]) {
+          const double in[3] = {2.0 * d.ksi - 1.0, 2.0 * d.eta - 1.0, 2.0 * d.zeta - 1.0};
+          const double dl[3] = {d.dx, d.dy, d.dz};
+          for (int j = 0; j < 12; ++j) {
+            const int ii = m_.ed[d.elem][j];
+            const auto& a = m_.xyz[m_.edge_nodes[ii][0]];
+            const auto& b = m_.xyz[m_.edge_nodes[ii][1]];
+            const double len = std::sqrt((b[0] - a[0]) * (b[0] - a[0]) + (b[1] - a[1]) * (b[1] - a[1]) +
+                                         (b[2] - a[2]) * (b[2] - a[2]));
+            S[ii + (size_t)p * n_] += basis_dot(j, in, dl) * 2.0 / len;
+          }
+        }
+    }
+    if (!(e = upload(&d_S_, S)).empty()) return e;
+  }
+  if (!(e = alloc((void**)&d_hist_, sizeof(double) * (size_t)ring_ * n_ * npls_)).empty()) return e;
+  if (!(e = alloc((void**)&d_rhs_, sizeof(double) * (size_t)n_ * npls_)).empty()) return e;
+  TRY_CUDA(cudaMemcpyAsync(layer(0), u0_.data(), sizeof(double) * u0_.size(), cudaMemcpyHostToDevice, s_));
+  pt_.setup_s = now_s() - t0;
+
+  // assembly of sigma*C and B/mu, one launch per element colour
+  {
+    const double ta = now_s();
+    std::vector<int> ed((size_t)m_.n_elem * 12);
+    std::vector<double> h((size_t)m_.n_elem * 3), sig(m_.n_elem), imu(m_.n_elem);
+    for (int el = 0; el < m_.n_elem; ++el) {
+      for (int j = 0; j < 12; ++j) ed[(size_t)el * 12 + j] = m_.ed[el][j];
+      for (int a = 0; a < 3; ++a) h[3 * el + a] = m_.xyz[m_.nver[el][7]][a] - m_.xyz[m_.nver[el][0]][a];
+      sig[el] = m_.sigma[m_.nvkat[el]];
+      imu[el] = 1.0 / m_.mu[m_.nvkat[el]];
+    }
+    // greedy colouring: elements sharing an edge get different colours
+    std::vector<std::vector<int>> edge_elems(n_);
+    for (int el = 0; el < m_.n_elem; ++el)
+      for (int j = 0; j < 12; ++j) edge_elems[m_.ed[el][j]].push_back(el);
+    std::vector<int> color(m_.n_elem, -1);
+    int ncol = 0;
+    for (int el = 0; el < m_.n_elem; ++el) {
+      uint64_t used = 0;
+      for (int j = 0; j < 12; ++j)
+        for (int o : edge_elems[m_.ed[el][j]])
+          if (color[o] >= 0 && color[o] < 64) used |= (1ull << color[o]);
+      int c = 0;
+      while (c < 64 && (used >> c & 1)) ++c;
+      if (c >= 64) return "element colouring needs more than 64 colours";
+      color[el] = c;
+      ncol = std::max(ncol, c + 1);
+    }
+    std::vector<int> order;
+    std::vector<int> cstart{0};
+    for (int c = 0; c < ncol; ++c) {
+      for (int el = 0; el < m_.n_elem; ++el)
+        if (color[el] == c) order.push_back(el);
+      cstart.push_back((int)order.size());
+    }
+    int *d_ed = nullptr, *d_order = nullptr;
+    double *d_h = nullptr, *d_sig = nullptr, *d_imu = nullptr;
+    if (!(e = upload(&d_ed, ed)).empty()) return e;
+    if (!(e = upload(&d_h, h)).empty()) return e;
+    if (!(e = upload(&d_sig, sig)).empty()) return e;
+    if (!(e = upload(&d_imu, imu)).empty()) return e;
+    if (!(e = upload(&d_order, order)).empty()) return e;
+    TRY_CUDA(cudaMemsetAsync(d_C_, 0, sizeof(double) * col_.size(), s_));
+    TRY_CUDA(cudaMemsetAsync(d_B_, 0, sizeof(double) * col_.size(), s_));
+    ElemDev ev{d_ed, d_h, d_sig, d_imu};
+    for (int c = 0; c < ncol; ++c) {
+      launch_assemble(ev, d_order + cstart[c], cstart[c + 1] - cstart[c], d_rowptr_, d_col_, d_C_, d_B_, s_);
+      ++launches_;
+    }
+    TRY_CUDA(cudaStreamSynchronize(s_));
+    TRY_CUDA(cudaGetLastError());
+    pt_.assemble_s = now_s() - ta;
+  }
+
+  // receivers
+  {
+    auto owners = [&](const std::vector<int>& ig, int nrec) {
+      std::vector<int> o(nrec, 0);
+      for (int p = 0; p < npls_; ++p)
+        for (int i = ig[p]; i < ig[p + 1] && i < nrec; ++i) o[i] = p;
+      return o;
+    };
+    e = build_receiver_operator(m_, m_.rec_b, owners(m_.rec_b_ig, (int)m_.rec_b.size()), true, rop_b_);
+    if (!e.empty()) return e;
+    e = build_receiver_operator(m_, m_.rec_e, owners(m_.rec_e_ig, (int)m_.rec_e.size()), false, rop_e_);
+    if (!e.empty()) return e;
+    if (!(e = upload(&d_rb_ptr_, rop_b_.rowptr)).empty()) return e;
+    if (!(e = upload(&d_rb_col_, rop_b_.col)).empty()) return e;
+    if (!(e = upload(&d_rb_val_, rop_b_.val)).empty()) return e;
+    if (!(e = upload(&d_rb_src_, rop_b_.src)).empty()) return e;
+    if (!(e = upload(&d_re_ptr_, rop_e_.rowptr)).empty()) return e;
+    if (!(e = upload(&d_re_col_, rop_e_.col)).empty()) return e;
+    if (!(e = upload(&d_re_val_, rop_e_.val)).empty()) return e;
+    if (!(e = upload(&d_re_src_, rop_e_.src)).empty()) return e;
+    const int nl = tll_ - tlf_ + 1;
+    const size_t rb = (size_t)3 * rop_b_.nrec, re = (size_t)3 * rop_e_.nrec;
+    if (!(e = alloc((void**)&d_vb_, sizeof(double) * nl * std::max<size_t>(rb, 1))).empty()) return e;
+    if (!(e = alloc((void**)&d_ve_, sizeof(double) * nl * std::max<size_t>(re, 1))).empty()) return e;
+    TRY_CUDA(cudaMemsetAsync(d_vb_, 0, sizeof(double) * nl * std::max<size_t>(rb, 1), s_));
+    TRY_CUDA(cudaMemsetAsync(d_ve_, 0, sizeof(double) * nl * std::max<size_t>(re, 1), s_));
+    if (!(e = upload(&d_time_, m_.time)).empty()) return e;
+  }
+  TRY_CUDA(cudaStreamSynchronize(s_));
+  pt_.setup_s = now_s() - t0 - pt_.assemble_s;
+  return "";
+}
+
+std::string TransientSolve::factor_with(double mult) {
+  launch_combine(d_C_, d_B_, d_src_, d_diag_, (int64_t)chol_->symbolic().nnz_lower, mult, d_avals_, s_);
+  chol_->factor(d_avals_, s_);
+  launches_ += 1 + chol_->kernel_launches_factor();
+  ++pt_.factorizations;
+  return "";
+}
+
+std::string TransientSolve::step(int itime, int t1, int t2, double m1, double m2, double coef) {
+  if (itime - t1 >= ring_ || (m2 != 0.0 && itime - t2 >= ring_))
+    return "time grid needs a restart layer older than the history ring holds";
+  const double* u1 = layer(t1);
+  const double* u2 = (t2 >= 0) ? layer(t2) : layer(t1);
+  launch_history_rhs(d_rowptr_, d_col_, d_C_, u1, u2, m1, (t2 >= 0) ? m2 : 0.0, d_S_, coef, d_bound_, n_, npls_,
+                     d_rhs_, s_);
+  double* x = layer(itime);
+  cudaMemsetAsync(x, 0, sizeof(double) * (size_t)n_ * npls_, s_);
+  chol_->solve(d_rhs_, x, n_, npls_, s_);
+  launches_ += 1 + chol_->kernel_launches_solve();
+  ++pt_.steps;
+  return "";
+}
+
+void TransientSolve::eval_receivers(int t) {
+  if (t < tlf_ || t > tll_) return;
+  const int li = t - tlf_;
+  if (rop_b_.nrec) {
+    launch_receivers(d_rb_ptr_, d_rb_col_, d_rb_val_, d_rb_src_, 3 * rop_b_.nrec, layer(t), n_,
+                     d_vb_ + (size_t)li * 3 * rop_b_.nrec, s_);
+    ++launches_;
+  }
+  if (rop_e_.nrec) {
+    launch_receivers(d_re_ptr_, d_re_col_, d_re_val_, d_re_src_, 3 * rop_e_.nrec, layer(t), n_,
+                     d_ve_ + (size_t)li * 3 * rop_e_.nrec, s_);
+    ++launches_;
+  }
+}
+
+std::string TransientSolve::run() {
+  const double tstart = now_s();
+  const std::vector<double>& t = m_.time;
+  dec_ig_ = decade_starts(t);
+  const int ndec = (int)dec_ig_.size() - 1;
+  vpre1_.assign(ntime_, -1);
+  vpre2_.assign(ntime_, -1);
+  std::string e;
+  double tf = 0.0;
+  auto timed_factor = [&](double mult) {
+    cudaStreamSynchronize(s_);
+    const double a = now_s();
+    factor_with(mult);
+    cudaStreamSynchronize(s_);
+    tf += now_s() - a;
+  };
+  auto check = [&]() -> std::string {
+    if (opt_.cancel && *opt_.cancel) return "cancelled";
+    return "";
+  };
+  int tn = 0, tn1 = 0, tn2 = 0;
+  if (opt_.scheme == 2) {
+    eval_receivers(0);
+    for (int d = 0; d < ndec; ++d) {
+      const int tbeg = dec_ig_[d], tend = dec_ig_[d + 1];
+      int npre1 = -1, npre2 = -1;
+      if (d > 0) {
+        if (tbeg + 1 >= ntime_) return "last decade has a single step";
+        const double h = t[tbeg + 1] - t[tbeg];
+        npre1 = find_time_layer(t, t[tbeg] - h);
+        npre2 = find_time_layer(t, t[tbeg] - 2 * h);
+        if (npre1 < 0 || npre2 < 0) return "restart layers of a decade not on the time grid";
+      }
+      bool first = true;
+      double mult = 0.0;
+      for (int it = std::max(tbeg, 1); it < tend; ++it) {
+        if (!(e = check()).empty()) return e;
+        if (first && it > 1) {
+          tn2 = npre2;
+          tn1 = npre1;
+          tn = it;
+        } else {
+          tn2 = tn1;
+          tn1 = tn;
+          tn = it;
+        }
+        vpre1_[it] = tn1;
+        vpre2_[it] = tn2;
+        if (first) {
+          mult = 1.0 / (t[it] - t[tn1]);
+          timed_factor(mult);
+          first = false;
+        }
+        if (!(e = step(it, tn1, tn2, mult, 0.0, source_coef(it, false, 0.0))).empty()) return e;
+        eval_receivers(it);
+      }
+    }
+  } else {
+    for (int d = 0; d < ndec; ++d) {
+      const int tbeg = dec_ig_[d], tend = dec_ig_[d + 1];
+      int npre1 = -1, npre2 = -1;
+      if (d > 0) {
+        if (tbeg + 1 >= ntime_) return "last decade has a single step";
+        const double h = t[tbeg + 1] - t[tbeg];
+        npre1 = find_time_layer(t, t[tbeg] - h);
+        npre2 = find_time_layer(t, t[tbeg] - 2 * h);
+        if (npre1 < 0 || npre2 < 0) return "restart layers of a decade not on the time grid";
+      }
+      if (1 >= tbeg && 1 < tend) {
+        // two backward-Euler steps with the first step length (Two_Layers_Schema)
+        if (tend < 3) return "first decade shorter than the two start-up steps";
+        const double dt = t[1] - t[0];
+        timed_factor(1.0 / dt);
+        for (int it = 1; it < 3; ++it) {
+          if (!(e = check()).empty()) return e;
+          vpre1_[it] = it - 1;
+          vpre2_[it] = it - 2;
+          if (!(e = step(it, it - 1, -1, 1.0 / dt, 0.0, source_coef(it, true, dt))).empty()) return e;
+          if (it == 2) eval_receivers(2);
+        }
+        tn2 = 0;
+        tn1 = 1;
+        tn = 2;
+      }
+      bool first = true;
+      double mult = 0, m1 = 0, m2 = 0;
+      for (int it = std::max(tbeg, 3); it < tend; ++it) {
+        if (!(e = check()).empty()) return e;
+        if (first && it != 3) {
+          tn2 = npre2;
+          tn1 = npre1;
+          tn = it;
+        } else {
+          tn2 = tn1;
+          tn1 = tn;
+          tn = it;
+        }
+        vpre1_[it] = tn1;
+        vpre2_[it] = tn2;
+        if (first) {
+          const double dt = t[it] - t[tn2], dt0 = t[it] - t[tn1], dt1 = t[tn1] - t[tn2];
+          mult = (dt + dt0) / (dt * dt0);
+          m1 = dt / (dt1 * dt0);
+          m2 = -dt0 / (dt * dt1);
+          timed_factor(mult);
+          first = false;
+        }
+        if (!(e = step(it, tn1, tn2, m1, m2, source_coef(it, false, 0.0))).empty()) return e;
+        eval_receivers(it);
+      }
+    }
+  }
+  TRY_CUDA(cudaStreamSynchronize(s_));
+  TRY_CUDA(cudaGetLastError());
+  const int bad = chol_->status(s_);
+  if (bad) return "factorization met a non-positive pivot at column " + std::to_string(bad);
+  pt_.factor_s = tf;
+  pt_.steps_s = now_s() - tstart - tf;
+  return "";
+}
+
+std::string TransientSolve::results(std::vector<double>& eall, std::vector<double>& emf,
+                                    std::vector<double>& ball) {
+  const int nl = tll_ - tlf_ + 1;
+  const size_t rb = (size_t)3 * rop_b_.nrec, re = (size_t)3 * rop_e_.nrec;
+  std::vector<double> vb(nl * rb), ve(nl * re);
+  if (rb) TRY_CUDA(cudaMemcpyAsync(vb.data(), d_vb_, sizeof(double) * vb.size(), cudaMemcpyDeviceToHost, s_));
+  if (re) TRY_CUDA(cudaMemcpyAsync(ve.data(), d_ve_, sizeof(double) * ve.size(), cudaMemcpyDeviceToHost, s_));
+  TRY_CUDA(cudaStreamSynchronize(s_));
+  if (opt_.formulation == 1) {
+    // E-form: receivers hold E and curl E; emf = -curl E, no differencing
+    eall = ve;
+    emf.resize(vb.size());
+    for (size_t i = 0; i < vb.size(); ++i) emf[i] = -vb[i];
+    ball.assign(vb.size(), 0.0);
+    return "";
+  }
+  // A-form: differencing on the device
+  double *d_out_b = nullptr, *d_out_e = nullptr;
+  int *d_v1 = nullptr, *d_v2 = nullptr;
+  std::string e;
+  if (!(e = alloc((void**)&d_out_b, sizeof(double) * std::max<size_t>(vb.size(), 1))).empty()) return e;
+  if (!(e = alloc((void**)&d_out_e, sizeof(double) * std::max<size_t>(ve.size(), 1))).empty()) return e;
+  if (!(e = upload(&d_v1, vpre1_)).empty()) return e;
+  if (!(e = upload(&d_v2, vpre2_)).empty()) return e;
+  launch_time_diff(d_vb_, nl, (int)rb, tlf_, d_time_, d_v1, d_v2, opt_.scheme, 1.0, d_out_b, s_);
+  launch_time_diff(d_ve_, nl, (int)re, tlf_, d_time_, d_v1, d_v2, opt_.scheme, -1.0, d_out_e, s_);
+  launches_ += 2;
+  emf.resize(vb.size());
+  eall.resize(ve.size());
+  if (rb) TRY_CUDA(cudaMemcpyAsync(emf.data(), d_out_b, sizeof(double) * emf.size(), cudaMemcpyDeviceToHost, s_));
+  if (re) TRY_CUDA(cudaMemcpyAsync(eall.data(), d_out_e, sizeof(double) * eall.size(), cudaMemcpyDeviceToHost, s_));
+  TRY_CUDA(cudaStreamSynchronize(s_));
+  TRY_CUDA(cudaGetLastError());
+  ball = vb;
+  return "";
+}
+
+std::string TransientSolve::write_outputs() {
+  const double ta = now_s();
+  std::vector<double> eall, emf, ball;
+  std::string e = results(eall, emf, ball);
+  if (!e.empty()) return e;
+  const int nl = tll_ - tlf_ + 1;
+  const int nb = rop_b_.nrec, ne = rop_e_.nrec;
+  auto header = [](FILE* f, const std::array<double, 3>& p, const char* cols) {
+    fprintf(f, "%d %d\n", (int)p[0], (int)p[1]);
+    fprintf(f, "%.16e %.16e %.16e\n", p[0], p[1], p[2]);
+    fprintf(f, "1\n1 1 1 1\n1\n%s\n", cols);
+  };
+  for (int p = 0; p < npls_; ++p) {
+    char fn[512];
+    // edsall_anom.N: emf (mV) = Edsx * (-1000)
+    snprintf(fn, sizeof fn, "%s/edsall_anom.%d", m_.dir.c_str(), p + 1);
+    FILE* f = fopen(fn, "w");
+    if (!f) return std::string("cannot write ") + fn;
+    for (int i = 0; i < nb; ++i) {
+      if (i < m_.rec_b_ig[p] || i >= m_.rec_b_ig[p + 1]) continue;
+      header(f, m_.rec_b[i], "      t (ms)         Emfx_anom (mV)     Emfy_anom (mV)     Emfz_anom (mV)");
+      for (int l = 0; l < nl; ++l) {
+        const double* v = emf.data() + (size_t)l * 3 * nb;
+        fprintf(f, "%.16e\t%.16e\t%.16e\t%.16e\n", m_.time[tlf_ + l] * 1000, v[i] * (-1000), v[nb + i] * (-1000),
+                v[2 * nb + i] * (-1000));
+      }
+    }
+    if (nb == 0) fprintf(f, " \n");
+    fclose(f);
+    snprintf(fn, sizeof fn, "%s/ball_anom.%d", m_.dir.c_str(), p + 1);
+    f = fopen(fn, "w");
+    if (!f) return std::string("cannot write ") + fn;
+    for (int i = 0; i < nb; ++i) {
+      if (i < m_.rec_b_ig[p] || i >= m_.rec_b_ig[p + 1]) continue;
+      header(f, m_.rec_b[i], "      t (ms)        Bx_anom (mTl)     By_anom (mTl)     Bz_anom (mTl)");
+      for (int l = 0; l < nl; ++l) {
+        const double* v = ball.data() + (size_t)l * 3 * nb;
+        if (opt_.formulation == 1)
+          fprintf(f, "%.16e\t%.16e\t%.16e\t%.16e\n", m_.time[tlf_ + l] * 1000, 0.0, 0.0, 0.0);
+        else
+          fprintf(f, "%.16e\t%.16e\t%.16e\t%.16e\n", m_.time[tlf_ + l] * 1000, v[i] * 1000, v[nb + i] * 1000,
+                  v[2 * nb + i] * 1000);
+      }
+    }
+    if (nb == 0) fprintf(f, " \n");
+    fclose(f);
+    snprintf(fn, sizeof fn, "%s/eall_anom.%d", m_.dir.c_str(), p + 1);
+    f = fopen(fn, "w");
+    if (!f) return std::string("cannot write ") + fn;
+    for (int i = 0; i < ne; ++i) {
+      if (i < m_.rec_e_ig[p] || i >= m_.rec_e_ig[p + 1]) continue;
+      header(f, m_.rec_e[i], "      t (ms)         Ex_anom n (mV)     Ey_anom a (mV)     Ez_anom s (mV)");
+      for (int l = 0; l < nl; ++l) {
+        const double* v = eall.data() + (size_t)l * 3 * ne;
+        fprintf(f, "%.16e\t%.16e\t%.16e\t%.16e\n", m_.time[tlf_ + l] * 1000, v[i] * 1000, v[ne + i] * 1000,
+                v[2 * ne + i] * 1000);
+      }
+    }
+    if (ne == 0) fprintf(f, " \n");
+    fclose(f);
+  }
+  pt_.output_s = now_s() - ta;
+  return "";
+}
+
+}  // namespace tdem

@@ -1,0 +1,109 @@
+// Transient edge-FEM forward solve on one GPU: the B200 counterpart of the
+// reference's CalcNonstat3DLine (CalcNonstat3DLine/TaskSP.cpp:445-711 CalcSP,
+// time_approx.cpp:289-1152 Prepare_To_Schema / Two_Layers_Schema /
+// Three_Layers_Schema, give_out_vec_loop.cpp:240-615 Gather_edsall).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "gpu_cholesky.h"
+#include "model.h"
+#include "receivers.h"
+
+namespace tdem {
+
+struct RunOptions {
+  int formulation = 0;   // 0 = A (vector potential), 1 = E (electric field)
+  int scheme = 2;        // 2 = two-point (backward Euler), 3 = three-point (BDF2)
+  int leaf_size = 128;   // nested-dissection leaf size
+  const volatile int* cancel = nullptr;  // checked between time steps when set
+};
+
+struct PhaseTimes {
+  double setup_s = 0, assemble_s = 0, factor_s = 0, steps_s = 0, output_s = 0;
+  int factorizations = 0, steps = 0;
+};
+
+class TransientSolve {
+ public:
+  TransientSolve();
+  ~TransientSolve();
+
+  // Loads and prepares everything that does not depend on the time step.
+  std::string prepare(const std::string& dir, const RunOptions& opt, cudaStream_t stream);
+  // Runs every time step of every decade.
+  std::string run();
+  // Host copies of the output tables (A-form: E = -dA/dt, emf = dB/dt, B; E-form:
+  // E, emf = -curl E, B = 0) indexed [layer - first][component][receiver].
+  std::string results(std::vector<double>& eall, std::vector<double>& emf, std::vector<double>& ball);
+  // Writes edsall_anom.N, ball_anom.N and eall_anom.N into the model directory.
+  std::string write_outputs();
+
+  const Model& model() const { return m_; }
+  const PhaseTimes& times() const { return pt_; }
+  int first_layer() const { return tlf_; }
+  int last_layer() const { return tll_; }
+  const GpuCholesky& cholesky() const { return *chol_; }
+  int64_t n_interior() const { return n_int_; }
+  int64_t nnz_full() const { return (int64_t)col_.size(); }
+  int kernel_launches() const { return launches_; }
+
+ private:
+  Model m_;
+  RunOptions opt_;
+  cudaStream_t s_ = nullptr;
+  std::unique_ptr<GpuCholesky> chol_;
+  PhaseTimes pt_;
+  int launches_ = 0;
+  int n_ = 0, npls_ = 0, ntime_ = 0;
+  int64_t n_int_ = 0;
+  int tlf_ = 0, tll_ = 0;
+  std::vector<int64_t> rowptr_;
+  std::vector<int> col_;
+  std::vector<int> dec_ig_;
+  std::vector<int> vpre1_, vpre2_;
+  std::vector<double> u0_;
+  ReceiverOperator rop_b_, rop_e_;
+  bool have_source_ = false;
+  // device buffers
+  int64_t* d_rowptr_ = nullptr;
+  int* d_col_ = nullptr;
+  double* d_C_ = nullptr;
+  double* d_B_ = nullptr;
+  int64_t* d_src_ = nullptr;   // interior lower entry -> full CSR index
+  uint8_t* d_diag_ = nullptr;
+  double* d_avals_ = nullptr;
+  uint8_t* d_bound_ = nullptr;
+  double* d_S_ = nullptr;      // source vectors
+  double* d_hist_ = nullptr;   // ring of solution layers
+  double* d_rhs_ = nullptr;
+  int ring_ = 8;
+  // receivers
+  int64_t* d_rb_ptr_ = nullptr; int* d_rb_col_ = nullptr; double* d_rb_val_ = nullptr; int* d_rb_src_ = nullptr;
+  int64_t* d_re_ptr_ = nullptr; int* d_re_col_ = nullptr; double* d_re_val_ = nullptr; int* d_re_src_ = nullptr;
+  double* d_vb_ = nullptr;     // B-type series (layers x rows)
+  double* d_ve_ = nullptr;     // E-type series
+  double* d_time_ = nullptr;
+  int* d_vpre1_ = nullptr;
+  int* d_vpre2_ = nullptr;
+  std::vector<void*> allocs_;
+
+  std::string alloc(void** p, size_t bytes);
+  template <class T>
+  std::string upload(T** d, const std::vector<T>& h);
+  double* layer(int t) { return d_hist_ + (int64_t)(t % ring_) * n_ * npls_; }
+  std::string factor_with(double mult);
+  std::string step(int itime, int t1, int t2, double m1, double m2, double coef);
+  void eval_receivers(int t);
+  double source_coef(int itime, bool two_layer, double dt) const;
+};
+
+// Decade starts: layers where the step length changes (TaskSP.cpp:351-398).
+std::vector<int> decade_starts(const std::vector<double>& time);
+// Layer whose time equals val within a relative 1e-6 (TaskSP.cpp:326-349).
+int find_time_layer(const std::vector<double>& time, double val);
+
+}  // namespace tdem

@@ -1,0 +1,233 @@
+// FEM kernels of the transient solve (see fem_kernels.h).
+//
+// Local matrices of the lowest-order Nedelec brick element.  With hx, hy, hz the
+// brick edges, the reference-cube coordinates in [-1, 1], L0 = (1 - t)/2,
+// L1 = (1 + t)/2 and the basis of local edge j scaled by 2/h along its axis
+// (CalcNonstat3DLine/T_Brick.cpp:741-836: edges 0-3 along x indexed by (y, z)
+// sides, 4-7 along y by (z, x), 8-11 along z by (x, y)), the 1D integrals
+//   M1[a][b] = int La Lb = {2/3, 1/3},  K1[a][b] = int La' Lb' = s_a s_b / 2,
+//   int La = 1,  int La' = s_a  (s_0 = -1, s_1 = +1)
+// give closed forms for the mass matrix C (T_Brick.cpp:311-474) and the curl-curl
+// matrix B (T_Brick.cpp:142-310); they are evaluated entry by entry here.
+#include "fem_kernels.h"
+
+#include <algorithm>
+
+namespace tdem {
+namespace {
+
+__device__ __forceinline__ double m1(int a, int b) { return a == b ? (2.0 / 3.0) : (1.0 / 3.0); }
+__device__ __forceinline__ double k1(int a, int b) { return a == b ? 0.5 : -0.5; }
+__device__ __forceinline__ double sg(int a) { return a ? 1.0 : -1.0; }
+
+// direction (0 = x, 1 = y, 2 = z) and the two side indices (first, second) of local edge j
+__device__ __forceinline__ void edge_desc(int j, int& dir, int& p, int& q) {
+  dir = j >> 2;
+  p = j & 1;          // first side index
+  q = (j >> 1) & 1;   // second side index
+}
+
+// Mass and curl-curl entries between local edges i and j of a brick.
+__device__ void local_entry(int i, int j, double hx, double hy, double hz, double& c, double& b) {
+  int di, ai, bi, dj, aj, bj;
+  edge_desc(i, di, ai, bi);
+  edge_desc(j, dj, aj, bj);
+  const double h[3] = {hx, hy, hz};
+  c = 0.0;
+  b = 0.0;
+  if (di == dj) {
+    // edge along axis d; its sides are the two other axes (u, v) in the order
+    // x: (y, z), y: (z, x), z: (x, y)
+    const int u = (di + 1) % 3, v = (di + 2) % 3;
+    const double scale = h[u] * h[v] / h[di];
+    c = scale * m1(ai, aj) * m1(bi, bj);
+    // curl components along u and v
+    b = scale * (4.0 / (h[v] * h[v]) * m1(ai, aj) * k1(bi, bj) +
+                 4.0 / (h[u] * h[u]) * k1(ai, aj) * m1(bi, bj));
+    return;
+  }
+  // different directions: the curls share the component along the third axis w
+  // (x-edge with y-edge -> z; y with z -> x; x with z -> y)
+  int dA = di, aA = ai, bA = bi, dB = dj, aB = aj, bB = bj;
+  if ((dA + 1) % 3 != dB) {  // order the pair so that dB follows dA cyclically
+    dA = dj; aA = aj; bA = bj;
+    dB = di; aB = ai; bB = bi;
+  }
+  const int w = (dA + 2) % 3;  // shared curl component
+  // Edge along dA has sides (dA+1, dA+2) = (dB, w): index aA on dB, bA on w.
+  // Edge along dB has sides (dB+1, dB+2) = (w, dA): index aB on w, bB on dA.
+  // Integral: -(2 h_w / (h_dA h_dB)) * s(aA) * s(bB) * M1(bA, aB).
+  b = -(2.0 * h[w] / (h[dA] * h[dB])) * sg(aA) * sg(bB) * m1(bA, aB);
+}
+
+__global__ void k_assemble(ElemDev E, const int* __restrict__ elems, int nelems,
+                           const int64_t* __restrict__ rowptr, const int* __restrict__ col,
+                           double* __restrict__ Cval, double* __restrict__ Bval) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= (int64_t)nelems * 144) return;
+  const int e = elems[t / 144];
+  const int ij = (int)(t % 144), i = ij / 12, j = ij % 12;
+  const int gi = E.ed[e * 12 + i], gj = E.ed[e * 12 + j];
+  double c, b;
+  local_entry(i, j, E.h[3 * e], E.h[3 * e + 1], E.h[3 * e + 2], c, b);
+  // locate column gj in row gi
+  int64_t lo = rowptr[gi], hi = rowptr[gi + 1] - 1;
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (col[mid] < gj) lo = mid + 1;
+    else hi = mid;
+  }
+  if (col[lo] != gj) return;  // cannot happen for a pattern built from the same elements
+  Cval[lo] += c * E.sigma[e];
+  Bval[lo] += b * E.inv_mu[e];
+}
+
+__global__ void k_combine(const double* __restrict__ C, const double* __restrict__ B,
+                          const int64_t* __restrict__ src, const uint8_t* __restrict__ diag, int64_t nnz,
+                          double mult, double* __restrict__ out) {
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nnz;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t p = src[q];
+    double v = C[p] * mult + B[p];
+    if (diag[q]) v += v * 1e-12;
+    out[q] = v;
+  }
+}
+
+// One warp per row.
+__global__ void k_history_rhs(const int64_t* __restrict__ rowptr, const int* __restrict__ col,
+                              const double* __restrict__ C, const double* __restrict__ u1,
+                              const double* __restrict__ u2, double m1c, double m2c,
+                              const double* __restrict__ S, double coef, const uint8_t* __restrict__ bound,
+                              int n, int npls, double* __restrict__ rhs) {
+  const int row = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (row >= n) return;
+  if (bound[row]) {
+    for (int p = lane; p < npls; p += 32) rhs[row + (int64_t)p * n] = 0.0;
+    return;
+  }
+  const int64_t b = rowptr[row], e = rowptr[row + 1];
+  for (int p = 0; p < npls; ++p) {
+    const double* a1 = u1 + (int64_t)p * n;
+    const double* a2 = u2 + (int64_t)p * n;
+    double acc = 0.0;
+    for (int64_t q = b + lane; q < e; q += 32) {
+      const int j = col[q];
+      acc = fma(C[q], a1[j] * m1c + a2[j] * m2c, acc);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if (lane == 0) {
+      double v = acc;
+      if (coef != 0.0) v += coef * S[row + (int64_t)p * n];
+      rhs[row + (int64_t)p * n] = v;
+    }
+  }
+}
+
+__global__ void k_receivers(const int64_t* __restrict__ rowptr, const int* __restrict__ col,
+                            const double* __restrict__ val, const int* __restrict__ src, int nrows,
+                            const double* __restrict__ u, int64_t ld, double* __restrict__ out) {
+  const int row = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (row >= nrows) return;
+  const double* x = u + (int64_t)src[row] * ld;
+  double acc = 0.0;
+  for (int64_t q = rowptr[row] + lane; q < rowptr[row + 1]; q += 32) acc = fma(val[q], x[col[q]], acc);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if (lane == 0) out[row] = acc;
+}
+
+__global__ void k_time_diff(const double* __restrict__ F, int nt, int nser, int t0,
+                            const double* __restrict__ time, const int* __restrict__ vpre1,
+                            const int* __restrict__ vpre2, int scheme, double sign, double* __restrict__ out) {
+  const int sidx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sidx >= nser || nt < 3) return;
+  auto val = [&](int layer) { return F[(int64_t)(layer - t0) * nser + sidx]; };
+  auto put = [&](int layer, double v) { out[(int64_t)(layer - t0) * nser + sidx] = sign * v; };
+  const int tl = t0 + nt - 1;
+  int j = t0, j1 = j + 1, j2 = j1 + 1;
+  double f0 = val(j), f1 = val(j1), f2 = val(j2);
+  double dt = time[j2] - time[j], dt1 = time[j1] - time[j], dt0 = time[j2] - time[j1];
+  double mt0 = -(dt + dt1) / (dt1 * dt), mt1 = dt / (dt1 * dt0), mt2 = -dt1 / (dt * dt0);
+  put(j, f0 * mt0 + f1 * mt1 + f2 * mt2);
+  for (;;) {
+    if (scheme == 2) {
+      mt0 = -1.0 / (time[j1] - time[j]);
+      mt1 = 1.0 / (time[j1] - time[j]);
+      mt2 = 0.0;
+    } else {
+      mt0 = (-dt0) / (dt1 * dt);
+      mt1 = -(dt1 - dt0) / (dt1 * dt0);
+      mt2 = (dt1) / (dt * dt0);
+    }
+    put(j1, f0 * mt0 + f1 * mt1 + f2 * mt2);
+    if (j2 == tl) break;
+    ++j2;
+    if (scheme == 2) {
+      j = vpre2[j2];
+      j1 = vpre1[j2];
+    } else {
+      j = j1;
+      j1 = vpre1[j2];
+    }
+    f2 = val(j2);
+    f0 = val(j);
+    f1 = val(j1);
+    dt = time[j2] - time[j];
+    dt1 = time[j1] - time[j];
+    dt0 = time[j2] - time[j1];
+  }
+  if (scheme == 2) {
+    mt0 = 0.0;
+    mt1 = -1.0 / (time[j2] - time[j1]);
+    mt2 = 1.0 / (time[j2] - time[j1]);
+  } else {
+    mt0 = (dt0) / (dt1 * dt);
+    mt1 = -(dt) / (dt1 * dt0);
+    mt2 = (dt + dt0) / (dt * dt0);
+  }
+  put(j2, f0 * mt0 + f1 * mt1 + f2 * mt2);
+}
+
+}  // namespace
+
+void launch_assemble(const ElemDev& e, const int* elems, int nelems, const int64_t* rowptr,
+                     const int* col, double* Cval, double* Bval, cudaStream_t s) {
+  if (nelems <= 0) return;
+  const int64_t work = (int64_t)nelems * 144;
+  k_assemble<<<(unsigned)((work + 255) / 256), 256, 0, s>>>(e, elems, nelems, rowptr, col, Cval, Bval);
+}
+
+void launch_combine(const double* Cval, const double* Bval, const int64_t* src, const uint8_t* diag,
+                    int64_t nnz, double mult, double* out, cudaStream_t s) {
+  if (nnz <= 0) return;
+  const unsigned g = (unsigned)std::min<int64_t>((nnz + 255) / 256, 148 * 64);
+  k_combine<<<g, 256, 0, s>>>(Cval, Bval, src, diag, nnz, mult, out);
+}
+
+void launch_history_rhs(const int64_t* rowptr, const int* col, const double* Cval, const double* u1,
+                        const double* u2, double m1c, double m2c, const double* S, double coef,
+                        const uint8_t* bound, int n, int npls, double* rhs, cudaStream_t s) {
+  const int64_t threads = (int64_t)n * 32;
+  k_history_rhs<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(rowptr, col, Cval, u1, u2, m1c, m2c, S, coef,
+                                                                  bound, n, npls, rhs);
+}
+
+void launch_receivers(const int64_t* rowptr, const int* col, const double* val, const int* src,
+                      int nrows, const double* u, int64_t ld, double* out, cudaStream_t s) {
+  if (nrows <= 0) return;
+  const int64_t threads = (int64_t)nrows * 32;
+  k_receivers<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(rowptr, col, val, src, nrows, u, ld, out);
+}
+
+void launch_time_diff(const double* series, int nt, int nser, int t0, const double* time,
+                      const int* vpre1, const int* vpre2, int scheme, double sign, double* out,
+                      cudaStream_t s) {
+  if (nser <= 0 || nt < 3) return;
+  k_time_diff<<<(nser + 127) / 128, 128, 0, s>>>(series, nt, nser, t0, time, vpre1, vpre2, scheme, sign, out);
+}
+
+}  // namespace tdem

@@ -1,0 +1,82 @@
+// GPU supernodal multifrontal Cholesky (FP64) and multi-RHS triangular solves.
+//
+// Replaces the numeric half of MKL PARDISO in the reference (phase 12 numeric
+// factorization and phase 33 solve, CalcNonstat3DLine/pardiso.cpp:69-120).  The
+// symbolic plan (symbolic.h) is uploaded once per sparsity pattern; factor() may
+// be called again with new values (one factorization per time-step size), and
+// solve() any number of times in between.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "symbolic.h"
+
+namespace tdem {
+
+class GpuCholesky {
+ public:
+  GpuCholesky() = default;
+  ~GpuCholesky();
+  GpuCholesky(const GpuCholesky&) = delete;
+  GpuCholesky& operator=(const GpuCholesky&) = delete;
+
+  // Takes ownership of the analysis and allocates device memory for nrhs_max
+  // right-hand sides.  perm_to_vec[p] is the position in the caller's vectors of
+  // permuted unknown p (lets the solve read and write the caller's natural-order
+  // vectors directly).
+  std::string setup(Symbolic&& sy, const std::vector<int>& perm_to_vec, int nrhs_max,
+                    cudaStream_t stream);
+
+  // Numeric factorization.  d_lower_vals holds the lower-CSR values of the
+  // analysed pattern (device, nnz_lower doubles).  Errors (non-positive pivot)
+  // are reported through status() after the stream is synchronised.
+  void factor(const double* d_lower_vals, cudaStream_t stream);
+
+  // x = A^-1 b for nrhs columns.  b and x are device arrays with leading
+  // dimension ld (positions given by perm_to_vec); x rows not covered by the
+  // system are left untouched.  b and x may alias.
+  void solve(const double* d_b, double* d_x, int64_t ld, int nrhs, cudaStream_t stream);
+
+  // 0 = ok, otherwise 1-based permuted column of the first non-positive pivot.
+  int status(cudaStream_t stream);
+
+  const Symbolic& symbolic() const { return sy_; }
+  size_t device_bytes() const { return bytes_; }
+  int kernel_launches_factor() const { return launches_factor_; }
+  int kernel_launches_solve() const { return launches_solve_; }
+
+ private:
+  Symbolic sy_;
+  int nrhs_max_ = 0;
+  size_t bytes_ = 0;
+  int launches_factor_ = 0, launches_solve_ = 0;
+  // device arrays
+  double* d_L_ = nullptr;
+  double* d_U_ = nullptr;
+  double* d_W_ = nullptr;        // solve front vectors (sum m) x nrhs_max
+  double* d_part_ = nullptr;     // backward partial sums
+  int64_t* d_l_off_ = nullptr;
+  int64_t* d_u_off_ = nullptr;
+  int64_t* d_w_off_ = nullptr;
+  int* d_m_ = nullptr;
+  int* d_k_ = nullptr;
+  int64_t* d_entry_ = nullptr;
+  int64_t* d_rel_off_ = nullptr;
+  int* d_rel_ = nullptr;
+  int64_t* d_rows_off_ = nullptr;
+  int* d_rows_ = nullptr;        // rows_all mapped to caller vector positions
+  int* d_tasks_ = nullptr;
+  int64_t* d_prefix_ = nullptr;
+  int* d_parent_ = nullptr;
+  int* d_c0_ = nullptr;
+  int* d_err_ = nullptr;
+  std::vector<void*> allocs_;
+  template <class T>
+  std::string upload(T** dst, const std::vector<T>& src, cudaStream_t s);
+  std::string alloc(void** p, size_t bytes);
+};
+
+}  // namespace tdem

@@ -1,0 +1,369 @@
+// Readers for the reference's direct-mode input files (see model.h).
+#include "model.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+
+namespace tdem {
+namespace {
+
+constexpr double kMu0Ref = 1.25663706143591729e-6;  // MU_0, CalcNonstat3DLine/vfem_const.h
+
+std::string path(const Model& m, const char* name) { return m.dir + "/" + name; }
+
+bool read_binary(const std::string& fn, void* dst, size_t bytes) {
+  FILE* f = fopen(fn.c_str(), "rb");
+  if (!f) return false;
+  size_t got = fread(dst, 1, bytes, f);
+  fclose(f);
+  return got == bytes;
+}
+
+template <class T>
+bool read_one(const std::string& fn, T& v) {
+  std::ifstream in(fn);
+  if (!in) return false;
+  in >> v;
+  return (bool)in;
+}
+
+}  // namespace
+
+std::string load_model(const std::string& dir, Model& m) {
+  m = Model();
+  m.dir = dir;
+
+  // --- materials: sig3d (index, sigma, sigma0), mu3d (index, mu, mu0) -----------
+  {
+    std::ifstream in(path(m, "sig3d"));
+    if (!in) return "cannot open sig3d";
+    int idx;
+    double a, b;
+    int nmat = 0;
+    std::vector<std::array<double, 3>> rows;
+    while (in >> idx >> a >> b) {
+      nmat = std::max(nmat, idx);
+      rows.push_back({(double)idx, a, b});
+    }
+    if (nmat <= 0) return "sig3d holds no materials";
+    m.sigma.assign(nmat, 0.0);
+    m.sigma0.assign(nmat, 0.0);
+    // the reference reads exactly n_materials records in file order
+    for (int i = 0; i < nmat && i < (int)rows.size(); ++i) {
+      const int k = (int)rows[i][0] - 1;
+      if (k < 0 || k >= nmat) return "sig3d: bad material index";
+      m.sigma[k] = rows[i][1];
+      m.sigma0[k] = rows[i][2];
+    }
+    std::ifstream mu(path(m, "mu3d"));
+    if (!mu) return "cannot open mu3d";
+    m.mu.assign(nmat, kMu0Ref);
+    for (int i = 0; i < nmat; ++i) {
+      double v0, v1;
+      if (!(mu >> idx >> v0 >> v1)) return "mu3d: too few records";
+      if (idx < 1 || idx > nmat) return "mu3d: bad material index";
+      m.mu[idx - 1] = v0 * kMu0Ref;
+    }
+  }
+
+  // --- receivers ---------------------------------------------------------------
+  auto read_recv = [&](const char* name, std::vector<std::array<double, 3>>& out) -> std::string {
+    std::ifstream in(path(m, name));
+    if (!in) return std::string("cannot open ") + name;
+    int n = 0;
+    in >> n;
+    if (!in || n < 0) return std::string("bad receiver count in ") + name;
+    out.resize(n);
+    for (int i = 0; i < n; ++i)
+      if (!(in >> out[i][0] >> out[i][1] >> out[i][2])) return std::string("truncated ") + name;
+    return "";
+  };
+  if (auto e = read_recv("xyzVectorB", m.rec_b); !e.empty()) return e;
+  if (auto e = read_recv("xyzVectorE", m.rec_e); !e.empty()) return e;
+
+  // --- inftry.dat ---------------------------------------------------------------
+  {
+    std::ifstream in(path(m, "inftry.dat"));
+    if (!in) return "cannot open inftry.dat";
+    std::string tok;
+    while (in >> tok) {
+      if (tok == "KUZLOV=") in >> m.n_nodes;
+      else if (tok == "KPAR=") in >> m.n_elem;
+      else if (tok == "KT1=") in >> m.n_bound_nodes;
+    }
+    if (m.n_nodes <= 0 || m.n_elem <= 0) return "inftry.dat: bad sizes";
+  }
+  {
+    std::vector<int32_t> buf((size_t)m.n_elem * 14);
+    if (!read_binary(path(m, "nver.dat"), buf.data(), buf.size() * 4)) return "cannot read nver.dat";
+    m.nver.resize(m.n_elem);
+    for (int e = 0; e < m.n_elem; ++e)
+      for (int j = 0; j < 8; ++j) {
+        const int v = buf[(size_t)e * 14 + j] - 1;
+        if (v < 0 || v >= m.n_nodes) return "nver.dat: node index out of range";
+        m.nver[e][j] = v;
+      }
+    std::vector<int32_t> mat(m.n_elem);
+    if (!read_binary(path(m, "nvkat.dat"), mat.data(), mat.size() * 4)) return "cannot read nvkat.dat";
+    m.nvkat.resize(m.n_elem);
+    for (int e = 0; e < m.n_elem; ++e) {
+      m.nvkat[e] = mat[e] - 1;
+      if (m.nvkat[e] < 0 || m.nvkat[e] >= (int)m.sigma.size()) return "nvkat.dat: material out of range";
+    }
+    std::vector<double> xyz((size_t)m.n_nodes * 3);
+    if (!read_binary(path(m, "xyz.dat"), xyz.data(), xyz.size() * 8)) return "cannot read xyz.dat";
+    m.xyz.resize(m.n_nodes);
+    for (int i = 0; i < m.n_nodes; ++i) m.xyz[i] = {xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]};
+    std::vector<int32_t> l1(m.n_bound_nodes);
+    if (!read_binary(path(m, "l13d.dat"), l1.data(), l1.size() * 4)) return "cannot read l13d.dat";
+    m.l13d.resize(m.n_bound_nodes);
+    for (int i = 0; i < m.n_bound_nodes; ++i) {
+      m.l13d[i] = l1[i] - 1;
+      if (m.l13d[i] < 0 || m.l13d[i] >= m.n_nodes) return "l13d.dat: node out of range";
+    }
+  }
+  {
+    int fd = 0;
+    if (read_one(path(m, "fdirect"), fd)) m.fdirect = fd != 0;
+  }
+
+  // --- edges (time_approx.cpp:243-287) ---------------------------------------------
+  {
+    std::ifstream in(path(m, "tsize3d_.dat"));
+    int j = 0;
+    if (!(in >> j >> m.n_edges) || m.n_edges <= 0) return "tsize3d_.dat: bad edge count";
+    std::vector<int32_t> nfe((size_t)m.n_edges * 2);
+    if (!read_binary(path(m, "nodesforedges.dat"), nfe.data(), nfe.size() * 4))
+      return "cannot read nodesforedges.dat";
+    m.edge_nodes.resize(m.n_edges);
+    for (int e = 0; e < m.n_edges; ++e) {
+      m.edge_nodes[e] = {nfe[2 * e] - 1, nfe[2 * e + 1] - 1};
+      if (m.edge_nodes[e][0] < 0 || m.edge_nodes[e][1] < 0 || m.edge_nodes[e][0] >= m.n_nodes ||
+          m.edge_nodes[e][1] >= m.n_nodes)
+        return "nodesforedges.dat: node out of range";
+    }
+    std::vector<int32_t> ed((size_t)m.n_elem * 25);
+    if (!read_binary(path(m, "edges.dat"), ed.data(), ed.size() * 4)) return "cannot read edges.dat";
+    m.ed.resize(m.n_elem);
+    for (int e = 0; e < m.n_elem; ++e)
+      for (int j = 0; j < 12; ++j) {
+        const int v = ed[(size_t)e * 25 + j] - 1;
+        if (v < 0 || v >= m.n_edges) return "edges.dat: edge index out of range";
+        m.ed[e][j] = v;
+      }
+  }
+  // Dirichlet edges: both end nodes on the boundary (T_Bound_Cond.cpp:58-89)
+  {
+    std::vector<char> bn(m.n_nodes, 0);
+    for (int v : m.l13d) bn[v] = 1;
+    m.edge_bound.assign(m.n_edges, 0);
+    for (int e = 0; e < m.n_edges; ++e)
+      m.edge_bound[e] = bn[m.edge_nodes[e][0]] && bn[m.edge_nodes[e][1]];
+  }
+
+  // --- time grid infite.0 (vec_prep_data.cpp:834-853) -----------------------------
+  {
+    std::ifstream in(path(m, "infite.0"));
+    if (!in) return "cannot open infite.0";
+    in.ignore(1000, '=');
+    int nt = 0;
+    in >> nt;
+    if (!in || nt < 3) return "infite.0: bad time count";
+    for (int k = 0; k < 4; ++k) in.ignore(1000, '\n');
+    m.time.resize(nt);
+    for (int i = 0; i < nt; ++i) {
+      if (!in.good()) return "infite.0: truncated";
+      in >> m.time[i];
+      in.ignore(1000, ';');
+    }
+  }
+  {
+    std::ifstream in(path(m, "timeintervalforprint"));
+    if (!(in >> m.print_left >> m.print_right)) return "cannot read timeintervalforprint";
+  }
+
+  // --- sources / receivers per source (TaskSP.cpp:467-535) --------------------------
+  {
+    std::ifstream in(path(m, "group"));
+    if (!in) return "cannot open group";
+    int ngrp = 0;
+    in >> ngrp;
+    m.npls = 0;
+    for (int i = 0; i < ngrp; ++i) {
+      int j, p1, p2;
+      if (!(in >> j >> p1 >> p2)) return "group: truncated";
+      m.npls += p2 - p1 + 1;
+    }
+    if (m.npls <= 0) return "group: no sources";
+    auto read_ig = [&](const char* name, std::vector<int>& ig, int total) -> std::string {
+      std::ifstream f(path(m, name));
+      if (!f) return std::string("cannot open ") + name;
+      ig.assign(m.npls + 1, 0);
+      for (int i = 0; i < m.npls; ++i) {
+        if (!(f >> ig[i + 1])) return std::string("truncated ") + name;
+        ig[i + 1] += ig[i];
+      }
+      if (ig[m.npls] > total) return std::string(name) + " lists more receivers than the receiver file";
+      return "";
+    };
+    if (auto e = read_ig("recvsb", m.rec_b_ig, (int)m.rec_b.size()); !e.empty()) return e;
+    if (auto e = read_ig("recvse", m.rec_e_ig, (int)m.rec_e.size()); !e.empty()) return e;
+  }
+  {
+    int nn = 0;
+    if (read_one(path(m, "n_neib"), nn)) m.n_neib = nn;
+  }
+
+  // --- direct-mode source (vec_prep_data.cpp:982-1048) ------------------------------
+  if (m.fdirect) {
+    std::ifstream in(path(m, "currentfunction"));
+    if (!in) return "cannot open currentfunction";
+    m.currentfunction.assign(m.time.size(), 0.0);
+    for (size_t i = 0; i < m.time.size(); ++i) {
+      double t;
+      in >> t >> m.currentfunction[i];
+    }
+    int ns = 0;
+    if (read_one(path(m, "nSrsRazb"), ns)) m.n_srs_razb = ns;
+    std::ifstream s(path(m, "sours"));
+    if (!s) return "cannot open sours";
+    m.wires.resize(m.npls);
+    for (int i = 0; i < m.npls; ++i)
+      for (int k = 0; k < 6; ++k)
+        if (!(s >> m.wires[i][k])) return "sours: truncated";
+  }
+  return "";
+}
+
+std::string locate_dipoles(Model& m) {
+  m.dipoles.assign(m.npls, {});
+  if (!m.fdirect || m.n_srs_razb <= 0) return "";
+  const int nd = m.n_srs_razb;
+  struct P { double x, y, z; };
+  std::vector<std::vector<P>> pos(m.npls);
+  for (int i = 0; i < m.npls; ++i) {
+    const auto& w = m.wires[i];
+    const double dx = (w[3] - w[0]) / nd, dy = (w[4] - w[1]) / nd, dz = (w[5] - w[2]) / nd;
+    m.dipoles[i].resize(nd);
+    pos[i].resize(nd);
+    for (int j = 0; j < nd; ++j) {
+      pos[i][j] = {w[0] + (j + 0.5) * dx, w[1] + (j + 0.5) * dy, w[2] + (j + 0.5) * dz};
+      m.dipoles[i][j].dx = dx;
+      m.dipoles[i][j].dy = dy;
+      m.dipoles[i][j].dz = dz;
+    }
+  }
+  const double lo = -1e-2, hi = 1.0 + 1e-2;
+  for (int e = 0; e < m.n_elem; ++e) {
+    double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
+    for (int k = 0; k < 8; ++k)
+      for (int a = 0; a < 3; ++a) {
+        mn[a] = std::min(mn[a], m.xyz[m.nver[e][k]][a]);
+        mx[a] = std::max(mx[a], m.xyz[m.nver[e][k]][a]);
+      }
+    const auto& p0 = m.xyz[m.nver[e][0]];
+    const auto& p7 = m.xyz[m.nver[e][7]];
+    for (int i = 0; i < m.npls; ++i)
+      for (int j = 0; j < nd; ++j) {
+        Dipole& d = m.dipoles[i][j];
+        if (d.elem != -1) continue;
+        const P& p = pos[i][j];
+        if (p.x < mn[0] - 1e-3 || p.x > mx[0] + 1e-3 || p.y < mn[1] - 1e-3 || p.y > mx[1] + 1e-3 ||
+            p.z < mn[2] - 1e-3 || p.z > mx[2] + 1e-3)
+          continue;
+        // local coordinates on the axis-aligned brick spanned by nodes 0 and 7
+        const double l0 = (p.x - p0[0]) / (p7[0] - p0[0]);
+        const double l1 = (p.y - p0[1]) / (p7[1] - p0[1]);
+        const double l2 = (p.z - p0[2]) / (p7[2] - p0[2]);
+        if (l0 > lo && l0 < hi && l1 > lo && l1 < hi && l2 > lo && l2 < hi) {
+          d.elem = e;
+          d.ksi = l0;
+          d.eta = l1;
+          d.zeta = l2;
+        }
+      }
+  }
+  for (int i = 0; i < m.npls; ++i)
+    for (int j = 0; j < nd; ++j)
+      if (m.dipoles[i][j].elem < 0) return "source dipole outside the mesh";
+  return "";
+}
+
+std::string load_initial_field(const Model& m, bool eform, std::vector<double>& u0) {
+  const size_t n = (size_t)m.n_edges, np = (size_t)m.npls;
+  u0.assign(n * np, 0.0);
+  const std::string edge_file = path(m, eform ? "e0.edge" : "a0.edge");
+  {
+    FILE* f = fopen(edge_file.c_str(), "rb");
+    if (f) {
+      size_t got = fread(u0.data(), 8, u0.size(), f);
+      fclose(f);
+      if (got != u0.size()) return "truncated initial edge field";
+      return "";
+    }
+  }
+  const size_t nn = (size_t)m.n_nodes;
+  if (!eform) {
+    std::vector<double> a0(nn * 3 * np);
+    if (!read_binary(path(m, "a0.dat"), a0.data(), a0.size() * 8)) return "cannot read a0.dat";
+    for (size_t p = 0; p < np; ++p)
+      for (size_t e = 0; e < n; ++e) {
+        const int v1 = m.edge_nodes[e][0], v2 = m.edge_nodes[e][1];
+        double axis[3], mid[3], len2 = 0.0, dot = 0.0;
+        for (int j = 0; j < 3; ++j) {
+          axis[j] = m.xyz[v2][j] - m.xyz[v1][j];
+          mid[j] = 0.5 * (a0[v1 * 3 + j + p * nn * 3] + a0[v2 * 3 + j + p * nn * 3]);
+          len2 += axis[j] * axis[j];
+          dot += mid[j] * axis[j];
+        }
+        const double len = std::sqrt(len2);
+        u0[e + p * n] = dot / std::sqrt(len2) * len * 0.5;
+      }
+  } else {
+    std::vector<double> va(nn * np);
+    if (!read_binary(path(m, "v3a.dat"), va.data(), va.size() * 8)) return "cannot read v3a.dat";
+    for (size_t p = 0; p < np; ++p)
+      for (size_t e = 0; e < n; ++e) {
+        const int v1 = m.edge_nodes[e][0], v2 = m.edge_nodes[e][1];
+        double len2 = 0.0;
+        for (int j = 0; j < 3; ++j) {
+          const double a = m.xyz[v2][j] - m.xyz[v1][j];
+          len2 += a * a;
+        }
+        const double len = std::sqrt(len2);
+        const double etan = -(va[v2 + p * nn] - va[v1 + p * nn]) / len;
+        u0[e + p * n] = etan * len * 0.5;
+      }
+  }
+  return "";
+}
+
+void edge_pattern(const Model& m, std::vector<int64_t>& rowptr, std::vector<int>& col) {
+  const int n = m.n_edges;
+  // each edge touches at most 4 elements with 12 edges each
+  std::vector<int64_t> cnt(n + 1, 0);
+  for (int e = 0; e < m.n_elem; ++e)
+    for (int i = 0; i < 12; ++i) cnt[m.ed[e][i] + 1] += 12;
+  for (int i = 0; i < n; ++i) cnt[i + 1] += cnt[i];
+  std::vector<int> tmp(cnt[n]);
+  std::vector<int64_t> fill(cnt.begin(), cnt.end() - 1);
+  for (int e = 0; e < m.n_elem; ++e)
+    for (int i = 0; i < 12; ++i)
+      for (int j = 0; j < 12; ++j) tmp[fill[m.ed[e][i]]++] = m.ed[e][j];
+  rowptr.assign(n + 1, 0);
+  col.clear();
+  col.reserve(cnt[n] / 2);
+  for (int i = 0; i < n; ++i) {
+    auto b = tmp.begin() + cnt[i], en = tmp.begin() + fill[i];
+    std::sort(b, en);
+    auto u = std::unique(b, en);
+    col.insert(col.end(), b, u);
+    rowptr[i + 1] = (int64_t)col.size();
+  }
+}
+
+}  // namespace tdem

@@ -1,0 +1,69 @@
+// Model description and readers for the reference's direct-mode input files.
+//
+// Mirrors the inputs CalcNonstat3DLine reads (CalcNonstat3DLine/vec_prep_data.cpp:83-257,
+// time_approx.cpp:243-287 inputvec, vec_prep_data.cpp:834-853 Read_infite0,
+// TaskSP.cpp:467-597, give_out_vec_loop.cpp:44-73, vec_prep_data.cpp:982-1270
+// LoadAndInitCurrent).  All indices are converted to 0-based on load.
+#pragma once
+#include <array>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace tdem {
+
+constexpr double kMu0 = 4.0e-7 * 3.14159265358979;  // MU_0 of vfem_const.h
+
+struct Dipole {
+  int elem = -1;                 // element holding the dipole
+  double ksi = 0, eta = 0, zeta = 0;  // local coordinates in [0,1]
+  double dx = 0, dy = 0, dz = 0;      // dipole vector (wire length / nSrsRazb)
+};
+
+struct Model {
+  // mesh
+  int n_nodes = 0, n_elem = 0, n_bound_nodes = 0, n_edges = 0;
+  std::vector<std::array<double, 3>> xyz;
+  std::vector<std::array<int, 8>> nver;       // element nodes
+  std::vector<int> nvkat;                     // element material (0-based)
+  std::vector<int> l13d;                      // boundary nodes
+  std::vector<std::array<int, 12>> ed;        // element edges
+  std::vector<std::array<int, 2>> edge_nodes; // edge end nodes (lower, upper)
+  // materials (per material index)
+  std::vector<double> sigma, sigma0, mu;      // mu in H/m
+  // time grid
+  std::vector<double> time;
+  std::vector<double> currentfunction;        // empty when no source file is needed
+  double print_left = 0, print_right = 0;
+  // sources and receivers
+  int npls = 0;
+  std::vector<std::array<double, 6>> wires;   // A(x,y,z), B(x,y,z) per source
+  int n_srs_razb = 500;
+  std::vector<std::vector<Dipole>> dipoles;   // per source
+  std::vector<std::array<double, 3>> rec_b, rec_e;
+  std::vector<int> rec_b_ig, rec_e_ig;        // per-source receiver ranges (npls+1)
+  int n_neib = 5;
+  bool fdirect = false;
+  double eps_reg = 1e-12;
+  // derived
+  std::vector<char> edge_bound;               // Dirichlet edge flag
+  std::string dir;
+};
+
+// Reads every input of one working directory.  Returns "" or an error message.
+std::string load_model(const std::string& dir, Model& m);
+
+// Initial field on the edges (n_edges x npls, column-major): a0.edge / e0.edge
+// when present, else the nodal a0.dat (A-form) / v3a.dat (E-form) projected onto
+// the edges (CalcNonstat3DLine time_approx.cpp:816-889, E-form time_approx.cpp:856-901).
+std::string load_initial_field(const Model& m, bool eform, std::vector<double>& u0);
+
+// Full symmetric CSR pattern over all edges (both triangles, sorted columns).
+void edge_pattern(const Model& m, std::vector<int64_t>& rowptr, std::vector<int>& col);
+
+// Dipole locations: each wire split into n_srs_razb dipoles placed in the first
+// element (in file order) whose box (+-1e-3) holds them with local coordinates in
+// (-0.01, 1.01), as LoadAndInitCurrent does (vec_prep_data.cpp:1050-1183).
+std::string locate_dipoles(Model& m);
+
+}  // namespace tdem

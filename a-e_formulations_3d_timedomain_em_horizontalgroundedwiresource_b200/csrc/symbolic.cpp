@@ -1,0 +1,502 @@
+// Host symbolic analysis: nested-dissection ordering, assembly tree, and the
+// flattened maps / task lists consumed by the GPU factorization and solves.
+#include "symbolic.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <climits>
+#include <numeric>
+
+namespace tdem {
+namespace {
+
+struct Graph {
+  int n = 0;
+  std::vector<int64_t> xadj;
+  std::vector<int> adj;
+};
+
+// Recursive dissection producing fronts in postorder.
+class Dissector {
+ public:
+  Dissector(const Graph& g, const double* xyz, int leaf)
+      : g_(g), xyz_(xyz), leaf_(leaf), mark_(g.n, 0), vis_(g.n, 0) {}
+
+  std::vector<int> order;  // new -> old
+  struct Node { int c0, c1; std::vector<int> kids; };
+  std::vector<Node> nodes;
+
+  int build(std::vector<int>& verts) {
+    if ((int)verts.size() <= leaf_) return emit(verts, {});
+    std::vector<int> L, S, R;
+    int kind = 0;
+    if (xyz_ && split_coords(verts, L, S, R)) kind = 1;
+    if (!kind) kind = split_levels(verts, L, S, R);
+    if (!kind) return emit(verts, {});
+    std::vector<int>().swap(verts);
+    std::vector<int> kids;
+    if (!L.empty()) kids.push_back(build(L));
+    if (!R.empty()) kids.push_back(build(R));
+    return emit(S, std::move(kids));
+  }
+
+ private:
+  const Graph& g_;
+  const double* xyz_;
+  int leaf_;
+  std::vector<int> mark_, vis_;
+  int stamp_ = 0;
+
+  int emit(const std::vector<int>& verts, std::vector<int> kids) {
+    Node nd;
+    nd.c0 = (int)order.size();
+    order.insert(order.end(), verts.begin(), verts.end());
+    nd.c1 = (int)order.size();
+    nd.kids = std::move(kids);
+    nodes.push_back(std::move(nd));
+    return (int)nodes.size() - 1;
+  }
+
+  double c(int v, int a) const { return xyz_[3 * (int64_t)v + a]; }
+
+  // Cut perpendicular to the axis with the most distinct positions, at the most
+  // populated coordinate value inside the central 30 % (a node plane on a
+  // tensor-product mesh).  The separator is the set of vertices at or above the
+  // cut that touch a vertex below it.
+  bool split_coords(const std::vector<int>& verts, std::vector<int>& L, std::vector<int>& S,
+                    std::vector<int>& R) {
+    const size_t nv = verts.size();
+    std::vector<double> vals(nv);
+    int ndist[3];
+    for (int a = 0; a < 3; ++a) {
+      for (size_t i = 0; i < nv; ++i) vals[i] = c(verts[i], a);
+      std::sort(vals.begin(), vals.end());
+      ndist[a] = (int)(std::unique(vals.begin(), vals.end()) - vals.begin());
+    }
+    int axes[3] = {0, 1, 2};
+    std::sort(axes, axes + 3, [&](int a, int b) { return ndist[a] > ndist[b]; });
+    for (int ai = 0; ai < 3; ++ai) {
+      const int a = axes[ai];
+      if (ndist[a] < 3) continue;
+      for (size_t i = 0; i < nv; ++i) vals[i] = c(verts[i], a);
+      std::sort(vals.begin(), vals.end());
+      const size_t q0 = nv * 35 / 100, q1 = std::max(q0 + 1, nv * 65 / 100);
+      double cut = vals[nv / 2];
+      size_t best = 0;
+      double bestd = 1e300;
+      for (size_t i = q0; i < q1;) {
+        size_t j = i;
+        while (j < nv && vals[j] == vals[i]) ++j;
+        const double d = std::fabs(0.5 * (double)(i + j) - 0.5 * (double)nv);
+        if (j - i > best || (j - i == best && d < bestd)) {
+          best = j - i;
+          bestd = d;
+          cut = vals[i];
+        }
+        i = j;
+      }
+      if (cut <= vals.front()) continue;
+      ++stamp_;
+      for (int v : verts) mark_[v] = stamp_;
+      L.clear();
+      S.clear();
+      R.clear();
+      for (int v : verts) {
+        if (c(v, a) < cut) {
+          L.push_back(v);
+          continue;
+        }
+        bool touch = false;
+        for (int64_t p = g_.xadj[v]; p < g_.xadj[v + 1] && !touch; ++p) {
+          const int u = g_.adj[p];
+          touch = (mark_[u] == stamp_ && c(u, a) < cut);
+        }
+        (touch ? S : R).push_back(v);
+      }
+      if (!L.empty() && !S.empty()) return true;
+    }
+    return false;
+  }
+
+  // Level-set bisection from a pseudo-peripheral vertex.  Returns 1 (split with a
+  // separator level), 2 (disconnected: L = one component, R = the rest), 0 (none).
+  int split_levels(const std::vector<int>& verts, std::vector<int>& L, std::vector<int>& S,
+                   std::vector<int>& R) {
+    const int in = ++stamp_;
+    for (int v : verts) mark_[v] = in;
+    std::vector<int> seen, lev;
+    auto bfs = [&](int s) {
+      const int vs = ++stamp_;
+      seen.assign(1, s);
+      lev.clear();
+      vis_[s] = vs;
+      size_t head = 0, level_end = 1;
+      int depth = 0;
+      while (head < seen.size()) {
+        const int v = seen[head++];
+        lev.push_back(depth);
+        for (int64_t p = g_.xadj[v]; p < g_.xadj[v + 1]; ++p) {
+          const int u = g_.adj[p];
+          if (mark_[u] == in && vis_[u] != vs) {
+            vis_[u] = vs;
+            seen.push_back(u);
+          }
+        }
+        if (head == level_end) {
+          ++depth;
+          level_end = seen.size();
+        }
+      }
+    };
+    int s = verts[0];
+    for (int it = 0; it < 2; ++it) {
+      bfs(s);
+      s = seen.back();
+    }
+    bfs(s);
+    if (seen.size() < verts.size()) {
+      const int vs = stamp_;  // the last bfs stamp marks the component
+      L = seen;
+      R.clear();
+      for (int v : verts)
+        if (vis_[v] != vs) R.push_back(v);
+      S.clear();
+      return 2;
+    }
+    const int maxd = lev.back();
+    if (maxd < 2) return 0;
+    int cut = 1;
+    for (size_t i = 0; i < seen.size(); ++i)
+      if (2 * (i + 1) >= seen.size()) {
+        cut = std::max(1, std::min(maxd - 1, lev[i]));
+        break;
+      }
+    L.clear();
+    S.clear();
+    R.clear();
+    for (size_t i = 0; i < seen.size(); ++i)
+      (lev[i] < cut ? L : lev[i] == cut ? S : R).push_back(seen[i]);
+    return 1;
+  }
+};
+
+void add_tasks(Symbolic& sy, TaskList& tl, const std::vector<int>& fr,
+               const std::vector<int64_t>& ctas) {
+  tl.off = (int64_t)sy.tasks.size();
+  tl.pre = (int64_t)sy.task_prefix.size();
+  tl.count = (int)fr.size();
+  int64_t acc = 0;
+  sy.task_prefix.push_back(0);
+  for (size_t i = 0; i < fr.size(); ++i) {
+    sy.tasks.push_back(fr[i]);
+    acc += ctas[i];
+    sy.task_prefix.push_back(acc);
+  }
+  tl.ctas = acc;
+}
+
+inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+}  // namespace
+
+std::string analyse(int n, const int64_t* rowptr, const int* colind, const double* coords,
+                    Symbolic& sy, int leaf_size) {
+  sy = Symbolic();
+  sy.n = n;
+  sy.nnz_lower = rowptr[n];
+  if (n <= 0) return "empty matrix";
+
+  // symmetric adjacency without the diagonal
+  Graph g;
+  g.n = n;
+  std::vector<int64_t> deg(n, 0);
+  for (int i = 0; i < n; ++i)
+    for (int64_t q = rowptr[i]; q < rowptr[i + 1]; ++q) {
+      const int j = colind[q];
+      if (j < 0 || j > i) return "lower-triangle pattern expected (column index out of range)";
+      if (j == i) continue;
+      ++deg[i];
+      ++deg[j];
+    }
+  g.xadj.assign(n + 1, 0);
+  for (int i = 0; i < n; ++i) g.xadj[i + 1] = g.xadj[i] + deg[i];
+  g.adj.resize(g.xadj[n]);
+  {
+    std::vector<int64_t> fill(g.xadj.begin(), g.xadj.end() - 1);
+    for (int i = 0; i < n; ++i)
+      for (int64_t q = rowptr[i]; q < rowptr[i + 1]; ++q) {
+        const int j = colind[q];
+        if (j == i) continue;
+        g.adj[fill[i]++] = j;
+        g.adj[fill[j]++] = i;
+      }
+  }
+
+  // ordering + tree
+  Dissector d(g, coords, std::max(8, leaf_size));
+  {
+    std::vector<int> all(n);
+    std::iota(all.begin(), all.end(), 0);
+    d.build(all);
+  }
+  sy.iperm = d.order;
+  if ((int)sy.iperm.size() != n) return "ordering lost vertices";
+  sy.perm.assign(n, -1);
+  for (int i = 0; i < n; ++i) sy.perm[sy.iperm[i]] = i;
+
+  const int nf = (int)d.nodes.size();
+  sy.fronts.assign(nf, FrontInfo());
+  for (int s = 0; s < nf; ++s) {
+    sy.fronts[s].c0 = d.nodes[s].c0;
+    sy.fronts[s].c1 = d.nodes[s].c1;
+    sy.fronts[s].children = d.nodes[s].kids;
+    for (int ch : d.nodes[s].kids) sy.fronts[ch].parent = s;
+  }
+  std::vector<int> colfront(n);
+  for (int s = 0; s < nf; ++s)
+    for (int cc = sy.fronts[s].c0; cc < sy.fronts[s].c1; ++cc) colfront[cc] = s;
+
+  // row structures (postorder: children first)
+  {
+    std::vector<int> st(n, -1), tmp;
+    for (int s = 0; s < nf; ++s) {
+      FrontInfo& f = sy.fronts[s];
+      tmp.clear();
+      for (int cc = f.c0; cc < f.c1; ++cc) {
+        const int i = sy.iperm[cc];
+        for (int64_t p = g.xadj[i]; p < g.xadj[i + 1]; ++p) {
+          const int r = sy.perm[g.adj[p]];
+          if (r >= f.c1 && st[r] != s) {
+            st[r] = s;
+            tmp.push_back(r);
+          }
+        }
+      }
+      for (int ch : f.children)
+        for (int r : sy.fronts[ch].rows)
+          if (r >= f.c1 && st[r] != s) {
+            st[r] = s;
+            tmp.push_back(r);
+          }
+      std::sort(tmp.begin(), tmp.end());
+      f.rows = tmp;
+      int lev = 0;
+      for (int ch : f.children) lev = std::max(lev, sy.fronts[ch].level + 1);
+      f.level = lev;
+    }
+  }
+
+  // offsets, sizes, stats
+  sy.l_off.resize(nf);
+  sy.u_off.assign(nf, 0);
+  sy.front_m.resize(nf);
+  sy.front_k.resize(nf);
+  sy.front_c0.resize(nf);
+  sy.front_parent.resize(nf);
+  sy.rows_off.resize(nf + 1);
+  sy.wvec_off.resize(nf);
+  int64_t off = 0, woff = 0, roff = 0;
+  for (int s = 0; s < nf; ++s) {
+    const FrontInfo& f = sy.fronts[s];
+    const int64_t m = f.m(), k = f.k();
+    sy.l_off[s] = off;
+    sy.front_m[s] = (int)m;
+    sy.front_k[s] = (int)k;
+    sy.front_c0[s] = f.c0;
+    sy.front_parent[s] = f.parent;
+    sy.wvec_off[s] = woff;
+    sy.rows_off[s] = roff;
+    off += m * k;
+    sy.u_sum += (m - k) * (m - k);
+    woff += m;
+    roff += m;
+    sy.nnz_l += m * k;
+    const double dm = (double)m, dk = (double)k;
+    sy.flops += 2.0 * (dk * dk * dk / 3.0 + (dm - dk) * dk * dk + (dm - dk) * (dm - dk) * dk);
+    sy.max_m = std::max(sy.max_m, (int)m);
+    sy.max_k = std::max(sy.max_k, (int)k);
+  }
+  sy.rows_off[nf] = roff;
+  sy.wvec_elems = woff;
+  sy.rows_all.resize(roff);
+  for (int s = 0; s < nf; ++s) {
+    const FrontInfo& f = sy.fronts[s];
+    int64_t o = sy.rows_off[s];
+    for (int cc = f.c0; cc < f.c1; ++cc) sy.rows_all[o++] = cc;
+    for (int r : f.rows) sy.rows_all[o++] = r;
+  }
+
+  // relative maps child rows -> parent front slots
+  {
+    std::vector<int> pos(n, -1);
+    sy.rel_off.assign(nf + 1, 0);
+    for (int s = 0; s < nf; ++s) sy.rel_off[s + 1] = sy.rel_off[s] + (int64_t)sy.fronts[s].rows.size();
+    sy.rel.assign(sy.rel_off[nf], -1);
+    for (int p = 0; p < nf; ++p) {
+      const FrontInfo& fp = sy.fronts[p];
+      for (int cc = fp.c0; cc < fp.c1; ++cc) pos[cc] = cc - fp.c0;
+      for (size_t t = 0; t < fp.rows.size(); ++t) pos[fp.rows[t]] = fp.k() + (int)t;
+      for (int ch : fp.children) {
+        const FrontInfo& fc = sy.fronts[ch];
+        for (size_t t = 0; t < fc.rows.size(); ++t) {
+          const int r = fc.rows[t];
+          const bool in_parent =
+              (r >= fp.c0 && r < fp.c1) || std::binary_search(fp.rows.begin(), fp.rows.end(), r);
+          if (!in_parent) return "internal error: child row missing from parent front";
+          sy.rel[sy.rel_off[ch] + t] = pos[r];
+        }
+      }
+    }
+    for (int s = 0; s < nf; ++s)
+      if (sy.fronts[s].parent < 0 && !sy.fronts[s].rows.empty())
+        return "internal error: root front with off-diagonal rows";
+  }
+
+  // entry map: lower-CSR entry -> front element
+  {
+    sy.entry_dst.assign(sy.nnz_lower, -1);
+    std::vector<int> pos(n, -1);
+    std::vector<std::vector<int64_t>> per_front(nf);
+    for (int i = 0; i < n; ++i)
+      for (int64_t q = rowptr[i]; q < rowptr[i + 1]; ++q) {
+        const int a = sy.perm[i], b = sy.perm[colind[q]];
+        per_front[colfront[std::min(a, b)]].push_back(q);
+      }
+    for (int s = 0; s < nf; ++s) {
+      const FrontInfo& f = sy.fronts[s];
+      for (int cc = f.c0; cc < f.c1; ++cc) pos[cc] = cc - f.c0;
+      for (size_t t = 0; t < f.rows.size(); ++t) pos[f.rows[t]] = f.k() + (int)t;
+      const int64_t m = f.m();
+      // find the row of q: binary search in rowptr
+      for (int64_t q : per_front[s]) {
+        const int i = (int)(std::upper_bound(rowptr, rowptr + n + 1, q) - rowptr) - 1;
+        const int a = sy.perm[i], b = sy.perm[colind[q]];
+        const int col = std::min(a, b), row = std::max(a, b);
+        const int lr = pos[row], lc = col - f.c0;
+        if (lr < 0 || lc < 0 || lc >= f.k() || lr < lc) return "internal error: entry outside its front";
+        sy.entry_dst[q] = sy.l_off[s] + lr + (int64_t)lc * m;
+      }
+    }
+  }
+
+  // level plans
+  int nlev = 0;
+  for (auto& f : sy.fronts) nlev = std::max(nlev, f.level + 1);
+  sy.levels.assign(nlev, LevelPlan());
+  for (int s = 0; s < nf; ++s) sy.levels[sy.fronts[s].level].fronts.push_back(s);
+  int64_t max_partials = 0;
+  for (int l = 0; l < nlev; ++l) {
+    LevelPlan& lp = sy.levels[l];
+    // extend-add slots: slot j = j-th child of each front at this level; one CTA
+    // per child column block of 8 columns
+    int max_kids = 0;
+    for (int s : lp.fronts) max_kids = std::max(max_kids, (int)sy.fronts[s].children.size());
+    for (int j = 0; j < max_kids; ++j) {
+      std::vector<int> fr;
+      std::vector<int64_t> ct, cv;
+      for (int s : lp.fronts)
+        if ((int)sy.fronts[s].children.size() > j) {
+          const int ch = sy.fronts[s].children[j];
+          const int64_t r = (int64_t)sy.fronts[ch].rows.size();
+          if (r == 0) continue;
+          fr.push_back(ch);
+          ct.push_back(cdiv(r, 8));
+          cv.push_back(cdiv(r, kSolveRows));
+        }
+      TaskList tl, tv;
+      add_tasks(sy, tl, fr, ct);
+      add_tasks(sy, tv, fr, cv);
+      lp.extend_slots.push_back(tl);
+      lp.extend_vec.push_back(tv);
+    }
+    {
+      std::vector<int64_t> ct;
+      for (int s : lp.fronts) ct.push_back(cdiv(sy.front_m[s], kSolveRows));
+      add_tasks(sy, lp.assemble, lp.fronts, ct);
+    }
+    int kmax = 0;
+    for (int s : lp.fronts) kmax = std::max(kmax, sy.front_k[s]);
+    for (int j0 = 0; j0 < kmax; j0 += kPanel) {
+      PanelStep ps;
+      ps.j0 = j0;
+      std::vector<int> fr;
+      std::vector<int64_t> c1, c2, c3, c4;
+      for (int s : lp.fronts) {
+        const int k = sy.front_k[s], m = sy.front_m[s];
+        if (k <= j0) continue;
+        const int j1 = std::min(k, j0 + kPanel);
+        const int64_t below = m - j1;
+        fr.push_back(s);
+        c1.push_back(1);
+        c2.push_back(cdiv(below, kTrsmRows));
+        const int64_t nt = cdiv(below, kTileSyrk);
+        c3.push_back(nt * (nt + 1) / 2);
+        c4.push_back(cdiv(below, kSolveRows));
+      }
+      add_tasks(sy, ps.potrf, fr, c1);
+      add_tasks(sy, ps.trsm, fr, c2);
+      add_tasks(sy, ps.syrk, fr, c3);
+      add_tasks(sy, ps.solve_upd, fr, c4);
+      max_partials = std::max(max_partials, ps.solve_upd.ctas);
+      lp.panels.push_back(ps);
+    }
+  }
+  sy.solve_partials = max_partials * kPanel;
+
+  // Update-block workspace: first-fit plan over the level sequence.  A block is
+  // allocated when its front's level starts and released once the parent's level
+  // has assembled it (children are consumed at the start of the parent's level).
+  {
+    struct Blk { int64_t off, len; };
+    std::vector<Blk> free_list{{0, INT64_MAX / 4}};
+    auto alloc = [&](int64_t len) -> int64_t {
+      len = (len + 31) / 32 * 32;  // 256-byte alignment in FP64
+      for (size_t i = 0; i < free_list.size(); ++i)
+        if (free_list[i].len >= len) {
+          const int64_t o = free_list[i].off;
+          free_list[i].off += len;
+          free_list[i].len -= len;
+          if (free_list[i].len == 0) free_list.erase(free_list.begin() + i);
+          return o;
+        }
+      return -1;
+    };
+    auto release = [&](int64_t o, int64_t len) {
+      len = (len + 31) / 32 * 32;
+      auto it = std::lower_bound(free_list.begin(), free_list.end(), o,
+                                 [](const Blk& b, int64_t v) { return b.off < v; });
+      it = free_list.insert(it, {o, len});
+      // merge with neighbours
+      size_t i = it - free_list.begin();
+      if (i + 1 < free_list.size() && free_list[i].off + free_list[i].len == free_list[i + 1].off) {
+        free_list[i].len += free_list[i + 1].len;
+        free_list.erase(free_list.begin() + i + 1);
+      }
+      if (i > 0 && free_list[i - 1].off + free_list[i - 1].len == free_list[i].off) {
+        free_list[i - 1].len += free_list[i].len;
+        free_list.erase(free_list.begin() + i);
+      }
+    };
+    int64_t peak = 0;
+    for (int l = 0; l < nlev; ++l) {
+      for (int s : sy.levels[l].fronts) {
+        const int64_t r = sy.front_m[s] - sy.front_k[s];
+        if (r == 0) continue;
+        const int64_t o = alloc(r * r);
+        if (o < 0) return "internal error: workspace plan failed";
+        sy.u_off[s] = o;
+        peak = std::max(peak, o + (r * r + 31) / 32 * 32);
+      }
+      for (int s : sy.levels[l].fronts)
+        for (int ch : sy.fronts[s].children) {
+          const int64_t r = sy.front_m[ch] - sy.front_k[ch];
+          if (r > 0) release(sy.u_off[ch], r * r);
+        }
+    }
+    sy.u_elems = peak;
+  }
+  return "";
+}
+
+}  // namespace tdem

@@ -1,0 +1,102 @@
+// Host-side symbolic analysis for the GPU multifrontal Cholesky.
+//
+// Replaces the analysis half of the reference's solver call (MKL PARDISO phase 12,
+// CalcNonstat3DLine/pardiso.cpp:69-111).  The ordering is a nested dissection:
+// coordinate bisection with one-sided vertex separators when unknown positions
+// are known (edge midpoints of the tensor-product mesh: the separators are then
+// exactly the in-plane edges of one node plane), breadth-first level-set
+// bisection otherwise.  The dissection tree is the assembly tree: every leaf
+// block and every separator becomes one front whose pivot columns are
+// contiguous in the new numbering.
+//
+// Everything the numeric phase needs on the device is flattened here:
+//   * front offsets / sizes, entry map (matrix value -> front slot),
+//   * child -> parent relative row maps for extend-add,
+//   * per-level, per-panel task lists for the batched dense kernels,
+//   * per-front row index lists for the triangular solves.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace tdem {
+
+constexpr int kPanel = 64;       // dense panel width of the factorization and solves
+constexpr int kTileSyrk = 64;    // trailing-update tile edge
+constexpr int kTrsmRows = 128;   // rows per CTA of the panel triangular solve
+constexpr int kSolveRows = 256;  // rows per CTA of the solve updates
+
+struct FrontInfo {
+  int c0 = 0, c1 = 0;      // pivot columns [c0, c1) (permuted numbering)
+  int parent = -1;
+  int level = 0;           // height in the assembly tree (leaves = 0)
+  std::vector<int> rows;   // rows below the pivot block (permuted, sorted)
+  std::vector<int> children;
+  int m() const { return (c1 - c0) + (int)rows.size(); }
+  int k() const { return c1 - c0; }
+};
+
+// One batched launch: a list of fronts and the CTA prefix over them.
+struct TaskList {
+  int64_t off = 0;     // offset (in ints) into Symbolic::tasks of the front list
+  int64_t pre = 0;     // offset (in int64) into Symbolic::task_prefix (count+1 entries)
+  int count = 0;       // number of fronts
+  int64_t ctas = 0;    // total CTAs
+};
+
+struct PanelStep {
+  int j0 = 0;          // panel start (fronts with k > j0 take part)
+  TaskList potrf;      // one CTA per front
+  TaskList trsm;       // ceil((m - j1) / kTrsmRows) CTAs per front
+  TaskList syrk;       // triangle of kTileSyrk tiles per front
+  TaskList solve_upd;  // ceil((m - j1) / kSolveRows) CTAs per front (fwd update / bwd partials)
+};
+
+struct LevelPlan {
+  std::vector<int> fronts;             // fronts at this height
+  std::vector<TaskList> extend_slots;  // extend-add launches (one per child slot), 8 columns per CTA
+  std::vector<TaskList> extend_vec;    // solve extend-add per child slot, kSolveRows rows per CTA
+  TaskList assemble;                   // solve: front-vector init, ceil(m / kSolveRows) CTAs each
+  std::vector<PanelStep> panels;
+};
+
+struct Symbolic {
+  int n = 0;                  // unknowns
+  int64_t nnz_lower = 0;      // entries of the analysed lower triangle (incl. diagonal)
+  std::vector<int> perm;      // perm[old] = new
+  std::vector<int> iperm;     // iperm[new] = old
+  std::vector<FrontInfo> fronts;
+  std::vector<LevelPlan> levels;
+
+  // device-bound flat arrays.  A front is stored split: its pivot columns (m x k,
+  // leading dimension m) live in the persistent factor L at l_off; its update
+  // block (r x r, r = m - k, leading dimension r) lives in the update workspace
+  // at u_off from the level it is factored until its parent has assembled it.
+  std::vector<int64_t> l_off;        // offset of each front's m x k block in L
+  std::vector<int64_t> u_off;        // offset of each front's r x r block in the workspace
+  std::vector<int> front_m, front_k, front_c0, front_parent;
+  std::vector<int64_t> entry_dst;    // lower-CSR entry q -> offset in L
+  std::vector<int64_t> rel_off;      // per front: offset of its rel map (rows -> parent slot)
+  std::vector<int> rel;              // concatenated rel maps
+  std::vector<int64_t> rows_off;     // per front: offset of its full row list (k + r entries)
+  std::vector<int> rows_all;         // concatenated [c0..c1) U rows, permuted numbering
+  std::vector<int64_t> wvec_off;     // per front: offset of its m-long solve vector
+  std::vector<int> tasks;            // concatenated task front lists
+  std::vector<int64_t> task_prefix;  // concatenated CTA prefix sums
+
+  int64_t u_elems = 0;        // peak update-workspace size (elements)
+  int64_t u_sum = 0;          // sum of r^2 (workspace without reuse)
+  int64_t wvec_elems = 0;     // sum of m
+  int64_t nnz_l = 0;          // sum of m*k (stored factor entries incl. diagonal blocks)
+  double flops = 0.0;         // factorization flops
+  int max_m = 0, max_k = 0;
+  int64_t solve_partials = 0; // scratch entries per RHS column for backward partial sums
+};
+
+// Analyse the lower triangle (row i holds columns j <= i, diagonal included)
+// of a symmetric n x n matrix.  coords (n x 3) are optional unknown positions.
+// Returns an empty string on success, an error message otherwise.
+std::string analyse(int n, const int64_t* rowptr, const int* colind, const double* coords,
+                    Symbolic& out, int leaf_size = 128);
+
+}  // namespace tdem

@@ -1,0 +1,126 @@
+/*
+ * C-ABI of the B200-native transient edge-FEM forward solve (libtdem_b200.so).
+ *
+ * Plain C types only.  Every entry point returns a tdem_status; the message of
+ * the last failure of a solver object is available from tdem_solver_error().
+ * Calls on one solver object are not thread-safe; separate objects are
+ * independent.  Each solver object owns its device memory and CUDA stream on
+ * the device it was created for.
+ *
+ * Reference interfaces replaced (paths inside the reference project):
+ *   - the process boundary of CalcNonstat3DLine: GeoCalculatorSP runs the
+ *     executable in the Calculations directory
+ *     (CODE/programs to folder Modules/GeoCalculatorSP/GeoCalculatorSP.cpp:1656-1662),
+ *     whose main enters CalcSP
+ *     (.../CalcNonstat3DLine/GeoCalculatorSP.cpp:56, TaskSP.cpp:445-711)
+ *     -> tdem_run_directory / tdem_solver_*;
+ *   - the in-process sparse solver boundary: MKL's pardiso_64 as called by
+ *     pardiso_solver (.../CalcNonstat3DLine/pardiso.cpp:69-126, pardiso.h:25-53)
+ *     -> pardiso_64 / tdem_pardiso_64 below.
+ */
+#ifndef TDEM_B200_H
+#define TDEM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum tdem_status {
+  TDEM_OK = 0,
+  TDEM_ERR_ARGUMENT = 1,  /* bad argument (null pointer, unknown formulation / scheme) */
+  TDEM_ERR_INPUT = 2,     /* missing, truncated or inconsistent input files */
+  TDEM_ERR_CUDA = 3,      /* CUDA runtime error (no device, out of memory, launch failure) */
+  TDEM_ERR_NUMERIC = 4,   /* non-positive pivot: the system is not positive definite */
+  TDEM_ERR_CANCELLED = 5, /* tdem_solver_cancel() was called during tdem_solver_run() */
+  TDEM_ERR_STATE = 6      /* call out of order (e.g. results before run) */
+} tdem_status;
+
+/* formulation: 0 = A (vector potential, CalcNonstat3DLine "A-formulation"),
+ *              1 = E (electric field, "E-formulation").
+ * scheme:      2 = two-point implicit (backward Euler),
+ *              3 = three-point implicit (BDF2). */
+
+/* Drop-in for one run of the reference's CalcNonstat3DLine in `workdir`: reads the
+ * direct-mode input files there, runs the transient on CUDA device `device` and
+ * writes edsall_anom.N, ball_anom.N and eall_anom.N (N = 1-based source index) in
+ * the reference's text format.  errbuf (may be NULL) receives a message on failure.
+ * Replaces: GeoCalculatorSP.cpp:1656-1662 -> CalcNonstat3DLine main -> CalcSP
+ * (TaskSP.cpp:445-711). */
+tdem_status tdem_run_directory(const char* workdir, int formulation, int scheme, int device,
+                               char* errbuf, size_t errlen);
+
+typedef struct tdem_solver tdem_solver;
+
+typedef struct tdem_info {
+  int64_t n_edges;          /* unknowns incl. Dirichlet edges */
+  int64_t n_interior;       /* unknowns of the factorized system */
+  int64_t nnz_matrix;       /* entries of the full symmetric system pattern */
+  int64_t nnz_factor;       /* stored factor entries (dense front blocks) */
+  double factor_flops;      /* flops of one numeric factorization */
+  int64_t device_bytes;     /* device memory held by the factorization */
+  int n_sources;            /* transmitter positions solved together (RHS columns) */
+  int n_times;              /* time layers incl. t0 */
+  int first_layer;          /* first printed layer */
+  int last_layer;           /* last printed layer */
+  int n_rec_b;              /* B / emf receivers */
+  int n_rec_e;              /* E receivers */
+  int factorizations;       /* numeric factorizations done by the last run */
+  int steps;                /* time steps done by the last run */
+  int kernel_launches;      /* kernels launched by the last run */
+  double t_setup_s, t_assemble_s, t_factor_s, t_steps_s, t_output_s;
+} tdem_info;
+
+/* Creates a solver for the model in `workdir` (reads the input files, analyses
+ * the sparsity pattern, assembles the FEM matrices on the device and prepares the
+ * receiver operators).  Replaces Read_data + Prepare_To_Schema
+ * (time_approx.cpp:169-557). */
+tdem_status tdem_solver_create(const char* workdir, int formulation, int scheme, int device,
+                               tdem_solver** out);
+/* Runs all decades / time steps (TaskSP.cpp:628-702, Three_Layers_Schema). */
+tdem_status tdem_solver_run(tdem_solver* s);
+/* Writes the reference output files into the model directory (Gather_edsall,
+ * give_out_vec_loop.cpp:240-615). */
+tdem_status tdem_solver_write_outputs(tdem_solver* s);
+/* Copies the output tables to host arrays of nlayers * 3 * nrec doubles laid out
+ * [layer][component][receiver] (layers first_layer .. last_layer): eall = E (mV),
+ * emf = emf (mV), ball = B (mTl), with the reference's units and signs as written
+ * to the files.  Any pointer may be NULL. */
+tdem_status tdem_solver_results(tdem_solver* s, double* eall, double* emf, double* ball);
+tdem_status tdem_solver_info(const tdem_solver* s, tdem_info* info);
+/* Requests cancellation of a running tdem_solver_run (checked between time steps;
+ * the reference polls a file named "stop", GeoCalculatorSP.cpp:27-39). */
+tdem_status tdem_solver_cancel(tdem_solver* s);
+const char* tdem_solver_error(const tdem_solver* s);
+void tdem_solver_destroy(tdem_solver* s);
+
+/* GPU-backed stand-in for MKL's pardiso_64 with the semantics the reference uses
+ * (pardiso.cpp:69-126): mtype = 2 (real SPD), upper-triangular CSR with 1-based
+ * int64 indices, phase 12 (analysis + numeric factorization; the analysis is
+ * reused while the pattern is unchanged), phase 33 (solve for nrhs column-major
+ * right-hand sides b -> x), phase -1 (release).  The handle lives in pt[0];
+ * maxfct, mnum, perm, iparm and msglvl are accepted and ignored.  *error: 0 ok,
+ * -1 bad input / unsupported phase or mtype, -2 out of memory or CUDA error,
+ * -4 non-positive pivot.  Runs on CUDA device 0 unless TDEM_PARDISO_DEVICE is set. */
+void tdem_pardiso_64(void* pt, const long long* maxfct, const long long* mnum, const long long* mtype,
+                     const long long* phase, const long long* n, const void* a, const long long* ia,
+                     const long long* ja, long long* perm, const long long* nrhs, long long* iparm,
+                     const long long* msglvl, void* b, void* x, long long* error);
+/* Same function under MKL's name, so a maintainer can link the reference's
+ * pardiso_solver against this library unchanged. */
+void pardiso_64(void* pt, const long long* maxfct, const long long* mnum, const long long* mtype,
+                const long long* phase, const long long* n, const void* a, const long long* ia,
+                const long long* ja, long long* perm, const long long* nrhs, long long* iparm,
+                const long long* msglvl, void* b, void* x, long long* error);
+/* MKL threading call made by pardiso_solver::factorize (pardiso.cpp:83); no-op here. */
+void mkl_set_num_threads(int n);
+
+/* Library version string. */
+const char* tdem_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TDEM_B200_H */
