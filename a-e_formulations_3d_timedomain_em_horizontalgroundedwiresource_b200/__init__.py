@@ -66,6 +66,11 @@ class TdemInfo(ctypes.Structure):
         ("t_factor_s", ctypes.c_double),
         ("t_steps_s", ctypes.c_double),
         ("t_output_s", ctypes.c_double),
+        ("run_gpu_ms", ctypes.c_double),
+        ("factor_gpu_ms", ctypes.c_double),
+        ("solve_gpu_ms", ctypes.c_double),
+        ("h2d_bytes", ctypes.c_int64),
+        ("d2h_bytes", ctypes.c_int64),
     ]
 
     def as_dict(self) -> dict:

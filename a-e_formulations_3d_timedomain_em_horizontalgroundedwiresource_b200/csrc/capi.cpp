@@ -119,6 +119,11 @@ tdem_status tdem_solver_info(const tdem_solver* s, tdem_info* info) {
   info->t_steps_s = pt.steps_s;
   info->t_output_s = pt.output_s;
   info->kernel_launches = s->solve.kernel_launches();
+  info->run_gpu_ms = pt.run_gpu_ms;
+  info->factor_gpu_ms = pt.factor_gpu_ms;
+  info->solve_gpu_ms = pt.solve_gpu_ms;
+  info->h2d_bytes = pt.h2d_bytes;
+  info->d2h_bytes = pt.d2h_bytes;
   if (m.n_edges > 0 && s->solve.n_interior() > 0) {
     const tdem::GpuCholesky& c = s->solve.cholesky();
     info->nnz_factor = c.symbolic().nnz_l;

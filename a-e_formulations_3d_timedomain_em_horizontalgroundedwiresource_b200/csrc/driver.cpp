@@ -73,6 +73,8 @@ int find_time_layer(const std::vector<double>& time, double val) {
 TransientSolve::TransientSolve() = default;
 TransientSolve::~TransientSolve() {
   chol_.reset();
+  for (cudaEvent_t& ev : ev_)
+    if (ev) cudaEventDestroy(ev);
   for (void* p : allocs_) cudaFree(p);
 }
 
@@ -89,6 +91,7 @@ std::string TransientSolve::upload(T** d, const std::vector<T>& h) {
   std::string e = alloc((void**)d, h.size() * sizeof(T));
   if (!e.empty()) return e;
   if (!h.empty()) TRY_CUDA(cudaMemcpyAsync(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s_));
+  pt_.h2d_bytes += (int64_t)(h.size() * sizeof(T));
   return "";
 }
 
@@ -221,7 +224,8 @@ std::string TransientSolve::prepare(const std::string& dir, const RunOptions& op
   }
   if (!(e = alloc((void**)&d_hist_, sizeof(double) * (size_t)ring_ * n_ * npls_)).empty()) return e;
   if (!(e = alloc((void**)&d_rhs_, sizeof(double) * (size_t)n_ * npls_)).empty()) return e;
-  TRY_CUDA(cudaMemcpyAsync(layer(0), u0_.data(), sizeof(double) * u0_.size(), cudaMemcpyHostToDevice, s_));
+  if (!(e = upload(&d_u0_, u0_)).empty()) return e;
+  for (cudaEvent_t& ev : ev_) TRY_CUDA(cudaEventCreate(&ev));
   pt_.setup_s = now_s() - t0;
 
   // assembly of sigma*C and B/mu, one launch per element colour
@@ -352,18 +356,31 @@ void TransientSolve::eval_receivers(int t) {
 std::string TransientSolve::run() {
   const double tstart = now_s();
   const std::vector<double>& t = m_.time;
+  pt_.factorizations = 0;
+  pt_.steps = 0;
+  pt_.factor_gpu_ms = pt_.solve_gpu_ms = pt_.run_gpu_ms = 0;
+  launches_ = 0;
+  TRY_CUDA(cudaEventRecord(ev_[0], s_));
+  TRY_CUDA(cudaMemcpyAsync(layer(0), d_u0_, sizeof(double) * u0_.size(), cudaMemcpyDeviceToDevice, s_));
   dec_ig_ = decade_starts(t);
   const int ndec = (int)dec_ig_.size() - 1;
   vpre1_.assign(ntime_, -1);
   vpre2_.assign(ntime_, -1);
   std::string e;
   double tf = 0.0;
+  // factorizations are bracketed by events on the launching stream; their device
+  // time is accumulated once the run has finished
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> fev;
   auto timed_factor = [&](double mult) {
-    cudaStreamSynchronize(s_);
-    const double a = now_s();
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, s_);
+    const double h0 = now_s();
     factor_with(mult);
-    cudaStreamSynchronize(s_);
-    tf += now_s() - a;
+    cudaEventRecord(b, s_);
+    tf += now_s() - h0;
+    fev.push_back({a, b});
   };
   auto check = [&]() -> std::string {
     if (opt_.cancel && *opt_.cancel) return "cancelled";
@@ -461,12 +478,24 @@ std::string TransientSolve::run() {
       }
     }
   }
+  TRY_CUDA(cudaEventRecord(ev_[1], s_));
   TRY_CUDA(cudaStreamSynchronize(s_));
   TRY_CUDA(cudaGetLastError());
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, ev_[0], ev_[1]);
+  pt_.run_gpu_ms = ms;
+  for (auto& pr : fev) {
+    cudaEventElapsedTime(&ms, pr.first, pr.second);
+    pt_.factor_gpu_ms += ms;
+    cudaEventDestroy(pr.first);
+    cudaEventDestroy(pr.second);
+  }
+  pt_.solve_gpu_ms = pt_.run_gpu_ms - pt_.factor_gpu_ms;
   const int bad = chol_->status(s_);
   if (bad) return "factorization met a non-positive pivot at column " + std::to_string(bad);
-  pt_.factor_s = tf;
-  pt_.steps_s = now_s() - tstart - tf;
+  pt_.factor_s = pt_.factor_gpu_ms * 1e-3;
+  pt_.steps_s = now_s() - tstart - pt_.factor_s;
+  (void)tf;
   return "";
 }
 
@@ -478,6 +507,7 @@ std::string TransientSolve::results(std::vector<double>& eall, std::vector<doubl
   if (rb) TRY_CUDA(cudaMemcpyAsync(vb.data(), d_vb_, sizeof(double) * vb.size(), cudaMemcpyDeviceToHost, s_));
   if (re) TRY_CUDA(cudaMemcpyAsync(ve.data(), d_ve_, sizeof(double) * ve.size(), cudaMemcpyDeviceToHost, s_));
   TRY_CUDA(cudaStreamSynchronize(s_));
+  pt_.d2h_bytes += (int64_t)((vb.size() + ve.size()) * sizeof(double));
   if (opt_.formulation == 1) {
     // E-form: receivers hold E and curl E; emf = -curl E, no differencing
     eall = ve;

@@ -24,7 +24,10 @@ struct RunOptions {
 
 struct PhaseTimes {
   double setup_s = 0, assemble_s = 0, factor_s = 0, steps_s = 0, output_s = 0;
+  // device time of the last run() from CUDA events on the solver's stream
+  double run_gpu_ms = 0, factor_gpu_ms = 0, solve_gpu_ms = 0;
   int factorizations = 0, steps = 0;
+  int64_t h2d_bytes = 0, d2h_bytes = 0;   // host<->device traffic of prepare/run/results
 };
 
 class TransientSolve {
@@ -79,6 +82,8 @@ class TransientSolve {
   uint8_t* d_bound_ = nullptr;
   double* d_S_ = nullptr;      // source vectors
   double* d_hist_ = nullptr;   // ring of solution layers
+  double* d_u0_ = nullptr;     // initial field (kept so run() can be repeated)
+  cudaEvent_t ev_[6] = {};
   double* d_rhs_ = nullptr;
   int ring_ = 8;
   // receivers

@@ -389,3 +389,40 @@ def small_model(cells: int = 10, n_dec: int = 3, steps_per_dec: int = 6, sigma: 
     return ModelSpec(x=x, y=y, z=z, layers=[(0.0, sigma), (-60.0, sigma * 0.1)], boxes=boxes,
                      sources=srcs, receivers_b=[rec] * len(srcs), receivers_e=[rec] * len(srcs),
                      times=t, n_srs_razb=100)
+
+
+# ----------------------------------------------------------------------------
+# analytic initial fields (synthetic stand-in for the stationary solve)
+# ----------------------------------------------------------------------------
+MU0 = 1.25663706143591729e-6
+
+
+def write_analytic_initial_field(path: str, spec: ModelSpec, current: float = 1.0, reg: float = 1.0) -> None:
+    """Writes a0.dat (nodal A0 of each straight wire in free space,
+    mu0 I / (4 pi) * integral dl / r) and v3a.dat / v3n.dat (nodal DC potential of
+    the wire's electrode pair on a half-space of the top layer's conductivity).
+    Distances below `reg` metres are clamped to keep the fields finite.  These are
+    smooth synthetic initial conditions with the right shape and scale; the
+    transient's cost does not depend on their values."""
+    Z, Y, X = np.meshgrid(spec.z, spec.y, spec.x, indexing="ij")
+    P = np.stack([X.reshape(-1), Y.reshape(-1), Z.reshape(-1)], 1)
+    sigma = spec.layers[0][1] if spec.layers else 0.01
+    a0 = np.zeros((len(spec.sources), P.shape[0], 3))
+    v = np.zeros((len(spec.sources), P.shape[0]))
+    for k, (A, B) in enumerate(spec.sources):
+        A = np.asarray(A, float)
+        B = np.asarray(B, float)
+        L = np.linalg.norm(B - A)
+        t = (B - A) / L
+        s = (P - A) @ t                      # along-wire coordinate
+        rho2 = np.maximum(np.sum((P - A) ** 2, 1) - s ** 2, reg * reg)
+        ra = np.sqrt(s ** 2 + rho2)
+        rb = np.sqrt((s - L) ** 2 + rho2)
+        pot = MU0 * current / (4 * np.pi) * np.log((ra + s) / (rb + s - L))
+        a0[k] = pot[:, None] * t[None, :]
+        rA = np.maximum(np.linalg.norm(P - A, axis=1), reg)
+        rB = np.maximum(np.linalg.norm(P - B, axis=1), reg)
+        v[k] = current / (2 * np.pi * sigma) * (1.0 / rB - 1.0 / rA)
+    a0.astype("<f8").tofile(os.path.join(path, "a0.dat"))
+    v.astype("<f8").tofile(os.path.join(path, "v3a.dat"))
+    np.zeros_like(v).astype("<f8").tofile(os.path.join(path, "v3n.dat"))

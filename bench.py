@@ -1,0 +1,436 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 transient edge-FEM forward solve.
+
+Metric: forward solves per second (one solve = one transmitter position's whole
+transient: every factorization, every time step, every receiver), on the 80^3
+three-layer-plus-block model with the E-formulation and the three-point (BDF2)
+scheme, 160 steps over 1e-6 .. 1e-1 s (the configuration the headline metric is
+quoted on).  Synthetic inputs are generated by the package's model generator;
+the grounded-wire initial field is the analytic half-space field
+(modelgen.write_analytic_initial_field).
+
+Usage:  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                        [--config c2|c1|c3|c5]
+Multi-GPU (one process per GPU, replicas: every rank solves its own copy of the
+workload, no data-path collective) is launched by torch.distributed.run.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+PKG = "a-e_formulations_3d_timedomain_em_horizontalgroundedwiresource_b200"
+METRIC = "forward solves/s + p50/p99 latency, mixed vs FP64 GPU, ≤1e-5 rel. error"
+
+
+# ---------------------------------------------------------------------------
+# workloads
+# ---------------------------------------------------------------------------
+def make_spec(cfg: str, mg, n_steps_override=None):
+    if cfg == "c1":
+        spec = mg.halfspace_model()
+        return spec, "A", 2, "40^3 half-space, A-form, two-point, 120 steps, 1 wire, 21 receivers"
+    if cfg == "c2":
+        spec = mg.layered_block_model()
+        return spec, "E", 3, "80^3 three-layer + 0.1 S/m block, E-form, BDF2, 160 steps, 1 wire, 21 receivers"
+    if cfg == "c3":
+        spec = mg.layered_block_model(sources=mg.wire_grid_sources())
+        return spec, "A", 3, "80^3 three-layer + block, A-form, BDF2, 160 steps, 32 wires as one n x 32 block"
+    if cfg == "c5":
+        spec = mg.layered_block_model(cells=120, n_dec=10, t_end=1.0)
+        return spec, "A", 3, "120^3-class three-layer model, A-form, BDF2, 200 steps"
+    raise ValueError(cfg)
+
+
+def write_workload(cfg: str, path: str):
+    mg = importlib.import_module(PKG + ".modelgen")
+    spec, form, scheme, desc = make_spec(cfg, mg)
+    info = mg.write_model(path, spec)
+    mg.write_analytic_initial_field(path, spec)
+    return spec, form, scheme, desc, info
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi while running."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.QUERY, "--format=csv,noheader",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                mhz = float(p[1].split()[0])
+                smax = float(p[2].split()[0])
+            except ValueError:
+                continue
+            sm.append(mhz)
+            for n, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": smax, "reasons": ["no samples"]}
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------
+def dist_init(n_gpus: int):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = os.environ.get("TDEM_BENCH_BACKEND", "nccl")
+        dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=1800))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(world, value: float) -> float:
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def shard_units(total: int, world: int, rank: int):
+    """Forward solves assigned to one rank when total solves are spread over world ranks."""
+    base, extra = divmod(total, world)
+    start = rank * base + min(rank, extra)
+    return list(range(start, start + base + (1 if rank < extra else 0)))
+
+
+# ---------------------------------------------------------------------------
+# measurements
+# ---------------------------------------------------------------------------
+def fp64_peak_tflops(device: int) -> float:
+    """Measured cuBLAS DGEMM throughput (8192^3, best of 3) -- the FP64 roofline."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda:%d" % device)
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda:%d" % device)
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(3):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        torch.cuda.synchronize()
+        best = min(best, s.elapsed_time(e) * 1e-3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def measured_peaks() -> dict:
+    p = os.path.join(HERE, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def cpu_baseline(cfg: str, spec, form: str, scheme: int, workdir: str, full_factorizations: int,
+                 full_steps: int, threads: int) -> dict:
+    """Times the reference's own CalcNonstat3DLine (built from source, oracle/_ref)
+    on a bounded sample of the same workload: the same mesh and matrices with the
+    time grid cut to its first 3 steps (one factorization).  The per-call wall
+    times logged by the pardiso_64 stand-in split the run into set-up,
+    factorization and per-step time, which are scaled to the full workload."""
+    sys.path.insert(0, os.path.join(HERE, "oracle"))
+    import run_ref  # noqa: E402  (oracle: baseline leg only)
+    mg = importlib.import_module(PKG + ".modelgen")
+    variant = form + "2"
+    if not run_ref.available("CalcNonstat3DLine_" + variant):
+        return {"value": None, "unit": "forward solves/s", "cores": threads, "kind": "reference",
+                "sample": "unavailable: oracle/_ref not built"}
+    import copy
+    s2 = copy.deepcopy(spec)
+    s2.times = spec.times[:4]
+    s2.print_interval = (float(s2.times[1]), float(s2.times[3]))
+    mg.write_model(workdir, s2)
+    mg.write_analytic_initial_field(workdir, s2)
+    timing = os.path.join(workdir, "pardiso_calls.txt")
+    if os.path.exists(timing):
+        os.unlink(timing)
+    env = run_ref.ref_env(threads)
+    env["TDEM_ORACLE_TIMING"] = timing
+    t0 = time.time()
+    with open(os.path.join(workdir, "ref.log"), "w") as log:
+        subprocess.run([run_ref.binary("CalcNonstat3DLine_" + variant)], cwd=workdir, env=env, stdout=log,
+                       stderr=subprocess.STDOUT, check=True, timeout=3600)
+    wall = time.time() - t0
+    n_big = spec.n_edges
+    fac, sol = [], []
+    first = None
+    last_end = 0.0
+    with open(timing) as f:
+        for line in f:
+            ph, n, nrhs, a, b = line.split()
+            if int(n) != n_big:
+                continue
+            a, b = float(a), float(b)
+            if int(ph) == 12:
+                fac.append(b - a)
+                first = a if first is None else first
+            if int(ph) == 33:
+                sol.append(b - a)
+                last_end = b
+    t_fact = sum(fac) / max(len(fac), 1)
+    steps = len(sol)
+    t_after = (last_end - (first + sum(fac))) if first is not None else 0.0
+    t_step = t_after / max(steps, 1)
+    t_setup = wall - t_fact * len(fac) - t_after
+    full = t_setup + full_factorizations * t_fact + full_steps * t_step
+    return {"value": 1.0 / full, "unit": "forward solves/s", "cores": threads, "kind": "reference",
+            "sample": "reference CalcNonstat3DLine_%s (built from source, CPU FP64 Cholesky stand-in for "
+                      "MKL PARDISO) on the same mesh cut to %d steps: wall %.1f s = set-up %.1f s + "
+                      "%d factorization(s) x %.2f s + %d steps x %.3f s; scaled to %d factorizations + %d "
+                      "steps = %.1f s per forward solve" % (variant, steps, wall, t_setup, len(fac), t_fact,
+                                                            steps, t_step, full_factorizations, full_steps,
+                                                            full)}
+
+
+# ---------------------------------------------------------------------------
+# arms
+# ---------------------------------------------------------------------------
+def run_reference_arm(args, world, rank, local):
+    if rank != 0:
+        return
+    mg = importlib.import_module(PKG + ".modelgen")
+    spec, form, scheme, desc = make_spec(args.config, mg)
+    threads = os.cpu_count() or 1
+    # full-workload counts: one factorization per distinct step length (+1 start-up
+    # factorization for the three-point scheme), one solve per time step
+    ts = spec.times
+    h = [ts[i + 1] - ts[i] for i in range(len(ts) - 1)]
+    distinct = 1 + sum(1 for i in range(1, len(h)) if abs(1 - h[i - 1] / h[i]) > 1e-3)
+    n_fact = distinct + (1 if scheme == 3 else 0)
+    n_steps = len(ts) - 1
+    base = tempfile.mkdtemp(prefix="tdem_ref_")
+    vals = []
+    try:
+        for i in range(args.warmup + args.steps):
+            d = os.path.join(base, "s%d" % i)
+            os.makedirs(d)
+            r = cpu_baseline(args.config, spec, form, scheme, d, n_fact, n_steps, threads)
+            if i >= args.warmup:
+                vals.append(r)
+            shutil.rmtree(d, ignore_errors=True)
+    finally:
+        shutil.rmtree(base, ignore_errors=True)
+    v = sum(x["value"] for x in vals) / len(vals) if vals and vals[0]["value"] else None
+    line = {"metric": METRIC, "value": v, "unit": "forward solves/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": (1000.0 / v) if v else None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": desc, "parallelism": "host cores"},
+            "cpu_baseline": dict(vals[-1]) if vals else None,
+            "e2e": {"value": v, "unit": "forward solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    pkg = importlib.import_module(PKG)
+    torch.cuda.set_device(local)
+    base = tempfile.mkdtemp(prefix="tdem_bench_r%d_" % rank)
+    try:
+        wdir = os.path.join(base, "model")
+        spec, form, scheme, desc, winfo = write_workload(args.config, wdir)
+        solver = pkg.Solver(wdir, form, scheme, device=local)
+        for _ in range(args.warmup):
+            solver.run()
+        # replicas: every rank solves its own copy of the workload
+        units = args.steps
+        sampler = ClockSampler(local)
+        sampler.start()
+        barrier(world)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        gpu_ms = factor_ms = solve_ms = 0.0
+        launches = 0
+        lat = []
+        for _ in range(units):
+            solver.run()
+            inf = solver.info()
+            gpu_ms += inf["run_gpu_ms"]
+            factor_ms += inf["factor_gpu_ms"]
+            solve_ms += inf["solve_gpu_ms"]
+            launches += inf["kernel_launches"]
+            lat.append(inf["run_gpu_ms"])
+        torch.cuda.synchronize()
+        barrier(world)
+        wall = time.perf_counter() - t0
+        clocks = sampler.stop()
+        t_job = max_over_ranks(world, gpu_ms * 1e-3)
+        value = world * units / t_job
+        inf = solver.info()
+        solver.close()
+
+        # e2e through the drop-in C-ABI path: files on the host -> device -> results on the host
+        e2e_steps = max(1, min(args.steps, 2))
+        barrier(world)
+        te = time.perf_counter()
+        h2d = d2h = 0
+        for _ in range(e2e_steps):
+            with pkg.Solver(wdir, form, scheme, device=local) as s:
+                s.run()
+                s.results()
+                ii = s.info()
+                h2d += ii["h2d_bytes"]
+                d2h += ii["d2h_bytes"]
+        torch.cuda.synchronize()
+        t_e2e = max_over_ranks(world, time.perf_counter() - te)
+        e2e = {"value": world * e2e_steps / t_e2e, "unit": "forward solves/s",
+               "h2d_bytes_per_step": h2d // e2e_steps, "d2h_bytes_per_step": d2h // e2e_steps,
+               "path": "tdem_solver_create (reads the input files, analysis, H2D) + run + results (D2H)"}
+
+        if rank == 0:
+            peaks = measured_peaks()
+            fp64 = fp64_peak_tflops(local)
+            n_fact = inf["factorizations"]
+            fac_ms_avg = factor_ms / max(units * n_fact, 1)
+            achieved = inf["factor_flops"] / (fac_ms_avg * 1e-3) / 1e12
+            # per-step HBM roofline of the solve phase: the factor is streamed twice per step
+            steps_per_run = inf["steps"]
+            solve_ms_step = solve_ms / max(units * steps_per_run, 1)
+            solve_bytes = 2.0 * 8.0 * inf["nnz_factor"] + 20.0 * inf["nnz_matrix"]
+            hbm = peaks.get("hbm_gbs")
+            roof = {"bound": "tensor", "kernel": "multifrontal FP64 factorization (dense front updates)",
+                    "achieved": achieved, "peak": fp64, "unit": "TFLOP/s", "frac": achieved / fp64,
+                    "peak_source": "measured on this GPU in bench.py: cuBLAS DGEMM 8192^3 (FP64 has no "
+                                   "entry in MEASURED_PEAKS.json)",
+                    "flops_per_launch": inf["factor_flops"], "avg_launch_ms": fac_ms_avg,
+                    "traffic": None}
+            roof_solve = {"bound": "hbm", "kernel": "per-step RHS + triangular solves",
+                          "achieved": solve_bytes / (solve_ms_step * 1e-3) / 1e9,
+                          "peak": hbm, "unit": "GB/s",
+                          "frac": (solve_bytes / (solve_ms_step * 1e-3) / 1e9 / hbm) if hbm else None,
+                          "bytes_per_step": solve_bytes, "avg_step_ms": solve_ms_step,
+                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if hbm else "fallback 6650"}
+            cpu = None
+            if not args.no_cpu_baseline:
+                d = os.path.join(base, "cpu_sample")
+                os.makedirs(d)
+                try:
+                    cpu = cpu_baseline(args.config, spec, form, scheme, d, n_fact, steps_per_run,
+                                       os.cpu_count() or 1)
+                except Exception as ex:  # the baseline is reported, never required
+                    cpu = {"value": None, "unit": "forward solves/s", "cores": os.cpu_count(),
+                           "kind": "reference", "sample": "failed: %s" % ex}
+            lat.sort()
+            line = {
+                "metric": METRIC,
+                "value": value,
+                "unit": "forward solves/s",
+                "n_gpus": world,
+                "steps": args.steps,
+                "warmup": args.warmup,
+                "ms_per_step": t_job * 1000.0 / units,
+                "higher_is_better": True,
+                "scaling": "weak",
+                "vs_baseline": None,
+                "dtype": "f64",
+                "data": "synthetic",
+                "config": {"workload": desc, "n_edges": winfo["n_edges"], "n_interior": inf["n_interior"],
+                           "nnz_matrix": inf["nnz_matrix"], "nnz_factor": inf["nnz_factor"],
+                           "factorizations_per_solve": n_fact, "steps_per_solve": steps_per_run,
+                           "parallelism": "replicas x%d" % world, "precision": "FP64 factor + FP64 solves",
+                           "l2": "inputs larger than L2 (factor %.1f GB)" % (8e-9 * inf["nnz_factor"])},
+                "latency_ms": {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
+                "phase_ms_per_solve": {"factor": factor_ms / units, "steps": solve_ms / units},
+                "wall_s": wall,
+                "gpu_launches": launches,
+                "clocks": clocks,
+                "roofline": roof,
+                "roofline_solve": roof_solve,
+                "cpu_baseline": cpu,
+                "e2e": e2e,
+            }
+            print(json.dumps(line), flush=True)
+    finally:
+        shutil.rmtree(base, ignore_errors=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c5"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_init(args.gpus)
+    try:
+        if args.impl == "reference":
+            run_reference_arm(args, world, rank, local)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -71,6 +71,10 @@ typedef struct tdem_info {
   int steps;                /* time steps done by the last run */
   int kernel_launches;      /* kernels launched by the last run */
   double t_setup_s, t_assemble_s, t_factor_s, t_steps_s, t_output_s;
+  /* device time of the last tdem_solver_run from CUDA events on the solver's stream */
+  double run_gpu_ms, factor_gpu_ms, solve_gpu_ms;
+  int64_t h2d_bytes;        /* host->device bytes copied so far by this solver */
+  int64_t d2h_bytes;        /* device->host bytes copied so far by this solver */
 } tdem_info;
 
 /* Creates a solver for the model in `workdir` (reads the input files, analyses

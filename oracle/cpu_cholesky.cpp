@@ -528,10 +528,12 @@ int SparseCholesky::factor(const double* val) {
   };
 
   if (nthreads > 1 && !subtrees_.empty()) {
+    // independent subtrees on separate threads, each calling single-threaded BLAS
+    if (g_blas.setnt) g_blas.setnt(1);
     std::atomic<int> aerr{0};
     parallel_for(nthreads, (int)subtrees_.size(), [&](int t) {
       for (int s : subtrees_[t]) {
-        int e = do_front(s, false);
+        int e = do_front(s, g_blas.setnt != nullptr);
         if (e) {
           int zero = 0;
           aerr.compare_exchange_strong(zero, e);
@@ -569,25 +571,32 @@ void SparseCholesky::solve(int nrhs, const double* b, double* x) const {
   std::vector<std::vector<std::pair<int64_t, double>>> deferred(subtrees_.size());
   auto fwd = [&](int s, std::vector<std::pair<int64_t, double>>* defer, int top_c0) {
     const Front& f = fronts[s];
-    const int m = f.m(), k = f.k();
+    const int m = f.m(), k = f.k(), r = m - k;
     const double* Ls = L.data() + f.lofs;
-    for (int r = 0; r < nrhs; ++r) {
-      double* yr = y.data() + (int64_t)r * n;
+    std::vector<double> tmp(r);
+    for (int rr = 0; rr < nrhs; ++rr) {
+      double* yr = y.data() + (int64_t)rr * n;
       double* xs = yr + f.c0;
+      // diagonal block: column-oriented forward substitution
       for (int j = 0; j < k; ++j) {
         const double* lj = Ls + (int64_t)j * m;
         const double v = xs[j] / lj[j];
         xs[j] = v;
         for (int i = j + 1; i < k; ++i) xs[i] -= lj[i] * v;
       }
-      for (size_t t = 0; t < f.rows.size(); ++t) {
-        double acc = 0.0;
-        const int row = k + (int)t;
-        for (int j = 0; j < k; ++j) acc += Ls[row + (int64_t)j * m] * xs[j];
+      // rows below: tmp = L21 * xs, streamed column by column
+      std::fill(tmp.begin(), tmp.end(), 0.0);
+      for (int j = 0; j < k; ++j) {
+        const double* lj = Ls + (int64_t)j * m + k;
+        const double v = xs[j];
+        if (v == 0.0) continue;
+        for (int t = 0; t < r; ++t) tmp[t] += lj[t] * v;
+      }
+      for (int t = 0; t < r; ++t) {
         if (defer && f.rows[t] >= top_c0) {
-          defer->push_back({(int64_t)r * n + f.rows[t], acc});
+          defer->push_back({(int64_t)rr * n + f.rows[t], tmp[t]});
         } else {
-          yr[f.rows[t]] -= acc;
+          yr[f.rows[t]] -= tmp[t];
         }
       }
     }
@@ -596,13 +605,15 @@ void SparseCholesky::solve(int nrhs, const double* b, double* x) const {
     const Front& f = fronts[s];
     const int m = f.m(), k = f.k();
     const double* Ls = L.data() + f.lofs;
+    std::vector<double> tmp(f.rows.size());
     for (int r = 0; r < nrhs; ++r) {
       double* yr = y.data() + (int64_t)r * n;
       double* xs = yr + f.c0;
+      for (size_t t = 0; t < f.rows.size(); ++t) tmp[t] = yr[f.rows[t]];
       for (int j = 0; j < k; ++j) {
-        const double* lj = Ls + (int64_t)j * m;
+        const double* lj = Ls + (int64_t)j * m + k;
         double acc = 0.0;
-        for (size_t t = 0; t < f.rows.size(); ++t) acc += lj[k + t] * yr[f.rows[t]];
+        for (size_t t = 0; t < tmp.size(); ++t) acc += lj[t] * tmp[t];
         xs[j] -= acc;
       }
       for (int j = k - 1; j >= 0; --j) {

@@ -15,6 +15,7 @@
 // the nested-dissection ordering; otherwise a graph ordering is used.  The
 // analysis is reused while the sparsity pattern is unchanged.  TDEM_ORACLE_THREADS
 // sets the thread count (default: all cores).
+#include <chrono>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -71,11 +72,34 @@ int thread_count() {
 }
 }  // namespace
 
+namespace {
+// Optional per-call wall-clock log (TDEM_ORACLE_TIMING=<file>): one line
+// "phase n nrhs t_begin t_end" in seconds since the first call, used to split a
+// reference run into set-up, factorization and per-step time.
+double now_rel() {
+  static const auto t0 = std::chrono::steady_clock::now();
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+struct CallLog {
+  long long phase, n, nrhs;
+  double t0;
+  ~CallLog() {
+    if (const char* f = getenv("TDEM_ORACLE_TIMING")) {
+      if (FILE* fp = fopen(f, "a")) {
+        fprintf(fp, "%lld %lld %lld %.6f %.6f\n", phase, n, nrhs, t0, now_rel());
+        fclose(fp);
+      }
+    }
+  }
+};
+}  // namespace
+
 extern "C" void pardiso_64(void* pt, const int64_t* /*maxfct*/, const int64_t* /*mnum*/,
                            const int64_t* mtype, const int64_t* phase, const int64_t* n,
                            const void* a, const int64_t* ia, const int64_t* ja, int64_t* /*perm*/,
                            const int64_t* nrhs, int64_t* /*iparm*/, const int64_t* /*msglvl*/,
                            void* b, void* x, int64_t* error) {
+  CallLog log_{*phase, *n, nrhs ? *nrhs : 0, now_rel()};
   void** ptv = (void**)pt;
   Handle* h = (Handle*)ptv[0];
   *error = 0;
