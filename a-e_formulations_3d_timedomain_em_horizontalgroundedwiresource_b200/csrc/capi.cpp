@@ -19,6 +19,7 @@ struct tdem_solver {
   int device = 0;
   std::string error;
   volatile int cancel = 0;
+  bool prepared = false;
   bool ran = false;
 };
 
@@ -58,6 +59,7 @@ tdem_status tdem_solver_create(const char* workdir, int formulation, int scheme,
   opt.scheme = scheme;
   opt.cancel = &s->cancel;
   s->error = s->solve.prepare(workdir, opt, s->stream);
+  s->prepared = s->error.empty();
   const tdem_status st = classify(s->error);
   *out = s.release();
   return st;
@@ -65,10 +67,11 @@ tdem_status tdem_solver_create(const char* workdir, int formulation, int scheme,
 
 tdem_status tdem_solver_run(tdem_solver* s) {
   if (!s) return TDEM_ERR_ARGUMENT;
-  if (!s->error.empty() && !s->ran) return TDEM_ERR_STATE;
+  if (!s->prepared) return TDEM_ERR_STATE;
   cudaSetDevice(s->device);
   s->error = s->solve.run();
   s->ran = s->error.empty();
+  s->cancel = 0;  // a cancellation request applies to one run
   return classify(s->error);
 }
 

@@ -1,0 +1,80 @@
+"""GPU parity: the CUDA path through the C-ABI against the reference's own
+CalcNonstat3DLine (golden outputs made by the reference built from source) and
+against the numpy oracle, for all four variants."""
+import os
+
+import numpy as np
+import pytest
+
+import tdem_oracle
+from conftest import FP64_TOL, GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+VARIANTS = ["A2", "A3", "E2", "E3"]
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+@pytest.mark.parametrize("case", ["cube6", "cube8_block", "cube8_two_wires"])
+def test_gpu_matches_reference_goldens(pkg, golden, outs, tmp_path, case, variant):
+    d = str(tmp_path / "gpu")
+    golden.write_case_inputs(case, d)
+    with pkg.Solver(d, variant[0], int(variant[1])) as s:
+        s.run()
+        s.write_outputs()
+        info = s.info()
+    assert info["kernel_launches"] > 0
+    npls = golden.CASES[case].get("n_sources", 1)
+    for o in golden.OUTPUTS:
+        for p in range(1, npls + 1):
+            err = outs.compare_files(os.path.join(d, "%s.%d" % (o, p)),
+                                     os.path.join(GOLDEN, case, "%s_%s.%d" % (variant, o, p)))
+            assert err <= FP64_TOL, (o, p, err)
+
+
+@pytest.mark.parametrize("variant", ["A3", "E2"])
+def test_gpu_matches_numpy_oracle(pkg, mg, outs, tmp_path, variant):
+    spec = mg.small_model(cells=10, n_dec=3, steps_per_dec=5, block=True)
+    a = str(tmp_path / "gpu")
+    b = str(tmp_path / "oracle")
+    for d in (a, b):
+        mg.write_model(d, spec)
+        mg.write_analytic_initial_field(d, spec)
+    with pkg.Solver(a, variant[0], int(variant[1])) as s:
+        s.run()
+        s.write_outputs()
+    tdem_oracle.run(b, variant[0], int(variant[1]))
+    for o in ("eall_anom.1", "edsall_anom.1", "ball_anom.1"):
+        assert outs.compare_files(os.path.join(a, o), os.path.join(b, o)) <= FP64_TOL
+
+
+def test_gpu_matches_reference_binary_at_test_time(pkg, mg, outs, tmp_path):
+    """A model not in the goldens, run through oracle/_ref now (when present)."""
+    import run_ref
+    if not run_ref.available("CalcNonstat3DLine_E3"):
+        pytest.skip("oracle/_ref not built")
+    spec = mg.small_model(cells=12, n_dec=3, steps_per_dec=6, block=True, n_receivers=6)
+    src = str(tmp_path / "src")
+    mg.write_model(src, spec)
+    run_ref.run_stationary(src)
+    for v in ("A2", "E3"):
+        g, r = str(tmp_path / ("g" + v)), str(tmp_path / ("r" + v))
+        run_ref.copy_inputs(src, g)
+        run_ref.copy_inputs(src, r)
+        pkg.run_directory(g, v[0], int(v[1]))
+        run_ref.run_transient(r, v)
+        for o in ("eall_anom.1", "edsall_anom.1", "ball_anom.1"):
+            assert outs.compare_files(os.path.join(g, o), os.path.join(r, o)) <= FP64_TOL
+
+
+def test_drop_in_executable(pkg, golden, outs, tmp_path):
+    """The tdem_calcnonstat3dline executable (one name per reference variant)."""
+    import subprocess
+    d = str(tmp_path / "exe")
+    golden.write_case_inputs("cube8_block", d)
+    link = str(tmp_path / "CalcNonstat3DLine_E3")
+    os.symlink(pkg.EXE_PATH, link)
+    subprocess.run([link], cwd=d, check=True, timeout=300)
+    for o in golden.OUTPUTS:
+        err = outs.compare_files(os.path.join(d, o + ".1"), os.path.join(GOLDEN, "cube8_block", "E3_%s.1" % o))
+        assert err <= FP64_TOL

@@ -1,0 +1,127 @@
+"""Pins of the oracle (test infrastructure) against the reference.
+
+  * element matrices: quadrature of the edge basis vs the reference's closed-form
+    entries (T_Brick.cpp:142-474) and the curl-curl null space;
+  * the numpy restatement of the whole transient vs the golden outputs of the
+    reference's own CalcNonstat3DLine built from source;
+  * the reference build in this checkout (oracle/_ref) reproduces the goldens;
+  * the CPU Cholesky behind the pardiso_64 stand-in vs a dense solve.
+"""
+import ctypes
+import os
+import shutil
+
+import numpy as np
+import pytest
+
+import tdem_oracle
+from conftest import FP64_TOL, GOLDEN, ROOT
+
+
+def closed_form_entries(hx, hy, hz):
+    """Selected entries of the reference's closed-form B and C (T_Brick.cpp:147-174, 316-332)."""
+    mx, my, mz = 2 * hx / (hy * hz), 2 * hy / (hx * hz), 2 * hz / (hx * hy)
+    cx = hy * hz / (2 * hx)
+    return {
+        ("B", 0, 0): 2.0 / 3.0 * (my + mz),
+        ("B", 0, 1): my / 3.0 - 2.0 / 3.0 * mz,
+        ("B", 0, 3): -(my + mz) / 3.0,
+        ("B", 0, 4): -2.0 / 3.0 * mz,
+        ("B", 0, 8): -2.0 / 3.0 * my,
+        ("B", 4, 8): -2.0 / 3.0 * mx,
+        ("B", 8, 11): -(mx + my) / 3.0,
+        ("C", 0, 0): 8.0 / 9.0 * cx,
+        ("C", 0, 1): 4.0 / 9.0 * cx,
+        ("C", 0, 3): 2.0 / 9.0 * cx,
+        ("C", 0, 4): 0.0,
+    }
+
+
+@pytest.mark.parametrize("h", [(1.0, 1.0, 1.0), (10.0, 20.0, 5.0), (3.7, 120.0, 0.8)])
+def test_element_matrices_known_answer(h):
+    B, C = tdem_oracle.local_matrices(np.array(h))
+    for (kind, i, j), v in closed_form_entries(*h).items():
+        got = (B if kind == "B" else C)[i, j]
+        assert abs(got - v) <= 1e-13 * max(1.0, abs(v)), (kind, i, j, got, v)
+    assert np.allclose(B, B.T, rtol=0, atol=1e-13 * abs(B).max())
+    assert np.all(np.linalg.eigvalsh(C) > 0)
+    # gradients of nodal functions lie in the curl-curl null space: edge DOF of
+    # grad(phi) is (phi(upper) - phi(lower)) / 2
+    pairs = [(0, 1), (2, 3), (4, 5), (6, 7), (0, 2), (4, 6), (1, 3), (5, 7), (0, 4), (1, 5), (2, 6), (3, 7)]
+    G = np.zeros((12, 8))
+    for k, (a, b) in enumerate(pairs):
+        G[k, a], G[k, b] = -0.5, 0.5
+    assert np.abs(B @ G).max() <= 1e-12 * abs(B).max()
+
+
+def _golden_case_dir(golden, name, tmp_path):
+    d = str(tmp_path / name)
+    golden.write_case_inputs(name, d)
+    return d
+
+
+@pytest.mark.parametrize("variant", ["A2", "A3", "E2", "E3"])
+@pytest.mark.parametrize("case", ["cube6", "cube8_block", "cube8_two_wires"])
+def test_numpy_oracle_matches_reference_goldens(golden, outs, tmp_path, case, variant):
+    d = _golden_case_dir(golden, case, tmp_path)
+    tdem_oracle.run(d, variant[0], int(variant[1]))
+    npls = golden.CASES[case].get("n_sources", 1)
+    for o in golden.OUTPUTS:
+        for p in range(1, npls + 1):
+            err = outs.compare_files(os.path.join(d, "%s.%d" % (o, p)),
+                                     os.path.join(GOLDEN, case, "%s_%s.%d" % (variant, o, p)))
+            assert err <= FP64_TOL, (o, p, err)
+
+
+def test_reference_build_reproduces_goldens(golden, outs, tmp_path):
+    import run_ref
+    if not run_ref.available("CalcNonstat3DLine_A3"):
+        pytest.skip("oracle/_ref not built")
+    d = _golden_case_dir(golden, "cube8_block", tmp_path)
+    run_ref.run_transient(d, "A3")
+    for o in golden.OUTPUTS:
+        err = outs.compare_files(os.path.join(d, o + ".1"), os.path.join(GOLDEN, "cube8_block", "A3_%s.1" % o))
+        assert err <= FP64_TOL
+
+
+def test_cpu_cholesky_pardiso_stand_in():
+    lib_path = os.path.join(ROOT, "oracle", "_ref", "liboracle.so")
+    if not os.path.exists(lib_path):
+        pytest.skip("oracle library not built")
+    import scipy.sparse as sp
+    lib = ctypes.CDLL(lib_path)
+    n = 700
+    A = sp.random(n, n, density=0.01, random_state=3, format="csr")
+    A = (A + A.T + sp.identity(n) * (abs(A).sum(1).max() + 1.0)).tocsr()
+    U = sp.triu(A).tocsr()
+    U.sort_indices()
+    ia = (U.indptr + 1).astype(np.int64)
+    ja = (U.indices + 1).astype(np.int64)
+    a = U.data.astype(np.float64)
+    pt = np.zeros(64, dtype=np.int64)
+    iparm = np.zeros(64, dtype=np.int64)
+    perm = np.zeros(n, dtype=np.int64)
+    b = np.random.default_rng(0).standard_normal((3, n))
+    x = np.zeros_like(b)
+    err = ctypes.c_longlong(0)
+    P = ctypes.POINTER(ctypes.c_longlong)
+
+    def ll(v):
+        return ctypes.byref(ctypes.c_longlong(v))
+
+    for phase in (12, 33, -1):
+        lib.pardiso_64(pt.ctypes.data_as(ctypes.c_void_p), ll(1), ll(1), ll(2), ll(phase), ll(n),
+                       a.ctypes.data_as(ctypes.c_void_p), ia.ctypes.data_as(P), ja.ctypes.data_as(P),
+                       perm.ctypes.data_as(P), ll(3), iparm.ctypes.data_as(P), ll(0),
+                       b.ctypes.data_as(ctypes.c_void_p), x.ctypes.data_as(ctypes.c_void_p), ctypes.byref(err))
+        assert err.value == 0
+    xr = np.linalg.solve(A.toarray(), b.T).T
+    assert np.abs(x - xr).max() <= 1e-12 * np.abs(xr).max()
+
+
+def test_decade_logic():
+    t = np.concatenate([np.arange(0, 5) * 1.0, 4 + np.arange(1, 5) * 2.0, 12 + np.arange(1, 4) * 4.0])
+    assert tdem_oracle.decade_starts(t) == [0, 5, 9, 12]
+    assert tdem_oracle.find_layer(t, 6.0) == 5
+    assert tdem_oracle.find_layer(t, 0.0) == 0
+    assert tdem_oracle.find_layer(t, 5.5) == -1
