@@ -71,10 +71,23 @@ class TdemInfo(ctypes.Structure):
         ("solve_gpu_ms", ctypes.c_double),
         ("h2d_bytes", ctypes.c_int64),
         ("d2h_bytes", ctypes.c_int64),
+        ("precision", ctypes.c_int),
+        ("refine_iters", ctypes.c_int),
+        ("refine_iters_max", ctypes.c_int),
+        ("refine_worst", ctypes.c_double),
     ]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class TdemOptions(ctypes.Structure):
+    _fields_ = [
+        ("precision", ctypes.c_int),
+        ("refine_tol", ctypes.c_double),
+        ("refine_maxit", ctypes.c_int),
+        ("leaf_size", ctypes.c_int),
+    ]
 
 
 _lib: Optional[ctypes.CDLL] = None
@@ -82,6 +95,7 @@ _lib: Optional[ctypes.CDLL] = None
 EXPORTED = [
     "tdem_run_directory",
     "tdem_solver_create",
+    "tdem_solver_create_ex",
     "tdem_solver_run",
     "tdem_solver_write_outputs",
     "tdem_solver_results",
@@ -92,6 +106,7 @@ EXPORTED = [
     "tdem_pardiso_64",
     "pardiso_64",
     "mkl_set_num_threads",
+    "tdem_residual_norms",
     "tdem_version",
 ]
 
@@ -112,6 +127,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.tdem_solver_create.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                        ctypes.POINTER(P)]
     lib.tdem_solver_create.restype = ctypes.c_int
+    lib.tdem_solver_create_ex.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                          ctypes.POINTER(TdemOptions), ctypes.POINTER(P)]
+    lib.tdem_solver_create_ex.restype = ctypes.c_int
     for name in ("tdem_solver_run", "tdem_solver_write_outputs", "tdem_solver_cancel"):
         getattr(lib, name).argtypes = [P]
         getattr(lib, name).restype = ctypes.c_int
@@ -129,6 +147,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         f = getattr(lib, name)
         f.argtypes = [P, pi, pi, pi, pi, pi, P, pi, pi, pi, pi, pi, pi, P, P, pi]
         f.restype = None
+    lib.tdem_residual_norms.argtypes = [ctypes.c_int, ctypes.c_int64, P, P, P, P, P, ctypes.c_int64,
+                                        ctypes.c_int, P, P]
+    lib.tdem_residual_norms.restype = ctypes.c_int
     _lib = lib
     return lib
 
@@ -152,11 +173,13 @@ def run_directory(workdir: str, formulation="A", scheme: int = 2, device: int = 
 class Solver:
     """A transient forward solve held on one GPU: create -> run -> results / write_outputs."""
 
-    def __init__(self, workdir: str, formulation="A", scheme: int = 2, device: int = 0):
+    def __init__(self, workdir: str, formulation="A", scheme: int = 2, device: int = 0, precision: int = 64,
+                 refine_tol: float = 1e-10, refine_maxit: int = 200, leaf_size: int = 128):
         self._lib = load_library()
         self._h = ctypes.c_void_p()
-        st = self._lib.tdem_solver_create(os.fsencode(workdir), _form(formulation), int(scheme), int(device),
-                                          ctypes.byref(self._h))
+        opts = TdemOptions(int(precision), float(refine_tol), int(refine_maxit), int(leaf_size))
+        st = self._lib.tdem_solver_create_ex(os.fsencode(workdir), _form(formulation), int(scheme), int(device),
+                                             ctypes.byref(opts), ctypes.byref(self._h))
         if st != 0:
             msg = self.error()
             self.close()
@@ -236,3 +259,13 @@ def pardiso_64(handle: np.ndarray, phase: int, a, ia, ja, nrhs: int = 1, b=None,
                    iparm.ctypes.data_as(pi), ll(0), None if b is None else b.ctypes.data,
                    None if x is None else x.ctypes.data, ctypes.byref(err))
     return int(err.value)
+
+
+def residual_norms(device: int, n: int, rowptr: int, col: int, val: int, x: int, b: int, ld: int,
+                   ncols: int, norms: int, stream: int = 0) -> None:
+    """tdem_residual_norms on device pointers (integers, e.g. torch's data_ptr()):
+    norms[2j] = ||b_j - A x_j||, norms[2j+1] = ||b_j|| for the full-CSR matrix A.
+    Queued on `stream` (a cudaStream_t handle, 0 for the default stream)."""
+    st = load_library().tdem_residual_norms(device, n, rowptr, col, val, x, b, ld, ncols, norms, stream)
+    if st != 0:
+        raise TdemError(st, "tdem_residual_norms failed (status %d)" % st)

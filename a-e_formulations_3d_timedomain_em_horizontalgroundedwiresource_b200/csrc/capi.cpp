@@ -19,6 +19,7 @@ struct tdem_solver {
   int device = 0;
   std::string error;
   volatile int cancel = 0;
+  int precision = 64;
   bool prepared = false;
   bool ran = false;
 };
@@ -30,6 +31,7 @@ tdem_status classify(const std::string& e) {
   if (e == "cancelled") return TDEM_ERR_CANCELLED;
   if (e.find("cuda") != std::string::npos || e.find("CUDA") != std::string::npos) return TDEM_ERR_CUDA;
   if (e.find("non-positive pivot") != std::string::npos) return TDEM_ERR_NUMERIC;
+  if (e.find("refinement") != std::string::npos) return TDEM_ERR_NUMERIC;
   return TDEM_ERR_INPUT;
 }
 
@@ -47,6 +49,11 @@ const char* tdem_version(void) { return "tdem-b200 0.1 (sm_100a, FP64 multifront
 
 tdem_status tdem_solver_create(const char* workdir, int formulation, int scheme, int device,
                                tdem_solver** out) {
+  return tdem_solver_create_ex(workdir, formulation, scheme, device, nullptr, out);
+}
+
+tdem_status tdem_solver_create_ex(const char* workdir, int formulation, int scheme, int device,
+                                  const tdem_options* opts, tdem_solver** out) {
   if (!workdir || !out) return TDEM_ERR_ARGUMENT;
   *out = nullptr;
   if ((formulation != 0 && formulation != 1) || (scheme != 2 && scheme != 3)) return TDEM_ERR_ARGUMENT;
@@ -58,6 +65,14 @@ tdem_status tdem_solver_create(const char* workdir, int formulation, int scheme,
   opt.formulation = formulation;
   opt.scheme = scheme;
   opt.cancel = &s->cancel;
+  if (opts) {
+    if (opts->precision) opt.precision = opts->precision;
+    if (opts->refine_tol > 0) opt.refine_tol = opts->refine_tol;
+    if (opts->refine_maxit > 0) opt.refine_maxit = opts->refine_maxit;
+    if (opts->leaf_size > 0) opt.leaf_size = opts->leaf_size;
+  }
+  if (opt.precision != 64 && opt.precision != 32) return TDEM_ERR_ARGUMENT;
+  s->precision = opt.precision;
   s->error = s->solve.prepare(workdir, opt, s->stream);
   s->prepared = s->error.empty();
   const tdem_status st = classify(s->error);
@@ -127,6 +142,10 @@ tdem_status tdem_solver_info(const tdem_solver* s, tdem_info* info) {
   info->solve_gpu_ms = pt.solve_gpu_ms;
   info->h2d_bytes = pt.h2d_bytes;
   info->d2h_bytes = pt.d2h_bytes;
+  info->precision = s->precision;
+  info->refine_iters = pt.refine_iters;
+  info->refine_iters_max = pt.refine_iters_max;
+  info->refine_worst = pt.refine_worst;
   if (m.n_edges > 0 && s->solve.n_interior() > 0) {
     const tdem::GpuCholesky& c = s->solve.cholesky();
     info->nnz_factor = c.symbolic().nnz_l;

@@ -5,6 +5,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include "fem_kernels.h"
@@ -186,9 +187,12 @@ std::string TransientSolve::prepare(const std::string& dir, const RunOptions& op
   if (!e.empty()) return "analysis: " + e;
   std::vector<int> p2v(n_int_);
   for (int64_t p = 0; p < n_int_; ++p) p2v[p] = int_edge[sy.iperm[p]];
+  if (opt.precision != 64 && opt.precision != 32) return "precision must be 64 or 32";
   chol_.reset(new GpuCholesky());
-  e = chol_->setup(std::move(sy), p2v, npls_, s_);
+  if (const char* tc = std::getenv("TDEM_TC_UPDATE")) chol_->set_tensor_core_update(tc[0] != '0');
+  e = chol_->setup(std::move(sy), p2v, npls_, s_, opt.precision == 32 ? 4 : 8);
   if (!e.empty()) return e;
+  if (const char* ps = std::getenv("TDEM_PANEL_SOLVE")) chol_->set_panel_solve(ps[0] == '1');
 
   // device buffers
   if (!(e = upload(&d_rowptr_, rowptr_)).empty()) return e;
@@ -224,6 +228,19 @@ std::string TransientSolve::prepare(const std::string& dir, const RunOptions& op
   }
   if (!(e = alloc((void**)&d_hist_, sizeof(double) * (size_t)ring_ * n_ * npls_)).empty()) return e;
   if (!(e = alloc((void**)&d_rhs_, sizeof(double) * (size_t)n_ * npls_)).empty()) return e;
+  if (!(e = alloc((void**)&d_x_, sizeof(double) * (size_t)n_ * npls_)).empty()) return e;
+  // Dirichlet entries of the solution are never written by the solve: they stay 0
+  TRY_CUDA(cudaMemsetAsync(d_x_, 0, sizeof(double) * (size_t)n_ * npls_, s_));
+  if (opt.precision == 32) {
+    const size_t vb = sizeof(double) * (size_t)n_ * npls_;
+    if (!(e = alloc((void**)&d_A_, sizeof(double) * col_.size())).empty()) return e;
+    for (double** v : {&d_r_, &d_z_, &d_p_, &d_q_})
+      if (!(e = alloc((void**)v, vb)).empty()) return e;
+    TRY_CUDA(cudaMemsetAsync(d_z_, 0, vb, s_));
+    if (!(e = alloc((void**)&d_work_, sizeof(double) * kDotBlocks * npls_)).empty()) return e;
+    for (double** v : {&d_rz_, &d_rzn_, &d_pq_, &d_rr_, &d_bn_})
+      if (!(e = alloc((void**)v, sizeof(double) * npls_)).empty()) return e;
+  }
   if (!(e = upload(&d_u0_, u0_)).empty()) return e;
   for (cudaEvent_t& ev : ev_) TRY_CUDA(cudaEventCreate(&ev));
   pt_.setup_s = now_s() - t0;
@@ -317,6 +334,10 @@ std::string TransientSolve::prepare(const std::string& dir, const RunOptions& op
 
 std::string TransientSolve::factor_with(double mult) {
   launch_combine(d_C_, d_B_, d_src_, d_diag_, (int64_t)chol_->symbolic().nnz_lower, mult, d_avals_, s_);
+  if (opt_.precision == 32) {
+    launch_combine_full(d_rowptr_, d_col_, d_C_, d_B_, d_bound_, n_, mult, d_A_, s_);
+    ++launches_;
+  }
   chol_->factor(d_avals_, s_);
   launches_ += 1 + chol_->kernel_launches_factor();
   ++pt_.factorizations;
@@ -330,11 +351,55 @@ std::string TransientSolve::step(int itime, int t1, int t2, double m1, double m2
   const double* u2 = (t2 >= 0) ? layer(t2) : layer(t1);
   launch_history_rhs(d_rowptr_, d_col_, d_C_, u1, u2, m1, (t2 >= 0) ? m2 : 0.0, d_S_, coef, d_bound_, n_, npls_,
                      d_rhs_, s_);
-  double* x = layer(itime);
-  cudaMemsetAsync(x, 0, sizeof(double) * (size_t)n_ * npls_, s_);
-  chol_->solve(d_rhs_, x, n_, npls_, s_);
+  std::string e = (opt_.precision == 32) ? refine(d_x_) : chol_->solve_graph(d_rhs_, d_x_, n_, npls_, s_);
+  if (!e.empty()) return e;
+  TRY_CUDA(cudaMemcpyAsync(layer(itime), d_x_, sizeof(double) * (size_t)n_ * npls_, cudaMemcpyDeviceToDevice, s_));
   launches_ += 1 + chol_->kernel_launches_solve();
   ++pt_.steps;
+  return "";
+}
+
+// FP64 conjugate gradients on the interior system preconditioned by the FP32
+// factor: x = A^-1 rhs to a relative residual of refine_tol in every column.
+std::string TransientSolve::refine(double* x) {
+  const size_t vb = sizeof(double) * (size_t)n_ * npls_;
+  std::vector<double> rr(npls_), bn(npls_);
+  TRY_CUDA(cudaMemsetAsync(x, 0, vb, s_));
+  TRY_CUDA(cudaMemcpyAsync(d_r_, d_rhs_, vb, cudaMemcpyDeviceToDevice, s_));
+  launch_dots(d_rhs_, d_rhs_, n_, npls_, d_work_, d_bn_, s_);
+  std::string e = chol_->solve_graph(d_r_, d_z_, n_, npls_, s_);
+  if (!e.empty()) return e;
+  TRY_CUDA(cudaMemcpyAsync(d_p_, d_z_, vb, cudaMemcpyDeviceToDevice, s_));
+  launch_dots(d_r_, d_z_, n_, npls_, d_work_, d_rz_, s_);
+  TRY_CUDA(cudaMemcpyAsync(bn.data(), d_bn_, sizeof(double) * npls_, cudaMemcpyDeviceToHost, s_));
+  launches_ += 4 + chol_->kernel_launches_solve();
+  int it = 0;
+  double worst = 0.0;
+  for (it = 1; it <= opt_.refine_maxit; ++it) {
+    launch_spmv(d_rowptr_, d_col_, d_A_, d_p_, n_, npls_, d_q_, s_);
+    launch_dots(d_p_, d_q_, n_, npls_, d_work_, d_pq_, s_);
+    launch_pcg_step(d_rz_, d_pq_, x, d_r_, d_p_, d_q_, n_, npls_, d_work_, d_rr_, s_);
+    TRY_CUDA(cudaMemcpyAsync(rr.data(), d_rr_, sizeof(double) * npls_, cudaMemcpyDeviceToHost, s_));
+    TRY_CUDA(cudaStreamSynchronize(s_));
+    launches_ += 5;
+    bool done = true;
+    worst = 0.0;
+    for (int p = 0; p < npls_; ++p) {
+      const double rel = bn[p] > 0 ? std::sqrt(rr[p] / bn[p]) : 0.0;
+      worst = std::max(worst, rel);
+      done = done && rel <= opt_.refine_tol;
+    }
+    if (done) break;
+    e = chol_->solve_graph(d_r_, d_z_, n_, npls_, s_);
+    if (!e.empty()) return e;
+    launch_dots(d_r_, d_z_, n_, npls_, d_work_, d_rzn_, s_);
+    launch_pcg_dir(d_rz_, d_rzn_, d_z_, d_p_, n_, npls_, s_);
+    launches_ += 4 + chol_->kernel_launches_solve();
+  }
+  if (it > opt_.refine_maxit) return "mixed-precision refinement did not reach the tolerance";
+  pt_.refine_iters += it;
+  pt_.refine_iters_max = std::max(pt_.refine_iters_max, it);
+  pt_.refine_worst = std::max(pt_.refine_worst, worst);
   return "";
 }
 
@@ -358,6 +423,8 @@ std::string TransientSolve::run() {
   const std::vector<double>& t = m_.time;
   pt_.factorizations = 0;
   pt_.steps = 0;
+  pt_.refine_iters = pt_.refine_iters_max = 0;
+  pt_.refine_worst = 0.0;
   pt_.factor_gpu_ms = pt_.solve_gpu_ms = pt_.run_gpu_ms = 0;
   launches_ = 0;
   TRY_CUDA(cudaEventRecord(ev_[0], s_));
@@ -493,6 +560,9 @@ std::string TransientSolve::run() {
   pt_.solve_gpu_ms = pt_.run_gpu_ms - pt_.factor_gpu_ms;
   const int bad = chol_->status(s_);
   if (bad) return "factorization met a non-positive pivot at column " + std::to_string(bad);
+  if (const int ss = chol_->solve_status(s_))
+    return ss == 1 ? "CUDA: a wait of the level triangular solves gave up"
+                   : "CUDA: a wait of the tensor-core update gave up";
   pt_.factor_s = pt_.factor_gpu_ms * 1e-3;
   pt_.steps_s = now_s() - tstart - pt_.factor_s;
   (void)tf;

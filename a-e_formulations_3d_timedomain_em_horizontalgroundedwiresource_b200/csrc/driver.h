@@ -19,6 +19,12 @@ struct RunOptions {
   int formulation = 0;   // 0 = A (vector potential), 1 = E (electric field)
   int scheme = 2;        // 2 = two-point (backward Euler), 3 = three-point (BDF2)
   int leaf_size = 128;   // nested-dissection leaf size
+  // 64: FP64 factor, one direct solve per step.  32: FP32 factor used as the
+  // preconditioner of an FP64 conjugate-gradient solve on the FP64 system, run to
+  // a relative residual of refine_tol in every column.
+  int precision = 64;
+  double refine_tol = 1e-10;
+  int refine_maxit = 200;
   const volatile int* cancel = nullptr;  // checked between time steps when set
 };
 
@@ -28,6 +34,8 @@ struct PhaseTimes {
   double run_gpu_ms = 0, factor_gpu_ms = 0, solve_gpu_ms = 0;
   int factorizations = 0, steps = 0;
   int64_t h2d_bytes = 0, d2h_bytes = 0;   // host<->device traffic of prepare/run/results
+  int refine_iters = 0, refine_iters_max = 0;  // CG iterations of the last run (mixed precision)
+  double refine_worst = 0.0;              // largest final relative residual of the last run
 };
 
 class TransientSolve {
@@ -85,6 +93,12 @@ class TransientSolve {
   double* d_u0_ = nullptr;     // initial field (kept so run() can be repeated)
   cudaEvent_t ev_[6] = {};
   double* d_rhs_ = nullptr;
+  double* d_x_ = nullptr;      // solve output (fixed, so the solve can be replayed as a graph)
+  // mixed precision: FP64 system values and CG work vectors
+  double* d_A_ = nullptr;
+  double *d_r_ = nullptr, *d_z_ = nullptr, *d_p_ = nullptr, *d_q_ = nullptr, *d_work_ = nullptr;
+  double *d_rz_ = nullptr, *d_rzn_ = nullptr, *d_pq_ = nullptr, *d_rr_ = nullptr, *d_bn_ = nullptr;
+  std::string refine(double* x);
   int ring_ = 8;
   // receivers
   int64_t* d_rb_ptr_ = nullptr; int* d_rb_col_ = nullptr; double* d_rb_val_ = nullptr; int* d_rb_src_ = nullptr;

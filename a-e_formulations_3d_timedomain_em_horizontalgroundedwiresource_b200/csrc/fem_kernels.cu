@@ -192,7 +192,144 @@ __global__ void k_time_diff(const double* __restrict__ F, int nt, int nser, int 
   put(j2, f0 * mt0 + f1 * mt1 + f2 * mt2);
 }
 
+__global__ void k_combine_full(const int64_t* __restrict__ rowptr, const int* __restrict__ col,
+                               const double* __restrict__ C, const double* __restrict__ B,
+                               const uint8_t* __restrict__ bound, int n, double mult, double* __restrict__ A) {
+  const int row = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (row >= n) return;
+  const bool brow = bound[row];
+  for (int64_t q = rowptr[row] + lane; q < rowptr[row + 1]; q += 32) {
+    const int j = col[q];
+    double v = C[q] * mult + B[q];
+    if (j == row) v += v * 1e-12;
+    A[q] = (brow || bound[j]) ? 0.0 : v;
+  }
+}
+
+__global__ void k_spmv(const int64_t* __restrict__ rowptr, const int* __restrict__ col,
+                       const double* __restrict__ A, const double* __restrict__ x, int n, int npls,
+                       double* __restrict__ y) {
+  const int row = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (row >= n) return;
+  const int64_t b = rowptr[row], e = rowptr[row + 1];
+  for (int p = 0; p < npls; ++p) {
+    const double* xp = x + (int64_t)p * n;
+    double acc = 0.0;
+    for (int64_t q = b + lane; q < e; q += 32) acc = fma(A[q], xp[col[q]], acc);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if (lane == 0) y[row + (int64_t)p * n] = acc;
+  }
+}
+
+// Block partial sums of a . b per column into work[col * kDotBlocks + block].
+__device__ __forceinline__ void block_reduce_store(double v, double* out) {
+  __shared__ double red[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    v = (lane < (int)(blockDim.x >> 5)) ? red[lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) *out = v;
+  }
+  __syncthreads();
+}
+
+__global__ void k_dot_partial(const double* __restrict__ a, const double* __restrict__ b, int n, int npls,
+                              double* __restrict__ work) {
+  for (int p = 0; p < npls; ++p) {
+    const double* ap = a + (int64_t)p * n;
+    const double* bp = b + (int64_t)p * n;
+    double v = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+      v = fma(ap[i], bp[i], v);
+    block_reduce_store(v, work + (int64_t)p * kDotBlocks + blockIdx.x);
+  }
+}
+
+__global__ void k_dot_final(const double* __restrict__ work, int npls, double* __restrict__ out) {
+  const int p = blockIdx.x;
+  double v = 0.0;
+  for (int i = threadIdx.x; i < kDotBlocks; i += blockDim.x) v += work[(int64_t)p * kDotBlocks + i];
+  __shared__ double red[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    if (p < npls) out[p] = t;
+  }
+}
+
+__global__ void k_pcg_step(const double* __restrict__ rz, const double* __restrict__ pq, double* __restrict__ x,
+                           double* __restrict__ r, const double* __restrict__ p, const double* __restrict__ q, int n,
+                           int npls, double* __restrict__ work) {
+  for (int c = 0; c < npls; ++c) {
+    const double alpha = (pq[c] != 0.0) ? rz[c] / pq[c] : 0.0;
+    const int64_t o = (int64_t)c * n;
+    double v = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+      x[o + i] = fma(alpha, p[o + i], x[o + i]);
+      const double ri = fma(-alpha, q[o + i], r[o + i]);
+      r[o + i] = ri;
+      v = fma(ri, ri, v);
+    }
+    block_reduce_store(v, work + (int64_t)c * kDotBlocks + blockIdx.x);
+  }
+}
+
+__global__ void k_pcg_dir(double* __restrict__ rz, const double* __restrict__ rz_new, const double* __restrict__ z,
+                          double* __restrict__ p, int n, int npls) {
+  for (int c = 0; c < npls; ++c) {
+    const double beta = (rz[c] != 0.0) ? rz_new[c] / rz[c] : 0.0;
+    const int64_t o = (int64_t)c * n;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+      p[o + i] = fma(beta, p[o + i], z[o + i]);
+  }
+}
+
+__global__ void k_copy_scalars(double* __restrict__ dst, const double* __restrict__ src, int n) {
+  if (threadIdx.x < n) dst[threadIdx.x] = src[threadIdx.x];
+}
+
 }  // namespace
+
+void launch_combine_full(const int64_t* rowptr, const int* col, const double* Cval, const double* Bval,
+                         const uint8_t* bound, int n, double mult, double* Aval, cudaStream_t s) {
+  const int64_t threads = (int64_t)n * 32;
+  k_combine_full<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(rowptr, col, Cval, Bval, bound, n, mult, Aval);
+}
+
+void launch_spmv(const int64_t* rowptr, const int* col, const double* Aval, const double* x, int n, int npls,
+                 double* y, cudaStream_t s) {
+  const int64_t threads = (int64_t)n * 32;
+  k_spmv<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(rowptr, col, Aval, x, n, npls, y);
+}
+
+void launch_dots(const double* a, const double* b, int n, int npls, double* work, double* out, cudaStream_t s) {
+  k_dot_partial<<<kDotBlocks, 256, 0, s>>>(a, b, n, npls, work);
+  k_dot_final<<<npls, 256, 0, s>>>(work, npls, out);
+}
+
+void launch_pcg_step(const double* rz, const double* pq, double* x, double* r, const double* p, const double* q,
+                     int n, int npls, double* work, double* rr, cudaStream_t s) {
+  k_pcg_step<<<kDotBlocks, 256, 0, s>>>(rz, pq, x, r, p, q, n, npls, work);
+  k_dot_final<<<npls, 256, 0, s>>>(work, npls, rr);
+}
+
+void launch_pcg_dir(double* rz, const double* rz_new, const double* z, double* p, int n, int npls, cudaStream_t s) {
+  k_pcg_dir<<<kDotBlocks, 256, 0, s>>>(rz, rz_new, z, p, n, npls);
+  k_copy_scalars<<<1, 64, 0, s>>>(rz, rz_new, npls);
+}
 
 void launch_assemble(const ElemDev& e, const int* elems, int nelems, const int64_t* rowptr,
                      const int* col, double* Cval, double* Bval, cudaStream_t s) {

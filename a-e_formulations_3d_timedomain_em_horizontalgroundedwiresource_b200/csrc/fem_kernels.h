@@ -38,6 +38,28 @@ void launch_history_rhs(const int64_t* rowptr, const int* col, const double* Cva
 void launch_receivers(const int64_t* rowptr, const int* col, const double* val, const int* src,
                       int nrows, const double* u, int64_t ld, double* out, cudaStream_t s);
 
+// A = mult * C + B on every entry of the full CSR, with the diagonal scaled by
+// (1 + 1e-12); rows and columns of Dirichlet edges are left out (their values
+// are set to 0), so A restricted to the interior equals the factorized matrix.
+void launch_combine_full(const int64_t* rowptr, const int* col, const double* Cval, const double* Bval,
+                         const uint8_t* bound, int n, double mult, double* Aval, cudaStream_t s);
+
+// y = A x for npls columns (leading dimension n).
+void launch_spmv(const int64_t* rowptr, const int* col, const double* Aval, const double* x, int n, int npls,
+                 double* y, cudaStream_t s);
+
+// Per-column dot products out[p] = sum_i a[i,p] b[i,p] (deterministic two-pass
+// reduction; `work` holds kDotBlocks * npls doubles).
+constexpr int kDotBlocks = 296;
+void launch_dots(const double* a, const double* b, int n, int npls, double* work, double* out, cudaStream_t s);
+
+// Preconditioned-CG vector updates with per-column scalars held on the device:
+//   pcg_step:  alpha = rz / pq;  x += alpha p;  r -= alpha q;  rr = r . r
+//   pcg_dir:   beta = rz_new / rz;  p = z + beta p;  rz = rz_new
+void launch_pcg_step(const double* rz, const double* pq, double* x, double* r, const double* p, const double* q,
+                     int n, int npls, double* work, double* rr, cudaStream_t s);
+void launch_pcg_dir(double* rz, const double* rz_new, const double* z, double* p, int n, int npls, cudaStream_t s);
+
 // Time differencing of receiver series (CalcNonstat3DLine/give_out_vec_loop.cpp:240-615,
 // 3-point variant CalcNonstat3DLine (3-point)/give_out_vec_loop.cpp).  series is
 // nt x nser (time-major); vpre1 / vpre2 give the earlier layers used at each layer

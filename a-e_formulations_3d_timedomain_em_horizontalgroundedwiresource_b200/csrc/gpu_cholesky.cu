@@ -1,5 +1,7 @@
-// GPU multifrontal Cholesky (FP64): batched dense front kernels driven level by
-// level and panel by panel from the host plan in symbolic.h.
+// GPU multifrontal Cholesky: batched dense front kernels driven level by level
+// and panel by panel from the host plan in symbolic.h.  Kernels are templated on
+// the factor's value type (FP64, or FP32 for the mixed-precision path); the
+// caller's right-hand sides and solutions are always FP64.
 //
 // Layout in HBM
 //   L   persistent factor; front s owns an m x k column-major block (ld = m) at l_off[s]
@@ -9,10 +11,19 @@
 // Every kernel receives a task list (fronts + CTA prefix sums) and finds its
 // front by binary search over the prefix, so one launch covers every front of a
 // level that takes part in the current panel.
+//
+// Factorization per level: zero the update blocks, extend-add the children,
+// then for each 64-wide inner panel [j0, j1): Cholesky of the diagonal block,
+// triangular solve of the rows below, rank-64 update of the rest of the 256-wide
+// outer panel [J0, J1); at the end of each outer panel one rank-(J1 - J0) update
+// of the whole trailing matrix on 128 x 128 register-blocked tiles.
 #include "gpu_cholesky.h"
 
 #include <algorithm>
 #include <cstdio>
+#include <type_traits>
+
+#include "tc_update.h"
 
 namespace tdem {
 namespace {
@@ -37,41 +48,45 @@ struct Fronts {
 };
 
 // Element (i, c), i >= c, of a split front.
-__device__ __forceinline__ double* felem(double* L, double* U, int64_t lo, int64_t uo, int m, int k,
-                                         int i, int c) {
+template <class T>
+__device__ __forceinline__ T* felem(T* L, T* U, int64_t lo, int64_t uo, int m, int k, int i, int c) {
   return (c < k) ? L + lo + i + (int64_t)c * m : U + uo + (i - k) + (int64_t)(c - k) * (m - k);
 }
+
+__device__ __forceinline__ double tsqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float tsqrt(float x) { return sqrtf(x); }
 
 // ---------------------------------------------------------------------------
 // factorization kernels
 // ---------------------------------------------------------------------------
-__global__ void k_scatter_entries(double* __restrict__ L, const int64_t* __restrict__ dst,
+template <class T>
+__global__ void k_scatter_entries(T* __restrict__ L, const int64_t* __restrict__ dst,
                                   const double* __restrict__ val, int64_t nnz) {
   for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nnz;
        q += (int64_t)gridDim.x * blockDim.x)
-    L[dst[q]] = val[q];
+    L[dst[q]] = (T)val[q];
 }
 
-// Zero the update blocks of the fronts of one level (kSolveRows columns per CTA).
-__global__ void k_zero_u(double* __restrict__ U, Fronts f, const int* __restrict__ fronts,
+template <class T>
+__global__ void k_zero_u(T* __restrict__ U, Fronts f, const int* __restrict__ fronts,
                          const int64_t* __restrict__ prefix, int count) {
   const int idx = find_task(prefix, count, blockIdx.x);
   const int s = fronts[idx];
   const int m = f.m[s], k = f.k[s], r = m - k;
   const int64_t t = blockIdx.x - prefix[idx];
   const int c0 = (int)t * kSolveRows, c1 = min(r, c0 + kSolveRows);
-  double* u = U + f.u_off[s];
+  T* u = U + f.u_off[s];
   for (int c = c0; c < c1; ++c)
-    for (int i = threadIdx.x; i < r; i += blockDim.x) u[i + (int64_t)c * r] = 0.0;
+    for (int i = threadIdx.x; i < r; i += blockDim.x) u[i + (int64_t)c * r] = (T)0;
 }
 
 // Extend-add of the children's update blocks into their parents (one child per
 // parent per launch, so no two CTAs write the same parent element).  One warp
 // per child column, 8 columns per CTA.
-__global__ void k_extend_add(double* __restrict__ L, double* __restrict__ U, Fronts f,
-                             const int* __restrict__ parent, const int64_t* __restrict__ rel_off,
-                             const int* __restrict__ rel, const int* __restrict__ kids,
-                             const int64_t* __restrict__ prefix, int count) {
+template <class T>
+__global__ void k_extend_add(T* __restrict__ L, T* __restrict__ U, Fronts f, const int* __restrict__ parent,
+                             const int64_t* __restrict__ rel_off, const int* __restrict__ rel,
+                             const int* __restrict__ kids, const int64_t* __restrict__ prefix, int count) {
   const int idx = find_task(prefix, count, blockIdx.x);
   const int c = kids[idx];
   const int p = parent[c];
@@ -79,41 +94,39 @@ __global__ void k_extend_add(double* __restrict__ L, double* __restrict__ U, Fro
   const int mp = f.m[p], kp = f.k[p];
   const int64_t lo = f.l_off[p], uo = f.u_off[p];
   const int* rl = rel + rel_off[c];
-  const double* uc = U + f.u_off[c];
+  const T* uc = U + f.u_off[c];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int b = (int)(blockIdx.x - prefix[idx]) * 8 + warp;
   if (b >= rc) return;
   const int pc = rl[b];
-  for (int a = b + lane; a < rc; a += 32) {
-    const int pr = rl[a];
-    *felem(L, U, lo, uo, mp, kp, pr, pc) += uc[a + (int64_t)b * rc];
-  }
+  for (int a = b + lane; a < rc; a += 32) *felem(L, U, lo, uo, mp, kp, rl[a], pc) += uc[a + (int64_t)b * rc];
 }
 
 // Cholesky of the w x w diagonal block of panel [j0, j0 + w) (one CTA per front).
-__global__ void k_potrf(double* __restrict__ L, Fronts f, const int* __restrict__ fronts, int j0,
+template <class T>
+__global__ void k_potrf(T* __restrict__ L, Fronts f, const int* __restrict__ fronts, int j0,
                         int* __restrict__ err, const int* __restrict__ c0_of) {
-  __shared__ double A[P][P + 1];
+  __shared__ T A[P][P + 1];
   const int s = fronts[blockIdx.x];
   const int m = f.m[s], k = f.k[s];
   const int w = min(P, k - j0);
-  double* F = L + f.l_off[s];
+  T* F = L + f.l_off[s];
   for (int idx = threadIdx.x; idx < w * w; idx += blockDim.x) {
     const int i = idx % w, j = idx / w;
-    A[i][j] = (i >= j) ? F[(j0 + i) + (int64_t)(j0 + j) * m] : 0.0;
+    A[i][j] = (i >= j) ? F[(j0 + i) + (int64_t)(j0 + j) * m] : (T)0;
   }
   __syncthreads();
   for (int j = 0; j < w; ++j) {
     if (threadIdx.x == 0) {
-      double d = A[j][j];
-      if (!(d > 0.0)) {
+      T d = A[j][j];
+      if (!(d > (T)0)) {
         atomicCAS(err, 0, c0_of[s] + j0 + j + 1);
-        d = 1.0;
+        d = (T)1;
       }
-      A[j][j] = sqrt(d);
+      A[j][j] = tsqrt(d);
     }
     __syncthreads();
-    const double inv = 1.0 / A[j][j];
+    const T inv = (T)1 / A[j][j];
     for (int i = j + 1 + threadIdx.x; i < w; i += blockDim.x) A[i][j] *= inv;
     __syncthreads();
     const int t = w - j - 1;
@@ -131,78 +144,81 @@ __global__ void k_potrf(double* __restrict__ L, Fronts f, const int* __restrict_
 
 // Panel triangular solve: rows [j1, m) of the panel columns times L_dd^-T.
 // kTrsmRows rows per CTA, one thread per row.
-__global__ void __launch_bounds__(kTrsmRows) k_trsm(double* __restrict__ L, Fronts f,
-                                                    const int* __restrict__ fronts,
+template <class T>
+__global__ void __launch_bounds__(kTrsmRows) k_trsm(T* __restrict__ L, Fronts f, const int* __restrict__ fronts,
                                                     const int64_t* __restrict__ prefix, int count, int j0) {
-  extern __shared__ double sm_trsm[];
-  double(*Ld)[P + 1] = reinterpret_cast<double(*)[P + 1]>(sm_trsm);
-  double(*X)[P + 1] = reinterpret_cast<double(*)[P + 1]>(sm_trsm + P * (P + 1));
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  T(*Ld)[P + 1] = reinterpret_cast<T(*)[P + 1]>(sm_raw);
+  T(*X)[P + 1] = reinterpret_cast<T(*)[P + 1]>(sm_raw + sizeof(T) * P * (P + 1));
   const int idx = find_task(prefix, count, blockIdx.x);
   const int s = fronts[idx];
   const int m = f.m[s], k = f.k[s];
   const int w = min(P, k - j0), j1 = j0 + w;
-  double* F = L + f.l_off[s];
+  T* F = L + f.l_off[s];
   const int r0 = j1 + (int)(blockIdx.x - prefix[idx]) * kTrsmRows;
-  for (int idx2 = threadIdx.x; idx2 < w * w; idx2 += blockDim.x) {
-    const int i = idx2 % w, j = idx2 / w;
-    Ld[i][j] = (i >= j) ? F[(j0 + i) + (int64_t)(j0 + j) * m] : 0.0;
+  for (int q = threadIdx.x; q < w * w; q += blockDim.x) {
+    const int i = q % w, j = q / w;
+    Ld[i][j] = (i >= j) ? F[(j0 + i) + (int64_t)(j0 + j) * m] : (T)0;
   }
-  for (int idx2 = threadIdx.x; idx2 < kTrsmRows * w; idx2 += blockDim.x) {
-    const int i = idx2 % kTrsmRows, j = idx2 / kTrsmRows;
+  for (int q = threadIdx.x; q < kTrsmRows * w; q += blockDim.x) {
+    const int i = q % kTrsmRows, j = q / kTrsmRows;
     const int row = r0 + i;
-    X[i][j] = (row < m) ? F[row + (int64_t)(j0 + j) * m] : 0.0;
+    X[i][j] = (row < m) ? F[row + (int64_t)(j0 + j) * m] : (T)0;
   }
   __syncthreads();
   const int t = threadIdx.x;
   for (int c = 0; c < w; ++c) {
-    double v = X[t][c];
+    T v = X[t][c];
     for (int cc = 0; cc < c; ++cc) v -= X[t][cc] * Ld[c][cc];
     X[t][c] = v / Ld[c][c];
   }
   __syncthreads();
-  for (int idx2 = threadIdx.x; idx2 < kTrsmRows * w; idx2 += blockDim.x) {
-    const int i = idx2 % kTrsmRows, j = idx2 / kTrsmRows;
+  for (int q = threadIdx.x; q < kTrsmRows * w; q += blockDim.x) {
+    const int i = q % kTrsmRows, j = q / kTrsmRows;
     const int row = r0 + i;
     if (row < m) F[row + (int64_t)(j0 + j) * m] = X[i][j];
   }
 }
 
-// Trailing update F[j1:m, j1:m] -= X X^T (lower triangle), X = panel rows [j1, m).
-// One 64 x 64 tile per CTA, 256 threads with 4 x 4 outputs each.
-__global__ void __launch_bounds__(256) k_syrk(double* __restrict__ L, double* __restrict__ U, Fronts f,
-                                              const int* __restrict__ fronts,
-                                              const int64_t* __restrict__ prefix, int count, int j0) {
-  constexpr int T = kTileSyrk;
-  extern __shared__ double sm_syrk[];
-  double(*As)[P + 1] = reinterpret_cast<double(*)[P + 1]>(sm_syrk);
-  double(*Bs)[P + 1] = reinterpret_cast<double(*)[P + 1]>(sm_syrk + T * (P + 1));
+// Update of the rest of the outer panel by the inner panel [j0, j1):
+// F[r, c] -= sum_p X[r, p] X[c, p] for c in [j1, J1), r >= c.  64 x 64 tiles,
+// 256 threads with 4 x 4 outputs each.
+template <class T>
+__global__ void __launch_bounds__(256) k_syrk_panel(T* __restrict__ L, Fronts f, const int* __restrict__ fronts,
+                                                    const int64_t* __restrict__ prefix, int count, int j0) {
+  constexpr int TS = kTileSyrk;
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  T(*As)[P + 1] = reinterpret_cast<T(*)[P + 1]>(sm_raw);
+  T(*Bs)[P + 1] = reinterpret_cast<T(*)[P + 1]>(sm_raw + sizeof(T) * TS * (P + 1));
   const int idx = find_task(prefix, count, blockIdx.x);
   const int s = fronts[idx];
   const int m = f.m[s], k = f.k[s];
   const int w = min(P, k - j0), j1 = j0 + w;
-  const int64_t lo = f.l_off[s], uo = f.u_off[s];
-  const double* F = L + lo;
-  const int64_t t = blockIdx.x - prefix[idx];
-  // decode the lower-triangle tile index t -> (bi, bj), bj <= bi
-  int bi = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
-  while ((int64_t)(bi + 1) * (bi + 2) / 2 <= t) ++bi;
-  while ((int64_t)bi * (bi + 1) / 2 > t) --bi;
-  const int bj = (int)(t - (int64_t)bi * (bi + 1) / 2);
-  const int r0 = j1 + bi * T, c0 = j1 + bj * T;
-  for (int q = threadIdx.x; q < T * w; q += blockDim.x) {
-    const int i = q % T, p = q / T;
-    As[i][p] = (r0 + i < m) ? F[(r0 + i) + (int64_t)(j0 + p) * m] : 0.0;
-    Bs[i][p] = (c0 + i < m) ? F[(c0 + i) + (int64_t)(j0 + p) * m] : 0.0;
+  const int J0 = (j0 / kOuter) * kOuter, J1 = min(k, J0 + kOuter);
+  T* F = L + f.l_off[s];
+  const int nr = (m - j1 + TS - 1) / TS;
+  int t = (int)(blockIdx.x - prefix[idx]);
+  int bj = 0;
+  while (t >= nr - bj) {
+    t -= nr - bj;
+    ++bj;
+  }
+  const int bi = bj + t;
+  const int r0 = j1 + bi * TS, c0 = j1 + bj * TS;
+  for (int q = threadIdx.x; q < TS * w; q += blockDim.x) {
+    const int i = q % TS, p = q / TS;
+    As[i][p] = (r0 + i < m) ? F[(r0 + i) + (int64_t)(j0 + p) * m] : (T)0;
+    Bs[i][p] = (c0 + i < J1) ? F[(c0 + i) + (int64_t)(j0 + p) * m] : (T)0;
   }
   __syncthreads();
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  double acc[4][4];
+  T acc[4][4];
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
-    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+    for (int b = 0; b < 4; ++b) acc[a][b] = (T)0;
   for (int p = 0; p < w; ++p) {
-    double av[4], bv[4];
+    T av[4], bv[4];
 #pragma unroll
     for (int a = 0; a < 4; ++a) av[a] = As[tx + 16 * a][p];
 #pragma unroll
@@ -218,6 +234,74 @@ __global__ void __launch_bounds__(256) k_syrk(double* __restrict__ L, double* __
     if (r >= m) continue;
 #pragma unroll
     for (int b = 0; b < 4; ++b) {
+      const int c = c0 + ty + 16 * b;
+      if (c >= J1 || c > r) continue;
+      F[r + (int64_t)c * m] -= acc[a][b];
+    }
+  }
+}
+
+// Trailing update at the end of an outer panel: F[J1:m, J1:m] -= X X^T with X the
+// outer panel rows [J1, m), columns [J0, J1).  128 x 128 tiles, 256 threads with
+// 8 x 8 outputs each, K consumed in chunks of 32.
+constexpr int KC = 32;
+template <class T>
+__global__ void __launch_bounds__(256) k_syrk_big(T* __restrict__ L, T* __restrict__ U, Fronts f,
+                                                  const int* __restrict__ fronts,
+                                                  const int64_t* __restrict__ prefix, int count, int j0) {
+  constexpr int TB = kTileBig;
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  T(*As)[TB + 1] = reinterpret_cast<T(*)[TB + 1]>(sm_raw);
+  T(*Bs)[TB + 1] = reinterpret_cast<T(*)[TB + 1]>(sm_raw + sizeof(T) * KC * (TB + 1));
+  const int idx = find_task(prefix, count, blockIdx.x);
+  const int s = fronts[idx];
+  const int m = f.m[s], k = f.k[s];
+  const int J0 = (j0 / kOuter) * kOuter, J1 = min(k, J0 + kOuter);
+  const int64_t lo = f.l_off[s], uo = f.u_off[s];
+  const T* F = L + lo;
+  const int64_t t = blockIdx.x - prefix[idx];
+  int bi = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+  while ((int64_t)(bi + 1) * (bi + 2) / 2 <= t) ++bi;
+  while ((int64_t)bi * (bi + 1) / 2 > t) --bi;
+  const int bj = (int)(t - (int64_t)bi * (bi + 1) / 2);
+  const int r0 = J1 + bi * TB, c0 = J1 + bj * TB;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  T acc[8][8];
+#pragma unroll
+  for (int a = 0; a < 8; ++a)
+#pragma unroll
+    for (int b = 0; b < 8; ++b) acc[a][b] = (T)0;
+  const int K = J1 - J0;
+  for (int k0 = 0; k0 < K; k0 += KC) {
+    const int kc = min(KC, K - k0);
+    for (int q = threadIdx.x; q < TB * KC; q += blockDim.x) {
+      const int i = q % TB, p = q / TB;
+      const bool okp = p < kc;
+      const int64_t col = (int64_t)(J0 + k0 + p) * m;
+      As[p][i] = (okp && r0 + i < m) ? F[(r0 + i) + col] : (T)0;
+      Bs[p][i] = (okp && c0 + i < m) ? F[(c0 + i) + col] : (T)0;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int p = 0; p < kc; ++p) {
+      T av[8], bv[8];
+#pragma unroll
+      for (int a = 0; a < 8; ++a) av[a] = As[p][tx + 16 * a];
+#pragma unroll
+      for (int b = 0; b < 8; ++b) bv[b] = Bs[p][ty + 16 * b];
+#pragma unroll
+      for (int a = 0; a < 8; ++a)
+#pragma unroll
+        for (int b = 0; b < 8; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    const int r = r0 + tx + 16 * a;
+    if (r >= m) continue;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
       const int c = c0 + ty + 16 * b;
       if (c >= m || c > r) continue;
       *felem(L, U, lo, uo, m, k, r, c) -= acc[a][b];
@@ -239,19 +323,21 @@ struct SolveArgs {
   int64_t ld;
 };
 
-__global__ void k_fwd_init(double* __restrict__ W, const double* __restrict__ b, SolveArgs a,
+template <class T>
+__global__ void k_fwd_init(T* __restrict__ W, const double* __restrict__ b, SolveArgs a,
                            const int* __restrict__ fronts, const int64_t* __restrict__ prefix, int count) {
   const int idx = find_task(prefix, count, blockIdx.x);
   const int s = fronts[idx];
   const int m = a.m[s], k = a.k[s];
   const int i = (int)(blockIdx.x - prefix[idx]) * kSolveRows + threadIdx.x;
   if (i >= m) return;
-  double* w = W + a.w_off[s] * a.nrhs;
+  T* w = W + a.w_off[s] * a.nrhs;
   const int pos = (i < k) ? a.rows[a.rows_off[s] + i] : -1;
-  for (int r = 0; r < a.nrhs; ++r) w[i + (int64_t)r * m] = (i < k) ? b[pos + r * a.ld] : 0.0;
+  for (int r = 0; r < a.nrhs; ++r) w[i + (int64_t)r * m] = (i < k) ? (T)b[pos + r * a.ld] : (T)0;
 }
 
-__global__ void k_fwd_extend(double* __restrict__ W, SolveArgs a, const int* __restrict__ parent,
+template <class T>
+__global__ void k_fwd_extend(T* __restrict__ W, SolveArgs a, const int* __restrict__ parent,
                              const int64_t* __restrict__ rel_off, const int* __restrict__ rel,
                              const int* __restrict__ kids, const int64_t* __restrict__ prefix, int count) {
   const int idx = find_task(prefix, count, blockIdx.x);
@@ -259,26 +345,28 @@ __global__ void k_fwd_extend(double* __restrict__ W, SolveArgs a, const int* __r
   const int mc = a.m[c], kc = a.k[c], rc = mc - kc, mp = a.m[p];
   const int i = (int)(blockIdx.x - prefix[idx]) * kSolveRows + threadIdx.x;
   if (i >= rc) return;
-  const double* wc = W + a.w_off[c] * a.nrhs;
-  double* wp = W + a.w_off[p] * a.nrhs;
+  const T* wc = W + a.w_off[c] * a.nrhs;
+  T* wp = W + a.w_off[p] * a.nrhs;
   const int pr = rel[rel_off[c] + i];
   for (int r = 0; r < a.nrhs; ++r) wp[pr + (int64_t)r * mp] += wc[kc + i + (int64_t)r * mc];
 }
 
 // Forward diagonal-block solve of panel [j0, j0 + w) (one CTA per front).
-__global__ void k_fwd_diag(const double* __restrict__ L, double* __restrict__ W, SolveArgs a,
+template <class T>
+__global__ void k_fwd_diag(const T* __restrict__ L, T* __restrict__ W, SolveArgs a,
                            const int* __restrict__ fronts, int j0) {
-  __shared__ double Ld[P][P + 1];
-  extern __shared__ double Y[];  // w x nrhs
+  __shared__ T Ld[P][P + 1];
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  T* Y = reinterpret_cast<T*>(sm_raw);  // P x nrhs
   const int s = fronts[blockIdx.x];
   const int m = a.m[s], k = a.k[s];
   const int w = min(P, k - j0);
-  const double* F = L + a.l_off[s];
-  double* wv = W + a.w_off[s] * a.nrhs;
+  const T* F = L + a.l_off[s];
+  T* wv = W + a.w_off[s] * a.nrhs;
   const int nr = a.nrhs;
   for (int q = threadIdx.x; q < w * w; q += blockDim.x) {
     const int i = q % w, j = q / w;
-    Ld[i][j] = (i >= j) ? F[(j0 + i) + (int64_t)(j0 + j) * m] : 0.0;
+    Ld[i][j] = (i >= j) ? F[(j0 + i) + (int64_t)(j0 + j) * m] : (T)0;
   }
   for (int q = threadIdx.x; q < w * nr; q += blockDim.x) {
     const int i = q % w, r = q / w;
@@ -301,18 +389,18 @@ __global__ void k_fwd_diag(const double* __restrict__ L, double* __restrict__ W,
 }
 
 // W[j1:m] -= L[j1:m, panel] * Y (one row per thread).
-__global__ void __launch_bounds__(kSolveRows) k_fwd_update(const double* __restrict__ L,
-                                                           double* __restrict__ W, SolveArgs a,
+template <class T>
+__global__ void __launch_bounds__(kSolveRows) k_fwd_update(const T* __restrict__ L, T* __restrict__ W, SolveArgs a,
                                                            const int* __restrict__ fronts,
-                                                           const int64_t* __restrict__ prefix,
-                                                           int count, int j0) {
-  extern __shared__ double Y[];  // P x nrhs
+                                                           const int64_t* __restrict__ prefix, int count, int j0) {
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  T* Y = reinterpret_cast<T*>(sm_raw);  // P x nrhs
   const int idx = find_task(prefix, count, blockIdx.x);
   const int s = fronts[idx];
   const int m = a.m[s], k = a.k[s];
   const int w = min(P, k - j0), j1 = j0 + w;
-  const double* F = L + a.l_off[s];
-  double* wv = W + a.w_off[s] * a.nrhs;
+  const T* F = L + a.l_off[s];
+  T* wv = W + a.w_off[s] * a.nrhs;
   const int nr = a.nrhs;
   for (int q = threadIdx.x; q < w * nr; q += blockDim.x) {
     const int i = q % w, r = q / w;
@@ -322,51 +410,51 @@ __global__ void __launch_bounds__(kSolveRows) k_fwd_update(const double* __restr
   const int row = j1 + (int)(blockIdx.x - prefix[idx]) * kSolveRows + threadIdx.x;
   if (row >= m) return;
   for (int r = 0; r < nr; ++r) {
-    double acc = 0.0;
+    T acc = (T)0;
     for (int c = 0; c < w; ++c) acc = fma(F[row + (int64_t)(j0 + c) * m], Y[c + r * P], acc);
     wv[row + (int64_t)r * m] -= acc;
   }
 }
 
-__global__ void k_bwd_init(double* __restrict__ W, const double* __restrict__ x, SolveArgs a,
+template <class T>
+__global__ void k_bwd_init(T* __restrict__ W, const double* __restrict__ x, SolveArgs a,
                            const int* __restrict__ fronts, const int64_t* __restrict__ prefix, int count) {
   const int idx = find_task(prefix, count, blockIdx.x);
   const int s = fronts[idx];
   const int m = a.m[s], k = a.k[s];
   const int i = (int)(blockIdx.x - prefix[idx]) * kSolveRows + threadIdx.x;
   if (i < k || i >= m) return;
-  double* w = W + a.w_off[s] * a.nrhs;
+  T* w = W + a.w_off[s] * a.nrhs;
   const int pos = a.rows[a.rows_off[s] + i];
-  for (int r = 0; r < a.nrhs; ++r) w[i + (int64_t)r * m] = x[pos + r * a.ld];
+  for (int r = 0; r < a.nrhs; ++r) w[i + (int64_t)r * m] = (T)x[pos + r * a.ld];
 }
 
 // Partial sums of L[j1:m, panel]^T W[j1:m] over one row chunk.
-__global__ void __launch_bounds__(kSolveRows) k_bwd_partial(const double* __restrict__ L,
-                                                            const double* __restrict__ W, SolveArgs a,
-                                                            double* __restrict__ part,
+template <class T>
+__global__ void __launch_bounds__(kSolveRows) k_bwd_partial(const T* __restrict__ L, const T* __restrict__ W,
+                                                            SolveArgs a, T* __restrict__ part,
                                                             const int* __restrict__ fronts,
-                                                            const int64_t* __restrict__ prefix,
-                                                            int count, int j0) {
-  __shared__ double red[kSolveRows / 32][P];
+                                                            const int64_t* __restrict__ prefix, int count, int j0) {
+  __shared__ T red[kSolveRows / 32][P];
   const int idx = find_task(prefix, count, blockIdx.x);
   const int s = fronts[idx];
   const int m = a.m[s], k = a.k[s];
   const int w = min(P, k - j0), j1 = j0 + w;
-  const double* F = L + a.l_off[s];
-  const double* wv = W + a.w_off[s] * a.nrhs;
+  const T* F = L + a.l_off[s];
+  const T* wv = W + a.w_off[s] * a.nrhs;
   const int row = j1 + (int)(blockIdx.x - prefix[idx]) * kSolveRows + threadIdx.x;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int r = 0; r < a.nrhs; ++r) {
-    const double xv = (row < m) ? wv[row + (int64_t)r * m] : 0.0;
+    const T xv = (row < m) ? wv[row + (int64_t)r * m] : (T)0;
     for (int c = 0; c < w; ++c) {
-      double v = (row < m) ? F[row + (int64_t)(j0 + c) * m] * xv : 0.0;
+      T v = (row < m) ? F[row + (int64_t)(j0 + c) * m] * xv : (T)0;
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
       if (lane == 0) red[warp][c] = v;
     }
     __syncthreads();
     if (threadIdx.x < w) {
-      double v = 0.0;
+      T v = (T)0;
       for (int q = 0; q < kSolveRows / 32; ++q) v += red[q][threadIdx.x];
       part[((int64_t)blockIdx.x * a.nrhs + r) * P + threadIdx.x] = v;
     }
@@ -375,25 +463,26 @@ __global__ void __launch_bounds__(kSolveRows) k_bwd_partial(const double* __rest
 }
 
 // Backward diagonal-block solve of panel [j0, j0 + w) after subtracting the partials.
-__global__ void k_bwd_diag(const double* __restrict__ L, double* __restrict__ W, SolveArgs a,
-                           const double* __restrict__ part, const int* __restrict__ fronts,
-                           const int64_t* __restrict__ prefix, int j0) {
-  __shared__ double Ld[P][P + 1];
-  extern __shared__ double Y[];
+template <class T>
+__global__ void k_bwd_diag(const T* __restrict__ L, T* __restrict__ W, SolveArgs a, const T* __restrict__ part,
+                           const int* __restrict__ fronts, const int64_t* __restrict__ prefix, int j0) {
+  __shared__ T Ld[P][P + 1];
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  T* Y = reinterpret_cast<T*>(sm_raw);
   const int s = fronts[blockIdx.x];
   const int m = a.m[s], k = a.k[s];
   const int w = min(P, k - j0);
-  const double* F = L + a.l_off[s];
-  double* wv = W + a.w_off[s] * a.nrhs;
+  const T* F = L + a.l_off[s];
+  T* wv = W + a.w_off[s] * a.nrhs;
   const int nr = a.nrhs;
   const int64_t b0 = prefix[blockIdx.x], b1 = prefix[blockIdx.x + 1];
   for (int q = threadIdx.x; q < w * w; q += blockDim.x) {
     const int i = q % w, j = q / w;
-    Ld[i][j] = (i >= j) ? F[(j0 + i) + (int64_t)(j0 + j) * m] : 0.0;
+    Ld[i][j] = (i >= j) ? F[(j0 + i) + (int64_t)(j0 + j) * m] : (T)0;
   }
   for (int q = threadIdx.x; q < w * nr; q += blockDim.x) {
     const int i = q % w, r = q / w;
-    double v = wv[j0 + i + (int64_t)r * m];
+    T v = wv[j0 + i + (int64_t)r * m];
     for (int64_t b = b0; b < b1; ++b) v -= part[(b * nr + r) * P + i];
     Y[i + r * P] = v;
   }
@@ -413,16 +502,341 @@ __global__ void k_bwd_diag(const double* __restrict__ L, double* __restrict__ W,
   }
 }
 
-__global__ void k_bwd_store(const double* __restrict__ W, double* __restrict__ x, SolveArgs a,
+template <class T>
+__global__ void k_bwd_store(const T* __restrict__ W, double* __restrict__ x, SolveArgs a,
                             const int* __restrict__ fronts, const int64_t* __restrict__ prefix, int count) {
   const int idx = find_task(prefix, count, blockIdx.x);
   const int s = fronts[idx];
   const int k = a.k[s], m = a.m[s];
   const int i = (int)(blockIdx.x - prefix[idx]) * kSolveRows + threadIdx.x;
   if (i >= k) return;
-  const double* w = W + a.w_off[s] * a.nrhs;
+  const T* w = W + a.w_off[s] * a.nrhs;
   const int pos = a.rows[a.rows_off[s] + i];
-  for (int r = 0; r < a.nrhs; ++r) x[pos + r * a.ld] = w[i + (int64_t)r * m];
+  for (int r = 0; r < a.nrhs; ++r) x[pos + r * a.ld] = (double)w[i + (int64_t)r * m];
+}
+
+// ---------------------------------------------------------------------------
+// fused level solves
+//
+// One launch per assembly-tree level and direction.  Every CTA owns one 64-row
+// block of one front; it takes a ticket (atomicAdd) that names its item, so the
+// items start in list order.  A block waits only for pivot blocks of its own
+// front that come earlier in the list (flag per pivot block, set with release
+// semantics after the block's values are stored), hence every block it waits for
+// is already running or finished.  Waits are bounded: after kSpinLimit polls the
+// CTA records err[1] and goes on (the results are then wrong and the host reports
+// the error; the kernel still ends).
+//
+// Diagonal blocks are applied through their inverses (Dinv, computed once per
+// factorization), so the dependency chain costs one 64 x 64 block product per
+// pivot block instead of a 64-step substitution.
+// ---------------------------------------------------------------------------
+constexpr int SB = kPanel;  // 64 rows per solve block
+constexpr unsigned kSpinLimit = 1u << 21;
+
+__device__ __forceinline__ int ld_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(int* p, int v) {
+  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Called by one thread.  Gives up after kSpinLimit polls (or at once when an
+// earlier wait of this solve gave up) and records the failure in *err.
+__device__ void wait_flag(const int* flag, int* err) {
+  if (*(volatile int*)err != 0) return;
+  for (unsigned it = 0; it < kSpinLimit; ++it) {
+    if (ld_acquire(flag) != 0) return;
+    __nanosleep(64);
+  }
+  atomicExch(err, 1);
+}
+
+struct FusedArgs {
+  const int* items;        // (front, block) pairs of this launch
+  int* ticket;             // launch-order counter (zeroed before the solve)
+  int* flags;              // one per pivot block (zeroed before the solve)
+  const int64_t* flag_off; // per front: first flag
+  const int64_t* dinv_off; // per front: first inverted diagonal block
+  int* err;                // err[1]: a wait gave up
+};
+
+// 64 x 64 block of a front (rows [r0, r0 + nr), columns [c0, c0 + nc), zero
+// outside) into 16 registers per thread: element (i, c) goes to thread
+// (i + 64 c) mod 256, slot (i + 64 c) / 256.
+template <class T>
+__device__ __forceinline__ void load_block(T (&pre)[16], const T* __restrict__ F, int64_t ld, int r0, int nr, int c0,
+                                           int nc) {
+#pragma unroll
+  for (int e = 0; e < 16; ++e) {
+    const int q = threadIdx.x + 256 * e;
+    const int i = q & 63, c = q >> 6;
+    pre[e] = (i < nr && c < nc) ? F[(r0 + i) + (int64_t)(c0 + c) * ld] : (T)0;
+  }
+}
+// registers -> Ls[c][i]
+template <class T>
+__device__ __forceinline__ void store_block(T (*Ls)[SB + 1], const T (&pre)[16]) {
+#pragma unroll
+  for (int e = 0; e < 16; ++e) {
+    const int q = threadIdx.x + 256 * e;
+    Ls[q >> 6][q & 63] = pre[e];
+  }
+}
+
+// Forward: CTA for block b of front s.  Pivot block (b < pb): rows [64b, ..) of the
+// pivot columns, y_b = Dinv_b (w_b - sum_{q<b} L_bq y_q).  Update block: rows
+// [k + 64 (b - pb), ..), w -= sum_{q<pb} L_bq y_q (gathered by the parent next).
+// Thread t: row i = t % 64 of the block, right-hand sides r = t / 64 + 4 j.
+template <class T, int RPT>
+__global__ void __launch_bounds__(256) k_fwd_level(const T* __restrict__ L, const T* __restrict__ Dinv, T* W,
+                                                   SolveArgs a, FusedArgs fa) {
+  __shared__ T Ls[SB][SB + 1];
+  __shared__ int s_item;
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  T* Ys = reinterpret_cast<T*>(sm_raw);  // SB x nrhs, [c * nrhs + r]
+  const int t = threadIdx.x, i = t & 63, g = t >> 6;
+  if (t == 0) s_item = atomicAdd(fa.ticket, 1);
+  __syncthreads();
+  const int s = fa.items[2 * s_item], b = fa.items[2 * s_item + 1];
+  const int m = a.m[s], k = a.k[s], nr_rhs = a.nrhs;
+  const int pb = (k + SB - 1) / SB;
+  const bool piv = b < pb;
+  const int r0 = piv ? SB * b : k + SB * (b - pb);
+  const int nr = min(SB, (piv ? k : m) - r0);
+  const int qmax = piv ? b : pb;
+  const T* F = L + a.l_off[s];
+  T* w = W + a.w_off[s] * nr_rhs;
+  const int* flags = fa.flags + fa.flag_off[s];
+  T acc[RPT];
+#pragma unroll
+  for (int j = 0; j < RPT; ++j) acc[j] = (T)0;
+  T pre[16];
+  if (qmax > 0) load_block(pre, F, m, r0, nr, 0, min(SB, k));
+  for (int q = 0; q < qmax; ++q) {
+    const int wq = min(SB, k - SB * q);
+    if (t == 0) wait_flag(flags + q, fa.err);
+    __syncthreads();
+    store_block(Ls, pre);
+    for (int e = t; e < SB * nr_rhs; e += 256) {
+      const int c = e % SB, r = e / SB;
+      Ys[c * nr_rhs + r] = (c < wq) ? __ldcg(w + SB * q + c + (int64_t)r * m) : (T)0;
+    }
+    __syncthreads();
+    if (q + 1 < qmax) load_block(pre, F, m, r0, nr, SB * (q + 1), min(SB, k - SB * (q + 1)));
+#pragma unroll 8
+    for (int c = 0; c < SB; ++c) {
+      const T l = Ls[c][i];
+#pragma unroll
+      for (int j = 0; j < RPT; ++j) {
+        const int r = g + 4 * j;
+        if (r < nr_rhs) acc[j] = fma(l, Ys[c * nr_rhs + r], acc[j]);
+      }
+    }
+  }
+  if (!piv) {
+    if (i < nr) {
+#pragma unroll
+      for (int j = 0; j < RPT; ++j) {
+        const int r = g + 4 * j;
+        if (r < nr_rhs) w[r0 + i + (int64_t)r * m] -= acc[j];
+      }
+    }
+    return;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < RPT; ++j) {
+    const int r = g + 4 * j;
+    if (r < nr_rhs) Ys[i * nr_rhs + r] = (i < nr) ? w[r0 + i + (int64_t)r * m] - acc[j] : (T)0;
+  }
+  const T* D = Dinv + fa.dinv_off[s] + (int64_t)b * SB * SB;
+  for (int e = t; e < SB * SB; e += 256) {
+    const int ii = e & 63, c = e >> 6;
+    Ls[c][ii] = (ii < nr && c < nr) ? D[ii + c * nr] : (T)0;
+  }
+  __syncthreads();
+  T y[RPT];
+#pragma unroll
+  for (int j = 0; j < RPT; ++j) y[j] = (T)0;
+#pragma unroll 8
+  for (int c = 0; c < SB; ++c) {
+    const T l = Ls[c][i];
+#pragma unroll
+    for (int j = 0; j < RPT; ++j) {
+      const int r = g + 4 * j;
+      if (r < nr_rhs) y[j] = fma(l, Ys[c * nr_rhs + r], y[j]);
+    }
+  }
+  if (i < nr) {
+#pragma unroll
+    for (int j = 0; j < RPT; ++j) {
+      const int r = g + 4 * j;
+      if (r < nr_rhs) w[r0 + i + (int64_t)r * m] = y[j];
+    }
+  }
+  __syncthreads();
+  if (t == 0) {
+    __threadfence();
+    st_release(fa.flags + fa.flag_off[s] + b, 1);
+  }
+}
+
+// Backward: CTA for pivot block p of front s (items in descending p):
+//   x_p = Dinv_p^T (y_p - sum_{rows below} L_rows,p^T x_rows)
+// over the update rows [k, m) (x of ancestors, staged in W by k_bwd_init) and the
+// pivot blocks q > p of the same front (waited for).  Thread t: column c = t % 64
+// of the block, right-hand sides r = t / 64 + 4 j.  Writes x_p to W and to the
+// caller's vector.
+template <class T, int RPT>
+__global__ void __launch_bounds__(256) k_bwd_level(const T* __restrict__ L, const T* __restrict__ Dinv, T* W,
+                                                   double* __restrict__ x, SolveArgs a, FusedArgs fa) {
+  __shared__ T Ls[SB][SB + 1];
+  __shared__ int s_item;
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  T* Ws = reinterpret_cast<T*>(sm_raw);  // SB x nrhs, [row * nrhs + r]
+  const int t = threadIdx.x, c = t & 63, g = t >> 6;
+  if (t == 0) s_item = atomicAdd(fa.ticket, 1);
+  __syncthreads();
+  const int s = fa.items[2 * s_item], p = fa.items[2 * s_item + 1];
+  const int m = a.m[s], k = a.k[s], nr_rhs = a.nrhs;
+  const int pb = (k + SB - 1) / SB;
+  const int c0 = SB * p, wc = min(SB, k - c0);
+  const int nub = (m - k + SB - 1) / SB;
+  const int nblk = nub + (pb - 1 - p);
+  const T* F = L + a.l_off[s];
+  T* w = W + a.w_off[s] * nr_rhs;
+  const int* flags = fa.flags + fa.flag_off[s];
+  T acc[RPT];
+#pragma unroll
+  for (int j = 0; j < RPT; ++j) acc[j] = (T)0;
+  auto block_rows = [&](int u, int& r0, int& nr, int& q) {
+    if (u < nub) {
+      r0 = k + SB * u;
+      nr = min(SB, m - r0);
+      q = -1;
+    } else {
+      q = pb - 1 - (u - nub);
+      r0 = SB * q;
+      nr = min(SB, k - r0);
+    }
+  };
+  T pre[16];
+  if (nblk > 0) {
+    int r0, nr, q;
+    block_rows(0, r0, nr, q);
+    load_block(pre, F, m, r0, nr, c0, wc);
+  }
+  for (int u = 0; u < nblk; ++u) {
+    int r0, nr, q;
+    block_rows(u, r0, nr, q);
+    if (q >= 0 && t == 0) wait_flag(flags + q, fa.err);
+    __syncthreads();
+    store_block(Ls, pre);
+    for (int e = t; e < SB * nr_rhs; e += 256) {
+      const int ii = e % SB, r = e / SB;
+      Ws[ii * nr_rhs + r] = (ii < nr) ? __ldcg(w + r0 + ii + (int64_t)r * m) : (T)0;
+    }
+    __syncthreads();
+    if (u + 1 < nblk) {
+      int r1, n1, q1;
+      block_rows(u + 1, r1, n1, q1);
+      load_block(pre, F, m, r1, n1, c0, wc);
+    }
+#pragma unroll 8
+    for (int ii = 0; ii < SB; ++ii) {
+      const T l = Ls[c][ii];
+#pragma unroll
+      for (int j = 0; j < RPT; ++j) {
+        const int r = g + 4 * j;
+        if (r < nr_rhs) acc[j] = fma(l, Ws[ii * nr_rhs + r], acc[j]);
+      }
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < RPT; ++j) {
+    const int r = g + 4 * j;
+    if (r < nr_rhs) Ws[c * nr_rhs + r] = (c < wc) ? w[c0 + c + (int64_t)r * m] - acc[j] : (T)0;
+  }
+  const T* D = Dinv + fa.dinv_off[s] + (int64_t)p * SB * SB;
+  for (int e = t; e < SB * SB; e += 256) {
+    const int ii = e & 63, cc = e >> 6;
+    Ls[cc][ii] = (ii < wc && cc < wc) ? D[ii + cc * wc] : (T)0;
+  }
+  __syncthreads();
+  T xv[RPT];
+#pragma unroll
+  for (int j = 0; j < RPT; ++j) xv[j] = (T)0;
+#pragma unroll 8
+  for (int ii = 0; ii < SB; ++ii) {
+    const T l = Ls[c][ii];
+#pragma unroll
+    for (int j = 0; j < RPT; ++j) {
+      const int r = g + 4 * j;
+      if (r < nr_rhs) xv[j] = fma(l, Ws[ii * nr_rhs + r], xv[j]);
+    }
+  }
+  if (c < wc) {
+    const int pos = a.rows[a.rows_off[s] + c0 + c];
+#pragma unroll
+    for (int j = 0; j < RPT; ++j) {
+      const int r = g + 4 * j;
+      if (r < nr_rhs) {
+        w[c0 + c + (int64_t)r * m] = xv[j];
+        x[pos + (int64_t)r * a.ld] = (double)xv[j];
+      }
+    }
+  }
+  __syncthreads();
+  if (t == 0) {
+    __threadfence();
+    st_release(fa.flags + fa.flag_off[s] + p, 1);
+  }
+}
+
+// Inverse of the lower-triangular diagonal block p of front s (w x w, w <= 64),
+// stored column-major with leading dimension w at dinv_off[s] + 64 * 64 * p.
+// Computed in FP64: four threads per column j run the substitution
+// X[i][j] = -(sum_{j <= l < i} A[i][l] X[l][j]) / A[i][i] down the column.
+template <class T>
+__global__ void __launch_bounds__(256) k_diag_inverse(const T* __restrict__ L, T* __restrict__ Dinv, Fronts f,
+                                                      const int64_t* __restrict__ dinv_off,
+                                                      const int* __restrict__ items) {
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  double(*A)[SB + 1] = reinterpret_cast<double(*)[SB + 1]>(sm_raw);
+  double(*X)[SB + 1] = reinterpret_cast<double(*)[SB + 1]>(sm_raw + sizeof(double) * SB * (SB + 1));
+  const int s = items[2 * blockIdx.x], p = items[2 * blockIdx.x + 1];
+  const int m = f.m[s], k = f.k[s];
+  const int c0 = SB * p, w = min(SB, k - c0);
+  const T* F = L + f.l_off[s];
+  for (int q = threadIdx.x; q < SB * SB; q += blockDim.x) {
+    const int i = q & 63, j = q >> 6;
+    A[i][j] = (i < w && j < w && i >= j) ? (double)F[(c0 + i) + (int64_t)(c0 + j) * m] : 0.0;
+  }
+  __syncthreads();
+  const int j = threadIdx.x >> 2, part = threadIdx.x & 3;
+  const unsigned mask = 0xFu << ((threadIdx.x & 31) & ~3);
+  if (j < w) {
+    if (part == 0) X[j][j] = 1.0 / A[j][j];
+    __syncwarp(mask);
+    for (int i = j + 1; i < w; ++i) {
+      double sum = 0.0;
+      for (int l = j + part; l < i; l += 4) sum = fma(A[i][l], X[l][j], sum);
+      sum += __shfl_xor_sync(mask, sum, 1);
+      sum += __shfl_xor_sync(mask, sum, 2);
+      if (part == 0) X[i][j] = -sum / A[i][i];
+      __syncwarp(mask);
+    }
+  }
+  __syncthreads();
+  T* D = Dinv + dinv_off[s] + (int64_t)p * SB * SB;
+  for (int q = threadIdx.x; q < w * w; q += blockDim.x) {
+    const int i = q % w, jj = q / w;
+    D[q] = (i >= jj) ? (T)X[i][jj] : (T)0;
+  }
 }
 
 #define TDEM_CUDA_TRY(x)                                                          \
@@ -432,12 +846,209 @@ __global__ void k_bwd_store(const double* __restrict__ W, double* __restrict__ x
   } while (0)
 
 inline unsigned grid_of(int64_t ctas) { return (unsigned)ctas; }
-constexpr size_t kTrsmSmem = sizeof(double) * (P + kTrsmRows) * (P + 1);
-constexpr size_t kSyrkSmem = sizeof(double) * 2 * kTileSyrk * (P + 1);
+template <class T>
+constexpr size_t trsm_smem() { return sizeof(T) * (P + kTrsmRows) * (P + 1); }
+template <class T>
+constexpr size_t syrk_smem() { return sizeof(T) * 2 * kTileSyrk * (P + 1); }
+template <class T>
+constexpr size_t big_smem() { return sizeof(T) * 2 * KC * (kTileBig + 1); }
+
+template <class T>
+std::string set_attributes() {
+  TDEM_CUDA_TRY(cudaFuncSetAttribute(k_trsm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_smem<T>()));
+  TDEM_CUDA_TRY(cudaFuncSetAttribute(k_syrk_panel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)syrk_smem<T>()));
+  TDEM_CUDA_TRY(cudaFuncSetAttribute(k_syrk_big<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big_smem<T>()));
+  TDEM_CUDA_TRY(cudaFuncSetAttribute(k_fwd_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+  TDEM_CUDA_TRY(cudaFuncSetAttribute(k_bwd_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+  TDEM_CUDA_TRY(cudaFuncSetAttribute(k_fwd_update<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+  return "";
+}
+
+template <class T>
+int launch_factor(const Symbolic& sy, T* L, T* U, const double* vals, const int64_t* entry, Fronts fr,
+                  const int* parent, const int64_t* rel_off, const int* rel, const int* tasks,
+                  const int64_t* prefix, int* err, const int* c0, bool use_tc, cudaStream_t s) {
+  int launches = 0;
+  cudaMemsetAsync(L, 0, sizeof(T) * sy.nnz_l, s);
+  {
+    const int64_t nnz = sy.nnz_lower;
+    const unsigned g = (unsigned)std::min<int64_t>((nnz + 255) / 256, 148 * 32);
+    if (nnz > 0) {
+      k_scatter_entries<T><<<g, 256, 0, s>>>(L, entry, vals, nnz);
+      ++launches;
+    }
+  }
+  for (const LevelPlan& lp : sy.levels) {
+    if (lp.assemble.ctas > 0) {
+      k_zero_u<T><<<grid_of(lp.assemble.ctas), 256, 0, s>>>(U, fr, tasks + lp.assemble.off, prefix + lp.assemble.pre,
+                                                           lp.assemble.count);
+      ++launches;
+    }
+    for (const TaskList& tl : lp.extend_slots) {
+      if (tl.ctas == 0) continue;
+      k_extend_add<T><<<grid_of(tl.ctas), 256, 0, s>>>(L, U, fr, parent, rel_off, rel, tasks + tl.off,
+                                                       prefix + tl.pre, tl.count);
+      ++launches;
+    }
+    for (const PanelStep& ps : lp.panels) {
+      k_potrf<T><<<ps.potrf.count, 256, 0, s>>>(L, fr, tasks + ps.potrf.off, ps.j0, err, c0);
+      ++launches;
+      if (ps.trsm.ctas > 0) {
+        k_trsm<T><<<grid_of(ps.trsm.ctas), kTrsmRows, trsm_smem<T>(), s>>>(L, fr, tasks + ps.trsm.off,
+                                                                           prefix + ps.trsm.pre, ps.trsm.count, ps.j0);
+        ++launches;
+      }
+      if (ps.syrk.ctas > 0) {
+        k_syrk_panel<T><<<grid_of(ps.syrk.ctas), 256, syrk_smem<T>(), s>>>(L, fr, tasks + ps.syrk.off,
+                                                                           prefix + ps.syrk.pre, ps.syrk.count, ps.j0);
+        ++launches;
+      }
+      if (ps.syrk_big.ctas > 0) {
+        if (std::is_same<T, float>::value && use_tc)
+          launch_syrk_tc((float*)L, (float*)U, fr.l_off, fr.u_off, fr.m, fr.k, tasks + ps.syrk_big.off,
+                         prefix + ps.syrk_big.pre, ps.syrk_big.count, ps.syrk_big.ctas, ps.j0, err, s);
+        else
+          k_syrk_big<T><<<grid_of(ps.syrk_big.ctas), 256, big_smem<T>(), s>>>(
+              L, U, fr, tasks + ps.syrk_big.off, prefix + ps.syrk_big.pre, ps.syrk_big.count, ps.j0);
+        ++launches;
+      }
+    }
+  }
+  return launches;
+}
+
+template <class T>
+int launch_solve(const Symbolic& sy, const T* L, T* W, T* part, const double* b, double* x, SolveArgs a,
+                 const int* parent, const int64_t* rel_off, const int* rel, const int* tasks, const int64_t* prefix,
+                 cudaStream_t s) {
+  int launches = 0;
+  const size_t ysm = sizeof(T) * P * a.nrhs;
+  for (const LevelPlan& lp : sy.levels) {
+    k_fwd_init<T><<<grid_of(lp.assemble.ctas), kSolveRows, 0, s>>>(W, b, a, tasks + lp.assemble.off,
+                                                                   prefix + lp.assemble.pre, lp.assemble.count);
+    ++launches;
+    for (const TaskList& tl : lp.extend_vec) {
+      if (tl.ctas == 0) continue;
+      k_fwd_extend<T><<<grid_of(tl.ctas), kSolveRows, 0, s>>>(W, a, parent, rel_off, rel, tasks + tl.off,
+                                                              prefix + tl.pre, tl.count);
+      ++launches;
+    }
+    for (const PanelStep& ps : lp.panels) {
+      k_fwd_diag<T><<<ps.potrf.count, 256, ysm, s>>>(L, W, a, tasks + ps.potrf.off, ps.j0);
+      ++launches;
+      if (ps.solve_upd.ctas > 0) {
+        k_fwd_update<T><<<grid_of(ps.solve_upd.ctas), kSolveRows, ysm, s>>>(
+            L, W, a, tasks + ps.solve_upd.off, prefix + ps.solve_upd.pre, ps.solve_upd.count, ps.j0);
+        ++launches;
+      }
+    }
+  }
+  for (int l = (int)sy.levels.size() - 1; l >= 0; --l) {
+    const LevelPlan& lp = sy.levels[l];
+    k_bwd_init<T><<<grid_of(lp.assemble.ctas), kSolveRows, 0, s>>>(W, x, a, tasks + lp.assemble.off,
+                                                                   prefix + lp.assemble.pre, lp.assemble.count);
+    ++launches;
+    for (int p = (int)lp.panels.size() - 1; p >= 0; --p) {
+      const PanelStep& ps = lp.panels[p];
+      if (ps.solve_upd.ctas > 0) {
+        k_bwd_partial<T><<<grid_of(ps.solve_upd.ctas), kSolveRows, 0, s>>>(
+            L, W, a, part, tasks + ps.solve_upd.off, prefix + ps.solve_upd.pre, ps.solve_upd.count, ps.j0);
+        ++launches;
+      }
+      k_bwd_diag<T><<<ps.potrf.count, 256, ysm, s>>>(L, W, a, part, tasks + ps.solve_upd.off,
+                                                      prefix + ps.solve_upd.pre, ps.j0);
+      ++launches;
+    }
+    k_bwd_store<T><<<grid_of(lp.assemble.ctas), kSolveRows, 0, s>>>(W, x, a, tasks + lp.assemble.off,
+                                                                    prefix + lp.assemble.pre, lp.assemble.count);
+    ++launches;
+  }
+  return launches;
+}
+
+template <class T, int RPT>
+void launch_level_solves(const Symbolic& sy, const T* L, const T* Dinv, T* W, const double* b, double* x,
+                         SolveArgs a, const int* parent, const int64_t* rel_off, const int* rel, const int* tasks,
+                         const int64_t* prefix, FusedArgs fa, int* sync, int& launches, cudaStream_t s) {
+  const int nlev = (int)sy.levels.size();
+  int* tickets = sync;
+  int* fflags = sync + 2 * nlev;
+  int* bflags = fflags + sy.n_flags;
+  cudaMemsetAsync(sync, 0, sizeof(int) * (2 * nlev + 2 * sy.n_flags), s);
+  const size_t ysm = sizeof(T) * SB * a.nrhs;
+  for (int l = 0; l < nlev; ++l) {
+    const LevelPlan& lp = sy.levels[l];
+    k_fwd_init<T><<<grid_of(lp.assemble.ctas), kSolveRows, 0, s>>>(W, b, a, tasks + lp.assemble.off,
+                                                                   prefix + lp.assemble.pre, lp.assemble.count);
+    ++launches;
+    for (const TaskList& tl : lp.extend_vec) {
+      if (tl.ctas == 0) continue;
+      k_fwd_extend<T><<<grid_of(tl.ctas), kSolveRows, 0, s>>>(W, a, parent, rel_off, rel, tasks + tl.off,
+                                                              prefix + tl.pre, tl.count);
+      ++launches;
+    }
+    FusedArgs f = fa;
+    f.items = fa.items + 2 * lp.fwd_off;
+    f.ticket = tickets + 2 * l;
+    f.flags = fflags;
+    k_fwd_level<T, RPT><<<grid_of(lp.fwd_count), 256, ysm, s>>>(L, Dinv, W, a, f);
+    ++launches;
+  }
+  for (int l = nlev - 1; l >= 0; --l) {
+    const LevelPlan& lp = sy.levels[l];
+    k_bwd_init<T><<<grid_of(lp.assemble.ctas), kSolveRows, 0, s>>>(W, x, a, tasks + lp.assemble.off,
+                                                                   prefix + lp.assemble.pre, lp.assemble.count);
+    ++launches;
+    FusedArgs f = fa;
+    f.items = fa.items + 2 * lp.bwd_off;
+    f.ticket = tickets + 2 * l + 1;
+    f.flags = bflags;
+    k_bwd_level<T, RPT><<<grid_of(lp.bwd_count), 256, ysm, s>>>(L, Dinv, W, x, a, f);
+    ++launches;
+  }
+}
+
+template <class T>
+int launch_solve_fused(const Symbolic& sy, const T* L, const T* Dinv, T* W, const double* b, double* x, SolveArgs a,
+                       const int* parent, const int64_t* rel_off, const int* rel, const int* tasks,
+                       const int64_t* prefix, FusedArgs fa, int* sync, cudaStream_t s) {
+  int launches = 0;
+  if (a.nrhs <= 4)
+    launch_level_solves<T, 1>(sy, L, Dinv, W, b, x, a, parent, rel_off, rel, tasks, prefix, fa, sync, launches, s);
+  else if (a.nrhs <= 8)
+    launch_level_solves<T, 2>(sy, L, Dinv, W, b, x, a, parent, rel_off, rel, tasks, prefix, fa, sync, launches, s);
+  else if (a.nrhs <= 16)
+    launch_level_solves<T, 4>(sy, L, Dinv, W, b, x, a, parent, rel_off, rel, tasks, prefix, fa, sync, launches, s);
+  else if (a.nrhs <= 32)
+    launch_level_solves<T, 8>(sy, L, Dinv, W, b, x, a, parent, rel_off, rel, tasks, prefix, fa, sync, launches, s);
+  else
+    launch_level_solves<T, 16>(sy, L, Dinv, W, b, x, a, parent, rel_off, rel, tasks, prefix, fa, sync, launches, s);
+  return launches;
+}
+
+template <class T>
+std::string set_fused_attributes() {
+  const int ysm = (int)(sizeof(T) * SB * kMaxRhs);
+  TDEM_CUDA_TRY(cudaFuncSetAttribute(k_fwd_level<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, ysm));
+  TDEM_CUDA_TRY(cudaFuncSetAttribute(k_fwd_level<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, ysm));
+  TDEM_CUDA_TRY(cudaFuncSetAttribute(k_fwd_level<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, ysm));
+  TDEM_CUDA_TRY(cudaFuncSetAttribute(k_fwd_level<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, ysm));
+  TDEM_CUDA_TRY(cudaFuncSetAttribute(k_fwd_level<T, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, ysm));
+  TDEM_CUDA_TRY(cudaFuncSetAttribute(k_bwd_level<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, ysm));
+  TDEM_CUDA_TRY(cudaFuncSetAttribute(k_bwd_level<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, ysm));
+  TDEM_CUDA_TRY(cudaFuncSetAttribute(k_bwd_level<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, ysm));
+  TDEM_CUDA_TRY(cudaFuncSetAttribute(k_bwd_level<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, ysm));
+  TDEM_CUDA_TRY(cudaFuncSetAttribute(k_bwd_level<T, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, ysm));
+  TDEM_CUDA_TRY(cudaFuncSetAttribute(k_diag_inverse<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(2 * sizeof(double) * SB * (SB + 1))));
+  return "";
+}
 
 }  // namespace
 
 GpuCholesky::~GpuCholesky() {
+  if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
   for (void* p : allocs_) cudaFree(p);
 }
 
@@ -461,18 +1072,17 @@ std::string GpuCholesky::upload(T** dst, const std::vector<T>& src, cudaStream_t
 }
 
 std::string GpuCholesky::setup(Symbolic&& sy, const std::vector<int>& perm_to_vec, int nrhs_max,
-                               cudaStream_t s) {
+                               cudaStream_t s, int precision_bytes) {
   sy_ = std::move(sy);
   nrhs_max_ = std::max(1, nrhs_max);
+  elem_ = (precision_bytes == 4) ? 4 : 8;
   if ((int)perm_to_vec.size() != sy_.n) return "perm_to_vec size mismatch";
-  if (nrhs_max_ * P * (int)sizeof(double) > 96 * 1024) return "too many right-hand sides";
+  if (nrhs_max_ > kMaxRhs) return "too many right-hand sides";
   std::string e;
-  if (!(e = alloc((void**)&d_L_, sizeof(double) * std::max<int64_t>(1, sy_.nnz_l))).empty()) return e;
-  if (!(e = alloc((void**)&d_U_, sizeof(double) * std::max<int64_t>(1, sy_.u_elems))).empty()) return e;
-  if (!(e = alloc((void**)&d_W_, sizeof(double) * std::max<int64_t>(1, sy_.wvec_elems) * nrhs_max_)).empty())
-    return e;
-  if (!(e = alloc((void**)&d_part_, sizeof(double) * std::max<int64_t>(1, sy_.solve_partials) * nrhs_max_)).empty())
-    return e;
+  if (!(e = alloc(&d_L_, elem_ * std::max<int64_t>(1, sy_.nnz_l))).empty()) return e;
+  if (!(e = alloc(&d_U_, elem_ * std::max<int64_t>(1, sy_.u_elems))).empty()) return e;
+  if (!(e = alloc(&d_W_, elem_ * std::max<int64_t>(1, sy_.wvec_elems) * nrhs_max_)).empty()) return e;
+  if (!(e = alloc(&d_part_, elem_ * std::max<int64_t>(1, sy_.solve_partials) * nrhs_max_)).empty()) return e;
   if (!(e = upload(&d_l_off_, sy_.l_off, s)).empty()) return e;
   if (!(e = upload(&d_u_off_, sy_.u_off, s)).empty()) return e;
   if (!(e = upload(&d_w_off_, sy_.wvec_off, s)).empty()) return e;
@@ -491,108 +1101,84 @@ std::string GpuCholesky::setup(Symbolic&& sy, const std::vector<int>& perm_to_ve
   if (!(e = upload(&d_prefix_, sy_.task_prefix, s)).empty()) return e;
   if (!(e = upload(&d_parent_, sy_.front_parent, s)).empty()) return e;
   if (!(e = upload(&d_c0_, sy_.front_c0, s)).empty()) return e;
-  if (!(e = alloc((void**)&d_err_, sizeof(int))).empty()) return e;
-  TDEM_CUDA_TRY(cudaMemsetAsync(d_err_, 0, sizeof(int), s));
-  TDEM_CUDA_TRY(cudaFuncSetAttribute(k_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsmSmem));
-  TDEM_CUDA_TRY(cudaFuncSetAttribute(k_syrk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSyrkSmem));
-  TDEM_CUDA_TRY(cudaFuncSetAttribute(k_fwd_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
-  TDEM_CUDA_TRY(cudaFuncSetAttribute(k_bwd_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
-  TDEM_CUDA_TRY(cudaFuncSetAttribute(k_fwd_update, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+  if (!(e = upload(&d_items_, sy_.solve_items, s)).empty()) return e;
+  if (!(e = upload(&d_flag_off_, sy_.flag_off, s)).empty()) return e;
+  if (!(e = upload(&d_dinv_off_, sy_.dinv_off, s)).empty()) return e;
+  if (!(e = alloc(&d_dinv_, elem_ * std::max<int64_t>(1, sy_.dinv_elems))).empty()) return e;
+  if (!(e = alloc((void**)&d_sync_, sizeof(int) * (2 * sy_.levels.size() + 2 * sy_.n_flags + 1))).empty())
+    return e;
+  if (!(e = alloc((void**)&d_err_, 3 * sizeof(int))).empty()) return e;
+  TDEM_CUDA_TRY(cudaMemsetAsync(d_err_, 0, 3 * sizeof(int), s));
+  if (elem_ == 4 && tc_update_ && !(e = tc_update_setup()).empty()) return e;
+  if (!(e = (elem_ == 4 ? set_attributes<float>() : set_attributes<double>())).empty()) return e;
+  if (!(e = (elem_ == 4 ? set_fused_attributes<float>() : set_fused_attributes<double>())).empty()) return e;
   TDEM_CUDA_TRY(cudaStreamSynchronize(s));
   return "";
 }
 
 void GpuCholesky::factor(const double* d_vals, cudaStream_t s) {
-  int launches = 0;
   Fronts fr{d_l_off_, d_u_off_, d_m_, d_k_};
-  cudaMemsetAsync(d_L_, 0, sizeof(double) * sy_.nnz_l, s);
-  {
-    const int64_t nnz = sy_.nnz_lower;
-    const unsigned g = (unsigned)std::min<int64_t>((nnz + 255) / 256, 148 * 32);
-    if (nnz > 0) {
-      k_scatter_entries<<<g, 256, 0, s>>>(d_L_, d_entry_, d_vals, nnz);
-      ++launches;
-    }
+  const unsigned ni = (unsigned)sy_.inv_count;
+  const size_t ism = 2 * sizeof(double) * SB * (SB + 1);
+  if (elem_ == 4) {
+    launches_factor_ = launch_factor<float>(sy_, (float*)d_L_, (float*)d_U_, d_vals, d_entry_, fr, d_parent_,
+                                            d_rel_off_, d_rel_, d_tasks_, d_prefix_, d_err_, d_c0_, tc_update_, s);
+    if (ni) k_diag_inverse<float><<<ni, 256, ism, s>>>((const float*)d_L_, (float*)d_dinv_, fr, d_dinv_off_,
+                                                       d_items_ + 2 * sy_.inv_off);
+  } else {
+    launches_factor_ = launch_factor<double>(sy_, (double*)d_L_, (double*)d_U_, d_vals, d_entry_, fr, d_parent_,
+                                             d_rel_off_, d_rel_, d_tasks_, d_prefix_, d_err_, d_c0_, false, s);
+    if (ni) k_diag_inverse<double><<<ni, 256, ism, s>>>((const double*)d_L_, (double*)d_dinv_, fr, d_dinv_off_,
+                                                        d_items_ + 2 * sy_.inv_off);
   }
-  const int* T = d_tasks_;
-  const int64_t* Pf = d_prefix_;
-  for (const LevelPlan& lp : sy_.levels) {
-    if (lp.assemble.ctas > 0) {
-      k_zero_u<<<grid_of(lp.assemble.ctas), 256, 0, s>>>(d_U_, fr, T + lp.assemble.off, Pf + lp.assemble.pre,
-                                                        lp.assemble.count);
-      ++launches;
-    }
-    for (const TaskList& tl : lp.extend_slots) {
-      if (tl.ctas == 0) continue;
-      k_extend_add<<<grid_of(tl.ctas), 256, 0, s>>>(d_L_, d_U_, fr, d_parent_, d_rel_off_, d_rel_, T + tl.off,
-                                                    Pf + tl.pre, tl.count);
-      ++launches;
-    }
-    for (const PanelStep& ps : lp.panels) {
-      k_potrf<<<ps.potrf.count, 256, 0, s>>>(d_L_, fr, T + ps.potrf.off, ps.j0, d_err_, d_c0_);
-      ++launches;
-      if (ps.trsm.ctas > 0) {
-        k_trsm<<<grid_of(ps.trsm.ctas), kTrsmRows, kTrsmSmem, s>>>(d_L_, fr, T + ps.trsm.off, Pf + ps.trsm.pre,
-                                                           ps.trsm.count, ps.j0);
-        ++launches;
-      }
-      if (ps.syrk.ctas > 0) {
-        k_syrk<<<grid_of(ps.syrk.ctas), 256, kSyrkSmem, s>>>(d_L_, d_U_, fr, T + ps.syrk.off, Pf + ps.syrk.pre,
-                                                     ps.syrk.count, ps.j0);
-        ++launches;
-      }
-    }
-  }
-  launches_factor_ = launches;
+  if (ni) ++launches_factor_;
 }
 
 void GpuCholesky::solve(const double* d_b, double* d_x, int64_t ld, int nrhs, cudaStream_t s) {
-  int launches = 0;
   SolveArgs a{d_l_off_, d_w_off_, d_m_, d_k_, d_rows_off_, d_rows_, nrhs, ld};
-  const int* T = d_tasks_;
-  const int64_t* Pf = d_prefix_;
-  const size_t ysm = sizeof(double) * P * nrhs;
-  for (const LevelPlan& lp : sy_.levels) {
-    k_fwd_init<<<grid_of(lp.assemble.ctas), kSolveRows, 0, s>>>(d_W_, d_b, a, T + lp.assemble.off,
-                                                                Pf + lp.assemble.pre, lp.assemble.count);
-    ++launches;
-    for (const TaskList& tl : lp.extend_vec) {
-      if (tl.ctas == 0) continue;
-      k_fwd_extend<<<grid_of(tl.ctas), kSolveRows, 0, s>>>(d_W_, a, d_parent_, d_rel_off_, d_rel_, T + tl.off,
-                                                           Pf + tl.pre, tl.count);
-      ++launches;
-    }
-    for (const PanelStep& ps : lp.panels) {
-      k_fwd_diag<<<ps.potrf.count, 256, ysm, s>>>(d_L_, d_W_, a, T + ps.potrf.off, ps.j0);
-      ++launches;
-      if (ps.solve_upd.ctas > 0) {
-        k_fwd_update<<<grid_of(ps.solve_upd.ctas), kSolveRows, ysm, s>>>(
-            d_L_, d_W_, a, T + ps.solve_upd.off, Pf + ps.solve_upd.pre, ps.solve_upd.count, ps.j0);
-        ++launches;
-      }
-    }
+  if (!panel_solve_) {
+    FusedArgs fa{d_items_, nullptr, nullptr, d_flag_off_, d_dinv_off_, d_err_};
+    if (elem_ == 4)
+      launches_solve_ = launch_solve_fused<float>(sy_, (const float*)d_L_, (const float*)d_dinv_, (float*)d_W_, d_b,
+                                                  d_x, a, d_parent_, d_rel_off_, d_rel_, d_tasks_, d_prefix_, fa,
+                                                  d_sync_, s);
+    else
+      launches_solve_ = launch_solve_fused<double>(sy_, (const double*)d_L_, (const double*)d_dinv_, (double*)d_W_,
+                                                   d_b, d_x, a, d_parent_, d_rel_off_, d_rel_, d_tasks_, d_prefix_,
+                                                   fa, d_sync_, s);
+    return;
   }
-  for (int l = (int)sy_.levels.size() - 1; l >= 0; --l) {
-    const LevelPlan& lp = sy_.levels[l];
-    k_bwd_init<<<grid_of(lp.assemble.ctas), kSolveRows, 0, s>>>(d_W_, d_x, a, T + lp.assemble.off,
-                                                                Pf + lp.assemble.pre, lp.assemble.count);
-    ++launches;
-    for (int p = (int)lp.panels.size() - 1; p >= 0; --p) {
-      const PanelStep& ps = lp.panels[p];
-      if (ps.solve_upd.ctas > 0) {
-        k_bwd_partial<<<grid_of(ps.solve_upd.ctas), kSolveRows, 0, s>>>(
-            d_L_, d_W_, a, d_part_, T + ps.solve_upd.off, Pf + ps.solve_upd.pre, ps.solve_upd.count, ps.j0);
-        ++launches;
-      }
-      k_bwd_diag<<<ps.potrf.count, 256, ysm, s>>>(d_L_, d_W_, a, d_part_, T + ps.solve_upd.off,
-                                                   Pf + ps.solve_upd.pre, ps.j0);
-      ++launches;
+  if (elem_ == 4)
+    launches_solve_ = launch_solve<float>(sy_, (const float*)d_L_, (float*)d_W_, (float*)d_part_, d_b, d_x, a,
+                                          d_parent_, d_rel_off_, d_rel_, d_tasks_, d_prefix_, s);
+  else
+    launches_solve_ = launch_solve<double>(sy_, (const double*)d_L_, (double*)d_W_, (double*)d_part_, d_b, d_x, a,
+                                           d_parent_, d_rel_off_, d_rel_, d_tasks_, d_prefix_, s);
+}
+
+std::string GpuCholesky::solve_graph(const double* d_b, double* d_x, int64_t ld, int nrhs, cudaStream_t s) {
+  if (!graph_exec_ || g_b_ != d_b || g_x_ != d_x || g_ld_ != ld || g_nrhs_ != nrhs) {
+    if (graph_exec_) {
+      cudaGraphExecDestroy(graph_exec_);
+      graph_exec_ = nullptr;
     }
-    k_bwd_store<<<grid_of(lp.assemble.ctas), kSolveRows, 0, s>>>(d_W_, d_x, a, T + lp.assemble.off,
-                                                                 Pf + lp.assemble.pre, lp.assemble.count);
-    ++launches;
+    cudaGraph_t g = nullptr;
+    TDEM_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    solve(d_b, d_x, ld, nrhs, s);
+    TDEM_CUDA_TRY(cudaStreamEndCapture(s, &g));
+    const cudaError_t ie = cudaGraphInstantiate(&graph_exec_, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) {
+      graph_exec_ = nullptr;
+      return std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ie);
+    }
+    g_b_ = d_b;
+    g_x_ = d_x;
+    g_ld_ = ld;
+    g_nrhs_ = nrhs;
   }
-  launches_solve_ = launches;
+  TDEM_CUDA_TRY(cudaGraphLaunch(graph_exec_, s));
+  return "";
 }
 
 int GpuCholesky::status(cudaStream_t s) {
@@ -600,6 +1186,13 @@ int GpuCholesky::status(cudaStream_t s) {
   cudaMemcpyAsync(&h, d_err_, sizeof(int), cudaMemcpyDeviceToHost, s);
   cudaStreamSynchronize(s);
   return h;
+}
+
+int GpuCholesky::solve_status(cudaStream_t s) {
+  int h[2] = {0, 0};
+  cudaMemcpyAsync(h, d_err_ + 1, 2 * sizeof(int), cudaMemcpyDeviceToHost, s);
+  cudaStreamSynchronize(s);
+  return h[0] ? 1 : (h[1] ? 2 : 0);
 }
 
 }  // namespace tdem

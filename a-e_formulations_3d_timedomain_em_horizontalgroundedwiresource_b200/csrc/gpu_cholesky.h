@@ -16,6 +16,8 @@
 
 namespace tdem {
 
+constexpr int kMaxRhs = 64;  // right-hand sides per solve
+
 class GpuCholesky {
  public:
   GpuCholesky() = default;
@@ -28,7 +30,7 @@ class GpuCholesky {
   // permuted unknown p (lets the solve read and write the caller's natural-order
   // vectors directly).
   std::string setup(Symbolic&& sy, const std::vector<int>& perm_to_vec, int nrhs_max,
-                    cudaStream_t stream);
+                    cudaStream_t stream, int precision_bytes = 8);
 
   // Numeric factorization.  d_lower_vals holds the lower-CSR values of the
   // analysed pattern (device, nnz_lower doubles).  Errors (non-positive pivot)
@@ -39,9 +41,22 @@ class GpuCholesky {
   // dimension ld (positions given by perm_to_vec); x rows not covered by the
   // system are left untouched.  b and x may alias.
   void solve(const double* d_b, double* d_x, int64_t ld, int nrhs, cudaStream_t stream);
+  // Same as solve(), replayed from a CUDA graph captured on first use for these
+  // buffers (the factor values may change between calls; the pointers may not).
+  std::string solve_graph(const double* d_b, double* d_x, int64_t ld, int nrhs, cudaStream_t stream);
+  int precision_bytes() const { return elem_; }
 
   // 0 = ok, otherwise 1-based permuted column of the first non-positive pivot.
   int status(cudaStream_t stream);
+  // 0 = ok; 1 = a wait of the level solves gave up, 2 = a wait of the
+  // tensor-core update gave up (results since setup are not valid).
+  int solve_status(cudaStream_t stream);
+  // FP32 factor: trailing updates on the tensor cores (3xTF32) or on the
+  // CUDA cores (default).  Takes effect at setup().
+  void set_tensor_core_update(bool on) { tc_update_ = on; }
+  // Selects the per-panel solve (one launch per 64-column panel and level) instead
+  // of the fused level solves; both compute the same triangular solves.
+  void set_panel_solve(bool on) { panel_solve_ = on; }
 
   const Symbolic& symbolic() const { return sy_; }
   size_t device_bytes() const { return bytes_; }
@@ -53,11 +68,19 @@ class GpuCholesky {
   int nrhs_max_ = 0;
   size_t bytes_ = 0;
   int launches_factor_ = 0, launches_solve_ = 0;
+  int elem_ = 8;                 // bytes per factor entry (8 = FP64, 4 = FP32)
+  bool panel_solve_ = false;
+  bool tc_update_ = false;
+  cudaGraphExec_t graph_exec_ = nullptr;
+  const double* g_b_ = nullptr;
+  double* g_x_ = nullptr;
+  int64_t g_ld_ = 0;
+  int g_nrhs_ = 0;
   // device arrays
-  double* d_L_ = nullptr;
-  double* d_U_ = nullptr;
-  double* d_W_ = nullptr;        // solve front vectors (sum m) x nrhs_max
-  double* d_part_ = nullptr;     // backward partial sums
+  void* d_L_ = nullptr;
+  void* d_U_ = nullptr;
+  void* d_W_ = nullptr;          // solve front vectors (sum m) x nrhs_max
+  void* d_part_ = nullptr;       // backward partial sums
   int64_t* d_l_off_ = nullptr;
   int64_t* d_u_off_ = nullptr;
   int64_t* d_w_off_ = nullptr;
@@ -72,7 +95,13 @@ class GpuCholesky {
   int64_t* d_prefix_ = nullptr;
   int* d_parent_ = nullptr;
   int* d_c0_ = nullptr;
-  int* d_err_ = nullptr;
+  int* d_err_ = nullptr;         // [0] first non-positive pivot, [1] level-solve wait gave up,
+                                 // [2] tensor-core update wait gave up
+  int* d_items_ = nullptr;       // solve / inversion items (front, block)
+  int64_t* d_flag_off_ = nullptr;
+  int64_t* d_dinv_off_ = nullptr;
+  void* d_dinv_ = nullptr;       // inverted diagonal blocks
+  int* d_sync_ = nullptr;        // level tickets + pivot-block flags of one solve
   std::vector<void*> allocs_;
   template <class T>
   std::string upload(T** dst, const std::vector<T>& src, cudaStream_t s);

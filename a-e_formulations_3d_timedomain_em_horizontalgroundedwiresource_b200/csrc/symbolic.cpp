@@ -420,29 +420,88 @@ std::string analyse(int n, const int64_t* rowptr, const int* colind, const doubl
     for (int j0 = 0; j0 < kmax; j0 += kPanel) {
       PanelStep ps;
       ps.j0 = j0;
-      std::vector<int> fr;
-      std::vector<int64_t> c1, c2, c3, c4;
+      std::vector<int> fr, fin, fbig;
+      std::vector<int64_t> c1, c2, c3, c4, c5;
+      const int J0 = (j0 / kOuter) * kOuter;
       for (int s : lp.fronts) {
         const int k = sy.front_k[s], m = sy.front_m[s];
         if (k <= j0) continue;
         const int j1 = std::min(k, j0 + kPanel);
+        const int J1 = std::min(k, J0 + kOuter);
         const int64_t below = m - j1;
         fr.push_back(s);
         c1.push_back(1);
         c2.push_back(cdiv(below, kTrsmRows));
-        const int64_t nt = cdiv(below, kTileSyrk);
-        c3.push_back(nt * (nt + 1) / 2);
         c4.push_back(cdiv(below, kSolveRows));
+        if (j1 < J1) {
+          // rows [j1, m) x columns [j1, J1) of the outer panel, lower-triangle tiles
+          const int64_t nr = cdiv(below, kTileSyrk), nc = cdiv(J1 - j1, kTileSyrk);
+          fin.push_back(s);
+          c3.push_back(nc * nr - nc * (nc - 1) / 2);
+        } else if (m > J1) {
+          const int64_t nt = cdiv(m - J1, kTileBig);
+          fbig.push_back(s);
+          c5.push_back(nt * (nt + 1) / 2);
+        }
       }
       add_tasks(sy, ps.potrf, fr, c1);
       add_tasks(sy, ps.trsm, fr, c2);
-      add_tasks(sy, ps.syrk, fr, c3);
+      add_tasks(sy, ps.syrk, fin, c3);
+      add_tasks(sy, ps.syrk_big, fbig, c5);
       add_tasks(sy, ps.solve_upd, fr, c4);
       max_partials = std::max(max_partials, ps.solve_upd.ctas);
       lp.panels.push_back(ps);
     }
   }
   sy.solve_partials = max_partials * kPanel;
+
+  // fused-solve items, flags and inverted diagonal blocks
+  {
+    sy.flag_off.assign(nf, 0);
+    sy.dinv_off.assign(nf, 0);
+    for (int s = 0; s < nf; ++s) {
+      const int k = sy.front_k[s];
+      const int pb = (int)cdiv(k, kPanel);
+      sy.flag_off[s] = sy.n_flags;
+      sy.n_flags += pb;
+      sy.dinv_off[s] = sy.dinv_elems;
+      sy.dinv_elems += (int64_t)(pb - 1) * kPanel * kPanel + (int64_t)(k - (pb - 1) * kPanel) * (k - (pb - 1) * kPanel);
+    }
+    auto push = [&](int s, int b) {
+      sy.solve_items.push_back(s);
+      sy.solve_items.push_back(b);
+    };
+    for (int l = 0; l < nlev; ++l) {
+      LevelPlan& lp = sy.levels[l];
+      // forward: block b of front s, b < pb pivot blocks, then update blocks
+      int bmax = 0;
+      for (int s : lp.fronts) {
+        const int m = sy.front_m[s], k = sy.front_k[s];
+        bmax = std::max(bmax, (int)(cdiv(k, kPanel) + cdiv(m - k, kPanel)));
+      }
+      lp.fwd_off = (int64_t)sy.solve_items.size() / 2;
+      for (int b = 0; b < bmax; ++b)
+        for (int s : lp.fronts) {
+          const int m = sy.front_m[s], k = sy.front_k[s];
+          if (b < cdiv(k, kPanel) + cdiv(m - k, kPanel)) push(s, b);
+        }
+      lp.fwd_count = (int64_t)sy.solve_items.size() / 2 - lp.fwd_off;
+      // backward: pivot blocks, last first
+      int pmax = 0;
+      for (int s : lp.fronts) pmax = std::max(pmax, (int)cdiv(sy.front_k[s], kPanel));
+      lp.bwd_off = (int64_t)sy.solve_items.size() / 2;
+      for (int d = 0; d < pmax; ++d)
+        for (int s : lp.fronts) {
+          const int pb = (int)cdiv(sy.front_k[s], kPanel);
+          if (d < pb) push(s, pb - 1 - d);
+        }
+      lp.bwd_count = (int64_t)sy.solve_items.size() / 2 - lp.bwd_off;
+    }
+    sy.inv_off = (int64_t)sy.solve_items.size() / 2;
+    for (int s = 0; s < nf; ++s)
+      for (int b = 0; b < cdiv(sy.front_k[s], kPanel); ++b) push(s, b);
+    sy.inv_count = (int64_t)sy.solve_items.size() / 2 - sy.inv_off;
+  }
 
   // Update-block workspace: first-fit plan over the level sequence.  A block is
   // allocated when its front's level starts and released once the parent's level

@@ -22,7 +22,9 @@
 namespace tdem {
 
 constexpr int kPanel = 64;       // dense panel width of the factorization and solves
-constexpr int kTileSyrk = 64;    // trailing-update tile edge
+constexpr int kOuter = 256;      // outer panel width: trailing updates of rank up to kOuter
+constexpr int kTileSyrk = 64;    // tile edge of the update inside an outer panel
+constexpr int kTileBig = 128;    // tile edge of the rank-kOuter trailing update
 constexpr int kTrsmRows = 128;   // rows per CTA of the panel triangular solve
 constexpr int kSolveRows = 256;  // rows per CTA of the solve updates
 
@@ -44,11 +46,14 @@ struct TaskList {
   int64_t ctas = 0;    // total CTAs
 };
 
+// One 64-wide inner panel [j0, j1) of the factorization, j1 = min(k, j0 + 64).  The
+// outer panel is [J0, J1), J0 = floor(j0 / kOuter) * kOuter, J1 = min(k, J0 + kOuter).
 struct PanelStep {
   int j0 = 0;          // panel start (fronts with k > j0 take part)
   TaskList potrf;      // one CTA per front
   TaskList trsm;       // ceil((m - j1) / kTrsmRows) CTAs per front
-  TaskList syrk;       // triangle of kTileSyrk tiles per front
+  TaskList syrk;       // update of columns [j1, J1) (rows >= j1) by the inner panel, 64-tiles
+  TaskList syrk_big;   // at the end of an outer panel: trailing [J1, m) by [J0, J1), 128-tiles
   TaskList solve_upd;  // ceil((m - j1) / kSolveRows) CTAs per front (fwd update / bwd partials)
 };
 
@@ -58,6 +63,13 @@ struct LevelPlan {
   std::vector<TaskList> extend_vec;    // solve extend-add per child slot, kSolveRows rows per CTA
   TaskList assemble;                   // solve: front-vector init, ceil(m / kSolveRows) CTAs each
   std::vector<PanelStep> panels;
+  // Fused triangular solves: one CTA per 64-row block of every front at this
+  // level, items (front, block) at solve_items[2 * off ...].  Forward blocks are
+  // the pivot blocks b < ceil(k / 64) then the update blocks; sorted by block
+  // index so every block a CTA waits for has a smaller ticket.  Backward items are
+  // the pivot blocks in descending order.
+  int64_t fwd_off = 0, fwd_count = 0;
+  int64_t bwd_off = 0, bwd_count = 0;
 };
 
 struct Symbolic {
@@ -83,6 +95,13 @@ struct Symbolic {
   std::vector<int64_t> wvec_off;     // per front: offset of its m-long solve vector
   std::vector<int> tasks;            // concatenated task front lists
   std::vector<int64_t> task_prefix;  // concatenated CTA prefix sums
+
+  std::vector<int> solve_items;      // (front, block) pairs of the fused solves and inversions
+  std::vector<int64_t> flag_off;     // per front: index of its first pivot-block flag
+  std::vector<int64_t> dinv_off;     // per front: offset of its inverted diagonal blocks
+  int64_t n_flags = 0;               // pivot blocks over all fronts
+  int64_t dinv_elems = 0;            // sum over pivot blocks of w^2 (w = block width)
+  int64_t inv_off = 0, inv_count = 0;  // items of the diagonal-block inversion (all pivot blocks)
 
   int64_t u_elems = 0;        // peak update-workspace size (elements)
   int64_t u_sum = 0;          // sum of r^2 (workspace without reuse)

@@ -75,7 +75,21 @@ typedef struct tdem_info {
   double run_gpu_ms, factor_gpu_ms, solve_gpu_ms;
   int64_t h2d_bytes;        /* host->device bytes copied so far by this solver */
   int64_t d2h_bytes;        /* device->host bytes copied so far by this solver */
+  int precision;            /* 64 = FP64 factor; 32 = FP32 factor + FP64 refinement */
+  int refine_iters;         /* conjugate-gradient iterations of the last run (precision 32) */
+  int refine_iters_max;     /* most iterations any time step needed */
+  double refine_worst;      /* largest final relative residual of any step / column */
 } tdem_info;
+
+/* Options of tdem_solver_create_ex (zero-initialise, then set what differs). */
+typedef struct tdem_options {
+  int precision;            /* 64 (default when 0): FP64 factorization, one direct solve per
+                               step.  32: FP32 factorization used as the preconditioner of an
+                               FP64 conjugate-gradient solve on the FP64 system */
+  double refine_tol;        /* relative residual to reach per step and column (default 1e-10) */
+  int refine_maxit;         /* iteration cap; exceeding it is TDEM_ERR_NUMERIC (default 200) */
+  int leaf_size;            /* nested-dissection leaf size (default 128) */
+} tdem_options;
 
 /* Creates a solver for the model in `workdir` (reads the input files, analyses
  * the sparsity pattern, assembles the FEM matrices on the device and prepares the
@@ -83,6 +97,9 @@ typedef struct tdem_info {
  * (time_approx.cpp:169-557). */
 tdem_status tdem_solver_create(const char* workdir, int formulation, int scheme, int device,
                                tdem_solver** out);
+/* tdem_solver_create with options (opts may be NULL for the defaults). */
+tdem_status tdem_solver_create_ex(const char* workdir, int formulation, int scheme, int device,
+                                  const tdem_options* opts, tdem_solver** out);
 /* Runs all decades / time steps (TaskSP.cpp:628-702, Three_Layers_Schema). */
 tdem_status tdem_solver_run(tdem_solver* s);
 /* Writes the reference output files into the model directory (Gather_edsall,
@@ -120,6 +137,20 @@ void pardiso_64(void* pt, const long long* maxfct, const long long* mnum, const 
                 const long long* msglvl, void* b, void* x, long long* error);
 /* MKL threading call made by pardiso_solver::factorize (pardiso.cpp:83); no-op here. */
 void mkl_set_num_threads(int n);
+
+/* Residual norms of a block of solutions, computed on CUDA device `device`:
+ * norms[2j] = ||b_j - A x_j||_2 and norms[2j+1] = ||b_j||_2 for j < ncols.
+ * A is n x n in full CSR (both triangles), 0-based: rowptr (n+1 int64), col
+ * (int32), val (FP64).  x, b: column-major n x ncols with leading dimension ld.
+ * Every pointer is device memory; the work is queued on `stream` (a cudaStream_t,
+ * NULL for the legacy default stream) and norms are valid once it completes.
+ * 1 <= ncols <= 64.  The result is deterministic (fixed reduction order).
+ * Scratch is taken from the stream-ordered allocator for each call.
+ * No counterpart in the reference: pardiso_solver::solve_nrhs (pardiso.cpp:113-120)
+ * never checks its solutions; this lets a caller of the solver boundary do so. */
+tdem_status tdem_residual_norms(int device, int64_t n, const int64_t* rowptr, const int* col,
+                                const double* val, const double* x, const double* b, int64_t ld,
+                                int ncols, double* norms, void* stream);
 
 /* Library version string. */
 const char* tdem_version(void);
