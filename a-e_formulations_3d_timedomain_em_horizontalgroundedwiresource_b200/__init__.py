@@ -87,6 +87,7 @@ class TdemOptions(ctypes.Structure):
         ("refine_tol", ctypes.c_double),
         ("refine_maxit", ctypes.c_int),
         ("leaf_size", ctypes.c_int),
+        ("fp32_update", ctypes.c_int),
     ]
 
 
@@ -94,6 +95,7 @@ _lib: Optional[ctypes.CDLL] = None
 
 EXPORTED = [
     "tdem_run_directory",
+    "tdem_stationary_directory",
     "tdem_solver_create",
     "tdem_solver_create_ex",
     "tdem_solver_run",
@@ -124,6 +126,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.tdem_run_directory.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                        ctypes.c_char_p, ctypes.c_size_t]
     lib.tdem_run_directory.restype = ctypes.c_int
+    lib.tdem_stationary_directory.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t]
+    lib.tdem_stationary_directory.restype = ctypes.c_int
     lib.tdem_solver_create.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                        ctypes.POINTER(P)]
     lib.tdem_solver_create.restype = ctypes.c_int
@@ -170,14 +174,29 @@ def run_directory(workdir: str, formulation="A", scheme: int = 2, device: int = 
         raise TdemError(st, buf.value.decode(errors="replace"))
 
 
+def stationary_directory(workdir: str, device: int = 0) -> None:
+    """Drop-in run of CalcStat3D_3T_A in workdir: the grounded-wire stationary
+    initial field on the GPU (writes v3n.dat, v3a.dat and a0.dat)."""
+    lib = load_library()
+    buf = ctypes.create_string_buffer(2048)
+    st = lib.tdem_stationary_directory(os.fsencode(workdir), int(device), buf, len(buf))
+    if st != 0:
+        raise TdemError(st, buf.value.decode(errors="replace"))
+
+
 class Solver:
     """A transient forward solve held on one GPU: create -> run -> results / write_outputs."""
 
     def __init__(self, workdir: str, formulation="A", scheme: int = 2, device: int = 0, precision: int = 64,
-                 refine_tol: float = 1e-10, refine_maxit: int = 200, leaf_size: int = 128):
+                 refine_tol: float = 1e-10, refine_maxit: int = 200, leaf_size: int = 128,
+                 fp32_update: str = "default"):
         self._lib = load_library()
         self._h = ctypes.c_void_p()
-        opts = TdemOptions(int(precision), float(refine_tol), int(refine_maxit), int(leaf_size))
+        engines = {"default": 0, "cuda_cores": 1, "tensor_cores": 2}
+        if fp32_update not in engines:
+            raise ValueError("fp32_update must be one of %s" % sorted(engines))
+        opts = TdemOptions(int(precision), float(refine_tol), int(refine_maxit), int(leaf_size),
+                           engines[fp32_update])
         st = self._lib.tdem_solver_create_ex(os.fsencode(workdir), _form(formulation), int(scheme), int(device),
                                              ctypes.byref(opts), ctypes.byref(self._h))
         if st != 0:

@@ -11,6 +11,7 @@
 
 #include "driver.h"
 #include "gpu_cholesky.h"
+#include "stationary.h"
 #include "symbolic.h"
 
 struct tdem_solver {
@@ -70,6 +71,8 @@ tdem_status tdem_solver_create_ex(const char* workdir, int formulation, int sche
     if (opts->refine_tol > 0) opt.refine_tol = opts->refine_tol;
     if (opts->refine_maxit > 0) opt.refine_maxit = opts->refine_maxit;
     if (opts->leaf_size > 0) opt.leaf_size = opts->leaf_size;
+    if (opts->fp32_update < 0 || opts->fp32_update > 2) return TDEM_ERR_ARGUMENT;
+    opt.fp32_update = opts->fp32_update;
   }
   if (opt.precision != 64 && opt.precision != 32) return TDEM_ERR_ARGUMENT;
   s->precision = opt.precision;
@@ -180,6 +183,13 @@ tdem_status tdem_run_directory(const char* workdir, int formulation, int scheme,
   put_err(errbuf, errlen, s ? s->error : std::string("invalid arguments"));
   tdem_solver_destroy(s);
   return st;
+}
+
+tdem_status tdem_stationary_directory(const char* workdir, int device, char* errbuf, size_t errlen) {
+  if (!workdir) return TDEM_ERR_ARGUMENT;
+  const std::string e = tdem::solve_stationary(workdir, device);
+  put_err(errbuf, errlen, e);
+  return classify(e);
 }
 
 // ---------------------------------------------------------------------------

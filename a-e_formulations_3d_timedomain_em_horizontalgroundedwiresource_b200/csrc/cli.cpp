@@ -6,6 +6,10 @@
 // Without flags the variant is taken from the program name when it ends in
 // _A2, _A3, _E2 or _E3 (one name per reference build), else A-form, two-point.
 // Unlike the reference, which always exits 0, the exit code is the tdem_status.
+//
+// Installed under a name containing CalcStat3D (or run with --stationary) it is
+// the drop-in for CalcStat3D_3T_A instead: the stationary initial field
+// (v3n.dat, v3a.dat, a0.dat) of the model in workdir.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -15,8 +19,10 @@
 
 int main(int argc, char** argv) {
   int form = 0, scheme = 2, device = 0;
+  bool stationary = false;
   std::string dir = ".";
   const std::string prog = argv[0];
+  if (prog.find("CalcStat3D") != std::string::npos) stationary = true;
   if (prog.size() >= 3) {
     const std::string tail = prog.substr(prog.size() - 3);
     if (tail == "_A2") { form = 0; scheme = 2; }
@@ -32,14 +38,21 @@ int main(int argc, char** argv) {
       scheme = atoi(argv[++i]);
     } else if (!strcmp(argv[i], "--device") && i + 1 < argc) {
       device = atoi(argv[++i]);
+    } else if (!strcmp(argv[i], "--stationary")) {
+      stationary = true;
     } else if (argv[i][0] == '-') {
-      fprintf(stderr, "usage: %s [--form A|E] [--scheme 2|3] [--device N] [workdir]\n", argv[0]);
+      fprintf(stderr, "usage: %s [--form A|E] [--scheme 2|3] [--stationary] [--device N] [workdir]\n", argv[0]);
       return (int)TDEM_ERR_ARGUMENT;
     } else {
       dir = argv[i];
     }
   }
   char err[1024] = {0};
+  if (stationary) {
+    const tdem_status st = tdem_stationary_directory(dir.c_str(), device, err, sizeof err);
+    if (st != TDEM_OK) fprintf(stderr, "CalcStat3D_3T_A (B200): %s\n", err);
+    return (int)st;
+  }
   const tdem_status st = tdem_run_directory(dir.c_str(), form, scheme, device, err, sizeof err);
   if (st != TDEM_OK) fprintf(stderr, "CalcNonstat3DLine (B200): %s\n", err);
   return (int)st;

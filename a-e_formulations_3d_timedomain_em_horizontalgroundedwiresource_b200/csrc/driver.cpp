@@ -189,7 +189,7 @@ std::string TransientSolve::prepare(const std::string& dir, const RunOptions& op
   for (int64_t p = 0; p < n_int_; ++p) p2v[p] = int_edge[sy.iperm[p]];
   if (opt.precision != 64 && opt.precision != 32) return "precision must be 64 or 32";
   chol_.reset(new GpuCholesky());
-  if (const char* tc = std::getenv("TDEM_TC_UPDATE")) chol_->set_tensor_core_update(tc[0] != '0');
+  if (opt.fp32_update != 0) chol_->set_tensor_core_update(opt.fp32_update == 2);
   e = chol_->setup(std::move(sy), p2v, npls_, s_, opt.precision == 32 ? 4 : 8);
   if (!e.empty()) return e;
   if (const char* ps = std::getenv("TDEM_PANEL_SOLVE")) chol_->set_panel_solve(ps[0] == '1');
@@ -396,7 +396,14 @@ std::string TransientSolve::refine(double* x) {
     launch_pcg_dir(d_rz_, d_rzn_, d_z_, d_p_, n_, npls_, s_);
     launches_ += 4 + chol_->kernel_launches_solve();
   }
-  if (it > opt_.refine_maxit) return "mixed-precision refinement did not reach the tolerance";
+  if (it > opt_.refine_maxit) {
+    char buf[160];
+    std::snprintf(buf, sizeof buf,
+                  "mixed-precision refinement did not reach the tolerance: relative residual %.3e after %d "
+                  "iterations (step %d)",
+                  worst, opt_.refine_maxit, pt_.steps + 1);
+    return buf;
+  }
   pt_.refine_iters += it;
   pt_.refine_iters_max = std::max(pt_.refine_iters_max, it);
   pt_.refine_worst = std::max(pt_.refine_worst, worst);

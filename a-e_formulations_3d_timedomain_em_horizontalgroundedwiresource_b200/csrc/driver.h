@@ -19,6 +19,7 @@ struct RunOptions {
   int formulation = 0;   // 0 = A (vector potential), 1 = E (electric field)
   int scheme = 2;        // 2 = two-point (backward Euler), 3 = three-point (BDF2)
   int leaf_size = 128;   // nested-dissection leaf size
+  int fp32_update = 0;   // precision 32 trailing updates: 0 default, 1 CUDA cores, 2 tensor cores
   // 64: FP64 factor, one direct solve per step.  32: FP32 factor used as the
   // preconditioner of an FP64 conjugate-gradient solve on the FP64 system, run to
   // a relative residual of refine_tol in every column.

@@ -11,8 +11,8 @@
 //
 // CTA = 9 warps.  Warps 0-7 are producers: they read the panel from global
 // memory (coalesced along rows, any alignment), split it and store both halves
-// into shared memory in the canonical MN-major 128-byte-swizzled layout that the
-// UMMA descriptors describe; warps 0-3 handle even K stages, 4-7 odd ones.
+// into shared memory in the K-major 128-byte-swizzled layout that the UMMA
+// descriptors describe; warps 0-3 handle even K stages, 4-7 odd ones.
 // Warp 8 issues tcgen05.mma (M = N = 128, K = 8 per instruction) from one lane
 // and commits each stage to an mbarrier that frees the stage's buffers.  After
 // the last stage the producer warps read the accumulator from tensor memory
@@ -41,10 +41,15 @@ constexpr int NPROD = 256;               // producer threads (8 warps)
 constexpr int NTHREADS = NPROD + 32;     // + the MMA warp
 constexpr size_t SMEM_BYTES = (size_t)NSTAGE * STAGE_BYTES + 1024 /* alignment */ + 256 /* barriers */;
 constexpr unsigned kWaitLimit = 1u << 22;
+constexpr int kTcLayout = 2;             // operand layout used by the factorization (K-major)
 
-// instruction descriptor: D F32, A/B TF32, both MN-major, M = N = 128
-constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | (1u << 15) | (1u << 16) |
-                            ((uint32_t)(TM >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
+// instruction descriptor: D F32, A/B TF32, M = N = 128; A and B MN-major (bits
+// 15, 16) for layouts 0 and 1, K-major for layout 2
+template <int LAYOUT>
+__host__ __device__ constexpr uint32_t idesc() {
+  return (1u << 4) | (2u << 7) | (2u << 10) | (LAYOUT == 2 ? 0u : (1u << 15) | (1u << 16)) |
+         ((uint32_t)(TM >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -56,19 +61,40 @@ __device__ __forceinline__ float tf32_rna(float x) {
   return __uint_as_float(r);
 }
 
-// byte offset of element (mn, kk) of a 128 x 32 operand half: 8 swizzle atoms of
-// 32 (MN) x 8 (K) elements, atom (a, g) at (4 g + a) * 1024; inside an atom line
-// kk % 8 holds 32 consecutive MN elements in 16-byte chunks XOR-ed with the line.
+// Operand layouts in shared memory (128-byte swizzle: the 16-byte chunk index
+// inside a 128-byte line is XOR-ed with the line index modulo 8).
+//   LAYOUT 0 / 1: MN-major.  8 atoms of 32 (MN) x 8 (K) elements, atom (a, g) at
+//     (4 g + a) * 1024; line kk % 8 of an atom holds 32 consecutive MN elements.
+//     Layout 0 gives the MN-atom stride (1024 B) as the leading byte offset and
+//     the K-group stride (4096 B) as the stride byte offset; layout 1 the reverse.
+//   LAYOUT 2: K-major.  16 groups of 8 MN rows, group at (mn / 8) * 1024; row
+//     mn % 8 is one line of 32 consecutive K elements.
+template <int LAYOUT>
 __device__ __forceinline__ uint32_t sw_off(int mn, int kk) {
+  if (LAYOUT == 2) {
+    const int row = mn & 7;
+    return (uint32_t)((mn >> 3) * 1024 + row * 128 + ((((kk >> 2) ^ row) & 7) << 4) + ((kk & 3) << 2));
+  }
   const int line = kk & 7;
   return (uint32_t)(((kk >> 3) * 4 + (mn >> 5)) * 1024 + line * 128 + ((((mn & 31) >> 2) ^ line) << 4) +
                     ((mn & 3) << 2));
 }
 
-// UMMA shared-memory descriptor of one K = 8 slice: LBO = MN-atom stride 1024 B,
-// SBO = K-group stride 4096 B, version 1, 128-byte swizzle.
-__device__ __forceinline__ uint64_t sdesc(uint32_t addr) {
-  return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)(1024 >> 4) << 16) | ((uint64_t)(4096 >> 4) << 32) |
+// UMMA shared-memory descriptor of the K = 8 slice ks of an operand half at addr
+// (version 1, 128-byte swizzle).
+template <int LAYOUT>
+__device__ __forceinline__ uint64_t sdesc(uint32_t addr, int ks) {
+  uint32_t start, lbo, sbo;
+  if (LAYOUT == 2) {
+    start = addr + 32 * ks;  // 8 K elements = 32 bytes along the line
+    lbo = 16;
+    sbo = 1024;
+  } else {
+    start = addr + 4096 * ks;
+    lbo = LAYOUT == 0 ? 1024 : 4096;
+    sbo = LAYOUT == 0 ? 4096 : 1024;
+  }
+  return (uint64_t)((start >> 4) & 0x3FFF) | ((uint64_t)(lbo >> 4) << 16) | ((uint64_t)(sbo >> 4) << 32) |
          (1ull << 46) | (2ull << 61);
 }
 
@@ -91,11 +117,12 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
   return false;
 }
 
-__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accum) {
+__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc_v,
+                                         uint32_t accum) {
   asm volatile(
       "{ .reg .pred p; setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p; }" ::"r"(tmem_d),
-      "l"(da), "l"(db), "r"(kIdesc), "r"(accum)
+      "l"(da), "l"(db), "r"(idesc_v), "r"(accum)
       : "memory");
 }
 __device__ __forceinline__ void mma_commit(uint32_t bar) {
@@ -116,6 +143,7 @@ __device__ __forceinline__ int find_task(const int64_t* __restrict__ prefix, int
 // Loads rows [r0, r0 + 128) x columns [kc, kc + 32) of the panel (ld = m, rows
 // >= m and columns >= kend read as 0), splits and stores both halves.
 // Producer thread p (0..127 within its group) handles rows p and columns 0..31.
+template <int LAYOUT>
 __device__ __forceinline__ void produce(const float* __restrict__ F, int m, int r0, int kc, int kend,
                                         unsigned char* big, unsigned char* small, int p) {
   const int row = r0 + p;
@@ -127,12 +155,13 @@ __device__ __forceinline__ void produce(const float* __restrict__ F, int m, int 
   for (int kk = 0; kk < TKS; ++kk) {
     const float b = tf32_rna(v[kk]);
     const float s = tf32_rna(v[kk] - b);
-    const uint32_t o = sw_off(p, kk);
+    const uint32_t o = sw_off<LAYOUT>(p, kk);
     *reinterpret_cast<float*>(big + o) = b;
     *reinterpret_cast<float*>(small + o) = s;
   }
 }
 
+template <int LAYOUT>
 __global__ void __launch_bounds__(NTHREADS, 1)
 k_syrk_tc(float* __restrict__ L, float* __restrict__ U, const int64_t* __restrict__ l_off,
           const int64_t* __restrict__ u_off, const int* __restrict__ fm, const int* __restrict__ fk,
@@ -195,8 +224,8 @@ k_syrk_tc(float* __restrict__ L, float* __restrict__ U, const int64_t* __restric
       if (*(volatile int*)s_fail) break;
       unsigned char* base = ops + buf * STAGE_BYTES;
       const int kc = J0 + st * TKS;
-      produce(F, m, r0, kc, J1, base, base + OPB, p);
-      if (!diag) produce(F, m, c0, kc, J1, base + 2 * OPB, base + 3 * OPB, p);
+      produce<LAYOUT>(F, m, r0, kc, J1, base, base + OPB, p);
+      if (!diag) produce<LAYOUT>(F, m, c0, kc, J1, base + 2 * OPB, base + 3 * OPB, p);
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_arrive(full0 + 8 * buf);
     }
@@ -216,12 +245,12 @@ k_syrk_tc(float* __restrict__ L, float* __restrict__ U, const int64_t* __restric
         const uint32_t base = smem_u32(ops + buf * STAGE_BYTES);
         const uint32_t ab = base, as = base + OPB;
         const uint32_t bb = diag ? ab : base + 2 * OPB, bs = diag ? as : base + 3 * OPB;
+        constexpr uint32_t id = idesc<LAYOUT>();
 #pragma unroll
         for (int ks = 0; ks < TKS / 8; ++ks) {
-          const uint32_t o = ks * 4096;
-          mma_tf32(tmem, sdesc(as + o), sdesc(bb + o), (st > 0 || ks > 0) ? 1u : 0u);
-          mma_tf32(tmem, sdesc(ab + o), sdesc(bs + o), 1u);
-          mma_tf32(tmem, sdesc(ab + o), sdesc(bb + o), 1u);
+          mma_tf32(tmem, sdesc<LAYOUT>(as, ks), sdesc<LAYOUT>(bb, ks), id, (st > 0 || ks > 0) ? 1u : 0u);
+          mma_tf32(tmem, sdesc<LAYOUT>(ab, ks), sdesc<LAYOUT>(bs, ks), id, 1u);
+          mma_tf32(tmem, sdesc<LAYOUT>(ab, ks), sdesc<LAYOUT>(bb, ks), id, 1u);
         }
         mma_commit(empty0 + 8 * buf);
       }
@@ -280,15 +309,16 @@ k_syrk_tc(float* __restrict__ L, float* __restrict__ U, const int64_t* __restric
 }  // namespace
 
 std::string tc_update_setup() {
-  const cudaError_t e =
-      cudaFuncSetAttribute(k_syrk_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES);
+  cudaError_t e = cudaFuncSetAttribute(k_syrk_tc<kTcLayout>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)SMEM_BYTES);
   return e == cudaSuccess ? std::string() : std::string("cudaFuncSetAttribute(k_syrk_tc): ") + cudaGetErrorString(e);
 }
 
 void launch_syrk_tc(float* L, float* U, const int64_t* l_off, const int64_t* u_off, const int* m, const int* k,
                     const int* fronts, const int64_t* prefix, int count, int64_t ctas, int j0, int* err,
                     cudaStream_t s) {
-  k_syrk_tc<<<(unsigned)ctas, NTHREADS, SMEM_BYTES, s>>>(L, U, l_off, u_off, m, k, fronts, prefix, count, j0, err);
+  k_syrk_tc<kTcLayout><<<(unsigned)ctas, NTHREADS, SMEM_BYTES, s>>>(L, U, l_off, u_off, m, k, fronts, prefix, count,
+                                                                    j0, err);
 }
 
 }  // namespace tdem

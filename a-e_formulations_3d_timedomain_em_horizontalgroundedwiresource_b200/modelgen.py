@@ -149,6 +149,7 @@ class ModelSpec:
     n_srs_razb: int = 500
     n_neib: int = 3
     nthreads: int = 1
+    sigma_air: float = SIGMA_AIR   # conductivity of material 1 (cells above z = 0)
 
     @property
     def n_nodes(self) -> int:
@@ -171,7 +172,7 @@ def cell_materials(spec: ModelSpec) -> Tuple[np.ndarray, List[float]]:
     yc = 0.5 * (spec.y[1:] + spec.y[:-1])
     zc = 0.5 * (spec.z[1:] + spec.z[:-1])
     Z, Y, X = np.meshgrid(zc, yc, xc, indexing="ij")
-    sig_table = [SIGMA_AIR]
+    sig_table = [spec.sigma_air]
     mat = np.ones(X.shape, dtype=np.int32)
     for li, (ztop, sig) in enumerate(spec.layers):
         zbot = spec.layers[li + 1][0] if li + 1 < len(spec.layers) else -np.inf

@@ -52,6 +52,16 @@ typedef enum tdem_status {
 tdem_status tdem_run_directory(const char* workdir, int formulation, int scheme, int device,
                                char* errbuf, size_t errlen);
 
+/* Drop-in for one run of the reference's CalcStat3D_3T_A in `workdir` (the
+ * grounded-wire stationary initial field, direct mode): reads inftry.dat, xyz.dat,
+ * nver.dat, nvkat.dat, l13d.dat, sig3d, group, sours and the optional nSrsRazb and
+ * ImpStatCur, solves the nodal potential V and the initial vector potential A0 with
+ * both factorizations and all solves on CUDA device `device` (FP64), and writes
+ * v3n.dat, v3a.dat and a0.dat in the reference's binary layout.
+ * Replaces: GeoCalculatorSP.cpp:1562 -> CalcStat3D_3T_A main -> CalcSP ->
+ * SolveStationarProblem3d(".", true, true) (MOD/CalcStat3D_3T_A/TaskSP.cpp:1625-2208). */
+tdem_status tdem_stationary_directory(const char* workdir, int device, char* errbuf, size_t errlen);
+
 typedef struct tdem_solver tdem_solver;
 
 typedef struct tdem_info {
@@ -89,6 +99,9 @@ typedef struct tdem_options {
   double refine_tol;        /* relative residual to reach per step and column (default 1e-10) */
   int refine_maxit;         /* iteration cap; exceeding it is TDEM_ERR_NUMERIC (default 200) */
   int leaf_size;            /* nested-dissection leaf size (default 128) */
+  int fp32_update;          /* precision 32, rank-256 trailing updates of the factorization:
+                               0 = library default, 1 = CUDA cores (FP32 FMA),
+                               2 = tensor cores (tcgen05, 3xTF32 with FP32 accumulation) */
 } tdem_options;
 
 /* Creates a solver for the model in `workdir` (reads the input files, analyses

@@ -102,6 +102,25 @@ def test_pardiso_gpu_multi_rhs_and_refactor(pkg):
     assert h[0] == 0
 
 
+def test_pardiso_gpu_dense_front(pkg):
+    """A dense SPD matrix is one front of 1,300 pivots: five outer panels of 256
+    columns, each ending in a rank-256 trailing update of the rest."""
+    n = 1300
+    rng = np.random.default_rng(5)
+    G = rng.standard_normal((n, n))
+    Ad = G @ G.T / n + np.eye(n)
+    import scipy.sparse as sp
+    a, ia, ja = _upper(sp.csr_matrix(Ad))
+    h = np.zeros(64, dtype=np.int64)
+    assert pkg.pardiso_64(h, 12, a, ia, ja) == 0
+    b = rng.standard_normal((2, n))
+    x = np.zeros_like(b)
+    assert pkg.pardiso_64(h, 33, a, ia, ja, nrhs=2, b=b, x=x) == 0
+    xr = np.linalg.solve(Ad, b.T).T
+    assert np.abs(x - xr).max() <= 1e-11 * np.abs(xr).max()
+    pkg.pardiso_64(h, -1, a, ia, ja)
+
+
 def test_pardiso_gpu_not_positive_definite(pkg):
     n = 400
     A = _spd(n, 9)
