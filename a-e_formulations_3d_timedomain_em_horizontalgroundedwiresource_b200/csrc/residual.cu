@@ -9,6 +9,8 @@
 // data give bit-identical norms.
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include "../../include/tdem.h"
 #include "residual.h"
 
@@ -119,4 +121,49 @@ extern "C" tdem_status tdem_residual_norms(int device, int64_t n, const int64_t*
   const cudaError_t e = tdem::launch_residual_norms(n, rowptr, col, val, x, b, ld, ncols, norms, scratch, s);
   const cudaError_t f = cudaFreeAsync(scratch, s);
   return (e == cudaSuccess && f == cudaSuccess) ? TDEM_OK : TDEM_ERR_CUDA;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant: the scratch is a file-scope device array of fixed
+// size (kResScratchBytes = 303,104 bytes: 296 CTAs x 64 columns x 2 sums), so a
+// call makes no device allocation.  Its device address is looked up once per
+// device (cudaGetSymbolAddress, with that device current) on the first call;
+// that first call may load the module and should happen before any stream
+// capture.  The scratch needs no initial value (pass 1 writes every entry pass 2
+// reads).  Calls whose executions overlap on one device share the scratch and
+// race: order them on one stream or synchronise between them.
+// ---------------------------------------------------------------------------
+namespace {
+
+__device__ __align__(256) double g_res_scratch[tdem::kResBlocks * tdem::kResMaxCols * 2];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mu;
+double* g_scratch_ptr[kMaxDevices] = {};
+
+// Device address of g_res_scratch on the current device `device` (nullptr on failure).
+double* scratch_address(int device) {
+  std::lock_guard<std::mutex> lk(g_scratch_mu);
+  if (!g_scratch_ptr[device]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_res_scratch) != cudaSuccess) return nullptr;
+    g_scratch_ptr[device] = static_cast<double*>(p);
+  }
+  return g_scratch_ptr[device];
+}
+
+}  // namespace
+
+extern "C" tdem_status tdem_residual_norms_noalloc(int device, int64_t n, const int64_t* rowptr, const int* col,
+                                                   const double* val, const double* x, const double* b, int64_t ld,
+                                                   int ncols, double* norms, void* stream) {
+  if (tdem::check_residual_args(n, rowptr, col, val, x, b, ld, ncols, norms)) return TDEM_ERR_ARGUMENT;
+  if (device < 0 || device >= kMaxDevices) return TDEM_ERR_ARGUMENT;
+  DeviceGuard g(device);
+  if (g.err != cudaSuccess) return TDEM_ERR_CUDA;
+  double* scratch = scratch_address(device);
+  if (!scratch) return TDEM_ERR_CUDA;
+  const cudaError_t e =
+      tdem::launch_residual_norms(n, rowptr, col, val, x, b, ld, ncols, norms, scratch, (cudaStream_t)stream);
+  return e == cudaSuccess ? TDEM_OK : TDEM_ERR_CUDA;
 }

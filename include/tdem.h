@@ -165,6 +165,21 @@ tdem_status tdem_residual_norms(int device, int64_t n, const int64_t* rowptr, co
                                 const double* val, const double* x, const double* b, int64_t ld,
                                 int ncols, double* norms, void* stream);
 
+/* tdem_residual_norms without any device allocation, for callers that may not
+ * allocate: code being captured into a CUDA graph (cudaMallocAsync inside a capture
+ * becomes part of the graph) and callers that run against a fixed memory budget.
+ * The scratch is a static device array of 303,104 bytes in the library (296 x 64 x 2
+ * doubles), so ncols is limited to 64 (larger is TDEM_ERR_ARGUMENT).  The first call
+ * on each device looks up the array's address (cudaGetSymbolAddress, which may load
+ * the module): make that first call before any stream capture.  The scratch needs no
+ * initial contents.  Calls whose executions overlap on one device share the scratch
+ * and race: issue them on one stream or synchronise between them.  Same arguments
+ * and results as tdem_residual_norms.
+ * No counterpart in the reference. */
+tdem_status tdem_residual_norms_noalloc(int device, int64_t n, const int64_t* rowptr, const int* col,
+                                        const double* val, const double* x, const double* b, int64_t ld,
+                                        int ncols, double* norms, void* stream);
+
 /* Library version string. */
 const char* tdem_version(void);
 
