@@ -91,6 +91,32 @@ class TdemOptions(ctypes.Structure):
     ]
 
 
+class TdemServerOptions(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("max_active", ctypes.c_int), ("prep_threads", ctypes.c_int),
+                ("hbm_budget_bytes", ctypes.c_int64)]
+
+
+class TdemRequestInfo(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("first_layer", ctypes.c_int), ("last_layer", ctypes.c_int),
+                ("n_rec_b", ctypes.c_int), ("n_rec_e", ctypes.c_int), ("n_sources", ctypes.c_int),
+                ("steps", ctypes.c_int), ("factorizations", ctypes.c_int), ("submit_s", ctypes.c_double),
+                ("admit_s", ctypes.c_double), ("done_s", ctypes.c_double), ("run_gpu_ms", ctypes.c_double),
+                ("device_bytes", ctypes.c_int64)]
+
+    def as_dict(self) -> dict:
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+class TdemServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("failed", ctypes.c_int64),
+                ("latency_p50_s", ctypes.c_double), ("latency_p99_s", ctypes.c_double),
+                ("makespan_s", ctypes.c_double), ("solves_per_s", ctypes.c_double),
+                ("peak_device_bytes", ctypes.c_int64), ("peak_active", ctypes.c_int)]
+
+    def as_dict(self) -> dict:
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
 _lib: Optional[ctypes.CDLL] = None
 
 EXPORTED = [
@@ -109,6 +135,13 @@ EXPORTED = [
     "pardiso_64",
     "mkl_set_num_threads",
     "tdem_residual_norms",
+    "tdem_server_create",
+    "tdem_server_submit",
+    "tdem_server_wait",
+    "tdem_server_results",
+    "tdem_server_error",
+    "tdem_server_stats_get",
+    "tdem_server_destroy",
     "tdem_version",
 ]
 
@@ -154,6 +187,21 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.tdem_residual_norms.argtypes = [ctypes.c_int, ctypes.c_int64, P, P, P, P, P, ctypes.c_int64,
                                         ctypes.c_int, P, P]
     lib.tdem_residual_norms.restype = ctypes.c_int
+    lib.tdem_server_create.argtypes = [ctypes.POINTER(TdemServerOptions), ctypes.POINTER(P)]
+    lib.tdem_server_create.restype = ctypes.c_int
+    lib.tdem_server_submit.argtypes = [P, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(TdemOptions),
+                                       ctypes.c_int, ctypes.POINTER(ctypes.c_int64)]
+    lib.tdem_server_submit.restype = ctypes.c_int
+    lib.tdem_server_wait.argtypes = [P, ctypes.c_int64, ctypes.POINTER(TdemRequestInfo)]
+    lib.tdem_server_wait.restype = ctypes.c_int
+    lib.tdem_server_results.argtypes = [P, ctypes.c_int64, P, P, P]
+    lib.tdem_server_results.restype = ctypes.c_int
+    lib.tdem_server_error.argtypes = [P, ctypes.c_int64]
+    lib.tdem_server_error.restype = ctypes.c_char_p
+    lib.tdem_server_stats_get.argtypes = [P, ctypes.POINTER(TdemServerStats)]
+    lib.tdem_server_stats_get.restype = ctypes.c_int
+    lib.tdem_server_destroy.argtypes = [P]
+    lib.tdem_server_destroy.restype = None
     _lib = lib
     return lib
 
@@ -288,3 +336,61 @@ def residual_norms(device: int, n: int, rowptr: int, col: int, val: int, x: int,
     st = load_library().tdem_residual_norms(device, n, rowptr, col, val, x, b, ld, ncols, norms, stream)
     if st != 0:
         raise TdemError(st, "tdem_residual_norms failed (status %d)" % st)
+
+
+class Server:
+    """Serving loop on one GPU (tdem_server_*): submit model directories, wait for
+    their transients; requests are admitted by the device memory their analysis
+    needs and run concurrently on their own streams."""
+
+    def __init__(self, device: int = 0, max_active: int = 4, prep_threads: int = 2, hbm_budget_bytes: int = 0):
+        self._lib = load_library()
+        self._h = ctypes.c_void_p()
+        o = TdemServerOptions(int(device), int(max_active), int(prep_threads), int(hbm_budget_bytes))
+        st = self._lib.tdem_server_create(ctypes.byref(o), ctypes.byref(self._h))
+        if st != 0:
+            raise TdemError(st, "tdem_server_create failed")
+
+    def submit(self, workdir: str, formulation="A", scheme: int = 2, precision: int = 64,
+               write_outputs: bool = False) -> int:
+        opts = TdemOptions(int(precision), 1e-10, 200, 128, 0)
+        rid = ctypes.c_int64(0)
+        st = self._lib.tdem_server_submit(self._h, os.fsencode(workdir), _form(formulation), int(scheme),
+                                          ctypes.byref(opts), int(bool(write_outputs)), ctypes.byref(rid))
+        if st != 0:
+            raise TdemError(st, "tdem_server_submit failed")
+        return int(rid.value)
+
+    def wait(self, request_id: int) -> dict:
+        """Blocks until the request is done; returns its info (raises on failure)."""
+        info = TdemRequestInfo()
+        st = self._lib.tdem_server_wait(self._h, int(request_id), ctypes.byref(info))
+        if st != 0:
+            raise TdemError(st, self._lib.tdem_server_error(self._h, int(request_id)).decode(errors="replace"))
+        return info.as_dict()
+
+    def results(self, request_id: int, info: dict):
+        nl = info["last_layer"] - info["first_layer"] + 1
+        e = np.zeros((nl, 3, info["n_rec_e"]))
+        m = np.zeros((nl, 3, info["n_rec_b"]))
+        b = np.zeros((nl, 3, info["n_rec_b"]))
+        st = self._lib.tdem_server_results(self._h, int(request_id), e.ctypes.data, m.ctypes.data, b.ctypes.data)
+        if st != 0:
+            raise TdemError(st, "tdem_server_results failed")
+        return e, m, b
+
+    def stats(self) -> dict:
+        s = TdemServerStats()
+        self._lib.tdem_server_stats_get(self._h, ctypes.byref(s))
+        return s.as_dict()
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.tdem_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

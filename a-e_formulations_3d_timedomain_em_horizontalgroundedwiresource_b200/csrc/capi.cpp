@@ -3,6 +3,9 @@
 
 #include <cuda_runtime.h>
 
+#include <map>
+#include <mutex>
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
 #include <memory>
@@ -11,6 +14,7 @@
 
 #include "driver.h"
 #include "gpu_cholesky.h"
+#include "server.h"
 #include "stationary.h"
 #include "symbolic.h"
 
@@ -184,6 +188,118 @@ tdem_status tdem_run_directory(const char* workdir, int formulation, int scheme,
   tdem_solver_destroy(s);
   return st;
 }
+
+struct tdem_server {
+  tdem::Server srv;
+  std::mutex mu;
+  std::map<int64_t, tdem::RequestResult> done;  // results fetched by tdem_server_wait
+};
+
+namespace {
+tdem::RunOptions run_options(int formulation, int scheme, const tdem_options* opts) {
+  tdem::RunOptions o;
+  o.formulation = formulation;
+  o.scheme = scheme;
+  if (opts) {
+    if (opts->precision) o.precision = opts->precision;
+    if (opts->refine_tol > 0) o.refine_tol = opts->refine_tol;
+    if (opts->refine_maxit > 0) o.refine_maxit = opts->refine_maxit;
+    if (opts->leaf_size > 0) o.leaf_size = opts->leaf_size;
+    o.fp32_update = opts->fp32_update;
+  }
+  return o;
+}
+}  // namespace
+
+tdem_status tdem_server_create(const tdem_server_options* opts, tdem_server** out) {
+  if (!out) return TDEM_ERR_ARGUMENT;
+  *out = nullptr;
+  tdem::ServerOptions o;
+  if (opts) {
+    o.device = opts->device;
+    if (opts->max_active > 0) o.max_active = opts->max_active;
+    if (opts->prep_threads > 0) o.prep_threads = opts->prep_threads;
+    o.hbm_budget = opts->hbm_budget_bytes;
+  }
+  auto s = std::make_unique<tdem_server>();
+  const std::string e = s->srv.start(o);
+  if (!e.empty()) return classify(e);
+  *out = s.release();
+  return TDEM_OK;
+}
+
+tdem_status tdem_server_submit(tdem_server* srv, const char* workdir, int formulation, int scheme,
+                               const tdem_options* opts, int write_outputs, int64_t* request_id) {
+  if (!srv || !workdir || !request_id) return TDEM_ERR_ARGUMENT;
+  if ((formulation != 0 && formulation != 1) || (scheme != 2 && scheme != 3)) return TDEM_ERR_ARGUMENT;
+  if (opts && (opts->precision != 0 && opts->precision != 32 && opts->precision != 64)) return TDEM_ERR_ARGUMENT;
+  if (opts && (opts->fp32_update < 0 || opts->fp32_update > 2)) return TDEM_ERR_ARGUMENT;
+  *request_id = srv->srv.submit(workdir, run_options(formulation, scheme, opts), write_outputs != 0);
+  return TDEM_OK;
+}
+
+tdem_status tdem_server_wait(tdem_server* srv, int64_t request_id, tdem_request_info* info) {
+  if (!srv) return TDEM_ERR_ARGUMENT;
+  tdem::RequestResult r;
+  if (!srv->srv.wait(request_id, &r)) return TDEM_ERR_ARGUMENT;
+  const tdem_status st = classify(r.error);
+  if (info) {
+    std::memset(info, 0, sizeof(*info));
+    info->status = st;
+    info->first_layer = r.first_layer;
+    info->last_layer = r.last_layer;
+    info->n_rec_b = r.n_rec_b;
+    info->n_rec_e = r.n_rec_e;
+    info->n_sources = r.n_sources;
+    info->steps = r.steps;
+    info->factorizations = r.factorizations;
+    info->submit_s = r.submit_s;
+    info->admit_s = r.admit_s;
+    info->done_s = r.done_s;
+    info->run_gpu_ms = r.run_gpu_ms;
+    info->device_bytes = r.device_bytes;
+  }
+  std::lock_guard<std::mutex> lk(srv->mu);
+  srv->done[request_id] = std::move(r);
+  return st;
+}
+
+tdem_status tdem_server_results(tdem_server* srv, int64_t request_id, double* eall, double* emf, double* ball) {
+  if (!srv) return TDEM_ERR_ARGUMENT;
+  std::lock_guard<std::mutex> lk(srv->mu);
+  auto it = srv->done.find(request_id);
+  if (it == srv->done.end()) return TDEM_ERR_STATE;
+  const tdem::RequestResult& r = it->second;
+  if (!r.error.empty()) return classify(r.error);
+  if (eall) std::copy(r.eall.begin(), r.eall.end(), eall);
+  if (emf) std::copy(r.emf.begin(), r.emf.end(), emf);
+  if (ball) std::copy(r.ball.begin(), r.ball.end(), ball);
+  return TDEM_OK;
+}
+
+const char* tdem_server_error(tdem_server* srv, int64_t request_id) {
+  if (!srv) return "";
+  std::lock_guard<std::mutex> lk(srv->mu);
+  auto it = srv->done.find(request_id);
+  return it == srv->done.end() ? "" : it->second.error.c_str();
+}
+
+tdem_status tdem_server_stats_get(tdem_server* srv, tdem_server_stats* st) {
+  if (!srv || !st) return TDEM_ERR_ARGUMENT;
+  const tdem::ServerStats s = srv->srv.stats();
+  st->submitted = s.submitted;
+  st->completed = s.completed;
+  st->failed = s.failed;
+  st->latency_p50_s = s.latency_p50_s;
+  st->latency_p99_s = s.latency_p99_s;
+  st->makespan_s = s.makespan_s;
+  st->solves_per_s = s.solves_per_s;
+  st->peak_device_bytes = s.peak_device_bytes;
+  st->peak_active = s.peak_active;
+  return TDEM_OK;
+}
+
+void tdem_server_destroy(tdem_server* srv) { delete srv; }
 
 tdem_status tdem_stationary_directory(const char* workdir, int device, char* errbuf, size_t errlen) {
   if (!workdir) return TDEM_ERR_ARGUMENT;

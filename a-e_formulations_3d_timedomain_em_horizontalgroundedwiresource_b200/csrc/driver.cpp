@@ -120,9 +120,14 @@ double TransientSolve::source_coef(int itime, bool two_layer, double dt) const {
 }
 
 std::string TransientSolve::prepare(const std::string& dir, const RunOptions& opt, cudaStream_t stream) {
+  std::string e = plan(dir, opt);
+  if (!e.empty()) return e;
+  return setup_device(stream);
+}
+
+std::string TransientSolve::plan(const std::string& dir, const RunOptions& opt) {
   const double t0 = now_s();
   opt_ = opt;
-  s_ = stream;
   if (opt.formulation != 0 && opt.formulation != 1) return "formulation must be 0 (A) or 1 (E)";
   if (opt.scheme != 2 && opt.scheme != 3) return "scheme must be 2 or 3";
   std::string e = load_model(dir, m_);
@@ -182,33 +187,18 @@ std::string TransientSolve::prepare(const std::string& dir, const RunOptions& op
     for (int a = 0; a < 3; ++a)
       xyz[3 * r + a] = 0.5 * (m_.xyz[m_.edge_nodes[i][0]][a] + m_.xyz[m_.edge_nodes[i][1]][a]);
   }
-  Symbolic sy;
-  e = analyse((int)n_int_, lptr.data(), lcol.data(), xyz.data(), sy, opt.leaf_size);
-  if (!e.empty()) return "analysis: " + e;
-  std::vector<int> p2v(n_int_);
-  for (int64_t p = 0; p < n_int_; ++p) p2v[p] = int_edge[sy.iperm[p]];
   if (opt.precision != 64 && opt.precision != 32) return "precision must be 64 or 32";
-  chol_.reset(new GpuCholesky());
-  if (opt.fp32_update != 0) chol_->set_tensor_core_update(opt.fp32_update == 2);
-  e = chol_->setup(std::move(sy), p2v, npls_, s_, opt.precision == 32 ? 4 : 8);
-  if (!e.empty()) return e;
-  if (const char* ps = std::getenv("TDEM_PANEL_SOLVE")) chol_->set_panel_solve(ps[0] == '1');
-
-  // device buffers
-  if (!(e = upload(&d_rowptr_, rowptr_)).empty()) return e;
-  if (!(e = upload(&d_col_, col_)).empty()) return e;
-  if (!(e = alloc((void**)&d_C_, sizeof(double) * col_.size())).empty()) return e;
-  if (!(e = alloc((void**)&d_B_, sizeof(double) * col_.size())).empty()) return e;
-  if (!(e = upload(&d_src_, src)).empty()) return e;
-  if (!(e = upload(&d_diag_, diag)).empty()) return e;
-  if (!(e = alloc((void**)&d_avals_, sizeof(double) * src.size())).empty()) return e;
-  {
-    std::vector<uint8_t> b(m_.edge_bound.begin(), m_.edge_bound.end());
-    if (!(e = upload(&d_bound_, b)).empty()) return e;
-  }
+  sy_.reset(new Symbolic());
+  e = analyse((int)n_int_, lptr.data(), lcol.data(), xyz.data(), *sy_, opt.leaf_size);
+  if (!e.empty()) return "analysis: " + e;
+  p2v_.resize(n_int_);
+  for (int64_t p = 0; p < n_int_; ++p) p2v_[p] = int_edge[sy_->iperm[p]];
+  src_ = std::move(src);
+  diag_ = std::move(diag);
   // source vectors S[e, p] = sum over dipoles of basis . dl * 2 / edge length
   {
-    std::vector<double> S((size_t)n_ * npls_, 0.0);
+    std::vector<double>& S = S_;
+    S.assign((size_t)n_ * npls_, 0.0);
     if (have_source_) {
       for (int p = 0; p < npls_; ++p)
         for (const Dipole& d : m_.dipoles[p]) {
@@ -224,8 +214,65 @@ std::string TransientSolve::prepare(const std::string& dir, const RunOptions& op
           }
         }
     }
-    if (!(e = upload(&d_S_, S)).empty()) return e;
   }
+  // receivers
+  {
+    auto owners = [&](const std::vector<int>& ig, int nrec) {
+      std::vector<int> o(nrec, 0);
+      for (int p = 0; p < npls_; ++p)
+        for (int i = ig[p]; i < ig[p + 1] && i < nrec; ++i) o[i] = p;
+      return o;
+    };
+    e = build_receiver_operator(m_, m_.rec_b, owners(m_.rec_b_ig, (int)m_.rec_b.size()), true, rop_b_);
+    if (!e.empty()) return e;
+    e = build_receiver_operator(m_, m_.rec_e, owners(m_.rec_e_ig, (int)m_.rec_e.size()), false, rop_e_);
+    if (!e.empty()) return e;
+  }
+  pt_.setup_s = now_s() - t0;
+  planned_ = true;
+  return "";
+}
+
+int64_t TransientSolve::device_bytes_needed() const {
+  if (!planned_ || !sy_) return 0;
+  const int64_t nn = n_, np = npls_, nnz = (int64_t)col_.size(), nl = (int64_t)src_.size();
+  int64_t b = GpuCholesky::bytes_needed(*sy_, npls_, opt_.precision == 32 ? 4 : 8);
+  b += 8 * (nn + 1) + 4 * nnz + 16 * nnz + 8 * nl + nl + 8 * nl + nn;  // pattern, C, B, map, diag, values, bound
+  b += 8 * nn * np * (ring_ + 4);                                       // S, history ring, rhs, x, u0
+  if (opt_.precision == 32) b += 8 * nnz + 8 * nn * np * 4;             // A and the CG vectors
+  b += 8 * (int64_t)(rop_b_.val.size() + rop_e_.val.size()) * 3;        // receiver operators (approx.)
+  b += 8 * (int64_t)(tll_ - tlf_ + 1) * 3 * (rop_b_.nrec + rop_e_.nrec) + 8 * ntime_;
+  b += (int64_t)m_.n_elem * (12 * 4 + 5 * 8 + 4);                       // assembly inputs
+  return b;
+}
+
+std::string TransientSolve::setup_device(cudaStream_t stream) {
+  if (!planned_) return "setup_device before plan";
+  const double t0 = now_s();
+  s_ = stream;
+  std::string e;
+  chol_.reset(new GpuCholesky());
+  if (opt_.fp32_update != 0) chol_->set_tensor_core_update(opt_.fp32_update == 2);
+  e = chol_->setup(std::move(*sy_), p2v_, npls_, s_, opt_.precision == 32 ? 4 : 8);
+  sy_.reset();
+  if (!e.empty()) return e;
+  if (const char* ps = std::getenv("TDEM_PANEL_SOLVE")) chol_->set_panel_solve(ps[0] == '1');
+  const RunOptions& opt = opt_;
+
+  // device buffers
+  if (!(e = upload(&d_rowptr_, rowptr_)).empty()) return e;
+  if (!(e = upload(&d_col_, col_)).empty()) return e;
+  if (!(e = alloc((void**)&d_C_, sizeof(double) * col_.size())).empty()) return e;
+  if (!(e = alloc((void**)&d_B_, sizeof(double) * col_.size())).empty()) return e;
+  if (!(e = upload(&d_src_, src_)).empty()) return e;
+  if (!(e = upload(&d_diag_, diag_)).empty()) return e;
+  if (!(e = alloc((void**)&d_avals_, sizeof(double) * src_.size())).empty()) return e;
+  {
+    std::vector<uint8_t> b(m_.edge_bound.begin(), m_.edge_bound.end());
+    if (!(e = upload(&d_bound_, b)).empty()) return e;
+  }
+  if (!(e = upload(&d_S_, S_)).empty()) return e;
+  std::vector<double>().swap(S_);
   if (!(e = alloc((void**)&d_hist_, sizeof(double) * (size_t)ring_ * n_ * npls_)).empty()) return e;
   if (!(e = alloc((void**)&d_rhs_, sizeof(double) * (size_t)n_ * npls_)).empty()) return e;
   if (!(e = alloc((void**)&d_x_, sizeof(double) * (size_t)n_ * npls_)).empty()) return e;
@@ -243,7 +290,6 @@ std::string TransientSolve::prepare(const std::string& dir, const RunOptions& op
   }
   if (!(e = upload(&d_u0_, u0_)).empty()) return e;
   for (cudaEvent_t& ev : ev_) TRY_CUDA(cudaEventCreate(&ev));
-  pt_.setup_s = now_s() - t0;
 
   // assembly of sigma*C and B/mu, one launch per element colour
   {
@@ -301,16 +347,6 @@ std::string TransientSolve::prepare(const std::string& dir, const RunOptions& op
 
   // receivers
   {
-    auto owners = [&](const std::vector<int>& ig, int nrec) {
-      std::vector<int> o(nrec, 0);
-      for (int p = 0; p < npls_; ++p)
-        for (int i = ig[p]; i < ig[p + 1] && i < nrec; ++i) o[i] = p;
-      return o;
-    };
-    e = build_receiver_operator(m_, m_.rec_b, owners(m_.rec_b_ig, (int)m_.rec_b.size()), true, rop_b_);
-    if (!e.empty()) return e;
-    e = build_receiver_operator(m_, m_.rec_e, owners(m_.rec_e_ig, (int)m_.rec_e.size()), false, rop_e_);
-    if (!e.empty()) return e;
     if (!(e = upload(&d_rb_ptr_, rop_b_.rowptr)).empty()) return e;
     if (!(e = upload(&d_rb_col_, rop_b_.col)).empty()) return e;
     if (!(e = upload(&d_rb_val_, rop_b_.val)).empty()) return e;
@@ -328,7 +364,7 @@ std::string TransientSolve::prepare(const std::string& dir, const RunOptions& op
     if (!(e = upload(&d_time_, m_.time)).empty()) return e;
   }
   TRY_CUDA(cudaStreamSynchronize(s_));
-  pt_.setup_s = now_s() - t0 - pt_.assemble_s;
+  pt_.setup_s += now_s() - t0 - pt_.assemble_s;
   return "";
 }
 

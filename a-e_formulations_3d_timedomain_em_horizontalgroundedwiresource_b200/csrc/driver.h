@@ -12,6 +12,7 @@
 #include "gpu_cholesky.h"
 #include "model.h"
 #include "receivers.h"
+#include "symbolic.h"
 
 namespace tdem {
 
@@ -44,8 +45,16 @@ class TransientSolve {
   TransientSolve();
   ~TransientSolve();
 
-  // Loads and prepares everything that does not depend on the time step.
+  // Loads and prepares everything that does not depend on the time step
+  // (plan() followed by setup_device()).
   std::string prepare(const std::string& dir, const RunOptions& opt, cudaStream_t stream);
+  // Host half: reads the inputs, builds the patterns, the analysis, the source
+  // vectors and the receiver operators.  Touches no device.
+  std::string plan(const std::string& dir, const RunOptions& opt);
+  // Device bytes setup_device() will allocate (valid after plan()).
+  int64_t device_bytes_needed() const;
+  // Device half: allocations, uploads and assembly on `stream`.
+  std::string setup_device(cudaStream_t stream);
   // Runs every time step of every decade.
   std::string run();
   // Host copies of the output tables (A-form: E = -dA/dt, emf = dB/dt, B; E-form:
@@ -68,6 +77,13 @@ class TransientSolve {
   RunOptions opt_;
   cudaStream_t s_ = nullptr;
   std::unique_ptr<GpuCholesky> chol_;
+  // host results of plan() consumed by setup_device()
+  bool planned_ = false;
+  std::unique_ptr<Symbolic> sy_;
+  std::vector<int> p2v_;
+  std::vector<int64_t> src_;
+  std::vector<uint8_t> diag_;
+  std::vector<double> S_;
   PhaseTimes pt_;
   int launches_ = 0;
   int n_ = 0, npls_ = 0, ntime_ = 0;

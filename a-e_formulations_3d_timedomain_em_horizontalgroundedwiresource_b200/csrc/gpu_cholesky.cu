@@ -228,17 +228,21 @@ __global__ void __launch_bounds__(256) k_syrk_panel(T* __restrict__ L, Fronts f,
 #pragma unroll
       for (int b = 0; b < 4; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
   }
+  T old[4][4];
 #pragma unroll
-  for (int a = 0; a < 4; ++a) {
-    const int r = r0 + tx + 16 * a;
-    if (r >= m) continue;
+  for (int a = 0; a < 4; ++a)
 #pragma unroll
     for (int b = 0; b < 4; ++b) {
-      const int c = c0 + ty + 16 * b;
-      if (c >= J1 || c > r) continue;
-      F[r + (int64_t)c * m] -= acc[a][b];
+      const int r = r0 + tx + 16 * a, c = c0 + ty + 16 * b;
+      old[a][b] = (r < m && c < J1 && c <= r) ? F[r + (int64_t)c * m] : (T)0;
     }
-  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int r = r0 + tx + 16 * a, c = c0 + ty + 16 * b;
+      if (r < m && c < J1 && c <= r) F[r + (int64_t)c * m] = old[a][b] - acc[a][b];
+    }
 }
 
 // Trailing update at the end of an outer panel: F[J1:m, J1:m] -= X X^T with X the
@@ -296,15 +300,22 @@ __global__ void __launch_bounds__(256) k_syrk_big(T* __restrict__ L, T* __restri
     }
     __syncthreads();
   }
+  // per output row: the 8 loads first, then the 8 stores (the element pointers may
+  // alias as far as the compiler knows, which would serialise load-store pairs)
 #pragma unroll
   for (int a = 0; a < 8; ++a) {
     const int r = r0 + tx + 16 * a;
     if (r >= m) continue;
+    T old[8];
 #pragma unroll
     for (int b = 0; b < 8; ++b) {
       const int c = c0 + ty + 16 * b;
-      if (c >= m || c > r) continue;
-      *felem(L, U, lo, uo, m, k, r, c) -= acc[a][b];
+      old[b] = (c < m && c <= r) ? *felem(L, U, lo, uo, m, k, r, c) : (T)0;
+    }
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      const int c = c0 + ty + 16 * b;
+      if (c < m && c <= r) *felem(L, U, lo, uo, m, k, r, c) = old[b] - acc[a][b];
     }
   }
 }
@@ -554,14 +565,61 @@ __device__ void wait_flag(const int* flag, int* err) {
   atomicExch(err, 1);
 }
 
+// Waits until *c reaches target (one thread; bounded like wait_flag).
+__device__ void wait_count(const int* c, int target, int* err) {
+  if (*(volatile int*)err != 0) return;
+  for (unsigned it = 0; it < kSpinLimit; ++it) {
+    if (ld_acquire(c) >= target) return;
+    __nanosleep(64);
+  }
+  atomicExch(err, 1);
+}
+
 struct FusedArgs {
-  const int* items;        // (front, block) pairs of this launch
+  const int* units;        // units of this launch (8 ints each, Symbolic::solve_units)
   int* ticket;             // launch-order counter (zeroed before the solve)
   int* flags;              // one per pivot block (zeroed before the solve)
+  int* counters;           // finished chunk units per row (zeroed before the solve)
   const int64_t* flag_off; // per front: first flag
   const int64_t* dinv_off; // per front: first inverted diagonal block
   int* err;                // err[1]: a wait gave up
 };
+
+// A chunk unit hands its partial sums (thread t: entries (t % 64, t / 64 + 4 j))
+// to the final unit of its row: store, then publish with a counter increment.
+template <class T, int RPT>
+__device__ __forceinline__ void publish_partial(T* part, const T (&acc)[RPT], int nr_rhs, int* counter) {
+  const int i = threadIdx.x & 63, g = threadIdx.x >> 6;
+#pragma unroll
+  for (int j = 0; j < RPT; ++j) {
+    const int r = g + 4 * j;
+    if (r < nr_rhs) part[i + SB * r] = acc[j];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(counter, 1);
+  }
+}
+
+// The final unit of a row: acc = (p_0 + p_1) + ... in a fixed order (left as is
+// when the row has no chunk units).
+template <class T, int RPT>
+__device__ __forceinline__ void gather_partials(const T* part, int nparts, int nr_rhs, const int* counter, int* err,
+                                                T (&acc)[RPT]) {
+  if (nparts == 0) return;
+  if (threadIdx.x == 0) wait_count(counter, nparts, err);
+  __syncthreads();
+  const int i = threadIdx.x & 63, g = threadIdx.x >> 6;
+#pragma unroll
+  for (int j = 0; j < RPT; ++j) {
+    const int r = g + 4 * j;
+    if (r >= nr_rhs) continue;
+    T tot = __ldcg(part + i + SB * r);
+    for (int c = 1; c < nparts; ++c) tot += __ldcg(part + (int64_t)c * SB * nr_rhs + i + SB * r);
+    acc[j] = tot;
+  }
+}
 
 // 64 x 64 block of a front (rows [r0, r0 + nr), columns [c0, c0 + nc), zero
 // outside) into 16 registers per thread: element (i, c) goes to thread
@@ -586,12 +644,14 @@ __device__ __forceinline__ void store_block(T (*Ls)[SB + 1], const T (&pre)[16])
   }
 }
 
-// Forward: CTA for block b of front s.  Pivot block (b < pb): rows [64b, ..) of the
-// pivot columns, y_b = Dinv_b (w_b - sum_{q<b} L_bq y_q).  Update block: rows
-// [k + 64 (b - pb), ..), w -= sum_{q<pb} L_bq y_q (gathered by the parent next).
+// Forward unit: row block R of front s (R < pb: pivot rows [64R, ..); else update
+// rows [k + 64 (R - pb), ..)), accumulating L_Rq y_q for the pivot blocks q in
+// [lo, hi).  Chunk units publish partial sums; the final unit (q = the last one
+// the row needs) adds them, then a pivot row solves y_R = Dinv_R (w_R - sum) and
+// raises its flag, an update row stores w_R - sum for the parent.
 // Thread t: row i = t % 64 of the block, right-hand sides r = t / 64 + 4 j.
 template <class T, int RPT>
-__global__ void __launch_bounds__(256) k_fwd_level(const T* __restrict__ L, const T* __restrict__ Dinv, T* W,
+__global__ void __launch_bounds__(256, 2) k_fwd_level(const T* __restrict__ L, const T* __restrict__ Dinv, T* W, T* part,
                                                    SolveArgs a, FusedArgs fa) {
   __shared__ T Ls[SB][SB + 1];
   __shared__ int s_item;
@@ -600,22 +660,49 @@ __global__ void __launch_bounds__(256) k_fwd_level(const T* __restrict__ L, cons
   const int t = threadIdx.x, i = t & 63, g = t >> 6;
   if (t == 0) s_item = atomicAdd(fa.ticket, 1);
   __syncthreads();
-  const int s = fa.items[2 * s_item], b = fa.items[2 * s_item + 1];
+  const int* u = fa.units + 8 * s_item;
+  const int s = u[0], R = u[1], lo = u[2], hi = u[3], slot = u[4], cnt = u[5], nparts = u[6], fin = u[7];
   const int m = a.m[s], k = a.k[s], nr_rhs = a.nrhs;
   const int pb = (k + SB - 1) / SB;
-  const bool piv = b < pb;
-  const int r0 = piv ? SB * b : k + SB * (b - pb);
+  const bool piv = R < pb;
+  const int r0 = piv ? SB * R : k + SB * (R - pb);
   const int nr = min(SB, (piv ? k : m) - r0);
-  const int qmax = piv ? b : pb;
   const T* F = L + a.l_off[s];
   T* w = W + a.w_off[s] * nr_rhs;
   const int* flags = fa.flags + fa.flag_off[s];
   T acc[RPT];
 #pragma unroll
   for (int j = 0; j < RPT; ++j) acc[j] = (T)0;
+  // final pivot unit: its inverted diagonal block and its own rows of W do not
+  // depend on this launch, so they are read before any wait
+  // (with many right-hand sides the registers go to the accumulators instead and
+  // the inverse is read after the last block)
+  constexpr bool kPreD = RPT <= 2;
+  const T* D = Dinv + fa.dinv_off[s] + (int64_t)R * SB * SB;
+  T dpre[kPreD ? 16 : 1], wrow[RPT];
+  if (fin && piv) {
+    if (kPreD) {
+#pragma unroll
+      for (int e = 0; e < 16; ++e) {
+        const int q = t + 256 * e, ii = q & 63, c = q >> 6;
+        dpre[e] = (ii < nr && c < nr) ? D[ii + c * nr] : (T)0;
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < RPT; ++j) {
+      const int r = g + 4 * j;
+      wrow[j] = (r < nr_rhs && i < nr) ? w[r0 + i + (int64_t)r * m] : (T)0;
+    }
+  }
+  T* my_part = part + (int64_t)slot * SB * nr_rhs;
+  T tot[RPT];
+#pragma unroll
+  for (int j = 0; j < RPT; ++j) tot[j] = (T)0;
+  // the chunk partials of this row are ready long before the last block's flag
+  if (fin) gather_partials<T, RPT>(my_part, nparts, nr_rhs, fa.counters + cnt, fa.err, tot);
   T pre[16];
-  if (qmax > 0) load_block(pre, F, m, r0, nr, 0, min(SB, k));
-  for (int q = 0; q < qmax; ++q) {
+  if (lo < hi) load_block(pre, F, m, r0, nr, SB * lo, min(SB, k - SB * lo));
+  for (int q = lo; q < hi; ++q) {
     const int wq = min(SB, k - SB * q);
     if (t == 0) wait_flag(flags + q, fa.err);
     __syncthreads();
@@ -625,7 +712,7 @@ __global__ void __launch_bounds__(256) k_fwd_level(const T* __restrict__ L, cons
       Ys[c * nr_rhs + r] = (c < wq) ? __ldcg(w + SB * q + c + (int64_t)r * m) : (T)0;
     }
     __syncthreads();
-    if (q + 1 < qmax) load_block(pre, F, m, r0, nr, SB * (q + 1), min(SB, k - SB * (q + 1)));
+    if (q + 1 < hi) load_block(pre, F, m, r0, nr, SB * (q + 1), min(SB, k - SB * (q + 1)));
 #pragma unroll 8
     for (int c = 0; c < SB; ++c) {
       const T l = Ls[c][i];
@@ -636,6 +723,12 @@ __global__ void __launch_bounds__(256) k_fwd_level(const T* __restrict__ L, cons
       }
     }
   }
+  if (!fin) {
+    publish_partial<T, RPT>(my_part, acc, nr_rhs, fa.counters + cnt);
+    return;
+  }
+#pragma unroll
+  for (int j = 0; j < RPT; ++j) acc[j] = tot[j] + acc[j];
   if (!piv) {
     if (i < nr) {
 #pragma unroll
@@ -650,12 +743,15 @@ __global__ void __launch_bounds__(256) k_fwd_level(const T* __restrict__ L, cons
 #pragma unroll
   for (int j = 0; j < RPT; ++j) {
     const int r = g + 4 * j;
-    if (r < nr_rhs) Ys[i * nr_rhs + r] = (i < nr) ? w[r0 + i + (int64_t)r * m] - acc[j] : (T)0;
+    if (r < nr_rhs) Ys[i * nr_rhs + r] = (i < nr) ? wrow[j] - acc[j] : (T)0;
   }
-  const T* D = Dinv + fa.dinv_off[s] + (int64_t)b * SB * SB;
-  for (int e = t; e < SB * SB; e += 256) {
-    const int ii = e & 63, c = e >> 6;
-    Ls[c][ii] = (ii < nr && c < nr) ? D[ii + c * nr] : (T)0;
+  if constexpr (kPreD) {
+    store_block(Ls, dpre);
+  } else {
+    for (int e = t; e < SB * SB; e += 256) {
+      const int ii = e & 63, c = e >> 6;
+      Ls[c][ii] = (ii < nr && c < nr) ? D[ii + c * nr] : (T)0;
+    }
   }
   __syncthreads();
   T y[RPT];
@@ -680,18 +776,18 @@ __global__ void __launch_bounds__(256) k_fwd_level(const T* __restrict__ L, cons
   __syncthreads();
   if (t == 0) {
     __threadfence();
-    st_release(fa.flags + fa.flag_off[s] + b, 1);
+    st_release(fa.flags + fa.flag_off[s] + R, 1);
   }
 }
 
-// Backward: CTA for pivot block p of front s (items in descending p):
-//   x_p = Dinv_p^T (y_p - sum_{rows below} L_rows,p^T x_rows)
-// over the update rows [k, m) (x of ancestors, staged in W by k_bwd_init) and the
-// pivot blocks q > p of the same front (waited for).  Thread t: column c = t % 64
-// of the block, right-hand sides r = t / 64 + 4 j.  Writes x_p to W and to the
-// caller's vector.
+// Backward unit: column block p of front s, accumulating L_Rp^T x_R over the row
+// blocks R in [lo, hi) (R < pb: pivot rows, waited for; else update rows, whose x
+// come from ancestors and were staged in W by k_bwd_init).  The final unit (row
+// block p + 1) adds the chunk partials and solves x_p = Dinv_p^T (y_p - sum),
+// written to W and to the caller's vector, then raises the column's flag.
+// Thread t: column c = t % 64 of the block, right-hand sides r = t / 64 + 4 j.
 template <class T, int RPT>
-__global__ void __launch_bounds__(256) k_bwd_level(const T* __restrict__ L, const T* __restrict__ Dinv, T* W,
+__global__ void __launch_bounds__(256, 2) k_bwd_level(const T* __restrict__ L, const T* __restrict__ Dinv, T* W, T* part,
                                                    double* __restrict__ x, SolveArgs a, FusedArgs fa) {
   __shared__ T Ls[SB][SB + 1];
   __shared__ int s_item;
@@ -700,39 +796,55 @@ __global__ void __launch_bounds__(256) k_bwd_level(const T* __restrict__ L, cons
   const int t = threadIdx.x, c = t & 63, g = t >> 6;
   if (t == 0) s_item = atomicAdd(fa.ticket, 1);
   __syncthreads();
-  const int s = fa.items[2 * s_item], p = fa.items[2 * s_item + 1];
+  const int* u = fa.units + 8 * s_item;
+  const int s = u[0], p = u[1], lo = u[2], hi = u[3], slot = u[4], cnt = u[5], nparts = u[6], fin = u[7];
   const int m = a.m[s], k = a.k[s], nr_rhs = a.nrhs;
   const int pb = (k + SB - 1) / SB;
   const int c0 = SB * p, wc = min(SB, k - c0);
-  const int nub = (m - k + SB - 1) / SB;
-  const int nblk = nub + (pb - 1 - p);
   const T* F = L + a.l_off[s];
   T* w = W + a.w_off[s] * nr_rhs;
   const int* flags = fa.flags + fa.flag_off[s];
   T acc[RPT];
 #pragma unroll
   for (int j = 0; j < RPT; ++j) acc[j] = (T)0;
-  auto block_rows = [&](int u, int& r0, int& nr, int& q) {
-    if (u < nub) {
-      r0 = k + SB * u;
-      nr = min(SB, m - r0);
-      q = -1;
-    } else {
-      q = pb - 1 - (u - nub);
-      r0 = SB * q;
-      nr = min(SB, k - r0);
+  constexpr bool kPreD = RPT <= 2;
+  const T* D = Dinv + fa.dinv_off[s] + (int64_t)p * SB * SB;
+  T dpre[kPreD ? 16 : 1], wrow[RPT];
+  if (fin) {
+    if (kPreD) {
+#pragma unroll
+      for (int e = 0; e < 16; ++e) {
+        const int q = t + 256 * e, ii = q & 63, cc = q >> 6;
+        dpre[e] = (ii < wc && cc < wc) ? D[ii + cc * wc] : (T)0;
+      }
     }
+#pragma unroll
+    for (int j = 0; j < RPT; ++j) {
+      const int r = g + 4 * j;
+      wrow[j] = (r < nr_rhs && c < wc) ? w[c0 + c + (int64_t)r * m] : (T)0;
+    }
+  }
+  T* my_part = part + (int64_t)slot * SB * nr_rhs;
+  T tot[RPT];
+#pragma unroll
+  for (int j = 0; j < RPT; ++j) tot[j] = (T)0;
+  if (fin) gather_partials<T, RPT>(my_part, nparts, nr_rhs, fa.counters + cnt, fa.err, tot);
+  auto rows_of = [&](int R, int& r0, int& nr) {
+    r0 = (R < pb) ? SB * R : k + SB * (R - pb);
+    nr = min(SB, (R < pb ? k : m) - r0);
   };
+  // rows farthest from the diagonal first: their x are known earliest (update rows
+  // from the ancestors, pivot blocks solved longest ago), the newest last
   T pre[16];
-  if (nblk > 0) {
-    int r0, nr, q;
-    block_rows(0, r0, nr, q);
+  if (lo < hi) {
+    int r0, nr;
+    rows_of(hi - 1, r0, nr);
     load_block(pre, F, m, r0, nr, c0, wc);
   }
-  for (int u = 0; u < nblk; ++u) {
-    int r0, nr, q;
-    block_rows(u, r0, nr, q);
-    if (q >= 0 && t == 0) wait_flag(flags + q, fa.err);
+  for (int R = hi - 1; R >= lo; --R) {
+    int r0, nr;
+    rows_of(R, r0, nr);
+    if (R < pb && t == 0) wait_flag(flags + R, fa.err);
     __syncthreads();
     store_block(Ls, pre);
     for (int e = t; e < SB * nr_rhs; e += 256) {
@@ -740,9 +852,9 @@ __global__ void __launch_bounds__(256) k_bwd_level(const T* __restrict__ L, cons
       Ws[ii * nr_rhs + r] = (ii < nr) ? __ldcg(w + r0 + ii + (int64_t)r * m) : (T)0;
     }
     __syncthreads();
-    if (u + 1 < nblk) {
-      int r1, n1, q1;
-      block_rows(u + 1, r1, n1, q1);
+    if (R - 1 >= lo) {
+      int r1, n1;
+      rows_of(R - 1, r1, n1);
       load_block(pre, F, m, r1, n1, c0, wc);
     }
 #pragma unroll 8
@@ -755,16 +867,23 @@ __global__ void __launch_bounds__(256) k_bwd_level(const T* __restrict__ L, cons
       }
     }
   }
+  if (!fin) {
+    publish_partial<T, RPT>(my_part, acc, nr_rhs, fa.counters + cnt);
+    return;
+  }
   __syncthreads();
 #pragma unroll
   for (int j = 0; j < RPT; ++j) {
     const int r = g + 4 * j;
-    if (r < nr_rhs) Ws[c * nr_rhs + r] = (c < wc) ? w[c0 + c + (int64_t)r * m] - acc[j] : (T)0;
+    if (r < nr_rhs) Ws[c * nr_rhs + r] = (c < wc) ? wrow[j] - (tot[j] + acc[j]) : (T)0;
   }
-  const T* D = Dinv + fa.dinv_off[s] + (int64_t)p * SB * SB;
-  for (int e = t; e < SB * SB; e += 256) {
-    const int ii = e & 63, cc = e >> 6;
-    Ls[cc][ii] = (ii < wc && cc < wc) ? D[ii + cc * wc] : (T)0;
+  if constexpr (kPreD) {
+    store_block(Ls, dpre);
+  } else {
+    for (int e = t; e < SB * SB; e += 256) {
+      const int ii = e & 63, cc = e >> 6;
+      Ls[cc][ii] = (ii < wc && cc < wc) ? D[ii + cc * wc] : (T)0;
+    }
   }
   __syncthreads();
   T xv[RPT];
@@ -968,14 +1087,15 @@ int launch_solve(const Symbolic& sy, const T* L, T* W, T* part, const double* b,
 }
 
 template <class T, int RPT>
-void launch_level_solves(const Symbolic& sy, const T* L, const T* Dinv, T* W, const double* b, double* x,
+void launch_level_solves(const Symbolic& sy, const T* L, const T* Dinv, T* W, T* part, const double* b, double* x,
                          SolveArgs a, const int* parent, const int64_t* rel_off, const int* rel, const int* tasks,
                          const int64_t* prefix, FusedArgs fa, int* sync, int& launches, cudaStream_t s) {
   const int nlev = (int)sy.levels.size();
   int* tickets = sync;
   int* fflags = sync + 2 * nlev;
   int* bflags = fflags + sy.n_flags;
-  cudaMemsetAsync(sync, 0, sizeof(int) * (2 * nlev + 2 * sy.n_flags), s);
+  fa.counters = bflags + sy.n_flags;
+  cudaMemsetAsync(sync, 0, sizeof(int) * (2 * nlev + 2 * sy.n_flags + sy.n_counters), s);
   const size_t ysm = sizeof(T) * SB * a.nrhs;
   for (int l = 0; l < nlev; ++l) {
     const LevelPlan& lp = sy.levels[l];
@@ -989,10 +1109,10 @@ void launch_level_solves(const Symbolic& sy, const T* L, const T* Dinv, T* W, co
       ++launches;
     }
     FusedArgs f = fa;
-    f.items = fa.items + 2 * lp.fwd_off;
+    f.units = fa.units + 8 * lp.fwd_off;
     f.ticket = tickets + 2 * l;
     f.flags = fflags;
-    k_fwd_level<T, RPT><<<grid_of(lp.fwd_count), 256, ysm, s>>>(L, Dinv, W, a, f);
+    k_fwd_level<T, RPT><<<grid_of(lp.fwd_count), 256, ysm, s>>>(L, Dinv, W, part, a, f);
     ++launches;
   }
   for (int l = nlev - 1; l >= 0; --l) {
@@ -1001,29 +1121,30 @@ void launch_level_solves(const Symbolic& sy, const T* L, const T* Dinv, T* W, co
                                                                    prefix + lp.assemble.pre, lp.assemble.count);
     ++launches;
     FusedArgs f = fa;
-    f.items = fa.items + 2 * lp.bwd_off;
+    f.units = fa.units + 8 * lp.bwd_off;
     f.ticket = tickets + 2 * l + 1;
     f.flags = bflags;
-    k_bwd_level<T, RPT><<<grid_of(lp.bwd_count), 256, ysm, s>>>(L, Dinv, W, x, a, f);
+    k_bwd_level<T, RPT><<<grid_of(lp.bwd_count), 256, ysm, s>>>(L, Dinv, W, part, x, a, f);
     ++launches;
   }
 }
 
 template <class T>
-int launch_solve_fused(const Symbolic& sy, const T* L, const T* Dinv, T* W, const double* b, double* x, SolveArgs a,
-                       const int* parent, const int64_t* rel_off, const int* rel, const int* tasks,
+int launch_solve_fused(const Symbolic& sy, const T* L, const T* Dinv, T* W, T* part, const double* b, double* x,
+                       SolveArgs a, const int* parent, const int64_t* rel_off, const int* rel, const int* tasks,
                        const int64_t* prefix, FusedArgs fa, int* sync, cudaStream_t s) {
   int launches = 0;
   if (a.nrhs <= 4)
-    launch_level_solves<T, 1>(sy, L, Dinv, W, b, x, a, parent, rel_off, rel, tasks, prefix, fa, sync, launches, s);
+    launch_level_solves<T, 1>(sy, L, Dinv, W, part, b, x, a, parent, rel_off, rel, tasks, prefix, fa, sync, launches, s);
   else if (a.nrhs <= 8)
-    launch_level_solves<T, 2>(sy, L, Dinv, W, b, x, a, parent, rel_off, rel, tasks, prefix, fa, sync, launches, s);
+    launch_level_solves<T, 2>(sy, L, Dinv, W, part, b, x, a, parent, rel_off, rel, tasks, prefix, fa, sync, launches, s);
   else if (a.nrhs <= 16)
-    launch_level_solves<T, 4>(sy, L, Dinv, W, b, x, a, parent, rel_off, rel, tasks, prefix, fa, sync, launches, s);
+    launch_level_solves<T, 4>(sy, L, Dinv, W, part, b, x, a, parent, rel_off, rel, tasks, prefix, fa, sync, launches, s);
   else if (a.nrhs <= 32)
-    launch_level_solves<T, 8>(sy, L, Dinv, W, b, x, a, parent, rel_off, rel, tasks, prefix, fa, sync, launches, s);
+    launch_level_solves<T, 8>(sy, L, Dinv, W, part, b, x, a, parent, rel_off, rel, tasks, prefix, fa, sync, launches, s);
   else
-    launch_level_solves<T, 16>(sy, L, Dinv, W, b, x, a, parent, rel_off, rel, tasks, prefix, fa, sync, launches, s);
+    launch_level_solves<T, 16>(sy, L, Dinv, W, part, b, x, a, parent, rel_off, rel, tasks, prefix, fa, sync, launches,
+                               s);
   return launches;
 }
 
@@ -1071,6 +1192,19 @@ std::string GpuCholesky::upload(T** dst, const std::vector<T>& src, cudaStream_t
   return "";
 }
 
+int64_t GpuCholesky::bytes_needed(const Symbolic& sy, int nrhs_max, int precision_bytes) {
+  const int64_t el = (precision_bytes == 4) ? 4 : 8, nr = std::max(1, nrhs_max);
+  int64_t b = el * (sy.nnz_l + sy.u_elems + sy.wvec_elems * nr + sy.solve_partials * nr + sy.dinv_elems +
+                    sy.solve_slots * kPanel * nr);
+  b += 8 * (int64_t)(sy.l_off.size() + sy.u_off.size() + sy.wvec_off.size() + sy.entry_dst.size() +
+                     sy.rel_off.size() + sy.rows_off.size() + sy.task_prefix.size() + sy.flag_off.size() +
+                     sy.dinv_off.size());
+  b += 4 * (int64_t)(sy.front_m.size() + sy.front_k.size() + sy.rel.size() + sy.rows_all.size() + sy.tasks.size() +
+                     sy.front_parent.size() + sy.front_c0.size() + sy.solve_items.size() + sy.solve_units.size() +
+                     2 * sy.levels.size() + 2 * sy.n_flags + sy.n_counters + 4);
+  return b;
+}
+
 std::string GpuCholesky::setup(Symbolic&& sy, const std::vector<int>& perm_to_vec, int nrhs_max,
                                cudaStream_t s, int precision_bytes) {
   sy_ = std::move(sy);
@@ -1105,7 +1239,10 @@ std::string GpuCholesky::setup(Symbolic&& sy, const std::vector<int>& perm_to_ve
   if (!(e = upload(&d_flag_off_, sy_.flag_off, s)).empty()) return e;
   if (!(e = upload(&d_dinv_off_, sy_.dinv_off, s)).empty()) return e;
   if (!(e = alloc(&d_dinv_, elem_ * std::max<int64_t>(1, sy_.dinv_elems))).empty()) return e;
-  if (!(e = alloc((void**)&d_sync_, sizeof(int) * (2 * sy_.levels.size() + 2 * sy_.n_flags + 1))).empty())
+  if (!(e = upload(&d_units_, sy_.solve_units, s)).empty()) return e;
+  if (!(e = alloc(&d_spart_, elem_ * std::max<int64_t>(1, sy_.solve_slots) * kPanel * nrhs_max_)).empty()) return e;
+  if (!(e = alloc((void**)&d_sync_,
+                  sizeof(int) * (2 * sy_.levels.size() + 2 * sy_.n_flags + sy_.n_counters + 1))).empty())
     return e;
   if (!(e = alloc((void**)&d_err_, 3 * sizeof(int))).empty()) return e;
   TDEM_CUDA_TRY(cudaMemsetAsync(d_err_, 0, 3 * sizeof(int), s));
@@ -1137,15 +1274,15 @@ void GpuCholesky::factor(const double* d_vals, cudaStream_t s) {
 void GpuCholesky::solve(const double* d_b, double* d_x, int64_t ld, int nrhs, cudaStream_t s) {
   SolveArgs a{d_l_off_, d_w_off_, d_m_, d_k_, d_rows_off_, d_rows_, nrhs, ld};
   if (!panel_solve_) {
-    FusedArgs fa{d_items_, nullptr, nullptr, d_flag_off_, d_dinv_off_, d_err_};
+    FusedArgs fa{d_units_, nullptr, nullptr, nullptr, d_flag_off_, d_dinv_off_, d_err_};
     if (elem_ == 4)
-      launches_solve_ = launch_solve_fused<float>(sy_, (const float*)d_L_, (const float*)d_dinv_, (float*)d_W_, d_b,
-                                                  d_x, a, d_parent_, d_rel_off_, d_rel_, d_tasks_, d_prefix_, fa,
-                                                  d_sync_, s);
+      launches_solve_ = launch_solve_fused<float>(sy_, (const float*)d_L_, (const float*)d_dinv_, (float*)d_W_,
+                                                  (float*)d_spart_, d_b, d_x, a, d_parent_, d_rel_off_, d_rel_,
+                                                  d_tasks_, d_prefix_, fa, d_sync_, s);
     else
       launches_solve_ = launch_solve_fused<double>(sy_, (const double*)d_L_, (const double*)d_dinv_, (double*)d_W_,
-                                                   d_b, d_x, a, d_parent_, d_rel_off_, d_rel_, d_tasks_, d_prefix_,
-                                                   fa, d_sync_, s);
+                                                   (double*)d_spart_, d_b, d_x, a, d_parent_, d_rel_off_, d_rel_,
+                                                   d_tasks_, d_prefix_, fa, d_sync_, s);
     return;
   }
   if (elem_ == 4)

@@ -32,6 +32,9 @@ class GpuCholesky {
   std::string setup(Symbolic&& sy, const std::vector<int>& perm_to_vec, int nrhs_max,
                     cudaStream_t stream, int precision_bytes = 8);
 
+  // Device bytes setup() allocates for this analysis (factor, workspaces, plans).
+  static int64_t bytes_needed(const Symbolic& sy, int nrhs_max, int precision_bytes);
+
   // Numeric factorization.  d_lower_vals holds the lower-CSR values of the
   // analysed pattern (device, nnz_lower doubles).  Errors (non-positive pivot)
   // are reported through status() after the stream is synchronised.
@@ -101,7 +104,9 @@ class GpuCholesky {
   int64_t* d_flag_off_ = nullptr;
   int64_t* d_dinv_off_ = nullptr;
   void* d_dinv_ = nullptr;       // inverted diagonal blocks
-  int* d_sync_ = nullptr;        // level tickets + pivot-block flags of one solve
+  int* d_sync_ = nullptr;        // level tickets + pivot-block flags + row counters of one solve
+  int* d_units_ = nullptr;       // level-solve units
+  void* d_spart_ = nullptr;      // level-solve partial sums (slots x 64 x nrhs)
   std::vector<void*> allocs_;
   template <class T>
   std::string upload(T** dst, const std::vector<T>& src, cudaStream_t s);

@@ -471,32 +471,67 @@ std::string analyse(int n, const int64_t* rowptr, const int* colind, const doubl
       sy.solve_items.push_back(s);
       sy.solve_items.push_back(b);
     };
+    // A unit of a level solve: front, row block (forward) or column block
+    // (backward), the block range [lo, hi) it accumulates, its partial-sum slot,
+    // the counter of its row and, for the final unit of a row, the number of
+    // partials to add.  Ranges are split into chunks of kSolveChunk blocks; the
+    // final unit takes the most recent dependency (the single block next to the
+    // diagonal) so the dependency chain advances by one block per link.
+    auto unit = [&](std::vector<int>& out, int s, int row, int lo, int hi, int slot, int cnt, int nparts,
+                    int fin) {
+      const int u[8] = {s, row, lo, hi, slot, cnt, nparts, fin};
+      out.insert(out.end(), u, u + 8);
+    };
+    int64_t max_slots = 0;
     for (int l = 0; l < nlev; ++l) {
       LevelPlan& lp = sy.levels[l];
-      // forward: block b of front s, b < pb pivot blocks, then update blocks
-      int bmax = 0;
-      for (int s : lp.fronts) {
-        const int m = sy.front_m[s], k = sy.front_k[s];
-        bmax = std::max(bmax, (int)(cdiv(k, kPanel) + cdiv(m - k, kPanel)));
-      }
-      lp.fwd_off = (int64_t)sy.solve_items.size() / 2;
-      for (int b = 0; b < bmax; ++b)
+      // forward: row block R < pb (pivot rows, needs q < R) or R >= pb (update rows,
+      // needs q < pb)
+      int rmax = 0;
+      for (int s : lp.fronts)
+        rmax = std::max(rmax, (int)(cdiv(sy.front_k[s], kPanel) + cdiv(sy.front_m[s] - sy.front_k[s], kPanel)));
+      lp.fwd_off = (int64_t)sy.solve_units.size() / 8;
+      int64_t slots = 0;
+      for (int R = 0; R < rmax; ++R)
         for (int s : lp.fronts) {
-          const int m = sy.front_m[s], k = sy.front_k[s];
-          if (b < cdiv(k, kPanel) + cdiv(m - k, kPanel)) push(s, b);
+          const int pb = (int)cdiv(sy.front_k[s], kPanel), ub = (int)cdiv(sy.front_m[s] - sy.front_k[s], kPanel);
+          if (R >= pb + ub) continue;
+          const int qmax = R < pb ? R : pb;
+          const int cnt = (int)sy.n_counters++;
+          // short rows stay in one unit; long ones leave only the newest block to the final unit
+          const int nch = qmax - 1 > kSolveChunk ? (int)cdiv(qmax - 1, kSolveChunk) : 0;
+          for (int c = 0; c < nch; ++c)
+            unit(sy.solve_units, s, R, c * kSolveChunk, std::min(qmax - 1, (c + 1) * kSolveChunk), (int)(slots + c),
+                 cnt, 0, 0);
+          unit(sy.solve_units, s, R, nch > 0 ? qmax - 1 : 0, qmax, (int)slots, cnt, nch, 1);
+          slots += nch;
         }
-      lp.fwd_count = (int64_t)sy.solve_items.size() / 2 - lp.fwd_off;
-      // backward: pivot blocks, last first
+      lp.fwd_count = (int64_t)sy.solve_units.size() / 8 - lp.fwd_off;
+      max_slots = std::max(max_slots, slots);
+      // backward: column block p (last first) needs the row blocks R in (p, pb + ub)
       int pmax = 0;
       for (int s : lp.fronts) pmax = std::max(pmax, (int)cdiv(sy.front_k[s], kPanel));
-      lp.bwd_off = (int64_t)sy.solve_items.size() / 2;
+      lp.bwd_off = (int64_t)sy.solve_units.size() / 8;
+      slots = 0;
       for (int d = 0; d < pmax; ++d)
         for (int s : lp.fronts) {
-          const int pb = (int)cdiv(sy.front_k[s], kPanel);
-          if (d < pb) push(s, pb - 1 - d);
+          const int pb = (int)cdiv(sy.front_k[s], kPanel), ub = (int)cdiv(sy.front_m[s] - sy.front_k[s], kPanel);
+          if (d >= pb) continue;
+          const int p = pb - 1 - d, rend = pb + ub;
+          const int cnt = (int)sy.n_counters++;
+          const bool split = rend - (p + 2) > kSolveChunk;
+          const int first = split ? p + 2 : rend;
+          const int nch = split ? (int)cdiv(rend - first, kSolveChunk) : 0;
+          for (int c = 0; c < nch; ++c)
+            unit(sy.solve_units, s, p, first + c * kSolveChunk, std::min(rend, first + (c + 1) * kSolveChunk),
+                 (int)(slots + c), cnt, 0, 0);
+          unit(sy.solve_units, s, p, std::min(p + 1, rend), first, (int)slots, cnt, nch, 1);
+          slots += nch;
         }
-      lp.bwd_count = (int64_t)sy.solve_items.size() / 2 - lp.bwd_off;
+      lp.bwd_count = (int64_t)sy.solve_units.size() / 8 - lp.bwd_off;
+      max_slots = std::max(max_slots, slots);
     }
+    sy.solve_slots = max_slots;
     sy.inv_off = (int64_t)sy.solve_items.size() / 2;
     for (int s = 0; s < nf; ++s)
       for (int b = 0; b < cdiv(sy.front_k[s], kPanel); ++b) push(s, b);

@@ -27,6 +27,7 @@ constexpr int kTileSyrk = 64;    // tile edge of the update inside an outer pane
 constexpr int kTileBig = 128;    // tile edge of the rank-kOuter trailing update
 constexpr int kTrsmRows = 128;   // rows per CTA of the panel triangular solve
 constexpr int kSolveRows = 256;  // rows per CTA of the solve updates
+constexpr int kSolveChunk = 8;   // 64 x 64 blocks accumulated by one level-solve unit
 
 struct FrontInfo {
   int c0 = 0, c1 = 0;      // pivot columns [c0, c1) (permuted numbering)
@@ -63,11 +64,11 @@ struct LevelPlan {
   std::vector<TaskList> extend_vec;    // solve extend-add per child slot, kSolveRows rows per CTA
   TaskList assemble;                   // solve: front-vector init, ceil(m / kSolveRows) CTAs each
   std::vector<PanelStep> panels;
-  // Fused triangular solves: one CTA per 64-row block of every front at this
-  // level, items (front, block) at solve_items[2 * off ...].  Forward blocks are
-  // the pivot blocks b < ceil(k / 64) then the update blocks; sorted by block
-  // index so every block a CTA waits for has a smaller ticket.  Backward items are
-  // the pivot blocks in descending order.
+  // Level triangular solves: units (8 ints each, see Symbolic::solve_units) at
+  // solve_units[8 * off ...], one CTA per unit.  Forward units are ordered by row
+  // block then front, backward units by distance of the column block from the
+  // last one then front; within a row the chunk units come before its final unit,
+  // so every unit a CTA waits for has a smaller ticket.
   int64_t fwd_off = 0, fwd_count = 0;
   int64_t bwd_off = 0, bwd_count = 0;
 };
@@ -96,7 +97,12 @@ struct Symbolic {
   std::vector<int> tasks;            // concatenated task front lists
   std::vector<int64_t> task_prefix;  // concatenated CTA prefix sums
 
-  std::vector<int> solve_items;      // (front, block) pairs of the fused solves and inversions
+  std::vector<int> solve_items;      // (front, block) pairs of the diagonal-block inversions
+  // level-solve units: {front, row/column block, lo, hi, partial slot, row counter,
+  // partials to add (final unit), final flag}
+  std::vector<int> solve_units;
+  int64_t n_counters = 0;            // row counters over all levels and both directions
+  int64_t solve_slots = 0;           // partial-sum slots (64 x nrhs each) of the largest level
   std::vector<int64_t> flag_off;     // per front: index of its first pivot-block flag
   std::vector<int64_t> dinv_off;     // per front: offset of its inverted diagonal blocks
   int64_t n_flags = 0;               // pivot blocks over all fronts

@@ -9,14 +9,15 @@
 // accumulated in FP32 in tensor memory as Xb Xb^T + Xb Xs^T + Xs Xb^T (the
 // dropped Xs Xs^T term is below FP32 rounding).
 //
-// CTA = 9 warps.  Warps 0-7 are producers: they read the panel from global
-// memory (coalesced along rows, any alignment), split it and store both halves
-// into shared memory in the K-major 128-byte-swizzled layout that the UMMA
-// descriptors describe; warps 0-3 handle even K stages, 4-7 odd ones.
-// Warp 8 issues tcgen05.mma (M = N = 128, K = 8 per instruction) from one lane
-// and commits each stage to an mbarrier that frees the stage's buffers.  After
-// the last stage the producer warps read the accumulator from tensor memory
-// (tcgen05.ld, warp w owns lanes 32 (w % 4) .. + 31) and subtract it from F.
+// CTA = 13 warps.  Warps 0-11 are producers in three groups of four; group g fills
+// K stages g, g + 3, ... into its own stage buffer: it reads the 128 rows of both
+// operands from global memory (coalesced along rows, any alignment; all loads of
+// a stage issued before the first use), splits them and stores both halves with
+// 16-byte stores in the K-major 128-byte-swizzled layout that the UMMA
+// descriptors describe.  Warp 12 issues tcgen05.mma (M = N = 128, K = 8 per
+// instruction) from one lane and commits each stage to an mbarrier that frees the
+// stage's buffer.  After the last stage warps 0-7 read the accumulator from tensor
+// memory (tcgen05.ld, warp w owns lanes 32 (w % 4) .. + 31) and subtract it from F.
 //
 // Every wait is bounded; a wait that gives up records err[2] and the CTA skips
 // the rest of its work, still waiting (bounded) for its own MMAs and freeing its
@@ -37,19 +38,16 @@ constexpr int TKS = 32;                  // K per pipeline stage
 constexpr int NSTAGE = 3;                // operand buffers in flight
 constexpr int OPB = TM * TKS * 4;        // bytes of one operand half (16 KB)
 constexpr int STAGE_BYTES = 4 * OPB;     // A big, A small, B big, B small
-constexpr int NPROD = 256;               // producer threads (8 warps)
+constexpr int NGROUP = 3;                // producer groups (one stage buffer each)
+constexpr int NPROD = 128 * NGROUP;      // producer threads (4 warps per group)
 constexpr int NTHREADS = NPROD + 32;     // + the MMA warp
 constexpr size_t SMEM_BYTES = (size_t)NSTAGE * STAGE_BYTES + 1024 /* alignment */ + 256 /* barriers */;
 constexpr unsigned kWaitLimit = 1u << 22;
-constexpr int kTcLayout = 2;             // operand layout used by the factorization (K-major)
+static_assert(NGROUP == NSTAGE, "producer group g owns stage buffer g");
 
-// instruction descriptor: D F32, A/B TF32, M = N = 128; A and B MN-major (bits
-// 15, 16) for layouts 0 and 1, K-major for layout 2
-template <int LAYOUT>
-__host__ __device__ constexpr uint32_t idesc() {
-  return (1u << 4) | (2u << 7) | (2u << 10) | (LAYOUT == 2 ? 0u : (1u << 15) | (1u << 16)) |
-         ((uint32_t)(TM >> 3) << 17) | ((uint32_t)(TM >> 4) << 24);
-}
+// instruction descriptor: D F32, A/B TF32, both K-major, M = N = 128
+constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TM >> 3) << 17) |
+                            ((uint32_t)(TM >> 4) << 24);
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -61,40 +59,21 @@ __device__ __forceinline__ float tf32_rna(float x) {
   return __uint_as_float(r);
 }
 
-// Operand layouts in shared memory (128-byte swizzle: the 16-byte chunk index
-// inside a 128-byte line is XOR-ed with the line index modulo 8).
-//   LAYOUT 0 / 1: MN-major.  8 atoms of 32 (MN) x 8 (K) elements, atom (a, g) at
-//     (4 g + a) * 1024; line kk % 8 of an atom holds 32 consecutive MN elements.
-//     Layout 0 gives the MN-atom stride (1024 B) as the leading byte offset and
-//     the K-group stride (4096 B) as the stride byte offset; layout 1 the reverse.
-//   LAYOUT 2: K-major.  16 groups of 8 MN rows, group at (mn / 8) * 1024; row
-//     mn % 8 is one line of 32 consecutive K elements.
-template <int LAYOUT>
-__device__ __forceinline__ uint32_t sw_off(int mn, int kk) {
-  if (LAYOUT == 2) {
-    const int row = mn & 7;
-    return (uint32_t)((mn >> 3) * 1024 + row * 128 + ((((kk >> 2) ^ row) & 7) << 4) + ((kk & 3) << 2));
-  }
-  const int line = kk & 7;
-  return (uint32_t)(((kk >> 3) * 4 + (mn >> 5)) * 1024 + line * 128 + ((((mn & 31) >> 2) ^ line) << 4) +
-                    ((mn & 3) << 2));
+// K-major operand half (128 rows x 32 K elements): 16 groups of 8 rows, group at
+// (mn / 8) * 1024; row mn % 8 is one 128-byte line of 32 consecutive K elements,
+// its 16-byte chunks (4 elements) XOR-swizzled with the row index.  Byte offset of
+// chunk c (elements 4c .. 4c + 3) of row mn:
+__device__ __forceinline__ uint32_t chunk_off(int mn, int c) {
+  const int row = mn & 7;
+  return (uint32_t)((mn >> 3) * 1024 + row * 128 + ((c ^ row) << 4));
 }
 
-// UMMA shared-memory descriptor of the K = 8 slice ks of an operand half at addr
-// (version 1, 128-byte swizzle).
-template <int LAYOUT>
+// UMMA shared-memory descriptor of the K = 8 slice ks (32 bytes along each line)
+// of an operand half at addr: stride byte offset 1024 (8-row groups), version 1,
+// 128-byte swizzle.
 __device__ __forceinline__ uint64_t sdesc(uint32_t addr, int ks) {
-  uint32_t start, lbo, sbo;
-  if (LAYOUT == 2) {
-    start = addr + 32 * ks;  // 8 K elements = 32 bytes along the line
-    lbo = 16;
-    sbo = 1024;
-  } else {
-    start = addr + 4096 * ks;
-    lbo = LAYOUT == 0 ? 1024 : 4096;
-    sbo = LAYOUT == 0 ? 4096 : 1024;
-  }
-  return (uint64_t)((start >> 4) & 0x3FFF) | ((uint64_t)(lbo >> 4) << 16) | ((uint64_t)(sbo >> 4) << 32) |
+  const uint32_t start = addr + 32 * ks;
+  return (uint64_t)((start >> 4) & 0x3FFF) | ((uint64_t)(16 >> 4) << 16) | ((uint64_t)(1024 >> 4) << 32) |
          (1ull << 46) | (2ull << 61);
 }
 
@@ -117,12 +96,11 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
   return false;
 }
 
-__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc_v,
-                                         uint32_t accum) {
+__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accum) {
   asm volatile(
       "{ .reg .pred p; setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p; }" ::"r"(tmem_d),
-      "l"(da), "l"(db), "r"(idesc_v), "r"(accum)
+      "l"(da), "l"(db), "r"(kIdesc), "r"(accum)
       : "memory");
 }
 __device__ __forceinline__ void mma_commit(uint32_t bar) {
@@ -140,28 +118,35 @@ __device__ __forceinline__ int find_task(const int64_t* __restrict__ prefix, int
   return lo;
 }
 
-// Loads rows [r0, r0 + 128) x columns [kc, kc + 32) of the panel (ld = m, rows
-// >= m and columns >= kend read as 0), splits and stores both halves.
-// Producer thread p (0..127 within its group) handles rows p and columns 0..31.
-template <int LAYOUT>
-__device__ __forceinline__ void produce(const float* __restrict__ F, int m, int r0, int kc, int kend,
-                                        unsigned char* big, unsigned char* small, int p) {
-  const int row = r0 + p;
-  const bool okr = row < m;
-  float v[TKS];
+// Splits 32 values into their TF32 halves and stores them as eight 16-byte chunks
+// of row p of both operand halves.
+__device__ __forceinline__ void split_store(const float (&v)[TKS], unsigned char* big, unsigned char* small, int p) {
 #pragma unroll
-  for (int kk = 0; kk < TKS; ++kk) v[kk] = (okr && kc + kk < kend) ? F[row + (int64_t)(kc + kk) * m] : 0.f;
-#pragma unroll
-  for (int kk = 0; kk < TKS; ++kk) {
-    const float b = tf32_rna(v[kk]);
-    const float s = tf32_rna(v[kk] - b);
-    const uint32_t o = sw_off<LAYOUT>(p, kk);
-    *reinterpret_cast<float*>(big + o) = b;
-    *reinterpret_cast<float*>(small + o) = s;
+  for (int c = 0; c < TKS / 4; ++c) {
+    float4 b, sm;
+    b.x = tf32_rna(v[4 * c + 0]);
+    b.y = tf32_rna(v[4 * c + 1]);
+    b.z = tf32_rna(v[4 * c + 2]);
+    b.w = tf32_rna(v[4 * c + 3]);
+    sm.x = tf32_rna(v[4 * c + 0] - b.x);
+    sm.y = tf32_rna(v[4 * c + 1] - b.y);
+    sm.z = tf32_rna(v[4 * c + 2] - b.z);
+    sm.w = tf32_rna(v[4 * c + 3] - b.w);
+    const uint32_t o = chunk_off(p, c);
+    *reinterpret_cast<float4*>(big + o) = b;
+    *reinterpret_cast<float4*>(small + o) = sm;
   }
 }
 
-template <int LAYOUT>
+// Row `row` of the panel, columns [kc, kc + 32) (ld = m; rows >= m and columns >=
+// kend read as 0).
+__device__ __forceinline__ void load_row(const float* __restrict__ F, int m, int row, int kc, int kend,
+                                         float (&v)[TKS]) {
+  const bool okr = row < m;
+#pragma unroll
+  for (int kk = 0; kk < TKS; ++kk) v[kk] = (okr && kc + kk < kend) ? F[row + (int64_t)(kc + kk) * m] : 0.f;
+}
+
 __global__ void __launch_bounds__(NTHREADS, 1)
 k_syrk_tc(float* __restrict__ L, float* __restrict__ U, const int64_t* __restrict__ l_off,
           const int64_t* __restrict__ u_off, const int* __restrict__ fm, const int* __restrict__ fk,
@@ -192,7 +177,7 @@ k_syrk_tc(float* __restrict__ L, float* __restrict__ U, const int64_t* __restric
 
   if (tid == 0) {
     for (int q = 0; q < NSTAGE; ++q) {
-      mbar_init(full0 + 8 * q, NPROD / 2);  // one producer group fills a stage
+      mbar_init(full0 + 8 * q, 128);  // one producer group fills a stage
       mbar_init(empty0 + 8 * q, 1);         // one tcgen05.commit frees it
     }
     *s_fail = 0;
@@ -209,11 +194,11 @@ k_syrk_tc(float* __restrict__ L, float* __restrict__ U, const int64_t* __restric
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
 
-  if (warp < 8) {
-    // producers: group g = warp / 4 takes stages st = g, g + 2, ...
+  if (warp < NPROD / 32) {
+    // producers: group g = warp / 4 takes stages st = g, g + NGROUP, ... in buffer g
     const int g = warp >> 2, p = tid & 127;
-    for (int st = g; st < nst; st += 2) {
-      const int buf = st % NSTAGE;
+    for (int st = g; st < nst; st += NGROUP) {
+      const int buf = g;
       if (st >= NSTAGE) {
         // the MMAs of stage st - NSTAGE must have consumed this buffer
         if (!mbar_wait(empty0 + 8 * buf, (uint32_t)(((st - NSTAGE) / NSTAGE) & 1))) {
@@ -224,8 +209,11 @@ k_syrk_tc(float* __restrict__ L, float* __restrict__ U, const int64_t* __restric
       if (*(volatile int*)s_fail) break;
       unsigned char* base = ops + buf * STAGE_BYTES;
       const int kc = J0 + st * TKS;
-      produce<LAYOUT>(F, m, r0, kc, J1, base, base + OPB, p);
-      if (!diag) produce<LAYOUT>(F, m, c0, kc, J1, base + 2 * OPB, base + 3 * OPB, p);
+      float va[TKS], vb[TKS];
+      load_row(F, m, r0 + p, kc, J1, va);
+      if (!diag) load_row(F, m, c0 + p, kc, J1, vb);
+      split_store(va, base, base + OPB, p);
+      if (!diag) split_store(vb, base + 2 * OPB, base + 3 * OPB, p);
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_arrive(full0 + 8 * buf);
     }
@@ -245,12 +233,11 @@ k_syrk_tc(float* __restrict__ L, float* __restrict__ U, const int64_t* __restric
         const uint32_t base = smem_u32(ops + buf * STAGE_BYTES);
         const uint32_t ab = base, as = base + OPB;
         const uint32_t bb = diag ? ab : base + 2 * OPB, bs = diag ? as : base + 3 * OPB;
-        constexpr uint32_t id = idesc<LAYOUT>();
 #pragma unroll
         for (int ks = 0; ks < TKS / 8; ++ks) {
-          mma_tf32(tmem, sdesc<LAYOUT>(as, ks), sdesc<LAYOUT>(bb, ks), id, (st > 0 || ks > 0) ? 1u : 0u);
-          mma_tf32(tmem, sdesc<LAYOUT>(ab, ks), sdesc<LAYOUT>(bs, ks), id, 1u);
-          mma_tf32(tmem, sdesc<LAYOUT>(ab, ks), sdesc<LAYOUT>(bb, ks), id, 1u);
+          mma_tf32(tmem, sdesc(as, ks), sdesc(bb, ks), (st > 0 || ks > 0) ? 1u : 0u);
+          mma_tf32(tmem, sdesc(ab, ks), sdesc(bs, ks), 1u);
+          mma_tf32(tmem, sdesc(ab, ks), sdesc(bb, ks), 1u);
         }
         mma_commit(empty0 + 8 * buf);
       }
@@ -286,12 +273,25 @@ k_syrk_tc(float* __restrict__ L, float* __restrict__ U, const int64_t* __restric
           : "r"(tmem + ((uint32_t)(32 * sub) << 16) + (uint32_t)col0));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
       if (r < m) {
+        // all loads of the 32 columns first, then all stores (the pointers may
+        // alias as far as the compiler knows, which would serialise them)
 #pragma unroll
-        for (int j = 0; j < 32; ++j) {
-          const int c = c0 + col0 + j;
-          if (c < m && c <= r) {
-            float* e = (c < k) ? L + lo + r + (int64_t)c * m : U + uo + (r - k) + (int64_t)(c - k) * (m - k);
-            *e -= __uint_as_float(v[j]);
+        for (int h = 0; h < 2; ++h) {
+          float old[16];
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const int c = c0 + col0 + 16 * h + j;
+            old[j] = 0.f;
+            if (c < m && c <= r)
+              old[j] = (c < k) ? L[lo + r + (int64_t)c * m] : U[uo + (r - k) + (int64_t)(c - k) * (m - k)];
+          }
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const int c = c0 + col0 + 16 * h + j;
+            if (c < m && c <= r) {
+              float* e = (c < k) ? L + lo + r + (int64_t)c * m : U + uo + (r - k) + (int64_t)(c - k) * (m - k);
+              *e = old[j] - __uint_as_float(v[16 * h + j]);
+            }
           }
         }
       }
@@ -309,16 +309,14 @@ k_syrk_tc(float* __restrict__ L, float* __restrict__ U, const int64_t* __restric
 }  // namespace
 
 std::string tc_update_setup() {
-  cudaError_t e = cudaFuncSetAttribute(k_syrk_tc<kTcLayout>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)SMEM_BYTES);
+  cudaError_t e = cudaFuncSetAttribute(k_syrk_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES);
   return e == cudaSuccess ? std::string() : std::string("cudaFuncSetAttribute(k_syrk_tc): ") + cudaGetErrorString(e);
 }
 
 void launch_syrk_tc(float* L, float* U, const int64_t* l_off, const int64_t* u_off, const int* m, const int* k,
                     const int* fronts, const int64_t* prefix, int count, int64_t ctas, int j0, int* err,
                     cudaStream_t s) {
-  k_syrk_tc<kTcLayout><<<(unsigned)ctas, NTHREADS, SMEM_BYTES, s>>>(L, U, l_off, u_off, m, k, fronts, prefix, count,
-                                                                    j0, err);
+  k_syrk_tc<<<(unsigned)ctas, NTHREADS, SMEM_BYTES, s>>>(L, U, l_off, u_off, m, k, fronts, prefix, count, j0, err);
 }
 
 }  // namespace tdem

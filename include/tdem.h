@@ -130,6 +130,51 @@ tdem_status tdem_solver_cancel(tdem_solver* s);
 const char* tdem_solver_error(const tdem_solver* s);
 void tdem_solver_destroy(tdem_solver* s);
 
+/* ---- Serving: a stream of forward-modelling requests on one GPU --------------------
+ * Requests (one model directory each, any mesh size, A/E, two/three-point) are planned
+ * on host threads (inputs, analysis), admitted first-in first-out when the device
+ * memory their analysis needs fits the HBM budget next to the running requests, and
+ * run concurrently on their own CUDA streams with factors and field histories resident
+ * until they finish.  Results are independent of what else runs (deterministic
+ * kernels).  No counterpart in the reference, which runs one CalcNonstat3DLine process
+ * per model (GeoCalculatorSP.cpp:1656-1662). */
+typedef struct tdem_server tdem_server;
+typedef struct tdem_server_options {
+  int device;               /* CUDA device */
+  int max_active;           /* requests on the device at once (default 4 when 0) */
+  int prep_threads;         /* host threads planning requests (default 2 when 0) */
+  int64_t hbm_budget_bytes; /* admission budget (default: 85% of the free device memory) */
+} tdem_server_options;
+typedef struct tdem_request_info {
+  int status;               /* tdem_status of the request */
+  int first_layer, last_layer, n_rec_b, n_rec_e, n_sources, steps, factorizations;
+  double submit_s, admit_s, done_s;  /* steady-clock seconds */
+  double run_gpu_ms;        /* device time of the request's time stepping */
+  int64_t device_bytes;     /* admission footprint */
+} tdem_request_info;
+typedef struct tdem_server_stats {
+  int64_t submitted, completed, failed;
+  double latency_p50_s, latency_p99_s; /* submit -> done */
+  double makespan_s, solves_per_s;     /* first submit -> last completion */
+  int64_t peak_device_bytes;
+  int peak_active;
+} tdem_server_stats;
+tdem_status tdem_server_create(const tdem_server_options* opts, tdem_server** out);
+/* Queues one request (write_outputs != 0: also write the reference output files into
+ * workdir); *request_id receives its id. */
+tdem_status tdem_server_submit(tdem_server* srv, const char* workdir, int formulation, int scheme,
+                               const tdem_options* opts, int write_outputs, int64_t* request_id);
+/* Blocks until the request has finished; returns its status.  info may be NULL. */
+tdem_status tdem_server_wait(tdem_server* srv, int64_t request_id, tdem_request_info* info);
+/* Output tables of a finished request, as tdem_solver_results. */
+tdem_status tdem_server_results(tdem_server* srv, int64_t request_id, double* eall, double* emf, double* ball);
+/* Error message of a finished request ("" when it succeeded); valid until the server
+ * is destroyed. */
+const char* tdem_server_error(tdem_server* srv, int64_t request_id);
+tdem_status tdem_server_stats_get(tdem_server* srv, tdem_server_stats* st);
+/* Runs every queued request to completion, then releases the server. */
+void tdem_server_destroy(tdem_server* srv);
+
 /* GPU-backed stand-in for MKL's pardiso_64 with the semantics the reference uses
  * (pardiso.cpp:69-126): mtype = 2 (real SPD), upper-triangular CSR with 1-based
  * int64 indices, phase 12 (analysis + numeric factorization; the analysis is
