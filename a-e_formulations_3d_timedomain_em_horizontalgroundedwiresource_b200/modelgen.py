@@ -357,6 +357,45 @@ def layered_block_model(cells: int = 80, core_h: float = 10.0, core_half: float 
                      receivers_e=[rec] * len(sources), times=t, n_srs_razb=n_srs_razb)
 
 
+def random_request_model(seed: int, cells_lo: int = 30, cells_hi: int = 100):
+    """One request of the served stream: mesh of U{cells_lo..cells_hi} cells per side,
+    1-3 layers with conductivity log-uniform in [1e-4, 1] S/m, 1-3 boxes of 50-400 m
+    edge with conductivity log-uniform in [1e-3, 1] S/m, A/E formulation and two- or
+    three-point scheme at random, 60-200 steps in doubling decades; every draw comes
+    from PCG64(seed).  Returns (spec, formulation, scheme)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    cells = int(rng.integers(cells_lo, cells_hi + 1))
+    form = "A" if rng.integers(0, 2) == 0 else "E"
+    scheme = int(rng.integers(2, 4))
+    n_core = max(8, cells // 2)
+    core_half = 200.0
+    core_h = 2 * core_half / n_core
+    n_side = (cells - n_core) // 2
+    x = symmetric_axis(core_half, core_h, n_side, 5000.0)
+    y = x.copy()
+    n_air = max(4, cells // 4)
+    n_earth = cells - n_air
+    n_earth_core = max(2, min(n_earth // 2, int(300.0 / core_h)))
+    z = vertical_axis(n_earth_core * core_h, core_h, n_earth - n_earth_core, 5000.0, n_air, 5000.0)
+    n_layers = int(rng.integers(1, 4))
+    tops = [0.0] + sorted((-rng.uniform(20.0, 400.0, n_layers - 1)).tolist(), reverse=True)
+    layers = [(t, float(10 ** rng.uniform(-4, 0))) for t in tops]
+    boxes = []
+    for _ in range(int(rng.integers(1, 4))):
+        e = rng.uniform(50.0, 400.0, 3)
+        c = (rng.uniform(-150, 150), rng.uniform(-150, 150), -rng.uniform(e[2] / 2 + 10, 400))
+        boxes.append(Box(c[0] - e[0] / 2, c[0] + e[0] / 2, c[1] - e[1] / 2, c[1] + e[1] / 2,
+                         c[2] - e[2] / 2, c[2] + e[2] / 2, float(10 ** rng.uniform(-3, 0))))
+    n_steps = int(rng.integers(60, 201))
+    n_dec = int(rng.integers(3, 9))
+    t = decade_time_grid(10 ** rng.uniform(-3, -1), n_dec, max(8, n_steps // n_dec))
+    src = [((-50.0, 0.0, 0.0), (50.0, 0.0, 0.0))]
+    rec = receivers_on_y_axis(11)
+    spec = ModelSpec(x=x, y=y, z=z, layers=layers, boxes=boxes, sources=src, receivers_b=[rec],
+                     receivers_e=[rec], times=t, n_srs_razb=100)
+    return spec, form, scheme
+
+
 def wire_grid_sources(nx: int = 4, ny: int = 8, spacing: float = 100.0, half: float = 50.0):
     """nx*ny 100 m x-directed wires with centres on a surface grid."""
     out = []

@@ -420,13 +420,79 @@ def run_ours(args, world, rank, local):
         shutil.rmtree(base, ignore_errors=True)
 
 
+def run_serving(args, world, rank, local):
+    """a Poisson stream of random forward-modelling requests through
+    the serving loop (tdem_server_*) on one GPU; prints solves/s and p50/p99 latency."""
+    import numpy as np
+    import torch
+    pkg = importlib.import_module(PKG)
+    mg = importlib.import_module(PKG + ".modelgen")
+    torch.cuda.set_device(local)
+    lo, hi = (int(v) for v in args.c4_cells.split(","))
+    s0 = 20261203
+    base = tempfile.mkdtemp(prefix="tdem_serve_r%d_" % rank)
+    try:
+        reqs = []
+        for i in range(args.c4_requests):
+            spec, form, scheme = mg.random_request_model(s0 + i, lo, hi)
+            d = os.path.join(base, "req%03d" % i)
+            info = mg.write_model(d, spec)
+            mg.write_analytic_initial_field(d, spec)
+            reqs.append((d, form, scheme, info["n_edges"]))
+        # single-stream service rate from the first requests run alone
+        t_alone = []
+        for d, form, scheme, _ in reqs[:2]:
+            t0 = time.perf_counter()
+            with pkg.Solver(d, form, scheme, device=local) as sv:
+                sv.run()
+                sv.results()
+            t_alone.append(time.perf_counter() - t0)
+        lam = 1.2 / (sum(t_alone) / len(t_alone))
+        rng = np.random.Generator(np.random.PCG64(s0))
+        arrivals = np.cumsum(rng.exponential(1.0 / lam, len(reqs)))
+        sampler = ClockSampler(local)
+        sampler.start()
+        with pkg.Server(device=local, max_active=args.c4_active) as srv:
+            t0 = time.perf_counter()
+            ids = []
+            for (d, form, scheme, _), ta in zip(reqs, arrivals):
+                delay = t0 + ta - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+                ids.append(srv.submit(d, form, scheme))
+            infos = [srv.wait(i) for i in ids]
+            st = srv.stats()
+        clocks = sampler.stop()
+        line = {"metric": "served forward solves/s + p50/p99 latency", "value": st["solves_per_s"],
+                "unit": "forward solves/s", "n_gpus": 1, "steps": len(reqs), "warmup": 0,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic",
+                "config": {"workload": "served stream: %d requests, %d^3..%d^3 cells, random A/E x 2/3-point, "
+                                       "1-3 layers + 1-3 boxes, 60-200 steps, PCG64(%d + i)" % (len(reqs), lo, hi, s0),
+                           "arrival_rate_per_s": lam, "single_stream_service_s": t_alone,
+                           "max_active": args.c4_active,
+                           "edges_min_max": [min(r[3] for r in reqs), max(r[3] for r in reqs)]},
+                "latency_s": {"p50": st["latency_p50_s"], "p99": st["latency_p99_s"]},
+                "makespan_s": st["makespan_s"], "completed": st["completed"], "failed": st["failed"],
+                "peak_device_gb": st["peak_device_bytes"] / 1e9, "peak_active": st["peak_active"],
+                "queue_wait_s_max": max(i["admit_s"] - i["submit_s"] for i in infos),
+                "clocks": clocks}
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+    finally:
+        shutil.rmtree(base, ignore_errors=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c5"])
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c5"])
+    ap.add_argument("--c4-requests", type=int, default=16, help="served-stream length (config c4)")
+    ap.add_argument("--c4-cells", default="30,60", help="mesh cells per side, lo,hi (config c4; 30,100 in full)")
+    ap.add_argument("--c4-active", type=int, default=4, help="requests on the device at once (config c4)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", type=int, default=64, choices=[64, 32],
                     help="64: FP64 factor; 32: FP32 factor preconditioning FP64 CG")
@@ -438,6 +504,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference_arm(args, world, rank, local)
+        elif args.config == "c4":
+            run_serving(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:
