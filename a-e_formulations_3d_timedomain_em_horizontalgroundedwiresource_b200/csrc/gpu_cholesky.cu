@@ -550,8 +550,14 @@ __device__ __forceinline__ int ld_acquire(const int* p) {
   asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
-__device__ __forceinline__ void st_release(int* p, int v) {
-  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+// Publishes the values the whole CTA stored before its last __syncthreads: the
+// acq_rel fence at GPU scope orders those stores (cumulatively, they were observed
+// through the barrier) before the relaxed flag store / counter increment.
+__device__ __forceinline__ void publish_flag(int* p) {
+  asm volatile("fence.acq_rel.gpu;\n\tst.relaxed.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(1) : "memory");
+}
+__device__ __forceinline__ void publish_add(int* p) {
+  asm volatile("fence.acq_rel.gpu;\n\tred.relaxed.gpu.global.add.s32 [%0], %1;" ::"l"(p), "r"(1) : "memory");
 }
 
 // Called by one thread.  Gives up after kSpinLimit polls (or at once when an
@@ -596,10 +602,7 @@ __device__ __forceinline__ void publish_partial(T* part, const T (&acc)[RPT], in
     if (r < nr_rhs) part[i + SB * r] = acc[j];
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    atomicAdd(counter, 1);
-  }
+  if (threadIdx.x == 0) publish_add(counter);
 }
 
 // The final unit of a row: acc = (p_0 + p_1) + ... in a fixed order (left as is
@@ -775,8 +778,7 @@ __global__ void __launch_bounds__(256, 2) k_fwd_level(const T* __restrict__ L, c
   }
   __syncthreads();
   if (t == 0) {
-    __threadfence();
-    st_release(fa.flags + fa.flag_off[s] + R, 1);
+    publish_flag(fa.flags + fa.flag_off[s] + R);
   }
 }
 
@@ -911,8 +913,7 @@ __global__ void __launch_bounds__(256, 2) k_bwd_level(const T* __restrict__ L, c
   }
   __syncthreads();
   if (t == 0) {
-    __threadfence();
-    st_release(fa.flags + fa.flag_off[s] + p, 1);
+    publish_flag(fa.flags + fa.flag_off[s] + p);
   }
 }
 
