@@ -582,14 +582,37 @@ __device__ void wait_count(const int* c, int target, int* err) {
 }
 
 struct FusedArgs {
-  const int* units;        // units of this launch (8 ints each, Symbolic::solve_units)
+  const int* units;        // units of this launch (kUnitInts ints each, Symbolic::solve_units)
+  int64_t count;           // units in this launch
   int* ticket;             // launch-order counter (zeroed before the solve)
   int* flags;              // one per pivot block (zeroed before the solve)
   int* counters;           // finished chunk units per row (zeroed before the solve)
-  const int64_t* flag_off; // per front: first flag
-  const int64_t* dinv_off; // per front: first inverted diagonal block
-  int* err;                // err[1]: a wait gave up
+  int* err;                // set to 1 when a wait gave up (the solver's err[1])
 };
+
+// A level-solve unit as unpacked from its 64-byte record.
+struct Unit {
+  int R, lo, hi, slot, cnt, nparts, fin, m, k, flag0;
+  int64_t l_off, w_off, dinv_off;
+};
+
+__device__ __forceinline__ int64_t join64(int lo, int hi) {
+  return (int64_t)(((uint64_t)(uint32_t)hi << 32) | (uint64_t)(uint32_t)lo);
+}
+
+// Every thread reads the same 64 bytes (one broadcast request per 16 bytes).
+__device__ __forceinline__ Unit load_unit(const int* __restrict__ units, int64_t idx) {
+  const int4* p = reinterpret_cast<const int4*>(units + (int64_t)kUnitInts * idx);
+  const int4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2), d = __ldg(p + 3);
+  Unit u;
+  u.R = a.x; u.lo = a.y; u.hi = a.z; u.slot = a.w;
+  u.cnt = b.x; u.nparts = b.y; u.fin = b.z; u.m = b.w;
+  u.k = c.x; u.flag0 = c.y;
+  u.l_off = join64(c.z, c.w);
+  u.w_off = join64(d.x, d.y);
+  u.dinv_off = join64(d.z, d.w);
+  return u;
+}
 
 // A chunk unit hands its partial sums (thread t: entries (t % 64, t / 64 + 4 j))
 // to the final unit of its row: store, then publish with a counter increment.
@@ -626,7 +649,8 @@ __device__ __forceinline__ void gather_partials(const T* part, int nparts, int n
 
 // 64 x 64 block of a front (rows [r0, r0 + nr), columns [c0, c0 + nc), zero
 // outside) into 16 registers per thread: element (i, c) goes to thread
-// (i + 64 c) mod 256, slot (i + 64 c) / 256.
+// (i + 64 c) mod 256, slot (i + 64 c) / 256, i.e. thread t holds row t % 64 of
+// columns t / 64 + 4 e.
 template <class T>
 __device__ __forceinline__ void load_block(T (&pre)[16], const T* __restrict__ F, int64_t ld, int r0, int nr, int c0,
                                            int nc) {
@@ -634,7 +658,7 @@ __device__ __forceinline__ void load_block(T (&pre)[16], const T* __restrict__ F
   for (int e = 0; e < 16; ++e) {
     const int q = threadIdx.x + 256 * e;
     const int i = q & 63, c = q >> 6;
-    pre[e] = (i < nr && c < nc) ? F[(r0 + i) + (int64_t)(c0 + c) * ld] : (T)0;
+    pre[e] = (i < nr && c < nc) ? __ldg(F + (r0 + i) + (int64_t)(c0 + c) * ld) : (T)0;
   }
 }
 // registers -> Ls[c][i]
@@ -647,15 +671,16 @@ __device__ __forceinline__ void store_block(T (*Ls)[SB + 1], const T (&pre)[16])
   }
 }
 
-// Forward unit: row block R of front s (R < pb: pivot rows [64R, ..); else update
-// rows [k + 64 (R - pb), ..)), accumulating L_Rq y_q for the pivot blocks q in
-// [lo, hi).  Chunk units publish partial sums; the final unit (q = the last one
-// the row needs) adds them, then a pivot row solves y_R = Dinv_R (w_R - sum) and
-// raises its flag, an update row stores w_R - sum for the parent.
+// Forward unit (many right-hand sides): row block R of front s (R < pb: pivot rows
+// [64R, ..); else update rows [k + 64 (R - pb), ..)), accumulating L_Rq y_q for
+// the pivot blocks q in [lo, hi).  Chunk units publish partial sums; the final
+// unit (q = the last one the row needs) adds them, then a pivot row solves
+// y_R = Dinv_R (w_R - sum) and raises its flag, an update row stores w_R - sum
+// for the parent.  One unit per CTA.
 // Thread t: row i = t % 64 of the block, right-hand sides r = t / 64 + 4 j.
 template <class T, int RPT>
 __global__ void __launch_bounds__(256, 2) k_fwd_level(const T* __restrict__ L, const T* __restrict__ Dinv, T* W, T* part,
-                                                   SolveArgs a, FusedArgs fa) {
+                                                   int nr_rhs, FusedArgs fa) {
   __shared__ T Ls[SB][SB + 1];
   __shared__ int s_item;
   extern __shared__ __align__(16) unsigned char sm_raw[];
@@ -663,16 +688,15 @@ __global__ void __launch_bounds__(256, 2) k_fwd_level(const T* __restrict__ L, c
   const int t = threadIdx.x, i = t & 63, g = t >> 6;
   if (t == 0) s_item = atomicAdd(fa.ticket, 1);
   __syncthreads();
-  const int* u = fa.units + 8 * s_item;
-  const int s = u[0], R = u[1], lo = u[2], hi = u[3], slot = u[4], cnt = u[5], nparts = u[6], fin = u[7];
-  const int m = a.m[s], k = a.k[s], nr_rhs = a.nrhs;
+  const Unit u = load_unit(fa.units, s_item);
+  const int R = u.R, lo = u.lo, hi = u.hi, m = u.m, k = u.k, fin = u.fin;
   const int pb = (k + SB - 1) / SB;
   const bool piv = R < pb;
   const int r0 = piv ? SB * R : k + SB * (R - pb);
   const int nr = min(SB, (piv ? k : m) - r0);
-  const T* F = L + a.l_off[s];
-  T* w = W + a.w_off[s] * nr_rhs;
-  const int* flags = fa.flags + fa.flag_off[s];
+  const T* F = L + u.l_off;
+  T* w = W + u.w_off * nr_rhs;
+  const int* flags = fa.flags + u.flag0;
   T acc[RPT];
 #pragma unroll
   for (int j = 0; j < RPT; ++j) acc[j] = (T)0;
@@ -681,7 +705,7 @@ __global__ void __launch_bounds__(256, 2) k_fwd_level(const T* __restrict__ L, c
   // (with many right-hand sides the registers go to the accumulators instead and
   // the inverse is read after the last block)
   constexpr bool kPreD = RPT <= 2;
-  const T* D = Dinv + fa.dinv_off[s] + (int64_t)R * SB * SB;
+  const T* D = Dinv + u.dinv_off + (int64_t)R * SB * SB;
   T dpre[kPreD ? 16 : 1], wrow[RPT];
   if (fin && piv) {
     if (kPreD) {
@@ -694,15 +718,15 @@ __global__ void __launch_bounds__(256, 2) k_fwd_level(const T* __restrict__ L, c
 #pragma unroll
     for (int j = 0; j < RPT; ++j) {
       const int r = g + 4 * j;
-      wrow[j] = (r < nr_rhs && i < nr) ? w[r0 + i + (int64_t)r * m] : (T)0;
+      wrow[j] = (r < nr_rhs && i < nr) ? __ldcg(w + r0 + i + (int64_t)r * m) : (T)0;
     }
   }
-  T* my_part = part + (int64_t)slot * SB * nr_rhs;
+  T* my_part = part + (int64_t)u.slot * SB * nr_rhs;
   T tot[RPT];
 #pragma unroll
   for (int j = 0; j < RPT; ++j) tot[j] = (T)0;
   // the chunk partials of this row are ready long before the last block's flag
-  if (fin) gather_partials<T, RPT>(my_part, nparts, nr_rhs, fa.counters + cnt, fa.err, tot);
+  if (fin) gather_partials<T, RPT>(my_part, u.nparts, nr_rhs, fa.counters + u.cnt, fa.err, tot);
   T pre[16];
   if (lo < hi) load_block(pre, F, m, r0, nr, SB * lo, min(SB, k - SB * lo));
   for (int q = lo; q < hi; ++q) {
@@ -727,7 +751,7 @@ __global__ void __launch_bounds__(256, 2) k_fwd_level(const T* __restrict__ L, c
     }
   }
   if (!fin) {
-    publish_partial<T, RPT>(my_part, acc, nr_rhs, fa.counters + cnt);
+    publish_partial<T, RPT>(my_part, acc, nr_rhs, fa.counters + u.cnt);
     return;
   }
 #pragma unroll
@@ -777,20 +801,20 @@ __global__ void __launch_bounds__(256, 2) k_fwd_level(const T* __restrict__ L, c
     }
   }
   __syncthreads();
-  if (t == 0) {
-    publish_flag(fa.flags + fa.flag_off[s] + R);
-  }
+  if (t == 0) publish_flag(fa.flags + u.flag0 + R);
 }
 
-// Backward unit: column block p of front s, accumulating L_Rp^T x_R over the row
-// blocks R in [lo, hi) (R < pb: pivot rows, waited for; else update rows, whose x
-// come from ancestors and were staged in W by k_bwd_init).  The final unit (row
-// block p + 1) adds the chunk partials and solves x_p = Dinv_p^T (y_p - sum),
-// written to W and to the caller's vector, then raises the column's flag.
+// Backward unit (many right-hand sides): column block p of front s, accumulating
+// L_Rp^T x_R over the row blocks R in [lo, hi) (R < pb: pivot rows, waited for;
+// else update rows, whose x come from ancestors and were staged in W by
+// k_bwd_init).  The final unit (row block p + 1) adds the chunk partials and
+// solves x_p = Dinv_p^T (y_p - sum), written to W and to the caller's vector,
+// then raises the column's flag.  One unit per CTA.
 // Thread t: column c = t % 64 of the block, right-hand sides r = t / 64 + 4 j.
 template <class T, int RPT>
 __global__ void __launch_bounds__(256, 2) k_bwd_level(const T* __restrict__ L, const T* __restrict__ Dinv, T* W, T* part,
-                                                   double* __restrict__ x, SolveArgs a, FusedArgs fa) {
+                                                   double* __restrict__ x, const int* __restrict__ rows, int64_t ldx,
+                                                   int nr_rhs, FusedArgs fa) {
   __shared__ T Ls[SB][SB + 1];
   __shared__ int s_item;
   extern __shared__ __align__(16) unsigned char sm_raw[];
@@ -798,19 +822,18 @@ __global__ void __launch_bounds__(256, 2) k_bwd_level(const T* __restrict__ L, c
   const int t = threadIdx.x, c = t & 63, g = t >> 6;
   if (t == 0) s_item = atomicAdd(fa.ticket, 1);
   __syncthreads();
-  const int* u = fa.units + 8 * s_item;
-  const int s = u[0], p = u[1], lo = u[2], hi = u[3], slot = u[4], cnt = u[5], nparts = u[6], fin = u[7];
-  const int m = a.m[s], k = a.k[s], nr_rhs = a.nrhs;
+  const Unit u = load_unit(fa.units, s_item);
+  const int p = u.R, lo = u.lo, hi = u.hi, m = u.m, k = u.k, fin = u.fin;
   const int pb = (k + SB - 1) / SB;
   const int c0 = SB * p, wc = min(SB, k - c0);
-  const T* F = L + a.l_off[s];
-  T* w = W + a.w_off[s] * nr_rhs;
-  const int* flags = fa.flags + fa.flag_off[s];
+  const T* F = L + u.l_off;
+  T* w = W + u.w_off * nr_rhs;
+  const int* flags = fa.flags + u.flag0;
   T acc[RPT];
 #pragma unroll
   for (int j = 0; j < RPT; ++j) acc[j] = (T)0;
   constexpr bool kPreD = RPT <= 2;
-  const T* D = Dinv + fa.dinv_off[s] + (int64_t)p * SB * SB;
+  const T* D = Dinv + u.dinv_off + (int64_t)p * SB * SB;
   T dpre[kPreD ? 16 : 1], wrow[RPT];
   if (fin) {
     if (kPreD) {
@@ -823,14 +846,14 @@ __global__ void __launch_bounds__(256, 2) k_bwd_level(const T* __restrict__ L, c
 #pragma unroll
     for (int j = 0; j < RPT; ++j) {
       const int r = g + 4 * j;
-      wrow[j] = (r < nr_rhs && c < wc) ? w[c0 + c + (int64_t)r * m] : (T)0;
+      wrow[j] = (r < nr_rhs && c < wc) ? __ldcg(w + c0 + c + (int64_t)r * m) : (T)0;
     }
   }
-  T* my_part = part + (int64_t)slot * SB * nr_rhs;
+  T* my_part = part + (int64_t)u.slot * SB * nr_rhs;
   T tot[RPT];
 #pragma unroll
   for (int j = 0; j < RPT; ++j) tot[j] = (T)0;
-  if (fin) gather_partials<T, RPT>(my_part, nparts, nr_rhs, fa.counters + cnt, fa.err, tot);
+  if (fin) gather_partials<T, RPT>(my_part, u.nparts, nr_rhs, fa.counters + u.cnt, fa.err, tot);
   auto rows_of = [&](int R, int& r0, int& nr) {
     r0 = (R < pb) ? SB * R : k + SB * (R - pb);
     nr = min(SB, (R < pb ? k : m) - r0);
@@ -870,7 +893,7 @@ __global__ void __launch_bounds__(256, 2) k_bwd_level(const T* __restrict__ L, c
     }
   }
   if (!fin) {
-    publish_partial<T, RPT>(my_part, acc, nr_rhs, fa.counters + cnt);
+    publish_partial<T, RPT>(my_part, acc, nr_rhs, fa.counters + u.cnt);
     return;
   }
   __syncthreads();
@@ -901,20 +924,474 @@ __global__ void __launch_bounds__(256, 2) k_bwd_level(const T* __restrict__ L, c
     }
   }
   if (c < wc) {
-    const int pos = a.rows[a.rows_off[s] + c0 + c];
+    const int pos = rows[u.w_off + c0 + c];
 #pragma unroll
     for (int j = 0; j < RPT; ++j) {
       const int r = g + 4 * j;
       if (r < nr_rhs) {
         w[c0 + c + (int64_t)r * m] = xv[j];
-        x[pos + (int64_t)r * a.ld] = (double)xv[j];
+        x[pos + (int64_t)r * ldx] = (double)xv[j];
       }
     }
   }
   __syncthreads();
-  if (t == 0) {
-    publish_flag(fa.flags + fa.flag_off[s] + p);
+  if (t == 0) publish_flag(fa.flags + u.flag0 + p);
+}
+
+// ---------------------------------------------------------------------------
+// Streaming level solves for one or two right-hand sides.
+//
+// Persistent CTAs (as many as fit on the device) take units by ticket until the
+// level's list is exhausted; the next ticket is taken when a unit starts, so its
+// latency hides behind the unit's work.  Each thread copies its own elements of
+// the unit's blocks into shared memory with cp.async, kStages blocks ahead of
+// their use (and the inverted diagonal block of a final unit at the start), so
+// a CTA keeps several 32 KB loads in flight without holding them in registers;
+// since a thread only reads back what it copied, no CTA barrier is needed
+// between copy and use.  Each warp waits for the pivot blocks it needs itself
+// (lane 0 polls, then a warp barrier).  The four column groups (forward) or 64
+// rows (backward) of a block are combined once per unit, in a fixed order, so
+// results are deterministic.
+// ---------------------------------------------------------------------------
+constexpr int kStages = 2;
+
+// cp.async of one element (4 or 8 bytes); src_bytes = 0 stores a zero instead.
+template <int BYTES>
+__device__ __forceinline__ void cp_async_elem(void* dst, const void* src, int src_bytes) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(d), "l"(src), "n"(BYTES), "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// This thread's 16 elements (row t % 64, columns t / 64 + 4 e) of the 64 x 64
+// block at rows [r0, r0 + nr), columns [c0, c0 + nc) of F (zero outside) into
+// buf[e * 256 + t].  Does not commit.
+template <class T>
+__device__ __forceinline__ void cp_block(T* buf, const T* __restrict__ F, int64_t ld, int r0, int nr, int c0, int nc) {
+  const int t = threadIdx.x, i = t & 63, g = t >> 6;
+#pragma unroll
+  for (int e = 0; e < 16; ++e) {
+    const int c = g + 4 * e;
+    const bool ok = i < nr && c < nc;
+    const T* src = ok ? F + (r0 + i) + (int64_t)(c0 + c) * ld : F;
+    cp_async_elem<(int)sizeof(T)>(buf + e * 256 + t, src, ok ? (int)sizeof(T) : 0);
   }
+}
+
+// Sum over the 32 lanes of a warp of v[e] for each e < 16 (recursive halving):
+// afterwards lane l holds the total of e = (l >> 1) & 15.  The additions happen
+// in an order fixed by the lane pattern alone.
+template <class T>
+__device__ __forceinline__ T warp_sum16(const T (&v)[16], int lane) {
+  T a8[8], a4[4], a2[2];
+  bool up = (lane & 16) != 0;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const T mine = up ? v[8 + j] : v[j], other = up ? v[j] : v[8 + j];
+    a8[j] = mine + __shfl_xor_sync(0xffffffffu, other, 16);
+  }
+  up = (lane & 8) != 0;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const T mine = up ? a8[4 + j] : a8[j], other = up ? a8[j] : a8[4 + j];
+    a4[j] = mine + __shfl_xor_sync(0xffffffffu, other, 8);
+  }
+  up = (lane & 4) != 0;
+#pragma unroll
+  for (int j = 0; j < 2; ++j) {
+    const T mine = up ? a4[2 + j] : a4[j], other = up ? a4[j] : a4[2 + j];
+    a2[j] = mine + __shfl_xor_sync(0xffffffffu, other, 4);
+  }
+  up = (lane & 2) != 0;
+  const T mine = up ? a2[1] : a2[0], other = up ? a2[0] : a2[1];
+  const T a1 = mine + __shfl_xor_sync(0xffffffffu, other, 2);
+  return a1 + __shfl_xor_sync(0xffffffffu, a1, 1);
+}
+
+// Lane 0 of the calling warp waits for *flag; the warp barrier then orders the
+// other lanes' later loads after the acquire.
+__device__ __forceinline__ void warp_wait_flag(const int* flag, int* err, int lane) {
+  if (lane == 0) wait_flag(flag, err);
+  __syncwarp();
+}
+__device__ __forceinline__ void warp_wait_count(const int* c, int target, int* err, int lane) {
+  if (lane == 0) wait_count(c, target, err);
+  __syncwarp();
+}
+
+// Waits (whole warp) until flags[lo .. hi) are all set, hi - lo <= 32: lane j
+// polls flag lo + j.  The polls back off to sleep_max ns, so units queued early
+// (bulk work waiting for the dependency chain) keep the L2 slice that holds the
+// flags free for the chain itself.  Bounded like wait_flag.
+__device__ __forceinline__ void warp_wait_range(const int* flags, int lo, int hi, int* err, int lane,
+                                                unsigned sleep_max) {
+  if (lo >= hi) return;
+  // every lane takes the same branch: lane 0's view of the error flag decides
+  if (__shfl_sync(0xffffffffu, *(volatile int*)err, 0) == 0) {
+    unsigned ns = 32;
+    unsigned it = 0;
+    for (; it < kSpinLimit; ++it) {
+      const int v = (lo + lane < hi) ? ld_acquire(flags + lo + lane) : 1;
+      if (__all_sync(0xffffffffu, v != 0)) break;
+      __nanosleep(ns);
+      ns = min(2 * ns, sleep_max);
+    }
+    if (it == kSpinLimit && lane == 0) atomicExch(err, 1);
+  }
+  __syncwarp();
+}
+
+static_assert(kUnitBlocks <= 32, "one lane per flag");
+
+// Dynamic shared memory of the streaming kernels: kStages block buffers and the
+// inverted diagonal block, 64 x 64 entries each.
+template <class T>
+constexpr size_t stream_smem() { return sizeof(T) * (kStages + 1) * SB * SB; }
+
+// Forward unit, streaming form (see k_fwd_level for the unit's meaning).
+// Thread t holds row i = t % 64 of columns g + 4 e (g = t / 64, e < 16) of each
+// block and accumulates its share of the row sums for every right-hand side.
+template <class T, int NR>
+__global__ void __launch_bounds__(256, 2) k_fwd_stream(const T* __restrict__ L, const T* __restrict__ Dinv, T* W,
+                                                    T* part, int nr_rhs, FusedArgs fa) {
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  T* stage = reinterpret_cast<T*>(sm_raw);     // kStages x 4096
+  T* dsm = stage + kStages * SB * SB;          // inverted diagonal block, 4096
+  __shared__ T red[4][SB][NR];  // per column group: partial row sums
+  __shared__ T zs[SB][NR];      // pivot rows: w - sum, the input of the inverse
+  __shared__ T ys[kUnitBlocks][SB][NR];  // bulk units: y of every block of the unit
+  __shared__ int s_tk[2];
+  const int t = threadIdx.x, i = t & 63, g = t >> 6, lane = t & 31;
+  if (t == 0) s_tk[0] = atomicAdd(fa.ticket, 1);
+  __syncthreads();
+  for (int par = 0;; par ^= 1) {
+    const int tk = s_tk[par];
+    if (tk >= fa.count) break;
+    int next = 0;
+    if (t == 0) next = atomicAdd(fa.ticket, 1);
+    const Unit u = load_unit(fa.units, tk);
+    const int R = u.R, lo = u.lo, hi = u.hi, m = u.m, k = u.k;
+    const bool fin = u.fin != 0;
+    const int pb = (k + SB - 1) / SB;
+    const bool piv = R < pb;
+    const int r0 = piv ? SB * R : k + SB * (R - pb);
+    const int nr = min(SB, (piv ? k : m) - r0);
+    const T* F = L + u.l_off;
+    T* w = W + u.w_off * nr_rhs;
+    const int* flags = fa.flags + u.flag0;
+    // final pivot unit: the inverted diagonal block (independent of this launch)
+    if (fin && piv) cp_block(dsm, Dinv + u.dinv_off + (int64_t)R * SB * SB, nr, 0, nr, 0, nr);
+#pragma unroll
+    for (int j = 0; j < kStages; ++j) {
+      const int q = lo + j;
+      if (q < hi) cp_block(stage + j * SB * SB, F, m, r0, nr, SB * q, min(SB, k - SB * q));
+      cp_async_commit();
+    }
+    T wrow[NR];
+    if (fin && g == 0) {
+#pragma unroll
+      for (int r = 0; r < NR; ++r) wrow[r] = (r < nr_rhs && i < nr) ? __ldcg(w + r0 + i + (int64_t)r * m) : (T)0;
+    }
+    T acc[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) acc[r] = (T)0;
+    // chunk partials of this row (warps of column group 0): gathered before the
+    // wait for the newest block, which is the last input of a chain unit
+    T tot[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) tot[r] = (T)0;
+    T* my_part = part + (int64_t)u.slot * SB * nr_rhs;
+    auto gather = [&]() {
+      if (fin && g == 0 && u.nparts > 0) {
+        warp_wait_count(fa.counters + u.cnt, u.nparts, fa.err, lane);
+        for (int c = 0; c < u.nparts; ++c)
+#pragma unroll
+          for (int r = 0; r < NR; ++r)
+            if (r < nr_rhs) tot[r] += __ldcg(my_part + (int64_t)c * SB * nr_rhs + i + SB * r);
+      }
+    };
+    // A chain unit (final unit of a pivot row) takes its blocks as their flags
+    // appear.  Any other unit normally finds all its flags set: it waits for them
+    // together and stages the y of all its blocks with one barrier.
+    const bool chain = fin && piv;
+    if (!chain) {
+      warp_wait_range(flags, lo, hi, fa.err, lane, 2048);
+      for (int e = t; e < (hi - lo) * SB * NR; e += 256) {
+        const int b = e / (SB * NR), c = (e / NR) % SB, r = e % NR;
+        const int q = lo + b;
+        ys[b][c][r] = (r < nr_rhs && c < min(SB, k - SB * q)) ? __ldcg(w + SB * q + c + (int64_t)r * m) : (T)0;
+      }
+      __syncthreads();
+    }
+    if (lo == hi) gather();
+    for (int q = lo; q < hi; ++q) {
+      const int slot = (q - lo) % kStages;
+      if (q == hi - 1) gather();
+      const T* blk = stage + slot * SB * SB + t;
+      if (chain) {
+        warp_wait_flag(flags + q, fa.err, lane);
+        const int wq = min(SB, k - SB * q), c = g + 4 * (lane & 15);
+        T yv[NR];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) yv[r] = (r < nr_rhs && c < wq) ? __ldcg(w + SB * q + c + (int64_t)r * m) : (T)0;
+        cp_async_wait<kStages - 1>();
+#pragma unroll
+        for (int e = 0; e < 16; ++e) {
+          const T l = blk[e * 256];
+#pragma unroll
+          for (int r = 0; r < NR; ++r) acc[r] = fma(l, __shfl_sync(0xffffffffu, yv[r], e), acc[r]);
+        }
+      } else {
+        cp_async_wait<kStages - 1>();
+        const T(*yb)[NR] = ys[q - lo];
+#pragma unroll
+        for (int e = 0; e < 16; ++e) {
+          const T l = blk[e * 256];
+#pragma unroll
+          for (int r = 0; r < NR; ++r) acc[r] = fma(l, yb[g + 4 * e][r], acc[r]);
+        }
+      }
+      // the slot's values are in registers and used: refill it
+      const int qn = q + kStages;
+      if (qn < hi) cp_block(stage + slot * SB * SB, F, m, r0, nr, SB * qn, min(SB, k - SB * qn));
+      cp_async_commit();
+    }
+    // row totals: chunk partials (in order), then the four column groups
+    if (g != 0) {
+#pragma unroll
+      for (int r = 0; r < NR; ++r) red[g][i][r] = acc[r];
+    }
+    __syncthreads();
+    if (g == 0) {
+#pragma unroll
+      for (int r = 0; r < NR; ++r) acc[r] = ((acc[r] + red[1][i][r]) + red[2][i][r]) + red[3][i][r];
+      if (!fin) {
+#pragma unroll
+        for (int r = 0; r < NR; ++r)
+          if (r < nr_rhs) my_part[i + SB * r] = acc[r];
+      } else if (!piv) {
+        if (i < nr) {
+#pragma unroll
+          for (int r = 0; r < NR; ++r)
+            if (r < nr_rhs) w[r0 + i + (int64_t)r * m] -= tot[r] + acc[r];
+        }
+      } else {
+#pragma unroll
+        for (int r = 0; r < NR; ++r) zs[i][r] = (i < nr) ? wrow[r] - (tot[r] + acc[r]) : (T)0;
+      }
+    }
+    if (fin && piv) {
+      // y_R = Dinv_R z: thread (i, g) sums its 16 columns, then the groups are added
+      cp_async_wait_all();
+      __syncthreads();
+      T y[NR];
+#pragma unroll
+      for (int r = 0; r < NR; ++r) y[r] = (T)0;
+#pragma unroll
+      for (int e = 0; e < 16; ++e) {
+        const T d = dsm[e * 256 + t];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) y[r] = fma(d, zs[g + 4 * e][r], y[r]);
+      }
+      if (g != 0) {
+#pragma unroll
+        for (int r = 0; r < NR; ++r) red[g][i][r] = y[r];
+      }
+      __syncthreads();
+      if (g == 0 && i < nr) {
+#pragma unroll
+        for (int r = 0; r < NR; ++r)
+          if (r < nr_rhs) w[r0 + i + (int64_t)r * m] = ((y[r] + red[1][i][r]) + red[2][i][r]) + red[3][i][r];
+      }
+    }
+    const bool publish = !fin || piv;
+    if (t == 0) s_tk[par ^ 1] = next;
+    __syncthreads();
+    if (t == 0 && publish) {
+      if (fin) publish_flag(fa.flags + u.flag0 + R);
+      else publish_add(fa.counters + u.cnt);
+    }
+  }
+  cp_async_wait_all();
+}
+
+// Backward unit, streaming form (see k_bwd_level for the unit's meaning).
+// Thread t holds row i = t % 64 of columns g + 4 e of each block and accumulates
+// L(i, c) x(i) per column; the 64 rows of a column are added once per unit.
+template <class T, int NR>
+__global__ void __launch_bounds__(256, 2) k_bwd_stream(const T* __restrict__ L, const T* __restrict__ Dinv, T* W,
+                                                    T* part, double* __restrict__ x, const int* __restrict__ rows,
+                                                    int64_t ldx, int nr_rhs, FusedArgs fa) {
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  T* stage = reinterpret_cast<T*>(sm_raw);
+  T* dsm = stage + kStages * SB * SB;
+  __shared__ T red[2][SB][NR];  // per row half: column sums
+  __shared__ T zs[SB][NR];      // y_p - sum, the input of the inverse
+  __shared__ T xs[kUnitBlocks][SB][NR];  // chunks: x of every row block of the unit
+  __shared__ int s_tk[2];
+  const int t = threadIdx.x, i = t & 63, g = t >> 6, lane = t & 31, half = (t >> 5) & 1;
+  // column of the warp-reduced value this lane holds
+  const int cl = g + 4 * ((lane >> 1) & 15);
+  if (t == 0) s_tk[0] = atomicAdd(fa.ticket, 1);
+  __syncthreads();
+  for (int par = 0;; par ^= 1) {
+    const int tk = s_tk[par];
+    if (tk >= fa.count) break;
+    int next = 0;
+    if (t == 0) next = atomicAdd(fa.ticket, 1);
+    const Unit u = load_unit(fa.units, tk);
+    const int p = u.R, lo = u.lo, hi = u.hi, m = u.m, k = u.k;
+    const bool fin = u.fin != 0;
+    const int pb = (k + SB - 1) / SB;
+    const int c0 = SB * p, wc = min(SB, k - c0);
+    const T* F = L + u.l_off;
+    T* w = W + u.w_off * nr_rhs;
+    const int* flags = fa.flags + u.flag0;
+    auto rows_of = [&](int R, int& r0, int& nr) {
+      r0 = (R < pb) ? SB * R : k + SB * (R - pb);
+      nr = min(SB, (R < pb ? k : m) - r0);
+    };
+    if (fin) cp_block(dsm, Dinv + u.dinv_off + (int64_t)p * SB * SB, wc, 0, wc, 0, wc);
+    // rows farthest from the diagonal first (their x are known earliest)
+#pragma unroll
+    for (int j = 0; j < kStages; ++j) {
+      const int R = hi - 1 - j;
+      if (R >= lo) {
+        int r0, nr;
+        rows_of(R, r0, nr);
+        cp_block(stage + j * SB * SB, F, m, r0, nr, c0, wc);
+      }
+      cp_async_commit();
+    }
+    T wrow[NR];
+    if (fin && t < SB) {
+#pragma unroll
+      for (int r = 0; r < NR; ++r) wrow[r] = (r < nr_rhs && t < wc) ? __ldcg(w + c0 + t + (int64_t)r * m) : (T)0;
+    }
+    T acc[NR][16];
+#pragma unroll
+    for (int r = 0; r < NR; ++r)
+#pragma unroll
+      for (int e = 0; e < 16; ++e) acc[r][e] = (T)0;
+    // chunk partials of this column (warps 0 and 1), gathered before the wait for
+    // the newest row block
+    T tot[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) tot[r] = (T)0;
+    T* my_part = part + (int64_t)u.slot * SB * nr_rhs;
+    auto gather = [&]() {
+      if (fin && t < SB && u.nparts > 0) {
+        warp_wait_count(fa.counters + u.cnt, u.nparts, fa.err, lane);
+        for (int c = 0; c < u.nparts; ++c)
+#pragma unroll
+          for (int r = 0; r < NR; ++r)
+            if (r < nr_rhs) tot[r] += __ldcg(my_part + (int64_t)c * SB * nr_rhs + t + SB * r);
+      }
+    };
+    // The final unit (a link of the chain) takes its row blocks as their flags
+    // appear; a chunk waits for all its flags together and stages x of all its
+    // row blocks with one barrier.
+    if (!fin) {
+      warp_wait_range(flags, lo, min(hi, pb), fa.err, lane, 2048);
+      for (int e = t; e < (hi - lo) * SB * NR; e += 256) {
+        const int b = e / (SB * NR), ii = (e / NR) % SB, r = e % NR;
+        int r0, nr;
+        rows_of(lo + b, r0, nr);
+        xs[b][ii][r] = (r < nr_rhs && ii < nr) ? __ldcg(w + r0 + ii + (int64_t)r * m) : (T)0;
+      }
+      __syncthreads();
+    }
+    if (lo == hi) gather();
+    for (int R = hi - 1; R >= lo; --R) {
+      const int slot = (hi - 1 - R) % kStages;
+      int r0, nr;
+      rows_of(R, r0, nr);
+      if (R == lo) gather();
+      T xv[NR];
+      if (fin) {
+        if (R < pb) warp_wait_flag(flags + R, fa.err, lane);
+#pragma unroll
+        for (int r = 0; r < NR; ++r) xv[r] = (r < nr_rhs && i < nr) ? __ldcg(w + r0 + i + (int64_t)r * m) : (T)0;
+      } else {
+#pragma unroll
+        for (int r = 0; r < NR; ++r) xv[r] = xs[R - lo][i][r];
+      }
+      cp_async_wait<kStages - 1>();
+      const T* blk = stage + slot * SB * SB + t;
+#pragma unroll
+      for (int e = 0; e < 16; ++e) {
+        const T l = blk[e * 256];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) acc[r][e] = fma(l, xv[r], acc[r][e]);
+      }
+      const int Rn = R - kStages;
+      if (Rn >= lo) {
+        int rn0, nrn;
+        rows_of(Rn, rn0, nrn);
+        cp_block(stage + slot * SB * SB, F, m, rn0, nrn, c0, wc);
+      }
+      cp_async_commit();
+    }
+    // column totals: rows within the warp, then the two row halves
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+      const T v = warp_sum16(acc[r], lane);
+      if ((lane & 1) == 0) red[half][cl][r] = v;
+    }
+    __syncthreads();
+    if (t < SB) {
+      T s[NR];
+#pragma unroll
+      for (int r = 0; r < NR; ++r) s[r] = red[0][t][r] + red[1][t][r];
+      if (!fin) {
+#pragma unroll
+        for (int r = 0; r < NR; ++r)
+          if (r < nr_rhs) my_part[t + SB * r] = s[r];
+      } else {
+#pragma unroll
+        for (int r = 0; r < NR; ++r) zs[t][r] = (t < wc) ? wrow[r] - (tot[r] + s[r]) : (T)0;
+      }
+    }
+    if (fin) {
+      // x_p = Dinv_p^T z: thread (i, g) forms D(i, c) z(i) for its 16 columns, then
+      // the rows are added as above
+      cp_async_wait_all();
+      __syncthreads();
+#pragma unroll
+      for (int r = 0; r < NR; ++r) {
+        const T zi = zs[i][r];
+#pragma unroll
+        for (int e = 0; e < 16; ++e) acc[r][e] = dsm[e * 256 + t] * zi;
+      }
+#pragma unroll
+      for (int r = 0; r < NR; ++r) {
+        const T v = warp_sum16(acc[r], lane);
+        if ((lane & 1) == 0) red[half][cl][r] = v;
+      }
+      __syncthreads();
+      if (t < wc) {
+        const int pos = rows[u.w_off + c0 + t];
+#pragma unroll
+        for (int r = 0; r < NR; ++r)
+          if (r < nr_rhs) {
+            const T xs = red[0][t][r] + red[1][t][r];
+            w[c0 + t + (int64_t)r * m] = xs;
+            x[pos + (int64_t)r * ldx] = (double)xs;
+          }
+      }
+    }
+    if (t == 0) s_tk[par ^ 1] = next;
+    __syncthreads();
+    if (t == 0) {
+      if (fin) publish_flag(fa.flags + u.flag0 + p);
+      else publish_add(fa.counters + u.cnt);
+    }
+  }
+  cp_async_wait_all();
 }
 
 // Inverse of the lower-triangular diagonal block p of front s (w x w, w <= 64),
@@ -1087,17 +1564,24 @@ int launch_solve(const Symbolic& sy, const T* L, T* W, T* part, const double* b,
   return launches;
 }
 
-template <class T, int RPT>
+// One forward and one backward launch per level (plus the front-vector set-up).
+// STREAM: the persistent streaming kernels (nrhs <= NR <= 4, grid = resident
+// CTAs); otherwise the one-unit-per-CTA kernels with RPT right-hand sides per thread.
+template <class T, int RPT, bool STREAM>
 void launch_level_solves(const Symbolic& sy, const T* L, const T* Dinv, T* W, T* part, const double* b, double* x,
                          SolveArgs a, const int* parent, const int64_t* rel_off, const int* rel, const int* tasks,
-                         const int64_t* prefix, FusedArgs fa, int* sync, int& launches, cudaStream_t s) {
+                         const int64_t* prefix, FusedArgs fa, int* sync, const int (&resident)[2], int& launches,
+                         cudaStream_t s) {
   const int nlev = (int)sy.levels.size();
   int* tickets = sync;
   int* fflags = sync + 2 * nlev;
   int* bflags = fflags + sy.n_flags;
   fa.counters = bflags + sy.n_flags;
   cudaMemsetAsync(sync, 0, sizeof(int) * (2 * nlev + 2 * sy.n_flags + sy.n_counters), s);
-  const size_t ysm = sizeof(T) * SB * a.nrhs;
+  const size_t ysm = STREAM ? stream_smem<T>() : sizeof(T) * SB * a.nrhs;
+  auto grid = [&](int64_t count, int dir) {
+    return STREAM ? (unsigned)std::min<int64_t>(count, resident[dir]) : grid_of(count);
+  };
   for (int l = 0; l < nlev; ++l) {
     const LevelPlan& lp = sy.levels[l];
     k_fwd_init<T><<<grid_of(lp.assemble.ctas), kSolveRows, 0, s>>>(W, b, a, tasks + lp.assemble.off,
@@ -1109,11 +1593,16 @@ void launch_level_solves(const Symbolic& sy, const T* L, const T* Dinv, T* W, T*
                                                               prefix + tl.pre, tl.count);
       ++launches;
     }
+    if (lp.fwd_count == 0) continue;
     FusedArgs f = fa;
-    f.units = fa.units + 8 * lp.fwd_off;
+    f.units = fa.units + (int64_t)kUnitInts * lp.fwd_off;
+    f.count = lp.fwd_count;
     f.ticket = tickets + 2 * l;
     f.flags = fflags;
-    k_fwd_level<T, RPT><<<grid_of(lp.fwd_count), 256, ysm, s>>>(L, Dinv, W, part, a, f);
+    if constexpr (STREAM)
+      k_fwd_stream<T, RPT><<<grid(lp.fwd_count, 0), 256, ysm, s>>>(L, Dinv, W, part, a.nrhs, f);
+    else
+      k_fwd_level<T, RPT><<<grid(lp.fwd_count, 0), 256, ysm, s>>>(L, Dinv, W, part, a.nrhs, f);
     ++launches;
   }
   for (int l = nlev - 1; l >= 0; --l) {
@@ -1121,11 +1610,16 @@ void launch_level_solves(const Symbolic& sy, const T* L, const T* Dinv, T* W, T*
     k_bwd_init<T><<<grid_of(lp.assemble.ctas), kSolveRows, 0, s>>>(W, x, a, tasks + lp.assemble.off,
                                                                    prefix + lp.assemble.pre, lp.assemble.count);
     ++launches;
+    if (lp.bwd_count == 0) continue;
     FusedArgs f = fa;
-    f.units = fa.units + 8 * lp.bwd_off;
+    f.units = fa.units + (int64_t)kUnitInts * lp.bwd_off;
+    f.count = lp.bwd_count;
     f.ticket = tickets + 2 * l + 1;
     f.flags = bflags;
-    k_bwd_level<T, RPT><<<grid_of(lp.bwd_count), 256, ysm, s>>>(L, Dinv, W, part, x, a, f);
+    if constexpr (STREAM)
+      k_bwd_stream<T, RPT><<<grid(lp.bwd_count, 1), 256, ysm, s>>>(L, Dinv, W, part, x, a.rows, a.ld, a.nrhs, f);
+    else
+      k_bwd_level<T, RPT><<<grid(lp.bwd_count, 1), 256, ysm, s>>>(L, Dinv, W, part, x, a.rows, a.ld, a.nrhs, f);
     ++launches;
   }
 }
@@ -1133,31 +1627,60 @@ void launch_level_solves(const Symbolic& sy, const T* L, const T* Dinv, T* W, T*
 template <class T>
 int launch_solve_fused(const Symbolic& sy, const T* L, const T* Dinv, T* W, T* part, const double* b, double* x,
                        SolveArgs a, const int* parent, const int64_t* rel_off, const int* rel, const int* tasks,
-                       const int64_t* prefix, FusedArgs fa, int* sync, cudaStream_t s) {
+                       const int64_t* prefix, FusedArgs fa, int* sync, const int (&resident)[2][2], cudaStream_t s) {
   int launches = 0;
-  if (a.nrhs <= 4)
-    launch_level_solves<T, 1>(sy, L, Dinv, W, part, b, x, a, parent, rel_off, rel, tasks, prefix, fa, sync, launches, s);
+#define TDEM_LEVELS(R, ST, RES) \
+  launch_level_solves<T, R, ST>(sy, L, Dinv, W, part, b, x, a, parent, rel_off, rel, tasks, prefix, fa, sync, RES, \
+                                launches, s)
+  if (a.nrhs == 1)
+    TDEM_LEVELS(1, true, resident[0]);
+  else if (a.nrhs == 2)
+    TDEM_LEVELS(2, true, resident[1]);
+  else if (a.nrhs <= 4)
+    TDEM_LEVELS(1, false, resident[0]);
   else if (a.nrhs <= 8)
-    launch_level_solves<T, 2>(sy, L, Dinv, W, part, b, x, a, parent, rel_off, rel, tasks, prefix, fa, sync, launches, s);
+    TDEM_LEVELS(2, false, resident[0]);
   else if (a.nrhs <= 16)
-    launch_level_solves<T, 4>(sy, L, Dinv, W, part, b, x, a, parent, rel_off, rel, tasks, prefix, fa, sync, launches, s);
+    TDEM_LEVELS(4, false, resident[0]);
   else if (a.nrhs <= 32)
-    launch_level_solves<T, 8>(sy, L, Dinv, W, part, b, x, a, parent, rel_off, rel, tasks, prefix, fa, sync, launches, s);
+    TDEM_LEVELS(8, false, resident[0]);
   else
-    launch_level_solves<T, 16>(sy, L, Dinv, W, part, b, x, a, parent, rel_off, rel, tasks, prefix, fa, sync, launches,
-                               s);
+    TDEM_LEVELS(16, false, resident[0]);
+#undef TDEM_LEVELS
   return launches;
+}
+
+// Resident CTAs on the device of each streaming kernel ([NR = 1, 2][forward, backward]).
+template <class T>
+std::string stream_residency(int (&resident)[2][2]) {
+  int dev = 0, sms = 0;
+  TDEM_CUDA_TRY(cudaGetDevice(&dev));
+  TDEM_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int sm = (int)stream_smem<T>();
+  TDEM_CUDA_TRY(cudaFuncSetAttribute(k_fwd_stream<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  TDEM_CUDA_TRY(cudaFuncSetAttribute(k_fwd_stream<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  TDEM_CUDA_TRY(cudaFuncSetAttribute(k_bwd_stream<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  TDEM_CUDA_TRY(cudaFuncSetAttribute(k_bwd_stream<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  int occ[2][2] = {};
+  TDEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[0][0], k_fwd_stream<T, 1>, 256, sm));
+  TDEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1][0], k_fwd_stream<T, 2>, 256, sm));
+  TDEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[0][1], k_bwd_stream<T, 1>, 256, sm));
+  TDEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1][1], k_bwd_stream<T, 2>, 256, sm));
+  for (int j = 0; j < 2; ++j)
+    for (int d = 0; d < 2; ++d) {
+      if (occ[j][d] < 1) return "streaming level solve does not fit on an SM";
+      resident[j][d] = occ[j][d] * sms;
+    }
+  return "";
 }
 
 template <class T>
 std::string set_fused_attributes() {
   const int ysm = (int)(sizeof(T) * SB * kMaxRhs);
-  TDEM_CUDA_TRY(cudaFuncSetAttribute(k_fwd_level<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, ysm));
   TDEM_CUDA_TRY(cudaFuncSetAttribute(k_fwd_level<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, ysm));
   TDEM_CUDA_TRY(cudaFuncSetAttribute(k_fwd_level<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, ysm));
   TDEM_CUDA_TRY(cudaFuncSetAttribute(k_fwd_level<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, ysm));
   TDEM_CUDA_TRY(cudaFuncSetAttribute(k_fwd_level<T, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, ysm));
-  TDEM_CUDA_TRY(cudaFuncSetAttribute(k_bwd_level<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, ysm));
   TDEM_CUDA_TRY(cudaFuncSetAttribute(k_bwd_level<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, ysm));
   TDEM_CUDA_TRY(cudaFuncSetAttribute(k_bwd_level<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, ysm));
   TDEM_CUDA_TRY(cudaFuncSetAttribute(k_bwd_level<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, ysm));
@@ -1250,6 +1773,7 @@ std::string GpuCholesky::setup(Symbolic&& sy, const std::vector<int>& perm_to_ve
   if (elem_ == 4 && tc_update_ && !(e = tc_update_setup()).empty()) return e;
   if (!(e = (elem_ == 4 ? set_attributes<float>() : set_attributes<double>())).empty()) return e;
   if (!(e = (elem_ == 4 ? set_fused_attributes<float>() : set_fused_attributes<double>())).empty()) return e;
+  if (!(e = (elem_ == 4 ? stream_residency<float>(resident_) : stream_residency<double>(resident_))).empty()) return e;
   TDEM_CUDA_TRY(cudaStreamSynchronize(s));
   return "";
 }
@@ -1275,15 +1799,15 @@ void GpuCholesky::factor(const double* d_vals, cudaStream_t s) {
 void GpuCholesky::solve(const double* d_b, double* d_x, int64_t ld, int nrhs, cudaStream_t s) {
   SolveArgs a{d_l_off_, d_w_off_, d_m_, d_k_, d_rows_off_, d_rows_, nrhs, ld};
   if (!panel_solve_) {
-    FusedArgs fa{d_units_, nullptr, nullptr, nullptr, d_flag_off_, d_dinv_off_, d_err_};
+    FusedArgs fa{d_units_, 0, nullptr, nullptr, nullptr, d_err_ + 1};
     if (elem_ == 4)
       launches_solve_ = launch_solve_fused<float>(sy_, (const float*)d_L_, (const float*)d_dinv_, (float*)d_W_,
                                                   (float*)d_spart_, d_b, d_x, a, d_parent_, d_rel_off_, d_rel_,
-                                                  d_tasks_, d_prefix_, fa, d_sync_, s);
+                                                  d_tasks_, d_prefix_, fa, d_sync_, resident_, s);
     else
       launches_solve_ = launch_solve_fused<double>(sy_, (const double*)d_L_, (const double*)d_dinv_, (double*)d_W_,
                                                    (double*)d_spart_, d_b, d_x, a, d_parent_, d_rel_off_, d_rel_,
-                                                   d_tasks_, d_prefix_, fa, d_sync_, s);
+                                                   d_tasks_, d_prefix_, fa, d_sync_, resident_, s);
     return;
   }
   if (elem_ == 4)

@@ -74,6 +74,7 @@ class GpuCholesky {
   int elem_ = 8;                 // bytes per factor entry (8 = FP64, 4 = FP32)
   bool panel_solve_ = false;
   bool tc_update_ = false;
+  int resident_[2][2] = {};      // resident CTAs of the streaming level solves [NR 1, 2][fwd, bwd]
   cudaGraphExec_t graph_exec_ = nullptr;
   const double* g_b_ = nullptr;
   double* g_x_ = nullptr;

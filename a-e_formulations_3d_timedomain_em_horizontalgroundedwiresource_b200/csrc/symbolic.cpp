@@ -471,47 +471,98 @@ std::string analyse(int n, const int64_t* rowptr, const int* colind, const doubl
       sy.solve_items.push_back(s);
       sy.solve_items.push_back(b);
     };
-    // A unit of a level solve: front, row block (forward) or column block
-    // (backward), the block range [lo, hi) it accumulates, its partial-sum slot,
-    // the counter of its row and, for the final unit of a row, the number of
-    // partials to add.  Ranges are split into chunks of kSolveChunk blocks; the
-    // final unit takes the most recent dependency (the single block next to the
-    // diagonal) so the dependency chain advances by one block per link.
-    auto unit = [&](std::vector<int>& out, int s, int row, int lo, int hi, int slot, int cnt, int nparts,
-                    int fin) {
-      const int u[8] = {s, row, lo, hi, slot, cnt, nparts, fin};
-      out.insert(out.end(), u, u + 8);
+    // A unit of a level solve: row block (forward) or column block (backward) R of
+    // one front, the block range [lo, hi) it accumulates, its partial-sum slot, the
+    // counter of its row and, for the final unit of a row, the number of partials
+    // to add.  The final unit of a row takes the newest blocks (the ones next to
+    // the diagonal), the older ones are split into chunks of kSolveChunk blocks
+    // whose partial sums it adds; the dependency chain then advances by one block
+    // per link.  The record also carries the front's sizes and offsets, so a CTA
+    // needs one load per unit.
+    struct Cand {
+      int key, cls;
+      int rec[kUnitInts];
+    };
+    auto make = [&](std::vector<Cand>& out, int key, int cls, int s, int row, int lo, int hi, int slot, int cnt,
+                    int nparts, int fin) {
+      Cand c;
+      c.key = key;
+      c.cls = cls;
+      int* r = c.rec;
+      r[0] = row; r[1] = lo; r[2] = hi; r[3] = slot; r[4] = cnt; r[5] = nparts; r[6] = fin;
+      r[7] = sy.front_m[s]; r[8] = sy.front_k[s]; r[9] = (int)sy.flag_off[s];
+      const int64_t o64[3] = {sy.l_off[s], sy.wvec_off[s], sy.dinv_off[s]};
+      for (int j = 0; j < 3; ++j) {
+        r[10 + 2 * j] = (int)(uint32_t)(o64[j] & 0xffffffffu);
+        r[11 + 2 * j] = (int)(uint32_t)((uint64_t)o64[j] >> 32);
+      }
+      out.push_back(c);
+    };
+    // Ticket order: by key (when the unit's inputs start to appear along the
+    // dependency chain), final units before the others of the same key, then by
+    // row (forward) or last column first (backward).  Every unit a unit waits for
+    // must hold a smaller ticket; the replay below checks this for every launch.
+    auto emit = [&](std::vector<Cand>& v) {
+      std::stable_sort(v.begin(), v.end(), [](const Cand& a, const Cand& b) {
+        return a.key != b.key ? a.key < b.key : a.cls < b.cls;
+      });
+      for (const Cand& c : v) sy.solve_units.insert(sy.solve_units.end(), c.rec, c.rec + kUnitInts);
     };
     int64_t max_slots = 0;
+    if ((int64_t)sy.n_flags >= (int64_t)INT32_MAX) return "too many pivot blocks";
     for (int l = 0; l < nlev; ++l) {
       LevelPlan& lp = sy.levels[l];
+      std::vector<Cand> cand;
       // forward: row block R < pb (pivot rows, needs q < R) or R >= pb (update rows,
-      // needs q < pb)
+      // needs q < pb).  A pivot row is a link of the dependency chain: its final
+      // unit takes the newest kSolveLookahead + 1 blocks and is queued by the first
+      // of them, so it is running (streaming its blocks as their flags appear) well
+      // before the chain reaches it.  Chunks and update rows are queued by the last
+      // block they need.
       int rmax = 0;
       for (int s : lp.fronts)
         rmax = std::max(rmax, (int)(cdiv(sy.front_k[s], kPanel) + cdiv(sy.front_m[s] - sy.front_k[s], kPanel)));
-      lp.fwd_off = (int64_t)sy.solve_units.size() / 8;
+      lp.fwd_off = (int64_t)sy.solve_units.size() / kUnitInts;
       int64_t slots = 0;
       for (int R = 0; R < rmax; ++R)
         for (int s : lp.fronts) {
           const int pb = (int)cdiv(sy.front_k[s], kPanel), ub = (int)cdiv(sy.front_m[s] - sy.front_k[s], kPanel);
           if (R >= pb + ub) continue;
-          const int qmax = R < pb ? R : pb;
           const int cnt = (int)sy.n_counters++;
-          // short rows stay in one unit; long ones leave only the newest block to the final unit
-          const int nch = qmax - 1 > kSolveChunk ? (int)cdiv(qmax - 1, kSolveChunk) : 0;
-          for (int c = 0; c < nch; ++c)
-            unit(sy.solve_units, s, R, c * kSolveChunk, std::min(qmax - 1, (c + 1) * kSolveChunk), (int)(slots + c),
-                 cnt, 0, 0);
-          unit(sy.solve_units, s, R, nch > 0 ? qmax - 1 : 0, qmax, (int)slots, cnt, nch, 1);
-          slots += nch;
+          if (R < pb) {
+            const int lo = std::max(0, R - 1 - kSolveLookahead);
+            const int nch = (int)cdiv(lo, kSolveChunk);
+            for (int c = 0; c < nch; ++c) {
+              const int hi = std::min(lo, (c + 1) * kSolveChunk);
+              make(cand, hi - 1, 1, s, R, c * kSolveChunk, hi, (int)(slots + c), cnt, 0, 0);
+            }
+            make(cand, R == 0 ? -1 : lo, 0, s, R, lo, R, (int)slots, cnt, nch, 1);
+            slots += nch;
+          } else {
+            // short rows stay in one unit; long ones leave only the newest block to the final unit
+            const int nch = pb - 1 > kSolveChunk ? (int)cdiv(pb - 1, kSolveChunk) : 0;
+            for (int c = 0; c < nch; ++c) {
+              const int hi = std::min(pb - 1, (c + 1) * kSolveChunk);
+              make(cand, hi - 1, 1, s, R, c * kSolveChunk, hi, (int)(slots + c), cnt, 0, 0);
+            }
+            make(cand, pb - 1, 1, s, R, nch > 0 ? pb - 1 : 0, pb, (int)slots, cnt, nch, 1);
+            slots += nch;
+          }
         }
-      lp.fwd_count = (int64_t)sy.solve_units.size() / 8 - lp.fwd_off;
+      emit(cand);
+      lp.fwd_count = (int64_t)sy.solve_units.size() / kUnitInts - lp.fwd_off;
       max_slots = std::max(max_slots, slots);
-      // backward: column block p (last first) needs the row blocks R in (p, pb + ub)
+      // backward: column block p (last first) needs the row blocks R in (p, pb + ub).
+      // Flag R is set at step pb - 1 - R of the chain.  The final unit of column p
+      // takes rows [p + 1, p + 2 + kSolveLookahead) and is queued by the earliest
+      // flag among them; chunks (the rows beyond) are queued by their latest flag.
+      // Units that wait for no flag come first: an empty final unit at -2, chunks
+      // over update rows only at -1, a final unit over update rows only at 0 (after
+      // its chunks).
+      cand.clear();
       int pmax = 0;
       for (int s : lp.fronts) pmax = std::max(pmax, (int)cdiv(sy.front_k[s], kPanel));
-      lp.bwd_off = (int64_t)sy.solve_units.size() / 8;
+      lp.bwd_off = (int64_t)sy.solve_units.size() / kUnitInts;
       slots = 0;
       for (int d = 0; d < pmax; ++d)
         for (int s : lp.fronts) {
@@ -519,19 +570,44 @@ std::string analyse(int n, const int64_t* rowptr, const int* colind, const doubl
           if (d >= pb) continue;
           const int p = pb - 1 - d, rend = pb + ub;
           const int cnt = (int)sy.n_counters++;
-          const bool split = rend - (p + 2) > kSolveChunk;
-          const int first = split ? p + 2 : rend;
-          const int nch = split ? (int)cdiv(rend - first, kSolveChunk) : 0;
-          for (int c = 0; c < nch; ++c)
-            unit(sy.solve_units, s, p, first + c * kSolveChunk, std::min(rend, first + (c + 1) * kSolveChunk),
-                 (int)(slots + c), cnt, 0, 0);
-          unit(sy.solve_units, s, p, std::min(p + 1, rend), first, (int)slots, cnt, nch, 1);
+          const int lo = std::min(p + 1, rend), first = std::min(rend, p + 2 + kSolveLookahead);
+          const int nch = (int)cdiv(rend - first, kSolveChunk);
+          for (int c = 0; c < nch; ++c) {
+            const int clo = first + c * kSolveChunk, chi = std::min(rend, first + (c + 1) * kSolveChunk);
+            make(cand, clo < pb ? pb - 1 - clo : -1, 1, s, p, clo, chi, (int)(slots + c), cnt, 0, 0);
+          }
+          const int fkey = lo == first ? -2 : (lo < pb ? pb - std::min(first, pb) : 0);
+          make(cand, fkey, 0, s, p, lo, first, (int)slots, cnt, nch, 1);
           slots += nch;
         }
-      lp.bwd_count = (int64_t)sy.solve_units.size() / 8 - lp.bwd_off;
+      emit(cand);
+      lp.bwd_count = (int64_t)sy.solve_units.size() / kUnitInts - lp.bwd_off;
       max_slots = std::max(max_slots, slots);
     }
     sy.solve_slots = max_slots;
+    // Replay every launch's units in ticket order: each pivot-block flag and
+    // chunk counter a unit waits for must come from an earlier unit, otherwise
+    // CTAs holding early tickets could wait for units that never start.
+    {
+      std::vector<char> flag(sy.n_flags);
+      std::vector<int> done(sy.n_counters);
+      for (int dir = 0; dir < 2; ++dir)
+        for (const LevelPlan& lp : sy.levels) {
+          const int64_t off = dir ? lp.bwd_off : lp.fwd_off, cnt = dir ? lp.bwd_count : lp.fwd_count;
+          for (int64_t x = off; x < off + cnt; ++x) {
+            const int* u = &sy.solve_units[kUnitInts * x];
+            const int R = u[0], lo = u[1], hi = u[2], c = u[4], nparts = u[5], fin = u[6], f0 = u[9];
+            const int pb = (int)cdiv(u[8], kPanel);
+            if (hi - lo > kUnitBlocks) return "internal error: level-solve unit longer than kUnitBlocks";
+            for (int q = lo; q < std::min(hi, pb); ++q)
+              if (!flag[f0 + q]) return "internal error: level-solve unit waits for a later unit";
+            if (fin && done[c] != nparts) return "internal error: level-solve row finishes before its chunks";
+            if (!fin) ++done[c];
+            else if (dir == 1 || R < pb) flag[f0 + R] = 1;
+          }
+          if (dir == 0 && &lp == &sy.levels.back()) std::fill(flag.begin(), flag.end(), 0);
+        }
+    }
     sy.inv_off = (int64_t)sy.solve_items.size() / 2;
     for (int s = 0; s < nf; ++s)
       for (int b = 0; b < cdiv(sy.front_k[s], kPanel); ++b) push(s, b);

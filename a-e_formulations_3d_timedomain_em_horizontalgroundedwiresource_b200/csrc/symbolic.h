@@ -28,6 +28,10 @@ constexpr int kTileBig = 128;    // tile edge of the rank-kOuter trailing update
 constexpr int kTrsmRows = 128;   // rows per CTA of the panel triangular solve
 constexpr int kSolveRows = 256;  // rows per CTA of the solve updates
 constexpr int kSolveChunk = 8;   // 64 x 64 blocks accumulated by one level-solve unit
+constexpr int kUnitInts = 16;    // ints per level-solve unit record (64 bytes)
+constexpr int kSolveLookahead = 8;  // extra blocks a chain unit takes ahead of its newest one
+// most blocks one level-solve unit accumulates (a chain unit, or a short row)
+constexpr int kUnitBlocks = (kSolveLookahead + 1 > kSolveChunk + 1) ? kSolveLookahead + 1 : kSolveChunk + 1;
 
 struct FrontInfo {
   int c0 = 0, c1 = 0;      // pivot columns [c0, c1) (permuted numbering)
@@ -64,11 +68,10 @@ struct LevelPlan {
   std::vector<TaskList> extend_vec;    // solve extend-add per child slot, kSolveRows rows per CTA
   TaskList assemble;                   // solve: front-vector init, ceil(m / kSolveRows) CTAs each
   std::vector<PanelStep> panels;
-  // Level triangular solves: units (8 ints each, see Symbolic::solve_units) at
-  // solve_units[8 * off ...], one CTA per unit.  Forward units are ordered by row
-  // block then front, backward units by distance of the column block from the
-  // last one then front; within a row the chunk units come before its final unit,
-  // so every unit a CTA waits for has a smaller ticket.
+  // Level triangular solves: units (kUnitInts ints each, see Symbolic::solve_units)
+  // at solve_units[kUnitInts * off ...], taken by CTAs in list (ticket) order.
+  // Units are sorted by the last pivot block they wait for, so every unit a CTA
+  // waits for has a smaller ticket.
   int64_t fwd_off = 0, fwd_count = 0;
   int64_t bwd_off = 0, bwd_count = 0;
 };
@@ -98,8 +101,10 @@ struct Symbolic {
   std::vector<int64_t> task_prefix;  // concatenated CTA prefix sums
 
   std::vector<int> solve_items;      // (front, block) pairs of the diagonal-block inversions
-  // level-solve units: {front, row/column block, lo, hi, partial slot, row counter,
-  // partials to add (final unit), final flag}
+  // level-solve units, kUnitInts ints each: {row/column block, lo, hi, partial
+  // slot, row counter, partials to add (final unit), final flag, m, k, first
+  // pivot-block flag of the front, l_off, w_off, dinv_off (int64 as lo/hi ints)};
+  // w_off is also the front's offset into rows_all
   std::vector<int> solve_units;
   int64_t n_counters = 0;            // row counters over all levels and both directions
   int64_t solve_slots = 0;           // partial-sum slots (64 x nrhs each) of the largest level
