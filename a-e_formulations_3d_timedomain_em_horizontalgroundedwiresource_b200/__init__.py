@@ -75,6 +75,7 @@ class TdemInfo(ctypes.Structure):
         ("refine_iters", ctypes.c_int),
         ("refine_iters_max", ctypes.c_int),
         ("refine_worst", ctypes.c_double),
+        ("factor_slots", ctypes.c_int),
     ]
 
     def as_dict(self) -> dict:
@@ -88,6 +89,7 @@ class TdemOptions(ctypes.Structure):
         ("refine_maxit", ctypes.c_int),
         ("leaf_size", ctypes.c_int),
         ("fp32_update", ctypes.c_int),
+        ("factor_slots", ctypes.c_int),
     ]
 
 
@@ -237,14 +239,14 @@ class Solver:
 
     def __init__(self, workdir: str, formulation="A", scheme: int = 2, device: int = 0, precision: int = 64,
                  refine_tol: float = 1e-10, refine_maxit: int = 200, leaf_size: int = 128,
-                 fp32_update: str = "default"):
+                 fp32_update: str = "default", factor_slots: int = 0):
         self._lib = load_library()
         self._h = ctypes.c_void_p()
         engines = {"default": 0, "cuda_cores": 1, "tensor_cores": 2}
         if fp32_update not in engines:
             raise ValueError("fp32_update must be one of %s" % sorted(engines))
         opts = TdemOptions(int(precision), float(refine_tol), int(refine_maxit), int(leaf_size),
-                           engines[fp32_update])
+                           engines[fp32_update], int(factor_slots))
         st = self._lib.tdem_solver_create_ex(os.fsencode(workdir), _form(formulation), int(scheme), int(device),
                                              ctypes.byref(opts), ctypes.byref(self._h))
         if st != 0:
@@ -353,7 +355,7 @@ class Server:
 
     def submit(self, workdir: str, formulation="A", scheme: int = 2, precision: int = 64,
                write_outputs: bool = False) -> int:
-        opts = TdemOptions(int(precision), 1e-10, 200, 128, 0)
+        opts = TdemOptions(int(precision), 1e-10, 200, 128, 0, 0)
         rid = ctypes.c_int64(0)
         st = self._lib.tdem_server_submit(self._h, os.fsencode(workdir), _form(formulation), int(scheme),
                                           ctypes.byref(opts), int(bool(write_outputs)), ctypes.byref(rid))

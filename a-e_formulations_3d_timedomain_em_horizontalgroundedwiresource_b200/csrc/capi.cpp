@@ -77,6 +77,8 @@ tdem_status tdem_solver_create_ex(const char* workdir, int formulation, int sche
     if (opts->leaf_size > 0) opt.leaf_size = opts->leaf_size;
     if (opts->fp32_update < 0 || opts->fp32_update > 2) return TDEM_ERR_ARGUMENT;
     opt.fp32_update = opts->fp32_update;
+    if (opts->factor_slots < 0 || opts->factor_slots > 2) return TDEM_ERR_ARGUMENT;
+    opt.factor_slots = opts->factor_slots;
   }
   if (opt.precision != 64 && opt.precision != 32) return TDEM_ERR_ARGUMENT;
   s->precision = opt.precision;
@@ -153,6 +155,7 @@ tdem_status tdem_solver_info(const tdem_solver* s, tdem_info* info) {
   info->refine_iters = pt.refine_iters;
   info->refine_iters_max = pt.refine_iters_max;
   info->refine_worst = pt.refine_worst;
+  info->factor_slots = pt.factor_slots;
   if (m.n_edges > 0 && s->solve.n_interior() > 0) {
     const tdem::GpuCholesky& c = s->solve.cholesky();
     info->nnz_factor = c.symbolic().nnz_l;
@@ -207,6 +210,8 @@ tdem::RunOptions run_options(int formulation, int scheme, const tdem_options* op
     if (opts->leaf_size > 0) o.leaf_size = opts->leaf_size;
     o.fp32_update = opts->fp32_update;
   }
+  // the admission budget counts one factor slot unless two are asked for
+  o.factor_slots = (opts && opts->factor_slots) ? opts->factor_slots : 1;
   return o;
 }
 }  // namespace
@@ -234,6 +239,7 @@ tdem_status tdem_server_submit(tdem_server* srv, const char* workdir, int formul
   if ((formulation != 0 && formulation != 1) || (scheme != 2 && scheme != 3)) return TDEM_ERR_ARGUMENT;
   if (opts && (opts->precision != 0 && opts->precision != 32 && opts->precision != 64)) return TDEM_ERR_ARGUMENT;
   if (opts && (opts->fp32_update < 0 || opts->fp32_update > 2)) return TDEM_ERR_ARGUMENT;
+  if (opts && (opts->factor_slots < 0 || opts->factor_slots > 2)) return TDEM_ERR_ARGUMENT;
   *request_id = srv->srv.submit(workdir, run_options(formulation, scheme, opts), write_outputs != 0);
   return TDEM_OK;
 }

@@ -74,6 +74,8 @@ int find_time_layer(const std::vector<double>& time, double val) {
 TransientSolve::TransientSolve() = default;
 TransientSolve::~TransientSolve() {
   chol_.reset();
+  if (hs_) cudaStreamDestroy(hs_);
+  if (fs_) cudaStreamDestroy(fs_);
   for (cudaEvent_t& ev : ev_)
     if (ev) cudaEventDestroy(ev);
   for (void* p : allocs_) cudaFree(p);
@@ -236,7 +238,9 @@ std::string TransientSolve::plan(const std::string& dir, const RunOptions& opt) 
 int64_t TransientSolve::device_bytes_needed() const {
   if (!planned_ || !sy_) return 0;
   const int64_t nn = n_, np = npls_, nnz = (int64_t)col_.size(), nl = (int64_t)src_.size();
-  int64_t b = GpuCholesky::bytes_needed(*sy_, npls_, opt_.precision == 32 ? 4 : 8);
+  // two factor slots are counted only when asked for (0 adds one only if free memory allows)
+  const int slots = (opt_.precision == 64 && opt_.factor_slots == 2) ? 2 : 1;
+  int64_t b = GpuCholesky::bytes_needed(*sy_, npls_, opt_.precision == 32 ? 4 : 8, slots);
   b += 8 * (nn + 1) + 4 * nnz + 16 * nnz + 8 * nl + nl + 8 * nl + nn;  // pattern, C, B, map, diag, values, bound
   b += 8 * nn * np * (ring_ + 4);                                       // S, history ring, rhs, x, u0
   if (opt_.precision == 32) b += 8 * nnz + 8 * nn * np * 4;             // A and the CG vectors
@@ -253,10 +257,30 @@ std::string TransientSolve::setup_device(cudaStream_t stream) {
   std::string e;
   chol_.reset(new GpuCholesky());
   if (opt_.fp32_update != 0) chol_->set_tensor_core_update(opt_.fp32_update == 2);
-  e = chol_->setup(std::move(*sy_), p2v_, npls_, s_, opt_.precision == 32 ? 4 : 8);
+  // a second factor slot only for FP64 (the mixed-precision run keeps its FP64
+  // system values in one buffer that both the factorization and the CG use)
+  int slots = opt_.precision == 32 ? 1 : opt_.factor_slots;
+  if (slots == 0) {
+    size_t free_b = 0, total_b = 0;
+    TRY_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const int64_t need = device_bytes_needed() + GpuCholesky::slot_bytes(*sy_, 8);  // one slot counted
+    slots = ((int64_t)free_b > need + (int64_t)(total_b / 20) + ((int64_t)2 << 30)) ? 2 : 1;
+  }
+  if (slots < 1 || slots > kMaxSlots) return "factor_slots must be 0, 1 or 2";
+  pt_.factor_slots = slots;
+  {
+    int least = 0, greatest = 0;
+    TRY_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    TRY_CUDA(cudaStreamCreateWithPriority(&hs_, cudaStreamNonBlocking, greatest));
+    TRY_CUDA(cudaStreamCreateWithPriority(&fs_, cudaStreamNonBlocking, least));
+  }
+  e = chol_->setup(std::move(*sy_), p2v_, npls_, s_, opt_.precision == 32 ? 4 : 8, slots);
   sy_.reset();
   if (!e.empty()) return e;
   if (const char* ps = std::getenv("TDEM_PANEL_SOLVE")) chol_->set_panel_solve(ps[0] == '1');
+  // with a factorization running beside the steps, the level solves keep one CTA
+  // per SM so the factor kernels can share every SM
+  if (slots > 1) chol_->set_solve_ctas_per_sm(1);
   const RunOptions& opt = opt_;
 
   // device buffers
@@ -368,13 +392,13 @@ std::string TransientSolve::setup_device(cudaStream_t stream) {
   return "";
 }
 
-std::string TransientSolve::factor_with(double mult) {
-  launch_combine(d_C_, d_B_, d_src_, d_diag_, (int64_t)chol_->symbolic().nnz_lower, mult, d_avals_, s_);
+std::string TransientSolve::factor_with(double mult, int slot, cudaStream_t s) {
+  launch_combine(d_C_, d_B_, d_src_, d_diag_, (int64_t)chol_->symbolic().nnz_lower, mult, d_avals_, s);
   if (opt_.precision == 32) {
-    launch_combine_full(d_rowptr_, d_col_, d_C_, d_B_, d_bound_, n_, mult, d_A_, s_);
+    launch_combine_full(d_rowptr_, d_col_, d_C_, d_B_, d_bound_, n_, mult, d_A_, s);
     ++launches_;
   }
-  chol_->factor(d_avals_, s_);
+  chol_->factor(d_avals_, s, slot);
   launches_ += 1 + chol_->kernel_launches_factor();
   ++pt_.factorizations;
   return "";
@@ -387,7 +411,7 @@ std::string TransientSolve::step(int itime, int t1, int t2, double m1, double m2
   const double* u2 = (t2 >= 0) ? layer(t2) : layer(t1);
   launch_history_rhs(d_rowptr_, d_col_, d_C_, u1, u2, m1, (t2 >= 0) ? m2 : 0.0, d_S_, coef, d_bound_, n_, npls_,
                      d_rhs_, s_);
-  std::string e = (opt_.precision == 32) ? refine(d_x_) : chol_->solve_graph(d_rhs_, d_x_, n_, npls_, s_);
+  std::string e = (opt_.precision == 32) ? refine(d_x_) : chol_->solve_graph(d_rhs_, d_x_, n_, npls_, s_, slot_);
   if (!e.empty()) return e;
   TRY_CUDA(cudaMemcpyAsync(layer(itime), d_x_, sizeof(double) * (size_t)n_ * npls_, cudaMemcpyDeviceToDevice, s_));
   launches_ += 1 + chol_->kernel_launches_solve();
@@ -470,6 +494,24 @@ std::string TransientSolve::run() {
   pt_.refine_worst = 0.0;
   pt_.factor_gpu_ms = pt_.solve_gpu_ms = pt_.run_gpu_ms = 0;
   launches_ = 0;
+  // Everything runs on the high-priority stream hs_ (factorizations ahead of use
+  // on fs_), ordered after the caller's stream and joined back into it at the end.
+  cudaStream_t caller = s_;
+  TRY_CUDA(cudaEventRecord(ev_[2], caller));
+  TRY_CUDA(cudaStreamWaitEvent(hs_, ev_[2], 0));
+  TRY_CUDA(cudaStreamWaitEvent(fs_, ev_[2], 0));
+  s_ = hs_;
+  struct Restore {
+    TransientSolve* ts;
+    cudaStream_t caller;
+    ~Restore() {
+      cudaEventRecord(ts->ev_[3], ts->hs_);
+      cudaEventRecord(ts->ev_[4], ts->fs_);
+      cudaStreamWaitEvent(caller, ts->ev_[3], 0);
+      cudaStreamWaitEvent(caller, ts->ev_[4], 0);
+      ts->s_ = caller;
+    }
+  } restore{this, caller};
   TRY_CUDA(cudaEventRecord(ev_[0], s_));
   TRY_CUDA(cudaMemcpyAsync(layer(0), d_u0_, sizeof(double) * u0_.size(), cudaMemcpyDeviceToDevice, s_));
   dec_ig_ = decade_starts(t);
@@ -477,138 +519,212 @@ std::string TransientSolve::run() {
   vpre1_.assign(ntime_, -1);
   vpre2_.assign(ntime_, -1);
   std::string e;
-  double tf = 0.0;
-  // factorizations are bracketed by events on the launching stream; their device
-  // time is accumulated once the run has finished
-  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> fev;
-  auto timed_factor = [&](double mult) {
-    cudaEvent_t a, b;
-    cudaEventCreate(&a);
-    cudaEventCreate(&b);
-    cudaEventRecord(a, s_);
-    const double h0 = now_s();
-    factor_with(mult);
-    cudaEventRecord(b, s_);
-    tf += now_s() - h0;
-    fev.push_back({a, b});
-  };
   auto check = [&]() -> std::string {
     if (opt_.cancel && *opt_.cancel) return "cancelled";
     return "";
   };
-  int tn = 0, tn1 = 0, tn2 = 0;
-  if (opt_.scheme == 2) {
-    eval_receivers(0);
-    for (int d = 0; d < ndec; ++d) {
-      const int tbeg = dec_ig_[d], tend = dec_ig_[d + 1];
-      int npre1 = -1, npre2 = -1;
-      if (d > 0) {
-        if (tbeg + 1 >= ntime_) return "last decade has a single step";
-        const double h = t[tbeg + 1] - t[tbeg];
-        npre1 = find_time_layer(t, t[tbeg] - h);
-        npre2 = find_time_layer(t, t[tbeg] - 2 * h);
-        if (npre1 < 0 || npre2 < 0) return "restart layers of a decade not on the time grid";
+
+  // The decades: `use(mult)` is called where a factorization with multiplier
+  // mult starts to be needed, `stepf(...)` for every time step, `recv(it)` for
+  // every stored layer.  A dry walk (no steps) lists the multipliers first, so
+  // every factorization is known before the first step runs.
+  auto walk = [&](auto&& use, auto&& stepf, auto&& recv) -> std::string {
+    int tn = 0, tn1 = 0, tn2 = 0;
+    if (opt_.scheme == 2) {
+      recv(0);
+      for (int d = 0; d < ndec; ++d) {
+        const int tbeg = dec_ig_[d], tend = dec_ig_[d + 1];
+        int npre1 = -1, npre2 = -1;
+        if (d > 0) {
+          if (tbeg + 1 >= ntime_) return "last decade has a single step";
+          const double h = t[tbeg + 1] - t[tbeg];
+          npre1 = find_time_layer(t, t[tbeg] - h);
+          npre2 = find_time_layer(t, t[tbeg] - 2 * h);
+          if (npre1 < 0 || npre2 < 0) return "restart layers of a decade not on the time grid";
+        }
+        bool first = true;
+        double mult = 0.0;
+        for (int it = std::max(tbeg, 1); it < tend; ++it) {
+          if (first && it > 1) {
+            tn2 = npre2;
+            tn1 = npre1;
+            tn = it;
+          } else {
+            tn2 = tn1;
+            tn1 = tn;
+            tn = it;
+          }
+          vpre1_[it] = tn1;
+          vpre2_[it] = tn2;
+          if (first) {
+            mult = 1.0 / (t[it] - t[tn1]);
+            std::string ue = use(mult);
+            if (!ue.empty()) return ue;
+            first = false;
+          }
+          std::string se = stepf(it, tn1, tn2, mult, 0.0, source_coef(it, false, 0.0));
+          if (!se.empty()) return se;
+          recv(it);
+        }
       }
-      bool first = true;
-      double mult = 0.0;
-      for (int it = std::max(tbeg, 1); it < tend; ++it) {
-        if (!(e = check()).empty()) return e;
-        if (first && it > 1) {
-          tn2 = npre2;
-          tn1 = npre1;
-          tn = it;
-        } else {
-          tn2 = tn1;
-          tn1 = tn;
-          tn = it;
+    } else {
+      for (int d = 0; d < ndec; ++d) {
+        const int tbeg = dec_ig_[d], tend = dec_ig_[d + 1];
+        int npre1 = -1, npre2 = -1;
+        if (d > 0) {
+          if (tbeg + 1 >= ntime_) return "last decade has a single step";
+          const double h = t[tbeg + 1] - t[tbeg];
+          npre1 = find_time_layer(t, t[tbeg] - h);
+          npre2 = find_time_layer(t, t[tbeg] - 2 * h);
+          if (npre1 < 0 || npre2 < 0) return "restart layers of a decade not on the time grid";
         }
-        vpre1_[it] = tn1;
-        vpre2_[it] = tn2;
-        if (first) {
-          mult = 1.0 / (t[it] - t[tn1]);
-          timed_factor(mult);
-          first = false;
+        if (1 >= tbeg && 1 < tend) {
+          // two backward-Euler steps with the first step length (Two_Layers_Schema)
+          if (tend < 3) return "first decade shorter than the two start-up steps";
+          const double dt = t[1] - t[0];
+          std::string ue = use(1.0 / dt);
+          if (!ue.empty()) return ue;
+          for (int it = 1; it < 3; ++it) {
+            vpre1_[it] = it - 1;
+            vpre2_[it] = it - 2;
+            std::string se = stepf(it, it - 1, -1, 1.0 / dt, 0.0, source_coef(it, true, dt));
+            if (!se.empty()) return se;
+            if (it == 2) recv(2);
+          }
+          tn2 = 0;
+          tn1 = 1;
+          tn = 2;
         }
-        if (!(e = step(it, tn1, tn2, mult, 0.0, source_coef(it, false, 0.0))).empty()) return e;
-        eval_receivers(it);
+        bool first = true;
+        double mult = 0, m1 = 0, m2 = 0;
+        for (int it = std::max(tbeg, 3); it < tend; ++it) {
+          if (first && it != 3) {
+            tn2 = npre2;
+            tn1 = npre1;
+            tn = it;
+          } else {
+            tn2 = tn1;
+            tn1 = tn;
+            tn = it;
+          }
+          vpre1_[it] = tn1;
+          vpre2_[it] = tn2;
+          if (first) {
+            const double dt = t[it] - t[tn2], dt0 = t[it] - t[tn1], dt1 = t[tn1] - t[tn2];
+            mult = (dt + dt0) / (dt * dt0);
+            m1 = dt / (dt1 * dt0);
+            m2 = -dt0 / (dt * dt1);
+            std::string ue = use(mult);
+            if (!ue.empty()) return ue;
+            first = false;
+          }
+          std::string se = stepf(it, tn1, tn2, m1, m2, source_coef(it, false, 0.0));
+          if (!se.empty()) return se;
+          recv(it);
+        }
       }
     }
-  } else {
-    for (int d = 0; d < ndec; ++d) {
-      const int tbeg = dec_ig_[d], tend = dec_ig_[d + 1];
-      int npre1 = -1, npre2 = -1;
-      if (d > 0) {
-        if (tbeg + 1 >= ntime_) return "last decade has a single step";
-        const double h = t[tbeg + 1] - t[tbeg];
-        npre1 = find_time_layer(t, t[tbeg] - h);
-        npre2 = find_time_layer(t, t[tbeg] - 2 * h);
-        if (npre1 < 0 || npre2 < 0) return "restart layers of a decade not on the time grid";
-      }
-      if (1 >= tbeg && 1 < tend) {
-        // two backward-Euler steps with the first step length (Two_Layers_Schema)
-        if (tend < 3) return "first decade shorter than the two start-up steps";
-        const double dt = t[1] - t[0];
-        timed_factor(1.0 / dt);
-        for (int it = 1; it < 3; ++it) {
-          if (!(e = check()).empty()) return e;
-          vpre1_[it] = it - 1;
-          vpre2_[it] = it - 2;
-          if (!(e = step(it, it - 1, -1, 1.0 / dt, 0.0, source_coef(it, true, dt))).empty()) return e;
-          if (it == 2) eval_receivers(2);
-        }
-        tn2 = 0;
-        tn1 = 1;
-        tn = 2;
-      }
-      bool first = true;
-      double mult = 0, m1 = 0, m2 = 0;
-      for (int it = std::max(tbeg, 3); it < tend; ++it) {
-        if (!(e = check()).empty()) return e;
-        if (first && it != 3) {
-          tn2 = npre2;
-          tn1 = npre1;
-          tn = it;
-        } else {
-          tn2 = tn1;
-          tn1 = tn;
-          tn = it;
-        }
-        vpre1_[it] = tn1;
-        vpre2_[it] = tn2;
-        if (first) {
-          const double dt = t[it] - t[tn2], dt0 = t[it] - t[tn1], dt1 = t[tn1] - t[tn2];
-          mult = (dt + dt0) / (dt * dt0);
-          m1 = dt / (dt1 * dt0);
-          m2 = -dt0 / (dt * dt1);
-          timed_factor(mult);
-          first = false;
-        }
-        if (!(e = step(it, tn1, tn2, m1, m2, source_coef(it, false, 0.0))).empty()) return e;
-        eval_receivers(it);
-      }
+    return "";
+  };
+
+  std::vector<double> mults;
+  auto no_step = [&](int, int, int, double, double, double) { return std::string(); };
+  e = walk([&](double mult) { mults.push_back(mult); return std::string(); }, no_step, [](int) {});
+  if (!e.empty()) return e;
+
+  const int nslots = chol_->slots();
+  const int nf = (int)mults.size();
+  // factorization f goes to slot f % nslots; its device time is bracketed by events
+  std::vector<cudaEvent_t> fev(2 * (size_t)nf, nullptr), dev_span;
+  struct EventPool {
+    std::vector<cudaEvent_t>* a;
+    std::vector<cudaEvent_t>* b;
+    ~EventPool() {
+      for (auto* v : {a, b})
+        for (cudaEvent_t ev : *v)
+          if (ev) cudaEventDestroy(ev);
     }
-  }
+  } pool{&fev, &dev_span};
+  for (cudaEvent_t& ev : fev) TRY_CUDA(cudaEventCreate(&ev));
+  // with one slot a factorization runs on hs_ between the decades; with two it
+  // runs on fs_ as soon as the steps that used its slot have been issued
+  auto enqueue_factor = [&](int f) -> std::string {
+    cudaStream_t fst = nslots > 1 ? fs_ : s_;
+    if (nslots > 1 && f >= nslots) {
+      // the slot was last used by the steps issued so far on hs_
+      TRY_CUDA(cudaEventRecord(ev_[5], s_));
+      TRY_CUDA(cudaStreamWaitEvent(fst, ev_[5], 0));
+    }
+    TRY_CUDA(cudaEventRecord(fev[2 * f], fst));
+    factor_with(mults[f], f % nslots, fst);
+    TRY_CUDA(cudaEventRecord(fev[2 * f + 1], fst));
+    return "";
+  };
+  int nextf = 0;   // next factorization to be used by the steps
+  int queued = 0;  // factorizations enqueued so far
+  if (nslots > 1)
+    while (queued < std::min(nf, nslots - 1)) {
+      if (!(e = enqueue_factor(queued)).empty()) return e;
+      ++queued;
+    }
+  auto span_mark = [&]() -> std::string {
+    cudaEvent_t ev;
+    TRY_CUDA(cudaEventCreate(&ev));
+    dev_span.push_back(ev);
+    TRY_CUDA(cudaEventRecord(ev, s_));
+    return "";
+  };
+  auto use = [&](double) -> std::string {
+    std::string ue;
+    if (!dev_span.empty() && dev_span.size() % 2 == 1 && !(ue = span_mark()).empty()) return ue;  // decade end
+    const int f = nextf++;
+    if (nslots == 1) {
+      if (!(ue = enqueue_factor(f)).empty()) return ue;
+      ++queued;
+    } else {
+      // keep nslots - 1 factorizations ahead: the one after f reuses the slot of f - 1
+      while (queued < std::min(nf, f + nslots)) {
+        if (!(ue = enqueue_factor(queued)).empty()) return ue;
+        ++queued;
+      }
+      TRY_CUDA(cudaStreamWaitEvent(s_, fev[2 * f + 1], 0));
+    }
+    slot_ = f % nslots;
+    return span_mark();  // decade start
+  };
+  auto stepf = [&](int it, int t1, int t2, double m1, double m2, double coef) -> std::string {
+    std::string ce = check();
+    if (!ce.empty()) return ce;
+    return step(it, t1, t2, m1, m2, coef);
+  };
+  e = walk(use, stepf, [&](int it) { eval_receivers(it); });
+  if (!e.empty()) return e;
+  if (dev_span.size() % 2 == 1 && !(e = span_mark()).empty()) return e;
+  // join the factor stream (nothing is left on it once every factor was used)
+  TRY_CUDA(cudaEventRecord(ev_[5], fs_));
+  TRY_CUDA(cudaStreamWaitEvent(s_, ev_[5], 0));
   TRY_CUDA(cudaEventRecord(ev_[1], s_));
   TRY_CUDA(cudaStreamSynchronize(s_));
   TRY_CUDA(cudaGetLastError());
   float ms = 0.f;
   cudaEventElapsedTime(&ms, ev_[0], ev_[1]);
   pt_.run_gpu_ms = ms;
-  for (auto& pr : fev) {
-    cudaEventElapsedTime(&ms, pr.first, pr.second);
+  for (int f = 0; f < nf; ++f) {
+    cudaEventElapsedTime(&ms, fev[2 * f], fev[2 * f + 1]);
     pt_.factor_gpu_ms += ms;
-    cudaEventDestroy(pr.first);
-    cudaEventDestroy(pr.second);
   }
-  pt_.solve_gpu_ms = pt_.run_gpu_ms - pt_.factor_gpu_ms;
+  for (size_t k = 0; k + 1 < dev_span.size(); k += 2) {
+    cudaEventElapsedTime(&ms, dev_span[k], dev_span[k + 1]);
+    pt_.solve_gpu_ms += ms;
+  }
   const int bad = chol_->status(s_);
   if (bad) return "factorization met a non-positive pivot at column " + std::to_string(bad);
   if (const int ss = chol_->solve_status(s_))
     return ss == 1 ? "CUDA: a wait of the level triangular solves gave up"
                    : "CUDA: a wait of the tensor-core update gave up";
   pt_.factor_s = pt_.factor_gpu_ms * 1e-3;
-  pt_.steps_s = now_s() - tstart - pt_.factor_s;
-  (void)tf;
+  pt_.steps_s = pt_.solve_gpu_ms * 1e-3;
+  (void)tstart;
   return "";
 }
 

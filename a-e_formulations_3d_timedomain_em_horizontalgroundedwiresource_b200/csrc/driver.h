@@ -27,14 +27,21 @@ struct RunOptions {
   int precision = 64;
   double refine_tol = 1e-10;
   int refine_maxit = 200;
+  // Numeric factors held on the device (precision 64): 2 factors the next time
+  // step size on a low-priority stream while the current decade's steps run on a
+  // high-priority one; 1 runs them in turn; 0 chooses 2 when free device memory
+  // holds the second factor with room to spare.  Results are the same either way.
+  int factor_slots = 0;
   const volatile int* cancel = nullptr;  // checked between time steps when set
 };
 
 struct PhaseTimes {
   double setup_s = 0, assemble_s = 0, factor_s = 0, steps_s = 0, output_s = 0;
   // device time of the last run() from CUDA events on the solver's stream
+  // (factor_gpu_ms sums the factorizations, solve_gpu_ms the time-step spans;
+  // with two factor slots they overlap and may add up to more than run_gpu_ms)
   double run_gpu_ms = 0, factor_gpu_ms = 0, solve_gpu_ms = 0;
-  int factorizations = 0, steps = 0;
+  int factorizations = 0, steps = 0, factor_slots = 1;
   int64_t h2d_bytes = 0, d2h_bytes = 0;   // host<->device traffic of prepare/run/results
   int refine_iters = 0, refine_iters_max = 0;  // CG iterations of the last run (mixed precision)
   double refine_worst = 0.0;              // largest final relative residual of the last run
@@ -77,6 +84,9 @@ class TransientSolve {
   RunOptions opt_;
   cudaStream_t s_ = nullptr;
   std::unique_ptr<GpuCholesky> chol_;
+  cudaStream_t hs_ = nullptr;  // time steps during run() (highest priority)
+  cudaStream_t fs_ = nullptr;  // factorizations ahead of use (lowest priority)
+  int slot_ = 0;               // factor slot the time steps use
   // host results of plan() consumed by setup_device()
   bool planned_ = false;
   std::unique_ptr<Symbolic> sy_;
@@ -131,7 +141,7 @@ class TransientSolve {
   template <class T>
   std::string upload(T** d, const std::vector<T>& h);
   double* layer(int t) { return d_hist_ + (int64_t)(t % ring_) * n_ * npls_; }
-  std::string factor_with(double mult);
+  std::string factor_with(double mult, int slot, cudaStream_t s);
   std::string step(int itime, int t1, int t2, double m1, double m2, double coef);
   void eval_receivers(int t);
   double source_coef(int itime, bool two_layer, double dt) const;

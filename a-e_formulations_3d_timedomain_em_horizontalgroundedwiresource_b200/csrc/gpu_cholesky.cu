@@ -1023,29 +1023,20 @@ __device__ __forceinline__ void warp_wait_count(const int* c, int target, int* e
   __syncwarp();
 }
 
-// Waits (whole warp) until flags[lo .. hi) are all set, hi - lo <= 32: lane j
-// polls flag lo + j.  The polls back off to sleep_max ns, so units queued early
-// (bulk work waiting for the dependency chain) keep the L2 slice that holds the
-// flags free for the chain itself.  Bounded like wait_flag.
-__device__ __forceinline__ void warp_wait_range(const int* flags, int lo, int hi, int* err, int lane,
-                                                unsigned sleep_max) {
-  if (lo >= hi) return;
-  // every lane takes the same branch: lane 0's view of the error flag decides
-  if (__shfl_sync(0xffffffffu, *(volatile int*)err, 0) == 0) {
-    unsigned ns = 32;
-    unsigned it = 0;
-    for (; it < kSpinLimit; ++it) {
-      const int v = (lo + lane < hi) ? ld_acquire(flags + lo + lane) : 1;
-      if (__all_sync(0xffffffffu, v != 0)) break;
-      __nanosleep(ns);
-      ns = min(2 * ns, sleep_max);
-    }
-    if (it == kSpinLimit && lane == 0) atomicExch(err, 1);
+// One thread waits for *flag like wait_flag, but the polls back off to
+// sleep_max ns: units queued early (bulk work waiting for the dependency chain)
+// then keep the L2 slice that holds the flags free for the chain itself.
+__device__ void wait_flag_backoff(const int* flag, int* err, unsigned sleep_max) {
+  if (*(volatile int*)err != 0) return;
+  unsigned ns = 32;
+  for (unsigned it = 0; it < kSpinLimit; ++it) {
+    if (ld_acquire(flag) != 0) return;
+    __nanosleep(ns);
+    ns = min(2 * ns, sleep_max);
   }
-  __syncwarp();
+  atomicExch(err, 1);
 }
 
-static_assert(kUnitBlocks <= 32, "one lane per flag");
 
 // Dynamic shared memory of the streaming kernels: kStages block buffers and the
 // inverted diagonal block, 64 x 64 entries each.
@@ -1063,8 +1054,8 @@ __global__ void __launch_bounds__(256, 2) k_fwd_stream(const T* __restrict__ L, 
   T* dsm = stage + kStages * SB * SB;          // inverted diagonal block, 4096
   __shared__ T red[4][SB][NR];  // per column group: partial row sums
   __shared__ T zs[SB][NR];      // pivot rows: w - sum, the input of the inverse
-  __shared__ T ys[kUnitBlocks][SB][NR];  // bulk units: y of every block of the unit
-  __shared__ int s_tk[2];
+  __shared__ T ys[kUnitBlocks][SB][NR];  // y of every block of the unit (when staged)
+  __shared__ int s_tk[2], s_ready;
   const int t = threadIdx.x, i = t & 63, g = t >> 6, lane = t & 31;
   if (t == 0) s_tk[0] = atomicAdd(fa.ticket, 1);
   __syncthreads();
@@ -1114,12 +1105,24 @@ __global__ void __launch_bounds__(256, 2) k_fwd_stream(const T* __restrict__ L, 
             if (r < nr_rhs) tot[r] += __ldcg(my_part + (int64_t)c * SB * nr_rhs + i + SB * r);
       }
     };
-    // A chain unit (final unit of a pivot row) takes its blocks as their flags
-    // appear.  Any other unit normally finds all its flags set: it waits for them
-    // together and stages the y of all its blocks with one barrier.
+    // The flags of a front are set in chain order (the unit that sets flag q has
+    // waited for flag q - 1), so the newest flag of the range stands for all of
+    // them.  A unit other than a chain unit (final unit of a pivot row) waits for
+    // it on one thread and stages the y of all its blocks with one barrier; a
+    // chain unit checks it once and, unless it is set, takes its blocks as their
+    // flags appear.
     const bool chain = fin && piv;
-    if (!chain) {
-      warp_wait_range(flags, lo, hi, fa.err, lane, 2048);
+    if (t == 0) {
+      int ready = 1;
+      if (lo < hi) {
+        if (!chain) wait_flag_backoff(flags + hi - 1, fa.err, 1024);
+        else ready = ld_acquire(flags + hi - 1) != 0;
+      }
+      s_ready = ready;
+    }
+    __syncthreads();
+    const bool staged = s_ready != 0;
+    if (staged && lo < hi) {
       for (int e = t; e < (hi - lo) * SB * NR; e += 256) {
         const int b = e / (SB * NR), c = (e / NR) % SB, r = e % NR;
         const int q = lo + b;
@@ -1132,7 +1135,7 @@ __global__ void __launch_bounds__(256, 2) k_fwd_stream(const T* __restrict__ L, 
       const int slot = (q - lo) % kStages;
       if (q == hi - 1) gather();
       const T* blk = stage + slot * SB * SB + t;
-      if (chain) {
+      if (!staged) {
         warp_wait_flag(flags + q, fa.err, lane);
         const int wq = min(SB, k - SB * q), c = g + 4 * (lane & 15);
         T yv[NR];
@@ -1231,8 +1234,8 @@ __global__ void __launch_bounds__(256, 2) k_bwd_stream(const T* __restrict__ L, 
   T* dsm = stage + kStages * SB * SB;
   __shared__ T red[2][SB][NR];  // per row half: column sums
   __shared__ T zs[SB][NR];      // y_p - sum, the input of the inverse
-  __shared__ T xs[kUnitBlocks][SB][NR];  // chunks: x of every row block of the unit
-  __shared__ int s_tk[2];
+  __shared__ T xs[kUnitBlocks][SB][NR];  // x of the row blocks of the unit (when staged)
+  __shared__ int s_tk[2], s_ready;
   const int t = threadIdx.x, i = t & 63, g = t >> 6, lane = t & 31, half = (t >> 5) & 1;
   // column of the warp-reduced value this lane holds
   const int cl = g + 4 * ((lane >> 1) & 15);
@@ -1292,16 +1295,28 @@ __global__ void __launch_bounds__(256, 2) k_bwd_stream(const T* __restrict__ L, 
             if (r < nr_rhs) tot[r] += __ldcg(my_part + (int64_t)c * SB * nr_rhs + t + SB * r);
       }
     };
-    // The final unit (a link of the chain) takes its row blocks as their flags
-    // appear; a chunk waits for all its flags together and stages x of all its
-    // row blocks with one barrier.
-    if (!fin) {
-      warp_wait_range(flags, lo, min(hi, pb), fa.err, lane, 2048);
-      for (int e = t; e < (hi - lo) * SB * NR; e += 256) {
+    // Flags are set in chain order (last column first), so flag lo stands for
+    // every pivot row block of the range.  A chunk waits for it on one thread and
+    // stages x of all its row blocks with one barrier; the final unit (a link of
+    // the chain) checks it once and, unless it is set, stages only the update
+    // rows (no flag) and takes the pivot row blocks as their flags appear.
+    if (t == 0) {
+      int ready = 1;
+      if (lo < hi && lo < pb) {
+        if (!fin) wait_flag_backoff(flags + lo, fa.err, 1024);
+        else ready = ld_acquire(flags + lo) != 0;
+      }
+      s_ready = ready;
+    }
+    __syncthreads();
+    const bool staged = s_ready != 0;
+    const int sfirst = staged ? lo : max(lo, pb);  // first staged row block
+    if (sfirst < hi) {
+      for (int e = t; e < (hi - sfirst) * SB * NR; e += 256) {
         const int b = e / (SB * NR), ii = (e / NR) % SB, r = e % NR;
         int r0, nr;
-        rows_of(lo + b, r0, nr);
-        xs[b][ii][r] = (r < nr_rhs && ii < nr) ? __ldcg(w + r0 + ii + (int64_t)r * m) : (T)0;
+        rows_of(sfirst + b, r0, nr);
+        xs[sfirst - lo + b][ii][r] = (r < nr_rhs && ii < nr) ? __ldcg(w + r0 + ii + (int64_t)r * m) : (T)0;
       }
       __syncthreads();
     }
@@ -1312,8 +1327,8 @@ __global__ void __launch_bounds__(256, 2) k_bwd_stream(const T* __restrict__ L, 
       rows_of(R, r0, nr);
       if (R == lo) gather();
       T xv[NR];
-      if (fin) {
-        if (R < pb) warp_wait_flag(flags + R, fa.err, lane);
+      if (R < sfirst) {
+        warp_wait_flag(flags + R, fa.err, lane);
 #pragma unroll
         for (int r = 0; r < NR; ++r) xv[r] = (r < nr_rhs && i < nr) ? __ldcg(w + r0 + i + (int64_t)r * m) : (T)0;
       } else {
@@ -1652,8 +1667,8 @@ int launch_solve_fused(const Symbolic& sy, const T* L, const T* Dinv, T* W, T* p
 
 // Resident CTAs on the device of each streaming kernel ([NR = 1, 2][forward, backward]).
 template <class T>
-std::string stream_residency(int (&resident)[2][2]) {
-  int dev = 0, sms = 0;
+std::string stream_residency(int (&resident)[2][2], int& sms) {
+  int dev = 0;
   TDEM_CUDA_TRY(cudaGetDevice(&dev));
   TDEM_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   const int sm = (int)stream_smem<T>();
@@ -1693,7 +1708,8 @@ std::string set_fused_attributes() {
 }  // namespace
 
 GpuCholesky::~GpuCholesky() {
-  if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+  for (SolveGraph& g : graph_)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
   for (void* p : allocs_) cudaFree(p);
 }
 
@@ -1716,10 +1732,15 @@ std::string GpuCholesky::upload(T** dst, const std::vector<T>& src, cudaStream_t
   return "";
 }
 
-int64_t GpuCholesky::bytes_needed(const Symbolic& sy, int nrhs_max, int precision_bytes) {
+int64_t GpuCholesky::slot_bytes(const Symbolic& sy, int precision_bytes) {
+  const int64_t el = (precision_bytes == 4) ? 4 : 8;
+  return el * (std::max<int64_t>(1, sy.nnz_l) + std::max<int64_t>(1, sy.dinv_elems));
+}
+
+int64_t GpuCholesky::bytes_needed(const Symbolic& sy, int nrhs_max, int precision_bytes, int nslots) {
   const int64_t el = (precision_bytes == 4) ? 4 : 8, nr = std::max(1, nrhs_max);
-  int64_t b = el * (sy.nnz_l + sy.u_elems + sy.wvec_elems * nr + sy.solve_partials * nr + sy.dinv_elems +
-                    sy.solve_slots * kPanel * nr);
+  int64_t b = el * (sy.u_elems + sy.wvec_elems * nr + sy.solve_partials * nr + sy.solve_slots * kPanel * nr);
+  b += std::max(1, std::min(nslots, kMaxSlots)) * slot_bytes(sy, precision_bytes);
   b += 8 * (int64_t)(sy.l_off.size() + sy.u_off.size() + sy.wvec_off.size() + sy.entry_dst.size() +
                      sy.rel_off.size() + sy.rows_off.size() + sy.task_prefix.size() + sy.flag_off.size() +
                      sy.dinv_off.size());
@@ -1730,14 +1751,19 @@ int64_t GpuCholesky::bytes_needed(const Symbolic& sy, int nrhs_max, int precisio
 }
 
 std::string GpuCholesky::setup(Symbolic&& sy, const std::vector<int>& perm_to_vec, int nrhs_max,
-                               cudaStream_t s, int precision_bytes) {
+                               cudaStream_t s, int precision_bytes, int nslots) {
   sy_ = std::move(sy);
   nrhs_max_ = std::max(1, nrhs_max);
   elem_ = (precision_bytes == 4) ? 4 : 8;
   if ((int)perm_to_vec.size() != sy_.n) return "perm_to_vec size mismatch";
   if (nrhs_max_ > kMaxRhs) return "too many right-hand sides";
+  if (nslots < 1 || nslots > kMaxSlots) return "factor slots must be 1 or 2";
+  nslots_ = nslots;
   std::string e;
-  if (!(e = alloc(&d_L_, elem_ * std::max<int64_t>(1, sy_.nnz_l))).empty()) return e;
+  for (int k = 0; k < nslots_; ++k) {
+    if (!(e = alloc(&d_L_[k], elem_ * std::max<int64_t>(1, sy_.nnz_l))).empty()) return e;
+    if (!(e = alloc(&d_dinv_[k], elem_ * std::max<int64_t>(1, sy_.dinv_elems))).empty()) return e;
+  }
   if (!(e = alloc(&d_U_, elem_ * std::max<int64_t>(1, sy_.u_elems))).empty()) return e;
   if (!(e = alloc(&d_W_, elem_ * std::max<int64_t>(1, sy_.wvec_elems) * nrhs_max_)).empty()) return e;
   if (!(e = alloc(&d_part_, elem_ * std::max<int64_t>(1, sy_.solve_partials) * nrhs_max_)).empty()) return e;
@@ -1762,7 +1788,6 @@ std::string GpuCholesky::setup(Symbolic&& sy, const std::vector<int>& perm_to_ve
   if (!(e = upload(&d_items_, sy_.solve_items, s)).empty()) return e;
   if (!(e = upload(&d_flag_off_, sy_.flag_off, s)).empty()) return e;
   if (!(e = upload(&d_dinv_off_, sy_.dinv_off, s)).empty()) return e;
-  if (!(e = alloc(&d_dinv_, elem_ * std::max<int64_t>(1, sy_.dinv_elems))).empty()) return e;
   if (!(e = upload(&d_units_, sy_.solve_units, s)).empty()) return e;
   if (!(e = alloc(&d_spart_, elem_ * std::max<int64_t>(1, sy_.solve_slots) * kPanel * nrhs_max_)).empty()) return e;
   if (!(e = alloc((void**)&d_sync_,
@@ -1773,73 +1798,85 @@ std::string GpuCholesky::setup(Symbolic&& sy, const std::vector<int>& perm_to_ve
   if (elem_ == 4 && tc_update_ && !(e = tc_update_setup()).empty()) return e;
   if (!(e = (elem_ == 4 ? set_attributes<float>() : set_attributes<double>())).empty()) return e;
   if (!(e = (elem_ == 4 ? set_fused_attributes<float>() : set_fused_attributes<double>())).empty()) return e;
-  if (!(e = (elem_ == 4 ? stream_residency<float>(resident_) : stream_residency<double>(resident_))).empty()) return e;
+  if (!(e = (elem_ == 4 ? stream_residency<float>(resident_, sms_) : stream_residency<double>(resident_, sms_)))
+           .empty())
+    return e;
   TDEM_CUDA_TRY(cudaStreamSynchronize(s));
   return "";
 }
 
-void GpuCholesky::factor(const double* d_vals, cudaStream_t s) {
+void GpuCholesky::factor(const double* d_vals, cudaStream_t s, int slot) {
   Fronts fr{d_l_off_, d_u_off_, d_m_, d_k_};
   const unsigned ni = (unsigned)sy_.inv_count;
   const size_t ism = 2 * sizeof(double) * SB * (SB + 1);
+  void* Lp = d_L_[slot];
+  void* Dp = d_dinv_[slot];
   if (elem_ == 4) {
-    launches_factor_ = launch_factor<float>(sy_, (float*)d_L_, (float*)d_U_, d_vals, d_entry_, fr, d_parent_,
+    launches_factor_ = launch_factor<float>(sy_, (float*)Lp, (float*)d_U_, d_vals, d_entry_, fr, d_parent_,
                                             d_rel_off_, d_rel_, d_tasks_, d_prefix_, d_err_, d_c0_, tc_update_, s);
-    if (ni) k_diag_inverse<float><<<ni, 256, ism, s>>>((const float*)d_L_, (float*)d_dinv_, fr, d_dinv_off_,
+    if (ni) k_diag_inverse<float><<<ni, 256, ism, s>>>((const float*)Lp, (float*)Dp, fr, d_dinv_off_,
                                                        d_items_ + 2 * sy_.inv_off);
   } else {
-    launches_factor_ = launch_factor<double>(sy_, (double*)d_L_, (double*)d_U_, d_vals, d_entry_, fr, d_parent_,
+    launches_factor_ = launch_factor<double>(sy_, (double*)Lp, (double*)d_U_, d_vals, d_entry_, fr, d_parent_,
                                              d_rel_off_, d_rel_, d_tasks_, d_prefix_, d_err_, d_c0_, false, s);
-    if (ni) k_diag_inverse<double><<<ni, 256, ism, s>>>((const double*)d_L_, (double*)d_dinv_, fr, d_dinv_off_,
+    if (ni) k_diag_inverse<double><<<ni, 256, ism, s>>>((const double*)Lp, (double*)Dp, fr, d_dinv_off_,
                                                         d_items_ + 2 * sy_.inv_off);
   }
   if (ni) ++launches_factor_;
 }
 
-void GpuCholesky::solve(const double* d_b, double* d_x, int64_t ld, int nrhs, cudaStream_t s) {
+void GpuCholesky::solve(const double* d_b, double* d_x, int64_t ld, int nrhs, cudaStream_t s, int slot) {
   SolveArgs a{d_l_off_, d_w_off_, d_m_, d_k_, d_rows_off_, d_rows_, nrhs, ld};
+  const void* Lp = d_L_[slot];
+  const void* Dp = d_dinv_[slot];
   if (!panel_solve_) {
     FusedArgs fa{d_units_, 0, nullptr, nullptr, nullptr, d_err_ + 1};
+    int res[2][2];
+    for (int j = 0; j < 2; ++j)
+      for (int d = 0; d < 2; ++d)
+        res[j][d] = solve_ctas_cap_ > 0 ? std::min(resident_[j][d], solve_ctas_cap_ * sms_) : resident_[j][d];
     if (elem_ == 4)
-      launches_solve_ = launch_solve_fused<float>(sy_, (const float*)d_L_, (const float*)d_dinv_, (float*)d_W_,
+      launches_solve_ = launch_solve_fused<float>(sy_, (const float*)Lp, (const float*)Dp, (float*)d_W_,
                                                   (float*)d_spart_, d_b, d_x, a, d_parent_, d_rel_off_, d_rel_,
-                                                  d_tasks_, d_prefix_, fa, d_sync_, resident_, s);
+                                                  d_tasks_, d_prefix_, fa, d_sync_, res, s);
     else
-      launches_solve_ = launch_solve_fused<double>(sy_, (const double*)d_L_, (const double*)d_dinv_, (double*)d_W_,
+      launches_solve_ = launch_solve_fused<double>(sy_, (const double*)Lp, (const double*)Dp, (double*)d_W_,
                                                    (double*)d_spart_, d_b, d_x, a, d_parent_, d_rel_off_, d_rel_,
-                                                   d_tasks_, d_prefix_, fa, d_sync_, resident_, s);
+                                                   d_tasks_, d_prefix_, fa, d_sync_, res, s);
     return;
   }
   if (elem_ == 4)
-    launches_solve_ = launch_solve<float>(sy_, (const float*)d_L_, (float*)d_W_, (float*)d_part_, d_b, d_x, a,
+    launches_solve_ = launch_solve<float>(sy_, (const float*)Lp, (float*)d_W_, (float*)d_part_, d_b, d_x, a,
                                           d_parent_, d_rel_off_, d_rel_, d_tasks_, d_prefix_, s);
   else
-    launches_solve_ = launch_solve<double>(sy_, (const double*)d_L_, (double*)d_W_, (double*)d_part_, d_b, d_x, a,
+    launches_solve_ = launch_solve<double>(sy_, (const double*)Lp, (double*)d_W_, (double*)d_part_, d_b, d_x, a,
                                            d_parent_, d_rel_off_, d_rel_, d_tasks_, d_prefix_, s);
 }
 
-std::string GpuCholesky::solve_graph(const double* d_b, double* d_x, int64_t ld, int nrhs, cudaStream_t s) {
-  if (!graph_exec_ || g_b_ != d_b || g_x_ != d_x || g_ld_ != ld || g_nrhs_ != nrhs) {
-    if (graph_exec_) {
-      cudaGraphExecDestroy(graph_exec_);
-      graph_exec_ = nullptr;
+std::string GpuCholesky::solve_graph(const double* d_b, double* d_x, int64_t ld, int nrhs, cudaStream_t s,
+                                     int slot) {
+  SolveGraph& sg = graph_[slot];
+  if (!sg.exec || sg.b != d_b || sg.x != d_x || sg.ld != ld || sg.nrhs != nrhs) {
+    if (sg.exec) {
+      cudaGraphExecDestroy(sg.exec);
+      sg.exec = nullptr;
     }
     cudaGraph_t g = nullptr;
     TDEM_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    solve(d_b, d_x, ld, nrhs, s);
+    solve(d_b, d_x, ld, nrhs, s, slot);
     TDEM_CUDA_TRY(cudaStreamEndCapture(s, &g));
-    const cudaError_t ie = cudaGraphInstantiate(&graph_exec_, g, 0);
+    const cudaError_t ie = cudaGraphInstantiate(&sg.exec, g, 0);
     cudaGraphDestroy(g);
     if (ie != cudaSuccess) {
-      graph_exec_ = nullptr;
+      sg.exec = nullptr;
       return std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ie);
     }
-    g_b_ = d_b;
-    g_x_ = d_x;
-    g_ld_ = ld;
-    g_nrhs_ = nrhs;
+    sg.b = d_b;
+    sg.x = d_x;
+    sg.ld = ld;
+    sg.nrhs = nrhs;
   }
-  TDEM_CUDA_TRY(cudaGraphLaunch(graph_exec_, s));
+  TDEM_CUDA_TRY(cudaGraphLaunch(sg.exec, s));
   return "";
 }
 

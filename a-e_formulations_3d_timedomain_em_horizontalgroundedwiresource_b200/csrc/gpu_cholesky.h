@@ -16,7 +16,8 @@
 
 namespace tdem {
 
-constexpr int kMaxRhs = 64;  // right-hand sides per solve
+constexpr int kMaxRhs = 64;    // right-hand sides per solve
+constexpr int kMaxSlots = 2;   // numeric factors held at once (one factored while the other solves)
 
 class GpuCholesky {
  public:
@@ -28,25 +29,34 @@ class GpuCholesky {
   // Takes ownership of the analysis and allocates device memory for nrhs_max
   // right-hand sides.  perm_to_vec[p] is the position in the caller's vectors of
   // permuted unknown p (lets the solve read and write the caller's natural-order
-  // vectors directly).
+  // vectors directly).  nslots numeric factors (1 or 2) are held: with two, one
+  // can be factored (on its own stream) while solves use the other.
   std::string setup(Symbolic&& sy, const std::vector<int>& perm_to_vec, int nrhs_max,
-                    cudaStream_t stream, int precision_bytes = 8);
+                    cudaStream_t stream, int precision_bytes = 8, int nslots = 1);
 
   // Device bytes setup() allocates for this analysis (factor, workspaces, plans).
-  static int64_t bytes_needed(const Symbolic& sy, int nrhs_max, int precision_bytes);
+  static int64_t bytes_needed(const Symbolic& sy, int nrhs_max, int precision_bytes, int nslots = 1);
+  // Device bytes of one numeric factor slot (factor entries + inverted diagonal blocks).
+  static int64_t slot_bytes(const Symbolic& sy, int precision_bytes);
+  int slots() const { return nslots_; }
 
-  // Numeric factorization.  d_lower_vals holds the lower-CSR values of the
-  // analysed pattern (device, nnz_lower doubles).  Errors (non-positive pivot)
-  // are reported through status() after the stream is synchronised.
-  void factor(const double* d_lower_vals, cudaStream_t stream);
+  // Numeric factorization into factor slot `slot`.  d_lower_vals holds the
+  // lower-CSR values of the analysed pattern (device, nnz_lower doubles).
+  // Errors (non-positive pivot) are reported through status() after the stream
+  // is synchronised.  Factorizations share one update workspace: they must not
+  // run concurrently with each other (solves may).
+  void factor(const double* d_lower_vals, cudaStream_t stream, int slot = 0);
 
-  // x = A^-1 b for nrhs columns.  b and x are device arrays with leading
-  // dimension ld (positions given by perm_to_vec); x rows not covered by the
-  // system are left untouched.  b and x may alias.
-  void solve(const double* d_b, double* d_x, int64_t ld, int nrhs, cudaStream_t stream);
+  // x = A^-1 b for nrhs columns with the factor in `slot`.  b and x are device
+  // arrays with leading dimension ld (positions given by perm_to_vec); x rows
+  // not covered by the system are left untouched.  b and x may alias.  Solves
+  // share their work vectors: they must not run concurrently with each other.
+  void solve(const double* d_b, double* d_x, int64_t ld, int nrhs, cudaStream_t stream, int slot = 0);
   // Same as solve(), replayed from a CUDA graph captured on first use for these
-  // buffers (the factor values may change between calls; the pointers may not).
-  std::string solve_graph(const double* d_b, double* d_x, int64_t ld, int nrhs, cudaStream_t stream);
+  // buffers and slot (the factor values may change between calls; the pointers
+  // may not).
+  std::string solve_graph(const double* d_b, double* d_x, int64_t ld, int nrhs, cudaStream_t stream,
+                          int slot = 0);
   int precision_bytes() const { return elem_; }
 
   // 0 = ok, otherwise 1-based permuted column of the first non-positive pivot.
@@ -60,6 +70,10 @@ class GpuCholesky {
   // Selects the per-panel solve (one launch per 64-column panel and level) instead
   // of the fused level solves; both compute the same triangular solves.
   void set_panel_solve(bool on) { panel_solve_ = on; }
+  // Caps the persistent level-solve kernels at this many CTAs per SM (0 = as many
+  // as fit): with one, half of every SM stays free for a factorization running
+  // beside the solves.  Takes effect for solves captured or launched afterwards.
+  void set_solve_ctas_per_sm(int n) { solve_ctas_cap_ = n; }
 
   const Symbolic& symbolic() const { return sy_; }
   size_t device_bytes() const { return bytes_; }
@@ -72,16 +86,22 @@ class GpuCholesky {
   size_t bytes_ = 0;
   int launches_factor_ = 0, launches_solve_ = 0;
   int elem_ = 8;                 // bytes per factor entry (8 = FP64, 4 = FP32)
+  int nslots_ = 1;
   bool panel_solve_ = false;
   bool tc_update_ = false;
   int resident_[2][2] = {};      // resident CTAs of the streaming level solves [NR 1, 2][fwd, bwd]
-  cudaGraphExec_t graph_exec_ = nullptr;
-  const double* g_b_ = nullptr;
-  double* g_x_ = nullptr;
-  int64_t g_ld_ = 0;
-  int g_nrhs_ = 0;
+  int sms_ = 0;                  // SMs of the device
+  int solve_ctas_cap_ = 0;       // CTAs per SM of the level solves (0 = occupancy limit)
+  struct SolveGraph {
+    cudaGraphExec_t exec = nullptr;
+    const double* b = nullptr;
+    double* x = nullptr;
+    int64_t ld = 0;
+    int nrhs = 0;
+  };
+  SolveGraph graph_[kMaxSlots];
   // device arrays
-  void* d_L_ = nullptr;
+  void* d_L_[kMaxSlots] = {};    // factor entries per slot
   void* d_U_ = nullptr;
   void* d_W_ = nullptr;          // solve front vectors (sum m) x nrhs_max
   void* d_part_ = nullptr;       // backward partial sums
@@ -104,7 +124,7 @@ class GpuCholesky {
   int* d_items_ = nullptr;       // solve / inversion items (front, block)
   int64_t* d_flag_off_ = nullptr;
   int64_t* d_dinv_off_ = nullptr;
-  void* d_dinv_ = nullptr;       // inverted diagonal blocks
+  void* d_dinv_[kMaxSlots] = {};  // inverted diagonal blocks per slot
   int* d_sync_ = nullptr;        // level tickets + pivot-block flags + row counters of one solve
   int* d_units_ = nullptr;       // level-solve units
   void* d_spart_ = nullptr;      // level-solve partial sums (slots x 64 x nrhs)

@@ -300,7 +300,7 @@ def run_ours(args, world, rank, local):
     try:
         wdir = os.path.join(base, "model")
         spec, form, scheme, desc, winfo = write_workload(args.config, wdir, args.air_sigma)
-        sopts = dict(precision=args.precision, fp32_update=args.fp32_update)
+        sopts = dict(precision=args.precision, fp32_update=args.fp32_update, factor_slots=args.factor_slots)
         solver = pkg.Solver(wdir, form, scheme, device=local, **sopts)
         # one run solves every transmitter position of the model (one RHS column each)
         per_run = solver.info()["n_sources"]
@@ -404,7 +404,10 @@ def run_ours(args, world, rank, local):
                            "factorizations_per_solve": n_fact, "steps_per_solve": steps_per_run,
                            "parallelism": "replicas x%d" % world, "precision": ("FP64 factor + FP64 solves" if args.precision == 64 else
                                          "FP32 factor (%s) + FP64 CG to 1e-10 relative residual" % args.fp32_update),
-                           "l2": "inputs larger than L2 (factor %.1f GB)" % (8e-9 * inf["nnz_factor"])},
+                           "l2": "inputs larger than L2 (factor %.1f GB)" % (8e-9 * inf["nnz_factor"]),
+                           "factor_slots": inf["factor_slots"],
+                           "overlap": ("factorization k+1 runs beside the time steps of decade k (phase times "
+                                       "overlap)") if inf["factor_slots"] > 1 else "none"},
                 "latency_ms": {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
                 "phase_ms_per_solve": {"factor": factor_ms / units, "steps": solve_ms / units},
                 "wall_s": wall,
@@ -497,6 +500,8 @@ def main():
     ap.add_argument("--precision", type=int, default=64, choices=[64, 32],
                     help="64: FP64 factor; 32: FP32 factor preconditioning FP64 CG")
     ap.add_argument("--fp32-update", default="default", choices=["default", "cuda_cores", "tensor_cores"])
+    ap.add_argument("--factor-slots", type=int, default=0, choices=[0, 1, 2],
+                    help="numeric factors held: 2 overlaps the next factorization with the steps, 0 = auto")
     ap.add_argument("--air-sigma", type=float, default=None,
                     help="conductivity of the air cells (default 1e-8 S/m as the reference's mesh builder)")
     args = ap.parse_args()

@@ -89,6 +89,8 @@ typedef struct tdem_info {
   int refine_iters;         /* conjugate-gradient iterations of the last run (precision 32) */
   int refine_iters_max;     /* most iterations any time step needed */
   double refine_worst;      /* largest final relative residual of any step / column */
+  int factor_slots;         /* numeric factors held (2: factorizations overlapped the steps;
+                               factor_gpu_ms and solve_gpu_ms then overlap in run_gpu_ms) */
 } tdem_info;
 
 /* Options of tdem_solver_create_ex (zero-initialise, then set what differs). */
@@ -102,6 +104,11 @@ typedef struct tdem_options {
   int fp32_update;          /* precision 32, rank-256 trailing updates of the factorization:
                                0 = library default, 1 = CUDA cores (FP32 FMA),
                                2 = tensor cores (tcgen05, 3xTF32 with FP32 accumulation) */
+  int factor_slots;         /* precision 64: numeric factors held on the device.  2 factors the
+                               next time-step size on a low-priority stream while the current
+                               decade's steps run (same results, a second factor's memory);
+                               1 factors between the decades; 0 (default) = 2 when free device
+                               memory holds it with room to spare.  The server treats 0 as 1. */
 } tdem_options;
 
 /* Creates a solver for the model in `workdir` (reads the input files, analyses

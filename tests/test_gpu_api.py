@@ -129,3 +129,33 @@ def test_pardiso_gpu_not_positive_definite(pkg):
     h = np.zeros(64, dtype=np.int64)
     assert pkg.pardiso_64(h, 12, a, ia, ja) == -4
     pkg.pardiso_64(h, -1, a, ia, ja)
+
+
+@pytest.mark.parametrize("form,scheme", [("A", 3), ("E", 2)])
+def test_factor_ahead_matches_sequential_bitwise(pkg, golden, tmp_path, form, scheme):
+    """Two factor slots (the next factorization overlapped with the current
+    decade's steps on a second stream) give bit-identical transients."""
+    d = str(tmp_path / "m")
+    golden.write_case_inputs("cube8_block", d)
+    out = {}
+    for slots in (1, 2):
+        with pkg.Solver(d, form, scheme, factor_slots=slots) as s:
+            s.run()
+            out[slots] = s.results()
+            info = s.info()
+            assert info["factor_slots"] == slots
+            assert info["factorizations"] >= 2
+            s.run()
+            again = s.results()
+        for a, b in zip(out[slots], again):
+            assert np.array_equal(a, b)
+    for a, b in zip(out[1], out[2]):
+        assert np.array_equal(a, b)
+
+
+def test_factor_slots_out_of_range_is_rejected(pkg, golden, tmp_path):
+    d = str(tmp_path / "m")
+    golden.write_case_inputs("cube6", d)
+    with pytest.raises(pkg.TdemError) as ei:
+        pkg.Solver(d, "A", 2, factor_slots=3)
+    assert ei.value.status == 1
