@@ -246,60 +246,107 @@ __global__ void __launch_bounds__(256) k_syrk_panel(T* __restrict__ L, Fronts f,
 }
 
 // Trailing update at the end of an outer panel: F[J1:m, J1:m] -= X X^T with X the
-// outer panel rows [J1, m), columns [J0, J1).  128 x 128 tiles, 256 threads with
-// 8 x 8 outputs each, K consumed in chunks of 32.
+// outer panel rows [J1, m), columns [J0, J1).  The task list counts 128 x 128
+// lower-triangle tiles; each is done by two CTAs of 128 threads (column halves of
+// 64), two CTAs per SM, so one CTA's operand loads and read-modify-write of its
+// tile overlap the other's FMAs.  A CTA streams K in chunks of KC through two
+// shared-memory buffers filled by cp.async (the next chunk lands while the
+// current one is consumed); each thread keeps an 8 x 8 block of the tile in
+// registers (rows tx + 16 a, columns ty + 8 b).
 constexpr int KC = 32;
+constexpr int kBigThreads = 128;
+constexpr int kBigCols = 64;  // columns per CTA (half a 128 x 128 tile)
+
+// cp.async of one element (4 or 8 bytes); src_bytes = 0 stores a zero instead.
+template <int BYTES>
+__device__ __forceinline__ void cp_async_elem(void* dst, const void* src, int src_bytes) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(d), "l"(src), "n"(BYTES), "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 template <class T>
-__global__ void __launch_bounds__(256) k_syrk_big(T* __restrict__ L, T* __restrict__ U, Fronts f,
-                                                  const int* __restrict__ fronts,
-                                                  const int64_t* __restrict__ prefix, int count, int j0) {
-  constexpr int TB = kTileBig;
+__global__ void __launch_bounds__(kBigThreads, 2) k_syrk_big(T* __restrict__ L, T* __restrict__ U, Fronts f,
+                                                              const int* __restrict__ fronts,
+                                                              const int64_t* __restrict__ prefix, int count, int j0) {
+  constexpr int TB = kTileBig, TC = kBigCols;
   extern __shared__ __align__(16) unsigned char sm_raw[];
-  T(*As)[TB + 1] = reinterpret_cast<T(*)[TB + 1]>(sm_raw);
-  T(*Bs)[TB + 1] = reinterpret_cast<T(*)[TB + 1]>(sm_raw + sizeof(T) * KC * (TB + 1));
-  const int idx = find_task(prefix, count, blockIdx.x);
+  // buffer s: As[s][p][i] (KC x TB), then Bs[s][p][j] (KC x TC)
+  T* sbuf = reinterpret_cast<T*>(sm_raw);
+  const int idx = find_task(prefix, count, blockIdx.x >> 1);
   const int s = fronts[idx];
   const int m = f.m[s], k = f.k[s];
   const int J0 = (j0 / kOuter) * kOuter, J1 = min(k, J0 + kOuter);
   const int64_t lo = f.l_off[s], uo = f.u_off[s];
   const T* F = L + lo;
-  const int64_t t = blockIdx.x - prefix[idx];
+  const int64_t t = (blockIdx.x >> 1) - prefix[idx];
   int bi = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
   while ((int64_t)(bi + 1) * (bi + 2) / 2 <= t) ++bi;
   while ((int64_t)bi * (bi + 1) / 2 > t) --bi;
   const int bj = (int)(t - (int64_t)bi * (bi + 1) / 2);
-  const int r0 = J1 + bi * TB, c0 = J1 + bj * TB;
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int r0 = J1 + bi * TB, c0 = J1 + bj * TB + (blockIdx.x & 1) * TC;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  // the upper half of a diagonal tile's right column half is above the diagonal
+  if (c0 >= m || (bi == bj && (blockIdx.x & 1) && r0 + TB <= c0)) return;
+  const int K = J1 - J0, nch = (K + KC - 1) / KC;
+  // thread tid copies rows tid of A (all KC columns) and rows tid % 64 of B
+  // (columns tid / 64 + 2 j): coalesced 256-byte rows per warp
+  const bool arow = r0 + tid < m;
+  const int bi_row = tid & (TC - 1), bp0 = tid >> 6;
+  const bool brow = c0 + bi_row < m;
+  auto load_chunk = [&](int ch, int buf) {
+    T* As = sbuf + (size_t)buf * KC * (TB + TC);
+    T* Bs = As + KC * TB;
+    const int k0 = ch * KC, kc = min(KC, K - k0);
+#pragma unroll 8
+    for (int p = 0; p < KC; ++p) {
+      const bool ok = arow && p < kc;
+      const T* src = ok ? F + (r0 + tid) + (int64_t)(J0 + k0 + p) * m : F;
+      cp_async_elem<(int)sizeof(T)>(As + p * TB + tid, src, ok ? (int)sizeof(T) : 0);
+    }
+#pragma unroll 8
+    for (int j = 0; j < KC / 2; ++j) {
+      const int p = bp0 + 2 * j;
+      const bool ok = brow && p < kc;
+      const T* src = ok ? F + (c0 + bi_row) + (int64_t)(J0 + k0 + p) * m : F;
+      cp_async_elem<(int)sizeof(T)>(Bs + p * TC + bi_row, src, ok ? (int)sizeof(T) : 0);
+    }
+  };
   T acc[8][8];
 #pragma unroll
   for (int a = 0; a < 8; ++a)
 #pragma unroll
     for (int b = 0; b < 8; ++b) acc[a][b] = (T)0;
-  const int K = J1 - J0;
-  for (int k0 = 0; k0 < K; k0 += KC) {
-    const int kc = min(KC, K - k0);
-    for (int q = threadIdx.x; q < TB * KC; q += blockDim.x) {
-      const int i = q % TB, p = q / TB;
-      const bool okp = p < kc;
-      const int64_t col = (int64_t)(J0 + k0 + p) * m;
-      As[p][i] = (okp && r0 + i < m) ? F[(r0 + i) + col] : (T)0;
-      Bs[p][i] = (okp && c0 + i < m) ? F[(c0 + i) + col] : (T)0;
-    }
+  load_chunk(0, 0);
+  cp_async_commit();
+  for (int ch = 0; ch < nch; ++ch) {
+    if (ch + 1 < nch) load_chunk(ch + 1, (ch + 1) & 1);
+    cp_async_commit();
+    cp_async_wait<1>();
     __syncthreads();
+    const T* As = sbuf + (size_t)(ch & 1) * KC * (TB + TC);
+    const T* Bs = As + KC * TB;
+    const int kc = min(KC, K - ch * KC);
 #pragma unroll 4
     for (int p = 0; p < kc; ++p) {
       T av[8], bv[8];
 #pragma unroll
-      for (int a = 0; a < 8; ++a) av[a] = As[p][tx + 16 * a];
+      for (int a = 0; a < 8; ++a) av[a] = As[p * TB + tx + 16 * a];
 #pragma unroll
-      for (int b = 0; b < 8; ++b) bv[b] = Bs[p][ty + 16 * b];
+      for (int b = 0; b < 8; ++b) bv[b] = Bs[p * TC + ty + 8 * b];
 #pragma unroll
       for (int a = 0; a < 8; ++a)
 #pragma unroll
         for (int b = 0; b < 8; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
     }
+    // the buffer is refilled by the next iteration's copies
     __syncthreads();
   }
+  cp_async_wait_all();
   // per output row: the 8 loads first, then the 8 stores (the element pointers may
   // alias as far as the compiler knows, which would serialise load-store pairs)
 #pragma unroll
@@ -309,12 +356,12 @@ __global__ void __launch_bounds__(256) k_syrk_big(T* __restrict__ L, T* __restri
     T old[8];
 #pragma unroll
     for (int b = 0; b < 8; ++b) {
-      const int c = c0 + ty + 16 * b;
+      const int c = c0 + ty + 8 * b;
       old[b] = (c < m && c <= r) ? *felem(L, U, lo, uo, m, k, r, c) : (T)0;
     }
 #pragma unroll
     for (int b = 0; b < 8; ++b) {
-      const int c = c0 + ty + 16 * b;
+      const int c = c0 + ty + 8 * b;
       if (c < m && c <= r) *felem(L, U, lo, uo, m, k, r, c) = old[b] - acc[a][b];
     }
   }
@@ -955,18 +1002,6 @@ __global__ void __launch_bounds__(256, 2) k_bwd_level(const T* __restrict__ L, c
 // ---------------------------------------------------------------------------
 constexpr int kStages = 2;
 
-// cp.async of one element (4 or 8 bytes); src_bytes = 0 stores a zero instead.
-template <int BYTES>
-__device__ __forceinline__ void cp_async_elem(void* dst, const void* src, int src_bytes) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(d), "l"(src), "n"(BYTES), "r"(src_bytes)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
-
 // This thread's 16 elements (row t % 64, columns t / 64 + 4 e) of the 64 x 64
 // block at rows [r0, r0 + nr), columns [c0, c0 + nc) of F (zero outside) into
 // buf[e * 256 + t].  Does not commit.
@@ -1463,7 +1498,7 @@ constexpr size_t trsm_smem() { return sizeof(T) * (P + kTrsmRows) * (P + 1); }
 template <class T>
 constexpr size_t syrk_smem() { return sizeof(T) * 2 * kTileSyrk * (P + 1); }
 template <class T>
-constexpr size_t big_smem() { return sizeof(T) * 2 * KC * (kTileBig + 1); }
+constexpr size_t big_smem() { return sizeof(T) * 2 * KC * (kTileBig + kBigCols); }
 
 template <class T>
 std::string set_attributes() {
@@ -1521,7 +1556,7 @@ int launch_factor(const Symbolic& sy, T* L, T* U, const double* vals, const int6
           launch_syrk_tc((float*)L, (float*)U, fr.l_off, fr.u_off, fr.m, fr.k, tasks + ps.syrk_big.off,
                          prefix + ps.syrk_big.pre, ps.syrk_big.count, ps.syrk_big.ctas, ps.j0, err, s);
         else
-          k_syrk_big<T><<<grid_of(ps.syrk_big.ctas), 256, big_smem<T>(), s>>>(
+          k_syrk_big<T><<<grid_of(2 * ps.syrk_big.ctas), kBigThreads, big_smem<T>(), s>>>(
               L, U, fr, tasks + ps.syrk_big.off, prefix + ps.syrk_big.pre, ps.syrk_big.count, ps.j0);
         ++launches;
       }

@@ -313,7 +313,9 @@ std::string analyse(int n, const int64_t* rowptr, const int* colind, const doubl
     roff += m;
     sy.nnz_l += m * k;
     const double dm = (double)m, dk = (double)k;
-    sy.flops += 2.0 * (dk * dk * dk / 3.0 + (dm - dk) * dk * dk + (dm - dk) * (dm - dk) * dk);
+    // k^3/3 (pivot block) + r k^2 (panel solve) + r^2 k (lower-triangle Schur update),
+    // r = m - k, a multiply-add counted as two flops
+    sy.flops += dk * dk * dk / 3.0 + (dm - dk) * dk * dk + (dm - dk) * (dm - dk) * dk;
     sy.max_m = std::max(sy.max_m, (int)m);
     sy.max_k = std::max(sy.max_k, (int)k);
   }
