@@ -367,6 +367,142 @@ __global__ void __launch_bounds__(kBigThreads, 2) k_syrk_big(T* __restrict__ L, 
   }
 }
 
+// FP64 trailing update on the FP64 tensor pipe (mma.sync m16n8k16 .f64): same
+// task list, tile split (two 128-thread CTAs per 128 x 128 tile, two CTAs per SM)
+// and cp.async double buffering as k_syrk_big, but each warp owns a 64 x 32 block
+// of its CTA's 128 x 64 tile as 4 x 4 MMA tiles, so one instruction does 2,048
+// multiply-adds instead of 32 and the issue slots stay free for the loads.
+// Shared layouts are k-major with the row (column) stride padded to 8 mod 16
+// doubles: a fragment load of 8 rows x 4 k then spans all 32 banks twice.
+constexpr int kLdA = kTileBig + 8;   // 136
+constexpr int kLdB = kBigCols + 8;   // 72
+constexpr int kLdC = kTileBig + 4;   // epilogue tile columns (fits in the operand buffers)
+static_assert(kBigCols * kLdC <= 2 * KC * (kLdA + kLdB), "epilogue tile must fit the operand buffers");
+
+__device__ __forceinline__ void dmma16816(double (&c)[4], const double (&a)[8], const double (&b)[4]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
+      "{%12,%13,%14,%15}, {%0,%1,%2,%3};"
+      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]), "d"(b[0]),
+        "d"(b[1]), "d"(b[2]), "d"(b[3]));
+}
+
+__global__ void __launch_bounds__(kBigThreads, 2) k_syrk_big_dmma(double* __restrict__ L, double* __restrict__ U,
+                                                                   Fronts f, const int* __restrict__ fronts,
+                                                                   const int64_t* __restrict__ prefix, int count,
+                                                                   int j0) {
+  constexpr int TB = kTileBig, TC = kBigCols;
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  double* sbuf = reinterpret_cast<double*>(sm_raw);  // buffer s: As (KC x kLdA) then Bs (KC x kLdB)
+  const int idx = find_task(prefix, count, blockIdx.x >> 1);
+  const int s = fronts[idx];
+  const int m = f.m[s], k = f.k[s];
+  const int J0 = (j0 / kOuter) * kOuter, J1 = min(k, J0 + kOuter);
+  const int64_t lo = f.l_off[s], uo = f.u_off[s];
+  const double* F = L + lo;
+  const int64_t t = (blockIdx.x >> 1) - prefix[idx];
+  int bi = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+  while ((int64_t)(bi + 1) * (bi + 2) / 2 <= t) ++bi;
+  while ((int64_t)bi * (bi + 1) / 2 > t) --bi;
+  const int bj = (int)(t - (int64_t)bi * (bi + 1) / 2);
+  const int r0 = J1 + bi * TB, c0 = J1 + bj * TB + (blockIdx.x & 1) * TC;
+  if (c0 >= m) return;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, q = lane & 3;
+  const int wr = (warp >> 1) * 64, wc = (warp & 1) * 32;  // warp block within the CTA tile
+  const int K = J1 - J0, nch = (K + KC - 1) / KC;
+  const bool arow = r0 + tid < m;
+  const int bi_row = tid & (TC - 1), bp0 = tid >> 6;
+  const bool brow = c0 + bi_row < m;
+  constexpr int kBuf = KC * (kLdA + kLdB);
+  auto load_chunk = [&](int ch, int buf) {
+    double* As = sbuf + buf * kBuf;
+    double* Bs = As + KC * kLdA;
+    const int k0 = ch * KC, kc = min(KC, K - k0);
+#pragma unroll 8
+    for (int p = 0; p < KC; ++p) {
+      const bool ok = arow && p < kc;
+      const double* src = ok ? F + (r0 + tid) + (int64_t)(J0 + k0 + p) * m : F;
+      cp_async_elem<8>(As + p * kLdA + tid, src, ok ? 8 : 0);
+    }
+#pragma unroll 8
+    for (int j = 0; j < KC / 2; ++j) {
+      const int p = bp0 + 2 * j;
+      const bool ok = brow && p < kc;
+      const double* src = ok ? F + (c0 + bi_row) + (int64_t)(J0 + k0 + p) * m : F;
+      cp_async_elem<8>(Bs + p * kLdB + bi_row, src, ok ? 8 : 0);
+    }
+  };
+  double acc[4][4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) acc[a][b][i] = 0.0;
+  load_chunk(0, 0);
+  cp_async_commit();
+  for (int ch = 0; ch < nch; ++ch) {
+    if (ch + 1 < nch) load_chunk(ch + 1, (ch + 1) & 1);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+    const double* As = sbuf + (ch & 1) * kBuf;
+    const double* Bs = As + KC * kLdA;
+    // zero-filled past K, so every chunk runs full k16 steps
+#pragma unroll 1
+    for (int k16 = 0; k16 < KC; k16 += 16) {
+      double bf[4][4];
+#pragma unroll
+      for (int n = 0; n < 4; ++n)
+#pragma unroll
+        for (int i = 0; i < 4; ++i) bf[n][i] = Bs[(k16 + q + 4 * i) * kLdB + wc + 8 * n + g];
+#pragma unroll
+      for (int mt = 0; mt < 4; ++mt) {
+        double af[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) af[i] = As[(k16 + q + 4 * (i >> 1)) * kLdA + wr + 16 * mt + g + 8 * (i & 1)];
+#pragma unroll
+        for (int n = 0; n < 4; ++n) dmma16816(acc[mt][n], af, bf[n]);
+      }
+    }
+    __syncthreads();
+  }
+  cp_async_wait_all();
+  // Epilogue through shared memory (the operand buffers are free now): the tile's
+  // old values arrive in one round of cp.async (row tid of every column), the
+  // accumulators are subtracted in place, and each column goes back as one
+  // coalesced store per warp.  Cs[c][r] holds column c, row r of the CTA tile.
+  double* Cs = sbuf;
+  const int tile_cols = min(TC, m - c0);
+#pragma unroll 8
+  for (int c = 0; c < TC; ++c) {
+    const int rr = r0 + tid, cc = c0 + c;
+    const bool ok = c < tile_cols && rr < m && cc <= rr;
+    const double* src = ok ? felem(L, U, lo, uo, m, k, rr, cc) : F;
+    cp_async_elem<8>(Cs + c * kLdC + tid, src, ok ? 8 : 0);
+  }
+  cp_async_commit();
+  cp_async_wait_all();
+  __syncthreads();
+  // element (mt, n, i): row wr + 16 mt + g + 8 (i / 2), column wc + 8 n + 2 q + (i & 1)
+#pragma unroll
+  for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+    for (int n = 0; n < 4; ++n)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int rl = wr + 16 * mt + g + 8 * (i >> 1), cl = wc + 8 * n + 2 * q + (i & 1);
+        Cs[cl * kLdC + rl] -= acc[mt][n][i];
+      }
+  __syncthreads();
+  for (int c = 0; c < tile_cols; ++c) {
+    const int rr = r0 + tid, cc = c0 + c;
+    if (rr < m && cc <= rr) *felem(L, U, lo, uo, m, k, rr, cc) = Cs[c * kLdC + tid];
+  }
+}
+
 // ---------------------------------------------------------------------------
 // solve kernels (front vectors W: m x nrhs per front, ld = m)
 // ---------------------------------------------------------------------------
@@ -1499,6 +1635,7 @@ template <class T>
 constexpr size_t syrk_smem() { return sizeof(T) * 2 * kTileSyrk * (P + 1); }
 template <class T>
 constexpr size_t big_smem() { return sizeof(T) * 2 * KC * (kTileBig + kBigCols); }
+constexpr size_t dmma_smem() { return sizeof(double) * 2 * KC * (kLdA + kLdB); }
 
 template <class T>
 std::string set_attributes() {
@@ -1506,6 +1643,7 @@ std::string set_attributes() {
   TDEM_CUDA_TRY(cudaFuncSetAttribute(k_syrk_panel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)syrk_smem<T>()));
   TDEM_CUDA_TRY(cudaFuncSetAttribute(k_syrk_big<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big_smem<T>()));
+  TDEM_CUDA_TRY(cudaFuncSetAttribute(k_syrk_big_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dmma_smem()));
   TDEM_CUDA_TRY(cudaFuncSetAttribute(k_fwd_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
   TDEM_CUDA_TRY(cudaFuncSetAttribute(k_bwd_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
   TDEM_CUDA_TRY(cudaFuncSetAttribute(k_fwd_update<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
@@ -1552,12 +1690,16 @@ int launch_factor(const Symbolic& sy, T* L, T* U, const double* vals, const int6
         ++launches;
       }
       if (ps.syrk_big.ctas > 0) {
-        if (std::is_same<T, float>::value && use_tc)
+        if constexpr (std::is_same<T, double>::value) {
+          k_syrk_big_dmma<<<grid_of(2 * ps.syrk_big.ctas), kBigThreads, dmma_smem(), s>>>(
+              L, U, fr, tasks + ps.syrk_big.off, prefix + ps.syrk_big.pre, ps.syrk_big.count, ps.j0);
+        } else if (use_tc) {
           launch_syrk_tc((float*)L, (float*)U, fr.l_off, fr.u_off, fr.m, fr.k, tasks + ps.syrk_big.off,
                          prefix + ps.syrk_big.pre, ps.syrk_big.count, ps.syrk_big.ctas, ps.j0, err, s);
-        else
+        } else {
           k_syrk_big<T><<<grid_of(2 * ps.syrk_big.ctas), kBigThreads, big_smem<T>(), s>>>(
               L, U, fr, tasks + ps.syrk_big.off, prefix + ps.syrk_big.pre, ps.syrk_big.count, ps.j0);
+        }
         ++launches;
       }
     }
