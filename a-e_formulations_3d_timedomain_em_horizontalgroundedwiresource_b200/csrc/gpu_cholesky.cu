@@ -14,7 +14,7 @@
 //
 // Factorization per level: zero the update blocks, extend-add the children,
 // then for each 64-wide inner panel [j0, j1): Cholesky of the diagonal block,
-// triangular solve of the rows below, rank-64 update of the rest of the 256-wide
+// triangular solve of the rows below, rank-64 update of the rest of the kOuter-wide
 // outer panel [J0, J1); at the end of each outer panel one rank-(J1 - J0) update
 // of the whole trailing matrix on 128 x 128 register-blocked tiles.
 #include "gpu_cholesky.h"
@@ -372,11 +372,14 @@ __global__ void __launch_bounds__(kBigThreads, 2) k_syrk_big(T* __restrict__ L, 
 // and cp.async double buffering as k_syrk_big, but each warp owns a 64 x 32 block
 // of its CTA's 128 x 64 tile as 4 x 4 MMA tiles, so one instruction does 2,048
 // multiply-adds instead of 32 and the issue slots stay free for the loads.
-// Shared layouts are k-major with the row (column) stride padded to 8 mod 16
-// doubles: a fragment load of 8 rows x 4 k then spans all 32 banks twice.
-constexpr int kLdA = kTileBig + 8;   // 136
-constexpr int kLdB = kBigCols + 8;   // 72
-constexpr int kLdC = kTileBig + 4;   // epilogue tile columns (fits in the operand buffers)
+// Shared layouts are k-major with the row (column) stride padded to 4 mod 16
+// doubles.  A 64-bit shared access is served per half-warp; a fragment load's
+// half-warp reads 4 rows x 4 k, which this stride spreads over all 32 banks.
+// The epilogue tile's column stride is 2 mod 8 for the same reason (its
+// fragment elements step two columns per q).
+constexpr int kLdA = kTileBig + 4;   // 132
+constexpr int kLdB = kBigCols + 4;   // 68
+constexpr int kLdC = kTileBig + 2;   // 130, epilogue tile columns (fits in the operand buffers)
 static_assert(kBigCols * kLdC <= 2 * KC * (kLdA + kLdB), "epilogue tile must fit the operand buffers");
 
 __device__ __forceinline__ void dmma16816(double (&c)[4], const double (&a)[8], const double (&b)[4]) {
@@ -388,33 +391,22 @@ __device__ __forceinline__ void dmma16816(double (&c)[4], const double (&a)[8], 
         "d"(b[1]), "d"(b[2]), "d"(b[3]));
 }
 
-__global__ void __launch_bounds__(kBigThreads, 2) k_syrk_big_dmma(double* __restrict__ L, double* __restrict__ U,
-                                                                   Fronts f, const int* __restrict__ fronts,
-                                                                   const int64_t* __restrict__ prefix, int count,
-                                                                   int j0) {
-  constexpr int TB = kTileBig, TC = kBigCols;
-  extern __shared__ __align__(16) unsigned char sm_raw[];
-  double* sbuf = reinterpret_cast<double*>(sm_raw);  // buffer s: As (KC x kLdA) then Bs (KC x kLdB)
-  const int idx = find_task(prefix, count, blockIdx.x >> 1);
-  const int s = fronts[idx];
-  const int m = f.m[s], k = f.k[s];
-  const int J0 = (j0 / kOuter) * kOuter, J1 = min(k, J0 + kOuter);
-  const int64_t lo = f.l_off[s], uo = f.u_off[s];
+// One 128 x 64 tile of F -= X X^T on the FP64 tensor pipe: rows [r0, r0 + 128)
+// below m, columns [c0, c0 + 64) below cend, lower triangle only; X is column
+// block [kb, kb + K) of the front (rows of X = rows and columns of the tile).
+// Called by all 128 threads of a CTA with kBigThreads threads and dmma_smem()
+// bytes of dynamic shared memory.
+__device__ __forceinline__ void dmma_tile(double* __restrict__ L, double* __restrict__ U, int64_t lo, int64_t uo,
+                                          int m, int k, int r0, int c0, int cend, int kb, int K, double* sbuf) {
+  constexpr int TC = kBigCols;
   const double* F = L + lo;
-  const int64_t t = (blockIdx.x >> 1) - prefix[idx];
-  int bi = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
-  while ((int64_t)(bi + 1) * (bi + 2) / 2 <= t) ++bi;
-  while ((int64_t)bi * (bi + 1) / 2 > t) --bi;
-  const int bj = (int)(t - (int64_t)bi * (bi + 1) / 2);
-  const int r0 = J1 + bi * TB, c0 = J1 + bj * TB + (blockIdx.x & 1) * TC;
-  if (c0 >= m) return;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, q = lane & 3;
   const int wr = (warp >> 1) * 64, wc = (warp & 1) * 32;  // warp block within the CTA tile
-  const int K = J1 - J0, nch = (K + KC - 1) / KC;
+  const int nch = (K + KC - 1) / KC;
   const bool arow = r0 + tid < m;
   const int bi_row = tid & (TC - 1), bp0 = tid >> 6;
-  const bool brow = c0 + bi_row < m;
+  const bool brow = c0 + bi_row < cend;
   constexpr int kBuf = KC * (kLdA + kLdB);
   auto load_chunk = [&](int ch, int buf) {
     double* As = sbuf + buf * kBuf;
@@ -423,14 +415,14 @@ __global__ void __launch_bounds__(kBigThreads, 2) k_syrk_big_dmma(double* __rest
 #pragma unroll 8
     for (int p = 0; p < KC; ++p) {
       const bool ok = arow && p < kc;
-      const double* src = ok ? F + (r0 + tid) + (int64_t)(J0 + k0 + p) * m : F;
+      const double* src = ok ? F + (r0 + tid) + (int64_t)(kb + k0 + p) * m : F;
       cp_async_elem<8>(As + p * kLdA + tid, src, ok ? 8 : 0);
     }
 #pragma unroll 8
     for (int j = 0; j < KC / 2; ++j) {
       const int p = bp0 + 2 * j;
       const bool ok = brow && p < kc;
-      const double* src = ok ? F + (c0 + bi_row) + (int64_t)(J0 + k0 + p) * m : F;
+      const double* src = ok ? F + (c0 + bi_row) + (int64_t)(kb + k0 + p) * m : F;
       cp_async_elem<8>(Bs + p * kLdB + bi_row, src, ok ? 8 : 0);
     }
   };
@@ -475,7 +467,7 @@ __global__ void __launch_bounds__(kBigThreads, 2) k_syrk_big_dmma(double* __rest
   // accumulators are subtracted in place, and each column goes back as one
   // coalesced store per warp.  Cs[c][r] holds column c, row r of the CTA tile.
   double* Cs = sbuf;
-  const int tile_cols = min(TC, m - c0);
+  const int tile_cols = min(TC, cend - c0);
 #pragma unroll 8
   for (int c = 0; c < TC; ++c) {
     const int rr = r0 + tid, cc = c0 + c;
@@ -501,6 +493,53 @@ __global__ void __launch_bounds__(kBigThreads, 2) k_syrk_big_dmma(double* __rest
     const int rr = r0 + tid, cc = c0 + c;
     if (rr < m && cc <= rr) *felem(L, U, lo, uo, m, k, rr, cc) = Cs[c * kLdC + tid];
   }
+}
+
+// Trailing update of an outer panel on the FP64 tensor pipe (two CTAs per task-list
+// tile of 128 x 128, one per 64-column half).
+__global__ void __launch_bounds__(kBigThreads, 2) k_syrk_big_dmma(double* __restrict__ L, double* __restrict__ U,
+                                                                   Fronts f, const int* __restrict__ fronts,
+                                                                   const int64_t* __restrict__ prefix, int count,
+                                                                   int j0) {
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  const int idx = find_task(prefix, count, blockIdx.x >> 1);
+  const int s = fronts[idx];
+  const int m = f.m[s], k = f.k[s];
+  const int J0 = (j0 / kOuter) * kOuter, J1 = min(k, J0 + kOuter);
+  const int64_t t = (blockIdx.x >> 1) - prefix[idx];
+  int bi = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+  while ((int64_t)(bi + 1) * (bi + 2) / 2 <= t) ++bi;
+  while ((int64_t)bi * (bi + 1) / 2 > t) --bi;
+  const int bj = (int)(t - (int64_t)bi * (bi + 1) / 2);
+  const int r0 = J1 + bi * kTileBig, c0 = J1 + bj * kTileBig + (blockIdx.x & 1) * kBigCols;
+  if (c0 >= m) return;
+  dmma_tile(L, U, f.l_off[s], f.u_off[s], m, k, r0, c0, m, J0, J1 - J0,
+            reinterpret_cast<double*>(sm_raw));
+}
+
+// Update of the rest of the outer panel by the inner panel [j0, j1) on the FP64
+// tensor pipe: F[r, c] -= sum_p X[r, p] X[c, p] for c in [j1, J1), r >= c, in 128 x
+// 64 tiles.  Column tile bj pairs with row tiles bi >= bj / 2 (the ones reaching
+// the diagonal), so a front has sum over bj of (nr - bj / 2) tiles.
+__global__ void __launch_bounds__(kBigThreads, 2) k_panel_dmma(double* __restrict__ L, double* __restrict__ U,
+                                                                Fronts f, const int* __restrict__ fronts,
+                                                                const int64_t* __restrict__ prefix, int count,
+                                                                int j0) {
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  const int idx = find_task(prefix, count, blockIdx.x);
+  const int s = fronts[idx];
+  const int m = f.m[s], k = f.k[s];
+  const int w = min(kPanel, k - j0), j1 = j0 + w;
+  const int J0 = (j0 / kOuter) * kOuter, J1 = min(k, J0 + kOuter);
+  const int nr = (m - j1 + kTileBig - 1) / kTileBig;
+  int t = (int)(blockIdx.x - prefix[idx]), bj = 0;
+  while (t >= nr - bj / 2) {
+    t -= nr - bj / 2;
+    ++bj;
+  }
+  const int bi = bj / 2 + t;
+  dmma_tile(L, U, f.l_off[s], f.u_off[s], m, k, j1 + bi * kTileBig, j1 + bj * kBigCols, J1, j0, w,
+            reinterpret_cast<double*>(sm_raw));
 }
 
 // ---------------------------------------------------------------------------
@@ -1644,6 +1683,7 @@ std::string set_attributes() {
                                      (int)syrk_smem<T>()));
   TDEM_CUDA_TRY(cudaFuncSetAttribute(k_syrk_big<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big_smem<T>()));
   TDEM_CUDA_TRY(cudaFuncSetAttribute(k_syrk_big_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dmma_smem()));
+  TDEM_CUDA_TRY(cudaFuncSetAttribute(k_panel_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dmma_smem()));
   TDEM_CUDA_TRY(cudaFuncSetAttribute(k_fwd_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
   TDEM_CUDA_TRY(cudaFuncSetAttribute(k_bwd_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
   TDEM_CUDA_TRY(cudaFuncSetAttribute(k_fwd_update<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
@@ -1685,8 +1725,13 @@ int launch_factor(const Symbolic& sy, T* L, T* U, const double* vals, const int6
         ++launches;
       }
       if (ps.syrk.ctas > 0) {
-        k_syrk_panel<T><<<grid_of(ps.syrk.ctas), 256, syrk_smem<T>(), s>>>(L, fr, tasks + ps.syrk.off,
-                                                                           prefix + ps.syrk.pre, ps.syrk.count, ps.j0);
+        if constexpr (std::is_same<T, double>::value)
+          k_panel_dmma<<<grid_of(ps.syrk_wide.ctas), kBigThreads, dmma_smem(), s>>>(
+              L, U, fr, tasks + ps.syrk_wide.off, prefix + ps.syrk_wide.pre, ps.syrk_wide.count, ps.j0);
+        else
+          k_syrk_panel<T><<<grid_of(ps.syrk.ctas), 256, syrk_smem<T>(), s>>>(L, fr, tasks + ps.syrk.off,
+                                                                             prefix + ps.syrk.pre, ps.syrk.count,
+                                                                             ps.j0);
         ++launches;
       }
       if (ps.syrk_big.ctas > 0) {

@@ -423,7 +423,7 @@ std::string analyse(int n, const int64_t* rowptr, const int* colind, const doubl
       PanelStep ps;
       ps.j0 = j0;
       std::vector<int> fr, fin, fbig;
-      std::vector<int64_t> c1, c2, c3, c4, c5;
+      std::vector<int64_t> c1, c2, c3, c4, c5, c6;
       const int J0 = (j0 / kOuter) * kOuter;
       for (int s : lp.fronts) {
         const int k = sy.front_k[s], m = sy.front_m[s];
@@ -440,6 +440,11 @@ std::string analyse(int n, const int64_t* rowptr, const int* colind, const doubl
           const int64_t nr = cdiv(below, kTileSyrk), nc = cdiv(J1 - j1, kTileSyrk);
           fin.push_back(s);
           c3.push_back(nc * nr - nc * (nc - 1) / 2);
+          // 128 x 64 tiles: column tile bj with row tiles bj / 2 .. nr128 - 1
+          const int64_t nr128 = cdiv(below, kTileBig), nc64 = cdiv(J1 - j1, 64);
+          int64_t w6 = 0;
+          for (int64_t bj = 0; bj < nc64; ++bj) w6 += nr128 - bj / 2;
+          c6.push_back(w6);
         } else if (m > J1) {
           const int64_t nt = cdiv(m - J1, kTileBig);
           fbig.push_back(s);
@@ -449,6 +454,7 @@ std::string analyse(int n, const int64_t* rowptr, const int* colind, const doubl
       add_tasks(sy, ps.potrf, fr, c1);
       add_tasks(sy, ps.trsm, fr, c2);
       add_tasks(sy, ps.syrk, fin, c3);
+      add_tasks(sy, ps.syrk_wide, fin, c6);
       add_tasks(sy, ps.syrk_big, fbig, c5);
       add_tasks(sy, ps.solve_upd, fr, c4);
       max_partials = std::max(max_partials, ps.solve_upd.ctas);

@@ -22,7 +22,7 @@
 namespace tdem {
 
 constexpr int kPanel = 64;       // dense panel width of the factorization and solves
-constexpr int kOuter = 256;      // outer panel width: trailing updates of rank up to kOuter
+constexpr int kOuter = 512;      // outer panel width: trailing updates of rank up to kOuter
 constexpr int kTileSyrk = 64;    // tile edge of the update inside an outer panel
 constexpr int kTileBig = 128;    // tile edge of the rank-kOuter trailing update
 constexpr int kTrsmRows = 128;   // rows per CTA of the panel triangular solve
@@ -58,6 +58,7 @@ struct PanelStep {
   TaskList potrf;      // one CTA per front
   TaskList trsm;       // ceil((m - j1) / kTrsmRows) CTAs per front
   TaskList syrk;       // update of columns [j1, J1) (rows >= j1) by the inner panel, 64-tiles
+  TaskList syrk_wide;  // the same update in 128-row x 64-column tiles (FP64 tensor-pipe kernel)
   TaskList syrk_big;   // at the end of an outer panel: trailing [J1, m) by [J0, J1), 128-tiles
   TaskList solve_upd;  // ceil((m - j1) / kSolveRows) CTAs per front (fwd update / bwd partials)
 };

@@ -101,7 +101,7 @@ typedef struct tdem_options {
   double refine_tol;        /* relative residual to reach per step and column (default 1e-10) */
   int refine_maxit;         /* iteration cap; exceeding it is TDEM_ERR_NUMERIC (default 200) */
   int leaf_size;            /* nested-dissection leaf size (default 128) */
-  int fp32_update;          /* precision 32, rank-256 trailing updates of the factorization:
+  int fp32_update;          /* precision 32, rank-512 trailing updates of the factorization:
                                0 = library default, 1 = CUDA cores (FP32 FMA),
                                2 = tensor cores (tcgen05, 3xTF32 with FP32 accumulation) */
   int factor_slots;         /* precision 64: numeric factors held on the device.  2 factors the
