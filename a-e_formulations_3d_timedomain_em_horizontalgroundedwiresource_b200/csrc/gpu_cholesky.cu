@@ -143,40 +143,41 @@ __global__ void k_potrf(T* __restrict__ L, Fronts f, const int* __restrict__ fro
 }
 
 // Panel triangular solve: rows [j1, m) of the panel columns times L_dd^-T.
-// kTrsmRows rows per CTA, one thread per row.
+// kTrsmRows rows per CTA, one row per thread held in registers (the substitution
+// is unrolled over the 64 columns, so every element has a fixed register); the
+// diagonal block is read from shared memory, the same address for the whole warp.
 template <class T>
 __global__ void __launch_bounds__(kTrsmRows) k_trsm(T* __restrict__ L, Fronts f, const int* __restrict__ fronts,
                                                     const int64_t* __restrict__ prefix, int count, int j0) {
-  extern __shared__ __align__(16) unsigned char sm_raw[];
-  T(*Ld)[P + 1] = reinterpret_cast<T(*)[P + 1]>(sm_raw);
-  T(*X)[P + 1] = reinterpret_cast<T(*)[P + 1]>(sm_raw + sizeof(T) * P * (P + 1));
+  __shared__ T Ld[P][P];  // Ld[c][cc] = L_dd(c, cc), cc <= c
   const int idx = find_task(prefix, count, blockIdx.x);
   const int s = fronts[idx];
   const int m = f.m[s], k = f.k[s];
   const int w = min(P, k - j0), j1 = j0 + w;
   T* F = L + f.l_off[s];
-  const int r0 = j1 + (int)(blockIdx.x - prefix[idx]) * kTrsmRows;
   for (int q = threadIdx.x; q < w * w; q += blockDim.x) {
     const int i = q % w, j = q / w;
     Ld[i][j] = (i >= j) ? F[(j0 + i) + (int64_t)(j0 + j) * m] : (T)0;
   }
-  for (int q = threadIdx.x; q < kTrsmRows * w; q += blockDim.x) {
-    const int i = q % kTrsmRows, j = q / kTrsmRows;
-    const int row = r0 + i;
-    X[i][j] = (row < m) ? F[row + (int64_t)(j0 + j) * m] : (T)0;
-  }
+  const int row = j1 + (int)(blockIdx.x - prefix[idx]) * kTrsmRows + threadIdx.x;
+  const bool live = row < m;
+  T x[P];
+#pragma unroll
+  for (int c = 0; c < P; ++c) x[c] = (live && c < w) ? F[row + (int64_t)(j0 + c) * m] : (T)0;
   __syncthreads();
-  const int t = threadIdx.x;
-  for (int c = 0; c < w; ++c) {
-    T v = X[t][c];
-    for (int cc = 0; cc < c; ++cc) v -= X[t][cc] * Ld[c][cc];
-    X[t][c] = v / Ld[c][c];
+#pragma unroll
+  for (int c = 0; c < P; ++c) {
+    if (c < w) {
+      T v = x[c];
+#pragma unroll
+      for (int cc = 0; cc < c; ++cc) v -= x[cc] * Ld[c][cc];
+      x[c] = v / Ld[c][c];
+    }
   }
-  __syncthreads();
-  for (int q = threadIdx.x; q < kTrsmRows * w; q += blockDim.x) {
-    const int i = q % kTrsmRows, j = q / kTrsmRows;
-    const int row = r0 + i;
-    if (row < m) F[row + (int64_t)(j0 + j) * m] = X[i][j];
+  if (live) {
+#pragma unroll
+    for (int c = 0; c < P; ++c)
+      if (c < w) F[row + (int64_t)(j0 + c) * m] = x[c];
   }
 }
 
@@ -1669,8 +1670,6 @@ __global__ void __launch_bounds__(256) k_diag_inverse(const T* __restrict__ L, T
 
 inline unsigned grid_of(int64_t ctas) { return (unsigned)ctas; }
 template <class T>
-constexpr size_t trsm_smem() { return sizeof(T) * (P + kTrsmRows) * (P + 1); }
-template <class T>
 constexpr size_t syrk_smem() { return sizeof(T) * 2 * kTileSyrk * (P + 1); }
 template <class T>
 constexpr size_t big_smem() { return sizeof(T) * 2 * KC * (kTileBig + kBigCols); }
@@ -1678,7 +1677,6 @@ constexpr size_t dmma_smem() { return sizeof(double) * 2 * KC * (kLdA + kLdB); }
 
 template <class T>
 std::string set_attributes() {
-  TDEM_CUDA_TRY(cudaFuncSetAttribute(k_trsm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_smem<T>()));
   TDEM_CUDA_TRY(cudaFuncSetAttribute(k_syrk_panel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)syrk_smem<T>()));
   TDEM_CUDA_TRY(cudaFuncSetAttribute(k_syrk_big<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big_smem<T>()));
@@ -1720,7 +1718,7 @@ int launch_factor(const Symbolic& sy, T* L, T* U, const double* vals, const int6
       k_potrf<T><<<ps.potrf.count, 256, 0, s>>>(L, fr, tasks + ps.potrf.off, ps.j0, err, c0);
       ++launches;
       if (ps.trsm.ctas > 0) {
-        k_trsm<T><<<grid_of(ps.trsm.ctas), kTrsmRows, trsm_smem<T>(), s>>>(L, fr, tasks + ps.trsm.off,
+        k_trsm<T><<<grid_of(ps.trsm.ctas), kTrsmRows, 0, s>>>(L, fr, tasks + ps.trsm.off,
                                                                            prefix + ps.trsm.pre, ps.trsm.count, ps.j0);
         ++launches;
       }
