@@ -327,7 +327,8 @@ struct PardisoHandle {
   std::vector<int64_t> upper_to_lower;  // upper-CSR entry -> lower-CSR entry
   double* d_vals = nullptr;
   double* d_x = nullptr;
-  int nrhs_cap = 0;
+  int nrhs_cap = 0;    // columns d_x holds
+  int solve_cols = 1;  // columns one solve takes (the nrhs given to the analysing phase 12)
 };
 
 uint64_t pattern_hash(int64_t n, const long long* ia, const long long* ja) {
@@ -363,7 +364,8 @@ int pardiso_analyse(PardisoHandle* h, int64_t n, const long long* ia, const long
   std::vector<int> p2v(n);
   for (int64_t p = 0; p < n; ++p) p2v[p] = sy.iperm[p];
   h->chol.reset(new tdem::GpuCholesky());
-  if (!h->chol->setup(std::move(sy), p2v, std::max(1, nrhs), h->stream).empty()) return -2;
+  h->solve_cols = std::min(tdem::kMaxRhs, std::max(1, nrhs));
+  if (!h->chol->setup(std::move(sy), p2v, h->solve_cols, h->stream).empty()) return -2;
   if (h->d_vals) cudaFree(h->d_vals);
   if (cudaMalloc(&h->d_vals, sizeof(double) * std::max<int64_t>(nnz, 1)) != cudaSuccess) return -2;
   h->n = n;
@@ -411,7 +413,9 @@ void tdem_pardiso_64(void* pt, const long long* /*maxfct*/, const long long* /*m
     }
     cudaSetDevice(h->device);
     if (!h->chol || h->n != *n || h->nnz != ia[*n] - 1 || h->hash != pattern_hash(*n, ia, ja)) {
-      const int r = pardiso_analyse(h, *n, ia, ja, 1);
+      // the solve workspace takes the nrhs of this call (the reference passes its
+      // right-hand-side count to every phase)
+      const int r = pardiso_analyse(h, *n, ia, ja, nrhs ? (int)std::min<long long>(*nrhs, tdem::kMaxRhs) : 1);
       if (r) {
         *error = r;
         return;
@@ -450,11 +454,11 @@ void tdem_pardiso_64(void* pt, const long long* /*maxfct*/, const long long* /*m
       }
       h->nrhs_cap = nr;
     }
-    // the solve workspace was sized for one column: solve column by column
-    for (int r = 0; r < nr; ++r) {
-      cudaMemcpyAsync(h->d_x + h->n * r, (const double*)b + h->n * r, sizeof(double) * h->n,
-                      cudaMemcpyHostToDevice, h->stream);
-      h->chol->solve(h->d_x + h->n * r, h->d_x + h->n * r, h->n, 1, h->stream);
+    // all columns in one copy, solved in blocks of the analysed right-hand-side count
+    cudaMemcpyAsync(h->d_x, b, sizeof(double) * h->n * nr, cudaMemcpyHostToDevice, h->stream);
+    for (int r = 0; r < nr; r += h->solve_cols) {
+      const int cols = std::min(h->solve_cols, nr - r);
+      h->chol->solve(h->d_x + h->n * r, h->d_x + h->n * r, h->n, cols, h->stream);
     }
     cudaMemcpyAsync(x, h->d_x, sizeof(double) * h->n * nr, cudaMemcpyDeviceToHost, h->stream);
     if (cudaStreamSynchronize(h->stream) != cudaSuccess) *error = -2;

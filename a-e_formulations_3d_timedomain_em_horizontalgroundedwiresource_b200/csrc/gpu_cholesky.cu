@@ -885,12 +885,63 @@ __device__ __forceinline__ void load_block(T (&pre)[16], const T* __restrict__ F
   }
 }
 // registers -> Ls[c][i]
+constexpr int kLdL = SB + 4;  // 68: fragment loads along either index hit all 32 banks
 template <class T>
-__device__ __forceinline__ void store_block(T (*Ls)[SB + 1], const T (&pre)[16]) {
+__device__ __forceinline__ void store_block(T (*Ls)[kLdL], const T (&pre)[16]) {
 #pragma unroll
   for (int e = 0; e < 16; ++e) {
     const int q = threadIdx.x + 256 * e;
     Ls[q >> 6][q & 63] = pre[e];
+  }
+}
+
+// Leading dimension of the staged solution values of a block (64 x nrhs): the
+// right-hand sides rounded up to MMA tiles of 8, plus 4 (4 mod 16 doubles keeps a
+// half-warp's fragment load on distinct banks).
+__host__ __device__ constexpr int ys_ld(int nrhs) { return 8 * ((nrhs + 7) / 8) + 4; }
+
+// acc[r][c-tile] += M (64 x 64) * V (64 x nrhs) on the FP64 tensor pipe for one
+// 64 x 64 block, M read from Ls: element (row, k) at Ls[k][row] (TRANS = false) or
+// Ls[row][k] (TRANS = true); V element (k, r) at Vs[k * ld + r].  Warp w owns row
+// tile w % 4 and column tiles w / 4 + 2 j; NTW = column tiles per warp.
+template <bool TRANS, int NTW>
+__device__ __forceinline__ void block_dmma(double (&acc)[NTW][4], const double (*Ls)[kLdL], const double* Vs, int ld,
+                                           int ntiles) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, q = lane & 3;
+  const int mt = warp & 3;
+#pragma unroll
+  for (int k16 = 0; k16 < SB; k16 += 16) {
+    double af[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int row = 16 * mt + g + 8 * (i & 1), kk = k16 + q + 4 * (i >> 1);
+      af[i] = TRANS ? Ls[row][kk] : Ls[kk][row];
+    }
+#pragma unroll
+    for (int j = 0; j < NTW; ++j) {
+      const int nt = (warp >> 2) + 2 * j;
+      if (nt < ntiles) {
+        double bf[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) bf[i] = Vs[(k16 + q + 4 * i) * ld + 8 * nt + g];
+        dmma16816(acc[j], af, bf);
+      }
+    }
+  }
+}
+
+// MMA accumulators -> Out[row * ld + r] (64 x 8 ntiles)
+template <int NTW>
+__device__ __forceinline__ void store_acc(const double (&acc)[NTW][4], double* Out, int ld, int ntiles) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, q = lane & 3;
+  const int mt = warp & 3;
+#pragma unroll
+  for (int j = 0; j < NTW; ++j) {
+    const int nt = (warp >> 2) + 2 * j;
+    if (nt < ntiles) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) Out[(16 * mt + g + 8 * (i >> 1)) * ld + 8 * nt + 2 * q + (i & 1)] = acc[j][i];
+    }
   }
 }
 
@@ -899,15 +950,19 @@ __device__ __forceinline__ void store_block(T (*Ls)[SB + 1], const T (&pre)[16])
 // the pivot blocks q in [lo, hi).  Chunk units publish partial sums; the final
 // unit (q = the last one the row needs) adds them, then a pivot row solves
 // y_R = Dinv_R (w_R - sum) and raises its flag, an update row stores w_R - sum
-// for the parent.  One unit per CTA.
+// for the parent.  One unit per CTA.  In FP64 the block products run on the
+// tensor pipe (the right-hand sides make them compute-bound).
 // Thread t: row i = t % 64 of the block, right-hand sides r = t / 64 + 4 j.
 template <class T, int RPT>
 __global__ void __launch_bounds__(256, 2) k_fwd_level(const T* __restrict__ L, const T* __restrict__ Dinv, T* W, T* part,
                                                    int nr_rhs, FusedArgs fa) {
-  __shared__ T Ls[SB][SB + 1];
+  __shared__ T Ls[SB][kLdL];
   __shared__ int s_item;
   extern __shared__ __align__(16) unsigned char sm_raw[];
-  T* Ys = reinterpret_cast<T*>(sm_raw);  // SB x nrhs, [c * nrhs + r]
+  T* Ys = reinterpret_cast<T*>(sm_raw);  // SB x ysl, [c * ysl + r]
+  const int ysl = ys_ld(nr_rhs), ntl = (nr_rhs + 7) / 8;
+  constexpr bool kMma = std::is_same<T, double>::value;
+  constexpr int NTW = (RPT + 3) / 4;  // column tiles per warp (nrhs <= 4 RPT)
   const int t = threadIdx.x, i = t & 63, g = t >> 6;
   if (t == 0) s_item = atomicAdd(fa.ticket, 1);
   __syncthreads();
@@ -923,6 +978,11 @@ __global__ void __launch_bounds__(256, 2) k_fwd_level(const T* __restrict__ L, c
   T acc[RPT];
 #pragma unroll
   for (int j = 0; j < RPT; ++j) acc[j] = (T)0;
+  double macc[NTW][4];
+#pragma unroll
+  for (int j = 0; j < NTW; ++j)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) macc[j][e] = 0.0;
   // final pivot unit: its inverted diagonal block and its own rows of W do not
   // depend on this launch, so they are read before any wait
   // (with many right-hand sides the registers go to the accumulators instead and
@@ -957,20 +1017,36 @@ __global__ void __launch_bounds__(256, 2) k_fwd_level(const T* __restrict__ L, c
     if (t == 0) wait_flag(flags + q, fa.err);
     __syncthreads();
     store_block(Ls, pre);
-    for (int e = t; e < SB * nr_rhs; e += 256) {
-      const int c = e % SB, r = e / SB;
-      Ys[c * nr_rhs + r] = (c < wq) ? __ldcg(w + SB * q + c + (int64_t)r * m) : (T)0;
+    for (int e = t; e < SB * ysl; e += 256) {
+      const int c = e / ysl, r = e % ysl;
+      Ys[e] = (c < wq && r < nr_rhs) ? __ldcg(w + SB * q + c + (int64_t)r * m) : (T)0;
     }
     __syncthreads();
     if (q + 1 < hi) load_block(pre, F, m, r0, nr, SB * (q + 1), min(SB, k - SB * (q + 1)));
+    if constexpr (kMma) {
+      block_dmma<false, NTW>(macc, Ls, Ys, ysl, ntl);
+    } else {
 #pragma unroll 8
-    for (int c = 0; c < SB; ++c) {
-      const T l = Ls[c][i];
+      for (int c = 0; c < SB; ++c) {
+        const T l = Ls[c][i];
 #pragma unroll
-      for (int j = 0; j < RPT; ++j) {
-        const int r = g + 4 * j;
-        if (r < nr_rhs) acc[j] = fma(l, Ys[c * nr_rhs + r], acc[j]);
+        for (int j = 0; j < RPT; ++j) {
+          const int r = g + 4 * j;
+          if (r < nr_rhs) acc[j] = fma(l, Ys[c * ysl + r], acc[j]);
+        }
       }
+    }
+  }
+  if constexpr (kMma) {
+    // the tensor-pipe sums go to the thread layout through the (now free) block tile
+    T* Acc = &Ls[0][0];
+    __syncthreads();
+    store_acc<NTW>(macc, Acc, kLdL, ntl);
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < RPT; ++j) {
+      const int r = g + 4 * j;
+      if (r < nr_rhs) acc[j] = Acc[i * kLdL + r];
     }
   }
   if (!fin) {
@@ -993,7 +1069,7 @@ __global__ void __launch_bounds__(256, 2) k_fwd_level(const T* __restrict__ L, c
 #pragma unroll
   for (int j = 0; j < RPT; ++j) {
     const int r = g + 4 * j;
-    if (r < nr_rhs) Ys[i * nr_rhs + r] = (i < nr) ? wrow[j] - acc[j] : (T)0;
+    if (r < nr_rhs) Ys[i * ysl + r] = (i < nr) ? wrow[j] - acc[j] : (T)0;
   }
   if constexpr (kPreD) {
     store_block(Ls, dpre);
@@ -1013,7 +1089,7 @@ __global__ void __launch_bounds__(256, 2) k_fwd_level(const T* __restrict__ L, c
 #pragma unroll
     for (int j = 0; j < RPT; ++j) {
       const int r = g + 4 * j;
-      if (r < nr_rhs) y[j] = fma(l, Ys[c * nr_rhs + r], y[j]);
+      if (r < nr_rhs) y[j] = fma(l, Ys[c * ysl + r], y[j]);
     }
   }
   if (i < nr) {
@@ -1032,16 +1108,20 @@ __global__ void __launch_bounds__(256, 2) k_fwd_level(const T* __restrict__ L, c
 // else update rows, whose x come from ancestors and were staged in W by
 // k_bwd_init).  The final unit (row block p + 1) adds the chunk partials and
 // solves x_p = Dinv_p^T (y_p - sum), written to W and to the caller's vector,
-// then raises the column's flag.  One unit per CTA.
+// then raises the column's flag.  One unit per CTA; FP64 block products on the
+// tensor pipe.
 // Thread t: column c = t % 64 of the block, right-hand sides r = t / 64 + 4 j.
 template <class T, int RPT>
 __global__ void __launch_bounds__(256, 2) k_bwd_level(const T* __restrict__ L, const T* __restrict__ Dinv, T* W, T* part,
                                                    double* __restrict__ x, const int* __restrict__ rows, int64_t ldx,
                                                    int nr_rhs, FusedArgs fa) {
-  __shared__ T Ls[SB][SB + 1];
+  __shared__ T Ls[SB][kLdL];
   __shared__ int s_item;
   extern __shared__ __align__(16) unsigned char sm_raw[];
-  T* Ws = reinterpret_cast<T*>(sm_raw);  // SB x nrhs, [row * nrhs + r]
+  T* Ws = reinterpret_cast<T*>(sm_raw);  // SB x ysl, [row * ysl + r]
+  const int ysl = ys_ld(nr_rhs), ntl = (nr_rhs + 7) / 8;
+  constexpr bool kMma = std::is_same<T, double>::value;
+  constexpr int NTW = (RPT + 3) / 4;
   const int t = threadIdx.x, c = t & 63, g = t >> 6;
   if (t == 0) s_item = atomicAdd(fa.ticket, 1);
   __syncthreads();
@@ -1055,6 +1135,11 @@ __global__ void __launch_bounds__(256, 2) k_bwd_level(const T* __restrict__ L, c
   T acc[RPT];
 #pragma unroll
   for (int j = 0; j < RPT; ++j) acc[j] = (T)0;
+  double macc[NTW][4];
+#pragma unroll
+  for (int j = 0; j < NTW; ++j)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) macc[j][e] = 0.0;
   constexpr bool kPreD = RPT <= 2;
   const T* D = Dinv + u.dinv_off + (int64_t)p * SB * SB;
   T dpre[kPreD ? 16 : 1], wrow[RPT];
@@ -1095,9 +1180,9 @@ __global__ void __launch_bounds__(256, 2) k_bwd_level(const T* __restrict__ L, c
     if (R < pb && t == 0) wait_flag(flags + R, fa.err);
     __syncthreads();
     store_block(Ls, pre);
-    for (int e = t; e < SB * nr_rhs; e += 256) {
-      const int ii = e % SB, r = e / SB;
-      Ws[ii * nr_rhs + r] = (ii < nr) ? __ldcg(w + r0 + ii + (int64_t)r * m) : (T)0;
+    for (int e = t; e < SB * ysl; e += 256) {
+      const int ii = e / ysl, r = e % ysl;
+      Ws[e] = (ii < nr && r < nr_rhs) ? __ldcg(w + r0 + ii + (int64_t)r * m) : (T)0;
     }
     __syncthreads();
     if (R - 1 >= lo) {
@@ -1105,14 +1190,29 @@ __global__ void __launch_bounds__(256, 2) k_bwd_level(const T* __restrict__ L, c
       rows_of(R - 1, r1, n1);
       load_block(pre, F, m, r1, n1, c0, wc);
     }
+    if constexpr (kMma) {
+      block_dmma<true, NTW>(macc, Ls, Ws, ysl, ntl);
+    } else {
 #pragma unroll 8
-    for (int ii = 0; ii < SB; ++ii) {
-      const T l = Ls[c][ii];
+      for (int ii = 0; ii < SB; ++ii) {
+        const T l = Ls[c][ii];
 #pragma unroll
-      for (int j = 0; j < RPT; ++j) {
-        const int r = g + 4 * j;
-        if (r < nr_rhs) acc[j] = fma(l, Ws[ii * nr_rhs + r], acc[j]);
+        for (int j = 0; j < RPT; ++j) {
+          const int r = g + 4 * j;
+          if (r < nr_rhs) acc[j] = fma(l, Ws[ii * ysl + r], acc[j]);
+        }
       }
+    }
+  }
+  if constexpr (kMma) {
+    T* Acc = &Ls[0][0];
+    __syncthreads();
+    store_acc<NTW>(macc, Acc, kLdL, ntl);
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < RPT; ++j) {
+      const int r = g + 4 * j;
+      if (r < nr_rhs) acc[j] = Acc[c * kLdL + r];
     }
   }
   if (!fin) {
@@ -1123,7 +1223,7 @@ __global__ void __launch_bounds__(256, 2) k_bwd_level(const T* __restrict__ L, c
 #pragma unroll
   for (int j = 0; j < RPT; ++j) {
     const int r = g + 4 * j;
-    if (r < nr_rhs) Ws[c * nr_rhs + r] = (c < wc) ? wrow[j] - (tot[j] + acc[j]) : (T)0;
+    if (r < nr_rhs) Ws[c * ysl + r] = (c < wc) ? wrow[j] - (tot[j] + acc[j]) : (T)0;
   }
   if constexpr (kPreD) {
     store_block(Ls, dpre);
@@ -1143,7 +1243,7 @@ __global__ void __launch_bounds__(256, 2) k_bwd_level(const T* __restrict__ L, c
 #pragma unroll
     for (int j = 0; j < RPT; ++j) {
       const int r = g + 4 * j;
-      if (r < nr_rhs) xv[j] = fma(l, Ws[ii * nr_rhs + r], xv[j]);
+      if (r < nr_rhs) xv[j] = fma(l, Ws[ii * ysl + r], xv[j]);
     }
   }
   if (c < wc) {
@@ -1813,7 +1913,7 @@ void launch_level_solves(const Symbolic& sy, const T* L, const T* Dinv, T* W, T*
   int* bflags = fflags + sy.n_flags;
   fa.counters = bflags + sy.n_flags;
   cudaMemsetAsync(sync, 0, sizeof(int) * (2 * nlev + 2 * sy.n_flags + sy.n_counters), s);
-  const size_t ysm = STREAM ? stream_smem<T>() : sizeof(T) * SB * a.nrhs;
+  const size_t ysm = STREAM ? stream_smem<T>() : sizeof(T) * SB * ys_ld(a.nrhs);
   auto grid = [&](int64_t count, int dir) {
     return STREAM ? (unsigned)std::min<int64_t>(count, resident[dir]) : grid_of(count);
   };
@@ -1911,7 +2011,7 @@ std::string stream_residency(int (&resident)[2][2], int& sms) {
 
 template <class T>
 std::string set_fused_attributes() {
-  const int ysm = (int)(sizeof(T) * SB * kMaxRhs);
+  const int ysm = (int)(sizeof(T) * SB * ys_ld(kMaxRhs));
   TDEM_CUDA_TRY(cudaFuncSetAttribute(k_fwd_level<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, ysm));
   TDEM_CUDA_TRY(cudaFuncSetAttribute(k_fwd_level<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, ysm));
   TDEM_CUDA_TRY(cudaFuncSetAttribute(k_fwd_level<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, ysm));

@@ -121,6 +121,28 @@ def test_pardiso_gpu_dense_front(pkg):
     pkg.pardiso_64(h, -1, a, ia, ja)
 
 
+@pytest.mark.parametrize("nrhs", [1, 2, 3, 8, 16, 31, 32, 64])
+def test_pardiso_gpu_block_solves(pkg, nrhs):
+    """All right-hand sides in one solve: the streaming level solves (1-2 columns)
+    and the tensor-pipe block kernels (3-64 columns) on a dense 1,300-pivot front
+    (chain, chunk and partial-sum paths) and on a sparse matrix (many fronts)."""
+    import scipy.sparse as sp
+    rng = np.random.default_rng(40 + nrhs)
+    n = 1300
+    G = rng.standard_normal((n, n))
+    Ad = G @ G.T / n + np.eye(n)
+    for A in (sp.csr_matrix(Ad), _spd(3000, 11)):
+        a, ia, ja = _upper(A)
+        h = np.zeros(64, dtype=np.int64)
+        assert pkg.pardiso_64(h, 12, a, ia, ja, nrhs=nrhs) == 0
+        b = rng.standard_normal((nrhs, A.shape[0]))
+        x = np.zeros_like(b)
+        assert pkg.pardiso_64(h, 33, a, ia, ja, nrhs=nrhs, b=b, x=x) == 0
+        xr = np.linalg.solve(A.toarray(), b.T).T
+        assert np.abs(x - xr).max() <= 1e-11 * np.abs(xr).max()
+        pkg.pardiso_64(h, -1, a, ia, ja)
+
+
 def test_pardiso_gpu_not_positive_definite(pkg):
     n = 400
     A = _spd(n, 9)
