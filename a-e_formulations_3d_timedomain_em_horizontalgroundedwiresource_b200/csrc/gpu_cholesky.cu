@@ -369,10 +369,11 @@ __global__ void __launch_bounds__(kBigThreads, 2) k_syrk_big(T* __restrict__ L, 
 }
 
 // FP64 trailing update on the FP64 tensor pipe (mma.sync m16n8k16 .f64): same
-// task list, tile split (two 128-thread CTAs per 128 x 128 tile, two CTAs per SM)
-// and cp.async double buffering as k_syrk_big, but each warp owns a 64 x 32 block
-// of its CTA's 128 x 64 tile as 4 x 4 MMA tiles, so one instruction does 2,048
-// multiply-adds instead of 32 and the issue slots stay free for the loads.
+// task list and tile split as k_syrk_big (two 128-thread CTAs per 128 x 128 tile,
+// two CTAs per SM), K streamed through kDStages cp.async stage buffers of KD
+// columns (three in flight), and each warp owns a 64 x 32 block of its CTA's
+// 128 x 64 tile as 4 x 4 MMA tiles, so one instruction does 2,048 multiply-adds
+// instead of 32 and the issue slots stay free for the loads.
 // Shared layouts are k-major with the row (column) stride padded to 4 mod 16
 // doubles.  A 64-bit shared access is served per half-warp; a fragment load's
 // half-warp reads 4 rows x 4 k, which this stride spreads over all 32 banks.
@@ -381,7 +382,9 @@ __global__ void __launch_bounds__(kBigThreads, 2) k_syrk_big(T* __restrict__ L, 
 constexpr int kLdA = kTileBig + 4;   // 132
 constexpr int kLdB = kBigCols + 4;   // 68
 constexpr int kLdC = kTileBig + 2;   // 130, epilogue tile columns (fits in the operand buffers)
-static_assert(kBigCols * kLdC <= 2 * KC * (kLdA + kLdB), "epilogue tile must fit the operand buffers");
+constexpr int KD = 16;               // K per stage of the tensor-pipe update (one k16 step)
+constexpr int kDStages = 4;          // stage buffers (three chunks in flight)
+static_assert(kBigCols * kLdC <= kDStages * KD * (kLdA + kLdB), "epilogue tile must fit the operand buffers");
 
 __device__ __forceinline__ void dmma16816(double (&c)[4], const double (&a)[8], const double (&b)[4]) {
   asm volatile(
@@ -404,28 +407,33 @@ __device__ __forceinline__ void dmma_tile(double* __restrict__ L, double* __rest
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, q = lane & 3;
   const int wr = (warp >> 1) * 64, wc = (warp & 1) * 32;  // warp block within the CTA tile
-  const int nch = (K + KC - 1) / KC;
+  const int nch = (K + KD - 1) / KD;
   const bool arow = r0 + tid < m;
   const int bi_row = tid & (TC - 1), bp0 = tid >> 6;
   const bool brow = c0 + bi_row < cend;
-  constexpr int kBuf = KC * (kLdA + kLdB);
+  constexpr int kBuf = KD * (kLdA + kLdB);
+  // chunk ch of K (KD columns) into stage buffer buf; commits one cp.async group
+  // (empty past the last chunk, which keeps the group count per iteration fixed)
   auto load_chunk = [&](int ch, int buf) {
-    double* As = sbuf + buf * kBuf;
-    double* Bs = As + KC * kLdA;
-    const int k0 = ch * KC, kc = min(KC, K - k0);
-#pragma unroll 8
-    for (int p = 0; p < KC; ++p) {
-      const bool ok = arow && p < kc;
-      const double* src = ok ? F + (r0 + tid) + (int64_t)(kb + k0 + p) * m : F;
-      cp_async_elem<8>(As + p * kLdA + tid, src, ok ? 8 : 0);
+    if (ch < nch) {
+      double* As = sbuf + buf * kBuf;
+      double* Bs = As + KD * kLdA;
+      const int k0 = ch * KD, kc = min(KD, K - k0);
+#pragma unroll
+      for (int p = 0; p < KD; ++p) {
+        const bool ok = arow && p < kc;
+        const double* src = ok ? F + (r0 + tid) + (int64_t)(kb + k0 + p) * m : F;
+        cp_async_elem<8>(As + p * kLdA + tid, src, ok ? 8 : 0);
+      }
+#pragma unroll
+      for (int j = 0; j < KD / 2; ++j) {
+        const int p = bp0 + 2 * j;
+        const bool ok = brow && p < kc;
+        const double* src = ok ? F + (c0 + bi_row) + (int64_t)(kb + k0 + p) * m : F;
+        cp_async_elem<8>(Bs + p * kLdB + bi_row, src, ok ? 8 : 0);
+      }
     }
-#pragma unroll 8
-    for (int j = 0; j < KC / 2; ++j) {
-      const int p = bp0 + 2 * j;
-      const bool ok = brow && p < kc;
-      const double* src = ok ? F + (c0 + bi_row) + (int64_t)(kb + k0 + p) * m : F;
-      cp_async_elem<8>(Bs + p * kLdB + bi_row, src, ok ? 8 : 0);
-    }
+    cp_async_commit();
   };
   double acc[4][4][4];
 #pragma unroll
@@ -434,35 +442,34 @@ __device__ __forceinline__ void dmma_tile(double* __restrict__ L, double* __rest
     for (int b = 0; b < 4; ++b)
 #pragma unroll
       for (int i = 0; i < 4; ++i) acc[a][b][i] = 0.0;
-  load_chunk(0, 0);
-  cp_async_commit();
+  // kDStages - 1 chunks in flight ahead of the one being multiplied; one barrier
+  // per chunk: after it every thread has finished the previous chunk, whose
+  // buffer is then refilled
+#pragma unroll
+  for (int st = 0; st < kDStages - 1; ++st) load_chunk(st, st);
   for (int ch = 0; ch < nch; ++ch) {
-    if (ch + 1 < nch) load_chunk(ch + 1, (ch + 1) & 1);
-    cp_async_commit();
-    cp_async_wait<1>();
+    cp_async_wait<kDStages - 2>();
     __syncthreads();
-    const double* As = sbuf + (ch & 1) * kBuf;
-    const double* Bs = As + KC * kLdA;
-    // zero-filled past K, so every chunk runs full k16 steps
-#pragma unroll 1
-    for (int k16 = 0; k16 < KC; k16 += 16) {
-      double bf[4][4];
+    load_chunk(ch + kDStages - 1, (ch + kDStages - 1) % kDStages);
+    const double* As = sbuf + (ch % kDStages) * kBuf;
+    const double* Bs = As + KD * kLdA;
+    // zero-filled past K, so every chunk is one full k16 step
+    double bf[4][4];
 #pragma unroll
-      for (int n = 0; n < 4; ++n)
+    for (int n = 0; n < 4; ++n)
 #pragma unroll
-        for (int i = 0; i < 4; ++i) bf[n][i] = Bs[(k16 + q + 4 * i) * kLdB + wc + 8 * n + g];
+      for (int i = 0; i < 4; ++i) bf[n][i] = Bs[(q + 4 * i) * kLdB + wc + 8 * n + g];
 #pragma unroll
-      for (int mt = 0; mt < 4; ++mt) {
-        double af[8];
+    for (int mt = 0; mt < 4; ++mt) {
+      double af[8];
 #pragma unroll
-        for (int i = 0; i < 8; ++i) af[i] = As[(k16 + q + 4 * (i >> 1)) * kLdA + wr + 16 * mt + g + 8 * (i & 1)];
+      for (int i = 0; i < 8; ++i) af[i] = As[(q + 4 * (i >> 1)) * kLdA + wr + 16 * mt + g + 8 * (i & 1)];
 #pragma unroll
-        for (int n = 0; n < 4; ++n) dmma16816(acc[mt][n], af, bf[n]);
-      }
+      for (int n = 0; n < 4; ++n) dmma16816(acc[mt][n], af, bf[n]);
     }
-    __syncthreads();
   }
   cp_async_wait_all();
+  __syncthreads();
   // Epilogue through shared memory (the operand buffers are free now): the tile's
   // old values arrive in one round of cp.async (row tid of every column), the
   // accumulators are subtracted in place, and each column goes back as one
@@ -1773,7 +1780,7 @@ template <class T>
 constexpr size_t syrk_smem() { return sizeof(T) * 2 * kTileSyrk * (P + 1); }
 template <class T>
 constexpr size_t big_smem() { return sizeof(T) * 2 * KC * (kTileBig + kBigCols); }
-constexpr size_t dmma_smem() { return sizeof(double) * 2 * KC * (kLdA + kLdB); }
+constexpr size_t dmma_smem() { return sizeof(double) * kDStages * KD * (kLdA + kLdB); }
 
 template <class T>
 std::string set_attributes() {
