@@ -196,21 +196,24 @@ def measured_peaks() -> dict:
 def cpu_baseline(cfg: str, spec, form: str, scheme: int, workdir: str, full_factorizations: int,
                  full_steps: int, threads: int) -> dict:
     """Times the reference's own CalcNonstat3DLine (built from source, oracle/_ref)
-    on a bounded sample of the same workload: the same mesh and matrices with the
-    time grid cut to its first 3 steps (one factorization).  The per-call wall
+    on a bounded sample of the same workload: the same variant, mesh and matrices
+    with the time grid cut to one factorization (the first 3 steps of the two-point
+    scheme; the first 2 of the three-point one, which takes them with the two-point
+    formula before its own).  The per-call wall
     times logged by the pardiso_64 stand-in split the run into set-up,
     factorization and per-step time, which are scaled to the full workload."""
     sys.path.insert(0, os.path.join(HERE, "oracle"))
     import run_ref  # noqa: E402  (oracle: baseline leg only)
     mg = importlib.import_module(PKG + ".modelgen")
-    variant = form + "2"
+    variant = form + str(scheme)  # the same variant as the GPU run
     if not run_ref.available("CalcNonstat3DLine_" + variant):
         return {"value": None, "unit": "forward solves/s", "cores": threads, "kind": "reference",
                 "sample": "unavailable: oracle/_ref not built"}
     import copy
     s2 = copy.deepcopy(spec)
-    s2.times = spec.times[:4]
-    s2.print_interval = (float(s2.times[1]), float(s2.times[3]))
+    cut = 4 if scheme == 2 else 3
+    s2.times = spec.times[:cut]
+    s2.print_interval = (float(s2.times[1]), float(s2.times[cut - 1]))
     mg.write_model(workdir, s2)
     mg.write_analytic_initial_field(workdir, s2)
     timing = os.path.join(workdir, "pardiso_calls.txt")
