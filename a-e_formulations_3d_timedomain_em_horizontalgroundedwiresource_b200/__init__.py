@@ -93,6 +93,16 @@ class TdemOptions(ctypes.Structure):
     ]
 
 
+class TdemPlanInfo(ctypes.Structure):
+    _fields_ = [("n_edges", ctypes.c_int64), ("n_interior", ctypes.c_int64), ("nnz_matrix", ctypes.c_int64),
+                ("nnz_factor", ctypes.c_int64), ("factor_flops", ctypes.c_double), ("device_bytes", ctypes.c_int64),
+                ("factor_slot_bytes", ctypes.c_int64), ("solve_units", ctypes.c_int64), ("n_fronts", ctypes.c_int),
+                ("tree_levels", ctypes.c_int), ("n_sources", ctypes.c_int), ("n_times", ctypes.c_int)]
+
+    def as_dict(self) -> dict:
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
 class TdemServerOptions(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("max_active", ctypes.c_int), ("prep_threads", ctypes.c_int),
                 ("hbm_budget_bytes", ctypes.c_int64)]
@@ -126,6 +136,7 @@ EXPORTED = [
     "tdem_stationary_directory",
     "tdem_solver_create",
     "tdem_solver_create_ex",
+    "tdem_solver_plan",
     "tdem_solver_run",
     "tdem_solver_write_outputs",
     "tdem_solver_results",
@@ -169,6 +180,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.tdem_solver_create_ex.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                           ctypes.POINTER(TdemOptions), ctypes.POINTER(P)]
     lib.tdem_solver_create_ex.restype = ctypes.c_int
+    lib.tdem_solver_plan.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(TdemOptions),
+                                     ctypes.POINTER(TdemPlanInfo), ctypes.c_char_p, ctypes.c_size_t]
+    lib.tdem_solver_plan.restype = ctypes.c_int
     for name in ("tdem_solver_run", "tdem_solver_write_outputs", "tdem_solver_cancel"):
         getattr(lib, name).argtypes = [P]
         getattr(lib, name).restype = ctypes.c_int
@@ -232,6 +246,21 @@ def stationary_directory(workdir: str, device: int = 0) -> None:
     st = lib.tdem_stationary_directory(os.fsencode(workdir), int(device), buf, len(buf))
     if st != 0:
         raise TdemError(st, buf.value.decode(errors="replace"))
+
+
+def plan(workdir: str, formulation="A", scheme: int = 2, precision: int = 64, leaf_size: int = 128,
+         factor_slots: int = 0) -> dict:
+    """Host-only planning of a forward solve (no GPU): sizes of the system and its
+    factor, factorization flops and the device memory a Solver would allocate."""
+    lib = load_library()
+    opts = TdemOptions(int(precision), 1e-10, 200, int(leaf_size), 0, int(factor_slots))
+    info = TdemPlanInfo()
+    buf = ctypes.create_string_buffer(2048)
+    st = lib.tdem_solver_plan(os.fsencode(workdir), _form(formulation), int(scheme), ctypes.byref(opts),
+                              ctypes.byref(info), buf, len(buf))
+    if st != 0:
+        raise TdemError(st, buf.value.decode(errors="replace"))
+    return info.as_dict()
 
 
 class Solver:

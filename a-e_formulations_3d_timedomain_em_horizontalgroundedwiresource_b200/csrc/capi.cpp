@@ -89,6 +89,50 @@ tdem_status tdem_solver_create_ex(const char* workdir, int formulation, int sche
   return st;
 }
 
+tdem_status tdem_solver_plan(const char* workdir, int formulation, int scheme, const tdem_options* opts,
+                             tdem_plan_info* out, char* err, size_t err_len) {
+  auto fail = [&](tdem_status st, const std::string& msg) {
+    if (err && err_len) {
+      std::strncpy(err, msg.c_str(), err_len - 1);
+      err[err_len - 1] = 0;
+    }
+    return st;
+  };
+  if (err && err_len) err[0] = 0;
+  if (!workdir || !out) return fail(TDEM_ERR_ARGUMENT, "null argument");
+  if ((formulation != 0 && formulation != 1) || (scheme != 2 && scheme != 3))
+    return fail(TDEM_ERR_ARGUMENT, "formulation must be 0 or 1 and scheme 2 or 3");
+  std::memset(out, 0, sizeof(*out));
+  tdem::RunOptions opt;
+  opt.formulation = formulation;
+  opt.scheme = scheme;
+  if (opts) {
+    if (opts->precision) opt.precision = opts->precision;
+    if (opts->leaf_size > 0) opt.leaf_size = opts->leaf_size;
+    if (opts->factor_slots < 0 || opts->factor_slots > 2) return fail(TDEM_ERR_ARGUMENT, "factor_slots out of range");
+    opt.factor_slots = opts->factor_slots;
+  }
+  if (opt.precision != 64 && opt.precision != 32) return fail(TDEM_ERR_ARGUMENT, "precision must be 64 or 32");
+  tdem::TransientSolve ts;
+  const std::string e = ts.plan(workdir, opt);
+  if (!e.empty()) return fail(classify(e), e);
+  const tdem::Symbolic* sy = ts.planned_symbolic();
+  const tdem::Model& m = ts.model();
+  out->n_edges = m.n_edges;
+  out->n_interior = ts.n_interior();
+  out->nnz_matrix = ts.nnz_full();
+  out->nnz_factor = sy->nnz_l;
+  out->factor_flops = sy->flops;
+  out->device_bytes = ts.device_bytes_needed();
+  out->factor_slot_bytes = tdem::GpuCholesky::slot_bytes(*sy, opt.precision == 32 ? 4 : 8);
+  out->solve_units = (int64_t)sy->solve_units.size() / tdem::kUnitInts;
+  out->n_fronts = (int)sy->fronts.size();
+  out->tree_levels = (int)sy->levels.size();
+  out->n_sources = m.npls;
+  out->n_times = (int)m.time.size();
+  return TDEM_OK;
+}
+
 tdem_status tdem_solver_run(tdem_solver* s) {
   if (!s) return TDEM_ERR_ARGUMENT;
   if (!s->prepared) return TDEM_ERR_STATE;

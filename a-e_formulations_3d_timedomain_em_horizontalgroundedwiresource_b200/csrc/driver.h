@@ -60,6 +60,8 @@ class TransientSolve {
   std::string plan(const std::string& dir, const RunOptions& opt);
   // Device bytes setup_device() will allocate (valid after plan()).
   int64_t device_bytes_needed() const;
+  // The analysis made by plan() (null before plan() and after setup_device()).
+  const Symbolic* planned_symbolic() const { return sy_.get(); }
   // Device half: allocations, uploads and assembly on `stream`.
   std::string setup_device(cudaStream_t stream);
   // Runs every time step of every decade.

@@ -120,6 +120,28 @@ tdem_status tdem_solver_create(const char* workdir, int formulation, int scheme,
 /* tdem_solver_create with options (opts may be NULL for the defaults). */
 tdem_status tdem_solver_create_ex(const char* workdir, int formulation, int scheme, int device,
                                   const tdem_options* opts, tdem_solver** out);
+/* Host-only planning of a forward solve: reads the inputs of `workdir` and analyses
+ * the sparsity pattern (nested-dissection ordering, assembly tree, launch plans,
+ * including the check that every level-solve unit waits only for units queued
+ * before it) without touching a GPU.  For sizing runs and admission decisions; no
+ * counterpart in the reference.  err (may be NULL) receives the message of a
+ * failure. */
+typedef struct tdem_plan_info {
+  int64_t n_edges;          /* unknowns incl. Dirichlet edges */
+  int64_t n_interior;       /* unknowns of the factorized system */
+  int64_t nnz_matrix;       /* entries of the full symmetric system pattern */
+  int64_t nnz_factor;       /* stored factor entries (dense front blocks) */
+  double factor_flops;      /* flops of one numeric factorization */
+  int64_t device_bytes;     /* device memory tdem_solver_create allocates with one factor slot */
+  int64_t factor_slot_bytes;/* device memory of one more factor slot */
+  int64_t solve_units;      /* level-solve units (forward + backward) */
+  int n_fronts;             /* fronts of the assembly tree */
+  int tree_levels;          /* levels of the assembly tree */
+  int n_sources;            /* right-hand-side columns per step */
+  int n_times;              /* time layers incl. t0 */
+} tdem_plan_info;
+tdem_status tdem_solver_plan(const char* workdir, int formulation, int scheme, const tdem_options* opts,
+                             tdem_plan_info* out, char* err, size_t err_len);
 /* Runs all decades / time steps (TaskSP.cpp:628-702, Three_Layers_Schema). */
 tdem_status tdem_solver_run(tdem_solver* s);
 /* Writes the reference output files into the model directory (Gather_edsall,

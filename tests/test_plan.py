@@ -1,0 +1,61 @@
+"""Host-only planning (tdem_solver_plan, no GPU): the input reading, nested
+dissection, assembly tree and launch plans of a forward solve, including the
+replay that every level-solve unit waits only for units queued before it, on
+models of several sizes, formulations and schemes."""
+import os
+
+import pytest
+
+
+def _counts_consistent(p):
+    assert 0 < p["n_interior"] < p["n_edges"]
+    # the factor holds at least the lower triangle of the interior system
+    assert p["nnz_factor"] >= (p["nnz_matrix"] * p["n_interior"] // p["n_edges"] + p["n_interior"]) // 2
+    assert p["device_bytes"] > 8 * p["nnz_factor"]
+    assert p["factor_slot_bytes"] >= 8 * p["nnz_factor"]
+    assert p["factor_flops"] > 0 and p["solve_units"] > 0
+    assert p["n_fronts"] > 0 and p["tree_levels"] >= 1
+
+
+@pytest.mark.parametrize("cells,form,scheme", [(8, "A", 2), (10, "E", 3), (14, "A", 3), (16, "E", 2)])
+def test_plan_small_models(pkg, mg, tmp_path, cells, form, scheme):
+    d = str(tmp_path / "m")
+    spec = mg.small_model(cells=cells, n_dec=2, steps_per_dec=4)
+    mg.write_model(d, spec)
+    mg.write_analytic_initial_field(d, spec)
+    p = pkg.plan(d, form, scheme)
+    _counts_consistent(p)
+    assert p["n_sources"] == 1
+    # leaf size changes the ordering but not the system
+    q = pkg.plan(d, form, scheme, leaf_size=48)
+    _counts_consistent(q)
+    assert (q["n_interior"], q["nnz_matrix"]) == (p["n_interior"], p["nnz_matrix"])
+
+
+def test_plan_two_wires_and_fp32(pkg, golden, tmp_path):
+    d = str(tmp_path / "m")
+    golden.write_case_inputs("cube8_two_wires", d)
+    p64 = pkg.plan(d, "A", 3)
+    assert p64["n_sources"] == 2
+    p32 = pkg.plan(d, "A", 3, precision=32)
+    # the FP32 factor halves the factor slot; the FP64 system copy for the CG is extra
+    assert p32["factor_slot_bytes"] * 2 == p64["factor_slot_bytes"]
+    assert p64["factor_flops"] == p32["factor_flops"]
+
+
+def test_plan_missing_input_is_an_input_error(pkg, golden, tmp_path):
+    d = str(tmp_path / "m")
+    golden.write_case_inputs("cube6", d)
+    os.unlink(os.path.join(d, "edges.dat"))
+    with pytest.raises(pkg.TdemError) as ei:
+        pkg.plan(d, "A", 2)
+    assert ei.value.status == 2 and "edges.dat" in str(ei.value)
+
+
+def test_plan_bad_arguments(pkg, tmp_path):
+    with pytest.raises(pkg.TdemError) as ei:
+        pkg.plan(str(tmp_path), "A", 4)
+    assert ei.value.status == 1
+    with pytest.raises(pkg.TdemError) as ei:
+        pkg.plan(str(tmp_path), "A", 2, factor_slots=3)
+    assert ei.value.status == 1
