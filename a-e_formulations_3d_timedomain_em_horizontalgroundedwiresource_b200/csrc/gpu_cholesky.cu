@@ -2069,8 +2069,7 @@ int64_t GpuCholesky::bytes_needed(const Symbolic& sy, int nrhs_max, int precisio
   int64_t b = el * (sy.u_elems + sy.wvec_elems * nr + sy.solve_partials * nr + sy.solve_slots * kPanel * nr);
   b += std::max(1, std::min(nslots, kMaxSlots)) * slot_bytes(sy, precision_bytes);
   b += 8 * (int64_t)(sy.l_off.size() + sy.u_off.size() + sy.wvec_off.size() + sy.entry_dst.size() +
-                     sy.rel_off.size() + sy.rows_off.size() + sy.task_prefix.size() + sy.flag_off.size() +
-                     sy.dinv_off.size());
+                     sy.rel_off.size() + sy.rows_off.size() + sy.task_prefix.size() + sy.dinv_off.size());
   b += 4 * (int64_t)(sy.front_m.size() + sy.front_k.size() + sy.rel.size() + sy.rows_all.size() + sy.tasks.size() +
                      sy.front_parent.size() + sy.front_c0.size() + sy.solve_items.size() + sy.solve_units.size() +
                      2 * sy.levels.size() + 2 * sy.n_flags + sy.n_counters + 4);
@@ -2113,7 +2112,6 @@ std::string GpuCholesky::setup(Symbolic&& sy, const std::vector<int>& perm_to_ve
   if (!(e = upload(&d_parent_, sy_.front_parent, s)).empty()) return e;
   if (!(e = upload(&d_c0_, sy_.front_c0, s)).empty()) return e;
   if (!(e = upload(&d_items_, sy_.solve_items, s)).empty()) return e;
-  if (!(e = upload(&d_flag_off_, sy_.flag_off, s)).empty()) return e;
   if (!(e = upload(&d_dinv_off_, sy_.dinv_off, s)).empty()) return e;
   if (!(e = upload(&d_units_, sy_.solve_units, s)).empty()) return e;
   if (!(e = alloc(&d_spart_, elem_ * std::max<int64_t>(1, sy_.solve_slots) * kPanel * nrhs_max_)).empty()) return e;

@@ -122,7 +122,6 @@ class GpuCholesky {
   int* d_err_ = nullptr;         // [0] first non-positive pivot, [1] level-solve wait gave up,
                                  // [2] tensor-core update wait gave up
   int* d_items_ = nullptr;       // solve / inversion items (front, block)
-  int64_t* d_flag_off_ = nullptr;
   int64_t* d_dinv_off_ = nullptr;
   void* d_dinv_[kMaxSlots] = {};  // inverted diagonal blocks per slot
   int* d_sync_ = nullptr;        // level tickets + pivot-block flags + row counters of one solve
