@@ -97,7 +97,8 @@ class TdemPlanInfo(ctypes.Structure):
     _fields_ = [("n_edges", ctypes.c_int64), ("n_interior", ctypes.c_int64), ("nnz_matrix", ctypes.c_int64),
                 ("nnz_factor", ctypes.c_int64), ("factor_flops", ctypes.c_double), ("device_bytes", ctypes.c_int64),
                 ("factor_slot_bytes", ctypes.c_int64), ("solve_units", ctypes.c_int64), ("n_fronts", ctypes.c_int),
-                ("tree_levels", ctypes.c_int), ("n_sources", ctypes.c_int), ("n_times", ctypes.c_int)]
+                ("tree_levels", ctypes.c_int), ("n_sources", ctypes.c_int), ("n_times", ctypes.c_int),
+                ("plan_seconds", ctypes.c_double), ("digest", ctypes.c_uint64)]
 
     def as_dict(self) -> dict:
         return {n: getattr(self, n) for n, _ in self._fields_}

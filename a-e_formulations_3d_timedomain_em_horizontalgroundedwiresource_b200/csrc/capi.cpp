@@ -130,6 +130,8 @@ tdem_status tdem_solver_plan(const char* workdir, int formulation, int scheme, c
   out->tree_levels = (int)sy->levels.size();
   out->n_sources = m.npls;
   out->n_times = (int)m.time.size();
+  out->plan_seconds = ts.times().setup_s;
+  out->digest = tdem::plan_digest(*sy);
   return TDEM_OK;
 }
 

@@ -1,8 +1,10 @@
 // Transient driver (see driver.h).
 #include "driver.h"
+#include "parallel.h"
 
 #include <algorithm>
 #include <chrono>
+#include <thread>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -127,76 +129,8 @@ std::string TransientSolve::prepare(const std::string& dir, const RunOptions& op
   return setup_device(stream);
 }
 
-std::string TransientSolve::plan(const std::string& dir, const RunOptions& opt) {
-  const double t0 = now_s();
-  opt_ = opt;
-  if (opt.formulation != 0 && opt.formulation != 1) return "formulation must be 0 (A) or 1 (E)";
-  if (opt.scheme != 2 && opt.scheme != 3) return "scheme must be 2 or 3";
-  std::string e = load_model(dir, m_);
-  if (!e.empty()) return e;
-  n_ = m_.n_edges;
-  npls_ = m_.npls;
-  ntime_ = (int)m_.time.size();
-
-  // printed layers (give_out_vec_loop.cpp:52-73)
-  tlf_ = tll_ = 2;
-  for (int i = 0; i < ntime_; ++i)
-    if (m_.time[i] >= m_.print_left) { tlf_ = i; break; }
-  if (tlf_ > ntime_ - 1) tlf_ = ntime_ - 1;
-  for (int i = 0; i < ntime_; ++i)
-    if (m_.time[i] >= m_.print_right - 1e-6) { tll_ = i; break; }
-  if (m_.print_right > m_.time[ntime_ - 1] - 1e-6) tll_ = ntime_ - 1;
-  if (tll_ - tlf_ < 2) return "fewer than three printed time layers";
-
-  // source
-  if (m_.fdirect) {
-    bool any = false;
-    for (int i = 1; i < ntime_; ++i) any = any || m_.currentfunction[i] != 0.0;
-    have_source_ = (opt.formulation == 1 || any) && m_.n_srs_razb > 0;
-    if (have_source_) {
-      e = locate_dipoles(m_);
-      if (!e.empty()) return e;
-    }
-  }
-  e = load_initial_field(m_, opt.formulation == 1, u0_);
-  if (!e.empty()) return e;
-
-  // patterns: full symmetric CSR over all edges, lower triangle of the interior system
-  edge_pattern(m_, rowptr_, col_);
-  std::vector<int> int_id(n_, -1), int_edge;
-  for (int i = 0; i < n_; ++i)
-    if (!m_.edge_bound[i]) {
-      int_id[i] = (int)int_edge.size();
-      int_edge.push_back(i);
-    }
-  n_int_ = (int64_t)int_edge.size();
-  if (n_int_ == 0) return "no interior edges";
-  std::vector<int64_t> lptr(n_int_ + 1, 0), src;
-  std::vector<int> lcol;
-  std::vector<uint8_t> diag;
-  std::vector<double> xyz((size_t)n_int_ * 3);
-  for (int64_t r = 0; r < n_int_; ++r) {
-    const int i = int_edge[r];
-    for (int64_t q = rowptr_[i]; q < rowptr_[i + 1]; ++q) {
-      const int j = col_[q];
-      if (int_id[j] >= 0 && int_id[j] <= r) {
-        lcol.push_back(int_id[j]);
-        src.push_back(q);
-        diag.push_back(int_id[j] == r);
-      }
-    }
-    lptr[r + 1] = (int64_t)lcol.size();
-    for (int a = 0; a < 3; ++a)
-      xyz[3 * r + a] = 0.5 * (m_.xyz[m_.edge_nodes[i][0]][a] + m_.xyz[m_.edge_nodes[i][1]][a]);
-  }
-  if (opt.precision != 64 && opt.precision != 32) return "precision must be 64 or 32";
-  sy_.reset(new Symbolic());
-  e = analyse((int)n_int_, lptr.data(), lcol.data(), xyz.data(), *sy_, opt.leaf_size);
-  if (!e.empty()) return "analysis: " + e;
-  p2v_.resize(n_int_);
-  for (int64_t p = 0; p < n_int_; ++p) p2v_[p] = int_edge[sy_->iperm[p]];
-  src_ = std::move(src);
-  diag_ = std::move(diag);
+std::string TransientSolve::build_sources_and_receivers() {
+  std::string e;
   // source vectors S[e, p] = sum over dipoles of basis . dl * 2 / edge length
   {
     std::vector<double>& S = S_;
@@ -230,6 +164,112 @@ std::string TransientSolve::plan(const std::string& dir, const RunOptions& opt) 
     e = build_receiver_operator(m_, m_.rec_e, owners(m_.rec_e_ig, (int)m_.rec_e.size()), false, rop_e_);
     if (!e.empty()) return e;
   }
+  return "";
+}
+
+std::string TransientSolve::plan(const std::string& dir, const RunOptions& opt) {
+  const double t0 = now_s();
+  opt_ = opt;
+  if (opt.formulation != 0 && opt.formulation != 1) return "formulation must be 0 (A) or 1 (E)";
+  if (opt.scheme != 2 && opt.scheme != 3) return "scheme must be 2 or 3";
+  std::string e = load_model(dir, m_);
+  if (!e.empty()) return e;
+  n_ = m_.n_edges;
+  npls_ = m_.npls;
+  ntime_ = (int)m_.time.size();
+
+  // printed layers (give_out_vec_loop.cpp:52-73)
+  tlf_ = tll_ = 2;
+  for (int i = 0; i < ntime_; ++i)
+    if (m_.time[i] >= m_.print_left) { tlf_ = i; break; }
+  if (tlf_ > ntime_ - 1) tlf_ = ntime_ - 1;
+  for (int i = 0; i < ntime_; ++i)
+    if (m_.time[i] >= m_.print_right - 1e-6) { tll_ = i; break; }
+  if (m_.print_right > m_.time[ntime_ - 1] - 1e-6) tll_ = ntime_ - 1;
+  if (tll_ - tlf_ < 2) return "fewer than three printed time layers";
+
+  // source
+  if (m_.fdirect) {
+    bool any = false;
+    for (int i = 1; i < ntime_; ++i) any = any || m_.currentfunction[i] != 0.0;
+    have_source_ = (opt.formulation == 1 || any) && m_.n_srs_razb > 0;
+    if (have_source_) {
+      e = locate_dipoles(m_);
+      if (!e.empty()) return e;
+    }
+  }
+  // the initial field, the source vectors and the receiver operators read only the
+  // model: they are built on a second thread while the patterns and the analysis run
+  std::string e_init, e_rec;
+  std::thread side([this, &opt, &e_init, &e_rec] {
+    e_init = load_initial_field(m_, opt.formulation == 1, u0_);
+    if (e_init.empty()) e_rec = build_sources_and_receivers();
+  });
+  struct Join {
+    std::thread& t;
+    ~Join() { if (t.joinable()) t.join(); }
+  } join{side};
+  auto main_error = [&](const std::string& err) {
+    side.join();
+    return e_init.empty() ? err : e_init;
+  };
+
+  // patterns: full symmetric CSR over all edges, lower triangle of the interior system
+  edge_pattern(m_, rowptr_, col_);
+  std::vector<int> int_id(n_, -1), int_edge;
+  for (int i = 0; i < n_; ++i)
+    if (!m_.edge_bound[i]) {
+      int_id[i] = (int)int_edge.size();
+      int_edge.push_back(i);
+    }
+  n_int_ = (int64_t)int_edge.size();
+  if (n_int_ == 0) return main_error("no interior edges");
+  // lower triangle of the interior system (rows independent: count, then fill)
+  std::vector<int64_t> lptr(n_int_ + 1, 0);
+  std::vector<double> xyz((size_t)n_int_ * 3);
+  parallel_ranges(n_int_, [&](int64_t r0, int64_t r1) {
+    for (int64_t r = r0; r < r1; ++r) {
+      const int i = int_edge[r];
+      int64_t c = 0;
+      for (int64_t q = rowptr_[i]; q < rowptr_[i + 1]; ++q) {
+        const int j = col_[q];
+        c += (int_id[j] >= 0 && int_id[j] <= r);
+      }
+      lptr[r + 1] = c;
+      for (int a = 0; a < 3; ++a)
+        xyz[3 * r + a] = 0.5 * (m_.xyz[m_.edge_nodes[i][0]][a] + m_.xyz[m_.edge_nodes[i][1]][a]);
+    }
+  });
+  for (int64_t r = 0; r < n_int_; ++r) lptr[r + 1] += lptr[r];
+  std::vector<int64_t> src(lptr[n_int_]);
+  std::vector<int> lcol(lptr[n_int_]);
+  std::vector<uint8_t> diag(lptr[n_int_]);
+  parallel_ranges(n_int_, [&](int64_t r0, int64_t r1) {
+    for (int64_t r = r0; r < r1; ++r) {
+      const int i = int_edge[r];
+      int64_t o = lptr[r];
+      for (int64_t q = rowptr_[i]; q < rowptr_[i + 1]; ++q) {
+        const int j = col_[q];
+        if (int_id[j] >= 0 && int_id[j] <= r) {
+          lcol[o] = int_id[j];
+          src[o] = q;
+          diag[o] = int_id[j] == r;
+          ++o;
+        }
+      }
+    }
+  });
+  if (opt.precision != 64 && opt.precision != 32) return main_error("precision must be 64 or 32");
+  sy_.reset(new Symbolic());
+  e = analyse((int)n_int_, lptr.data(), lcol.data(), xyz.data(), *sy_, opt.leaf_size);
+  if (!e.empty()) return main_error("analysis: " + e);
+  p2v_.resize(n_int_);
+  for (int64_t p = 0; p < n_int_; ++p) p2v_[p] = int_edge[sy_->iperm[p]];
+  src_ = std::move(src);
+  diag_ = std::move(diag);
+  side.join();
+  if (!e_init.empty()) return e_init;
+  if (!e_rec.empty()) return e_rec;
   pt_.setup_s = now_s() - t0;
   planned_ = true;
   return "";

@@ -144,6 +144,8 @@ class TransientSolve {
   std::string upload(T** d, const std::vector<T>& h);
   double* layer(int t) { return d_hist_ + (int64_t)(t % ring_) * n_ * npls_; }
   std::string factor_with(double mult, int slot, cudaStream_t s);
+  // source vectors and receiver operators of the planned model (reads the model only)
+  std::string build_sources_and_receivers();
   std::string step(int itime, int t1, int t2, double m1, double m2, double coef);
   void eval_receivers(int t);
   double source_coef(int itime, bool two_layer, double dt) const;

@@ -1,5 +1,6 @@
 // Readers for the reference's direct-mode input files (see model.h).
 #include "model.h"
+#include "parallel.h"
 
 #include <algorithm>
 #include <cmath>
@@ -257,36 +258,56 @@ std::string locate_dipoles(Model& m) {
       m.dipoles[i][j].dz = dz;
     }
   }
+  // every dipole goes to the first element (in element order) that holds it: each
+  // range of elements finds its first candidates, the lowest range wins
   const double lo = -1e-2, hi = 1.0 + 1e-2;
-  for (int e = 0; e < m.n_elem; ++e) {
-    double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
-    for (int k = 0; k < 8; ++k)
-      for (int a = 0; a < 3; ++a) {
-        mn[a] = std::min(mn[a], m.xyz[m.nver[e][k]][a]);
-        mx[a] = std::max(mx[a], m.xyz[m.nver[e][k]][a]);
-      }
+  const int nall = m.npls * nd;
+  auto local = [&](int e, const P& p, double l[3]) {
     const auto& p0 = m.xyz[m.nver[e][0]];
     const auto& p7 = m.xyz[m.nver[e][7]];
-    for (int i = 0; i < m.npls; ++i)
-      for (int j = 0; j < nd; ++j) {
-        Dipole& d = m.dipoles[i][j];
-        if (d.elem != -1) continue;
-        const P& p = pos[i][j];
-        if (p.x < mn[0] - 1e-3 || p.x > mx[0] + 1e-3 || p.y < mn[1] - 1e-3 || p.y > mx[1] + 1e-3 ||
-            p.z < mn[2] - 1e-3 || p.z > mx[2] + 1e-3)
-          continue;
-        // local coordinates on the axis-aligned brick spanned by nodes 0 and 7
-        const double l0 = (p.x - p0[0]) / (p7[0] - p0[0]);
-        const double l1 = (p.y - p0[1]) / (p7[1] - p0[1]);
-        const double l2 = (p.z - p0[2]) / (p7[2] - p0[2]);
-        if (l0 > lo && l0 < hi && l1 > lo && l1 < hi && l2 > lo && l2 < hi) {
-          d.elem = e;
-          d.ksi = l0;
-          d.eta = l1;
-          d.zeta = l2;
+    // local coordinates on the axis-aligned brick spanned by nodes 0 and 7
+    l[0] = (p.x - p0[0]) / (p7[0] - p0[0]);
+    l[1] = (p.y - p0[1]) / (p7[1] - p0[1]);
+    l[2] = (p.z - p0[2]) / (p7[2] - p0[2]);
+  };
+  const int nt = chunk_count(m.n_elem, 16384);
+  std::vector<int> found((size_t)nt * nall, -1);
+  parallel_chunks(m.n_elem, nt, [&](int t, int64_t e0, int64_t e1) {
+    int* fnd = found.data() + (size_t)t * nall;
+    for (int e = (int)e0; e < (int)e1; ++e) {
+      double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
+      for (int k = 0; k < 8; ++k)
+        for (int a = 0; a < 3; ++a) {
+          mn[a] = std::min(mn[a], m.xyz[m.nver[e][k]][a]);
+          mx[a] = std::max(mx[a], m.xyz[m.nver[e][k]][a]);
         }
+      for (int i = 0; i < m.npls; ++i)
+        for (int j = 0; j < nd; ++j) {
+          if (fnd[i * nd + j] != -1) continue;
+          const P& p = pos[i][j];
+          if (p.x < mn[0] - 1e-3 || p.x > mx[0] + 1e-3 || p.y < mn[1] - 1e-3 || p.y > mx[1] + 1e-3 ||
+              p.z < mn[2] - 1e-3 || p.z > mx[2] + 1e-3)
+            continue;
+          double l[3];
+          local(e, p, l);
+          if (l[0] > lo && l[0] < hi && l[1] > lo && l[1] < hi && l[2] > lo && l[2] < hi) fnd[i * nd + j] = e;
+        }
+    }
+  });
+  for (int i = 0; i < m.npls; ++i)
+    for (int j = 0; j < nd; ++j)
+      for (int t = 0; t < nt; ++t) {
+        const int e = found[(size_t)t * nall + i * nd + j];
+        if (e < 0) continue;
+        Dipole& d = m.dipoles[i][j];
+        double l[3];
+        local(e, pos[i][j], l);
+        d.elem = e;
+        d.ksi = l[0];
+        d.eta = l[1];
+        d.zeta = l[2];
+        break;
       }
-  }
   for (int i = 0; i < m.npls; ++i)
     for (int j = 0; j < nd; ++j)
       if (m.dipoles[i][j].elem < 0) return "source dipole outside the mesh";
@@ -344,26 +365,43 @@ std::string load_initial_field(const Model& m, bool eform, std::vector<double>& 
 
 void edge_pattern(const Model& m, std::vector<int64_t>& rowptr, std::vector<int>& col) {
   const int n = m.n_edges;
-  // each edge touches at most 4 elements with 12 edges each
-  std::vector<int64_t> cnt(n + 1, 0);
+  // elements of every edge (ascending), then each row gathers the 12 edges of each
+  // of its elements (at most 4 x 12), sorts and deduplicates them
+  std::vector<int64_t> eptr(n + 1, 0);
   for (int e = 0; e < m.n_elem; ++e)
-    for (int i = 0; i < 12; ++i) cnt[m.ed[e][i] + 1] += 12;
-  for (int i = 0; i < n; ++i) cnt[i + 1] += cnt[i];
-  std::vector<int> tmp(cnt[n]);
-  std::vector<int64_t> fill(cnt.begin(), cnt.end() - 1);
-  for (int e = 0; e < m.n_elem; ++e)
-    for (int i = 0; i < 12; ++i)
-      for (int j = 0; j < 12; ++j) tmp[fill[m.ed[e][i]]++] = m.ed[e][j];
-  rowptr.assign(n + 1, 0);
-  col.clear();
-  col.reserve(cnt[n] / 2);
-  for (int i = 0; i < n; ++i) {
-    auto b = tmp.begin() + cnt[i], en = tmp.begin() + fill[i];
-    std::sort(b, en);
-    auto u = std::unique(b, en);
-    col.insert(col.end(), b, u);
-    rowptr[i + 1] = (int64_t)col.size();
+    for (int i = 0; i < 12; ++i) ++eptr[m.ed[e][i] + 1];
+  for (int i = 0; i < n; ++i) eptr[i + 1] += eptr[i];
+  std::vector<int> elems(eptr[n]);
+  {
+    std::vector<int64_t> fill(eptr.begin(), eptr.end() - 1);
+    for (int e = 0; e < m.n_elem; ++e)
+      for (int i = 0; i < 12; ++i) elems[fill[m.ed[e][i]]++] = e;
   }
+  // two passes (row lengths, then the rows), so no buffer of all gathered edges
+  auto row = [&](int64_t i, std::vector<int>& buf) {
+    buf.clear();
+    for (int64_t q = eptr[i]; q < eptr[i + 1]; ++q)
+      for (int j = 0; j < 12; ++j) buf.push_back(m.ed[elems[q]][j]);
+    std::sort(buf.begin(), buf.end());
+    buf.erase(std::unique(buf.begin(), buf.end()), buf.end());
+  };
+  rowptr.assign(n + 1, 0);
+  parallel_ranges(n, [&](int64_t r0, int64_t r1) {
+    std::vector<int> buf;
+    for (int64_t i = r0; i < r1; ++i) {
+      row(i, buf);
+      rowptr[i + 1] = (int64_t)buf.size();
+    }
+  });
+  for (int i = 0; i < n; ++i) rowptr[i + 1] += rowptr[i];
+  col.assign(rowptr[n], 0);
+  parallel_ranges(n, [&](int64_t r0, int64_t r1) {
+    std::vector<int> buf;
+    for (int64_t i = r0; i < r1; ++i) {
+      row(i, buf);
+      std::copy(buf.begin(), buf.end(), col.begin() + rowptr[i]);
+    }
+  });
 }
 
 }  // namespace tdem

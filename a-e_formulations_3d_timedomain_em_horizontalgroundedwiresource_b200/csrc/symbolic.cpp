@@ -1,12 +1,14 @@
 // Host symbolic analysis: nested-dissection ordering, assembly tree, and the
 // flattened maps / task lists consumed by the GPU factorization and solves.
 #include "symbolic.h"
+#include "parallel.h"
 
 #include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <climits>
 #include <numeric>
+#include <thread>
 
 namespace tdem {
 namespace {
@@ -18,16 +20,38 @@ struct Graph {
 };
 
 // Recursive dissection producing fronts in postorder.
+// The two halves of a split near the top of the tree are dissected on separate
+// threads, each by its own Dissector (own marks and stamps); the right half's
+// nodes are then appended after the left half's, which is the serial postorder,
+// so the ordering does not depend on the threading.
 class Dissector {
  public:
   Dissector(const Graph& g, const double* xyz, int leaf)
-      : g_(g), xyz_(xyz), leaf_(leaf), mark_(g.n, 0), vis_(g.n, 0) {}
+      : g_(g), xyz_(xyz), leaf_(leaf), mark_(g.n, 0), vis_(g.n, 0) {
+    // rank of every coordinate among the distinct values of its axis: the splits
+    // then count values instead of sorting them (same order, same cuts)
+    if (xyz_) {
+      own_rank_.resize(3 * (size_t)g.n);
+      parallel_ranges(3, [&](int64_t a0, int64_t a1) {
+        for (int a = (int)a0; a < (int)a1; ++a) {
+          std::vector<double> vals(g.n);
+          for (int v = 0; v < g.n; ++v) vals[v] = c(v, a);
+          std::sort(vals.begin(), vals.end());
+          vals.erase(std::unique(vals.begin(), vals.end()), vals.end());
+          for (int v = 0; v < g.n; ++v)
+            own_rank_[3 * (size_t)v + a] = (int)(std::lower_bound(vals.begin(), vals.end(), c(v, a)) - vals.begin());
+        }
+      }, 1);
+      grank_ = own_rank_.data();
+    }
+  }
 
   std::vector<int> order;  // new -> old
   struct Node { int c0, c1; std::vector<int> kids; };
   std::vector<Node> nodes;
 
-  int build(std::vector<int>& verts) {
+  // depth: splits still allowed to fork a thread below this call
+  int build(std::vector<int>& verts, int depth = 3) {
     if ((int)verts.size() <= leaf_) return emit(verts, {});
     std::vector<int> L, S, R;
     int kind = 0;
@@ -36,17 +60,46 @@ class Dissector {
     if (!kind) return emit(verts, {});
     std::vector<int>().swap(verts);
     std::vector<int> kids;
-    if (!L.empty()) kids.push_back(build(L));
-    if (!R.empty()) kids.push_back(build(R));
+    if (depth > 0 && L.size() >= kForkMin && R.size() >= kForkMin) {
+      Dissector right(*this);
+      int rroot = -1;
+      std::thread t([&] { rroot = right.build(R, depth - 1); });
+      kids.push_back(build(L, depth - 1));
+      t.join();
+      kids.push_back(append(right, rroot));
+    } else {
+      if (!L.empty()) kids.push_back(build(L, depth - 1));
+      if (!R.empty()) kids.push_back(build(R, depth - 1));
+    }
     return emit(S, std::move(kids));
   }
 
  private:
+  static constexpr size_t kForkMin = 20000;
   const Graph& g_;
   const double* xyz_;
   int leaf_;
   std::vector<int> mark_, vis_;
+  std::vector<int> own_rank_;
+  const int* grank_ = nullptr;  // per vertex and axis: rank of the coordinate
+  std::vector<int> cnt_[3];
   int stamp_ = 0;
+
+  // a dissector for a disjoint part of the same graph, sharing the coordinate ranks
+  Dissector(const Dissector& o)
+      : g_(o.g_), xyz_(o.xyz_), leaf_(o.leaf_), mark_(o.g_.n, 0), vis_(o.g_.n, 0), grank_(o.grank_) {}
+
+  // appends another dissector's nodes (postorder, renumbered); returns its root's index
+  int append(const Dissector& o, int root) {
+    const int nb = (int)nodes.size(), cb = (int)order.size();
+    order.insert(order.end(), o.order.begin(), o.order.end());
+    for (const Node& x : o.nodes) {
+      Node nd{x.c0 + cb, x.c1 + cb, x.kids};
+      for (int& k : nd.kids) k += nb;
+      nodes.push_back(std::move(nd));
+    }
+    return root + nb;
+  }
 
   int emit(const std::vector<int>& verts, std::vector<int> kids) {
     Node nd;
@@ -59,6 +112,7 @@ class Dissector {
   }
 
   double c(int v, int a) const { return xyz_[3 * (int64_t)v + a]; }
+  int rank(int v, int a) const { return grank_[3 * (size_t)v + a]; }
 
   // Cut perpendicular to the axis with the most distinct positions, at the most
   // populated coordinate value inside the central 30 % (a node plane on a
@@ -67,50 +121,62 @@ class Dissector {
   bool split_coords(const std::vector<int>& verts, std::vector<int>& L, std::vector<int>& S,
                     std::vector<int>& R) {
     const size_t nv = verts.size();
-    std::vector<double> vals(nv);
-    int ndist[3];
+    // per axis: histogram of the coordinate ranks over [lo, hi]
+    int ndist[3], lo[3];
     for (int a = 0; a < 3; ++a) {
-      for (size_t i = 0; i < nv; ++i) vals[i] = c(verts[i], a);
-      std::sort(vals.begin(), vals.end());
-      ndist[a] = (int)(std::unique(vals.begin(), vals.end()) - vals.begin());
+      int l = INT_MAX, h = -1;
+      for (int v : verts) {
+        const int r = rank(v, a);
+        l = std::min(l, r);
+        h = std::max(h, r);
+      }
+      lo[a] = l;
+      std::vector<int>& cnt = cnt_[a];
+      cnt.assign((size_t)(h - l + 1), 0);
+      for (int v : verts) ++cnt[rank(v, a) - l];
+      ndist[a] = (int)(cnt.size() - std::count(cnt.begin(), cnt.end(), 0));
     }
     int axes[3] = {0, 1, 2};
     std::sort(axes, axes + 3, [&](int a, int b) { return ndist[a] > ndist[b]; });
     for (int ai = 0; ai < 3; ++ai) {
       const int a = axes[ai];
       if (ndist[a] < 3) continue;
-      for (size_t i = 0; i < nv; ++i) vals[i] = c(verts[i], a);
-      std::sort(vals.begin(), vals.end());
+      // runs of equal values in sorted order: rank lo + idx occupies positions
+      // [s0, s0 + cnt[idx]); the window starts at q0 (possibly inside a run)
       const size_t q0 = nv * 35 / 100, q1 = std::max(q0 + 1, nv * 65 / 100);
-      double cut = vals[nv / 2];
-      size_t best = 0;
+      const std::vector<int>& cnt = cnt_[a];
+      int cut = -1;
+      size_t best = 0, pos = 0;
       double bestd = 1e300;
-      for (size_t i = q0; i < q1;) {
-        size_t j = i;
-        while (j < nv && vals[j] == vals[i]) ++j;
+      for (size_t idx = 0; idx < cnt.size(); ++idx) {
+        if (!cnt[idx]) continue;
+        const size_t s0 = pos, e0 = pos + (size_t)cnt[idx];
+        pos = e0;
+        if (e0 <= q0) continue;
+        const size_t i = std::max(s0, q0), j = e0;
+        if (i >= q1) break;
         const double d = std::fabs(0.5 * (double)(i + j) - 0.5 * (double)nv);
         if (j - i > best || (j - i == best && d < bestd)) {
           best = j - i;
           bestd = d;
-          cut = vals[i];
+          cut = lo[a] + (int)idx;
         }
-        i = j;
       }
-      if (cut <= vals.front()) continue;
+      if (cut <= lo[a]) continue;
       ++stamp_;
       for (int v : verts) mark_[v] = stamp_;
       L.clear();
       S.clear();
       R.clear();
       for (int v : verts) {
-        if (c(v, a) < cut) {
+        if (rank(v, a) < cut) {
           L.push_back(v);
           continue;
         }
         bool touch = false;
         for (int64_t p = g_.xadj[v]; p < g_.xadj[v + 1] && !touch; ++p) {
           const int u = g_.adj[p];
-          touch = (mark_[u] == stamp_ && c(u, a) < cut);
+          touch = (mark_[u] == stamp_ && rank(u, a) < cut);
         }
         (touch ? S : R).push_back(v);
       }
@@ -355,31 +421,63 @@ std::string analyse(int n, const int64_t* rowptr, const int* colind, const doubl
         return "internal error: root front with off-diagonal rows";
   }
 
-  // entry map: lower-CSR entry -> front element
+  // entry map: lower-CSR entry -> front element.  Entries are bucketed by front
+  // (counting sort, keeping each entry's row), then placed front by front.
   {
     sy.entry_dst.assign(sy.nnz_lower, -1);
-    std::vector<int> pos(n, -1);
-    std::vector<std::vector<int64_t>> per_front(nf);
-    for (int i = 0; i < n; ++i)
-      for (int64_t q = rowptr[i]; q < rowptr[i + 1]; ++q) {
-        const int a = sy.perm[i], b = sy.perm[colind[q]];
-        per_front[colfront[std::min(a, b)]].push_back(q);
-      }
+    // per row range: count its entries of every front, then place them after the
+    // entries of the lower ranges (the order inside a front is the serial one)
+    const int nt = chunk_count(n, 16384);
+    std::vector<int64_t> hist((size_t)nt * nf, 0), fstart(nf + 1, 0);
+    parallel_chunks(n, nt, [&](int t, int64_t i0, int64_t i1) {
+      int64_t* h = hist.data() + (size_t)t * nf;
+      for (int64_t i = i0; i < i1; ++i)
+        for (int64_t q = rowptr[i]; q < rowptr[i + 1]; ++q) ++h[colfront[std::min(sy.perm[i], sy.perm[colind[q]])]];
+    });
     for (int s = 0; s < nf; ++s) {
-      const FrontInfo& f = sy.fronts[s];
-      for (int cc = f.c0; cc < f.c1; ++cc) pos[cc] = cc - f.c0;
-      for (size_t t = 0; t < f.rows.size(); ++t) pos[f.rows[t]] = f.k() + (int)t;
-      const int64_t m = f.m();
-      // find the row of q: binary search in rowptr
-      for (int64_t q : per_front[s]) {
-        const int i = (int)(std::upper_bound(rowptr, rowptr + n + 1, q) - rowptr) - 1;
-        const int a = sy.perm[i], b = sy.perm[colind[q]];
-        const int col = std::min(a, b), row = std::max(a, b);
-        const int lr = pos[row], lc = col - f.c0;
-        if (lr < 0 || lc < 0 || lc >= f.k() || lr < lc) return "internal error: entry outside its front";
-        sy.entry_dst[q] = sy.l_off[s] + lr + (int64_t)lc * m;
+      int64_t acc = fstart[s];
+      for (int t = 0; t < nt; ++t) {
+        const int64_t c = hist[(size_t)t * nf + s];
+        hist[(size_t)t * nf + s] = acc;
+        acc += c;
       }
+      fstart[s + 1] = acc;
     }
+    std::vector<int64_t> eq(sy.nnz_lower);
+    std::vector<int> er(sy.nnz_lower);
+    parallel_chunks(n, nt, [&](int t, int64_t i0, int64_t i1) {
+      int64_t* fill = hist.data() + (size_t)t * nf;
+      for (int64_t i = i0; i < i1; ++i)
+        for (int64_t q = rowptr[i]; q < rowptr[i + 1]; ++q) {
+          const int64_t at = fill[colfront[std::min(sy.perm[i], sy.perm[colind[q]])]]++;
+          eq[at] = q;
+          er[at] = (int)i;
+        }
+    });
+    // fronts in parallel, each thread with its own row -> slot map
+    std::vector<char> bad(host_threads() + 1, 0);
+    parallel_ranges(nf, [&](int64_t s0, int64_t s1) {
+      std::vector<int> pos(n, -1);
+      for (int64_t s = s0; s < s1; ++s) {
+        const FrontInfo& f = sy.fronts[s];
+        for (int cc = f.c0; cc < f.c1; ++cc) pos[cc] = cc - f.c0;
+        for (size_t t = 0; t < f.rows.size(); ++t) pos[f.rows[t]] = f.k() + (int)t;
+        const int64_t m = f.m();
+        for (int64_t t = fstart[s]; t < fstart[s + 1]; ++t) {
+          const int64_t q = eq[t];
+          const int i = er[t];
+          const int a = sy.perm[i], b = sy.perm[colind[q]];
+          const int col = std::min(a, b), row = std::max(a, b);
+          const int lr = pos[row], lc = col - f.c0;
+          if (lr < 0 || lc < 0 || lc >= f.k() || lr < lc) {
+            bad[0] = 1;
+            return;
+          }
+          sy.entry_dst[q] = sy.l_off[s] + lr + (int64_t)lc * m;
+        }
+      }
+    }, 64);
+    if (bad[0]) return "internal error: entry outside its front";
   }
 
   // level plans
@@ -675,6 +773,26 @@ std::string analyse(int n, const int64_t* rowptr, const int* colind, const doubl
     sy.u_elems = peak;
   }
   return "";
+}
+
+uint64_t plan_digest(const Symbolic& sy) {
+  uint64_t h = 1469598103934665603ull;
+  auto word = [&](uint64_t u) {
+    for (int b = 0; b < 8; ++b) h = (h ^ ((u >> (8 * b)) & 0xff)) * 1099511628211ull;
+  };
+  auto ints = [&](const auto& v) {
+    word(v.size());
+    for (auto x : v) word((uint64_t)(int64_t)x);
+  };
+  ints(sy.perm);
+  for (const FrontInfo& f : sy.fronts) {
+    word((uint64_t)f.c0);
+    word((uint64_t)f.c1);
+    ints(f.rows);
+  }
+  ints(sy.entry_dst);
+  ints(sy.solve_units);
+  return h;
 }
 
 }  // namespace tdem

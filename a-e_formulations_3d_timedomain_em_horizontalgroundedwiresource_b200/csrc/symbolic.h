@@ -127,6 +127,10 @@ struct Symbolic {
 // Analyse the lower triangle (row i holds columns j <= i, diagonal included)
 // of a symmetric n x n matrix.  coords (n x 3) are optional unknown positions.
 // Returns an empty string on success, an error message otherwise.
+// FNV-1a hash of the ordering, the fronts' columns and rows, the entry map and the
+// level-solve units (equal hashes: identical factorization and solve launches)
+uint64_t plan_digest(const Symbolic& sy);
+
 std::string analyse(int n, const int64_t* rowptr, const int* colind, const double* coords,
                     Symbolic& out, int leaf_size = 128);
 

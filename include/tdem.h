@@ -139,6 +139,9 @@ typedef struct tdem_plan_info {
   int tree_levels;          /* levels of the assembly tree */
   int n_sources;            /* right-hand-side columns per step */
   int n_times;              /* time layers incl. t0 */
+  double plan_seconds;      /* host time of the planning (inputs, patterns, analysis) */
+  uint64_t digest;          /* hash of the elimination order, the fronts, the entry map and the
+                               solve units: equal digests mean identical launch plans */
 } tdem_plan_info;
 tdem_status tdem_solver_plan(const char* workdir, int formulation, int scheme, const tdem_options* opts,
                              tdem_plan_info* out, char* err, size_t err_len);

@@ -59,3 +59,22 @@ def test_plan_bad_arguments(pkg, tmp_path):
     with pytest.raises(pkg.TdemError) as ei:
         pkg.plan(str(tmp_path), "A", 2, factor_slots=3)
     assert ei.value.status == 1
+
+
+def test_plan_digest_independent_of_host_threads(pkg, mg, tmp_path, monkeypatch):
+    # large enough that the dissection forks and every parallel pass cuts several ranges
+    d = str(tmp_path / "m")
+    spec = mg.small_model(cells=28, n_dec=2, steps_per_dec=4)
+    mg.write_model(d, spec)
+    mg.write_analytic_initial_field(d, spec)
+    digests = {}
+    for t in ("1", "3", "8"):
+        monkeypatch.setenv("TDEM_HOST_THREADS", t)
+        p = pkg.plan(d, "E", 2)
+        _counts_consistent(p)
+        assert p["plan_seconds"] > 0
+        digests[t] = p["digest"]
+    assert p["n_interior"] > 40000
+    assert len(set(digests.values())) == 1, digests
+    # the digest does see a different ordering
+    assert pkg.plan(d, "E", 2, leaf_size=48)["digest"] != digests["1"]
