@@ -135,6 +135,8 @@ _lib: Optional[ctypes.CDLL] = None
 EXPORTED = [
     "tdem_run_directory",
     "tdem_stationary_directory",
+    "tdem_sum_nonstat_3d_only",
+    "tdem_summator_edmn",
     "tdem_solver_create",
     "tdem_solver_create_ex",
     "tdem_solver_plan",
@@ -175,6 +177,11 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.tdem_run_directory.restype = ctypes.c_int
     lib.tdem_stationary_directory.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t]
     lib.tdem_stationary_directory.restype = ctypes.c_int
+    lib.tdem_sum_nonstat_3d_only.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_size_t]
+    lib.tdem_sum_nonstat_3d_only.restype = ctypes.c_int
+    lib.tdem_summator_edmn.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_char_p,
+                                       ctypes.c_size_t]
+    lib.tdem_summator_edmn.restype = ctypes.c_int
     lib.tdem_solver_create.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                        ctypes.POINTER(P)]
     lib.tdem_solver_create.restype = ctypes.c_int
@@ -245,6 +252,26 @@ def stationary_directory(workdir: str, device: int = 0) -> None:
     lib = load_library()
     buf = ctypes.create_string_buffer(2048)
     st = lib.tdem_stationary_directory(os.fsencode(workdir), int(device), buf, len(buf))
+    if st != 0:
+        raise TdemError(st, buf.value.decode(errors="replace"))
+
+
+def sum_nonstat_3d_only(workdir: str) -> None:
+    """Drop-in run of SumNonstat3DOnly in workdir (host only): the per-component
+    files Bxall.N .. Ezall.N from ball_anom.N, edsall_anom.N and eall_anom.N."""
+    lib = load_library()
+    buf = ctypes.create_string_buffer(2048)
+    st = lib.tdem_sum_nonstat_3d_only(os.fsencode(workdir), buf, len(buf))
+    if st != 0:
+        raise TdemError(st, buf.value.decode(errors="replace"))
+
+
+def summator_edmn(workdir: str, with_ddv: bool, profile: int, place: int) -> None:
+    """Drop-in run of SummatorEDMN in workdir (host only): line voltages
+    edmnall<profile>_<place> (and edmoonall.. with with_ddv)."""
+    lib = load_library()
+    buf = ctypes.create_string_buffer(2048)
+    st = lib.tdem_summator_edmn(os.fsencode(workdir), int(bool(with_ddv)), int(profile), int(place), buf, len(buf))
     if st != 0:
         raise TdemError(st, buf.value.decode(errors="replace"))
 

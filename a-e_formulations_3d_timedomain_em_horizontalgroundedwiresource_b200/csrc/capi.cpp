@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "driver.h"
+#include "postprocess.h"
 #include "gpu_cholesky.h"
 #include "server.h"
 #include "stationary.h"
@@ -352,6 +353,21 @@ tdem_status tdem_server_stats_get(tdem_server* srv, tdem_server_stats* st) {
 }
 
 void tdem_server_destroy(tdem_server* srv) { delete srv; }
+
+tdem_status tdem_sum_nonstat_3d_only(const char* workdir, char* errbuf, size_t errlen) {
+  if (!workdir) return TDEM_ERR_ARGUMENT;
+  const std::string e = tdem::split_components(workdir);
+  put_err(errbuf, errlen, e);
+  return e.empty() ? TDEM_OK : TDEM_ERR_INPUT;
+}
+
+tdem_status tdem_summator_edmn(const char* workdir, int with_ddv, int profile, int place, char* errbuf,
+                               size_t errlen) {
+  if (!workdir) return TDEM_ERR_ARGUMENT;
+  const std::string e = tdem::line_voltages(workdir, with_ddv != 0, profile, place);
+  put_err(errbuf, errlen, e);
+  return e.empty() ? TDEM_OK : TDEM_ERR_INPUT;
+}
 
 tdem_status tdem_stationary_directory(const char* workdir, int device, char* errbuf, size_t errlen) {
   if (!workdir) return TDEM_ERR_ARGUMENT;

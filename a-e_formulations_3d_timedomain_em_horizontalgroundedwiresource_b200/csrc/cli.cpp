@@ -10,6 +10,14 @@
 // Installed under a name containing CalcStat3D (or run with --stationary) it is
 // the drop-in for CalcStat3D_3T_A instead: the stationary initial field
 // (v3n.dat, v3a.dat, a0.dat) of the model in workdir.
+//
+// Installed under a name containing SumNonstat3DOnly (or run with
+// --sum-nonstat-3d-only [workdir]) it is the drop-in for that module: the
+// per-component files of the results in workdir (default the current directory,
+// where GeoCalculatorSP.cpp:1673 runs it).  Installed under a name containing
+// SummatorEDMN (or run with --summator-edmn) it takes that module's command line,
+//   SummatorEDMN WithDDV profile place [--dir workdir]
+// (SummatorEDMN/main.cpp:253-294) and writes the line voltages.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -17,7 +25,52 @@
 
 #include "../../include/tdem.h"
 
+namespace {
+
+// SumNonstat3DOnly [workdir] / SummatorEDMN WithDDV profile place [--dir workdir]
+int post_main(bool summator, int argc, char** argv, int first) {
+  std::string dir = ".";
+  const char* pos[3] = {nullptr, nullptr, nullptr};
+  int npos = 0;
+  for (int i = first; i < argc; ++i) {
+    if (!strcmp(argv[i], "--dir") && i + 1 < argc) {
+      dir = argv[++i];
+    } else if (summator && npos < 3) {
+      pos[npos++] = argv[i];
+    } else if (!summator && argv[i][0] != '-') {
+      dir = argv[i];
+    } else {
+      fprintf(stderr, summator ? "usage: %s WithDDV profile place [--dir workdir]\n" : "usage: %s [workdir]\n",
+              argv[0]);
+      return (int)TDEM_ERR_ARGUMENT;
+    }
+  }
+  char err[1024] = {0};
+  tdem_status st;
+  if (summator) {
+    if (npos < 3) {
+      fprintf(stderr, "usage: %s WithDDV profile place [--dir workdir]\n", argv[0]);
+      return (int)TDEM_ERR_ARGUMENT;
+    }
+    st = tdem_summator_edmn(dir.c_str(), atoi(pos[0]), atoi(pos[1]), atoi(pos[2]), err, sizeof err);
+    if (st != TDEM_OK) fprintf(stderr, "SummatorEDMN: %s\n", err);
+  } else {
+    st = tdem_sum_nonstat_3d_only(dir.c_str(), err, sizeof err);
+    if (st != TDEM_OK) fprintf(stderr, "SumNonstat3DOnly: %s\n", err);
+  }
+  return (int)st;
+}
+
+}  // namespace
+
 int main(int argc, char** argv) {
+  {
+    const std::string prog = argv[0];
+    if (prog.find("SummatorEDMN") != std::string::npos) return post_main(true, argc, argv, 1);
+    if (prog.find("SumNonstat3DOnly") != std::string::npos) return post_main(false, argc, argv, 1);
+    if (argc > 1 && !strcmp(argv[1], "--summator-edmn")) return post_main(true, argc, argv, 2);
+    if (argc > 1 && !strcmp(argv[1], "--sum-nonstat-3d-only")) return post_main(false, argc, argv, 2);
+  }
   int form = 0, scheme = 2, device = 0;
   bool stationary = false;
   std::string dir = ".";

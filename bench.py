@@ -489,6 +489,134 @@ def run_serving(args, world, rank, local):
         shutil.rmtree(base, ignore_errors=True)
 
 
+# ---------------------------------------------------------------------------
+# post-processing modules (host): SumNonstat3DOnly + SummatorEDMN
+# ---------------------------------------------------------------------------
+def write_postprocess_workload(path: str, npls=32, nb=21, npts=21, nlines=5, per_line=20, nt=160, seed=7):
+    """Result files of a 32-transmitter run (the 32-wire configuration's shape): per
+    transmitter nb B receivers, npts E point receivers plus nlines lines of per_line
+    points, nt printed layers; values seeded, in CalcNonstat3DLine's text layout."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    t = np.concatenate([[0.0], np.cumsum(np.repeat(1e-6 * 2.0 ** np.arange(8), nt // 8 + 1)[:nt - 1])])
+    hdr = ["    ktime=  %d;  ntstop=  %d;   kiter=    1;   ntime=    1;   niter=    1;\n" % (nt, nt),
+           "   kprogm=    1;  kpropi=    1;  kpropt=   -1;  kitrel=  250;              ;\n",
+           "       u0=   0.00000e+000\n", " T I M E :\n"]
+    hdr += ["".join(" %.13e;" % v for v in t[i:i + 5]) + "\n" for i in range(0, nt, 5)]
+    files = {"infite.0": "".join(hdr), "timeintervalforprint": "%.13e %.13e\n" % (t[0], t[-1]),
+             "group": "1\n1 0 %d\n" % (npls - 1)}
+    ne = npts + nlines * per_line
+    pts_b = rng.uniform(-1000, 1000, (npls, nb, 3))
+    pts_e = rng.uniform(-1000, 1000, (npls, ne, 3))
+    files["xyzVectorB"] = "%d\n" % (npls * nb) + "".join("%.6f %.6f %.6f\n" % tuple(q) for q in pts_b.reshape(-1, 3))
+    files["xyzVectorE"] = "%d\n" % (npls * ne) + "".join("%.6f %.6f %.6f\n" % tuple(q) for q in pts_e.reshape(-1, 3))
+    files["recvsb"] = ("%d\n" % nb) * npls
+    files["recvse"] = ("%d\n" % ne) * npls
+    files["xyzmn"] = "%d\n" % (npls * nlines)
+    t_ms = t * 1000.0
+
+    def block(pts, legend):
+        out = []
+        for q in pts:
+            out.append("%d %d\n%.16e %.16e %.16e\n1\n1 1 1 1\n1\n%s\n" % (int(q[0]), int(q[1]), q[0], q[1], q[2],
+                                                                          legend))
+            v = rng.standard_normal((nt, 3)) * 10.0 ** rng.integers(-6, 2)
+            out.append("".join("%.16e\t%.16e\t%.16e\t%.16e\n" % (t_ms[k], v[k, 0], v[k, 1], v[k, 2])
+                               for k in range(nt)))
+        return "".join(out)
+
+    legs = {"ball_anom": "      t (ms)        Bx_anom (mTl)     By_anom (mTl)     Bz_anom (mTl)",
+            "edsall_anom": "      t (ms)         Emfx_anom (mV)     Emfy_anom (mV)     Emfz_anom (mV)",
+            "eall_anom": "      t (ms)         Ex_anom n (mV)     Ey_anom a (mV)     Ez_anom s (mV)"}
+    for p in range(npls):
+        files["ball_anom.%d" % (p + 1)] = block(pts_b[p], legs["ball_anom"])
+        files["edsall_anom.%d" % (p + 1)] = block(pts_b[p], legs["edsall_anom"])
+        files["eall_anom.%d" % (p + 1)] = block(pts_e[p], legs["eall_anom"])
+        ab = rng.uniform(-1000, 1000, (nlines, 6))
+        files["xyzmn%d_1" % (p + 1)] = "%d\n" % nlines + "".join(" ".join("%.16e" % v for v in r) + "\n" for r in ab)
+        files["xyzVectorElin%d_1" % (p + 1)] = "%d\n" % (nlines * per_line) + "".join(
+            "%.16e %.16e %.16e\n" % tuple(q) for q in pts_e[p, npts:])
+    os.makedirs(path, exist_ok=True)
+    for name, text in files.items():
+        with open(os.path.join(path, name), "w") as f:
+            f.write(text)
+    return npls
+
+
+def run_postprocess(args):
+    """Times SumNonstat3DOnly + SummatorEDMN (WithDDV = 1, every transmitter) on the
+    32-transmitter workload: the package's host modules against the reference's
+    programs compiled from source (oracle/_ref), outputs compared byte for byte."""
+    pkg = importlib.import_module(PKG)
+    ref_bin = os.path.join(HERE, "oracle", "_ref")
+    have_ref = all(os.path.exists(os.path.join(ref_bin, n)) for n in ("SumNonstat3DOnly", "SummatorEDMN"))
+    root = tempfile.mkdtemp(prefix="tdem_post_")
+    try:
+        base = os.path.join(root, "in")
+        npls = write_postprocess_workload(base)
+
+        def stage_lines(d, prefix):
+            for p in range(npls):
+                for c in "xyz":
+                    shutil.copy(os.path.join(d, "E%sall.%d" % (c, p + 1)), os.path.join(d, prefix + "e%sall1_%d" % (c, p)))
+
+        def one(run_split, run_lines, prefix):
+            d = os.path.join(root, "run")
+            shutil.rmtree(d, ignore_errors=True)
+            shutil.copytree(base, d)
+            t0 = time.perf_counter()
+            run_split(d)
+            t1 = time.perf_counter()
+            stage_lines(d, prefix)  # the pipeline's renaming, not timed
+            t2 = time.perf_counter()
+            for p in range(npls):
+                run_lines(d, p)
+            t3 = time.perf_counter()
+            outs = {}
+            for p in range(npls):
+                for stem in ("Exall.%d" % (p + 1), "Bzall.%d" % (p + 1), "Edsall.%d" % (p + 1)):
+                    with open(os.path.join(d, stem), "rb") as f:
+                        outs[stem] = f.read()
+                for stem in ("edmnall1_%d" % p, "edmoonall1_%d" % p):
+                    with open(os.path.join(d, prefix + stem), "rb") as f:
+                        outs[stem] = f.read()
+            return (t1 - t0) + (t3 - t2), outs
+
+        def ours():
+            return one(pkg.sum_nonstat_3d_only, lambda d, p: pkg.summator_edmn(d, 1, 1, p), "")
+
+        def ref():
+            # the reference's SummatorEDMN names its files ".\\<name>" (a backslash-joined path)
+            return one(lambda d: subprocess.run([os.path.join(ref_bin, "SumNonstat3DOnly")], cwd=d, check=True,
+                                                capture_output=True),
+                       lambda d, p: subprocess.run([os.path.join(ref_bin, "SummatorEDMN"), "1", "1", str(p)], cwd=d,
+                                                   check=True, capture_output=True), ".\\")
+
+        for _ in range(max(1, args.warmup)):
+            ours()
+        t_ours = []
+        for _ in range(max(1, args.steps)):
+            dt, out_ours = ours()
+            t_ours.append(dt)
+        t_best = min(t_ours)
+        line = {"metric": "post-processing (SumNonstat3DOnly + SummatorEDMN) transmitters/s", "unit": "transmitters/s",
+                "value": npls / t_best, "ms_per_step": 1000 * t_best, "steps": args.steps, "warmup": args.warmup,
+                "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": "32 transmitters x (21 B + 21 E point receivers + 5 lines x 20 points), "
+                                       "160 layers", "device": "host (text transforms, no GPU)",
+                           "host_threads": os.cpu_count()}}
+        if have_ref:
+            t_ref, out_ref = ref()
+            line["reference"] = {"value": npls / t_ref, "unit": "transmitters/s", "cores": 1,
+                                 "kind": "reference programs built from source (oracle/_ref)"}
+            line["identical_outputs"] = out_ref == out_ours
+        else:
+            line["reference"] = {"unavailable": "oracle/_ref programs not built"}
+        print(json.dumps(line), flush=True)
+    finally:
+        shutil.rmtree(root, ignore_errors=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -507,7 +635,12 @@ def main():
                     help="numeric factors held: 2 overlaps the next factorization with the steps, 0 = auto")
     ap.add_argument("--air-sigma", type=float, default=None,
                     help="conductivity of the air cells (default 1e-8 S/m as the reference's mesh builder)")
+    ap.add_argument("--postprocess", action="store_true",
+                    help="time the host post-processing modules (SumNonstat3DOnly, SummatorEDMN) instead")
     args = ap.parse_args()
+    if args.postprocess:
+        run_postprocess(args)
+        return
     world, rank, local = dist_init(args.gpus)
     try:
         if args.impl == "reference":

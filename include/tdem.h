@@ -62,6 +62,29 @@ tdem_status tdem_run_directory(const char* workdir, int formulation, int scheme,
  * SolveStationarProblem3d(".", true, true) (MOD/CalcStat3D_3T_A/TaskSP.cpp:1625-2208). */
 tdem_status tdem_stationary_directory(const char* workdir, int device, char* errbuf, size_t errlen);
 
+/* ---- Post-processing modules run after CalcNonstat3DLine (host only, no GPU) ----------
+ * Drop-in for the reference's SumNonstat3DOnly in `workdir`: reads group,
+ * timeintervalforprint, infite.0, xyzVectorB / recvsb, xyzVectorE / recvse and the
+ * results ball_anom.N, edsall_anom.N, eall_anom.N, and writes one file per component
+ * (Bxall.N, Byall.N, Bzall.N, Edsxall.N, Edsyall.N, Edsall.N, Exall.N, Eyall.N,
+ * Ezall.N: t in ms, normal part 0, anomalous part, total), byte-identical to the
+ * reference's.  Transmitters are processed on parallel host threads.
+ * Replaces: GeoCalculatorSP.cpp:1673 -> SumNonstat3DOnly main
+ * (SumNonstat3DOnly/main.cpp:171-384). */
+tdem_status tdem_sum_nonstat_3d_only(const char* workdir, char* errbuf, size_t errlen);
+
+/* Drop-in for the reference's SummatorEDMN in `workdir` (arguments as its command
+ * line: WithDDV, profile number, place number): the voltage of each receiver line MN
+ * of that transmitter, dV(t) = sum over the line's points of E(t) . dl, from
+ * exall<profile>_<place>, eyall.., ezall.., xyzmn<place+1>_<profile> and
+ * xyzVectorElin<place+1>_<profile>; writes edmnall<profile>_<place> and, when with_ddv
+ * is nonzero, edmoonall<profile>_<place> (first half of the line minus the second),
+ * byte-identical to the reference's.  Does nothing when xyzmn lists no lines.
+ * Replaces: GeoCalculatorSP.cpp:2312-2314 -> SummatorEDMN main
+ * (SummatorEDMN/main.cpp:37-294). */
+tdem_status tdem_summator_edmn(const char* workdir, int with_ddv, int profile, int place, char* errbuf,
+                               size_t errlen);
+
 typedef struct tdem_solver tdem_solver;
 
 typedef struct tdem_info {

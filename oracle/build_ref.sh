@@ -6,6 +6,9 @@
 #                                          unmodified from its sources with the shim headers in
 #                                          oracle/shim and the pardiso_64 stand-in
 #   oracle/_ref/CalcStat3D_3T_A            the reference's stationary A0 / V solver, same way
+#   oracle/_ref/SumNonstat3DOnly           the reference's per-component split of the 3D results
+#   oracle/_ref/SummatorEDMN               the reference's line-voltage integration (main.cpp
+#                                          only: utils.cpp needs headers absent from the tree)
 #
 # The reference sources are read in place (default /root/reference, override with
 # TDEM_REFERENCE_ROOT); nothing is copied into the repository.  When the reference
@@ -79,3 +82,13 @@ build_variant CalcNonstat3DLine_A3 "$MOD/!programs for 3-point implicit scheme/!
 build_variant CalcNonstat3DLine_E2 "$MOD/!programs for 2-point implicit scheme/!programs for E-formulation/CalcNonstat3DLine"
 build_variant CalcNonstat3DLine_E3 "$MOD/!programs for 3-point implicit scheme/!programs for E-formulation/CalcNonstat3DLine"
 build_variant CalcStat3D_3T_A "$MOD/CalcStat3D_3T_A" "-Dsprintf_s=sprintf"
+
+build_plain() {  # name, sources...
+  local name="$1"
+  shift
+  $CXX $REFFLAGS "$@" -o "$OUT/$name"
+  echo "built $OUT/$name"
+}
+build_plain SumNonstat3DOnly "$MOD/SumNonstat3DOnly/main.cpp" "$MOD/SumNonstat3DOnly/openclose.cpp" \
+  "$MOD/SumNonstat3DOnly/picket.cpp" "$MOD/SumNonstat3DOnly/utils.cpp" "$MOD/SumNonstat3DOnly/utils_direct_solver.cpp"
+build_plain SummatorEDMN "$MOD/SummatorEDMN/main.cpp"

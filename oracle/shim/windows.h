@@ -42,3 +42,23 @@ inline int _itoa_s(int v, char* b, size_t n, int) { return snprintf(b, n, "%d", 
 template <size_t N>
 inline int _itoa_s(int v, char (&b)[N], int) { return snprintf(b, N, "%d", v) < 0; }
 #define sprintf_s sprintf
+
+// Process-creation stand-ins: the post-processing modules define helpers that
+// start child processes but never call them in the paths the oracle runs; here
+// every process creation fails.
+typedef char* LPSTR;
+typedef DWORD* LPDWORD;
+#define INFINITE 0xffffffffu
+#define CREATE_NO_WINDOW 0x08000000
+struct STARTUPINFOA { DWORD cb; };
+struct PROCESS_INFORMATION { HANDLE hProcess, hThread; DWORD dwProcessId, dwThreadId; };
+#define ZeroMemory(p, n) memset((p), 0, (n))
+inline int CreateProcessA(const char*, LPSTR, void*, void*, int, DWORD, void*, const char*, STARTUPINFOA*,
+                          PROCESS_INFORMATION*) {
+  return 0;
+}
+inline DWORD WaitForSingleObject(HANDLE, DWORD) { return 0; }
+inline int GetExitCodeProcess(HANDLE, LPDWORD c) {
+  if (c) *c = 1;
+  return 0;
+}
