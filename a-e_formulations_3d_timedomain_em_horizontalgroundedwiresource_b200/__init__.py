@@ -135,6 +135,8 @@ _lib: Optional[ctypes.CDLL] = None
 EXPORTED = [
     "tdem_run_directory",
     "tdem_stationary_directory",
+    "tdem_time_direct_solver",
+    "tdem_correct_time_mesh",
     "tdem_sum_nonstat_3d_only",
     "tdem_summator_edmn",
     "tdem_solver_create",
@@ -177,6 +179,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.tdem_run_directory.restype = ctypes.c_int
     lib.tdem_stationary_directory.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t]
     lib.tdem_stationary_directory.restype = ctypes.c_int
+    for name in ("tdem_time_direct_solver", "tdem_correct_time_mesh"):
+        getattr(lib, name).argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_size_t]
+        getattr(lib, name).restype = ctypes.c_int
     lib.tdem_sum_nonstat_3d_only.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_size_t]
     lib.tdem_sum_nonstat_3d_only.restype = ctypes.c_int
     lib.tdem_summator_edmn.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_char_p,
@@ -252,6 +257,27 @@ def stationary_directory(workdir: str, device: int = 0) -> None:
     lib = load_library()
     buf = ctypes.create_string_buffer(2048)
     st = lib.tdem_stationary_directory(os.fsencode(workdir), int(device), buf, len(buf))
+    if st != 0:
+        raise TdemError(st, buf.value.decode(errors="replace"))
+
+
+def time_direct_solver(workdir: str) -> None:
+    """Drop-in run of TimeDirectSolver in workdir (host only): infite.0 becomes the
+    piecewise-uniform grid with step growth tcff; currentfunction and deltafunction
+    are interpolated onto it."""
+    lib = load_library()
+    buf = ctypes.create_string_buffer(2048)
+    st = lib.tdem_time_direct_solver(os.fsencode(workdir), buf, len(buf))
+    if st != 0:
+        raise TdemError(st, buf.value.decode(errors="replace"))
+
+
+def correct_time_mesh(workdir: str) -> None:
+    """Drop-in run of CorrectTimeMesh in workdir (host only): short decades of
+    infite.0 are refilled with the previous decade's step."""
+    lib = load_library()
+    buf = ctypes.create_string_buffer(2048)
+    st = lib.tdem_correct_time_mesh(os.fsencode(workdir), buf, len(buf))
     if st != 0:
         raise TdemError(st, buf.value.decode(errors="replace"))
 

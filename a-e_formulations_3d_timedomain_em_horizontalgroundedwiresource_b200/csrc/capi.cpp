@@ -14,6 +14,7 @@
 
 #include "driver.h"
 #include "postprocess.h"
+#include "timegrid.h"
 #include "gpu_cholesky.h"
 #include "server.h"
 #include "stationary.h"
@@ -353,6 +354,20 @@ tdem_status tdem_server_stats_get(tdem_server* srv, tdem_server_stats* st) {
 }
 
 void tdem_server_destroy(tdem_server* srv) { delete srv; }
+
+tdem_status tdem_time_direct_solver(const char* workdir, char* errbuf, size_t errlen) {
+  if (!workdir) return TDEM_ERR_ARGUMENT;
+  const std::string e = tdem::time_direct_solver(workdir);
+  put_err(errbuf, errlen, e);
+  return e.empty() ? TDEM_OK : TDEM_ERR_INPUT;
+}
+
+tdem_status tdem_correct_time_mesh(const char* workdir, char* errbuf, size_t errlen) {
+  if (!workdir) return TDEM_ERR_ARGUMENT;
+  const std::string e = tdem::correct_time_mesh(workdir);
+  put_err(errbuf, errlen, e);
+  return e.empty() ? TDEM_OK : TDEM_ERR_INPUT;
+}
 
 tdem_status tdem_sum_nonstat_3d_only(const char* workdir, char* errbuf, size_t errlen) {
   if (!workdir) return TDEM_ERR_ARGUMENT;

@@ -17,7 +17,9 @@
 // where GeoCalculatorSP.cpp:1673 runs it).  Installed under a name containing
 // SummatorEDMN (or run with --summator-edmn) it takes that module's command line,
 //   SummatorEDMN WithDDV profile place [--dir workdir]
-// (SummatorEDMN/main.cpp:253-294) and writes the line voltages.
+// (SummatorEDMN/main.cpp:253-294) and writes the line voltages.  Under a name
+// containing TimeDirectSolver or CorrectTimeMesh (or with --time-direct-solver /
+// --correct-time-mesh [workdir]) it prepares the time grid as those modules do.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -61,11 +63,32 @@ int post_main(bool summator, int argc, char** argv, int first) {
   return (int)st;
 }
 
+// TimeDirectSolver [workdir] / CorrectTimeMesh [workdir]
+int grid_main(bool correct, int argc, char** argv, int first) {
+  std::string dir = ".";
+  for (int i = first; i < argc; ++i) {
+    if (argv[i][0] == '-') {
+      fprintf(stderr, "usage: %s [workdir]\n", argv[0]);
+      return (int)TDEM_ERR_ARGUMENT;
+    }
+    dir = argv[i];
+  }
+  char err[1024] = {0};
+  const tdem_status st = correct ? tdem_correct_time_mesh(dir.c_str(), err, sizeof err)
+                                 : tdem_time_direct_solver(dir.c_str(), err, sizeof err);
+  if (st != TDEM_OK) fprintf(stderr, "%s: %s\n", correct ? "CorrectTimeMesh" : "TimeDirectSolver", err);
+  return (int)st;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
   {
     const std::string prog = argv[0];
+    if (prog.find("TimeDirectSolver") != std::string::npos) return grid_main(false, argc, argv, 1);
+    if (prog.find("CorrectTimeMesh") != std::string::npos) return grid_main(true, argc, argv, 1);
+    if (argc > 1 && !strcmp(argv[1], "--time-direct-solver")) return grid_main(false, argc, argv, 2);
+    if (argc > 1 && !strcmp(argv[1], "--correct-time-mesh")) return grid_main(true, argc, argv, 2);
     if (prog.find("SummatorEDMN") != std::string::npos) return post_main(true, argc, argv, 1);
     if (prog.find("SumNonstat3DOnly") != std::string::npos) return post_main(false, argc, argv, 1);
     if (argc > 1 && !strcmp(argv[1], "--summator-edmn")) return post_main(true, argc, argv, 2);

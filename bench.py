@@ -545,6 +545,51 @@ def write_postprocess_workload(path: str, npls=32, nb=21, npts=21, nlines=5, per
     return npls
 
 
+def time_grid_timing(pkg, ref_bin, root):
+    """TimeDirectSolver + CorrectTimeMesh on a 200-time log-spaced grid (1e-7 .. 1 s,
+    tcff 2), the package's modules against the reference programs."""
+    import numpy as np
+    t = np.concatenate([[0.0], np.geomspace(1e-7, 1.0, 200)])
+    files = {"tcff": "2\n", "currentfunction": "".join("%.13e\t%.13e\n" % (v, 1.0 if i == 0 else 0.0)
+                                                      for i, v in enumerate(t)),
+             "deltafunction": "50.0\n%d\n" % len(t) + "".join("%.13e %.13e\n" % (v, np.exp(-v)) for v in t)}
+    hdr = ["    ktime=  %d;  ntstop=  %d;   kiter=    1;   ntime=    1;   niter=    1;\n" % (len(t), len(t)),
+           "   kprogm=    1;  kpropi=    1;  kpropt=   -1;  kitrel=  250;              ;\n",
+           "       u0=   0.00000e+000\n", " T I M E :\n"]
+    files["infite.0"] = "".join(hdr + ["".join(" %.13e;" % v for v in t[i:i + 5]) + "\n" for i in range(0, len(t), 5)])
+
+    def one(run):
+        d = os.path.join(root, "grid")
+        shutil.rmtree(d, ignore_errors=True)
+        os.makedirs(d)
+        for k, v in files.items():
+            with open(os.path.join(d, k), "w") as f:
+                f.write(v)
+        t0 = time.perf_counter()
+        run(d)
+        dt = time.perf_counter() - t0
+        out = {}
+        for k in ("infite.0", "currentfunction", "deltafunction"):
+            with open(os.path.join(d, k), "rb") as f:
+                out[k] = f.read()
+        return dt, out
+
+    def ours(d):
+        pkg.time_direct_solver(d)
+        pkg.correct_time_mesh(d)
+
+    t_ours = min(one(ours)[0] for _ in range(5))
+    res = {"workload": "200-time log grid 1e-7..1 s, tcff 2", "ms": 1000 * t_ours}
+    if all(os.path.exists(os.path.join(ref_bin, n)) for n in ("TimeDirectSolver", "CorrectTimeMesh")):
+        def ref(d):
+            for n in ("TimeDirectSolver", "CorrectTimeMesh"):
+                subprocess.run([os.path.join(ref_bin, n)], cwd=d, check=True, capture_output=True)
+        t_ref, out_ref = one(ref)
+        res["reference_ms"] = 1000 * t_ref
+        res["identical_outputs"] = out_ref == one(ours)[1]
+    return res
+
+
 def run_postprocess(args):
     """Times SumNonstat3DOnly + SummatorEDMN (WithDDV = 1, every transmitter) on the
     32-transmitter workload: the package's host modules against the reference's
@@ -614,6 +659,7 @@ def run_postprocess(args):
             line["identical_outputs"] = out_ref == out_ours
         else:
             line["reference"] = {"unavailable": "oracle/_ref programs not built"}
+        line["time_grid"] = time_grid_timing(pkg, ref_bin, root)
         print(json.dumps(line), flush=True)
     finally:
         shutil.rmtree(root, ignore_errors=True)
@@ -638,7 +684,8 @@ def main():
     ap.add_argument("--air-sigma", type=float, default=None,
                     help="conductivity of the air cells (default 1e-8 S/m as the reference's mesh builder)")
     ap.add_argument("--postprocess", action="store_true",
-                    help="time the host post-processing modules (SumNonstat3DOnly, SummatorEDMN) instead")
+                    help="time the host modules around the solve (SumNonstat3DOnly, SummatorEDMN, "
+                         "TimeDirectSolver, CorrectTimeMesh) instead")
     args = ap.parse_args()
     if args.postprocess:
         run_postprocess(args)

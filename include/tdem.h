@@ -62,6 +62,24 @@ tdem_status tdem_run_directory(const char* workdir, int formulation, int scheme,
  * SolveStationarProblem3d(".", true, true) (MOD/CalcStat3D_3T_A/TaskSP.cpp:1625-2208). */
 tdem_status tdem_stationary_directory(const char* workdir, int device, char* errbuf, size_t errlen);
 
+/* ---- Time-grid modules run before CalcNonstat3DLine (host only, no GPU) ---------------
+ * Drop-in for the reference's TimeDirectSolver in `workdir`: reads tcff (step growth
+ * factor) and infite.0, replaces the times by a piecewise-uniform grid whose step grows
+ * by tcff from one interval to the next, and interpolates currentfunction and
+ * deltafunction onto it; the three files are rewritten (the old ones renamed with a
+ * leading "!"), byte-identical to the reference's.  Replaces: GeoCalculatorSP.cpp:2111
+ * -> TimeDirectSolver main (TimeDirectSolver/main.cpp:98-219, TimeStep.cpp:37-168). */
+tdem_status tdem_time_direct_solver(const char* workdir, char* errbuf, size_t errlen);
+
+/* Drop-in for the reference's CorrectTimeMesh in `workdir`: decades of the grid in
+ * infite.0 that are too short for their step (fewer than 1/tcff of the previous
+ * decade's times) are refilled with the previous decade's step; infite.0, deltafunction
+ * and currentfunction are rewritten on the corrected times (old ones renamed with a
+ * leading "!!"; both function files carry deltafunction's values, as in the reference),
+ * byte-identical to the reference's.  Replaces: GeoCalculatorSP.cpp:2120 ->
+ * CorrectTimeMesh main (CorrectTimeMesh/main.cpp:87-269). */
+tdem_status tdem_correct_time_mesh(const char* workdir, char* errbuf, size_t errlen);
+
 /* ---- Post-processing modules run after CalcNonstat3DLine (host only, no GPU) ----------
  * Drop-in for the reference's SumNonstat3DOnly in `workdir`: reads group,
  * timeintervalforprint, infite.0, xyzVectorB / recvsb, xyzVectorE / recvse and the

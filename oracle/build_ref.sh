@@ -9,6 +9,8 @@
 #   oracle/_ref/SumNonstat3DOnly           the reference's per-component split of the 3D results
 #   oracle/_ref/SummatorEDMN               the reference's line-voltage integration (main.cpp
 #                                          only: utils.cpp needs headers absent from the tree)
+#   oracle/_ref/TimeDirectSolver           the reference's time-grid regularisation
+#   oracle/_ref/CorrectTimeMesh            the reference's short-decade correction
 #
 # The reference sources are read in place (default /root/reference, override with
 # TDEM_REFERENCE_ROOT); nothing is copied into the repository.  When the reference
@@ -92,3 +94,5 @@ build_plain() {  # name, sources...
 build_plain SumNonstat3DOnly "$MOD/SumNonstat3DOnly/main.cpp" "$MOD/SumNonstat3DOnly/openclose.cpp" \
   "$MOD/SumNonstat3DOnly/picket.cpp" "$MOD/SumNonstat3DOnly/utils.cpp" "$MOD/SumNonstat3DOnly/utils_direct_solver.cpp"
 build_plain SummatorEDMN "$MOD/SummatorEDMN/main.cpp"
+build_plain TimeDirectSolver "$MOD/TimeDirectSolver/main.cpp" "$MOD/TimeDirectSolver/TimeStep.cpp"
+build_plain CorrectTimeMesh "$MOD/CorrectTimeMesh/main.cpp"
