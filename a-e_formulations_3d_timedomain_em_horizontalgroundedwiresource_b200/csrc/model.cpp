@@ -377,30 +377,27 @@ void edge_pattern(const Model& m, std::vector<int64_t>& rowptr, std::vector<int>
     for (int e = 0; e < m.n_elem; ++e)
       for (int i = 0; i < 12; ++i) elems[fill[m.ed[e][i]]++] = e;
   }
-  // two passes (row lengths, then the rows), so no buffer of all gathered edges
-  auto row = [&](int64_t i, std::vector<int>& buf) {
-    buf.clear();
-    for (int64_t q = eptr[i]; q < eptr[i + 1]; ++q)
-      for (int j = 0; j < 12; ++j) buf.push_back(m.ed[elems[q]][j]);
-    std::sort(buf.begin(), buf.end());
-    buf.erase(std::unique(buf.begin(), buf.end()), buf.end());
-  };
+  // each range of rows is gathered, sorted and deduplicated into its own buffer;
+  // the buffers are then placed one after the other
+  const int nt = chunk_count(n, 4096);
+  std::vector<std::vector<int>> part(nt);
   rowptr.assign(n + 1, 0);
-  parallel_ranges(n, [&](int64_t r0, int64_t r1) {
-    std::vector<int> buf;
+  parallel_chunks(n, nt, [&](int t, int64_t r0, int64_t r1) {
+    std::vector<int>& out = part[t];
+    out.reserve((size_t)(r1 - r0) * 36);
     for (int64_t i = r0; i < r1; ++i) {
-      row(i, buf);
-      rowptr[i + 1] = (int64_t)buf.size();
+      const size_t b = out.size();
+      for (int64_t q = eptr[i]; q < eptr[i + 1]; ++q)
+        for (int j = 0; j < 12; ++j) out.push_back(m.ed[elems[q]][j]);
+      std::sort(out.begin() + b, out.end());
+      out.erase(std::unique(out.begin() + b, out.end()), out.end());
+      rowptr[i + 1] = (int64_t)(out.size() - b);
     }
   });
   for (int i = 0; i < n; ++i) rowptr[i + 1] += rowptr[i];
-  col.assign(rowptr[n], 0);
-  parallel_ranges(n, [&](int64_t r0, int64_t r1) {
-    std::vector<int> buf;
-    for (int64_t i = r0; i < r1; ++i) {
-      row(i, buf);
-      std::copy(buf.begin(), buf.end(), col.begin() + rowptr[i]);
-    }
+  col.resize(rowptr[n]);
+  parallel_chunks(n, nt, [&](int t, int64_t r0, int64_t) {
+    std::copy(part[t].begin(), part[t].end(), col.begin() + rowptr[r0]);
   });
 }
 

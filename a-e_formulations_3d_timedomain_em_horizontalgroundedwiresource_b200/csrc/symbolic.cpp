@@ -276,27 +276,61 @@ std::string analyse(int n, const int64_t* rowptr, const int* colind, const doubl
   // symmetric adjacency without the diagonal
   Graph g;
   g.n = n;
-  std::vector<int64_t> deg(n, 0);
-  for (int i = 0; i < n; ++i)
-    for (int64_t q = rowptr[i]; q < rowptr[i + 1]; ++q) {
-      const int j = colind[q];
-      if (j < 0 || j > i) return "lower-triangle pattern expected (column index out of range)";
-      if (j == i) continue;
-      ++deg[i];
-      ++deg[j];
-    }
-  g.xadj.assign(n + 1, 0);
-  for (int i = 0; i < n; ++i) g.xadj[i + 1] = g.xadj[i] + deg[i];
-  g.adj.resize(g.xadj[n]);
+  // Row v lists its own lower entries (CSR order) and then the rows i > v that hold
+  // an entry in column v, ascending.  The transposed part is placed per range of
+  // rows after the entries of the lower ranges, which keeps that order.
   {
-    std::vector<int64_t> fill(g.xadj.begin(), g.xadj.end() - 1);
-    for (int i = 0; i < n; ++i)
-      for (int64_t q = rowptr[i]; q < rowptr[i + 1]; ++q) {
-        const int j = colind[q];
-        if (j == i) continue;
-        g.adj[fill[i]++] = j;
-        g.adj[fill[j]++] = i;
+    const int nt = chunk_count(n, 16384);
+    std::vector<int64_t> own(n, 0);
+    std::vector<int> upper((size_t)nt * n, 0);  // per range: entries of each column
+    std::vector<char> bad(nt, 0);
+    parallel_chunks(n, nt, [&](int t, int64_t i0, int64_t i1) {
+      int* up = upper.data() + (size_t)t * n;
+      for (int64_t i = i0; i < i1; ++i)
+        for (int64_t q = rowptr[i]; q < rowptr[i + 1]; ++q) {
+          const int j = colind[q];
+          if (j < 0 || j > i) {
+            bad[t] = 1;
+            return;
+          }
+          if (j == i) continue;
+          ++own[i];
+          ++up[j];
+        }
+    });
+    for (char b : bad)
+      if (b) return "lower-triangle pattern expected (column index out of range)";
+    g.xadj.assign(n + 1, 0);
+    for (int v = 0; v < n; ++v) {
+      int64_t d = own[v];
+      for (int t = 0; t < nt; ++t) d += upper[(size_t)t * n + v];
+      g.xadj[v + 1] = g.xadj[v] + d;
+    }
+    // turn the per-range counts into the first slot of each range in each column
+    parallel_ranges(n, [&](int64_t v0, int64_t v1) {
+      for (int64_t v = v0; v < v1; ++v) {
+        int64_t at = g.xadj[v] + own[v];
+        for (int t = 0; t < nt; ++t) {
+          int& c = upper[(size_t)t * n + v];
+          const int k = c;
+          c = (int)(at - g.xadj[v]);
+          at += k;
+        }
       }
+    });
+    g.adj.resize(g.xadj[n]);
+    parallel_chunks(n, nt, [&](int t, int64_t i0, int64_t i1) {
+      int* up = upper.data() + (size_t)t * n;
+      for (int64_t i = i0; i < i1; ++i) {
+        int64_t o = g.xadj[i];
+        for (int64_t q = rowptr[i]; q < rowptr[i + 1]; ++q) {
+          const int j = colind[q];
+          if (j == i) continue;
+          g.adj[o++] = j;
+          g.adj[g.xadj[j] + up[j]++] = (int)i;
+        }
+      }
+    });
   }
 
   // ordering + tree
@@ -323,33 +357,51 @@ std::string analyse(int n, const int64_t* rowptr, const int* colind, const doubl
   for (int s = 0; s < nf; ++s)
     for (int cc = sy.fronts[s].c0; cc < sy.fronts[s].c1; ++cc) colfront[cc] = s;
 
-  // row structures (postorder: children first)
+  // row structures: a front's rows are its columns' neighbours and its children's
+  // rows beyond its columns.  Tree levels first (postorder: children first), then
+  // the fronts of one level in parallel, each thread with its own marks.
   {
-    std::vector<int> st(n, -1), tmp;
     for (int s = 0; s < nf; ++s) {
-      FrontInfo& f = sy.fronts[s];
-      tmp.clear();
-      for (int cc = f.c0; cc < f.c1; ++cc) {
-        const int i = sy.iperm[cc];
-        for (int64_t p = g.xadj[i]; p < g.xadj[i + 1]; ++p) {
-          const int r = sy.perm[g.adj[p]];
-          if (r >= f.c1 && st[r] != s) {
-            st[r] = s;
-            tmp.push_back(r);
-          }
-        }
-      }
-      for (int ch : f.children)
-        for (int r : sy.fronts[ch].rows)
-          if (r >= f.c1 && st[r] != s) {
-            st[r] = s;
-            tmp.push_back(r);
-          }
-      std::sort(tmp.begin(), tmp.end());
-      f.rows = tmp;
       int lev = 0;
-      for (int ch : f.children) lev = std::max(lev, sy.fronts[ch].level + 1);
-      f.level = lev;
+      for (int ch : sy.fronts[s].children) lev = std::max(lev, sy.fronts[ch].level + 1);
+      sy.fronts[s].level = lev;
+    }
+    int nlev_rs = 0;
+    for (const FrontInfo& f : sy.fronts) nlev_rs = std::max(nlev_rs, f.level + 1);
+    std::vector<std::vector<int>> by_level(nlev_rs);
+    for (int s = 0; s < nf; ++s) by_level[sy.fronts[s].level].push_back(s);
+    const int nth = host_threads();
+    std::vector<std::vector<int>> marks(nth);
+    for (const std::vector<int>& lvl : by_level) {
+      const int nt = std::min(nth, chunk_count((int64_t)lvl.size(), 8));
+      parallel_chunks((int64_t)lvl.size(), nt, [&](int t, int64_t a, int64_t b) {
+        std::vector<int>& st = marks[t];
+        if (st.empty()) st.assign(n, -1);
+        std::vector<int> tmp;
+        for (int64_t x = a; x < b; ++x) {
+          const int s = lvl[x];
+          FrontInfo& f = sy.fronts[s];
+          tmp.clear();
+          for (int cc = f.c0; cc < f.c1; ++cc) {
+            const int i = sy.iperm[cc];
+            for (int64_t p = g.xadj[i]; p < g.xadj[i + 1]; ++p) {
+              const int r = sy.perm[g.adj[p]];
+              if (r >= f.c1 && st[r] != s) {
+                st[r] = s;
+                tmp.push_back(r);
+              }
+            }
+          }
+          for (int ch : f.children)
+            for (int r : sy.fronts[ch].rows)
+              if (r >= f.c1 && st[r] != s) {
+                st[r] = s;
+                tmp.push_back(r);
+              }
+          std::sort(tmp.begin(), tmp.end());
+          f.rows = tmp;
+        }
+      });
     }
   }
 
@@ -395,27 +447,41 @@ std::string analyse(int n, const int64_t* rowptr, const int* colind, const doubl
     for (int r : f.rows) sy.rows_all[o++] = r;
   }
 
-  // relative maps child rows -> parent front slots
+  // relative maps child rows -> parent front slots (parents in parallel, each thread
+  // with its own slot map and the parent that set each slot)
   {
-    std::vector<int> pos(n, -1);
     sy.rel_off.assign(nf + 1, 0);
     for (int s = 0; s < nf; ++s) sy.rel_off[s + 1] = sy.rel_off[s] + (int64_t)sy.fronts[s].rows.size();
     sy.rel.assign(sy.rel_off[nf], -1);
-    for (int p = 0; p < nf; ++p) {
-      const FrontInfo& fp = sy.fronts[p];
-      for (int cc = fp.c0; cc < fp.c1; ++cc) pos[cc] = cc - fp.c0;
-      for (size_t t = 0; t < fp.rows.size(); ++t) pos[fp.rows[t]] = fp.k() + (int)t;
-      for (int ch : fp.children) {
-        const FrontInfo& fc = sy.fronts[ch];
-        for (size_t t = 0; t < fc.rows.size(); ++t) {
-          const int r = fc.rows[t];
-          const bool in_parent =
-              (r >= fp.c0 && r < fp.c1) || std::binary_search(fp.rows.begin(), fp.rows.end(), r);
-          if (!in_parent) return "internal error: child row missing from parent front";
-          sy.rel[sy.rel_off[ch] + t] = pos[r];
+    const int nt = chunk_count(nf, 64);
+    std::vector<char> missing(nt, 0);
+    parallel_chunks(nf, nt, [&](int t, int64_t p0, int64_t p1) {
+      std::vector<int> pos(n, -1), owner(n, -1);
+      for (int64_t p = p0; p < p1; ++p) {
+        const FrontInfo& fp = sy.fronts[p];
+        for (int cc = fp.c0; cc < fp.c1; ++cc) {
+          pos[cc] = cc - fp.c0;
+          owner[cc] = (int)p;
+        }
+        for (size_t x = 0; x < fp.rows.size(); ++x) {
+          pos[fp.rows[x]] = fp.k() + (int)x;
+          owner[fp.rows[x]] = (int)p;
+        }
+        for (int ch : fp.children) {
+          const FrontInfo& fc = sy.fronts[ch];
+          for (size_t x = 0; x < fc.rows.size(); ++x) {
+            const int r = fc.rows[x];
+            if (owner[r] != p) {
+              missing[t] = 1;
+              return;
+            }
+            sy.rel[sy.rel_off[ch] + x] = pos[r];
+          }
         }
       }
-    }
+    });
+    for (char b : missing)
+      if (b) return "internal error: child row missing from parent front";
     for (int s = 0; s < nf; ++s)
       if (sy.fronts[s].parent < 0 && !sy.fronts[s].rows.empty())
         return "internal error: root front with off-diagonal rows";
