@@ -48,6 +48,9 @@ if [ ! -d "$MOD" ]; then
   exit 0
 fi
 
+# objects are rebuilt when a shim header changes too
+SHIM_NEWEST="$(ls -t "$HERE"/shim/*.h | head -1)"
+
 # flags that let the MSVC sources compile with g++ (no source edits)
 REFFLAGS="-std=c++17 $OPT -fpermissive -w -D__forceinline=inline -include cmath -include cfloat \
  -include cstring -include ctime -include algorithm -include iterator -include $HERE/shim/llp64_stdio.h \
@@ -68,7 +71,7 @@ build_variant() {  # name, source dir, extra compiler flags
     local b
     b="$(basename "$f" .cpp)"
     objs+=("$obj/$b.o")
-    if [ ! -f "$obj/$b.o" ] || [ "$f" -nt "$obj/$b.o" ]; then
+    if [ ! -f "$obj/$b.o" ] || [ "$f" -nt "$obj/$b.o" ] || [ "$SHIM_NEWEST" -nt "$obj/$b.o" ]; then
       $CXX $REFFLAGS $extra -I"$inc" -c "$f" -o "$obj/$b.o" &
       pids+=($!)
       if [ "${#pids[@]}" -ge "$JOBS" ]; then wait "${pids[0]}"; pids=("${pids[@]:1}"); fi

@@ -125,3 +125,24 @@ def test_decade_logic():
     assert tdem_oracle.find_layer(t, 6.0) == 5
     assert tdem_oracle.find_layer(t, 0.0) == 0
     assert tdem_oracle.find_layer(t, 5.5) == -1
+
+
+def test_reference_build_reproduces_primary_secondary_goldens(outs, tmp_path):
+    """The primary-secondary fixtures come from the reference reading the normal field
+    through its named-shared-memory calls (served from files by the oracle build)."""
+    import run_ref
+    import sys
+    sys.path.insert(0, GOLDEN)
+    import make_ps_golden as ps
+    if not run_ref.available("CalcNonstat3DLine_A2"):
+        pytest.skip("oracle/_ref not built")
+    d = str(tmp_path / "ps")
+    ps.write_case_inputs(d)
+    run_ref.run_transient(d, "A2")
+    for o in ps.OUTPUTS:
+        err = outs.compare_files(os.path.join(d, o + ".1"), os.path.join(GOLDEN, ps.CASE, "A2_%s.1" % o))
+        assert err <= 1e-12, (o, err)
+    # without the anomalous-edge list the normal field is not read and the result differs
+    os.unlink(os.path.join(d, "mtrsizeforE0"))
+    run_ref.run_transient(d, "A2")
+    assert outs.compare_files(os.path.join(d, "eall_anom.1"), os.path.join(GOLDEN, ps.CASE, "A2_eall_anom.1")) > 0.1
