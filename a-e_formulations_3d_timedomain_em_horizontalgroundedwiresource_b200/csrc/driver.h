@@ -108,6 +108,18 @@ class TransientSolve {
   std::vector<double> u0_;
   ReceiverOperator rop_b_, rop_e_;
   bool have_source_ = false;
+  // primary-secondary mode (fdirect 0 with anomalous edges): C_dsigma on the full
+  // pattern, the normal field of the current layer as edge values, its float copy
+  // as read, the anomalous edges and their lengths
+  bool ps_ = false;
+  std::vector<int> anom_idx_;
+  std::vector<double> anom_len_;
+  std::vector<float> ef_host_;
+  double* d_Cds_ = nullptr;
+  double* d_En_ = nullptr;
+  float* d_Ef_ = nullptr;
+  int* d_anom_ = nullptr;
+  double* d_alen_ = nullptr;
   // device buffers
   int64_t* d_rowptr_ = nullptr;
   int* d_col_ = nullptr;
@@ -147,6 +159,8 @@ class TransientSolve {
   // source vectors and receiver operators of the planned model (reads the model only)
   std::string build_sources_and_receivers();
   std::string step(int itime, int t1, int t2, double m1, double m2, double coef);
+  // adds C_dsigma * En(itime) to the step's right-hand side (primary-secondary mode)
+  std::string anomaly_source(int itime);
   void eval_receivers(int t);
   double source_coef(int itime, bool two_layer, double dt) const;
 };

@@ -79,7 +79,35 @@ __global__ void k_assemble(ElemDev E, const int* __restrict__ elems, int nelems,
   }
   if (col[lo] != gj) return;  // cannot happen for a pattern built from the same elements
   Cval[lo] += c * E.sigma[e];
-  Bval[lo] += b * E.inv_mu[e];
+  if (Bval) Bval[lo] += b * E.inv_mu[e];
+}
+
+__global__ void k_normal_field(const float* __restrict__ f, const int* __restrict__ idx,
+                               const double* __restrict__ len, int nanom, int n, int npls,
+                               double* __restrict__ En) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= (int64_t)nanom * npls) return;
+  const int p = (int)(t / nanom), k = (int)(t % nanom);
+  En[idx[k] + (int64_t)p * n] = (double)f[t] * len[k] * 0.5;
+}
+
+// One warp per row: rhs += C_dsigma * En (time_approx.cpp:682, mult_symmetr on the
+// lower-stored C_dsigma; here the full symmetric pattern).
+__global__ void k_anomaly_rhs(const int64_t* __restrict__ rowptr, const int* __restrict__ col,
+                              const double* __restrict__ Cds, const double* __restrict__ En,
+                              const uint8_t* __restrict__ bound, int n, int npls, double* __restrict__ rhs) {
+  const int row = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (row >= n || bound[row]) return;
+  const int64_t b = rowptr[row], e = rowptr[row + 1];
+  for (int p = 0; p < npls; ++p) {
+    const double* x = En + (int64_t)p * n;
+    double acc = 0.0;
+    for (int64_t q = b + lane; q < e; q += 32) acc = fma(Cds[q], x[col[q]], acc);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if (lane == 0) rhs[row + (int64_t)p * n] += acc;
+  }
 }
 
 __global__ void k_combine(const double* __restrict__ C, const double* __restrict__ B,
@@ -351,6 +379,19 @@ void launch_history_rhs(const int64_t* rowptr, const int* col, const double* Cva
   const int64_t threads = (int64_t)n * 32;
   k_history_rhs<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(rowptr, col, Cval, u1, u2, m1c, m2c, S, coef,
                                                                   bound, n, npls, rhs);
+}
+
+void launch_normal_field(const float* f, const int* idx, const double* len, int nanom, int n, int npls, double* En,
+                         cudaStream_t s) {
+  const int64_t t = (int64_t)nanom * npls;
+  if (t <= 0) return;
+  k_normal_field<<<(unsigned)((t + 255) / 256), 256, 0, s>>>(f, idx, len, nanom, n, npls, En);
+}
+
+void launch_anomaly_rhs(const int64_t* rowptr, const int* col, const double* Cds, const double* En,
+                        const uint8_t* bound, int n, int npls, double* rhs, cudaStream_t s) {
+  const int64_t threads = (int64_t)n * 32;
+  k_anomaly_rhs<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(rowptr, col, Cds, En, bound, n, npls, rhs);
 }
 
 void launch_receivers(const int64_t* rowptr, const int* col, const double* val, const int* src,

@@ -16,7 +16,8 @@ struct ElemDev {
 };
 
 // Adds sigma * C_e and B_e / mu of the elements in `elems` (one colour: no two
-// share an edge) into the full symmetric CSR values Cval / Bval.
+// share an edge) into the full symmetric CSR values Cval / Bval (Bval may be null:
+// mass term only).
 void launch_assemble(const ElemDev& e, const int* elems, int nelems, const int64_t* rowptr,
                      const int* col, double* Cval, double* Bval, cudaStream_t s);
 
@@ -35,6 +36,15 @@ void launch_history_rhs(const int64_t* rowptr, const int* col, const double* Cva
                         const uint8_t* bound, int n, int npls, double* rhs, cudaStream_t s);
 
 // Receiver values: out[row] = sum_j R[row, j] * u[j, src[row]] for every operator row.
+// Primary-secondary source of one time layer.  The normal field f (float, V/m,
+// nanom values per source, source-major) of the anomalous edges idx becomes edge
+// degrees of freedom En = f * len * 0.5 (the other entries of En stay as they are,
+// zero); then rhs += C_dsigma * En on the rows that are not Dirichlet edges.
+void launch_normal_field(const float* f, const int* idx, const double* len, int nanom, int n, int npls, double* En,
+                         cudaStream_t s);
+void launch_anomaly_rhs(const int64_t* rowptr, const int* col, const double* Cds, const double* En,
+                        const uint8_t* bound, int n, int npls, double* rhs, cudaStream_t s);
+
 void launch_receivers(const int64_t* rowptr, const int* col, const double* val, const int* src,
                       int nrows, const double* u, int64_t ld, double* out, cudaStream_t s);
 

@@ -166,6 +166,23 @@ std::string load_model(const std::string& dir, Model& m) {
       m.edge_bound[e] = bn[m.edge_nodes[e][0]] && bn[m.edge_nodes[e][1]];
   }
 
+  // --- anomalous edges of the primary-secondary mode (time_approx.cpp:351-368) -------
+  {
+    std::ifstream in(path(m, "mtrsizeforE0"));
+    m.edge_anom.assign(m.n_edges, 0);
+    m.n_anom = 0;
+    if (in) {
+      for (int e = 0; e < m.n_edges; ++e) {
+        int k = 0;
+        if (!(in >> k)) return "mtrsizeforE0: fewer flags than edges";
+        m.edge_anom[e] = k != 0;
+        m.n_anom += k != 0;
+      }
+    }
+    std::ifstream pn(path(m, "PName"));
+    if (pn) pn >> m.pname;
+  }
+
   // --- time grid infite.0 (vec_prep_data.cpp:834-853) -----------------------------
   {
     std::ifstream in(path(m, "infite.0"));

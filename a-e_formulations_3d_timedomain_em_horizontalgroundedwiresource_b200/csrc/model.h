@@ -45,6 +45,12 @@ struct Model {
   int n_neib = 5;
   bool fdirect = false;
   double eps_reg = 1e-12;
+  // primary-secondary mode (fdirect 0): the edges whose normal field enters the
+  // source (mtrsizeforE0, one flag per edge) and the name in the normal-field files
+  // m<pname>.enor.NNNN (PName)
+  std::vector<char> edge_anom;
+  int n_anom = 0;
+  std::string pname;
   // derived
   std::vector<char> edge_bound;               // Dirichlet edge flag
   std::string dir;

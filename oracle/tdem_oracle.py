@@ -53,8 +53,10 @@ def read_model(d: str) -> Dict:
                 rows.append((int(p[0]), float(p[1]), float(p[2])))
     nmat = max(r[0] for r in rows)
     m["sigma"] = np.zeros(nmat)
+    m["sigma0"] = np.zeros(nmat)
     for r in rows[:nmat]:
         m["sigma"][r[0] - 1] = r[1]
+        m["sigma0"][r[0] - 1] = r[2]
     m["mu"] = np.full(nmat, MU0)
     with open(os.path.join(d, "mu3d")) as f:
         vals = f.read().split()
@@ -99,6 +101,14 @@ def read_model(d: str) -> Dict:
         nsr = os.path.join(d, "nSrsRazb")
         m["nsrs"] = int(open(nsr).read().split()[0]) if os.path.exists(nsr) else 500
         m["wires"] = np.array([float(v) for v in open(os.path.join(d, "sours")).read().split()]).reshape(-1, 6)[:npls]
+    # primary-secondary mode: anomalous edges and the normal-field file name
+    # (time_approx.cpp:351-368, 1263-1348)
+    mf = os.path.join(d, "mtrsizeforE0")
+    m["anom"] = np.zeros(m["n"], bool)
+    if os.path.exists(mf):
+        m["anom"] = np.array([int(v) for v in open(mf).read().split()[:m["n"]]]) != 0
+    pn = os.path.join(d, "PName")
+    m["pname"] = open(pn).read().split()[0] if os.path.exists(pn) else ""
     m["dir"] = d
     return m
 
@@ -156,7 +166,7 @@ def local_matrices(h: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
 
 def assemble(m: Dict):
     """Global sigma*C and B/mu over all edges (T_Global_SLAE.cpp:76-215)."""
-    rows, cols, cv, bv = [], [], [], []
+    rows, cols, cv, bv, dv = [], [], [], [], []
     cache = {}
     for e in range(m["nver"].shape[0]):
         p0, p7 = m["xyz"][m["nver"][e, 0]], m["xyz"][m["nver"][e, 7]]
@@ -171,11 +181,26 @@ def assemble(m: Dict):
         cols.append(cc.ravel())
         cv.append((Cl * m["sigma"][m["nvkat"][e]]).ravel())
         bv.append((Bl / m["mu"][m["nvkat"][e]]).ravel())
+        dv.append((Cl * (m["sigma"][m["nvkat"][e]] - m["sigma0"][m["nvkat"][e]])).ravel())
     n = m["n"]
     r, c = np.concatenate(rows), np.concatenate(cols)
     Cg = sp.csr_matrix((np.concatenate(cv), (r, c)), shape=(n, n))
     Bg = sp.csr_matrix((np.concatenate(bv), (r, c)), shape=(n, n))
+    m["Cds"] = sp.csr_matrix((np.concatenate(dv), (r, c)), shape=(n, n))  # (sigma - sigma0) C
     return Cg, Bg
+
+
+def normal_field(m: Dict, it: int) -> np.ndarray:
+    """Normal field of layer it as edge values (time_approx.cpp:1263-1348): float32 per
+    anomalous edge and source from m<PName>.enor.NNNN, times half the edge length."""
+    idx = np.nonzero(m["anom"])[0]
+    f = np.fromfile(os.path.join(m["dir"], "m%s.enor.%04d" % (m["pname"], it)), "<f4")
+    f = f[: len(idx) * m["npls"]].reshape(m["npls"], len(idx)).astype(np.float64)
+    ax = m["xyz"][m["edges"][idx, 1]] - m["xyz"][m["edges"][idx, 0]]
+    ln = np.sqrt(ax[:, 0] * ax[:, 0] + ax[:, 1] * ax[:, 1] + ax[:, 2] * ax[:, 2])
+    En = np.zeros((m["n"], m["npls"]))
+    En[idx] = (f * ln * 0.5).T
+    return En
 
 
 # ---------------------------------------------------------------------------
@@ -421,9 +446,15 @@ def run(d: str, formulation: str, scheme: int) -> Dict:
             djdt = (cf[it] - cf[it - 1]) / (dt if two else (t[it] - t[it - 1]))
         return -djdt
 
+    ps = (not m["fdirect"]) and bool(m["anom"].any())
+    if ps and eform:
+        raise NotImplementedError("primary-secondary mode of the E-formulation")
+
     def step(it, t1, t2, m1, m2, c):
         hist = U[t1] * m1 + (U[t2] * m2 if m2 != 0 else 0.0)
         rhs = Cg @ hist + c * S
+        if ps:
+            rhs = rhs + m["Cds"] @ normal_field(m, it)
         rhs[bound] = 0.0
         x = np.zeros((n, npls))
         x[inner] = lu.solve(rhs[inner])

@@ -78,3 +78,21 @@ def test_drop_in_executable(pkg, golden, outs, tmp_path):
     for o in golden.OUTPUTS:
         err = outs.compare_files(os.path.join(d, o + ".1"), os.path.join(GOLDEN, "cube8_block", "E3_%s.1" % o))
         assert err <= FP64_TOL
+
+
+@pytest.mark.parametrize("variant", ["A2", "A3"])
+def test_gpu_primary_secondary_matches_reference(pkg, outs, tmp_path, variant):
+    """Primary-secondary mode (fdirect 0): the normal field of every layer, read from the
+    m<PName>.enor.NNNN files, drives the anomalous block through C_dsigma; against the
+    reference's own outputs on the same files."""
+    import sys
+    sys.path.insert(0, GOLDEN)
+    import make_ps_golden as ps
+    d = str(tmp_path / "ps")
+    ps.write_case_inputs(d)
+    with pkg.Solver(d, variant[0], int(variant[1])) as s:
+        s.run()
+        s.write_outputs()
+    for o in ps.OUTPUTS:
+        err = outs.compare_files(os.path.join(d, o + ".1"), os.path.join(GOLDEN, ps.CASE, "%s_%s.1" % (variant, o)))
+        assert err <= FP64_TOL, (o, err)

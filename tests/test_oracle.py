@@ -146,3 +146,18 @@ def test_reference_build_reproduces_primary_secondary_goldens(outs, tmp_path):
     os.unlink(os.path.join(d, "mtrsizeforE0"))
     run_ref.run_transient(d, "A2")
     assert outs.compare_files(os.path.join(d, "eall_anom.1"), os.path.join(GOLDEN, ps.CASE, "A2_eall_anom.1")) > 0.1
+
+
+@pytest.mark.parametrize("variant", ["A2", "A3"])
+def test_numpy_oracle_primary_secondary_matches_reference(outs, tmp_path, variant):
+    """The restatement of the primary-secondary source (C_dsigma times the normal
+    field's edge values, time_approx.cpp:671-683, 1263-1348) against the reference."""
+    import sys
+    sys.path.insert(0, GOLDEN)
+    import make_ps_golden as ps
+    d = str(tmp_path / "ps")
+    ps.write_case_inputs(d)
+    tdem_oracle.run(d, variant[0], int(variant[1]))
+    for o in ps.OUTPUTS:
+        err = outs.compare_files(os.path.join(d, o + ".1"), os.path.join(GOLDEN, ps.CASE, "%s_%s.1" % (variant, o)))
+        assert err <= FP64_TOL, (o, err)

@@ -78,3 +78,22 @@ def test_plan_digest_independent_of_host_threads(pkg, mg, tmp_path, monkeypatch)
     assert len(set(digests.values())) == 1, digests
     # the digest does see a different ordering
     assert pkg.plan(d, "E", 2, leaf_size=48)["digest"] != digests["1"]
+
+
+def test_plan_primary_secondary_mode(pkg, tmp_path):
+    """fdirect 0 with anomalous edges: the A-formulation plans (the normal field is read
+    per step); the E-formulation is refused with a clear message."""
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    import make_ps_golden as ps
+    d = str(tmp_path / "ps")
+    ps.write_case_inputs(d)
+    p = pkg.plan(d, "A", 3)
+    _counts_consistent(p)
+    with pytest.raises(pkg.TdemError) as ei:
+        pkg.plan(d, "E", 2)
+    assert ei.value.status == 2 and "A-formulation only" in str(ei.value)
+    os.unlink(os.path.join(d, "PName"))
+    with pytest.raises(pkg.TdemError) as ei:
+        pkg.plan(d, "A", 2)
+    assert "PName" in str(ei.value)
