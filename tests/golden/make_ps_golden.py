@@ -1,5 +1,5 @@
 """Golden fixtures of the primary-secondary mode (fdirect = 0 with a normal field):
-the reference's own CalcNonstat3DLine_{A2,A3} built from source by
+the reference's own CalcNonstat3DLine_{A2,A3,E2,E3} built from source by
 oracle/build_ref.sh, run on the golden case cube8_block turned into a
 primary-secondary problem:
 
@@ -31,7 +31,7 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 CASE = "cube8_block_ps"
 BASE = "cube8_block"
 PNAME = "tdemps"
-VARIANTS = ("A2", "A3")
+VARIANTS = ("A2", "A3", "E2", "E3")
 OUTPUTS = ("eall_anom", "edsall_anom", "ball_anom")
 
 

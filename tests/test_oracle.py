@@ -148,10 +148,12 @@ def test_reference_build_reproduces_primary_secondary_goldens(outs, tmp_path):
     assert outs.compare_files(os.path.join(d, "eall_anom.1"), os.path.join(GOLDEN, ps.CASE, "A2_eall_anom.1")) > 0.1
 
 
-@pytest.mark.parametrize("variant", ["A2", "A3"])
+@pytest.mark.parametrize("variant", ["A2", "A3", "E2", "E3"])
 def test_numpy_oracle_primary_secondary_matches_reference(outs, tmp_path, variant):
-    """The restatement of the primary-secondary source (C_dsigma times the normal
-    field's edge values, time_approx.cpp:671-683, 1263-1348) against the reference."""
+    """The restatement of the primary-secondary source against the reference: C_dsigma
+    times the normal field's edge values (A, time_approx.cpp:671-683, 1263-1348) or
+    times minus their time derivative, layer 0 from the normal potential (E,
+    E2/time_approx.cpp:1384-1431, E3/time_approx.cpp:1400-1460)."""
     import sys
     sys.path.insert(0, GOLDEN)
     import make_ps_golden as ps
