@@ -201,20 +201,11 @@ std::string TransientSolve::plan(const std::string& dir, const RunOptions& opt) 
   // primary-secondary mode: the normal field of the anomalous edges is the source
   // (time_approx.cpp:351-368, 671-683, 1263-1348)
   ps_ = !m_.fdirect && m_.n_anom > 0;
-  anom_idx_.clear();
-  anom_len_.clear();
+  nf_ = NormalField();
   if (ps_) {
-    if (opt.formulation == 1)
-      return "primary-secondary mode (fdirect 0 with mtrsizeforE0) is built for the A-formulation only";
     if (m_.pname.empty()) return "cannot read PName (it names the normal-field files m<PName>.enor.NNNN)";
-    for (int i = 0; i < n_; ++i) {
-      if (!m_.edge_anom[i]) continue;
-      const auto& a = m_.xyz[m_.edge_nodes[i][0]];
-      const auto& b = m_.xyz[m_.edge_nodes[i][1]];
-      const double d0 = b[0] - a[0], d1 = b[1] - a[1], d2 = b[2] - a[2];
-      anom_idx_.push_back(i);
-      anom_len_.push_back(std::sqrt(d0 * d0 + d1 * d1 + d2 * d2));
-    }
+    e = init_normal_field(m_, opt.formulation == 1, nf_);
+    if (!e.empty()) return e;
   }
 
   // the initial field, the source vectors and the receiver operators read only the
@@ -306,7 +297,7 @@ int64_t TransientSolve::device_bytes_needed() const {
   b += 8 * (int64_t)(rop_b_.val.size() + rop_e_.val.size()) * 3;        // receiver operators (approx.)
   b += 8 * (int64_t)(tll_ - tlf_ + 1) * 3 * (rop_b_.nrec + rop_e_.nrec) + 8 * ntime_;
   b += (int64_t)m_.n_elem * (12 * 4 + 5 * 8 + 4);                       // assembly inputs
-  if (ps_) b += 8 * nnz + 8 * nn * np + (int64_t)anom_idx_.size() * (4 * np + 12);  // C_dsigma, En, staging
+  if (ps_) b += 8 * nnz + 8 * nn * np + (int64_t)nf_.idx.size() * (4 * np + 12);  // C_dsigma, En, staging
   return b;
 }
 
@@ -440,10 +431,10 @@ std::string TransientSolve::setup_device(cudaStream_t stream) {
       const size_t ve = sizeof(double) * (size_t)n_ * npls_;
       if (!(e = alloc((void**)&d_En_, ve)).empty()) return e;
       TRY_CUDA(cudaMemsetAsync(d_En_, 0, ve, s_));  // entries of normal edges stay 0
-      if (!(e = alloc((void**)&d_Ef_, sizeof(float) * anom_idx_.size() * npls_)).empty()) return e;
-      if (!(e = upload(&d_anom_, anom_idx_)).empty()) return e;
-      if (!(e = upload(&d_alen_, anom_len_)).empty()) return e;
-      ef_host_.assign(anom_idx_.size() * (size_t)npls_, 0.0f);
+      if (!(e = alloc((void**)&d_Ef_, sizeof(float) * nf_.idx.size() * npls_)).empty()) return e;
+      if (!(e = upload(&d_anom_, nf_.idx)).empty()) return e;
+      if (!(e = upload(&d_alen_, nf_.len)).empty()) return e;
+      ef_host_.assign(nf_.idx.size() * (size_t)npls_, 0.0f);
     }
     TRY_CUDA(cudaStreamSynchronize(s_));
     TRY_CUDA(cudaGetLastError());
@@ -493,7 +484,7 @@ std::string TransientSolve::step(int itime, int t1, int t2, double m1, double m2
   launch_history_rhs(d_rowptr_, d_col_, d_C_, u1, u2, m1, (t2 >= 0) ? m2 : 0.0, d_S_, coef, d_bound_, n_, npls_,
                      d_rhs_, s_);
   if (ps_) {
-    const std::string se = anomaly_source(itime);
+    const std::string se = anomaly_source(itime, t1, t2);
     if (!se.empty()) return se;
   }
   std::string e = (opt_.precision == 32) ? refine(d_x_) : chol_->solve_graph(d_rhs_, d_x_, n_, npls_, s_, slot_);
@@ -504,12 +495,25 @@ std::string TransientSolve::step(int itime, int t1, int t2, double m1, double m2
   return "";
 }
 
-// The normal field of layer itime, float32 per anomalous edge (ascending) and source
-// (source-major), from the file m<PName>.enor.<itime as %04d> in the model directory:
-// the Linux stand-in for the named shared memory the reference maps
-// (time_approx.cpp:1263-1348).  Its edge values f * len / 2 times C_dsigma are added
-// to the right-hand side of the step.
-std::string TransientSolve::anomaly_source(int itime) {
+// Primary-secondary source of the step to layer itime (history layers t1, t2).
+// A-form: the normal field of layer itime, float32 per anomalous edge (ascending)
+// and source (source-major), from the file m<PName>.enor.<itime as %04d> in the model
+// directory, the Linux stand-in for the named shared memory the reference maps
+// (time_approx.cpp:1263-1348); it is scaled onto the edges on the device.  E-form:
+// minus its rate over the history layers, formed on the host on every edge (layer 0,
+// the normal potential's gradient, is dense) and copied whole.  Either is multiplied
+// by C_dsigma and added to the right-hand side.
+std::string TransientSolve::anomaly_source(int itime, int t1, int t2) {
+  if (opt_.formulation == 1) {
+    const bool three = opt_.scheme == 3 && itime > 2 && t2 >= 0;
+    const std::string e = normal_field_rate(m_, nf_, itime, t1, t2, three, en_host_);
+    if (!e.empty()) return e;
+    TRY_CUDA(cudaMemcpyAsync(d_En_, en_host_.data(), sizeof(double) * en_host_.size(), cudaMemcpyHostToDevice, s_));
+    pt_.h2d_bytes += (int64_t)(sizeof(double) * en_host_.size());
+    launch_anomaly_rhs(d_rowptr_, d_col_, d_Cds_, d_En_, d_bound_, n_, npls_, d_rhs_, s_);
+    launches_ += 1;
+    return "";
+  }
   char name[512];
   std::snprintf(name, sizeof name, "%s/m%s.enor.%04d", m_.dir.c_str(), m_.pname.c_str(), itime);
   FILE* f = std::fopen(name, "rb");
@@ -520,7 +524,7 @@ std::string TransientSolve::anomaly_source(int itime) {
   if (got != want) return std::string("normal field too short: ") + name;
   TRY_CUDA(cudaMemcpyAsync(d_Ef_, ef_host_.data(), sizeof(float) * want, cudaMemcpyHostToDevice, s_));
   pt_.h2d_bytes += (int64_t)(sizeof(float) * want);
-  launch_normal_field(d_Ef_, d_anom_, d_alen_, (int)anom_idx_.size(), n_, npls_, d_En_, s_);
+  launch_normal_field(d_Ef_, d_anom_, d_alen_, (int)nf_.idx.size(), n_, npls_, d_En_, s_);
   launch_anomaly_rhs(d_rowptr_, d_col_, d_Cds_, d_En_, d_bound_, n_, npls_, d_rhs_, s_);
   launches_ += 2;
   return "";

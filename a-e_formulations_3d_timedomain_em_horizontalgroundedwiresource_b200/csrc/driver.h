@@ -112,9 +112,9 @@ class TransientSolve {
   // pattern, the normal field of the current layer as edge values, its float copy
   // as read, the anomalous edges and their lengths
   bool ps_ = false;
-  std::vector<int> anom_idx_;
-  std::vector<double> anom_len_;
-  std::vector<float> ef_host_;
+  NormalField nf_;
+  std::vector<float> ef_host_;   // A-form: one layer as read
+  std::vector<double> en_host_;  // E-form: the step's source values on every edge
   double* d_Cds_ = nullptr;
   double* d_En_ = nullptr;
   float* d_Ef_ = nullptr;
@@ -159,8 +159,9 @@ class TransientSolve {
   // source vectors and receiver operators of the planned model (reads the model only)
   std::string build_sources_and_receivers();
   std::string step(int itime, int t1, int t2, double m1, double m2, double coef);
-  // adds C_dsigma * En(itime) to the step's right-hand side (primary-secondary mode)
-  std::string anomaly_source(int itime);
+  // adds C_dsigma times the normal field of layer itime (A) or minus its rate over
+  // the step's history layers (E) to the step's right-hand side (primary-secondary mode)
+  std::string anomaly_source(int itime, int t1, int t2);
   void eval_receivers(int t);
   double source_coef(int itime, bool two_layer, double dt) const;
 };

@@ -418,4 +418,74 @@ void edge_pattern(const Model& m, std::vector<int64_t>& rowptr, std::vector<int>
   });
 }
 
+std::string init_normal_field(const Model& m, bool eform, NormalField& nf) {
+  nf = NormalField();
+  auto length = [&](int i) {
+    const auto& a = m.xyz[m.edge_nodes[i][0]];
+    const auto& b = m.xyz[m.edge_nodes[i][1]];
+    const double d0 = b[0] - a[0], d1 = b[1] - a[1], d2 = b[2] - a[2];
+    return std::sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+  };
+  for (int i = 0; i < m.n_edges; ++i)
+    if (m.edge_anom[i]) {
+      nf.idx.push_back(i);
+      nf.len.push_back(length(i));
+    }
+  if (!eform) return "";
+  const size_t nv = (size_t)m.n_nodes * m.npls;
+  std::vector<double> V(nv);
+  if (!read_binary(path(m, "v3n.dat"), V.data(), nv * sizeof(double)))
+    return "cannot read v3n.dat (the normal potential, layer 0 of the normal field)";
+  nf.e0.assign((size_t)m.n_edges * m.npls, 0.0);
+  for (int p = 0; p < m.npls; ++p)
+    for (int i = 0; i < m.n_edges; ++i) {
+      const int v1 = m.edge_nodes[i][0], v2 = m.edge_nodes[i][1];
+      const double len = length(i);
+      const double etan = -(V[v2 + (size_t)p * m.n_nodes] - V[v1 + (size_t)p * m.n_nodes]) / len;
+      nf.e0[i + (size_t)p * m.n_edges] = etan * len * 0.5;
+    }
+  return "";
+}
+
+std::string normal_field_layer(const Model& m, const NormalField& nf, int layer, std::vector<double>& out) {
+  const size_t n = (size_t)m.n_edges;
+  if (layer == 0 && !nf.e0.empty()) {
+    out = nf.e0;
+    return "";
+  }
+  out.assign(n * m.npls, 0.0);
+  char name[512];
+  std::snprintf(name, sizeof name, "%s/m%s.enor.%04d", m.dir.c_str(), m.pname.c_str(), layer);
+  FILE* f = std::fopen(name, "rb");
+  if (!f) return std::string("cannot open the normal field ") + name;
+  std::vector<float> v(nf.idx.size() * (size_t)m.npls);
+  const size_t got = std::fread(v.data(), sizeof(float), v.size(), f);
+  std::fclose(f);
+  if (got != v.size()) return std::string("normal field too short: ") + name;
+  for (int p = 0; p < m.npls; ++p)
+    for (size_t k = 0; k < nf.idx.size(); ++k)
+      out[nf.idx[k] + (size_t)p * n] = v[k + (size_t)p * nf.idx.size()] * nf.len[k] * 0.5;
+  return "";
+}
+
+std::string normal_field_rate(const Model& m, const NormalField& nf, int it, int t1, int t2, bool three_point,
+                              std::vector<double>& out) {
+  std::vector<double> e1, e2;
+  std::string e = normal_field_layer(m, nf, it, out);
+  if (e.empty()) e = normal_field_layer(m, nf, t1, e1);
+  if (!e.empty()) return e;
+  const std::vector<double>& t = m.time;
+  if (!three_point) {
+    for (size_t j = 0; j < out.size(); ++j) out[j] = -(out[j] - e1[j]) / (t[it] - t[t1]);
+    return "";
+  }
+  if (!(e = normal_field_layer(m, nf, t2, e2)).empty()) return e;
+  const double tj = t[it], tj1 = t[t1], tj2 = t[t2], tt = t[it];
+  const double dt = tj - tj2, dt0 = tj - tj1, dt1 = tj1 - tj2;
+  for (size_t j = 0; j < out.size(); ++j)
+    out[j] = -(e2[j] * (2.0 * tt - tj - tj1) / (dt1 * dt) - e1[j] * (2.0 * tt - tj - tj2) / (dt1 * dt0) +
+               out[j] * (2.0 * tt - tj1 - tj2) / (dt * dt0));
+  return "";
+}
+
 }  // namespace tdem

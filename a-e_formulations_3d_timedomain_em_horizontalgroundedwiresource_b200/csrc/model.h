@@ -72,4 +72,27 @@ void edge_pattern(const Model& m, std::vector<int64_t>& rowptr, std::vector<int>
 // (-0.01, 1.01), as LoadAndInitCurrent does (vec_prep_data.cpp:1050-1183).
 std::string locate_dipoles(Model& m);
 
+// Primary-secondary mode: the normal field of the anomalous edges (m.edge_anom) as
+// edge values, in the reference's scaling f * len / 2.
+struct NormalField {
+  std::vector<int> idx;      // anomalous edges, ascending
+  std::vector<double> len;   // their lengths
+  std::vector<double> e0;    // E-form: layer 0 on every edge and source (-grad V of v3n.dat)
+};
+
+// Builds the anomalous-edge list; for the E-formulation also layer 0 from the normal
+// potential v3n.dat (E2/time_approx.cpp:1384-1412).
+std::string init_normal_field(const Model& m, bool eform, NormalField& nf);
+
+// Layer `layer` of the normal field on every edge and source (n_edges x npls,
+// source-major): layer 0 of the E-formulation from nf.e0, otherwise the float32 file
+// m<PName>.enor.NNNN on the anomalous edges and 0 elsewhere (time_approx.cpp:1263-1348).
+std::string normal_field_layer(const Model& m, const NormalField& nf, int layer, std::vector<double>& out);
+
+// The E-formulation's source values of the step to layer `it` with history layers t1
+// (and t2): minus the time derivative of the normal field, two-point, or three-point
+// when `three_point` (E2/time_approx.cpp:1419-1431, E3/time_approx.cpp:1400-1460).
+std::string normal_field_rate(const Model& m, const NormalField& nf, int it, int t1, int t2, bool three_point,
+                              std::vector<double>& out);
+
 }  // namespace tdem

@@ -47,10 +47,11 @@ typedef enum tdem_status {
  * direct-mode input files there, runs the transient on CUDA device `device` and
  * writes edsall_anom.N, ball_anom.N and eall_anom.N (N = 1-based source index) in
  * the reference's text format.  errbuf (may be NULL) receives a message on failure.
- * Primary-secondary mode (fdirect 0 with mtrsizeforE0 flagging anomalous edges,
- * A-formulation): the normal field of each time layer is read from the file
- * m<PName>.enor.NNNN in `workdir` (float32 per anomalous edge and source), the
- * stand-in for the named shared memory the reference maps (time_approx.cpp:1263-1348). 
+ * Primary-secondary mode (fdirect 0 with mtrsizeforE0 flagging anomalous edges): the
+ * normal field of each time layer is read from the file m<PName>.enor.NNNN in
+ * `workdir` (float32 per anomalous edge and source), the stand-in for the named
+ * shared memory the reference maps (time_approx.cpp:1263-1348); the E-formulation
+ * also reads the normal potential v3n.dat for layer 0. 
  * Replaces: GeoCalculatorSP.cpp:1656-1662 -> CalcNonstat3DLine main -> CalcSP
  * (TaskSP.cpp:445-711). */
 tdem_status tdem_run_directory(const char* workdir, int formulation, int scheme, int device,

@@ -203,6 +203,36 @@ def normal_field(m: Dict, it: int) -> np.ndarray:
     return En
 
 
+def normal_field_layer(m: Dict, it: int) -> np.ndarray:
+    """Layer it of the normal field on the edges for the E-formulation; layer 0 is
+    -grad of the normal potential v3n.dat on every edge (E2/time_approx.cpp:1384-1412)."""
+    if it > 0:
+        return normal_field(m, it)
+    npls = m["npls"]
+    V = np.fromfile(os.path.join(m["dir"], "v3n.dat"), "<f8")[: m["kuzlov"] * npls].reshape(npls, m["kuzlov"])
+    v1, v2 = m["edges"][:, 0], m["edges"][:, 1]
+    ax = m["xyz"][v2] - m["xyz"][v1]
+    ln = np.sqrt(ax[:, 0] * ax[:, 0] + ax[:, 1] * ax[:, 1] + ax[:, 2] * ax[:, 2])
+    etan = -(V[:, v2] - V[:, v1]) / ln
+    return (etan * ln * 0.5).T
+
+
+def normal_field_rate(m: Dict, it: int, t1: int, t2: int, three_point: bool) -> np.ndarray:
+    """Minus the time derivative of the normal field at layer it: two-point over
+    (it, t1), or three-point over (it, t1, t2) (E2/time_approx.cpp:1419-1431,
+    E3/time_approx.cpp:1400-1460)."""
+    t = m["time"]
+    e0, e1 = normal_field_layer(m, it), normal_field_layer(m, t1)
+    if not three_point:
+        return -(e0 - e1) / (t[it] - t[t1])
+    e2 = normal_field_layer(m, t2)
+    tj, tj1, tj2 = t[it], t[t1], t[t2]
+    dt, dt0, dt1 = tj - tj2, tj - tj1, tj1 - tj2
+    tt = tj
+    return -(e2 * (2.0 * tt - tj - tj1) / (dt1 * dt) - e1 * (2.0 * tt - tj - tj2) / (dt1 * dt0)
+             + e0 * (2.0 * tt - tj1 - tj2) / (dt * dt0))
+
+
 # ---------------------------------------------------------------------------
 # initial field and source
 # ---------------------------------------------------------------------------
@@ -448,35 +478,11 @@ def run(d: str, formulation: str, scheme: int) -> Dict:
 
     ps = (not m["fdirect"]) and bool(m["anom"].any())
 
-    def e_layer(it):
-        """Normal field of layer it on the edges; layer 0 is -grad of the normal
-        potential v3n.dat on every edge (E2/time_approx.cpp:1384-1412)."""
-        if it > 0:
-            return normal_field(m, it)
-        V = np.fromfile(os.path.join(d, "v3n.dat"), "<f8")[: m["kuzlov"] * npls].reshape(npls, m["kuzlov"])
-        v1, v2 = m["edges"][:, 0], m["edges"][:, 1]
-        ax = m["xyz"][v2] - m["xyz"][v1]
-        ln = np.sqrt(ax[:, 0] * ax[:, 0] + ax[:, 1] * ax[:, 1] + ax[:, 2] * ax[:, 2])
-        etan = -(V[:, v2] - V[:, v1]) / ln
-        return (etan * ln * 0.5).T
-
     def ps_source(it, t1, t2):
-        """C_dsigma times the normal field (A) or its time derivative, negated (E):
-        two-point, or three-point past the first layers of the three-point scheme
-        (E3/time_approx.cpp:1400-1460)."""
+        """C_dsigma times the normal field (A) or minus its time derivative (E)."""
         if not eform:
             return m["Cds"] @ normal_field(m, it)
-        e0, e1 = e_layer(it), e_layer(t1)
-        if scheme == 2 or it <= 2:
-            en = -(e0 - e1) / (t[it] - t[t1])
-        else:
-            e2 = e_layer(t2)
-            tj, tj1, tj2 = t[it], t[t1], t[t2]
-            dt, dt0, dt1 = tj - tj2, tj - tj1, tj1 - tj2
-            tt = tj
-            en = -(e2 * (2.0 * tt - tj - tj1) / (dt1 * dt) - e1 * (2.0 * tt - tj - tj2) / (dt1 * dt0)
-                   + e0 * (2.0 * tt - tj1 - tj2) / (dt * dt0))
-        return m["Cds"] @ en
+        return m["Cds"] @ normal_field_rate(m, it, t1, t2, scheme == 3 and it > 2)
 
     def step(it, t1, t2, m1, m2, c):
         hist = U[t1] * m1 + (U[t2] * m2 if m2 != 0 else 0.0)

@@ -80,11 +80,12 @@ def test_drop_in_executable(pkg, golden, outs, tmp_path):
         assert err <= FP64_TOL
 
 
-@pytest.mark.parametrize("variant", ["A2", "A3"])
+@pytest.mark.parametrize("variant", ["A2", "A3", "E2", "E3"])
 def test_gpu_primary_secondary_matches_reference(pkg, outs, tmp_path, variant):
     """Primary-secondary mode (fdirect 0): the normal field of every layer, read from the
-    m<PName>.enor.NNNN files, drives the anomalous block through C_dsigma; against the
-    reference's own outputs on the same files."""
+    m<PName>.enor.NNNN files, drives the anomalous block through C_dsigma (the field
+    itself for A, minus its time derivative for E); against the reference's own
+    outputs on the same files."""
     import sys
     sys.path.insert(0, GOLDEN)
     import make_ps_golden as ps

@@ -81,18 +81,20 @@ def test_plan_digest_independent_of_host_threads(pkg, mg, tmp_path, monkeypatch)
 
 
 def test_plan_primary_secondary_mode(pkg, tmp_path):
-    """fdirect 0 with anomalous edges: the A-formulation plans (the normal field is read
-    per step); the E-formulation is refused with a clear message."""
+    """fdirect 0 with anomalous edges: both formulations plan (the normal field is read
+    per step); the E-formulation also needs the normal potential v3n.dat (layer 0)."""
     import sys
     sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
     import make_ps_golden as ps
     d = str(tmp_path / "ps")
     ps.write_case_inputs(d)
-    p = pkg.plan(d, "A", 3)
-    _counts_consistent(p)
+    for form, scheme in (("A", 3), ("E", 2)):
+        _counts_consistent(pkg.plan(d, form, scheme))
+    os.unlink(os.path.join(d, "v3n.dat"))
     with pytest.raises(pkg.TdemError) as ei:
-        pkg.plan(d, "E", 2)
-    assert ei.value.status == 2 and "A-formulation only" in str(ei.value)
+        pkg.plan(d, "E", 3)
+    assert ei.value.status == 2 and "v3n.dat" in str(ei.value)
+    pkg.plan(d, "A", 2)  # the A-formulation does not read it
     os.unlink(os.path.join(d, "PName"))
     with pytest.raises(pkg.TdemError) as ei:
         pkg.plan(d, "A", 2)
