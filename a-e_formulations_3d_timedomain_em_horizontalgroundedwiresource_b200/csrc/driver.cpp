@@ -514,9 +514,8 @@ std::string TransientSolve::anomaly_source(int itime, int t1, int t2) {
     launches_ += 1;
     return "";
   }
-  char name[512];
-  std::snprintf(name, sizeof name, "%s/m%s.enor.%04d", m_.dir.c_str(), m_.pname.c_str(), itime);
-  FILE* f = std::fopen(name, "rb");
+  const std::string name = normal_field_file(m_, itime);
+  FILE* f = std::fopen(name.c_str(), "rb");
   if (!f) return std::string("cannot open the normal field ") + name;
   const size_t want = ef_host_.size();
   const size_t got = std::fread(ef_host_.data(), sizeof(float), want, f);

@@ -181,6 +181,15 @@ std::string load_model(const std::string& dir, Model& m) {
     }
     std::ifstream pn(path(m, "PName"));
     if (pn) pn >> m.pname;
+    // one anomaly of several (TaskSP.cpp:539-596): its index names the normal-field files
+    int at = 0;
+    m.anomal_type = read_one(path(m, "AnomalType"), at) ? at : 0;
+    m.anomaly = -1;
+    if (m.anomal_type) {
+      std::ifstream ia(path(m, "ia"));
+      if (!ia) return "cannot open ia (AnomalType is set)";
+      ia >> m.anomaly;
+    }
   }
 
   // --- time grid infite.0 (vec_prep_data.cpp:834-853) -----------------------------
@@ -447,6 +456,15 @@ std::string init_normal_field(const Model& m, bool eform, NormalField& nf) {
   return "";
 }
 
+std::string normal_field_file(const Model& m, int layer) {
+  char num[48];
+  if (m.anomal_type)
+    std::snprintf(num, sizeof num, "%04d_%d", layer, m.anomaly);
+  else
+    std::snprintf(num, sizeof num, "%04d", layer);
+  return m.dir + "/m" + m.pname + ".enor." + num;
+}
+
 std::string normal_field_layer(const Model& m, const NormalField& nf, int layer, std::vector<double>& out) {
   const size_t n = (size_t)m.n_edges;
   if (layer == 0 && !nf.e0.empty()) {
@@ -454,9 +472,8 @@ std::string normal_field_layer(const Model& m, const NormalField& nf, int layer,
     return "";
   }
   out.assign(n * m.npls, 0.0);
-  char name[512];
-  std::snprintf(name, sizeof name, "%s/m%s.enor.%04d", m.dir.c_str(), m.pname.c_str(), layer);
-  FILE* f = std::fopen(name, "rb");
+  const std::string name = normal_field_file(m, layer);
+  FILE* f = std::fopen(name.c_str(), "rb");
   if (!f) return std::string("cannot open the normal field ") + name;
   std::vector<float> v(nf.idx.size() * (size_t)m.npls);
   const size_t got = std::fread(v.data(), sizeof(float), v.size(), f);

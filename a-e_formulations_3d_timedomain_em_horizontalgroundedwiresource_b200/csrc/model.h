@@ -51,6 +51,8 @@ struct Model {
   std::vector<char> edge_anom;
   int n_anom = 0;
   std::string pname;
+  int anomal_type = 0;  // AnomalType: nonzero when each anomaly has its own normal-field files
+  int anomaly = -1;     // ia: the anomaly of this run (file suffix _<ia>)
   // derived
   std::vector<char> edge_bound;               // Dirichlet edge flag
   std::string dir;
@@ -83,6 +85,10 @@ struct NormalField {
 // Builds the anomalous-edge list; for the E-formulation also layer 0 from the normal
 // potential v3n.dat (E2/time_approx.cpp:1384-1412).
 std::string init_normal_field(const Model& m, bool eform, NormalField& nf);
+
+// File of layer `layer` of the normal field: <dir>/m<PName>.enor.NNNN, with the suffix
+// _<ia> when AnomalType is set (time_approx.cpp:1280-1287).
+std::string normal_field_file(const Model& m, int layer);
 
 // Layer `layer` of the normal field on every edge and source (n_edges x npls,
 // source-major): layer 0 of the E-formulation from nf.e0, otherwise the float32 file

@@ -109,6 +109,11 @@ def read_model(d: str) -> Dict:
         m["anom"] = np.array([int(v) for v in open(mf).read().split()[:m["n"]]]) != 0
     pn = os.path.join(d, "PName")
     m["pname"] = open(pn).read().split()[0] if os.path.exists(pn) else ""
+    # one anomaly of several: its index ia suffixes the files (TaskSP.cpp:539-596, time_approx.cpp:1280-1287)
+    at = os.path.join(d, "AnomalType")
+    m["anomaly"] = None
+    if os.path.exists(at) and int(open(at).read().split()[0]) != 0:
+        m["anomaly"] = int(open(os.path.join(d, "ia")).read().split()[0])
     m["dir"] = d
     return m
 
@@ -194,7 +199,10 @@ def normal_field(m: Dict, it: int) -> np.ndarray:
     """Normal field of layer it as edge values (time_approx.cpp:1263-1348): float32 per
     anomalous edge and source from m<PName>.enor.NNNN, times half the edge length."""
     idx = np.nonzero(m["anom"])[0]
-    f = np.fromfile(os.path.join(m["dir"], "m%s.enor.%04d" % (m["pname"], it)), "<f4")
+    name = "m%s.enor.%04d" % (m["pname"], it)
+    if m["anomaly"] is not None:
+        name += "_%d" % m["anomaly"]
+    f = np.fromfile(os.path.join(m["dir"], name), "<f4")
     f = f[: len(idx) * m["npls"]].reshape(m["npls"], len(idx)).astype(np.float64)
     ax = m["xyz"][m["edges"][idx, 1]] - m["xyz"][m["edges"][idx, 0]]
     ln = np.sqrt(ax[:, 0] * ax[:, 0] + ax[:, 1] * ax[:, 1] + ax[:, 2] * ax[:, 2])

@@ -41,8 +41,10 @@ def _time_count(d: str) -> int:
     return int(head.split(";")[0])
 
 
-def make_primary_secondary(d: str, seed: int = 7) -> None:
-    """Turns the direct-mode model in d into the primary-secondary problem above."""
+def make_primary_secondary(d: str, seed: int = 7, anomaly=None) -> None:
+    """Turns the direct-mode model in d into the primary-secondary problem above; with
+    `anomaly` the run is one anomaly of several (AnomalType 1, ia = anomaly, files
+    suffixed _<ia>)."""
     rows = [line.split() for line in open(os.path.join(d, "sig3d")) if line.strip()]
     sig = np.array([float(r[1]) for r in rows])
     background = 0.01  # the half-space of small_model
@@ -67,10 +69,15 @@ def make_primary_secondary(d: str, seed: int = 7) -> None:
     rng = np.random.default_rng(seed)
     k = rng.uniform(0.5, 2.0, (npls, 3))
     t = _infite_times(d)
+    suffix = "" if anomaly is None else "_%d" % anomaly
+    if anomaly is not None:
+        for name, v in (("AnomalType", 1), ("ia", anomaly)):
+            with open(os.path.join(d, name), "w") as f:
+                f.write("%d\n" % v)
     for it in range(1, len(t)):
         vals = np.stack([np.cos(k[p, 0] * idx / len(idx) * 6.0 + k[p, 1]) * np.exp(-t[it] / (2e-4 * k[p, 2]))
                          for p in range(npls)]) * 1e-3
-        vals.astype("<f4").tofile(os.path.join(d, "m%s.enor.%04d" % (PNAME, it)))
+        vals.astype("<f4").tofile(os.path.join(d, "m%s.enor.%04d%s" % (PNAME, it, suffix)))
 
 
 def _infite_times(d: str):
@@ -82,32 +89,45 @@ def _infite_times(d: str):
 
 
 def ps_files(d: str):
-    return ["sig3d", "fdirect", "PName", "mtrsizeforE0"] + sorted(f for f in os.listdir(d) if f.startswith("m" + PNAME))
+    extra = [f for f in ("AnomalType", "ia") if os.path.exists(os.path.join(d, f))]
+    return ["sig3d", "fdirect", "PName", "mtrsizeforE0"] + extra + sorted(
+        f for f in os.listdir(d) if f.startswith("m" + PNAME))
 
 
-def write_case_inputs(path: str) -> None:
-    """cube8_block's inputs with the stored primary-secondary files."""
+def write_case_inputs(path: str, case: str = CASE) -> None:
+    """cube8_block's inputs with the stored primary-secondary files of `case`."""
     import make_golden
     make_golden.write_case_inputs(BASE, path)
-    src = os.path.join(HERE, CASE)
+    src = os.path.join(HERE, case)
     for f in os.listdir(src):
         if not f.startswith(VARIANTS):
             shutil.copy2(os.path.join(src, f), os.path.join(path, f))
 
 
+# the second case: one anomaly of several (file suffix _2), A2 and E3 only
+CASE_IA = "cube8_block_ps_ia"
+ANOMALY = 2
+VARIANTS_IA = ("A2", "E3")
+
+
 def main() -> None:
+    for case, anomaly, variants in ((CASE, None, VARIANTS), (CASE_IA, ANOMALY, VARIANTS_IA)):
+        make_case(case, anomaly, variants)
+
+
+def make_case(case, anomaly, variants) -> None:
     import make_golden
     import run_ref
-    out = os.path.join(HERE, CASE)
+    out = os.path.join(HERE, case)
     shutil.rmtree(out, ignore_errors=True)
     os.makedirs(out)
     work = tempfile.mkdtemp(prefix="golden_ps_")
     try:
         make_golden.write_case_inputs(BASE, work)
-        make_primary_secondary(work)
+        make_primary_secondary(work, anomaly=anomaly)
         for f in ps_files(work):
             shutil.copy2(os.path.join(work, f), os.path.join(out, f))
-        for v in VARIANTS:
+        for v in variants:
             d = os.path.join(work, v)
             run_ref.copy_inputs(work, d)
             run_ref.run_transient(d, v)

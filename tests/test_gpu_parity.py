@@ -80,8 +80,9 @@ def test_drop_in_executable(pkg, golden, outs, tmp_path):
         assert err <= FP64_TOL
 
 
-@pytest.mark.parametrize("variant", ["A2", "A3", "E2", "E3"])
-def test_gpu_primary_secondary_matches_reference(pkg, outs, tmp_path, variant):
+@pytest.mark.parametrize("case,variant", [("cube8_block_ps", v) for v in ("A2", "A3", "E2", "E3")] +
+                         [("cube8_block_ps_ia", v) for v in ("A2", "E3")])
+def test_gpu_primary_secondary_matches_reference(pkg, outs, tmp_path, case, variant):
     """Primary-secondary mode (fdirect 0): the normal field of every layer, read from the
     m<PName>.enor.NNNN files, drives the anomalous block through C_dsigma (the field
     itself for A, minus its time derivative for E); against the reference's own
@@ -90,10 +91,10 @@ def test_gpu_primary_secondary_matches_reference(pkg, outs, tmp_path, variant):
     sys.path.insert(0, GOLDEN)
     import make_ps_golden as ps
     d = str(tmp_path / "ps")
-    ps.write_case_inputs(d)
+    ps.write_case_inputs(d, case)
     with pkg.Solver(d, variant[0], int(variant[1])) as s:
         s.run()
         s.write_outputs()
     for o in ps.OUTPUTS:
-        err = outs.compare_files(os.path.join(d, o + ".1"), os.path.join(GOLDEN, ps.CASE, "%s_%s.1" % (variant, o)))
+        err = outs.compare_files(os.path.join(d, o + ".1"), os.path.join(GOLDEN, case, "%s_%s.1" % (variant, o)))
         assert err <= FP64_TOL, (o, err)

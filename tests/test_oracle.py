@@ -148,8 +148,9 @@ def test_reference_build_reproduces_primary_secondary_goldens(outs, tmp_path):
     assert outs.compare_files(os.path.join(d, "eall_anom.1"), os.path.join(GOLDEN, ps.CASE, "A2_eall_anom.1")) > 0.1
 
 
-@pytest.mark.parametrize("variant", ["A2", "A3", "E2", "E3"])
-def test_numpy_oracle_primary_secondary_matches_reference(outs, tmp_path, variant):
+@pytest.mark.parametrize("case,variant", [("cube8_block_ps", v) for v in ("A2", "A3", "E2", "E3")] +
+                         [("cube8_block_ps_ia", v) for v in ("A2", "E3")])
+def test_numpy_oracle_primary_secondary_matches_reference(outs, tmp_path, case, variant):
     """The restatement of the primary-secondary source against the reference: C_dsigma
     times the normal field's edge values (A, time_approx.cpp:671-683, 1263-1348) or
     times minus their time derivative, layer 0 from the normal potential (E,
@@ -158,8 +159,8 @@ def test_numpy_oracle_primary_secondary_matches_reference(outs, tmp_path, varian
     sys.path.insert(0, GOLDEN)
     import make_ps_golden as ps
     d = str(tmp_path / "ps")
-    ps.write_case_inputs(d)
+    ps.write_case_inputs(d, case)
     tdem_oracle.run(d, variant[0], int(variant[1]))
     for o in ps.OUTPUTS:
-        err = outs.compare_files(os.path.join(d, o + ".1"), os.path.join(GOLDEN, ps.CASE, "%s_%s.1" % (variant, o)))
+        err = outs.compare_files(os.path.join(d, o + ".1"), os.path.join(GOLDEN, case, "%s_%s.1" % (variant, o)))
         assert err <= FP64_TOL, (o, err)

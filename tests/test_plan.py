@@ -99,3 +99,16 @@ def test_plan_primary_secondary_mode(pkg, tmp_path):
     with pytest.raises(pkg.TdemError) as ei:
         pkg.plan(d, "A", 2)
     assert "PName" in str(ei.value)
+
+
+def test_plan_anomaly_index_required_with_anomal_type(pkg, tmp_path):
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    import make_ps_golden as ps
+    d = str(tmp_path / "ps")
+    ps.write_case_inputs(d, ps.CASE_IA)
+    _counts_consistent(pkg.plan(d, "E", 3))
+    os.unlink(os.path.join(d, "ia"))
+    with pytest.raises(pkg.TdemError) as ei:
+        pkg.plan(d, "A", 2)
+    assert ei.value.status == 2 and "ia" in str(ei.value)

@@ -17,7 +17,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 
 @pytest.mark.skipif(shutil.which("g++") is None, reason="no C++ compiler")
-def test_normal_field_rate_matches_oracle(pkg, tmp_path):
+@pytest.mark.parametrize("case", ["cube8_block_ps", "cube8_block_ps_ia"])
+def test_normal_field_rate_matches_oracle(pkg, tmp_path, case):
     sys.path.insert(0, GOLDEN)
     import make_ps_golden as ps
     lib_dir = os.path.dirname(pkg.LIB_PATH)
@@ -26,7 +27,7 @@ def test_normal_field_rate_matches_oracle(pkg, tmp_path):
                     os.path.join(HERE, "native", "normal_field_rate.cpp"), "-L" + lib_dir, "-ltdem_b200",
                     "-Wl,-rpath," + lib_dir, "-o", exe], check=True)
     d = str(tmp_path / "ps")
-    ps.write_case_inputs(d)
+    ps.write_case_inputs(d, case)
     m = tdem_oracle.read_model(d)
     steps = [(1, 0, -1, 0), (2, 1, 0, 0), (3, 2, 1, 1), (4, 3, 2, 1), (8, 6, 4, 1), (12, 10, 8, 1), (5, 4, 3, 0)]
     out = str(tmp_path / "rate.bin")
