@@ -378,29 +378,9 @@ std::string TransientSolve::setup_device(cudaStream_t stream) {
       imu[el] = 1.0 / m_.mu[m_.nvkat[el]];
     }
     // greedy colouring: elements sharing an edge get different colours
-    std::vector<std::vector<int>> edge_elems(n_);
-    for (int el = 0; el < m_.n_elem; ++el)
-      for (int j = 0; j < 12; ++j) edge_elems[m_.ed[el][j]].push_back(el);
-    std::vector<int> color(m_.n_elem, -1);
-    int ncol = 0;
-    for (int el = 0; el < m_.n_elem; ++el) {
-      uint64_t used = 0;
-      for (int j = 0; j < 12; ++j)
-        for (int o : edge_elems[m_.ed[el][j]])
-          if (color[o] >= 0 && color[o] < 64) used |= (1ull << color[o]);
-      int c = 0;
-      while (c < 64 && (used >> c & 1)) ++c;
-      if (c >= 64) return "element colouring needs more than 64 colours";
-      color[el] = c;
-      ncol = std::max(ncol, c + 1);
-    }
-    std::vector<int> order;
-    std::vector<int> cstart{0};
-    for (int c = 0; c < ncol; ++c) {
-      for (int el = 0; el < m_.n_elem; ++el)
-        if (color[el] == c) order.push_back(el);
-      cstart.push_back((int)order.size());
-    }
+    std::vector<int> order, cstart;
+    if (!(e = element_colouring(m_, order, cstart)).empty()) return e;
+    const int ncol = (int)cstart.size() - 1;
     int *d_ed = nullptr, *d_order = nullptr;
     double *d_h = nullptr, *d_sig = nullptr, *d_imu = nullptr;
     if (!(e = upload(&d_ed, ed)).empty()) return e;

@@ -505,4 +505,44 @@ std::string normal_field_rate(const Model& m, const NormalField& nf, int it, int
   return "";
 }
 
+std::string element_colouring(const Model& m, std::vector<int>& order, std::vector<int>& cstart) {
+  const int ne = m.n_elem, n = m.n_edges;
+  // elements of every edge, ascending (CSR)
+  std::vector<int64_t> ptr(n + 1, 0);
+  for (int el = 0; el < ne; ++el)
+    for (int j = 0; j < 12; ++j) ++ptr[m.ed[el][j] + 1];
+  for (int i = 0; i < n; ++i) ptr[i + 1] += ptr[i];
+  std::vector<int> elems(ptr[n]);
+  {
+    std::vector<int64_t> fill(ptr.begin(), ptr.end() - 1);
+    for (int el = 0; el < ne; ++el)
+      for (int j = 0; j < 12; ++j) elems[fill[m.ed[el][j]]++] = el;
+  }
+  std::vector<int> color(ne, -1);
+  int ncol = 0;
+  for (int el = 0; el < ne; ++el) {
+    uint64_t used = 0;
+    for (int j = 0; j < 12; ++j) {
+      const int ed = m.ed[el][j];
+      for (int64_t q = ptr[ed]; q < ptr[ed + 1]; ++q) {
+        const int c = color[elems[q]];
+        if (c >= 0 && c < 64) used |= (1ull << c);
+      }
+    }
+    int c = 0;
+    while (c < 64 && (used >> c & 1)) ++c;
+    if (c >= 64) return "element colouring needs more than 64 colours";
+    color[el] = c;
+    ncol = std::max(ncol, c + 1);
+  }
+  // counting sort by colour keeps the elements ascending inside a colour
+  cstart.assign(ncol + 1, 0);
+  for (int el = 0; el < ne; ++el) ++cstart[color[el] + 1];
+  for (int c = 0; c < ncol; ++c) cstart[c + 1] += cstart[c];
+  order.assign(ne, 0);
+  std::vector<int> at(cstart.begin(), cstart.end() - 1);
+  for (int el = 0; el < ne; ++el) order[at[color[el]]++] = el;
+  return "";
+}
+
 }  // namespace tdem

@@ -74,6 +74,12 @@ void edge_pattern(const Model& m, std::vector<int64_t>& rowptr, std::vector<int>
 // (-0.01, 1.01), as LoadAndInitCurrent does (vec_prep_data.cpp:1050-1183).
 std::string locate_dipoles(Model& m);
 
+// Greedy element colouring for assembly without atomics: elements in file order take
+// the lowest colour (< 64) that no element sharing an edge holds yet.  `order` lists
+// the elements colour by colour (ascending inside a colour), colour c in
+// [cstart[c], cstart[c + 1]).  Returns "" or an error when 64 colours do not suffice.
+std::string element_colouring(const Model& m, std::vector<int>& order, std::vector<int>& cstart);
+
 // Primary-secondary mode: the normal field of the anomalous edges (m.edge_anom) as
 // edge values, in the reference's scaling f * len / 2.
 struct NormalField {

@@ -112,3 +112,24 @@ def test_plan_anomaly_index_required_with_anomal_type(pkg, tmp_path):
     with pytest.raises(pkg.TdemError) as ei:
         pkg.plan(d, "A", 2)
     assert ei.value.status == 2 and "ia" in str(ei.value)
+
+
+def test_element_colouring_is_valid_and_greedy(pkg, mg, tmp_path):
+    """Assembly colours (host): conflict-free, ascending per colour, greedy (CPU driver
+    compiled against the library)."""
+    import shutil
+    import subprocess
+    if shutil.which("g++") is None:
+        pytest.skip("no C++ compiler")
+    here = os.path.dirname(os.path.abspath(__file__))
+    lib_dir = os.path.dirname(pkg.LIB_PATH)
+    exe = str(tmp_path / "colouring")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", os.path.join(os.path.dirname(pkg.__file__), "csrc"),
+                    os.path.join(here, "native", "colouring.cpp"), "-L" + lib_dir, "-ltdem_b200",
+                    "-Wl,-rpath," + lib_dir, "-o", exe], check=True)
+    d = str(tmp_path / "m")
+    spec = mg.small_model(cells=12, n_dec=2, steps_per_dec=4, block=True)
+    mg.write_model(d, spec)
+    mg.write_analytic_initial_field(d, spec)
+    r = subprocess.run([exe, d], capture_output=True, text=True)
+    assert r.returncode == 0 and r.stdout.startswith("ok"), r.stdout
