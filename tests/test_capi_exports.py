@@ -28,6 +28,21 @@ def test_library_exports_every_declared_symbol(pkg):
     assert set(pkg.EXPORTED) <= set(declared_functions())
 
 
+def test_header_is_plain_c(tmp_path):
+    """The boundary header compiles as C99 with warnings as errors (cgo, FFI and C
+    callers include it as is)."""
+    import shutil
+    import subprocess
+    import pytest
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    src = tmp_path / "use.c"
+    src.write_text('#include "tdem.h"\nint main(void) { return tdem_version() == 0; }\n')
+    subprocess.run([cc, "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    "-c", str(src), "-o", str(tmp_path / "use.o")], check=True)
+
+
 def test_version_string(pkg):
     lib = pkg.load_library()
     assert b"sm_100a" in lib.tdem_version()
