@@ -36,3 +36,30 @@ def test_normal_field_rate_matches_oracle(pkg, tmp_path, case):
     for k, (it, t1, t2, three) in enumerate(steps):
         ref = tdem_oracle.normal_field_rate(m, it, t1, t2, bool(three)).T
         assert np.array_equal(got[k], ref), (it, t1, t2, three)
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="no C++ compiler")
+def test_normal_field_errors(pkg, tmp_path):
+    """A missing or short layer file and a missing normal potential are reported."""
+    sys.path.insert(0, GOLDEN)
+    import make_ps_golden as ps
+    lib_dir = os.path.dirname(pkg.LIB_PATH)
+    exe = str(tmp_path / "rate")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", os.path.join(os.path.dirname(pkg.__file__), "csrc"),
+                    os.path.join(HERE, "native", "normal_field_rate.cpp"), "-L" + lib_dir, "-ltdem_b200",
+                    "-Wl,-rpath," + lib_dir, "-o", exe], check=True)
+    d = str(tmp_path / "ps")
+    ps.write_case_inputs(d)
+    f3 = os.path.join(d, "m%s.enor.%04d" % (ps.PNAME, 3))
+    with open(f3, "rb") as f:
+        data = f.read()
+    with open(f3, "wb") as f:
+        f.write(data[:-4])
+    r = subprocess.run([exe, d, str(tmp_path / "o.bin"), "3", "2", "1", "1"], capture_output=True, text=True)
+    assert r.returncode != 0 and "too short" in r.stdout
+    os.unlink(f3)
+    r = subprocess.run([exe, d, str(tmp_path / "o.bin"), "3", "2", "1", "1"], capture_output=True, text=True)
+    assert r.returncode != 0 and "cannot open the normal field" in r.stdout
+    os.unlink(os.path.join(d, "v3n.dat"))
+    r = subprocess.run([exe, d, str(tmp_path / "o.bin"), "2", "1", "0", "0"], capture_output=True, text=True)
+    assert r.returncode != 0 and "v3n.dat" in r.stdout
