@@ -35,6 +35,7 @@ STATUS = {
     4: "TDEM_ERR_NUMERIC",
     5: "TDEM_ERR_CANCELLED",
     6: "TDEM_ERR_STATE",
+    7: "TDEM_ERR_HOST",
 }
 
 

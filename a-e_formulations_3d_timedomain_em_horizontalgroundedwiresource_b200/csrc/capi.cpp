@@ -14,6 +14,9 @@
 
 #include "driver.h"
 #include "postprocess.h"
+
+#include <exception>
+#include <new>
 #include "timegrid.h"
 #include "gpu_cholesky.h"
 #include "server.h"
@@ -36,6 +39,7 @@ namespace {
 tdem_status classify(const std::string& e) {
   if (e.empty()) return TDEM_OK;
   if (e == "cancelled") return TDEM_ERR_CANCELLED;
+  if (e.rfind("host error", 0) == 0 || e.rfind("host memory", 0) == 0) return TDEM_ERR_HOST;
   if (e.find("cuda") != std::string::npos || e.find("CUDA") != std::string::npos) return TDEM_ERR_CUDA;
   if (e.find("non-positive pivot") != std::string::npos) return TDEM_ERR_NUMERIC;
   if (e.find("refinement") != std::string::npos) return TDEM_ERR_NUMERIC;
@@ -48,6 +52,28 @@ void put_err(char* buf, size_t len, const std::string& e) {
   buf[len - 1] = 0;
 }
 
+// Runs one entry point; a C++ exception (host memory exhausted, or any other) becomes
+// TDEM_ERR_HOST with its message in errbuf / *msg instead of crossing the C boundary.
+template <class F>
+tdem_status guard(F&& f, char* errbuf = nullptr, size_t errlen = 0, std::string* msg = nullptr) noexcept {
+  std::string what;
+  try {
+    return f();
+  } catch (const std::bad_alloc&) {
+    what = "host memory exhausted";
+  } catch (const std::exception& x) {
+    what = std::string("host error: ") + x.what();
+  } catch (...) {
+    what = "host error";
+  }
+  try {
+    put_err(errbuf, errlen, what);
+    if (msg) *msg = what;
+  } catch (...) {
+  }
+  return TDEM_ERR_HOST;
+}
+
 }  // namespace
 
 extern "C" {
@@ -56,167 +82,183 @@ const char* tdem_version(void) { return "tdem-b200 0.1 (sm_100a, FP64 multifront
 
 tdem_status tdem_solver_create(const char* workdir, int formulation, int scheme, int device,
                                tdem_solver** out) {
-  return tdem_solver_create_ex(workdir, formulation, scheme, device, nullptr, out);
+  return guard([&]() -> tdem_status {
+    return tdem_solver_create_ex(workdir, formulation, scheme, device, nullptr, out);
+  });
 }
 
 tdem_status tdem_solver_create_ex(const char* workdir, int formulation, int scheme, int device,
                                   const tdem_options* opts, tdem_solver** out) {
-  if (!workdir || !out) return TDEM_ERR_ARGUMENT;
-  *out = nullptr;
-  if ((formulation != 0 && formulation != 1) || (scheme != 2 && scheme != 3)) return TDEM_ERR_ARGUMENT;
-  auto s = std::make_unique<tdem_solver>();
-  s->device = device;
-  if (cudaSetDevice(device) != cudaSuccess) return TDEM_ERR_CUDA;
-  if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) return TDEM_ERR_CUDA;
-  tdem::RunOptions opt;
-  opt.formulation = formulation;
-  opt.scheme = scheme;
-  opt.cancel = &s->cancel;
-  if (opts) {
-    if (opts->precision) opt.precision = opts->precision;
-    if (opts->refine_tol > 0) opt.refine_tol = opts->refine_tol;
-    if (opts->refine_maxit > 0) opt.refine_maxit = opts->refine_maxit;
-    if (opts->leaf_size > 0) opt.leaf_size = opts->leaf_size;
-    if (opts->fp32_update < 0 || opts->fp32_update > 2) return TDEM_ERR_ARGUMENT;
-    opt.fp32_update = opts->fp32_update;
-    if (opts->factor_slots < 0 || opts->factor_slots > 2) return TDEM_ERR_ARGUMENT;
-    opt.factor_slots = opts->factor_slots;
-  }
-  if (opt.precision != 64 && opt.precision != 32) return TDEM_ERR_ARGUMENT;
-  s->precision = opt.precision;
-  s->error = s->solve.prepare(workdir, opt, s->stream);
-  s->prepared = s->error.empty();
-  const tdem_status st = classify(s->error);
-  *out = s.release();
-  return st;
+  return guard([&]() -> tdem_status {
+    if (!workdir || !out) return TDEM_ERR_ARGUMENT;
+    *out = nullptr;
+    if ((formulation != 0 && formulation != 1) || (scheme != 2 && scheme != 3)) return TDEM_ERR_ARGUMENT;
+    auto s = std::make_unique<tdem_solver>();
+    s->device = device;
+    if (cudaSetDevice(device) != cudaSuccess) return TDEM_ERR_CUDA;
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) return TDEM_ERR_CUDA;
+    tdem::RunOptions opt;
+    opt.formulation = formulation;
+    opt.scheme = scheme;
+    opt.cancel = &s->cancel;
+    if (opts) {
+      if (opts->precision) opt.precision = opts->precision;
+      if (opts->refine_tol > 0) opt.refine_tol = opts->refine_tol;
+      if (opts->refine_maxit > 0) opt.refine_maxit = opts->refine_maxit;
+      if (opts->leaf_size > 0) opt.leaf_size = opts->leaf_size;
+      if (opts->fp32_update < 0 || opts->fp32_update > 2) return TDEM_ERR_ARGUMENT;
+      opt.fp32_update = opts->fp32_update;
+      if (opts->factor_slots < 0 || opts->factor_slots > 2) return TDEM_ERR_ARGUMENT;
+      opt.factor_slots = opts->factor_slots;
+    }
+    if (opt.precision != 64 && opt.precision != 32) return TDEM_ERR_ARGUMENT;
+    s->precision = opt.precision;
+    s->error = s->solve.prepare(workdir, opt, s->stream);
+    s->prepared = s->error.empty();
+    const tdem_status st = classify(s->error);
+    *out = s.release();
+    return st;
+  });
 }
 
 tdem_status tdem_solver_plan(const char* workdir, int formulation, int scheme, const tdem_options* opts,
                              tdem_plan_info* out, char* err, size_t err_len) {
-  auto fail = [&](tdem_status st, const std::string& msg) {
-    if (err && err_len) {
-      std::strncpy(err, msg.c_str(), err_len - 1);
-      err[err_len - 1] = 0;
+  return guard([&]() -> tdem_status {
+    auto fail = [&](tdem_status st, const std::string& msg) {
+      if (err && err_len) {
+        std::strncpy(err, msg.c_str(), err_len - 1);
+        err[err_len - 1] = 0;
+      }
+      return st;
+    };
+    if (err && err_len) err[0] = 0;
+    if (!workdir || !out) return fail(TDEM_ERR_ARGUMENT, "null argument");
+    if ((formulation != 0 && formulation != 1) || (scheme != 2 && scheme != 3))
+      return fail(TDEM_ERR_ARGUMENT, "formulation must be 0 or 1 and scheme 2 or 3");
+    std::memset(out, 0, sizeof(*out));
+    tdem::RunOptions opt;
+    opt.formulation = formulation;
+    opt.scheme = scheme;
+    if (opts) {
+      if (opts->precision) opt.precision = opts->precision;
+      if (opts->leaf_size > 0) opt.leaf_size = opts->leaf_size;
+      if (opts->factor_slots < 0 || opts->factor_slots > 2) return fail(TDEM_ERR_ARGUMENT, "factor_slots out of range");
+      opt.factor_slots = opts->factor_slots;
     }
-    return st;
-  };
-  if (err && err_len) err[0] = 0;
-  if (!workdir || !out) return fail(TDEM_ERR_ARGUMENT, "null argument");
-  if ((formulation != 0 && formulation != 1) || (scheme != 2 && scheme != 3))
-    return fail(TDEM_ERR_ARGUMENT, "formulation must be 0 or 1 and scheme 2 or 3");
-  std::memset(out, 0, sizeof(*out));
-  tdem::RunOptions opt;
-  opt.formulation = formulation;
-  opt.scheme = scheme;
-  if (opts) {
-    if (opts->precision) opt.precision = opts->precision;
-    if (opts->leaf_size > 0) opt.leaf_size = opts->leaf_size;
-    if (opts->factor_slots < 0 || opts->factor_slots > 2) return fail(TDEM_ERR_ARGUMENT, "factor_slots out of range");
-    opt.factor_slots = opts->factor_slots;
-  }
-  if (opt.precision != 64 && opt.precision != 32) return fail(TDEM_ERR_ARGUMENT, "precision must be 64 or 32");
-  tdem::TransientSolve ts;
-  const std::string e = ts.plan(workdir, opt);
-  if (!e.empty()) return fail(classify(e), e);
-  const tdem::Symbolic* sy = ts.planned_symbolic();
-  const tdem::Model& m = ts.model();
-  out->n_edges = m.n_edges;
-  out->n_interior = ts.n_interior();
-  out->nnz_matrix = ts.nnz_full();
-  out->nnz_factor = sy->nnz_l;
-  out->factor_flops = sy->flops;
-  out->device_bytes = ts.device_bytes_needed();
-  out->factor_slot_bytes = tdem::GpuCholesky::slot_bytes(*sy, opt.precision == 32 ? 4 : 8);
-  out->solve_units = (int64_t)sy->solve_units.size() / tdem::kUnitInts;
-  out->n_fronts = (int)sy->fronts.size();
-  out->tree_levels = (int)sy->levels.size();
-  out->n_sources = m.npls;
-  out->n_times = (int)m.time.size();
-  out->plan_seconds = ts.times().setup_s;
-  out->digest = tdem::plan_digest(*sy);
-  return TDEM_OK;
+    if (opt.precision != 64 && opt.precision != 32) return fail(TDEM_ERR_ARGUMENT, "precision must be 64 or 32");
+    tdem::TransientSolve ts;
+    const std::string e = ts.plan(workdir, opt);
+    if (!e.empty()) return fail(classify(e), e);
+    const tdem::Symbolic* sy = ts.planned_symbolic();
+    const tdem::Model& m = ts.model();
+    out->n_edges = m.n_edges;
+    out->n_interior = ts.n_interior();
+    out->nnz_matrix = ts.nnz_full();
+    out->nnz_factor = sy->nnz_l;
+    out->factor_flops = sy->flops;
+    out->device_bytes = ts.device_bytes_needed();
+    out->factor_slot_bytes = tdem::GpuCholesky::slot_bytes(*sy, opt.precision == 32 ? 4 : 8);
+    out->solve_units = (int64_t)sy->solve_units.size() / tdem::kUnitInts;
+    out->n_fronts = (int)sy->fronts.size();
+    out->tree_levels = (int)sy->levels.size();
+    out->n_sources = m.npls;
+    out->n_times = (int)m.time.size();
+    out->plan_seconds = ts.times().setup_s;
+    out->digest = tdem::plan_digest(*sy);
+    return TDEM_OK;
+  }, err, err_len);
 }
 
 tdem_status tdem_solver_run(tdem_solver* s) {
-  if (!s) return TDEM_ERR_ARGUMENT;
-  if (!s->prepared) return TDEM_ERR_STATE;
-  cudaSetDevice(s->device);
-  s->error = s->solve.run();
-  s->ran = s->error.empty();
-  s->cancel = 0;  // a cancellation request applies to one run
-  return classify(s->error);
+  return guard([&]() -> tdem_status {
+    if (!s) return TDEM_ERR_ARGUMENT;
+    if (!s->prepared) return TDEM_ERR_STATE;
+    cudaSetDevice(s->device);
+    s->error = s->solve.run();
+    s->ran = s->error.empty();
+    s->cancel = 0;  // a cancellation request applies to one run
+    return classify(s->error);
+  }, nullptr, 0, s ? &s->error : nullptr);
 }
 
 tdem_status tdem_solver_write_outputs(tdem_solver* s) {
-  if (!s) return TDEM_ERR_ARGUMENT;
-  if (!s->ran) return TDEM_ERR_STATE;
-  cudaSetDevice(s->device);
-  s->error = s->solve.write_outputs();
-  return classify(s->error);
+  return guard([&]() -> tdem_status {
+    if (!s) return TDEM_ERR_ARGUMENT;
+    if (!s->ran) return TDEM_ERR_STATE;
+    cudaSetDevice(s->device);
+    s->error = s->solve.write_outputs();
+    return classify(s->error);
+  }, nullptr, 0, s ? &s->error : nullptr);
 }
 
 tdem_status tdem_solver_results(tdem_solver* s, double* eall, double* emf, double* ball) {
-  if (!s) return TDEM_ERR_ARGUMENT;
-  if (!s->ran) return TDEM_ERR_STATE;
-  cudaSetDevice(s->device);
-  std::vector<double> e, m, b;
-  s->error = s->solve.results(e, m, b);
-  if (!s->error.empty()) return classify(s->error);
-  // units and signs as written to the files (Gather_edsall)
-  if (eall)
-    for (size_t i = 0; i < e.size(); ++i) eall[i] = e[i] * 1000;
-  if (emf)
-    for (size_t i = 0; i < m.size(); ++i) emf[i] = m[i] * (-1000);
-  if (ball)
-    for (size_t i = 0; i < b.size(); ++i) ball[i] = b[i] * 1000;
-  return TDEM_OK;
+  return guard([&]() -> tdem_status {
+    if (!s) return TDEM_ERR_ARGUMENT;
+    if (!s->ran) return TDEM_ERR_STATE;
+    cudaSetDevice(s->device);
+    std::vector<double> e, m, b;
+    s->error = s->solve.results(e, m, b);
+    if (!s->error.empty()) return classify(s->error);
+    // units and signs as written to the files (Gather_edsall)
+    if (eall)
+      for (size_t i = 0; i < e.size(); ++i) eall[i] = e[i] * 1000;
+    if (emf)
+      for (size_t i = 0; i < m.size(); ++i) emf[i] = m[i] * (-1000);
+    if (ball)
+      for (size_t i = 0; i < b.size(); ++i) ball[i] = b[i] * 1000;
+    return TDEM_OK;
+  }, nullptr, 0, s ? &s->error : nullptr);
 }
 
 tdem_status tdem_solver_info(const tdem_solver* s, tdem_info* info) {
-  if (!s || !info) return TDEM_ERR_ARGUMENT;
-  std::memset(info, 0, sizeof(*info));
-  const tdem::Model& m = s->solve.model();
-  info->n_edges = m.n_edges;
-  info->n_sources = m.npls;
-  info->n_times = (int)m.time.size();
-  info->n_rec_b = (int)m.rec_b.size();
-  info->n_rec_e = (int)m.rec_e.size();
-  info->first_layer = s->solve.first_layer();
-  info->last_layer = s->solve.last_layer();
-  info->n_interior = s->solve.n_interior();
-  info->nnz_matrix = s->solve.nnz_full();
-  const tdem::PhaseTimes& pt = s->solve.times();
-  info->factorizations = pt.factorizations;
-  info->steps = pt.steps;
-  info->t_setup_s = pt.setup_s;
-  info->t_assemble_s = pt.assemble_s;
-  info->t_factor_s = pt.factor_s;
-  info->t_steps_s = pt.steps_s;
-  info->t_output_s = pt.output_s;
-  info->kernel_launches = s->solve.kernel_launches();
-  info->run_gpu_ms = pt.run_gpu_ms;
-  info->factor_gpu_ms = pt.factor_gpu_ms;
-  info->solve_gpu_ms = pt.solve_gpu_ms;
-  info->h2d_bytes = pt.h2d_bytes;
-  info->d2h_bytes = pt.d2h_bytes;
-  info->precision = s->precision;
-  info->refine_iters = pt.refine_iters;
-  info->refine_iters_max = pt.refine_iters_max;
-  info->refine_worst = pt.refine_worst;
-  info->factor_slots = pt.factor_slots;
-  if (m.n_edges > 0 && s->solve.n_interior() > 0) {
-    const tdem::GpuCholesky& c = s->solve.cholesky();
-    info->nnz_factor = c.symbolic().nnz_l;
-    info->factor_flops = c.symbolic().flops;
-    info->device_bytes = (int64_t)c.device_bytes();
-  }
-  return TDEM_OK;
+  return guard([&]() -> tdem_status {
+    if (!s || !info) return TDEM_ERR_ARGUMENT;
+    std::memset(info, 0, sizeof(*info));
+    const tdem::Model& m = s->solve.model();
+    info->n_edges = m.n_edges;
+    info->n_sources = m.npls;
+    info->n_times = (int)m.time.size();
+    info->n_rec_b = (int)m.rec_b.size();
+    info->n_rec_e = (int)m.rec_e.size();
+    info->first_layer = s->solve.first_layer();
+    info->last_layer = s->solve.last_layer();
+    info->n_interior = s->solve.n_interior();
+    info->nnz_matrix = s->solve.nnz_full();
+    const tdem::PhaseTimes& pt = s->solve.times();
+    info->factorizations = pt.factorizations;
+    info->steps = pt.steps;
+    info->t_setup_s = pt.setup_s;
+    info->t_assemble_s = pt.assemble_s;
+    info->t_factor_s = pt.factor_s;
+    info->t_steps_s = pt.steps_s;
+    info->t_output_s = pt.output_s;
+    info->kernel_launches = s->solve.kernel_launches();
+    info->run_gpu_ms = pt.run_gpu_ms;
+    info->factor_gpu_ms = pt.factor_gpu_ms;
+    info->solve_gpu_ms = pt.solve_gpu_ms;
+    info->h2d_bytes = pt.h2d_bytes;
+    info->d2h_bytes = pt.d2h_bytes;
+    info->precision = s->precision;
+    info->refine_iters = pt.refine_iters;
+    info->refine_iters_max = pt.refine_iters_max;
+    info->refine_worst = pt.refine_worst;
+    info->factor_slots = pt.factor_slots;
+    if (m.n_edges > 0 && s->solve.n_interior() > 0) {
+      const tdem::GpuCholesky& c = s->solve.cholesky();
+      info->nnz_factor = c.symbolic().nnz_l;
+      info->factor_flops = c.symbolic().flops;
+      info->device_bytes = (int64_t)c.device_bytes();
+    }
+    return TDEM_OK;
+  });
 }
 
 tdem_status tdem_solver_cancel(tdem_solver* s) {
-  if (!s) return TDEM_ERR_ARGUMENT;
-  s->cancel = 1;
-  return TDEM_OK;
+  return guard([&]() -> tdem_status {
+    if (!s) return TDEM_ERR_ARGUMENT;
+    s->cancel = 1;
+    return TDEM_OK;
+  }, nullptr, 0, s ? &s->error : nullptr);
 }
 
 const char* tdem_solver_error(const tdem_solver* s) { return s ? s->error.c_str() : "null solver"; }
@@ -231,13 +273,15 @@ void tdem_solver_destroy(tdem_solver* s) {
 
 tdem_status tdem_run_directory(const char* workdir, int formulation, int scheme, int device, char* errbuf,
                                size_t errlen) {
-  tdem_solver* s = nullptr;
-  tdem_status st = tdem_solver_create(workdir, formulation, scheme, device, &s);
-  if (st == TDEM_OK) st = tdem_solver_run(s);
-  if (st == TDEM_OK) st = tdem_solver_write_outputs(s);
-  put_err(errbuf, errlen, s ? s->error : std::string("invalid arguments"));
-  tdem_solver_destroy(s);
-  return st;
+  return guard([&]() -> tdem_status {
+    tdem_solver* s = nullptr;
+    tdem_status st = tdem_solver_create(workdir, formulation, scheme, device, &s);
+    if (st == TDEM_OK) st = tdem_solver_run(s);
+    if (st == TDEM_OK) st = tdem_solver_write_outputs(s);
+    put_err(errbuf, errlen, s ? s->error : std::string("invalid arguments"));
+    tdem_solver_destroy(s);
+    return st;
+  }, errbuf, errlen);
 }
 
 struct tdem_server {
@@ -265,70 +309,78 @@ tdem::RunOptions run_options(int formulation, int scheme, const tdem_options* op
 }  // namespace
 
 tdem_status tdem_server_create(const tdem_server_options* opts, tdem_server** out) {
-  if (!out) return TDEM_ERR_ARGUMENT;
-  *out = nullptr;
-  tdem::ServerOptions o;
-  if (opts) {
-    o.device = opts->device;
-    if (opts->max_active > 0) o.max_active = opts->max_active;
-    if (opts->prep_threads > 0) o.prep_threads = opts->prep_threads;
-    o.hbm_budget = opts->hbm_budget_bytes;
-  }
-  auto s = std::make_unique<tdem_server>();
-  const std::string e = s->srv.start(o);
-  if (!e.empty()) return classify(e);
-  *out = s.release();
-  return TDEM_OK;
+  return guard([&]() -> tdem_status {
+    if (!out) return TDEM_ERR_ARGUMENT;
+    *out = nullptr;
+    tdem::ServerOptions o;
+    if (opts) {
+      o.device = opts->device;
+      if (opts->max_active > 0) o.max_active = opts->max_active;
+      if (opts->prep_threads > 0) o.prep_threads = opts->prep_threads;
+      o.hbm_budget = opts->hbm_budget_bytes;
+    }
+    auto s = std::make_unique<tdem_server>();
+    const std::string e = s->srv.start(o);
+    if (!e.empty()) return classify(e);
+    *out = s.release();
+    return TDEM_OK;
+  });
 }
 
 tdem_status tdem_server_submit(tdem_server* srv, const char* workdir, int formulation, int scheme,
                                const tdem_options* opts, int write_outputs, int64_t* request_id) {
-  if (!srv || !workdir || !request_id) return TDEM_ERR_ARGUMENT;
-  if ((formulation != 0 && formulation != 1) || (scheme != 2 && scheme != 3)) return TDEM_ERR_ARGUMENT;
-  if (opts && (opts->precision != 0 && opts->precision != 32 && opts->precision != 64)) return TDEM_ERR_ARGUMENT;
-  if (opts && (opts->fp32_update < 0 || opts->fp32_update > 2)) return TDEM_ERR_ARGUMENT;
-  if (opts && (opts->factor_slots < 0 || opts->factor_slots > 2)) return TDEM_ERR_ARGUMENT;
-  *request_id = srv->srv.submit(workdir, run_options(formulation, scheme, opts), write_outputs != 0);
-  return TDEM_OK;
+  return guard([&]() -> tdem_status {
+    if (!srv || !workdir || !request_id) return TDEM_ERR_ARGUMENT;
+    if ((formulation != 0 && formulation != 1) || (scheme != 2 && scheme != 3)) return TDEM_ERR_ARGUMENT;
+    if (opts && (opts->precision != 0 && opts->precision != 32 && opts->precision != 64)) return TDEM_ERR_ARGUMENT;
+    if (opts && (opts->fp32_update < 0 || opts->fp32_update > 2)) return TDEM_ERR_ARGUMENT;
+    if (opts && (opts->factor_slots < 0 || opts->factor_slots > 2)) return TDEM_ERR_ARGUMENT;
+    *request_id = srv->srv.submit(workdir, run_options(formulation, scheme, opts), write_outputs != 0);
+    return TDEM_OK;
+  });
 }
 
 tdem_status tdem_server_wait(tdem_server* srv, int64_t request_id, tdem_request_info* info) {
-  if (!srv) return TDEM_ERR_ARGUMENT;
-  tdem::RequestResult r;
-  if (!srv->srv.wait(request_id, &r)) return TDEM_ERR_ARGUMENT;
-  const tdem_status st = classify(r.error);
-  if (info) {
-    std::memset(info, 0, sizeof(*info));
-    info->status = st;
-    info->first_layer = r.first_layer;
-    info->last_layer = r.last_layer;
-    info->n_rec_b = r.n_rec_b;
-    info->n_rec_e = r.n_rec_e;
-    info->n_sources = r.n_sources;
-    info->steps = r.steps;
-    info->factorizations = r.factorizations;
-    info->submit_s = r.submit_s;
-    info->admit_s = r.admit_s;
-    info->done_s = r.done_s;
-    info->run_gpu_ms = r.run_gpu_ms;
-    info->device_bytes = r.device_bytes;
-  }
-  std::lock_guard<std::mutex> lk(srv->mu);
-  srv->done[request_id] = std::move(r);
-  return st;
+  return guard([&]() -> tdem_status {
+    if (!srv) return TDEM_ERR_ARGUMENT;
+    tdem::RequestResult r;
+    if (!srv->srv.wait(request_id, &r)) return TDEM_ERR_ARGUMENT;
+    const tdem_status st = classify(r.error);
+    if (info) {
+      std::memset(info, 0, sizeof(*info));
+      info->status = st;
+      info->first_layer = r.first_layer;
+      info->last_layer = r.last_layer;
+      info->n_rec_b = r.n_rec_b;
+      info->n_rec_e = r.n_rec_e;
+      info->n_sources = r.n_sources;
+      info->steps = r.steps;
+      info->factorizations = r.factorizations;
+      info->submit_s = r.submit_s;
+      info->admit_s = r.admit_s;
+      info->done_s = r.done_s;
+      info->run_gpu_ms = r.run_gpu_ms;
+      info->device_bytes = r.device_bytes;
+    }
+    std::lock_guard<std::mutex> lk(srv->mu);
+    srv->done[request_id] = std::move(r);
+    return st;
+  });
 }
 
 tdem_status tdem_server_results(tdem_server* srv, int64_t request_id, double* eall, double* emf, double* ball) {
-  if (!srv) return TDEM_ERR_ARGUMENT;
-  std::lock_guard<std::mutex> lk(srv->mu);
-  auto it = srv->done.find(request_id);
-  if (it == srv->done.end()) return TDEM_ERR_STATE;
-  const tdem::RequestResult& r = it->second;
-  if (!r.error.empty()) return classify(r.error);
-  if (eall) std::copy(r.eall.begin(), r.eall.end(), eall);
-  if (emf) std::copy(r.emf.begin(), r.emf.end(), emf);
-  if (ball) std::copy(r.ball.begin(), r.ball.end(), ball);
-  return TDEM_OK;
+  return guard([&]() -> tdem_status {
+    if (!srv) return TDEM_ERR_ARGUMENT;
+    std::lock_guard<std::mutex> lk(srv->mu);
+    auto it = srv->done.find(request_id);
+    if (it == srv->done.end()) return TDEM_ERR_STATE;
+    const tdem::RequestResult& r = it->second;
+    if (!r.error.empty()) return classify(r.error);
+    if (eall) std::copy(r.eall.begin(), r.eall.end(), eall);
+    if (emf) std::copy(r.emf.begin(), r.emf.end(), emf);
+    if (ball) std::copy(r.ball.begin(), r.ball.end(), ball);
+    return TDEM_OK;
+  });
 }
 
 const char* tdem_server_error(tdem_server* srv, int64_t request_id) {
@@ -339,56 +391,68 @@ const char* tdem_server_error(tdem_server* srv, int64_t request_id) {
 }
 
 tdem_status tdem_server_stats_get(tdem_server* srv, tdem_server_stats* st) {
-  if (!srv || !st) return TDEM_ERR_ARGUMENT;
-  const tdem::ServerStats s = srv->srv.stats();
-  st->submitted = s.submitted;
-  st->completed = s.completed;
-  st->failed = s.failed;
-  st->latency_p50_s = s.latency_p50_s;
-  st->latency_p99_s = s.latency_p99_s;
-  st->makespan_s = s.makespan_s;
-  st->solves_per_s = s.solves_per_s;
-  st->peak_device_bytes = s.peak_device_bytes;
-  st->peak_active = s.peak_active;
-  return TDEM_OK;
+  return guard([&]() -> tdem_status {
+    if (!srv || !st) return TDEM_ERR_ARGUMENT;
+    const tdem::ServerStats s = srv->srv.stats();
+    st->submitted = s.submitted;
+    st->completed = s.completed;
+    st->failed = s.failed;
+    st->latency_p50_s = s.latency_p50_s;
+    st->latency_p99_s = s.latency_p99_s;
+    st->makespan_s = s.makespan_s;
+    st->solves_per_s = s.solves_per_s;
+    st->peak_device_bytes = s.peak_device_bytes;
+    st->peak_active = s.peak_active;
+    return TDEM_OK;
+  });
 }
 
 void tdem_server_destroy(tdem_server* srv) { delete srv; }
 
 tdem_status tdem_time_direct_solver(const char* workdir, char* errbuf, size_t errlen) {
-  if (!workdir) return TDEM_ERR_ARGUMENT;
-  const std::string e = tdem::time_direct_solver(workdir);
-  put_err(errbuf, errlen, e);
-  return e.empty() ? TDEM_OK : TDEM_ERR_INPUT;
+  return guard([&]() -> tdem_status {
+    if (!workdir) return TDEM_ERR_ARGUMENT;
+    const std::string e = tdem::time_direct_solver(workdir);
+    put_err(errbuf, errlen, e);
+    return e.empty() ? TDEM_OK : TDEM_ERR_INPUT;
+  }, errbuf, errlen);
 }
 
 tdem_status tdem_correct_time_mesh(const char* workdir, char* errbuf, size_t errlen) {
-  if (!workdir) return TDEM_ERR_ARGUMENT;
-  const std::string e = tdem::correct_time_mesh(workdir);
-  put_err(errbuf, errlen, e);
-  return e.empty() ? TDEM_OK : TDEM_ERR_INPUT;
+  return guard([&]() -> tdem_status {
+    if (!workdir) return TDEM_ERR_ARGUMENT;
+    const std::string e = tdem::correct_time_mesh(workdir);
+    put_err(errbuf, errlen, e);
+    return e.empty() ? TDEM_OK : TDEM_ERR_INPUT;
+  }, errbuf, errlen);
 }
 
 tdem_status tdem_sum_nonstat_3d_only(const char* workdir, char* errbuf, size_t errlen) {
-  if (!workdir) return TDEM_ERR_ARGUMENT;
-  const std::string e = tdem::split_components(workdir);
-  put_err(errbuf, errlen, e);
-  return e.empty() ? TDEM_OK : TDEM_ERR_INPUT;
+  return guard([&]() -> tdem_status {
+    if (!workdir) return TDEM_ERR_ARGUMENT;
+    const std::string e = tdem::split_components(workdir);
+    put_err(errbuf, errlen, e);
+    return e.empty() ? TDEM_OK : TDEM_ERR_INPUT;
+  }, errbuf, errlen);
 }
 
 tdem_status tdem_summator_edmn(const char* workdir, int with_ddv, int profile, int place, char* errbuf,
                                size_t errlen) {
-  if (!workdir) return TDEM_ERR_ARGUMENT;
-  const std::string e = tdem::line_voltages(workdir, with_ddv != 0, profile, place);
-  put_err(errbuf, errlen, e);
-  return e.empty() ? TDEM_OK : TDEM_ERR_INPUT;
+  return guard([&]() -> tdem_status {
+    if (!workdir) return TDEM_ERR_ARGUMENT;
+    const std::string e = tdem::line_voltages(workdir, with_ddv != 0, profile, place);
+    put_err(errbuf, errlen, e);
+    return e.empty() ? TDEM_OK : TDEM_ERR_INPUT;
+  }, errbuf, errlen);
 }
 
 tdem_status tdem_stationary_directory(const char* workdir, int device, char* errbuf, size_t errlen) {
-  if (!workdir) return TDEM_ERR_ARGUMENT;
-  const std::string e = tdem::solve_stationary(workdir, device);
-  put_err(errbuf, errlen, e);
-  return classify(e);
+  return guard([&]() -> tdem_status {
+    if (!workdir) return TDEM_ERR_ARGUMENT;
+    const std::string e = tdem::solve_stationary(workdir, device);
+    put_err(errbuf, errlen, e);
+    return classify(e);
+  }, errbuf, errlen);
 }
 
 // ---------------------------------------------------------------------------
@@ -452,10 +516,9 @@ int pardiso_analyse(PardisoHandle* h, int64_t n, const long long* ia, const long
 }
 }  // namespace
 
-void tdem_pardiso_64(void* pt, const long long* /*maxfct*/, const long long* /*mnum*/, const long long* mtype,
-                     const long long* phase, const long long* n, const void* a, const long long* ia,
-                     const long long* ja, long long* /*perm*/, const long long* nrhs, long long* /*iparm*/,
-                     const long long* /*msglvl*/, void* b, void* x, long long* error) {
+static void pardiso_impl(void* pt, const long long* mtype, const long long* phase, const long long* n,
+                         const void* a, const long long* ia, const long long* ja, const long long* nrhs, void* b,
+                         void* x, long long* error) {
   void** ptv = (void**)pt;
   PardisoHandle* h = (PardisoHandle*)ptv[0];
   *error = 0;
@@ -542,6 +605,21 @@ void tdem_pardiso_64(void* pt, const long long* /*maxfct*/, const long long* /*m
     return;
   }
   *error = -1;
+}
+
+// A C++ exception inside the adapter becomes PARDISO's error -2 (not enough memory)
+// for exhausted host memory and -1 otherwise, instead of crossing the C boundary.
+void tdem_pardiso_64(void* pt, const long long* /*maxfct*/, const long long* /*mnum*/, const long long* mtype,
+                     const long long* phase, const long long* n, const void* a, const long long* ia,
+                     const long long* ja, long long* /*perm*/, const long long* nrhs, long long* /*iparm*/,
+                     const long long* /*msglvl*/, void* b, void* x, long long* error) {
+  try {
+    pardiso_impl(pt, mtype, phase, n, a, ia, ja, nrhs, b, x, error);
+  } catch (const std::bad_alloc&) {
+    *error = -2;
+  } catch (...) {
+    *error = -1;
+  }
 }
 
 void pardiso_64(void* pt, const long long* maxfct, const long long* mnum, const long long* mtype,

@@ -212,8 +212,12 @@ std::string TransientSolve::plan(const std::string& dir, const RunOptions& opt) 
   // model: they are built on a second thread while the patterns and the analysis run
   std::string e_init, e_rec;
   std::thread side([this, &opt, &e_init, &e_rec] {
-    e_init = load_initial_field(m_, opt.formulation == 1, u0_);
-    if (e_init.empty()) e_rec = build_sources_and_receivers();
+    try {
+      e_init = load_initial_field(m_, opt.formulation == 1, u0_);
+      if (e_init.empty()) e_rec = build_sources_and_receivers();
+    } catch (const std::exception& x) {
+      e_init = std::string("host error: ") + x.what();
+    }
   });
   struct Join {
     std::thread& t;

@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstdlib>
+#include <exception>
 #include <thread>
 #include <vector>
 
@@ -28,24 +29,32 @@ inline int chunk_count(int64_t n, int64_t min_per_thread = 4096) {
   return (int)std::max<int64_t>(1, std::min<int64_t>(host_threads(), n / std::max<int64_t>(1, min_per_thread)));
 }
 
-// f(t, begin, end) for the t-th of nt contiguous ranges of [0, n), range t on its own thread
+// f(t, begin, end) for the t-th of nt contiguous ranges of [0, n), range t on its own
+// thread; an exception thrown by any range is rethrown here after all have ended
 template <class F>
 void parallel_chunks(int64_t n, int nt, F&& f) {
   nt = std::max(1, nt);
   const int64_t step = (n + nt - 1) / nt;
+  std::vector<std::exception_ptr> err(nt);
   auto range = [&](int t) {
-    const int64_t b = std::min(n, t * step), e = std::min(n, (t + 1) * step);
-    f(t, b, e);
+    try {
+      const int64_t b = std::min(n, t * step), e = std::min(n, (t + 1) * step);
+      f(t, b, e);
+    } catch (...) {
+      err[t] = std::current_exception();
+    }
   };
-  if (nt == 1) {
+  if (nt > 1) {
+    std::vector<std::thread> pool;
+    pool.reserve(nt - 1);
+    for (int t = 1; t < nt; ++t) pool.emplace_back([&range, t] { range(t); });
     range(0);
-    return;
+    for (std::thread& th : pool) th.join();
+  } else {
+    range(0);
   }
-  std::vector<std::thread> pool;
-  pool.reserve(nt - 1);
-  for (int t = 1; t < nt; ++t) pool.emplace_back([&range, t] { range(t); });
-  range(0);
-  for (std::thread& th : pool) th.join();
+  for (const std::exception_ptr& x : err)
+    if (x) std::rethrow_exception(x);
 }
 
 template <class F>

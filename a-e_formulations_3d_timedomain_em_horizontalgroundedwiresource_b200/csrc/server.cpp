@@ -71,8 +71,13 @@ void Server::plan_loop() {
       to_plan_.pop_front();
       r = reqs_[id].get();
     }
-    r->solve.reset(new TransientSolve());
-    const std::string e = r->solve->plan(r->dir, r->opt);
+    std::string e;
+    try {
+      r->solve.reset(new TransientSolve());
+      e = r->solve->plan(r->dir, r->opt);
+    } catch (const std::exception& x) {  // host memory exhausted or another host failure
+      e = std::string("host error: ") + x.what();
+    }
     {
       std::lock_guard<std::mutex> lk(mu_);
       if (!e.empty()) {
@@ -121,18 +126,22 @@ void Server::run_loop() {
     std::string e;
     cudaStream_t s = nullptr;
     if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) e = "CUDA: cudaStreamCreate failed";
-    if (e.empty()) e = r->solve->setup_device(s);
-    if (e.empty()) e = r->solve->run();
-    if (e.empty() && r->write_outputs) e = r->solve->write_outputs();
-    if (e.empty()) {
-      std::vector<double> ea, em, eb;
-      e = r->solve->results(ea, em, eb);
-      for (double& v : ea) v *= 1000;    // units and signs as written to the files
-      for (double& v : em) v *= -1000;
-      for (double& v : eb) v *= 1000;
-      r->res.eall.swap(ea);
-      r->res.emf.swap(em);
-      r->res.ball.swap(eb);
+    try {
+      if (e.empty()) e = r->solve->setup_device(s);
+      if (e.empty()) e = r->solve->run();
+      if (e.empty() && r->write_outputs) e = r->solve->write_outputs();
+      if (e.empty()) {
+        std::vector<double> ea, em, eb;
+        e = r->solve->results(ea, em, eb);
+        for (double& v : ea) v *= 1000;    // units and signs as written to the files
+        for (double& v : em) v *= -1000;
+        for (double& v : eb) v *= 1000;
+        r->res.eall.swap(ea);
+        r->res.emf.swap(em);
+        r->res.ball.swap(eb);
+      }
+    } catch (const std::exception& x) {  // host memory exhausted or another host failure
+      e = std::string("host error: ") + x.what();
     }
     const Model& m = r->solve->model();
     r->res.first_layer = r->solve->first_layer();

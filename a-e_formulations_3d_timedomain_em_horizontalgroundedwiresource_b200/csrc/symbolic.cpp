@@ -8,6 +8,7 @@
 #include <cstring>
 #include <climits>
 #include <numeric>
+#include <exception>
 #include <thread>
 
 namespace tdem {
@@ -63,9 +64,22 @@ class Dissector {
     if (depth > 0 && L.size() >= kForkMin && R.size() >= kForkMin) {
       Dissector right(*this);
       int rroot = -1;
-      std::thread t([&] { rroot = right.build(R, depth - 1); });
-      kids.push_back(build(L, depth - 1));
+      std::exception_ptr err;
+      std::thread t([&] {
+        try {
+          rroot = right.build(R, depth - 1);
+        } catch (...) {
+          err = std::current_exception();
+        }
+      });
+      try {
+        kids.push_back(build(L, depth - 1));
+      } catch (...) {
+        t.join();
+        throw;
+      }
       t.join();
+      if (err) std::rethrow_exception(err);
       kids.push_back(append(right, rroot));
     } else {
       if (!L.empty()) kids.push_back(build(L, depth - 1));

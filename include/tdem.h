@@ -35,7 +35,8 @@ typedef enum tdem_status {
   TDEM_ERR_CUDA = 3,      /* CUDA runtime error (no device, out of memory, launch failure) */
   TDEM_ERR_NUMERIC = 4,   /* non-positive pivot: the system is not positive definite */
   TDEM_ERR_CANCELLED = 5, /* tdem_solver_cancel() was called during tdem_solver_run() */
-  TDEM_ERR_STATE = 6      /* call out of order (e.g. results before run) */
+  TDEM_ERR_STATE = 6,     /* call out of order (e.g. results before run) */
+  TDEM_ERR_HOST = 7       /* host-side failure: host memory exhausted or another internal error */
 } tdem_status;
 
 /* formulation: 0 = A (vector potential, CalcNonstat3DLine "A-formulation"),
