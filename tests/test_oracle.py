@@ -164,3 +164,27 @@ def test_numpy_oracle_primary_secondary_matches_reference(outs, tmp_path, case, 
     for o in ps.OUTPUTS:
         err = outs.compare_files(os.path.join(d, o + ".1"), os.path.join(GOLDEN, case, "%s_%s.1" % (variant, o)))
         assert err <= FP64_TOL, (o, err)
+
+
+def test_three_point_formulas_exact_for_quadratics():
+    """Known answers of the time discretisation (reference math, no reference run):
+    the BDF2 step coefficients (A3/time_approx.cpp:943-945) and the three-point
+    derivative used for outputs and the E-form sources (E3/time_approx.cpp:1434-1460)
+    differentiate quadratics exactly on non-uniform steps."""
+    rng = np.random.default_rng(5)
+    for _ in range(50):
+        a, b, c = rng.standard_normal(3)
+        u = lambda t: a + b * t + c * t * t
+        du = lambda t: b + 2 * c * t
+        tj2 = rng.uniform(0, 1)
+        tj1 = tj2 + rng.uniform(0.1, 1)
+        tj = tj1 + rng.uniform(0.1, 1)
+        dt, dt0, dt1 = tj - tj2, tj - tj1, tj1 - tj2
+        mult = (dt + dt0) / (dt * dt0)
+        m1 = dt / (dt1 * dt0)
+        m2 = -dt0 / (dt * dt1)
+        # the step solves (C mult + B) u_j = C (m1 u_j1 + m2 u_j2) + ...: mult u_j - m1 u_j1 - m2 u_j2 = du/dt
+        assert abs(mult * u(tj) - m1 * u(tj1) - m2 * u(tj2) - du(tj)) <= 1e-9 * (1 + abs(du(tj)))
+        for t in (tj2, tj1, tj, 0.5 * (tj1 + tj)):
+            got = tdem_oracle._dA_dt(t, u(tj), u(tj1), u(tj2), dt, dt0, dt1, tj, tj1, tj2)
+            assert abs(got - du(t)) <= 1e-9 * (1 + abs(du(t)))
