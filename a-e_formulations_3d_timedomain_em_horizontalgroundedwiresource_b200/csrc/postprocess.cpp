@@ -18,7 +18,6 @@
 #include <cstring>
 #include <fstream>
 #include <iterator>
-#include <thread>
 #include <vector>
 
 namespace tdem {
@@ -477,19 +476,13 @@ std::string line_voltages(const std::string& dir, bool with_ddv, int profile, in
   // E curves of every point of every line, in line order (SummatorEDMN/main.cpp:108-130);
   // the three files are read on their own threads
   std::vector<Curve> E[3];
-  {
-    auto parse = [&](int c) {
-      E[c].assign((size_t)nlines * per_line, Curve());
-      LineReader in(std::move(text[c]));
-      std::string line;
-      in.getline(line);
-      for (Curve& cv : E[c]) read_curve(in, line, cv);
-    };
-    std::thread ty(parse, 1), tz(parse, 2);
-    parse(0);
-    ty.join();
-    tz.join();
-  }
+  parallel_chunks(3, 3, [&](int c, int64_t, int64_t) {
+    E[c].assign((size_t)nlines * per_line, Curve());
+    LineReader in(std::move(text[c]));
+    std::string line;
+    in.getline(line);
+    for (Curve& cv : E[c]) read_curve(in, line, cv);
+  });
 
   // dV = sum of E . dl over the line's points; dl of the first point is twice the
   // distance from A (the points are the midpoints of equal segments), else the
