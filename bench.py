@@ -429,7 +429,7 @@ def run_ours(args, world, rank, local):
 
 
 def run_serving(args, world, rank, local):
-    """a Poisson stream of random forward-modelling requests through
+    """Config c4: a Poisson stream of random forward-modelling requests through
     the serving loop (tdem_server_*) on one GPU; prints solves/s and p50/p99 latency."""
     import numpy as np
     import torch
