@@ -153,6 +153,7 @@ EXPORTED = [
     "tdem_pardiso_64",
     "pardiso_64",
     "mkl_set_num_threads",
+    "tdem_pardiso_handles",
     "tdem_residual_norms",
     "tdem_server_create",
     "tdem_server_submit",
@@ -214,6 +215,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         f = getattr(lib, name)
         f.argtypes = [P, pi, pi, pi, pi, pi, P, pi, pi, pi, pi, pi, pi, P, P, pi]
         f.restype = None
+    lib.tdem_pardiso_handles.argtypes = []
+    lib.tdem_pardiso_handles.restype = ctypes.c_int
     lib.tdem_residual_norms.argtypes = [ctypes.c_int, ctypes.c_int64, P, P, P, P, P, ctypes.c_int64,
                                         ctypes.c_int, P, P]
     lib.tdem_residual_norms.restype = ctypes.c_int

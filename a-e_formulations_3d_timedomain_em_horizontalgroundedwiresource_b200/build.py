@@ -49,16 +49,24 @@ def build(verbose: bool = False) -> str:
     hdr_time = _newest(headers)
     sources = sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
     sources = [s for s in sources if os.path.basename(s) != "cli.cpp"]
-    objs = []
+    objs, cmds = [], []
     for src in sources:
         obj = os.path.join(OBJ_DIR, os.path.basename(src) + ".o")
         objs.append(obj)
         if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(src), hdr_time):
             continue
-        cmd = [nvcc] + ARCH + COMMON + ["-c", src, "-o", obj]
+        cmds.append([nvcc] + ARCH + COMMON + ["-c", src, "-o", obj])
+    # the out-of-date objects compile side by side (one nvcc process each)
+    from concurrent.futures import ThreadPoolExecutor
+
+    def compile_one(cmd):
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(compile_one, c) for c in cmds]:
+            f.result()
     if not os.path.exists(LIB) or os.path.getmtime(LIB) < _newest(objs):
         cmd = [nvcc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
         if verbose:

@@ -23,7 +23,22 @@
 #include "stationary.h"
 #include "symbolic.h"
 
+// Owns the solver's stream; declared before the solve so that it is destroyed
+// after it (members are destroyed in reverse order), on every path: a failed
+// create as well as tdem_solver_destroy.
+struct StreamHolder {
+  cudaStream_t stream = nullptr;
+  int device = 0;
+  ~StreamHolder() {
+    if (stream) {
+      cudaSetDevice(device);
+      cudaStreamDestroy(stream);
+    }
+  }
+};
+
 struct tdem_solver {
+  StreamHolder owned;
   tdem::TransientSolve solve;
   cudaStream_t stream = nullptr;
   int device = 0;
@@ -87,20 +102,29 @@ tdem_status tdem_solver_create(const char* workdir, int formulation, int scheme,
   });
 }
 
+namespace {
+// module_mode: the behaviour of the reference's executable in its Calculations
+// directory (a `stop` file ends the run, phase marks go to TimeWatcher.log).
+tdem_status create_solver(const char* workdir, int formulation, int scheme, int device, const tdem_options* opts,
+                          bool module_mode, tdem_solver** out);
+}  // namespace
+
 tdem_status tdem_solver_create_ex(const char* workdir, int formulation, int scheme, int device,
                                   const tdem_options* opts, tdem_solver** out) {
+  return create_solver(workdir, formulation, scheme, device, opts, false, out);
+}
+
+namespace {
+tdem_status create_solver(const char* workdir, int formulation, int scheme, int device, const tdem_options* opts,
+                          bool module_mode, tdem_solver** out) {
   return guard([&]() -> tdem_status {
     if (!workdir || !out) return TDEM_ERR_ARGUMENT;
     *out = nullptr;
     if ((formulation != 0 && formulation != 1) || (scheme != 2 && scheme != 3)) return TDEM_ERR_ARGUMENT;
-    auto s = std::make_unique<tdem_solver>();
-    s->device = device;
-    if (cudaSetDevice(device) != cudaSuccess) return TDEM_ERR_CUDA;
-    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) return TDEM_ERR_CUDA;
+    // options are checked before any device resource exists
     tdem::RunOptions opt;
     opt.formulation = formulation;
     opt.scheme = scheme;
-    opt.cancel = &s->cancel;
     if (opts) {
       if (opts->precision) opt.precision = opts->precision;
       if (opts->refine_tol > 0) opt.refine_tol = opts->refine_tol;
@@ -112,6 +136,17 @@ tdem_status tdem_solver_create_ex(const char* workdir, int formulation, int sche
       opt.factor_slots = opts->factor_slots;
     }
     if (opt.precision != 64 && opt.precision != 32) return TDEM_ERR_ARGUMENT;
+    if (module_mode) {
+      opt.stop_file = std::string(workdir) + "/stop";
+      opt.time_watcher = std::string(workdir) + "/TimeWatcher.log";
+    }
+    auto s = std::make_unique<tdem_solver>();
+    s->device = device;
+    opt.cancel = &s->cancel;
+    if (cudaSetDevice(device) != cudaSuccess) return TDEM_ERR_CUDA;
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) return TDEM_ERR_CUDA;
+    s->owned.stream = s->stream;
+    s->owned.device = device;
     s->precision = opt.precision;
     s->error = s->solve.prepare(workdir, opt, s->stream);
     s->prepared = s->error.empty();
@@ -120,6 +155,7 @@ tdem_status tdem_solver_create_ex(const char* workdir, int formulation, int sche
     return st;
   });
 }
+}  // namespace
 
 tdem_status tdem_solver_plan(const char* workdir, int formulation, int scheme, const tdem_options* opts,
                              tdem_plan_info* out, char* err, size_t err_len) {
@@ -266,16 +302,14 @@ const char* tdem_solver_error(const tdem_solver* s) { return s ? s->error.c_str(
 void tdem_solver_destroy(tdem_solver* s) {
   if (!s) return;
   cudaSetDevice(s->device);
-  cudaStream_t st = s->stream;
-  delete s;
-  if (st) cudaStreamDestroy(st);
+  delete s;  // the solve's buffers first, then its stream (StreamHolder)
 }
 
 tdem_status tdem_run_directory(const char* workdir, int formulation, int scheme, int device, char* errbuf,
                                size_t errlen) {
   return guard([&]() -> tdem_status {
     tdem_solver* s = nullptr;
-    tdem_status st = tdem_solver_create(workdir, formulation, scheme, device, &s);
+    tdem_status st = create_solver(workdir, formulation, scheme, device, nullptr, true, &s);
     if (st == TDEM_OK) st = tdem_solver_run(s);
     if (st == TDEM_OK) st = tdem_solver_write_outputs(s);
     put_err(errbuf, errlen, s ? s->error : std::string("invalid arguments"));
@@ -479,6 +513,31 @@ uint64_t pattern_hash(int64_t n, const long long* ia, const long long* ja) {
   return h;
 }
 
+// Handles by the address of the caller's pt array.  The reference's
+// pardiso_solver::factorize zeroes pt[0..63] before every phase 12 and calls phase
+// -1 only at the end of the run (CalcNonstat3DLine/pardiso.cpp:43-58, 76, 104;
+// time_approx.cpp:755, 1002, 1149), so a phase 12 that finds pt[0] null looks its
+// handle up here: one analysis, one device factor and one stream per pt array for
+// the whole run instead of a new set per factorization.  pt is a member of the
+// caller's solver object, so its address is stable for the object's life; phase
+// -1 forgets it.
+std::mutex g_pardiso_mu;
+std::map<const void*, PardisoHandle*> g_pardiso_handles;
+
+PardisoHandle* pardiso_lookup(const void* pt) {
+  std::lock_guard<std::mutex> lk(g_pardiso_mu);
+  auto it = g_pardiso_handles.find(pt);
+  return it == g_pardiso_handles.end() ? nullptr : it->second;
+}
+
+void pardiso_register(const void* pt, PardisoHandle* h) {
+  std::lock_guard<std::mutex> lk(g_pardiso_mu);
+  if (h)
+    g_pardiso_handles[pt] = h;
+  else
+    g_pardiso_handles.erase(pt);
+}
+
 int pardiso_analyse(PardisoHandle* h, int64_t n, const long long* ia, const long long* ja, int nrhs) {
   // upper 1-based CSR (row i: columns j >= i) -> lower 0-based CSR (row j: columns i <= j)
   const int64_t nnz = ia[n] - 1;
@@ -507,8 +566,11 @@ int pardiso_analyse(PardisoHandle* h, int64_t n, const long long* ia, const long
   h->chol.reset(new tdem::GpuCholesky());
   h->solve_cols = std::min(tdem::kMaxRhs, std::max(1, nrhs));
   if (!h->chol->setup(std::move(sy), p2v, h->solve_cols, h->stream).empty()) return -2;
-  if (h->d_vals) cudaFree(h->d_vals);
-  if (cudaMalloc(&h->d_vals, sizeof(double) * std::max<int64_t>(nnz, 1)) != cudaSuccess) return -2;
+  if (!h->d_vals || h->nnz != nnz) {  // the values stay when only the column count changes
+    if (h->d_vals) cudaFree(h->d_vals);
+    h->d_vals = nullptr;
+    if (cudaMalloc(&h->d_vals, sizeof(double) * std::max<int64_t>(nnz, 1)) != cudaSuccess) return -2;
+  }
   h->n = n;
   h->nnz = nnz;
   h->hash = pattern_hash(n, ia, ja);
@@ -521,6 +583,11 @@ static void pardiso_impl(void* pt, const long long* mtype, const long long* phas
                          void* x, long long* error) {
   void** ptv = (void**)pt;
   PardisoHandle* h = (PardisoHandle*)ptv[0];
+  if (!h) {
+    // pt zeroed by the caller since the handle was made (see g_pardiso_handles)
+    h = pardiso_lookup(pt);
+    ptv[0] = h;
+  }
   *error = 0;
   if (*phase == -1) {
     if (h) {
@@ -531,6 +598,7 @@ static void pardiso_impl(void* pt, const long long* mtype, const long long* phas
       if (h->stream) cudaStreamDestroy(h->stream);
       delete h;
     }
+    pardiso_register(pt, nullptr);
     ptv[0] = nullptr;
     return;
   }
@@ -550,6 +618,7 @@ static void pardiso_impl(void* pt, const long long* mtype, const long long* phas
         return;
       }
       ptv[0] = h;
+      pardiso_register(pt, h);
     }
     cudaSetDevice(h->device);
     if (!h->chol || h->n != *n || h->nnz != ia[*n] - 1 || h->hash != pattern_hash(*n, ia, ja)) {
@@ -594,6 +663,26 @@ static void pardiso_impl(void* pt, const long long* mtype, const long long* phas
       }
       h->nrhs_cap = nr;
     }
+    if (nr > h->solve_cols && h->solve_cols < tdem::kMaxRhs && ia && ja && h->n == *n &&
+        h->hash == pattern_hash(*n, ia, ja)) {
+      // The reference analyses with nrhs = 1 (pardiso_solver::init) and then solves
+      // npls columns per call (pardiso.cpp:113-120): widen the solve to this call's
+      // column count once, refactoring from the values already on the device.
+      const int r = pardiso_analyse(h, *n, ia, ja, std::min(nr, tdem::kMaxRhs));
+      if (r) {
+        *error = r;
+        return;
+      }
+      h->chol->factor(h->d_vals, h->stream);
+      if (cudaStreamSynchronize(h->stream) != cudaSuccess) {
+        *error = -2;
+        return;
+      }
+      if (h->chol->status(h->stream)) {
+        *error = -4;
+        return;
+      }
+    }
     // all columns in one copy, solved in blocks of the analysed right-hand-side count
     cudaMemcpyAsync(h->d_x, b, sizeof(double) * h->n * nr, cudaMemcpyHostToDevice, h->stream);
     for (int r = 0; r < nr; r += h->solve_cols) {
@@ -630,5 +719,10 @@ void pardiso_64(void* pt, const long long* maxfct, const long long* mnum, const 
 }
 
 void mkl_set_num_threads(int) {}
+
+int tdem_pardiso_handles(void) {
+  std::lock_guard<std::mutex> lk(g_pardiso_mu);
+  return (int)g_pardiso_handles.size();
+}
 
 }  // extern "C"

@@ -10,6 +10,10 @@
 #include <cstdlib>
 #include <cstring>
 
+#include <ctime>
+#include <sys/stat.h>
+#include <nvtx3/nvToolsExt.h>
+
 #include "fem_kernels.h"
 #include "symbolic.h"
 
@@ -18,6 +22,15 @@ namespace {
 
 double now_s() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// Wall time at library load: phase marks count clock ticks from here, as clock()
+// counts from process start on the reference's platform.
+const double g_process_origin_s = now_s();
+
+bool file_exists(const std::string& path) {
+  struct stat st;
+  return !path.empty() && ::stat(path.c_str(), &st) == 0;
 }
 
 #define TRY_CUDA(x)                                                              \
@@ -73,8 +86,58 @@ int find_time_layer(const std::vector<double>& time, double val) {
   return -1;
 }
 
+void TransientSolve::mark_host(const std::string& label) {
+  if (opt_.time_watcher.empty()) return;
+  nvtxMarkA(label.c_str());
+  PhaseMark m;
+  m.label = label;
+  m.wall_s = now_s();
+  marks_.push_back(std::move(m));
+}
+
+std::string TransientSolve::mark_device(const std::string& label, cudaStream_t s) {
+  if (opt_.time_watcher.empty()) return "";
+  nvtxMarkA(label.c_str());
+  PhaseMark m;
+  m.label = label;
+  TRY_CUDA(cudaEventCreate(&m.ev));
+  marks_.push_back(m);
+  TRY_CUDA(cudaEventRecord(m.ev, s));
+  return "";
+}
+
+std::string TransientSolve::flush_marks() {
+  if (opt_.time_watcher.empty() || marks_.empty()) return "";
+  std::vector<std::pair<double, std::string>> lines;
+  std::string err;
+  for (PhaseMark& m : marks_) {
+    double w = m.wall_s;
+    if (m.ev) {
+      float ms = 0.f;
+      if (mark_origin_ && cudaEventElapsedTime(&ms, mark_origin_, m.ev) == cudaSuccess)
+        w = mark_origin_s_ + 1e-3 * ms;
+      else
+        err = "CUDA: a phase mark did not complete";
+      cudaEventDestroy(m.ev);
+    }
+    lines.emplace_back(w, m.label);
+  }
+  marks_.clear();
+  std::stable_sort(lines.begin(), lines.end(),
+                   [](const auto& a, const auto& b) { return a.first < b.first; });
+  FILE* f = std::fopen(opt_.time_watcher.c_str(), "a");
+  if (!f) return "cannot append to " + opt_.time_watcher;
+  for (const auto& l : lines)
+    std::fprintf(f, "%lld\t%s\n", (long long)((l.first - g_process_origin_s) * CLOCKS_PER_SEC), l.second.c_str());
+  std::fclose(f);
+  return err;
+}
+
 TransientSolve::TransientSolve() = default;
 TransientSolve::~TransientSolve() {
+  for (PhaseMark& m : marks_)
+    if (m.ev) cudaEventDestroy(m.ev);
+  if (mark_origin_) cudaEventDestroy(mark_origin_);
   chol_.reset();
   if (hs_) cudaStreamDestroy(hs_);
   if (fs_) cudaStreamDestroy(fs_);
@@ -124,9 +187,15 @@ double TransientSolve::source_coef(int itime, bool two_layer, double dt) const {
 }
 
 std::string TransientSolve::prepare(const std::string& dir, const RunOptions& opt, cudaStream_t stream) {
+  opt_.time_watcher = opt.time_watcher;  // the marks below precede plan()'s copy of the options
+  mark_host("Start CalcSP");
+  if (file_exists(opt.stop_file)) return "cancelled";  // TaskSP.cpp:462
+  mark_host("Start Prepare_To_Schema");
   std::string e = plan(dir, opt);
   if (!e.empty()) return e;
-  return setup_device(stream);
+  if (!(e = setup_device(stream)).empty()) return e;
+  mark_host("Finish Prepare_To_Schema");
+  return flush_marks();
 }
 
 std::string TransientSolve::build_sources_and_receivers() {
@@ -454,6 +523,8 @@ std::string TransientSolve::factor_with(double mult, int slot, cudaStream_t s) {
     launch_combine_full(d_rowptr_, d_col_, d_C_, d_B_, d_bound_, n_, mult, d_A_, s);
     ++launches_;
   }
+  const std::string me = mark_device("Start factorization", s);
+  if (!me.empty()) return me;
   chol_->factor(d_avals_, s, slot);
   launches_ += 1 + chol_->kernel_launches_factor();
   ++pt_.factorizations;
@@ -588,6 +659,9 @@ std::string TransientSolve::run() {
   pt_.refine_worst = 0.0;
   pt_.factor_gpu_ms = pt_.solve_gpu_ms = pt_.run_gpu_ms = 0;
   launches_ = 0;
+  for (PhaseMark& m : marks_)  // marks of a run that ended early are dropped
+    if (m.ev) cudaEventDestroy(m.ev);
+  marks_.clear();
   // Everything runs on the high-priority stream hs_ (factorizations ahead of use
   // on fs_), ordered after the caller's stream and joined back into it at the end.
   cudaStream_t caller = s_;
@@ -607,6 +681,11 @@ std::string TransientSolve::run() {
     }
   } restore{this, caller};
   TRY_CUDA(cudaEventRecord(ev_[0], s_));
+  if (!opt_.time_watcher.empty()) {
+    if (!mark_origin_) TRY_CUDA(cudaEventCreate(&mark_origin_));
+    TRY_CUDA(cudaEventRecord(mark_origin_, s_));
+    mark_origin_s_ = now_s();
+  }
   TRY_CUDA(cudaMemcpyAsync(layer(0), d_u0_, sizeof(double) * u0_.size(), cudaMemcpyDeviceToDevice, s_));
   dec_ig_ = decade_starts(t);
   const int ndec = (int)dec_ig_.size() - 1;
@@ -615,6 +694,7 @@ std::string TransientSolve::run() {
   std::string e;
   auto check = [&]() -> std::string {
     if (opt_.cancel && *opt_.cancel) return "cancelled";
+    if (file_exists(opt_.stop_file)) return "cancelled";
     return "";
   };
 
@@ -750,9 +830,14 @@ std::string TransientSolve::run() {
       TRY_CUDA(cudaStreamWaitEvent(fst, ev_[5], 0));
     }
     TRY_CUDA(cudaEventRecord(fev[2 * f], fst));
-    factor_with(mults[f], f % nslots, fst);
+    std::string me;
+    if (!(me = mark_device("Start prepare matrix for new decade", fst)).empty()) return me;
+    nvtxRangePushA("factorization");
+    me = factor_with(mults[f], f % nslots, fst);
+    nvtxRangePop();
+    if (!me.empty()) return me;
     TRY_CUDA(cudaEventRecord(fev[2 * f + 1], fst));
-    return "";
+    return mark_device("Finish factorization", fst);
   };
   int nextf = 0;   // next factorization to be used by the steps
   int queued = 0;  // factorizations enqueued so far
@@ -768,9 +853,24 @@ std::string TransientSolve::run() {
     TRY_CUDA(cudaEventRecord(ev, s_));
     return "";
   };
+  int decade = 0;  // decade whose steps are being issued (the reference's iDec)
+  auto decade_end = [&]() -> std::string {
+    std::string me;
+    if (!(me = mark_device("Processing decade results iDec= " + std::to_string(decade), s_)).empty()) return me;
+    if (!(me = mark_device("Finish decade iDec= " + std::to_string(decade), s_)).empty()) return me;
+    nvtxRangePop();
+    ++decade;
+    return "";
+  };
   auto use = [&](double) -> std::string {
     std::string ue;
-    if (!dev_span.empty() && dev_span.size() % 2 == 1 && !(ue = span_mark()).empty()) return ue;  // decade end
+    if (!dev_span.empty() && dev_span.size() % 2 == 1) {  // decade end
+      if (!(ue = span_mark()).empty()) return ue;
+      if (!(ue = decade_end()).empty()) return ue;
+    }
+    nvtxRangePushA(("decade " + std::to_string(decade)).c_str());
+    if (!(ue = mark_device("Start decade iDec= " + std::to_string(decade), s_)).empty()) return ue;
+    if (!(ue = mark_device("Start schema iDec= " + std::to_string(decade), s_)).empty()) return ue;
     const int f = nextf++;
     if (nslots == 1) {
       if (!(ue = enqueue_factor(f)).empty()) return ue;
@@ -789,11 +889,24 @@ std::string TransientSolve::run() {
   auto stepf = [&](int it, int t1, int t2, double m1, double m2, double coef) -> std::string {
     std::string ce = check();
     if (!ce.empty()) return ce;
-    return step(it, t1, t2, m1, m2, coef);
+    if (!(ce = mark_device("Start Direct-Inverse", s_)).empty()) return ce;
+    nvtxRangePushA("time step");
+    ce = step(it, t1, t2, m1, m2, coef);
+    nvtxRangePop();
+    if (!ce.empty()) return ce;
+    return mark_device("Finish Direct-Inverse", s_);
   };
-  e = walk(use, stepf, [&](int it) { eval_receivers(it); });
+  auto recvf = [&](int it) {
+    mark_device("Start Resultant", s_);
+    eval_receivers(it);
+    mark_device("Finish Resultant", s_);
+  };
+  e = walk(use, stepf, recvf);
   if (!e.empty()) return e;
-  if (dev_span.size() % 2 == 1 && !(e = span_mark()).empty()) return e;
+  if (dev_span.size() % 2 == 1) {
+    if (!(e = span_mark()).empty()) return e;
+    if (!(e = decade_end()).empty()) return e;
+  }
   // join the factor stream (nothing is left on it once every factor was used)
   TRY_CUDA(cudaEventRecord(ev_[5], fs_));
   TRY_CUDA(cudaStreamWaitEvent(s_, ev_[5], 0));
@@ -819,7 +932,7 @@ std::string TransientSolve::run() {
   pt_.factor_s = pt_.factor_gpu_ms * 1e-3;
   pt_.steps_s = pt_.solve_gpu_ms * 1e-3;
   (void)tstart;
-  return "";
+  return flush_marks();
 }
 
 std::string TransientSolve::results(std::vector<double>& eall, std::vector<double>& emf,

@@ -33,6 +33,14 @@ struct RunOptions {
   // holds the second factor with room to spare.  Results are the same either way.
   int factor_slots = 0;
   const volatile int* cancel = nullptr;  // checked between time steps when set
+  // Drop-in module behaviour (tdem_run_directory and the executable).
+  // stop_file: a file whose presence ends the run before the next time step, as the
+  // reference's `stop` file does (CheckStop, GeoCalculatorSP.cpp:27-39, polled per
+  // step at time_approx.cpp:908).  time_watcher: file the phase marks are appended
+  // to, one "<ticks>\t<label>" line each with the reference's labels
+  // (TimeWatcher.cpp:37-44; TaskSP.cpp:459-701, time_approx.cpp:983-1131).
+  std::string stop_file;
+  std::string time_watcher;
 };
 
 struct PhaseTimes {
@@ -72,6 +80,12 @@ class TransientSolve {
   // Writes edsall_anom.N, ball_anom.N and eall_anom.N into the model directory.
   std::string write_outputs();
 
+  // Host phase mark (time_watcher only; also an NVTX mark).
+  void mark_host(const std::string& label);
+  // Appends the marks collected since the last call to the time_watcher file,
+  // ordered by time.  Device marks must have completed.
+  std::string flush_marks();
+
   const Model& model() const { return m_; }
   const PhaseTimes& times() const { return pt_; }
   int first_layer() const { return tlf_; }
@@ -97,6 +111,18 @@ class TransientSolve {
   std::vector<uint8_t> diag_;
   std::vector<double> S_;
   PhaseTimes pt_;
+  // phase marks (time_watcher only): host marks carry a wall time, device marks an
+  // event on the stream doing the work, converted through mark_origin_ (recorded
+  // at the start of run() together with its wall time)
+  struct PhaseMark {
+    std::string label;
+    cudaEvent_t ev = nullptr;
+    double wall_s = 0;
+  };
+  std::vector<PhaseMark> marks_;
+  cudaEvent_t mark_origin_ = nullptr;
+  double mark_origin_s_ = 0;
+  std::string mark_device(const std::string& label, cudaStream_t s);
   int launches_ = 0;
   int n_ = 0, npls_ = 0, ntime_ = 0;
   int64_t n_int_ = 0;

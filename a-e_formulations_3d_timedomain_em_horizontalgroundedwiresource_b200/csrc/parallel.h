@@ -47,8 +47,16 @@ void parallel_chunks(int64_t n, int nt, F&& f) {
   if (nt > 1) {
     std::vector<std::thread> pool;
     pool.reserve(nt - 1);
-    for (int t = 1; t < nt; ++t) pool.emplace_back([&range, t] { range(t); });
+    // a range whose thread cannot be started (std::system_error) runs inline on this
+    // thread after the started ones, so every range runs once and every started
+    // thread is joined before anything leaves this scope
+    int started = 1;
+    try {
+      for (; started < nt; ++started) pool.emplace_back([&range, t = started] { range(t); });
+    } catch (...) {
+    }
     range(0);
+    for (int t = started; t < nt; ++t) range(t);
     for (std::thread& th : pool) th.join();
   } else {
     range(0);

@@ -126,9 +126,10 @@ extern "C" tdem_status tdem_residual_norms(int device, int64_t n, const int64_t*
 // ---------------------------------------------------------------------------
 // Allocation-free variant: the scratch is a file-scope device array of fixed
 // size (kResScratchBytes = 303,104 bytes: 296 CTAs x 64 columns x 2 sums), so a
-// call makes no device allocation.  Its device address is looked up once per
-// device (cudaGetSymbolAddress, with that device current) on the first call;
-// that first call may load the module and should happen before any stream
+// call makes no device allocation.  Its device address is looked up on every
+// call (cudaGetSymbolAddress, with the call's device current): cheap once the
+// module is loaded, and never stale, also after a caller's cudaDeviceReset.  The
+// first call on a device may load the module and should happen before any stream
 // capture.  The scratch needs no initial value (pass 1 writes every entry pass 2
 // reads).  Calls whose executions overlap on one device share the scratch and
 // race: order them on one stream or synchronise between them.
@@ -138,18 +139,12 @@ namespace {
 __device__ __align__(256) double g_res_scratch[tdem::kResBlocks * tdem::kResMaxCols * 2];
 
 constexpr int kMaxDevices = 64;
-std::mutex g_scratch_mu;
-double* g_scratch_ptr[kMaxDevices] = {};
 
-// Device address of g_res_scratch on the current device `device` (nullptr on failure).
-double* scratch_address(int device) {
-  std::lock_guard<std::mutex> lk(g_scratch_mu);
-  if (!g_scratch_ptr[device]) {
-    void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_res_scratch) != cudaSuccess) return nullptr;
-    g_scratch_ptr[device] = static_cast<double*>(p);
-  }
-  return g_scratch_ptr[device];
+// Device address of g_res_scratch on the current device (nullptr on failure).
+double* scratch_address() {
+  void* p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_res_scratch) != cudaSuccess) return nullptr;
+  return static_cast<double*>(p);
 }
 
 }  // namespace
@@ -161,7 +156,7 @@ extern "C" tdem_status tdem_residual_norms_noalloc(int device, int64_t n, const 
   if (device < 0 || device >= kMaxDevices) return TDEM_ERR_ARGUMENT;
   DeviceGuard g(device);
   if (g.err != cudaSuccess) return TDEM_ERR_CUDA;
-  double* scratch = scratch_address(device);
+  double* scratch = scratch_address();
   if (!scratch) return TDEM_ERR_CUDA;
   const cudaError_t e =
       tdem::launch_residual_norms(n, rowptr, col, val, x, b, ld, ncols, norms, scratch, (cudaStream_t)stream);

@@ -52,7 +52,18 @@ typedef enum tdem_status {
  * normal field of each time layer is read from the file m<PName>.enor.NNNN in
  * `workdir` (float32 per anomalous edge and source), the stand-in for the named
  * shared memory the reference maps (time_approx.cpp:1263-1348); the E-formulation
- * also reads the normal potential v3n.dat for layer 0. 
+ * also reads the normal potential v3n.dat for layer 0.
+ * As the reference's module does: a file named `stop` in `workdir` ends the run
+ * (before it starts, or before the next time step; CheckStop,
+ * GeoCalculatorSP.cpp:27-39, TaskSP.cpp:462, time_approx.cpp:908) with
+ * TDEM_ERR_CANCELLED and no outputs; phase marks are appended to
+ * `workdir`/TimeWatcher.log as "<clock ticks>\t<label>" lines with the
+ * reference's labels (TimeWatcher.cpp:37-44: Start CalcSP, Start/Finish
+ * Prepare_To_Schema, Start decade / Start schema / Processing decade results /
+ * Finish decade iDec= N, Start prepare matrix for new decade, Start/Finish
+ * factorization, Start/Finish Direct-Inverse, Start/Finish Resultant); the times
+ * of device work are taken from CUDA events on the streams that do it, and the
+ * same labels are NVTX marks.
  * Replaces: GeoCalculatorSP.cpp:1656-1662 -> CalcNonstat3DLine main -> CalcSP
  * (TaskSP.cpp:445-711). */
 tdem_status tdem_run_directory(const char* workdir, int formulation, int scheme, int device,
@@ -261,7 +272,14 @@ void tdem_server_destroy(tdem_server* srv);
  * right-hand sides b -> x), phase -1 (release).  The handle lives in pt[0];
  * maxfct, mnum, perm, iparm and msglvl are accepted and ignored.  *error: 0 ok,
  * -1 bad input / unsupported phase or mtype, -2 out of memory or CUDA error,
- * -4 non-positive pivot.  Runs on CUDA device 0 unless TDEM_PARDISO_DEVICE is set. */
+ * -4 non-positive pivot.  Runs on CUDA device 0 unless TDEM_PARDISO_DEVICE is set.
+ * The reference zeroes pt before every phase 12 (pardiso_solver::init,
+ * pardiso.cpp:43-58, 76): the handle is also kept by the address of pt, so a
+ * phase 12 on a zeroed pt reuses the analysis, factor memory and stream made
+ * for that array, and phase -1 releases them.  A phase 33 with more columns than
+ * the analysing phase 12 was given (the reference analyses with nrhs = 1 and
+ * solves npls columns) widens the solve once, refactoring from the values
+ * already on the device. */
 void tdem_pardiso_64(void* pt, const long long* maxfct, const long long* mnum, const long long* mtype,
                      const long long* phase, const long long* n, const void* a, const long long* ia,
                      const long long* ja, long long* perm, const long long* nrhs, long long* iparm,
@@ -274,6 +292,10 @@ void pardiso_64(void* pt, const long long* maxfct, const long long* mnum, const 
                 const long long* msglvl, void* b, void* x, long long* error);
 /* MKL threading call made by pardiso_solver::factorize (pardiso.cpp:83); no-op here. */
 void mkl_set_num_threads(int n);
+/* Live pardiso_64 handles (made by phase 12, released by phase -1).  No counterpart
+ * in the reference: lets a caller check that repeated factorizations through the
+ * boundary hold one handle per pt array. */
+int tdem_pardiso_handles(void);
 
 /* Residual norms of a block of solutions, computed on CUDA device `device`:
  * norms[2j] = ||b_j - A x_j||_2 and norms[2j+1] = ||b_j||_2 for j < ncols.
@@ -293,9 +315,10 @@ tdem_status tdem_residual_norms(int device, int64_t n, const int64_t* rowptr, co
  * allocate: code being captured into a CUDA graph (cudaMallocAsync inside a capture
  * becomes part of the graph) and callers that run against a fixed memory budget.
  * The scratch is a static device array of 303,104 bytes in the library (296 x 64 x 2
- * doubles), so ncols is limited to 64 (larger is TDEM_ERR_ARGUMENT).  The first call
- * on each device looks up the array's address (cudaGetSymbolAddress, which may load
- * the module): make that first call before any stream capture.  The scratch needs no
+ * doubles), so ncols is limited to 64 (larger is TDEM_ERR_ARGUMENT).  Every call
+ * looks up the array's address on its device (cudaGetSymbolAddress; the first call
+ * on a device may load the module, so make it before any stream capture), so the
+ * address is never stale, also after a cudaDeviceReset.  The scratch needs no
  * initial contents.  Calls whose executions overlap on one device share the scratch
  * and race: issue them on one stream or synchronise between them.  Same arguments
  * and results as tdem_residual_norms.

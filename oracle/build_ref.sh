@@ -12,14 +12,15 @@
 #   oracle/_ref/TimeDirectSolver           the reference's time-grid regularisation
 #   oracle/_ref/CorrectTimeMesh            the reference's short-decade correction
 #
-# The reference sources are read in place (default /root/reference, override with
-# TDEM_REFERENCE_ROOT); nothing is copied into the repository.  When the reference
+# The reference sources are read in place: TDEM_REFERENCE_ROOT, else a checkout
+# named "reference" beside the repository (../reference from the repository
+# root); nothing is copied into the repository.  When the reference
 # tree is absent (for example on a machine that only runs the prebuilt files) the
 # reference binaries are skipped and only liboracle.so is built.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
 OUT="$HERE/_ref"
-REF="${TDEM_REFERENCE_ROOT:-/root/reference}"
+REF="${TDEM_REFERENCE_ROOT:-$HERE/../../reference}"
 MOD="$REF/CODE/programs to folder Modules"
 JOBS="${JOBS:-$(nproc)}"
 CXX="${TDEM_CXX:-g++}"

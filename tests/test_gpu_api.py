@@ -102,9 +102,42 @@ def test_pardiso_gpu_multi_rhs_and_refactor(pkg):
     assert h[0] == 0
 
 
+def test_pardiso_gpu_zeroed_pt_reuses_its_handle(pkg):
+    """The reference zeroes pt before every phase 12 (pardiso_solver::init) and
+    releases it once at the end: every refactorization must reuse the handle kept
+    for that pt array, holding one factor on the device, not one per call."""
+    import torch
+    lib = pkg.load_library()
+    n = 3000
+    A = _spd(n, 13)
+    a, ia, ja = _upper(A)
+    h = np.zeros(64, dtype=np.int64)
+    before = lib.tdem_pardiso_handles()
+    rng = np.random.default_rng(3)
+    b = rng.standard_normal((8, n))
+    x = np.zeros_like(b)
+    xr = np.linalg.solve(A.toarray(), b.T).T
+    free = []
+    for k in range(4):
+        h[:] = 0  # what pardiso_solver::factorize does before each phase 12
+        scale = 1.0 + k
+        a2 = a * scale
+        assert pkg.pardiso_64(h, 12, a2, ia, ja) == 0  # analysed with nrhs = 1, as the reference does
+        assert lib.tdem_pardiso_handles() == before + 1
+        x[:] = 0
+        assert pkg.pardiso_64(h, 33, a2, ia, ja, nrhs=8, b=b, x=x) == 0  # widens to 8 columns once
+        assert np.abs(x - xr / scale).max() <= 1e-11 * np.abs(xr).max()
+        torch.cuda.synchronize()
+        free.append(torch.cuda.mem_get_info()[0])
+    # no factor, stream or workspace accumulates across refactorizations
+    assert free[-1] >= free[1] - (1 << 20)
+    assert pkg.pardiso_64(h, -1, a, ia, ja) == 0
+    assert h[0] == 0 and lib.tdem_pardiso_handles() == before
+
+
 def test_pardiso_gpu_dense_front(pkg):
-    """A dense SPD matrix is one front of 1,300 pivots: five outer panels of 256
-    columns, each ending in a rank-256 trailing update of the rest."""
+    """A dense SPD matrix is one front of 1,300 pivots: three outer panels of up
+    to 512 columns, the first two ending in a rank-512 trailing update of the rest."""
     n = 1300
     rng = np.random.default_rng(5)
     G = rng.standard_normal((n, n))
@@ -181,3 +214,49 @@ def test_factor_slots_out_of_range_is_rejected(pkg, golden, tmp_path):
     with pytest.raises(pkg.TdemError) as ei:
         pkg.Solver(d, "A", 2, factor_slots=3)
     assert ei.value.status == 1
+
+
+def test_stop_file_ends_the_drop_in_run(pkg, golden, tmp_path):
+    """A `stop` file in the run directory ends the module run before any output is
+    written, as the reference's CheckStop does (TaskSP.cpp:462)."""
+    d = str(tmp_path / "m")
+    golden.write_case_inputs("cube6", d)
+    open(os.path.join(d, "stop"), "w").close()
+    with pytest.raises(pkg.TdemError) as ei:
+        pkg.run_directory(d, "A", 2)
+    assert ei.value.status == 5
+    assert not os.path.exists(os.path.join(d, "eall_anom.1"))
+    os.unlink(os.path.join(d, "stop"))
+    pkg.run_directory(d, "A", 2)
+    assert os.path.exists(os.path.join(d, "eall_anom.1"))
+
+
+@pytest.mark.parametrize("form,scheme", [("A", 2), ("E", 3)])
+def test_time_watcher_log_has_the_reference_phases(pkg, golden, tmp_path, form, scheme):
+    """The module run appends the reference's TimeWatcher labels, one per phase,
+    in time order: one factorization mark pair per factorization, one solve and
+    one receiver pair per step."""
+    d = str(tmp_path / "m")
+    golden.write_case_inputs("cube8_block", d)
+    pkg.run_directory(d, form, scheme)
+    with pkg.Solver(d, form, scheme) as s:  # counts of the same run (no log here)
+        s.run()
+        info = s.info()
+    lines = [ln.rstrip("\n").split("\t", 1) for ln in open(os.path.join(d, "TimeWatcher.log"))]
+    ticks = [int(t) for t, _ in lines]
+    labels = [lab for _, lab in lines]
+    assert labels[:2] == ["Start CalcSP", "Start Prepare_To_Schema"]
+    assert "Finish Prepare_To_Schema" in labels
+    assert ticks == sorted(ticks)
+    assert labels.count("Start factorization") == info["factorizations"]
+    assert labels.count("Finish factorization") == info["factorizations"]
+    assert labels.count("Start prepare matrix for new decade") == info["factorizations"]
+    assert labels.count("Start Direct-Inverse") == info["steps"]
+    assert labels.count("Finish Direct-Inverse") == info["steps"]
+    n_dec = labels.count("Start schema iDec= 0") and sum(1 for x in labels if x.startswith("Start decade iDec="))
+    assert n_dec >= 2 and n_dec == sum(1 for x in labels if x.startswith("Finish decade iDec="))
+    assert labels[-1] == "Finish decade iDec= %d" % (n_dec - 1)
+    # every factorization finishes after it starts
+    for a, b in zip([i for i, x in enumerate(labels) if x == "Start factorization"],
+                    [i for i, x in enumerate(labels) if x == "Finish factorization"]):
+        assert a < b

@@ -36,14 +36,19 @@ def test_noalloc_matches_allocating_entry_point_twice(pkg):
     ref_fn, na_fn = _bind(lib, "tdem_residual_norms"), _bind(lib, "tdem_residual_norms_noalloc")
     dev = torch.device("cuda:0")
     stream = torch.cuda.current_stream().cuda_stream
-    for n, per_row, ncols, seed in ((30_000, 12, 64, 1), (5_000, 5, 7, 2)):
+    # the last case stores its columns with a leading dimension larger than n
+    for n, per_row, ncols, seed, pad in ((30_000, 12, 64, 1, 0), (5_000, 5, 7, 2, 0), (4_000, 6, 5, 3, 37)):
         a, x, b = _system(n, per_row, ncols, seed)
+        ld = n + pad
+        xp = np.zeros((ncols, ld))
+        bp = np.full((ncols, ld), 1e300)  # padding rows must not be read
+        xp[:, :n], bp[:, :n] = x, b
         rp = torch.from_numpy(a.indptr.astype(np.int64)).to(dev)
         ci = torch.from_numpy(a.indices.astype(np.int32)).to(dev)
         va = torch.from_numpy(a.data).to(dev)
-        xd = torch.from_numpy(np.ascontiguousarray(x)).to(dev)
-        bd = torch.from_numpy(np.ascontiguousarray(b)).to(dev)
-        args = (0, n, rp.data_ptr(), ci.data_ptr(), va.data_ptr(), xd.data_ptr(), bd.data_ptr(), n, ncols)
+        xd = torch.from_numpy(xp).to(dev)
+        bd = torch.from_numpy(bp).to(dev)
+        args = (0, n, rp.data_ptr(), ci.data_ptr(), va.data_ptr(), xd.data_ptr(), bd.data_ptr(), ld, ncols)
         ref = torch.zeros(2 * ncols, dtype=torch.float64, device=dev)
         assert ref_fn(*args, ref.data_ptr(), stream) == 0
         for _ in range(2):
