@@ -148,6 +148,7 @@ EXPORTED = [
     "tdem_solver_results",
     "tdem_solver_info",
     "tdem_solver_cancel",
+    "tdem_solver_time_step",
     "tdem_solver_error",
     "tdem_solver_destroy",
     "tdem_pardiso_64",
@@ -201,6 +202,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     for name in ("tdem_solver_run", "tdem_solver_write_outputs", "tdem_solver_cancel"):
         getattr(lib, name).argtypes = [P]
         getattr(lib, name).restype = ctypes.c_int
+    lib.tdem_solver_time_step.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    lib.tdem_solver_time_step.restype = ctypes.c_int
     lib.tdem_solver_results.argtypes = [P, P, P, P]
     lib.tdem_solver_results.restype = ctypes.c_int
     lib.tdem_solver_info.argtypes = [P, ctypes.POINTER(TdemInfo)]
@@ -356,6 +359,13 @@ class Solver:
 
     def cancel(self) -> None:
         self._check(self._lib.tdem_solver_cancel(self._h))
+
+    def time_step(self, block: bool = True, reps: int = 5) -> float:
+        """Device ms of one time step's RHS + solves of every source on the last
+        run's factor: one n x npls block, or npls single-column steps in turn."""
+        ms = ctypes.c_double(0.0)
+        self._check(self._lib.tdem_solver_time_step(self._h, 1 if block else 0, int(reps), ctypes.byref(ms)))
+        return ms.value
 
     def write_outputs(self) -> None:
         self._check(self._lib.tdem_solver_write_outputs(self._h))

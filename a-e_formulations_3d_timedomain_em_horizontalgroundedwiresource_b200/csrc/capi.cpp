@@ -289,6 +289,16 @@ tdem_status tdem_solver_info(const tdem_solver* s, tdem_info* info) {
   });
 }
 
+tdem_status tdem_solver_time_step(tdem_solver* s, int block, int reps, double* ms_per_step) {
+  return guard([&]() -> tdem_status {
+    if (!s || !ms_per_step || reps < 1) return TDEM_ERR_ARGUMENT;
+    if (!s->ran) return TDEM_ERR_STATE;
+    cudaSetDevice(s->device);
+    s->error = s->solve.time_step(block != 0, reps, ms_per_step);
+    return classify(s->error);
+  }, nullptr, 0, s ? &s->error : nullptr);
+}
+
 tdem_status tdem_solver_cancel(tdem_solver* s) {
   return guard([&]() -> tdem_status {
     if (!s) return TDEM_ERR_ARGUMENT;

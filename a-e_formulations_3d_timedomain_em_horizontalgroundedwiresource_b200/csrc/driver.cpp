@@ -935,6 +935,39 @@ std::string TransientSolve::run() {
   return flush_marks();
 }
 
+std::string TransientSolve::time_step(bool block, int reps, double* ms) {
+  if (pt_.steps == 0) return "time_step needs a completed run";
+  if (reps < 1) return "time_step: reps must be positive";
+  if (opt_.precision != 64) return "time_step: FP64 solves only";
+  const int64_t n = n_;
+  const double* u = layer(0);  // any finite history: only the time is measured
+  auto one = [&]() -> std::string {
+    if (block) {
+      launch_history_rhs(d_rowptr_, d_col_, d_C_, u, u, 1.0, 0.0, d_S_, 0.0, d_bound_, n_, npls_, d_rhs_, s_);
+      return chol_->solve_graph(d_rhs_, d_x_, n_, npls_, s_, slot_);
+    }
+    for (int j = 0; j < npls_; ++j) {
+      launch_history_rhs(d_rowptr_, d_col_, d_C_, u + j * n, u + j * n, 1.0, 0.0, d_S_ + j * n, 0.0, d_bound_, n_,
+                         1, d_rhs_ + j * n, s_);
+      chol_->solve(d_rhs_ + j * n, d_x_ + j * n, n_, 1, s_, slot_);
+    }
+    return "";
+  };
+  std::string e = one();  // warm-up (captures the block graph on first use)
+  if (!e.empty()) return e;
+  TRY_CUDA(cudaEventRecord(ev_[0], s_));
+  for (int r = 0; r < reps; ++r)
+    if (!(e = one()).empty()) return e;
+  TRY_CUDA(cudaEventRecord(ev_[1], s_));
+  TRY_CUDA(cudaStreamSynchronize(s_));
+  TRY_CUDA(cudaGetLastError());
+  float t = 0.f;
+  TRY_CUDA(cudaEventElapsedTime(&t, ev_[0], ev_[1]));
+  *ms = t / reps;
+  if (chol_->solve_status(s_)) return "CUDA: a wait of the level triangular solves gave up";
+  return "";
+}
+
 std::string TransientSolve::results(std::vector<double>& eall, std::vector<double>& emf,
                                     std::vector<double>& ball) {
   const int nl = tll_ - tlf_ + 1;

@@ -80,6 +80,12 @@ class TransientSolve {
   // Writes edsall_anom.N, ball_anom.N and eall_anom.N into the model directory.
   std::string write_outputs();
 
+  // Device time of one time step's work on the factor the last run() ended with:
+  // the history right-hand side and the triangular solves of every source, as one
+  // n x npls block (block = true; the solve replayed from its CUDA graph, as run()
+  // does) or as npls single-column steps issued one after another (block = false).
+  // Average over reps repetitions, in ms.  The solution history is not changed.
+  std::string time_step(bool block, int reps, double* ms);
   // Host phase mark (time_watcher only; also an NVTX mark).
   void mark_host(const std::string& label);
   // Appends the marks collected since the last call to the time_watcher file,

@@ -336,14 +336,16 @@ def layered_block_model(cells: int = 80, core_h: float = 10.0, core_half: float 
                         extent: float = 5000.0, n_air: int = 20, n_dec: int = 8,
                         steps_per_dec: int = 20, t_end: float = 1e-1,
                         sources: Optional[Sequence] = None, n_receivers: int = 21,
-                        n_srs_razb: int = 500) -> ModelSpec:
+                        n_srs_razb: int = 500, cells_z: Optional[int] = None,
+                        boxes: Optional[Sequence["Box"]] = None) -> ModelSpec:
     """Three-layer earth (100 Ohm.m 0-50 m, 10 Ohm.m 50-300 m, 1000 Ohm.m below) with a
-    0.1 S/m 200x200x100 m block whose top is at 150 m depth."""
+    0.1 S/m 200x200x100 m block whose top is at 150 m depth (or the given boxes);
+    cells per horizontal side, cells_z vertically (default: cells)."""
     n_core = int(round(2 * core_half / core_h))
     n_side = (cells - n_core) // 2
     x = symmetric_axis(core_half, core_h, n_side, extent)
     y = x.copy()
-    n_earth = cells - n_air
+    n_earth = (cells if cells_z is None else cells_z) - n_air
     n_earth_core = min(30, n_earth - 1)
     z = vertical_axis(n_earth_core * core_h, core_h, n_earth - n_earth_core, extent, n_air, extent)
     t = decade_time_grid(t_end, n_dec, steps_per_dec)
@@ -352,9 +354,38 @@ def layered_block_model(cells: int = 80, core_h: float = 10.0, core_half: float 
     rec = receivers_on_y_axis(n_receivers)
     return ModelSpec(x=x, y=y, z=z,
                      layers=[(0.0, 1.0 / 100.0), (-50.0, 1.0 / 10.0), (-300.0, 1.0 / 1000.0)],
-                     boxes=[Box(-100.0, 100.0, -100.0, 100.0, -250.0, -150.0, 0.1)],
+                     boxes=(list(boxes) if boxes is not None
+                            else [Box(-100.0, 100.0, -100.0, 100.0, -250.0, -150.0, 0.1)]),
                      sources=list(sources), receivers_b=[rec] * len(sources),
                      receivers_e=[rec] * len(sources), times=t, n_srs_razb=n_srs_razb)
+
+
+def random_blocks(seed: int, count: int = 5, sigma_lo: float = 0.05, sigma_hi: float = 1.0,
+                  edge_lo: float = 50.0, edge_hi: float = 200.0, half_width: float = 180.0,
+                  depth_lo: float = 20.0, depth_hi: float = 300.0) -> List["Box"]:
+    """count axis-aligned blocks drawn from PCG64(seed): edges uniform in
+    [edge_lo, edge_hi] m, centres uniform in the core (|x|, |y| <= half_width minus
+    half an edge) with tops between depth_lo and depth_hi, conductivity log-uniform
+    in [sigma_lo, sigma_hi] S/m."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for _ in range(count):
+        e = rng.uniform(edge_lo, edge_hi, 3)
+        cx = rng.uniform(-half_width + e[0] / 2, half_width - e[0] / 2)
+        cy = rng.uniform(-half_width + e[1] / 2, half_width - e[1] / 2)
+        top = -rng.uniform(depth_lo, depth_hi)
+        sig = float(10 ** rng.uniform(np.log10(sigma_lo), np.log10(sigma_hi)))
+        out.append(Box(cx - e[0] / 2, cx + e[0] / 2, cy - e[1] / 2, cy + e[1] / 2, top - e[2], top, sig))
+    return out
+
+
+def largest_model(seed: int = 20261203) -> ModelSpec:
+    """The largest single model: 120 x 120 x 100 cells, the three-layer earth with five
+    random conductive blocks of 0.05-1 S/m (random_blocks(seed)), a 200 m grounded
+    wire along x centred at the origin, 200 steps (10 doubling decades of 20) to 1 s."""
+    return layered_block_model(cells=120, cells_z=100, n_dec=10, t_end=1.0,
+                               sources=[((-100.0, 0.0, 0.0), (100.0, 0.0, 0.0))],
+                               boxes=random_blocks(seed))
 
 
 def random_request_model(seed: int, cells_lo: int = 30, cells_hi: int = 100):

@@ -47,8 +47,9 @@ def make_spec(cfg: str, mg, n_steps_override=None):
         spec = mg.layered_block_model(sources=mg.wire_grid_sources())
         return spec, "A", 3, "80^3 three-layer + block, A-form, BDF2, 160 steps, 32 wires as one n x 32 block"
     if cfg == "c5":
-        spec = mg.layered_block_model(cells=120, n_dec=10, t_end=1.0)
-        return spec, "A", 3, "120^3-class three-layer model, A-form, BDF2, 200 steps"
+        spec = mg.largest_model(20261203)
+        return spec, "A", 3, ("120x120x100 three-layer + 5 random 0.05-1 S/m blocks (PCG64(20261203)), A-form, "
+                              "BDF2, 200 steps to 1 s, 200 m wire, 21 receivers")
     raise ValueError(cfg)
 
 
@@ -193,15 +194,24 @@ def measured_peaks() -> dict:
         return {}
 
 
+def count_factorizations(times, scheme: int):
+    """Factorizations of a full solve: one per distinct step length, plus the
+    two-point start-up factorization of the three-point scheme."""
+    h = [times[i + 1] - times[i] for i in range(len(times) - 1)]
+    distinct = 1 + sum(1 for i in range(1, len(h)) if abs(1 - h[i - 1] / h[i]) > 1e-3)
+    return distinct + (1 if scheme == 3 else 0)
+
+
 def cpu_baseline(cfg: str, spec, form: str, scheme: int, workdir: str, full_factorizations: int,
                  full_steps: int, threads: int) -> dict:
     """Times the reference's own CalcNonstat3DLine (built from source, oracle/_ref)
     on a bounded sample of the same workload: the same variant, mesh and matrices
     with the time grid cut to one factorization (the first 3 steps of the two-point
     scheme; the first 2 of the three-point one, which takes them with the two-point
-    formula before its own).  The per-call wall
-    times logged by the pardiso_64 stand-in split the run into set-up,
-    factorization and per-step time, which are scaled to the full workload."""
+    formula before its own).  The per-call wall times logged by the pardiso_64
+    stand-in split the run into set-up, factorization and per-step time; the full
+    solve's time is extrapolated from them (set-up + factorizations x factor time +
+    steps x step time) and labelled as such.  The sample's outputs stay in workdir."""
     sys.path.insert(0, os.path.join(HERE, "oracle"))
     import run_ref  # noqa: E402  (oracle: baseline leg only)
     mg = importlib.import_module(PKG + ".modelgen")
@@ -249,48 +259,94 @@ def cpu_baseline(cfg: str, spec, form: str, scheme: int, workdir: str, full_fact
     t_setup = wall - t_fact * len(fac) - t_after
     full = t_setup + full_factorizations * t_fact + full_steps * t_step
     return {"value": 1.0 / full, "unit": "forward solves/s", "cores": threads, "kind": "reference",
+            "extrapolated": True, "measured_wall_s": wall, "sampled_steps": steps,
+            "sampled_factorizations": len(fac), "setup_s": t_setup, "factor_s": t_fact, "step_s": t_step,
+            "extrapolated_solve_s": full, "full_factorizations": full_factorizations, "full_steps": full_steps,
             "sample": "reference CalcNonstat3DLine_%s (built from source, CPU FP64 Cholesky stand-in for "
                       "MKL PARDISO) on the same mesh cut to %d steps: wall %.1f s = set-up %.1f s + "
-                      "%d factorization(s) x %.2f s + %d steps x %.3f s; scaled to %d factorizations + %d "
-                      "steps = %.1f s per forward solve" % (variant, steps, wall, t_setup, len(fac), t_fact,
-                                                            steps, t_step, full_factorizations, full_steps,
-                                                            full)}
+                      "%d factorization(s) x %.2f s + %d steps x %.3f s; extrapolated to %d factorizations + "
+                      "%d steps = %.1f s per forward solve" % (variant, steps, wall, t_setup, len(fac), t_fact,
+                                                               steps, t_step, full_factorizations, full_steps,
+                                                               full)}
+
+
+def gpu_parity(pkg, outs, ref_dir: str, work: str, form: str, scheme: int, device: int, label: str) -> dict:
+    """Runs the GPU solver on the inputs of a reference run (ref_dir, outputs
+    present) and compares every result file: the largest deviation of any component
+    from the reference, relative to the peak of that receiver's vector transient
+    (outputs.compare_files)."""
+    sys.path.insert(0, os.path.join(HERE, "oracle"))
+    import run_ref  # noqa: E402  (oracle: the checker)
+    run_ref.copy_inputs(ref_dir, work)
+    with pkg.Solver(work, form, scheme, device=device) as s:
+        s.run()
+        s.write_outputs()
+        npls = s.info()["n_sources"]
+    worst = 0.0
+    for p in range(1, npls + 1):
+        for stem in ("eall_anom", "edsall_anom", "ball_anom"):
+            name = "%s.%d" % (stem, p)
+            worst = max(worst, outs.compare_files(os.path.join(work, name), os.path.join(ref_dir, name)))
+    return {"case": label, "max_rel_err": worst, "files": 3 * npls}
 
 
 # ---------------------------------------------------------------------------
 # arms
 # ---------------------------------------------------------------------------
 def run_reference_arm(args, world, rank, local):
+    """The reference's own CalcNonstat3DLine on the host cores.  A full solve of the
+    80^3 workload takes ~13 min on 16 cores, so each sample runs the workload cut to
+    one factorization and the full solve is extrapolated (labelled so in the line,
+    with the measured phases); the extrapolation is checked once per run against a
+    full reference solve of the 40^3 half-space (A-form, two-point, 120 steps),
+    extrapolated and measured side by side."""
     if rank != 0:
         return
     mg = importlib.import_module(PKG + ".modelgen")
     spec, form, scheme, desc = make_spec(args.config, mg)
     threads = os.cpu_count() or 1
-    # full-workload counts: one factorization per distinct step length (+1 start-up
-    # factorization for the three-point scheme), one solve per time step
-    ts = spec.times
-    h = [ts[i + 1] - ts[i] for i in range(len(ts) - 1)]
-    distinct = 1 + sum(1 for i in range(1, len(h)) if abs(1 - h[i - 1] / h[i]) > 1e-3)
-    n_fact = distinct + (1 if scheme == 3 else 0)
-    n_steps = len(ts) - 1
+    n_fact = count_factorizations(spec.times, scheme)
+    n_steps = len(spec.times) - 1
+    samples = max(1, min(args.steps, args.ref_samples))
     base = tempfile.mkdtemp(prefix="tdem_ref_")
     vals = []
+    check = None
     try:
-        for i in range(args.warmup + args.steps):
+        t_run = time.time()
+        for i in range(samples):
             d = os.path.join(base, "s%d" % i)
             os.makedirs(d)
-            r = cpu_baseline(args.config, spec, form, scheme, d, n_fact, n_steps, threads)
-            if i >= args.warmup:
-                vals.append(r)
+            vals.append(cpu_baseline(args.config, spec, form, scheme, d, n_fact, n_steps, threads))
             shutil.rmtree(d, ignore_errors=True)
+        if not args.no_ref_check and vals and vals[0].get("value"):
+            sys.path.insert(0, os.path.join(HERE, "oracle"))
+            import run_ref  # noqa: E402  (oracle: reference arm only)
+            c1 = mg.halfspace_model()
+            d = os.path.join(base, "c1_cut")
+            os.makedirs(d)
+            est = cpu_baseline("c1", c1, "A", 2, d, count_factorizations(c1.times, 2), len(c1.times) - 1, threads)
+            d = os.path.join(base, "c1_full")
+            mg.write_model(d, c1)
+            mg.write_analytic_initial_field(d, c1)
+            meas = run_ref.run_transient(d, "A2", threads=threads)
+            check = {"workload": "40^3 half-space, A-form, two-point, 120 steps (full reference solve)",
+                     "extrapolated_s": est["extrapolated_solve_s"], "measured_s": meas,
+                     "measured_over_extrapolated": meas / est["extrapolated_solve_s"]}
+        ref_wall = time.time() - t_run
     finally:
         shutil.rmtree(base, ignore_errors=True)
-    v = sum(x["value"] for x in vals) / len(vals) if vals and vals[0]["value"] else None
+    ok = [x for x in vals if x.get("value")]
+    v = sum(x["value"] for x in ok) / len(ok) if ok else None
+    last = dict(vals[-1]) if vals else None
     line = {"metric": METRIC, "value": v, "unit": "forward solves/s", "impl": "reference", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": (1000.0 / v) if v else None,
+            "steps": len(vals), "warmup": 0, "steps_requested": args.steps, "warmup_requested": args.warmup,
+            "extrapolated": True,
+            "ms_per_step": (1000.0 * sum(x["measured_wall_s"] for x in ok) / len(ok)) if ok else None,
+            "ms_per_step_is": "measured wall time of one sample (the workload cut to one factorization)",
+            "extrapolated_ms_per_solve": (1000.0 / v) if v else None,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": desc, "parallelism": "host cores"},
-            "cpu_baseline": dict(vals[-1]) if vals else None,
+            "data": "synthetic", "config": {"workload": desc, "parallelism": "host cores (%d threads)" % threads},
+            "cpu_baseline": last, "extrapolation_check": check, "wall_s": ref_wall,
             "e2e": {"value": v, "unit": "forward solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -380,6 +436,7 @@ def run_ours(args, world, rank, local):
                           "peak_source": ("MEASURED_PEAKS.json hbm_gbs (measured)" if hbm_measured
                                           else "fallback 6650 GB/s (MEASURED_PEAKS.json absent)")}
             cpu = None
+            parity = None
             if not args.no_cpu_baseline:
                 d = os.path.join(base, "cpu_sample")
                 os.makedirs(d)
@@ -389,6 +446,20 @@ def run_ours(args, world, rank, local):
                 except Exception as ex:  # the baseline is reported, never required
                     cpu = {"value": None, "unit": "forward solves/s", "cores": os.cpu_count(),
                            "kind": "reference", "sample": "failed: %s" % ex}
+                if cpu.get("value"):
+                    # the GPU path on the very inputs the reference sample ran: its outputs
+                    # against the reference's own, file by file
+                    outs = importlib.import_module(PKG + ".outputs")
+                    try:
+                        pc = gpu_parity(pkg, outs, d, os.path.join(base, "gpu_on_cpu_sample"), form, scheme,
+                                        local, "%s mesh (%d edges), %s%d, time grid cut to one factorization" %
+                                        (args.config, winfo["n_edges"], form, scheme))
+                        parity = {"max_rel_err": pc["max_rel_err"], "tol": 1e-9,
+                                  "pass": pc["max_rel_err"] <= 1e-9, "cases": [pc],
+                                  "measure": "max over receivers, time and components of |gpu - ref| / peak "
+                                             "of the reference receiver's vector transient"}
+                    except Exception as ex:
+                        parity = {"max_rel_err": None, "tol": 1e-9, "pass": False, "error": str(ex)}
             lat.sort()
             line = {
                 "metric": METRIC,
@@ -421,11 +492,46 @@ def run_ours(args, world, rank, local):
                 "roofline": roof,
                 "roofline_solve": roof_solve,
                 "cpu_baseline": cpu,
+                "parity": parity,
                 "e2e": e2e,
             }
+            if args.config == "c2" and not args.no_batched:
+                line["batched"] = batched_leg(args, pkg, base, form, scheme, local, value)
             print(json.dumps(line), flush=True)
     finally:
         shutil.rmtree(base, ignore_errors=True)
+
+
+def batched_leg(args, pkg, base: str, form: str, scheme: int, device: int, single_value: float) -> dict:
+    """The same model, formulation and scheme with 32 wires (centres on a 4 x 8
+    surface grid, 100 m apart) solved as one n x 32 block per time step, FP64: forward
+    solves/s of the block run against the single-wire FP64 rate of this run, and one
+    time step's device time as the graph-replayed block against 32 single-column
+    steps issued in turn on the same factor."""
+    mg = importlib.import_module(PKG + ".modelgen")
+    d = os.path.join(base, "batched")
+    spec = mg.layered_block_model(sources=mg.wire_grid_sources())
+    mg.write_model(d, spec)
+    mg.write_analytic_initial_field(d, spec)
+    with pkg.Solver(d, form, scheme, device=device) as s:
+        s.run()  # warm-up
+        runs = []
+        for _ in range(max(1, args.batched_runs)):
+            s.run()
+            runs.append(s.info()["run_gpu_ms"])
+        inf = s.info()
+        step_block = s.time_step(True, 5)
+        step_seq = s.time_step(False, 2)
+    ms = sum(runs) / len(runs)
+    npls = inf["n_sources"]
+    return {"workload": "same model, %s-form, %s, %d wires as one n x %d block per step, FP64" %
+                        (form, "BDF2" if scheme == 3 else "backward Euler", npls, npls),
+            "value": npls / (ms * 1e-3), "unit": "forward solves/s", "ms_per_run": ms, "runs": len(runs),
+            "vs_single_wire_fp64": npls / (ms * 1e-3) / single_value,
+            "step_ms": {"block_graph": step_block, "sequential_single_column": step_seq,
+                        "sequential_over_block": step_seq / step_block},
+            "factor_gpu_ms_per_run": inf["factor_gpu_ms"], "solve_gpu_ms_per_run": inf["solve_gpu_ms"],
+            "steps": inf["steps"], "factorizations": inf["factorizations"]}
 
 
 def run_serving(args, world, rank, local):
@@ -676,6 +782,12 @@ def main():
     ap.add_argument("--c4-cells", default="30,60", help="mesh cells per side, lo,hi (config c4; 30,100 in full)")
     ap.add_argument("--c4-active", type=int, default=4, help="requests on the device at once (config c4)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the 32-wire block leg (config c2)")
+    ap.add_argument("--batched-runs", type=int, default=1, help="timed runs of the 32-wire block leg")
+    ap.add_argument("--ref-samples", type=int, default=2,
+                    help="reference arm: samples of the cut workload (at most --steps)")
+    ap.add_argument("--no-ref-check", action="store_true",
+                    help="reference arm: skip the full 40^3 solve that checks the extrapolation")
     ap.add_argument("--precision", type=int, default=64, choices=[64, 32],
                     help="64: FP64 factor; 32: FP32 factor preconditioning FP64 CG")
     ap.add_argument("--fp32-update", default="default", choices=["default", "cuda_cores", "tensor_cores"])

@@ -214,6 +214,15 @@ tdem_status tdem_solver_write_outputs(tdem_solver* s);
  * to the files.  Any pointer may be NULL. */
 tdem_status tdem_solver_results(tdem_solver* s, double* eall, double* emf, double* ball);
 tdem_status tdem_solver_info(const tdem_solver* s, tdem_info* info);
+/* Device time of one time step's work on the factor the last tdem_solver_run ended
+ * with (FP64 solvers): the history right-hand side and the triangular solves of
+ * every source, either as one n x npls block (block != 0: the solve replayed from
+ * its CUDA graph, as the run does) or as npls single-column steps issued one after
+ * another (block == 0).  Average of reps repetitions in *ms_per_step; the solution
+ * history and the results are not changed.  TDEM_ERR_STATE before a completed run.
+ * No counterpart in the reference: it lets a caller compare the batched step with
+ * sequential per-source solves (pardiso.cpp:113-120 solves npls columns per call). */
+tdem_status tdem_solver_time_step(tdem_solver* s, int block, int reps, double* ms_per_step);
 /* Requests cancellation of a running tdem_solver_run (checked between time steps;
  * the reference polls a file named "stop", GeoCalculatorSP.cpp:27-39). */
 tdem_status tdem_solver_cancel(tdem_solver* s);

@@ -5,6 +5,9 @@
 #                                          the reference's own 3D transient solver, compiled
 #                                          unmodified from its sources with the shim headers in
 #                                          oracle/shim and the pardiso_64 stand-in
+#   oracle/_ref/CalcNonstat3DLine_{A2,A3,E2,E3}_gpu
+#                                          the same objects linked against the product
+#                                          library's pardiso_64 (the in-process boundary)
 #   oracle/_ref/CalcStat3D_3T_A            the reference's stationary A0 / V solver, same way
 #   oracle/_ref/SumNonstat3DOnly           the reference's per-component split of the 3D results
 #   oracle/_ref/SummatorEDMN               the reference's line-voltage integration (main.cpp
@@ -88,6 +91,19 @@ build_variant CalcNonstat3DLine_A3 "$MOD/!programs for 3-point implicit scheme/!
 build_variant CalcNonstat3DLine_E2 "$MOD/!programs for 2-point implicit scheme/!programs for E-formulation/CalcNonstat3DLine"
 build_variant CalcNonstat3DLine_E3 "$MOD/!programs for 3-point implicit scheme/!programs for E-formulation/CalcNonstat3DLine"
 build_variant CalcStat3D_3T_A "$MOD/CalcStat3D_3T_A" "-Dsprintf_s=sprintf"
+
+# The same unmodified reference objects linked against the product library's
+# pardiso_64 instead of the CPU stand-in: the in-process solver boundary as a
+# maintainer would wire it (oracle/_ref/CalcNonstat3DLine_<V>_gpu, run by the GPU
+# tests).  Built when the package library exists (build it first).
+PKGLIB="$HERE/../a-e_formulations_3d_timedomain_em_horizontalgroundedwiresource_b200/lib"
+if [ -f "$PKGLIB/libtdem_b200.so" ]; then
+  for v in A2 A3 E2 E3; do
+    $CXX -pthread -o "$OUT/CalcNonstat3DLine_${v}_gpu" "$OUT/obj_CalcNonstat3DLine_$v"/*.o \
+      -L"$PKGLIB" -ltdem_b200 -Wl,-rpath,'$ORIGIN/../../a-e_formulations_3d_timedomain_em_horizontalgroundedwiresource_b200/lib'
+    echo "built $OUT/CalcNonstat3DLine_${v}_gpu (pardiso_64 from libtdem_b200.so)"
+  done
+fi
 
 build_plain() {  # name, sources...
   local name="$1"

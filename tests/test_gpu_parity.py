@@ -2,6 +2,7 @@
 CalcNonstat3DLine (golden outputs made by the reference built from source) and
 against the numpy oracle, for all four variants."""
 import os
+import sys
 
 import numpy as np
 import pytest
@@ -98,3 +99,32 @@ def test_gpu_primary_secondary_matches_reference(pkg, outs, tmp_path, case, vari
     for o in ps.OUTPUTS:
         err = outs.compare_files(os.path.join(d, o + ".1"), os.path.join(GOLDEN, case, "%s_%s.1" % (variant, o)))
         assert err <= FP64_TOL, (o, err)
+
+
+@pytest.mark.parametrize("case,variant", [("cube8_block", "A2"), ("cube8_two_wires", "E3"), ("wires32", "A3")])
+def test_unmodified_reference_linked_to_gpu_pardiso(pkg, golden, outs, tmp_path, case, variant):
+    """The in-process boundary end to end: the reference's own CalcNonstat3DLine,
+    compiled from its sources unchanged and linked against this library's
+    pardiso_64 (oracle/_ref/CalcNonstat3DLine_<V>_gpu), reproduces the goldens.  Its
+    pardiso_solver zeroes pt before every factorization and solves npls columns
+    (32 for wires32) per call; its receiver projections are further handles."""
+    import subprocess
+    import run_ref
+    exe = run_ref.binary("CalcNonstat3DLine_%s_gpu" % variant)
+    if not os.path.exists(exe):
+        pytest.skip("oracle/_ref/CalcNonstat3DLine_%s_gpu not built" % variant)
+    d = str(tmp_path / "ref_gpu")
+    if case == "wires32":
+        sys.path.insert(0, GOLDEN)
+        import make_scale_golden as sg
+        sg.write_case_inputs(case, d)
+        gdir, npls = os.path.join(GOLDEN, "scale", case), 32
+    else:
+        golden.write_case_inputs(case, d)
+        gdir, npls = os.path.join(GOLDEN, case), golden.CASES[case].get("n_sources", 1)
+    with open(os.path.join(d, "run.log"), "w") as log:
+        subprocess.run([exe], cwd=d, stdout=log, stderr=subprocess.STDOUT, check=True, timeout=600)
+    for o in golden.OUTPUTS:
+        for p in range(1, npls + 1):
+            err = outs.compare_files(os.path.join(d, "%s.%d" % (o, p)), os.path.join(gdir, "%s_%s.%d" % (variant, o, p)))
+            assert err <= FP64_TOL, (o, p, err)

@@ -1,0 +1,55 @@
+"""GPU parity at the benchmark's scales against the reference's own
+CalcNonstat3DLine (golden outputs in tests/golden/scale, made by
+tests/golden/make_scale_golden.py from the reference built from source):
+
+  * the plain-method configuration in full: 40^3 half-space, A-formulation,
+    backward Euler, all 120 steps (6 factorizations);
+  * 32 wires solved as one n x 32 block per step (the batched path), A- and
+    E-formulation with the three-point scheme, every transmitter's three files.
+"""
+import os
+import sys
+
+import pytest
+
+from conftest import FP64_TOL, GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+sys.path.insert(0, GOLDEN)
+import make_scale_golden as sg  # noqa: E402
+
+SCALE = os.path.join(GOLDEN, "scale")
+
+
+def _compare(outs, d, case, variant, npls):
+    worst = 0.0
+    for o in sg.OUTPUTS:
+        for p in range(1, npls + 1):
+            err = outs.compare_files(os.path.join(d, "%s.%d" % (o, p)),
+                                     os.path.join(SCALE, case, "%s_%s.%d" % (variant, o, p)))
+            assert err <= FP64_TOL, (o, p, err)
+            worst = max(worst, err)
+    return worst
+
+
+def test_c1_full_transient_matches_reference(pkg, outs, tmp_path):
+    d = str(tmp_path / "c1")
+    sg.write_case_inputs("c1", d)
+    with pkg.Solver(d, "A", 2) as s:
+        s.run()
+        s.write_outputs()
+        info = s.info()
+    assert info["steps"] == 120 and info["factorizations"] == 6 and info["n_edges"] == 201720
+    _compare(outs, d, "c1", "A2", 1)
+
+
+@pytest.mark.parametrize("variant", ["A3", "E3"])
+def test_32_wires_as_one_block_match_reference(pkg, outs, tmp_path, variant):
+    d = str(tmp_path / "w")
+    sg.write_case_inputs("wires32", d)
+    with pkg.Solver(d, variant[0], int(variant[1])) as s:
+        s.run()
+        s.write_outputs()
+        assert s.info()["n_sources"] == 32
+    _compare(outs, d, "wires32", variant, 32)

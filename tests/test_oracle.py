@@ -9,6 +9,7 @@
 """
 import ctypes
 import os
+import sys
 import shutil
 
 import numpy as np
@@ -188,3 +189,19 @@ def test_three_point_formulas_exact_for_quadratics():
         for t in (tj2, tj1, tj, 0.5 * (tj1 + tj)):
             got = tdem_oracle._dA_dt(t, u(tj), u(tj1), u(tj2), dt, dt0, dt1, tj, tj1, tj2)
             assert abs(got - du(t)) <= 1e-9 * (1 + abs(du(t)))
+
+
+@pytest.mark.parametrize("variant", ["A3", "E3"])
+def test_numpy_oracle_matches_32_wire_golden(outs, tmp_path, variant):
+    """The restatement on the 32-wire block case of tests/golden/scale (12^3, 32
+    right-hand sides per step, made by the reference's own CalcNonstat3DLine)."""
+    sys.path.insert(0, GOLDEN)
+    import make_scale_golden as sg
+    d = str(tmp_path / "w")
+    sg.write_case_inputs("wires32", d)
+    tdem_oracle.run(d, variant[0], int(variant[1]))
+    for o in sg.OUTPUTS:
+        for p in range(1, 33):
+            err = outs.compare_files(os.path.join(d, "%s.%d" % (o, p)),
+                                     os.path.join(GOLDEN, "scale", "wires32", "%s_%s.%d" % (variant, o, p)))
+            assert err <= FP64_TOL, (o, p, err)
