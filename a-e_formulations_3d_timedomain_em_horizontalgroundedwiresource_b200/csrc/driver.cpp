@@ -362,11 +362,11 @@ int64_t TransientSolve::device_bytes_needed() const {
   if (!planned_ || !sy_) return 0;
   const int64_t nn = n_, np = npls_, nnz = (int64_t)col_.size(), nl = (int64_t)src_.size();
   // two factor slots are counted only when asked for (0 adds one only if free memory allows)
-  const int slots = (opt_.precision == 64 && opt_.factor_slots == 2) ? 2 : 1;
-  int64_t b = GpuCholesky::bytes_needed(*sy_, npls_, opt_.precision == 32 ? 4 : 8, slots);
+  const int slots = opt_.factor_slots == 2 ? 2 : 1;
+  int64_t b = GpuCholesky::bytes_needed(*sy_, npls_, opt_.precision == 32 ? 4 : 8, slots, factor_bytes());
   b += 8 * (nn + 1) + 4 * nnz + 16 * nnz + 8 * nl + nl + 8 * nl + nn;  // pattern, C, B, map, diag, values, bound
   b += 8 * nn * np * (ring_ + 4);                                       // S, history ring, rhs, x, u0
-  if (opt_.precision == 32) b += 8 * nnz + 8 * nn * np * 4;             // A and the CG vectors
+  if (opt_.precision == 32) b += 8 * nnz * slots + 8 * nn * np * 4;     // A per slot and the CG vectors
   b += 8 * (int64_t)(rop_b_.val.size() + rop_e_.val.size()) * 3;        // receiver operators (approx.)
   b += 8 * (int64_t)(tll_ - tlf_ + 1) * 3 * (rop_b_.nrec + rop_e_.nrec) + 8 * ntime_;
   b += (int64_t)m_.n_elem * (12 * 4 + 5 * 8 + 4);                       // assembly inputs
@@ -381,13 +381,13 @@ std::string TransientSolve::setup_device(cudaStream_t stream) {
   std::string e;
   chol_.reset(new GpuCholesky());
   if (opt_.fp32_update != 0) chol_->set_tensor_core_update(opt_.fp32_update == 2);
-  // a second factor slot only for FP64 (the mixed-precision run keeps its FP64
-  // system values in one buffer that both the factorization and the CG use)
-  int slots = opt_.precision == 32 ? 1 : opt_.factor_slots;
+  int slots = opt_.factor_slots;
   if (slots == 0) {
     size_t free_b = 0, total_b = 0;
     TRY_CUDA(cudaMemGetInfo(&free_b, &total_b));
-    const int64_t need = device_bytes_needed() + GpuCholesky::slot_bytes(*sy_, 8);  // one slot counted
+    // one slot counted: a second adds its factor (and the system values of mixed precision)
+    const int64_t need = device_bytes_needed() + GpuCholesky::slot_bytes(*sy_, opt_.precision == 32 ? 4 : 8) +
+                         (opt_.precision == 32 ? 8 * (int64_t)col_.size() : 0);
     slots = ((int64_t)free_b > need + (int64_t)(total_b / 20) + ((int64_t)2 << 30)) ? 2 : 1;
   }
   if (slots < 1 || slots > kMaxSlots) return "factor_slots must be 0, 1 or 2";
@@ -398,7 +398,7 @@ std::string TransientSolve::setup_device(cudaStream_t stream) {
     TRY_CUDA(cudaStreamCreateWithPriority(&hs_, cudaStreamNonBlocking, greatest));
     TRY_CUDA(cudaStreamCreateWithPriority(&fs_, cudaStreamNonBlocking, least));
   }
-  e = chol_->setup(std::move(*sy_), p2v_, npls_, s_, opt_.precision == 32 ? 4 : 8, slots);
+  e = chol_->setup(std::move(*sy_), p2v_, npls_, s_, opt_.precision == 32 ? 4 : 8, slots, factor_bytes());
   sy_.reset();
   if (!e.empty()) return e;
   if (const char* ps = std::getenv("TDEM_PANEL_SOLVE")) chol_->set_panel_solve(ps[0] == '1');
@@ -428,7 +428,8 @@ std::string TransientSolve::setup_device(cudaStream_t stream) {
   TRY_CUDA(cudaMemsetAsync(d_x_, 0, sizeof(double) * (size_t)n_ * npls_, s_));
   if (opt.precision == 32) {
     const size_t vb = sizeof(double) * (size_t)n_ * npls_;
-    if (!(e = alloc((void**)&d_A_, sizeof(double) * col_.size())).empty()) return e;
+    for (int k = 0; k < slots; ++k)
+      if (!(e = alloc((void**)&d_Aslot_[k], sizeof(double) * col_.size())).empty()) return e;
     for (double** v : {&d_r_, &d_z_, &d_p_, &d_q_})
       if (!(e = alloc((void**)v, vb)).empty()) return e;
     TRY_CUDA(cudaMemsetAsync(d_z_, 0, vb, s_));
@@ -520,7 +521,7 @@ std::string TransientSolve::setup_device(cudaStream_t stream) {
 std::string TransientSolve::factor_with(double mult, int slot, cudaStream_t s) {
   launch_combine(d_C_, d_B_, d_src_, d_diag_, (int64_t)chol_->symbolic().nnz_lower, mult, d_avals_, s);
   if (opt_.precision == 32) {
-    launch_combine_full(d_rowptr_, d_col_, d_C_, d_B_, d_bound_, n_, mult, d_A_, s);
+    launch_combine_full(d_rowptr_, d_col_, d_C_, d_B_, d_bound_, n_, mult, d_Aslot_[slot], s);
     ++launches_;
   }
   const std::string me = mark_device("Start factorization", s);
@@ -592,7 +593,7 @@ std::string TransientSolve::refine(double* x) {
   TRY_CUDA(cudaMemsetAsync(x, 0, vb, s_));
   TRY_CUDA(cudaMemcpyAsync(d_r_, d_rhs_, vb, cudaMemcpyDeviceToDevice, s_));
   launch_dots(d_rhs_, d_rhs_, n_, npls_, d_work_, d_bn_, s_);
-  std::string e = chol_->solve_graph(d_r_, d_z_, n_, npls_, s_);
+  std::string e = chol_->solve_graph(d_r_, d_z_, n_, npls_, s_, slot_);
   if (!e.empty()) return e;
   TRY_CUDA(cudaMemcpyAsync(d_p_, d_z_, vb, cudaMemcpyDeviceToDevice, s_));
   launch_dots(d_r_, d_z_, n_, npls_, d_work_, d_rz_, s_);
@@ -601,7 +602,7 @@ std::string TransientSolve::refine(double* x) {
   int it = 0;
   double worst = 0.0;
   for (it = 1; it <= opt_.refine_maxit; ++it) {
-    launch_spmv(d_rowptr_, d_col_, d_A_, d_p_, n_, npls_, d_q_, s_);
+    launch_spmv(d_rowptr_, d_col_, d_Aslot_[slot_], d_p_, n_, npls_, d_q_, s_);
     launch_dots(d_p_, d_q_, n_, npls_, d_work_, d_pq_, s_);
     launch_pcg_step(d_rz_, d_pq_, x, d_r_, d_p_, d_q_, n_, npls_, d_work_, d_rr_, s_);
     TRY_CUDA(cudaMemcpyAsync(rr.data(), d_rr_, sizeof(double) * npls_, cudaMemcpyDeviceToHost, s_));
@@ -615,7 +616,7 @@ std::string TransientSolve::refine(double* x) {
       done = done && rel <= opt_.refine_tol;
     }
     if (done) break;
-    e = chol_->solve_graph(d_r_, d_z_, n_, npls_, s_);
+    e = chol_->solve_graph(d_r_, d_z_, n_, npls_, s_, slot_);
     if (!e.empty()) return e;
     launch_dots(d_r_, d_z_, n_, npls_, d_work_, d_rzn_, s_);
     launch_pcg_dir(d_rz_, d_rzn_, d_z_, d_p_, n_, npls_, s_);

@@ -20,7 +20,9 @@ struct RunOptions {
   int formulation = 0;   // 0 = A (vector potential), 1 = E (electric field)
   int scheme = 2;        // 2 = two-point (backward Euler), 3 = three-point (BDF2)
   int leaf_size = 128;   // nested-dissection leaf size
-  int fp32_update = 0;   // precision 32 trailing updates: 0 default, 1 CUDA cores, 2 tensor cores
+  // precision 32, the factorization: 0 FP64 (factor held rounded to FP32), 1 FP32 with
+  // CUDA-core updates, 2 FP32 with tensor-core (tcgen05 3xTF32) updates
+  int fp32_update = 0;
   // 64: FP64 factor, one direct solve per step.  32: FP32 factor used as the
   // preconditioner of an FP64 conjugate-gradient solve on the FP64 system, run to
   // a relative residual of refine_tol in every column.
@@ -167,8 +169,10 @@ class TransientSolve {
   cudaEvent_t ev_[6] = {};
   double* d_rhs_ = nullptr;
   double* d_x_ = nullptr;      // solve output (fixed, so the solve can be replayed as a graph)
-  // mixed precision: FP64 system values and CG work vectors
-  double* d_A_ = nullptr;
+  // mixed precision: FP64 system values per factor slot (the CG of a decade reads
+  // its slot's while the next factorization writes the other) and CG work vectors
+  double* d_Aslot_[kMaxSlots] = {};
+  int factor_bytes() const { return (opt_.precision == 32 && opt_.fp32_update != 0) ? 4 : 8; }
   double *d_r_ = nullptr, *d_z_ = nullptr, *d_p_ = nullptr, *d_q_ = nullptr, *d_work_ = nullptr;
   double *d_rz_ = nullptr, *d_rzn_ = nullptr, *d_pq_ = nullptr, *d_rr_ = nullptr, *d_bn_ = nullptr;
   std::string refine(double* x);

@@ -1024,9 +1024,11 @@ __global__ void __launch_bounds__(256, 2) k_fwd_level(const T* __restrict__ L, c
     if (t == 0) wait_flag(flags + q, fa.err);
     __syncthreads();
     store_block(Ls, pre);
-    for (int e = t; e < SB * ysl; e += 256) {
-      const int c = e / ysl, r = e % ysl;
-      Ys[e] = (c < wq && r < nr_rhs) ? __ldcg(w + SB * q + c + (int64_t)r * m) : (T)0;
+    // the block's solution values, one right-hand side (64 contiguous values of
+    // W) per pair of warps: coalesced reads; columns up to the last MMA tile
+    for (int e = t; e < SB * 8 * ntl; e += 256) {
+      const int c = e & (SB - 1), r = e / SB;
+      Ys[c * ysl + r] = (c < wq && r < nr_rhs) ? __ldcg(w + SB * q + c + (int64_t)r * m) : (T)0;
     }
     __syncthreads();
     if (q + 1 < hi) load_block(pre, F, m, r0, nr, SB * (q + 1), min(SB, k - SB * (q + 1)));
@@ -1187,9 +1189,10 @@ __global__ void __launch_bounds__(256, 2) k_bwd_level(const T* __restrict__ L, c
     if (R < pb && t == 0) wait_flag(flags + R, fa.err);
     __syncthreads();
     store_block(Ls, pre);
-    for (int e = t; e < SB * ysl; e += 256) {
-      const int ii = e / ysl, r = e % ysl;
-      Ws[e] = (ii < nr && r < nr_rhs) ? __ldcg(w + r0 + ii + (int64_t)r * m) : (T)0;
+    // coalesced as in k_fwd_level
+    for (int e = t; e < SB * 8 * ntl; e += 256) {
+      const int ii = e & (SB - 1), r = e / SB;
+      Ws[ii * ysl + r] = (ii < nr && r < nr_rhs) ? __ldcg(w + r0 + ii + (int64_t)r * m) : (T)0;
     }
     __syncthreads();
     if (R - 1 >= lo) {
@@ -1776,6 +1779,18 @@ __global__ void __launch_bounds__(256) k_diag_inverse(const T* __restrict__ L, T
   } while (0)
 
 inline unsigned grid_of(int64_t ctas) { return (unsigned)ctas; }
+// dst[i] = (float)src[i], two elements per thread and iteration (16-byte loads
+// where the pair is aligned; n may be odd), grid-stride.
+__global__ void __launch_bounds__(256) k_round_to_float(const double* __restrict__ src, float* __restrict__ dst,
+                                                        int64_t n) {
+  const int64_t pairs = n / 2;
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < pairs; p += (int64_t)gridDim.x * blockDim.x) {
+    const double2 v = __ldcs(reinterpret_cast<const double2*>(src) + p);
+    __stcs(reinterpret_cast<float2*>(dst) + p, make_float2((float)v.x, (float)v.y));
+  }
+  if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) dst[n - 1] = (float)src[n - 1];
+}
+
 template <class T>
 constexpr size_t syrk_smem() { return sizeof(T) * 2 * kTileSyrk * (P + 1); }
 template <class T>
@@ -2064,10 +2079,13 @@ int64_t GpuCholesky::slot_bytes(const Symbolic& sy, int precision_bytes) {
   return el * (std::max<int64_t>(1, sy.nnz_l) + std::max<int64_t>(1, sy.dinv_elems));
 }
 
-int64_t GpuCholesky::bytes_needed(const Symbolic& sy, int nrhs_max, int precision_bytes, int nslots) {
+int64_t GpuCholesky::bytes_needed(const Symbolic& sy, int nrhs_max, int precision_bytes, int nslots,
+                                  int factor_bytes) {
   const int64_t el = (precision_bytes == 4) ? 4 : 8, nr = std::max(1, nrhs_max);
-  int64_t b = el * (sy.u_elems + sy.wvec_elems * nr + sy.solve_partials * nr + sy.solve_slots * kPanel * nr);
+  const int64_t fel = factor_bytes == 0 ? el : (factor_bytes == 4 ? 4 : 8);
+  int64_t b = fel * sy.u_elems + el * (sy.wvec_elems * nr + sy.solve_partials * nr + sy.solve_slots * kPanel * nr);
   b += std::max(1, std::min(nslots, kMaxSlots)) * slot_bytes(sy, precision_bytes);
+  if (fel != el) b += slot_bytes(sy, (int)fel);  // the FP64 work factor of a demoted setup
   b += 8 * (int64_t)(sy.l_off.size() + sy.u_off.size() + sy.wvec_off.size() + sy.entry_dst.size() +
                      sy.rel_off.size() + sy.rows_off.size() + sy.task_prefix.size() + sy.dinv_off.size());
   b += 4 * (int64_t)(sy.front_m.size() + sy.front_k.size() + sy.rel.size() + sy.rows_all.size() + sy.tasks.size() +
@@ -2077,10 +2095,12 @@ int64_t GpuCholesky::bytes_needed(const Symbolic& sy, int nrhs_max, int precisio
 }
 
 std::string GpuCholesky::setup(Symbolic&& sy, const std::vector<int>& perm_to_vec, int nrhs_max,
-                               cudaStream_t s, int precision_bytes, int nslots) {
+                               cudaStream_t s, int precision_bytes, int nslots, int factor_bytes) {
   sy_ = std::move(sy);
   nrhs_max_ = std::max(1, nrhs_max);
   elem_ = (precision_bytes == 4) ? 4 : 8;
+  fac_elem_ = factor_bytes == 0 ? elem_ : (factor_bytes == 4 ? 4 : 8);
+  if (fac_elem_ < elem_) return "the factorization cannot be less precise than the held factor";
   if ((int)perm_to_vec.size() != sy_.n) return "perm_to_vec size mismatch";
   if (nrhs_max_ > kMaxRhs) return "too many right-hand sides";
   if (nslots < 1 || nslots > kMaxSlots) return "factor slots must be 1 or 2";
@@ -2090,7 +2110,11 @@ std::string GpuCholesky::setup(Symbolic&& sy, const std::vector<int>& perm_to_ve
     if (!(e = alloc(&d_L_[k], elem_ * std::max<int64_t>(1, sy_.nnz_l))).empty()) return e;
     if (!(e = alloc(&d_dinv_[k], elem_ * std::max<int64_t>(1, sy_.dinv_elems))).empty()) return e;
   }
-  if (!(e = alloc(&d_U_, elem_ * std::max<int64_t>(1, sy_.u_elems))).empty()) return e;
+  if (demoted()) {
+    if (!(e = alloc(&d_Lw_, sizeof(double) * std::max<int64_t>(1, sy_.nnz_l))).empty()) return e;
+    if (!(e = alloc(&d_dinvw_, sizeof(double) * std::max<int64_t>(1, sy_.dinv_elems))).empty()) return e;
+  }
+  if (!(e = alloc(&d_U_, fac_elem_ * std::max<int64_t>(1, sy_.u_elems))).empty()) return e;
   if (!(e = alloc(&d_W_, elem_ * std::max<int64_t>(1, sy_.wvec_elems) * nrhs_max_)).empty()) return e;
   if (!(e = alloc(&d_part_, elem_ * std::max<int64_t>(1, sy_.solve_partials) * nrhs_max_)).empty()) return e;
   if (!(e = upload(&d_l_off_, sy_.l_off, s)).empty()) return e;
@@ -2120,8 +2144,9 @@ std::string GpuCholesky::setup(Symbolic&& sy, const std::vector<int>& perm_to_ve
     return e;
   if (!(e = alloc((void**)&d_err_, 3 * sizeof(int))).empty()) return e;
   TDEM_CUDA_TRY(cudaMemsetAsync(d_err_, 0, 3 * sizeof(int), s));
-  if (elem_ == 4 && tc_update_ && !(e = tc_update_setup()).empty()) return e;
+  if (fac_elem_ == 4 && tc_update_ && !(e = tc_update_setup()).empty()) return e;
   if (!(e = (elem_ == 4 ? set_attributes<float>() : set_attributes<double>())).empty()) return e;
+  if (demoted() && !(e = set_attributes<double>()).empty()) return e;
   if (!(e = (elem_ == 4 ? set_fused_attributes<float>() : set_fused_attributes<double>())).empty()) return e;
   if (!(e = (elem_ == 4 ? stream_residency<float>(resident_, sms_) : stream_residency<double>(resident_, sms_)))
            .empty())
@@ -2136,6 +2161,23 @@ void GpuCholesky::factor(const double* d_vals, cudaStream_t s, int slot) {
   const size_t ism = 2 * sizeof(double) * SB * (SB + 1);
   void* Lp = d_L_[slot];
   void* Dp = d_dinv_[slot];
+  if (demoted()) {
+    // FP64 factorization into the work factor, then both arrays rounded into the slot
+    launches_factor_ = launch_factor<double>(sy_, (double*)d_Lw_, (double*)d_U_, d_vals, d_entry_, fr, d_parent_,
+                                             d_rel_off_, d_rel_, d_tasks_, d_prefix_, d_err_, d_c0_, false, s);
+    if (ni) {
+      k_diag_inverse<double><<<ni, 256, ism, s>>>((const double*)d_Lw_, (double*)d_dinvw_, fr, d_dinv_off_,
+                                                  d_items_ + 2 * sy_.inv_off);
+      ++launches_factor_;
+    }
+    const int64_t nl = std::max<int64_t>(1, sy_.nnz_l), nd = std::max<int64_t>(1, sy_.dinv_elems);
+    k_round_to_float<<<(unsigned)std::min<int64_t>((nl / 2 + 255) / 256, 148 * 16), 256, 0, s>>>(
+        (const double*)d_Lw_, (float*)Lp, nl);
+    k_round_to_float<<<(unsigned)std::min<int64_t>((nd / 2 + 255) / 256, 148 * 16), 256, 0, s>>>(
+        (const double*)d_dinvw_, (float*)Dp, nd);
+    launches_factor_ += 2;
+    return;
+  }
   if (elem_ == 4) {
     launches_factor_ = launch_factor<float>(sy_, (float*)Lp, (float*)d_U_, d_vals, d_entry_, fr, d_parent_,
                                             d_rel_off_, d_rel_, d_tasks_, d_prefix_, d_err_, d_c0_, tc_update_, s);

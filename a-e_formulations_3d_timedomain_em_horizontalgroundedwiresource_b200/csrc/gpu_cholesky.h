@@ -31,13 +31,21 @@ class GpuCholesky {
   // permuted unknown p (lets the solve read and write the caller's natural-order
   // vectors directly).  nslots numeric factors (1 or 2) are held: with two, one
   // can be factored (on its own stream) while solves use the other.
+  // precision_bytes: element size of the held factors and of the solves (8 FP64,
+  // 4 FP32).  factor_bytes: arithmetic of the factorization (0 = precision_bytes).
+  // factor_bytes 8 with precision_bytes 4 factors in FP64 into one FP64 work
+  // factor and stores each slot's factor (and inverted diagonal blocks) rounded
+  // to FP32, for FP32 solves inside an FP64 refinement.
   std::string setup(Symbolic&& sy, const std::vector<int>& perm_to_vec, int nrhs_max,
-                    cudaStream_t stream, int precision_bytes = 8, int nslots = 1);
+                    cudaStream_t stream, int precision_bytes = 8, int nslots = 1, int factor_bytes = 0);
 
   // Device bytes setup() allocates for this analysis (factor, workspaces, plans).
-  static int64_t bytes_needed(const Symbolic& sy, int nrhs_max, int precision_bytes, int nslots = 1);
+  static int64_t bytes_needed(const Symbolic& sy, int nrhs_max, int precision_bytes, int nslots = 1,
+                              int factor_bytes = 0);
   // Device bytes of one numeric factor slot (factor entries + inverted diagonal blocks).
   static int64_t slot_bytes(const Symbolic& sy, int precision_bytes);
+  // True when the factorization runs in FP64 and the slots hold FP32 copies.
+  bool demoted() const { return fac_elem_ == 8 && elem_ == 4; }
   int slots() const { return nslots_; }
 
   // Numeric factorization into factor slot `slot`.  d_lower_vals holds the
@@ -85,7 +93,10 @@ class GpuCholesky {
   int nrhs_max_ = 0;
   size_t bytes_ = 0;
   int launches_factor_ = 0, launches_solve_ = 0;
-  int elem_ = 8;                 // bytes per factor entry (8 = FP64, 4 = FP32)
+  int elem_ = 8;                 // bytes per held factor entry and solve value (8 = FP64, 4 = FP32)
+  int fac_elem_ = 8;             // bytes per entry of the factorization's arithmetic
+  void* d_Lw_ = nullptr;         // FP64 work factor of a demoted setup (slots hold FP32 copies)
+  void* d_dinvw_ = nullptr;      // its inverted diagonal blocks
   int nslots_ = 1;
   bool panel_solve_ = false;
   bool tc_update_ = false;

@@ -390,6 +390,8 @@ def run_ours(args, world, rank, local):
         t_job = max_over_ranks(world, gpu_ms * 1e-3)
         value = world * units * per_run / t_job
         inf = solver.info()
+        fp64_results = solver.results() if (args.precision == 64 and args.config == "c2" and not args.no_mixed) \
+            else None
         solver.close()
 
         # e2e through the drop-in C-ABI path: files on the host -> device -> results on the host
@@ -497,9 +499,48 @@ def run_ours(args, world, rank, local):
             }
             if args.config == "c2" and not args.no_batched:
                 line["batched"] = batched_leg(args, pkg, base, form, scheme, local, value)
+            if fp64_results is not None:
+                line["mixed_vs_fp64"] = mixed_leg(args, pkg, wdir, form, scheme, local, value, fp64_results)
             print(json.dumps(line), flush=True)
     finally:
         shutil.rmtree(base, ignore_errors=True)
+
+
+def peak_rel_err(got, ref) -> float:
+    """Largest |got - ref| over time and components of a receiver, relative to the
+    peak of that receiver's reference transient, over all receivers and tables."""
+    import numpy as np
+    worst = 0.0
+    for a, b in zip(got, ref):
+        for i in range(b.shape[2]):
+            sc = np.abs(b[:, :, i]).max()
+            if sc > 0:
+                worst = max(worst, float(np.abs(a[:, :, i] - b[:, :, i]).max() / sc))
+    return worst
+
+
+def mixed_leg(args, pkg, wdir: str, form: str, scheme: int, device: int, fp64_value: float, fp64_results) -> dict:
+    """The same workload with precision 32: FP64 factorization held rounded to FP32,
+    FP32 triangular solves inside an FP64 conjugate gradient to a 1e-10 relative
+    residual per step.  Forward solves/s against the FP64 path of this run, and the
+    largest receiver deviation from the FP64 transients."""
+    with pkg.Solver(wdir, form, scheme, device=device, precision=32) as s:
+        s.run()  # warm-up
+        runs = []
+        for _ in range(max(1, args.batched_runs)):
+            s.run()
+            runs.append(s.info()["run_gpu_ms"])
+        inf = s.info()
+        got = s.results()
+    ms = sum(runs) / len(runs)
+    v = inf["n_sources"] / (ms * 1e-3)
+    return {"workload": "same model and scheme, precision 32 (FP64 factorization held in FP32, FP32 solves, "
+                        "FP64 CG to 1e-10 per step)",
+            "value": v, "unit": "forward solves/s", "vs_fp64": v / fp64_value, "ms_per_run": ms,
+            "max_rel_err_vs_fp64": peak_rel_err(got, fp64_results), "accept": 1e-5,
+            "cg_iterations": inf["refine_iters"], "cg_iterations_max_per_step": inf["refine_iters_max"],
+            "worst_relative_residual": inf["refine_worst"], "steps": inf["steps"],
+            "factor_gpu_ms_per_run": inf["factor_gpu_ms"], "solve_gpu_ms_per_run": inf["solve_gpu_ms"]}
 
 
 def batched_leg(args, pkg, base: str, form: str, scheme: int, device: int, single_value: float) -> dict:
@@ -783,14 +824,17 @@ def main():
     ap.add_argument("--c4-active", type=int, default=4, help="requests on the device at once (config c4)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the 32-wire block leg (config c2)")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the precision-32 leg (config c2)")
     ap.add_argument("--batched-runs", type=int, default=1, help="timed runs of the 32-wire block leg")
     ap.add_argument("--ref-samples", type=int, default=2,
                     help="reference arm: samples of the cut workload (at most --steps)")
     ap.add_argument("--no-ref-check", action="store_true",
                     help="reference arm: skip the full 40^3 solve that checks the extrapolation")
     ap.add_argument("--precision", type=int, default=64, choices=[64, 32],
-                    help="64: FP64 factor; 32: FP32 factor preconditioning FP64 CG")
-    ap.add_argument("--fp32-update", default="default", choices=["default", "cuda_cores", "tensor_cores"])
+                    help="64: FP64 factor and solves; 32: FP32 solves preconditioning an FP64 CG")
+    ap.add_argument("--fp32-update", default="default", choices=["default", "cuda_cores", "tensor_cores"],
+                    help="precision 32: default = FP64 factorization held in FP32; cuda_cores / tensor_cores = "
+                         "FP32 factorization")
     ap.add_argument("--factor-slots", type=int, default=0, choices=[0, 1, 2],
                     help="numeric factors held: 2 overlaps the next factorization with the steps, 0 = auto")
     ap.add_argument("--air-sigma", type=float, default=None,

@@ -154,15 +154,22 @@ typedef struct tdem_info {
 /* Options of tdem_solver_create_ex (zero-initialise, then set what differs). */
 typedef struct tdem_options {
   int precision;            /* 64 (default when 0): FP64 factorization, one direct solve per
-                               step.  32: FP32 factorization used as the preconditioner of an
-                               FP64 conjugate-gradient solve on the FP64 system */
+                               step.  32: the per-step triangular solves run in FP32 on an FP32
+                               factor, as the preconditioner of an FP64 conjugate-gradient
+                               solve on the FP64 system (residuals, history and receivers in
+                               FP64); the factor is the FP64 factorization rounded to FP32
+                               unless fp32_update asks for an FP32 factorization */
   double refine_tol;        /* relative residual to reach per step and column (default 1e-10) */
   int refine_maxit;         /* iteration cap; exceeding it is TDEM_ERR_NUMERIC (default 200) */
   int leaf_size;            /* nested-dissection leaf size (default 128) */
-  int fp32_update;          /* precision 32, rank-512 trailing updates of the factorization:
-                               0 = library default, 1 = CUDA cores (FP32 FMA),
-                               2 = tensor cores (tcgen05, 3xTF32 with FP32 accumulation) */
-  int factor_slots;         /* precision 64: numeric factors held on the device.  2 factors the
+  int fp32_update;          /* precision 32, the factorization: 0 = FP64 factorization (FP64
+                               tensor pipe), its factor held rounded to FP32; 1 = FP32
+                               factorization with FP32 FMA trailing updates; 2 = FP32
+                               factorization with tensor-core trailing updates (tcgen05, 3xTF32,
+                               FP32 accumulation).  1 and 2 break down (non-positive pivot) on
+                               systems whose condition number is beyond FP32, as the benchmark
+                               models' air (1e-8 S/m) makes them */
+  int factor_slots;         /* numeric factors held on the device.  2 factors the
                                next time-step size on a low-priority stream while the current
                                decade's steps run (same results, a second factor's memory);
                                1 factors between the decades; 0 (default) = 2 when free device
