@@ -77,6 +77,10 @@ class TdemInfo(ctypes.Structure):
         ("refine_iters_max", ctypes.c_int),
         ("refine_worst", ctypes.c_double),
         ("factor_slots", ctypes.c_int),
+        ("solve_schedule", ctypes.c_int),
+        ("solve_split", ctypes.c_int),
+        ("solve_candidates", ctypes.c_int),
+        ("solve_tuned_ms", ctypes.c_double),
     ]
 
     def as_dict(self) -> dict:

@@ -284,6 +284,12 @@ tdem_status tdem_solver_info(const tdem_solver* s, tdem_info* info) {
       info->nnz_factor = c.symbolic().nnz_l;
       info->factor_flops = c.symbolic().flops;
       info->device_bytes = (int64_t)c.device_bytes();
+      const tdem::SolveSchedule sc = c.schedule_for(m.npls);
+      info->solve_schedule = sc.kind;
+      info->solve_split = sc.split;
+      info->solve_tuned_ms = sc.ms;
+      for (const auto& t : c.tune_log())
+        if (t.first == m.npls) info->solve_candidates = (int)t.second.size();
     }
     return TDEM_OK;
   });

@@ -402,6 +402,7 @@ std::string TransientSolve::setup_device(cudaStream_t stream) {
   sy_.reset();
   if (!e.empty()) return e;
   if (const char* ps = std::getenv("TDEM_PANEL_SOLVE")) chol_->set_panel_solve(ps[0] == '1');
+  if (const char* at = std::getenv("TDEM_SOLVE_AUTOTUNE")) chol_->set_autotune(at[0] != '0');
   // with a factorization running beside the steps, the level solves keep one CTA
   // per SM so the factor kernels can share every SM
   if (slots > 1) chol_->set_solve_ctas_per_sm(1);

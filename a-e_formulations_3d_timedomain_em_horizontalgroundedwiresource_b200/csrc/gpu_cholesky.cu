@@ -2192,11 +2192,40 @@ void GpuCholesky::factor(const double* d_vals, cudaStream_t s, int slot) {
   if (ni) ++launches_factor_;
 }
 
+SolveSchedule GpuCholesky::schedule_for(int nrhs) const {
+  SolveSchedule d;
+  if (panel_solve_) {
+    d.kind = 1;
+    return d;
+  }
+  for (const auto& t : tuned_)
+    if (t.first == nrhs) return t.second;
+  return d;
+}
+
 void GpuCholesky::solve(const double* d_b, double* d_x, int64_t ld, int nrhs, cudaStream_t s, int slot) {
+  solve_with(schedule_for(nrhs), d_b, d_x, ld, nrhs, s, slot);
+}
+
+void GpuCholesky::solve_with(const SolveSchedule& sc, const double* d_b, double* d_x, int64_t ld, int nrhs,
+                             cudaStream_t s, int slot) {
+  if (sc.split > 1 && nrhs > 1) {
+    // column groups one after another (each its own complete solve)
+    const int per = (nrhs + sc.split - 1) / sc.split;
+    SolveSchedule one = sc;
+    one.split = 1;
+    int total = 0;
+    for (int c = 0; c < nrhs; c += per) {
+      solve_with(one, d_b + (int64_t)c * ld, d_x + (int64_t)c * ld, ld, std::min(per, nrhs - c), s, slot);
+      total += launches_solve_;
+    }
+    launches_solve_ = total;
+    return;
+  }
   SolveArgs a{d_l_off_, d_w_off_, d_m_, d_k_, d_rows_off_, d_rows_, nrhs, ld};
   const void* Lp = d_L_[slot];
   const void* Dp = d_dinv_[slot];
-  if (!panel_solve_) {
+  if (sc.kind == 0) {
     FusedArgs fa{d_units_, 0, nullptr, nullptr, nullptr, d_err_ + 1};
     int res[2][2];
     for (int j = 0; j < 2; ++j)
@@ -2220,9 +2249,70 @@ void GpuCholesky::solve(const double* d_b, double* d_x, int64_t ld, int nrhs, cu
                                            d_parent_, d_rel_off_, d_rel_, d_tasks_, d_prefix_, s);
 }
 
+// Times every candidate schedule for nrhs columns on the factor in `slot` (stream
+// s, CUDA events, the median of three solves after one warm-up each) with scratch
+// copies of zero right-hand sides, and keeps the fastest.  Run before the solve's
+// graph is captured, so the graph replays the chosen schedule.
+std::string GpuCholesky::tune_solve(int nrhs, int64_t ld, cudaStream_t s, int slot) {
+  std::vector<SolveSchedule> cand;
+  for (int kind = 0; kind < 2; ++kind)
+    for (int split : {1, 2, 4})
+      if (split == 1 || nrhs / split >= 2) {
+        SolveSchedule c;
+        c.kind = kind;
+        c.split = split;
+        cand.push_back(c);
+      }
+  double* tb = nullptr;
+  const size_t vb = sizeof(double) * (size_t)ld * nrhs;
+  TDEM_CUDA_TRY(cudaMallocAsync((void**)&tb, 2 * vb, s));
+  struct Free {
+    double* p;
+    cudaStream_t s;
+    ~Free() { cudaFreeAsync(p, s); }
+  } fr{tb, s};
+  TDEM_CUDA_TRY(cudaMemsetAsync(tb, 0, 2 * vb, s));
+  cudaEvent_t ev[2];
+  TDEM_CUDA_TRY(cudaEventCreate(&ev[0]));
+  TDEM_CUDA_TRY(cudaEventCreate(&ev[1]));
+  std::string err;
+  size_t best = 0;
+  for (size_t i = 0; i < cand.size() && err.empty(); ++i) {
+    solve_with(cand[i], tb, tb + (size_t)ld * nrhs, ld, nrhs, s, slot);  // warm-up
+    float t[3];
+    for (float& ti : t) {
+      cudaEventRecord(ev[0], s);
+      solve_with(cand[i], tb, tb + (size_t)ld * nrhs, ld, nrhs, s, slot);
+      cudaEventRecord(ev[1], s);
+      if (cudaEventSynchronize(ev[1]) != cudaSuccess || cudaEventElapsedTime(&ti, ev[0], ev[1]) != cudaSuccess) {
+        err = "CUDA: solve autotuner timing failed";
+        break;
+      }
+    }
+    std::sort(t, t + 3);
+    cand[i].ms = t[1];
+    if (cand[i].ms < cand[best].ms) best = i;
+  }
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+  if (!err.empty()) return err;
+  TDEM_CUDA_TRY(cudaGetLastError());
+  tuned_.emplace_back(nrhs, cand[best]);
+  tune_log_.emplace_back(nrhs, cand);
+  return "";
+}
+
 std::string GpuCholesky::solve_graph(const double* d_b, double* d_x, int64_t ld, int nrhs, cudaStream_t s,
                                      int slot) {
   SolveGraph& sg = graph_[slot];
+  if (autotune_ && !panel_solve_ && nrhs > 2) {
+    bool known = false;
+    for (const auto& t : tuned_) known = known || t.first == nrhs;
+    if (!known) {
+      const std::string e = tune_solve(nrhs, ld, s, slot);
+      if (!e.empty()) return e;
+    }
+  }
   if (!sg.exec || sg.b != d_b || sg.x != d_x || sg.ld != ld || sg.nrhs != nrhs) {
     if (sg.exec) {
       cudaGraphExecDestroy(sg.exec);

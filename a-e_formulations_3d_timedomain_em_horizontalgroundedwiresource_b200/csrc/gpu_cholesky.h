@@ -19,6 +19,15 @@ namespace tdem {
 constexpr int kMaxRhs = 64;    // right-hand sides per solve
 constexpr int kMaxSlots = 2;   // numeric factors held at once (one factored while the other solves)
 
+// How a solve of several right-hand sides is scheduled (chosen per column count by
+// the solve autotuner, GpuCholesky::tune_solve).
+struct SolveSchedule {
+  int kind = 0;   // 0: fused level solves (one launch per tree level and direction);
+                  // 1: panel solves (launches per 64-column panel and level)
+  int split = 1;  // the columns are solved in this many groups one after another
+  float ms = 0;   // measured device time of one solve with this schedule (0: not measured)
+};
+
 class GpuCholesky {
  public:
   GpuCholesky() = default;
@@ -76,8 +85,19 @@ class GpuCholesky {
   // CUDA cores (default).  Takes effect at setup().
   void set_tensor_core_update(bool on) { tc_update_ = on; }
   // Selects the per-panel solve (one launch per 64-column panel and level) instead
-  // of the fused level solves; both compute the same triangular solves.
+  // of the fused level solves; both compute the same triangular solves.  Turns the
+  // autotuner off.
   void set_panel_solve(bool on) { panel_solve_ = on; }
+  // Solve autotuner: the first graph-replayed solve of more than two right-hand
+  // sides times every candidate schedule (fused or panel solves, the columns in 1,
+  // 2 or 4 groups) on the factor at hand and keeps the fastest for that column
+  // count; later solves of that count use it.  Every schedule computes the same
+  // triangular solves (bitwise the same per column as the schedule solving the
+  // columns together, not across schedules).  On by default.
+  void set_autotune(bool on) { autotune_ = on; }
+  // The schedule used for nrhs columns (tuned or default) and the tuner's record.
+  SolveSchedule schedule_for(int nrhs) const;
+  const std::vector<std::pair<int, std::vector<SolveSchedule>>>& tune_log() const { return tune_log_; }
   // Caps the persistent level-solve kernels at this many CTAs per SM (0 = as many
   // as fit): with one, half of every SM stays free for a factorization running
   // beside the solves.  Takes effect for solves captured or launched afterwards.
@@ -93,6 +113,12 @@ class GpuCholesky {
   int nrhs_max_ = 0;
   size_t bytes_ = 0;
   int launches_factor_ = 0, launches_solve_ = 0;
+  bool autotune_ = true;
+  std::vector<std::pair<int, SolveSchedule>> tuned_;  // (column count, chosen schedule)
+  std::vector<std::pair<int, std::vector<SolveSchedule>>> tune_log_;  // every candidate measured
+  void solve_with(const SolveSchedule& sc, const double* d_b, double* d_x, int64_t ld, int nrhs, cudaStream_t s,
+                  int slot);
+  std::string tune_solve(int nrhs, int64_t ld, cudaStream_t s, int slot);
   int elem_ = 8;                 // bytes per held factor entry and solve value (8 = FP64, 4 = FP32)
   int fac_elem_ = 8;             // bytes per entry of the factorization's arithmetic
   void* d_Lw_ = nullptr;         // FP64 work factor of a demoted setup (slots hold FP32 copies)

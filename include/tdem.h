@@ -149,6 +149,12 @@ typedef struct tdem_info {
   double refine_worst;      /* largest final relative residual of any step / column */
   int factor_slots;         /* numeric factors held (2: factorizations overlapped the steps;
                                factor_gpu_ms and solve_gpu_ms then overlap in run_gpu_ms) */
+  int solve_schedule;       /* per-step solve of the n_sources columns: 0 fused level solves,
+                               1 panel solves (chosen by the solve autotuner for more than two
+                               columns, measured on the first step of the first run) */
+  int solve_split;          /* column groups that solve is split into */
+  int solve_candidates;     /* schedules the autotuner measured (0: not tuned) */
+  double solve_tuned_ms;    /* the chosen schedule's measured device time per solve */
 } tdem_info;
 
 /* Options of tdem_solver_create_ex (zero-initialise, then set what differs). */

@@ -53,3 +53,28 @@ def test_32_wires_as_one_block_match_reference(pkg, outs, tmp_path, variant):
         s.write_outputs()
         assert s.info()["n_sources"] == 32
     _compare(outs, d, "wires32", variant, 32)
+
+
+def test_solve_autotuner_measures_every_schedule(pkg, outs, tmp_path, monkeypatch):
+    """The 32-column step solve is tuned on the first step: six schedules (fused or
+    panel solves, the columns in 1, 2 or 4 groups) are timed and the fastest kept;
+    the transients stay within the FP64 tolerance of the reference whichever wins,
+    and with the tuner off (fused, one group) as well."""
+    d = str(tmp_path / "w")
+    sg.write_case_inputs("wires32", d)
+    with pkg.Solver(d, "A", 3) as s:
+        s.run()
+        s.write_outputs()
+        info = s.info()
+    assert info["solve_candidates"] == 6 and info["solve_tuned_ms"] > 0
+    assert info["solve_schedule"] in (0, 1) and info["solve_split"] in (1, 2, 4)
+    _compare(outs, d, "wires32", "A3", 32)
+    monkeypatch.setenv("TDEM_SOLVE_AUTOTUNE", "0")
+    d2 = str(tmp_path / "w2")
+    sg.write_case_inputs("wires32", d2)
+    with pkg.Solver(d2, "A", 3) as s:
+        s.run()
+        s.write_outputs()
+        info = s.info()
+    assert info["solve_candidates"] == 0 and info["solve_schedule"] == 0 and info["solve_split"] == 1
+    _compare(outs, d2, "wires32", "A3", 32)
