@@ -403,6 +403,14 @@ std::string TransientSolve::setup_device(cudaStream_t stream) {
   if (!e.empty()) return e;
   if (const char* ps = std::getenv("TDEM_PANEL_SOLVE")) chol_->set_panel_solve(ps[0] == '1');
   if (const char* at = std::getenv("TDEM_SOLVE_AUTOTUNE")) chol_->set_autotune(at[0] != '0');
+  if (const char* fs = std::getenv("TDEM_SOLVE_SCHEDULE")) {  // "kind,split": a fixed schedule
+    SolveSchedule sc;
+    if (std::sscanf(fs, "%d,%d", &sc.kind, &sc.split) == 2 && sc.kind >= 0 && sc.kind <= 2 && sc.split >= 1 &&
+        sc.split <= kMaxRhs)
+      chol_->force_schedule(sc);
+    else
+      return "TDEM_SOLVE_SCHEDULE must be \"kind,split\" with kind 0, 1 or 2";
+  }
   // with a factorization running beside the steps, the level solves keep one CTA
   // per SM so the factor kernels can share every SM
   if (slots > 1) chol_->set_solve_ctas_per_sm(1);

@@ -1730,6 +1730,409 @@ __global__ void __launch_bounds__(256, 2) k_bwd_stream(const T* __restrict__ L, 
   cp_async_wait_all();
 }
 
+// ---------------------------------------------------------------------------
+// Persistent level solves for many right-hand sides (FP64, 3..32 columns).
+//
+// The units and their meaning are those of k_fwd_level / k_bwd_level; the CTAs
+// are persistent (as many as fit, two per SM) and take units by ticket like the
+// streaming kernels.  A unit's 64 x 64 factor blocks and 64 x nrhs solution
+// blocks are copied into two shared-memory stages with cp.async, the next block
+// while the current one is multiplied on the FP64 tensor pipe (block_dmma).  A
+// unit whose inputs are all solved (every unit except a chain link caught before
+// its newest block is ready) waits once and prefetches solution blocks as well;
+// a chain link waits per block and reads that block's solution values directly.
+// Diagonal inverses of final pivot units are held in registers from the start.
+// Results are bitwise those of k_fwd_level / k_bwd_level (same products in the
+// same order).
+// ---------------------------------------------------------------------------
+constexpr int kMrStages = 2;
+constexpr int kMrYld = ys_ld(32);  // solution-block stage leading dimension (32 columns)
+constexpr size_t mr_smem() { return sizeof(double) * kMrStages * (SB * kLdL + SB * kMrYld); }
+
+// This thread's 16 elements (row t % 64, columns t / 64 + 4 e) of the 64 x 64 block
+// at rows [r0, r0 + nr), columns [c0, c0 + nc) of F into Ls[c][i] (zero outside).
+// Does not commit.
+__device__ __forceinline__ void cp_block_ls(double (*Ls)[kLdL], const double* __restrict__ F, int64_t ld, int r0,
+                                            int nr, int c0, int nc) {
+  const int t = threadIdx.x, i = t & 63, g = t >> 6;
+#pragma unroll
+  for (int e = 0; e < 16; ++e) {
+    const int c = g + 4 * e;
+    const bool ok = i < nr && c < nc;
+    cp_async_elem<8>(&Ls[c][i], ok ? F + (r0 + i) + (int64_t)(c0 + c) * ld : F, ok ? 8 : 0);
+  }
+}
+
+// rows [r0, r0 + nr) of the front vectors w (ld m), columns < nr_rhs, into
+// Vs[row * ysl + r] for columns up to 8 ntl (zero outside).  Does not commit.
+__device__ __forceinline__ void cp_vec_block(double* Vs, int ysl, const double* w, int64_t m, int r0, int nr,
+                                             int nr_rhs, int ntl) {
+  for (int e = threadIdx.x; e < SB * 8 * ntl; e += 256) {
+    const int c = e & (SB - 1), r = e / SB;
+    const bool ok = c < nr && r < nr_rhs;
+    cp_async_elem<8>(Vs + c * ysl + r, ok ? w + r0 + c + (int64_t)r * m : w, ok ? 8 : 0);
+  }
+}
+__device__ __forceinline__ void ld_vec_block(double* Vs, int ysl, const double* w, int64_t m, int r0, int nr,
+                                             int nr_rhs, int ntl) {
+  for (int e = threadIdx.x; e < SB * 8 * ntl; e += 256) {
+    const int c = e & (SB - 1), r = e / SB;
+    Vs[c * ysl + r] = (c < nr && r < nr_rhs) ? __ldcg(w + r0 + c + (int64_t)r * m) : 0.0;
+  }
+}
+
+template <int RPT>
+__global__ void __launch_bounds__(256, 2) k_fwd_mrhs(const double* __restrict__ L, const double* __restrict__ Dinv,
+                                                  double* W, double* part, int nr_rhs, FusedArgs fa) {
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  double(*Lst)[SB][kLdL] = reinterpret_cast<double(*)[SB][kLdL]>(sm_raw);
+  double* Yst = reinterpret_cast<double*>(sm_raw + sizeof(double) * kMrStages * SB * kLdL);
+  __shared__ int s_tk[2], s_ready;
+  constexpr int NTW = (RPT + 3) / 4;
+  const int ysl = ys_ld(nr_rhs), ntl = (nr_rhs + 7) / 8;
+  const int t = threadIdx.x, i = t & 63, g = t >> 6;
+  if (t == 0) s_tk[0] = atomicAdd(fa.ticket, 1);
+  __syncthreads();
+  for (int par = 0;; par ^= 1) {
+    const int tk = s_tk[par];
+    if (tk >= fa.count) break;
+    int next = 0;
+    if (t == 0) next = atomicAdd(fa.ticket, 1);
+    const Unit u = load_unit(fa.units, tk);
+    const int R = u.R, lo = u.lo, hi = u.hi, m = u.m, k = u.k;
+    const bool fin = u.fin != 0;
+    const int pb = (k + SB - 1) / SB;
+    const bool piv = R < pb;
+    const int r0 = piv ? SB * R : k + SB * (R - pb);
+    const int nr = min(SB, (piv ? k : m) - r0);
+    const double* F = L + u.l_off;
+    double* w = W + u.w_off * nr_rhs;
+    const int* flags = fa.flags + u.flag0;
+#pragma unroll
+    for (int j = 0; j < kMrStages; ++j) {
+      const int q = lo + j;
+      if (q < hi) cp_block_ls(Lst[j], F, m, r0, nr, SB * q, min(SB, k - SB * q));
+      cp_async_commit();
+    }
+    // final pivot unit: its inverted diagonal block and its own rows of W do not
+    // depend on this launch
+    double dpre[16], wrow[RPT];
+    if (fin && piv) {
+      const double* D = Dinv + u.dinv_off + (int64_t)R * SB * SB;
+#pragma unroll
+      for (int e = 0; e < 16; ++e) {
+        const int q = t + 256 * e, ii = q & 63, c = q >> 6;
+        dpre[e] = (ii < nr && c < nr) ? __ldg(D + ii + c * nr) : 0.0;
+      }
+#pragma unroll
+      for (int j = 0; j < RPT; ++j) {
+        const int r = g + 4 * j;
+        wrow[j] = (r < nr_rhs && i < nr) ? __ldcg(w + r0 + i + (int64_t)r * m) : 0.0;
+      }
+    }
+    double* my_part = part + (int64_t)u.slot * SB * nr_rhs;
+    double tot[RPT];
+#pragma unroll
+    for (int j = 0; j < RPT; ++j) tot[j] = 0.0;
+    if (fin) gather_partials<double, RPT>(my_part, u.nparts, nr_rhs, fa.counters + u.cnt, fa.err, tot);
+    // flags of a front are set in chain order: the newest flag of the range stands
+    // for all of them (see k_fwd_stream)
+    const bool chain = fin && piv;
+    if (t == 0) {
+      int ready = 1;
+      if (lo < hi) {
+        if (!chain) wait_flag_backoff(flags + hi - 1, fa.err, 1024);
+        else ready = ld_acquire(flags + hi - 1) != 0;
+      }
+      s_ready = ready;
+    }
+    __syncthreads();
+    const bool staged = s_ready != 0;
+    if (staged) {
+#pragma unroll
+      for (int j = 0; j < kMrStages; ++j) {
+        const int q = lo + j;
+        if (q < hi) cp_vec_block(Yst + j * SB * kMrYld, ysl, w, m, SB * q, min(SB, k - SB * q), nr_rhs, ntl);
+        cp_async_commit();
+      }
+    }
+    double macc[NTW][4];
+#pragma unroll
+    for (int j = 0; j < NTW; ++j)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) macc[j][e] = 0.0;
+    for (int q = lo; q < hi; ++q) {
+      const int st = (q - lo) % kMrStages;
+      double* Ys = Yst + st * SB * kMrYld;
+      if (!staged) {
+        if (t == 0) wait_flag(flags + q, fa.err);
+        __syncthreads();
+        ld_vec_block(Ys, ysl, w, m, SB * q, min(SB, k - SB * q), nr_rhs, ntl);
+      }
+      cp_async_wait<1>();
+      __syncthreads();
+      block_dmma<false, NTW>(macc, Lst[st], Ys, ysl, ntl);
+      __syncthreads();
+      const int qn = q + kMrStages;
+      if (qn < hi) {
+        cp_block_ls(Lst[st], F, m, r0, nr, SB * qn, min(SB, k - SB * qn));
+        if (staged) cp_vec_block(Ys, ysl, w, m, SB * qn, min(SB, k - SB * qn), nr_rhs, ntl);
+      }
+      cp_async_commit();
+    }
+    cp_async_wait_all();
+    // the tensor-pipe sums to the thread layout through stage 0
+    double* Acc = &Lst[0][0][0];
+    __syncthreads();
+    store_acc<NTW>(macc, Acc, kLdL, ntl);
+    __syncthreads();
+    double acc[RPT];
+#pragma unroll
+    for (int j = 0; j < RPT; ++j) {
+      const int r = g + 4 * j;
+      acc[j] = (r < nr_rhs) ? Acc[i * kLdL + r] : 0.0;
+    }
+    if (!fin) {
+#pragma unroll
+      for (int j = 0; j < RPT; ++j) {
+        const int r = g + 4 * j;
+        if (r < nr_rhs) my_part[i + SB * r] = acc[j];
+      }
+    } else if (!piv) {
+      if (i < nr) {
+#pragma unroll
+        for (int j = 0; j < RPT; ++j) {
+          const int r = g + 4 * j;
+          if (r < nr_rhs) w[r0 + i + (int64_t)r * m] -= tot[j] + acc[j];
+        }
+      }
+    } else {
+      // y_R = Dinv_R (w_R - sum): z through stage 0 of the vectors, Dinv through stage 1
+      double* Zs = Yst;
+      double(*Ds)[kLdL] = Lst[1];
+      __syncthreads();
+#pragma unroll
+      for (int j = 0; j < RPT; ++j) {
+        const int r = g + 4 * j;
+        if (r < nr_rhs) Zs[i * ysl + r] = (i < nr) ? wrow[j] - (tot[j] + acc[j]) : 0.0;
+      }
+#pragma unroll
+      for (int e = 0; e < 16; ++e) {
+        const int q = t + 256 * e;
+        Ds[q >> 6][q & 63] = dpre[e];
+      }
+      __syncthreads();
+      double y[RPT];
+#pragma unroll
+      for (int j = 0; j < RPT; ++j) y[j] = 0.0;
+#pragma unroll 8
+      for (int c = 0; c < SB; ++c) {
+        const double l = Ds[c][i];
+#pragma unroll
+        for (int j = 0; j < RPT; ++j) {
+          const int r = g + 4 * j;
+          if (r < nr_rhs) y[j] = fma(l, Zs[c * ysl + r], y[j]);
+        }
+      }
+      if (i < nr) {
+#pragma unroll
+        for (int j = 0; j < RPT; ++j) {
+          const int r = g + 4 * j;
+          if (r < nr_rhs) w[r0 + i + (int64_t)r * m] = y[j];
+        }
+      }
+    }
+    const bool publish = !fin || piv;
+    if (t == 0) s_tk[par ^ 1] = next;
+    __syncthreads();
+    if (t == 0 && publish) {
+      if (fin) publish_flag(fa.flags + u.flag0 + R);
+      else publish_add(fa.counters + u.cnt);
+    }
+  }
+  cp_async_wait_all();
+}
+
+template <int RPT>
+__global__ void __launch_bounds__(256, 2) k_bwd_mrhs(const double* __restrict__ L, const double* __restrict__ Dinv,
+                                                  double* W, double* part, double* __restrict__ x,
+                                                  const int* __restrict__ rows, int64_t ldx, int nr_rhs,
+                                                  FusedArgs fa) {
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  double(*Lst)[SB][kLdL] = reinterpret_cast<double(*)[SB][kLdL]>(sm_raw);
+  double* Wst = reinterpret_cast<double*>(sm_raw + sizeof(double) * kMrStages * SB * kLdL);
+  __shared__ int s_tk[2], s_ready;
+  constexpr int NTW = (RPT + 3) / 4;
+  const int ysl = ys_ld(nr_rhs), ntl = (nr_rhs + 7) / 8;
+  const int t = threadIdx.x, c = t & 63, g = t >> 6;
+  if (t == 0) s_tk[0] = atomicAdd(fa.ticket, 1);
+  __syncthreads();
+  for (int par = 0;; par ^= 1) {
+    const int tk = s_tk[par];
+    if (tk >= fa.count) break;
+    int next = 0;
+    if (t == 0) next = atomicAdd(fa.ticket, 1);
+    const Unit u = load_unit(fa.units, tk);
+    const int p = u.R, lo = u.lo, hi = u.hi, m = u.m, k = u.k;
+    const bool fin = u.fin != 0;
+    const int pb = (k + SB - 1) / SB;
+    const int c0 = SB * p, wc = min(SB, k - c0);
+    const double* F = L + u.l_off;
+    double* w = W + u.w_off * nr_rhs;
+    const int* flags = fa.flags + u.flag0;
+    auto rows_of = [&](int Rr, int& rr0, int& nrr) {
+      rr0 = (Rr < pb) ? SB * Rr : k + SB * (Rr - pb);
+      nrr = min(SB, (Rr < pb ? k : m) - rr0);
+    };
+    // row blocks from the farthest (hi - 1) down to lo
+#pragma unroll
+    for (int j = 0; j < kMrStages; ++j) {
+      const int Rr = hi - 1 - j;
+      if (Rr >= lo) {
+        int rr0, nrr;
+        rows_of(Rr, rr0, nrr);
+        cp_block_ls(Lst[j], F, m, rr0, nrr, c0, wc);
+      }
+      cp_async_commit();
+    }
+    double dpre[16], wrow[RPT];
+    if (fin) {
+      const double* D = Dinv + u.dinv_off + (int64_t)p * SB * SB;
+#pragma unroll
+      for (int e = 0; e < 16; ++e) {
+        const int q = t + 256 * e, ii = q & 63, cc = q >> 6;
+        dpre[e] = (ii < wc && cc < wc) ? __ldg(D + ii + cc * wc) : 0.0;
+      }
+#pragma unroll
+      for (int j = 0; j < RPT; ++j) {
+        const int r = g + 4 * j;
+        wrow[j] = (r < nr_rhs && c < wc) ? __ldcg(w + c0 + c + (int64_t)r * m) : 0.0;
+      }
+    }
+    double* my_part = part + (int64_t)u.slot * SB * nr_rhs;
+    double tot[RPT];
+#pragma unroll
+    for (int j = 0; j < RPT; ++j) tot[j] = 0.0;
+    if (fin) gather_partials<double, RPT>(my_part, u.nparts, nr_rhs, fa.counters + u.cnt, fa.err, tot);
+    // flags are set last column first: flag lo stands for every pivot row block of
+    // the range (see k_bwd_stream); update rows need no flag
+    if (t == 0) {
+      int ready = 1;
+      if (lo < hi && lo < pb) {
+        if (!fin) wait_flag_backoff(flags + lo, fa.err, 1024);
+        else ready = ld_acquire(flags + lo) != 0;
+      }
+      s_ready = ready;
+    }
+    __syncthreads();
+    const bool staged = s_ready != 0;
+    // a row block's x values may be prefetched when staged or when it is an update row
+    auto prefetchable = [&](int Rr) { return staged || Rr >= pb; };
+#pragma unroll
+    for (int j = 0; j < kMrStages; ++j) {
+      const int Rr = hi - 1 - j;
+      if (Rr >= lo && prefetchable(Rr)) {
+        int rr0, nrr;
+        rows_of(Rr, rr0, nrr);
+        cp_vec_block(Wst + j * SB * kMrYld, ysl, w, m, rr0, nrr, nr_rhs, ntl);
+      }
+      cp_async_commit();
+    }
+    double macc[NTW][4];
+#pragma unroll
+    for (int j = 0; j < NTW; ++j)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) macc[j][e] = 0.0;
+    for (int Rr = hi - 1; Rr >= lo; --Rr) {
+      const int st = (hi - 1 - Rr) % kMrStages;
+      double* Ws = Wst + st * SB * kMrYld;
+      if (!prefetchable(Rr)) {
+        if (t == 0) wait_flag(flags + Rr, fa.err);
+        __syncthreads();
+        int rr0, nrr;
+        rows_of(Rr, rr0, nrr);
+        ld_vec_block(Ws, ysl, w, m, rr0, nrr, nr_rhs, ntl);
+      }
+      cp_async_wait<1>();
+      __syncthreads();
+      block_dmma<true, NTW>(macc, Lst[st], Ws, ysl, ntl);
+      __syncthreads();
+      const int Rn = Rr - kMrStages;
+      if (Rn >= lo) {
+        int rn0, nrn;
+        rows_of(Rn, rn0, nrn);
+        cp_block_ls(Lst[st], F, m, rn0, nrn, c0, wc);
+        if (prefetchable(Rn)) cp_vec_block(Ws, ysl, w, m, rn0, nrn, nr_rhs, ntl);
+      }
+      cp_async_commit();
+    }
+    cp_async_wait_all();
+    double* Acc = &Lst[0][0][0];
+    __syncthreads();
+    store_acc<NTW>(macc, Acc, kLdL, ntl);
+    __syncthreads();
+    double acc[RPT];
+#pragma unroll
+    for (int j = 0; j < RPT; ++j) {
+      const int r = g + 4 * j;
+      acc[j] = (r < nr_rhs) ? Acc[c * kLdL + r] : 0.0;
+    }
+    if (!fin) {
+#pragma unroll
+      for (int j = 0; j < RPT; ++j) {
+        const int r = g + 4 * j;
+        if (r < nr_rhs) my_part[c + SB * r] = acc[j];
+      }
+    } else {
+      // x_p = Dinv_p^T (y_p - sum): z through stage 0 of the vectors, Dinv through stage 1
+      double* Zs = Wst;
+      double(*Ds)[kLdL] = Lst[1];
+      __syncthreads();
+#pragma unroll
+      for (int j = 0; j < RPT; ++j) {
+        const int r = g + 4 * j;
+        if (r < nr_rhs) Zs[c * ysl + r] = (c < wc) ? wrow[j] - (tot[j] + acc[j]) : 0.0;
+      }
+#pragma unroll
+      for (int e = 0; e < 16; ++e) {
+        const int q = t + 256 * e;
+        Ds[q >> 6][q & 63] = dpre[e];
+      }
+      __syncthreads();
+      double xv[RPT];
+#pragma unroll
+      for (int j = 0; j < RPT; ++j) xv[j] = 0.0;
+#pragma unroll 8
+      for (int ii = 0; ii < SB; ++ii) {
+        const double l = Ds[c][ii];
+#pragma unroll
+        for (int j = 0; j < RPT; ++j) {
+          const int r = g + 4 * j;
+          if (r < nr_rhs) xv[j] = fma(l, Zs[ii * ysl + r], xv[j]);
+        }
+      }
+      if (c < wc) {
+        const int pos = rows[u.w_off + c0 + c];
+#pragma unroll
+        for (int j = 0; j < RPT; ++j) {
+          const int r = g + 4 * j;
+          if (r < nr_rhs) {
+            w[c0 + c + (int64_t)r * m] = xv[j];
+            x[pos + (int64_t)r * ldx] = xv[j];
+          }
+        }
+      }
+    }
+    if (t == 0) s_tk[par ^ 1] = next;
+    __syncthreads();
+    if (t == 0) {
+      if (fin) publish_flag(fa.flags + u.flag0 + p);
+      else publish_add(fa.counters + u.cnt);
+    }
+  }
+  cp_async_wait_all();
+}
+
 // Inverse of the lower-triangular diagonal block p of front s (w x w, w <= 64),
 // stored column-major with leading dimension w at dinv_off[s] + 64 * 64 * p.
 // Computed in FP64: four threads per column j run the substitution
@@ -1923,21 +2326,24 @@ int launch_solve(const Symbolic& sy, const T* L, T* W, T* part, const double* b,
 
 // One forward and one backward launch per level (plus the front-vector set-up).
 // STREAM: the persistent streaming kernels (nrhs <= NR <= 4, grid = resident
-// CTAs); otherwise the one-unit-per-CTA kernels with RPT right-hand sides per thread.
-template <class T, int RPT, bool STREAM>
+// CTAs); MR: the persistent many-column kernels (FP64, 3..32 columns, grid =
+// resident CTAs); otherwise the one-unit-per-CTA kernels with RPT right-hand
+// sides per thread.
+template <class T, int RPT, bool STREAM, bool MR = false>
 void launch_level_solves(const Symbolic& sy, const T* L, const T* Dinv, T* W, T* part, const double* b, double* x,
                          SolveArgs a, const int* parent, const int64_t* rel_off, const int* rel, const int* tasks,
                          const int64_t* prefix, FusedArgs fa, int* sync, const int (&resident)[2], int& launches,
                          cudaStream_t s) {
+  static_assert(!MR || std::is_same<T, double>::value, "the many-column persistent kernels are FP64");
   const int nlev = (int)sy.levels.size();
   int* tickets = sync;
   int* fflags = sync + 2 * nlev;
   int* bflags = fflags + sy.n_flags;
   fa.counters = bflags + sy.n_flags;
   cudaMemsetAsync(sync, 0, sizeof(int) * (2 * nlev + 2 * sy.n_flags + sy.n_counters), s);
-  const size_t ysm = STREAM ? stream_smem<T>() : sizeof(T) * SB * ys_ld(a.nrhs);
+  const size_t ysm = STREAM ? stream_smem<T>() : (MR ? mr_smem() : sizeof(T) * SB * ys_ld(a.nrhs));
   auto grid = [&](int64_t count, int dir) {
-    return STREAM ? (unsigned)std::min<int64_t>(count, resident[dir]) : grid_of(count);
+    return (STREAM || MR) ? (unsigned)std::min<int64_t>(count, resident[dir]) : grid_of(count);
   };
   for (int l = 0; l < nlev; ++l) {
     const LevelPlan& lp = sy.levels[l];
@@ -1956,7 +2362,9 @@ void launch_level_solves(const Symbolic& sy, const T* L, const T* Dinv, T* W, T*
     f.count = lp.fwd_count;
     f.ticket = tickets + 2 * l;
     f.flags = fflags;
-    if constexpr (STREAM)
+    if constexpr (MR)
+      k_fwd_mrhs<RPT><<<grid(lp.fwd_count, 0), 256, ysm, s>>>(L, Dinv, W, part, a.nrhs, f);
+    else if constexpr (STREAM)
       k_fwd_stream<T, RPT><<<grid(lp.fwd_count, 0), 256, ysm, s>>>(L, Dinv, W, part, a.nrhs, f);
     else
       k_fwd_level<T, RPT><<<grid(lp.fwd_count, 0), 256, ysm, s>>>(L, Dinv, W, part, a.nrhs, f);
@@ -1973,7 +2381,9 @@ void launch_level_solves(const Symbolic& sy, const T* L, const T* Dinv, T* W, T*
     f.count = lp.bwd_count;
     f.ticket = tickets + 2 * l + 1;
     f.flags = bflags;
-    if constexpr (STREAM)
+    if constexpr (MR)
+      k_bwd_mrhs<RPT><<<grid(lp.bwd_count, 1), 256, ysm, s>>>(L, Dinv, W, part, x, a.rows, a.ld, a.nrhs, f);
+    else if constexpr (STREAM)
       k_bwd_stream<T, RPT><<<grid(lp.bwd_count, 1), 256, ysm, s>>>(L, Dinv, W, part, x, a.rows, a.ld, a.nrhs, f);
     else
       k_bwd_level<T, RPT><<<grid(lp.bwd_count, 1), 256, ysm, s>>>(L, Dinv, W, part, x, a.rows, a.ld, a.nrhs, f);
@@ -2005,6 +2415,50 @@ int launch_solve_fused(const Symbolic& sy, const T* L, const T* Dinv, T* W, T* p
     TDEM_LEVELS(16, false, resident[0]);
 #undef TDEM_LEVELS
   return launches;
+}
+
+// The persistent many-column level solves (FP64, 3 <= nrhs <= 32).
+int launch_solve_mr(const Symbolic& sy, const double* L, const double* Dinv, double* W, double* part, const double* b,
+                    double* x, SolveArgs a, const int* parent, const int64_t* rel_off, const int* rel,
+                    const int* tasks, const int64_t* prefix, FusedArgs fa, int* sync, const int (&resident)[2],
+                    cudaStream_t s) {
+  int launches = 0;
+#define TDEM_MR(R) \
+  launch_level_solves<double, R, false, true>(sy, L, Dinv, W, part, b, x, a, parent, rel_off, rel, tasks, prefix, \
+                                              fa, sync, resident, launches, s)
+  if (a.nrhs <= 4)
+    TDEM_MR(1);
+  else if (a.nrhs <= 8)
+    TDEM_MR(2);
+  else if (a.nrhs <= 16)
+    TDEM_MR(4);
+  else
+    TDEM_MR(8);
+#undef TDEM_MR
+  return launches;
+}
+
+// Resident CTAs of the persistent many-column kernels ([forward, backward]).
+std::string mr_residency(int (&resident)[2], int sms) {
+  const int sm = (int)mr_smem();
+  int occ[2][4] = {};
+#define TDEM_OCC(J, R)                                                                                              \
+  TDEM_CUDA_TRY(cudaFuncSetAttribute(k_fwd_mrhs<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));             \
+  TDEM_CUDA_TRY(cudaFuncSetAttribute(k_bwd_mrhs<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));             \
+  TDEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[0][J], k_fwd_mrhs<R>, 256, sm));                \
+  TDEM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1][J], k_bwd_mrhs<R>, 256, sm));
+  TDEM_OCC(0, 1)
+  TDEM_OCC(1, 2)
+  TDEM_OCC(2, 4)
+  TDEM_OCC(3, 8)
+#undef TDEM_OCC
+  for (int d = 0; d < 2; ++d) {
+    int least = occ[d][0];
+    for (int j = 1; j < 4; ++j) least = std::min(least, occ[d][j]);
+    if (least < 1) return "many-column level solve does not fit on an SM";
+    resident[d] = least * sms;
+  }
+  return "";
 }
 
 // Resident CTAs on the device of each streaming kernel ([NR = 1, 2][forward, backward]).
@@ -2151,6 +2605,7 @@ std::string GpuCholesky::setup(Symbolic&& sy, const std::vector<int>& perm_to_ve
   if (!(e = (elem_ == 4 ? stream_residency<float>(resident_, sms_) : stream_residency<double>(resident_, sms_)))
            .empty())
     return e;
+  if (elem_ == 8 && !(e = mr_residency(resident_mr_, sms_)).empty()) return e;
   TDEM_CUDA_TRY(cudaStreamSynchronize(s));
   return "";
 }
@@ -2198,6 +2653,7 @@ SolveSchedule GpuCholesky::schedule_for(int nrhs) const {
     d.kind = 1;
     return d;
   }
+  if (has_forced_ && nrhs > 2) return forced_;
   for (const auto& t : tuned_)
     if (t.first == nrhs) return t.second;
   return d;
@@ -2225,7 +2681,17 @@ void GpuCholesky::solve_with(const SolveSchedule& sc, const double* d_b, double*
   SolveArgs a{d_l_off_, d_w_off_, d_m_, d_k_, d_rows_off_, d_rows_, nrhs, ld};
   const void* Lp = d_L_[slot];
   const void* Dp = d_dinv_[slot];
-  if (sc.kind == 0) {
+  if (sc.kind == 2 && elem_ == 8 && nrhs > 2 && nrhs <= 32) {
+    FusedArgs fa{d_units_, 0, nullptr, nullptr, nullptr, d_err_ + 1};
+    int res[2];
+    for (int d = 0; d < 2; ++d)
+      res[d] = solve_ctas_cap_ > 0 ? std::min(resident_mr_[d], solve_ctas_cap_ * sms_) : resident_mr_[d];
+    launches_solve_ = launch_solve_mr(sy_, (const double*)Lp, (const double*)Dp, (double*)d_W_, (double*)d_spart_,
+                                      d_b, d_x, a, d_parent_, d_rel_off_, d_rel_, d_tasks_, d_prefix_, fa, d_sync_,
+                                      res, s);
+    return;
+  }
+  if (sc.kind != 1) {
     FusedArgs fa{d_units_, 0, nullptr, nullptr, nullptr, d_err_ + 1};
     int res[2][2];
     for (int j = 0; j < 2; ++j)
@@ -2255,9 +2721,10 @@ void GpuCholesky::solve_with(const SolveSchedule& sc, const double* d_b, double*
 // graph is captured, so the graph replays the chosen schedule.
 std::string GpuCholesky::tune_solve(int nrhs, int64_t ld, cudaStream_t s, int slot) {
   std::vector<SolveSchedule> cand;
-  for (int kind = 0; kind < 2; ++kind)
+  for (int kind = 0; kind < 3; ++kind)
     for (int split : {1, 2, 4})
-      if (split == 1 || nrhs / split >= 2) {
+      if ((split == 1 || nrhs / split >= 2) &&
+          (kind != 2 || (elem_ == 8 && (nrhs + split - 1) / split > 2 && (nrhs + split - 1) / split <= 32))) {
         SolveSchedule c;
         c.kind = kind;
         c.split = split;
@@ -2305,7 +2772,7 @@ std::string GpuCholesky::tune_solve(int nrhs, int64_t ld, cudaStream_t s, int sl
 std::string GpuCholesky::solve_graph(const double* d_b, double* d_x, int64_t ld, int nrhs, cudaStream_t s,
                                      int slot) {
   SolveGraph& sg = graph_[slot];
-  if (autotune_ && !panel_solve_ && nrhs > 2) {
+  if (autotune_ && !panel_solve_ && !has_forced_ && nrhs > 2) {
     bool known = false;
     for (const auto& t : tuned_) known = known || t.first == nrhs;
     if (!known) {

@@ -22,8 +22,11 @@ constexpr int kMaxSlots = 2;   // numeric factors held at once (one factored whi
 // How a solve of several right-hand sides is scheduled (chosen per column count by
 // the solve autotuner, GpuCholesky::tune_solve).
 struct SolveSchedule {
-  int kind = 0;   // 0: fused level solves (one launch per tree level and direction);
-                  // 1: panel solves (launches per 64-column panel and level)
+  int kind = 0;   // 0: fused level solves (one launch per tree level and direction,
+                  //    one unit per CTA); 1: panel solves (launches per 64-column panel
+                  //    and level); 2: persistent fused level solves (FP64, 3..32
+                  //    columns per group: CTAs stay resident and stream their units'
+                  //    blocks through shared-memory stages)
   int split = 1;  // the columns are solved in this many groups one after another
   float ms = 0;   // measured device time of one solve with this schedule (0: not measured)
 };
@@ -89,12 +92,14 @@ class GpuCholesky {
   // autotuner off.
   void set_panel_solve(bool on) { panel_solve_ = on; }
   // Solve autotuner: the first graph-replayed solve of more than two right-hand
-  // sides times every candidate schedule (fused or panel solves, the columns in 1,
-  // 2 or 4 groups) on the factor at hand and keeps the fastest for that column
+  // sides times every candidate schedule (fused, panel or persistent fused solves,
+  // the columns in 1, 2 or 4 groups) on the factor at hand and keeps the fastest for that column
   // count; later solves of that count use it.  Every schedule computes the same
   // triangular solves (bitwise the same per column as the schedule solving the
   // columns together, not across schedules).  On by default.
   void set_autotune(bool on) { autotune_ = on; }
+  // Uses this schedule for every solve of more than two columns (no tuning).
+  void force_schedule(const SolveSchedule& sc) { forced_ = sc; has_forced_ = true; }
   // The schedule used for nrhs columns (tuned or default) and the tuner's record.
   SolveSchedule schedule_for(int nrhs) const;
   const std::vector<std::pair<int, std::vector<SolveSchedule>>>& tune_log() const { return tune_log_; }
@@ -114,6 +119,8 @@ class GpuCholesky {
   size_t bytes_ = 0;
   int launches_factor_ = 0, launches_solve_ = 0;
   bool autotune_ = true;
+  bool has_forced_ = false;
+  SolveSchedule forced_;
   std::vector<std::pair<int, SolveSchedule>> tuned_;  // (column count, chosen schedule)
   std::vector<std::pair<int, std::vector<SolveSchedule>>> tune_log_;  // every candidate measured
   void solve_with(const SolveSchedule& sc, const double* d_b, double* d_x, int64_t ld, int nrhs, cudaStream_t s,
@@ -127,6 +134,7 @@ class GpuCholesky {
   bool panel_solve_ = false;
   bool tc_update_ = false;
   int resident_[2][2] = {};      // resident CTAs of the streaming level solves [NR 1, 2][fwd, bwd]
+  int resident_mr_[2] = {};      // resident CTAs of the persistent many-column level solves [fwd, bwd]
   int sms_ = 0;                  // SMs of the device
   int solve_ctas_cap_ = 0;       // CTAs per SM of the level solves (0 = occupancy limit)
   struct SolveGraph {
