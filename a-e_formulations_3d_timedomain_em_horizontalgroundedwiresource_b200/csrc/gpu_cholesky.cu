@@ -102,11 +102,21 @@ __global__ void k_extend_add(T* __restrict__ L, T* __restrict__ U, Fronts f, con
   for (int a = b + lane; a < rc; a += 32) *felem(L, U, lo, uo, mp, kp, rl[a], pc) += uc[a + (int64_t)b * rc];
 }
 
-// Cholesky of the w x w diagonal block of panel [j0, j0 + w) (one CTA per front).
+// Cholesky of the w x w diagonal block of panel [j0, j0 + w) (one CTA of 256
+// threads per front), right-looking in shared memory with one barrier per column.
+// Thread t owns row i = t % 64 and, of it, the columns c = t / 64 (mod 4).  Step j
+// scales column j on the fly (L(r, j) = A(r, j) / sqrt(A(j, j)), recomputed by
+// every thread that needs it) and subtracts L(i, j) L(c, j) from A(i, c) for
+// j < c <= i; the finished column goes to the upper triangle A[j][r] (r > j) and
+// the diagonal to diag[j], which no later step reads, so column j is read
+// unchanged throughout its step.  Same operations in the same order per element
+// as a column-at-a-time factorization: the result does not depend on the thread
+// layout.
 template <class T>
-__global__ void k_potrf(T* __restrict__ L, Fronts f, const int* __restrict__ fronts, int j0,
-                        int* __restrict__ err, const int* __restrict__ c0_of) {
+__global__ void __launch_bounds__(256) k_potrf(T* __restrict__ L, Fronts f, const int* __restrict__ fronts, int j0,
+                                               int* __restrict__ err, const int* __restrict__ c0_of) {
   __shared__ T A[P][P + 1];
+  __shared__ T diag[P];
   const int s = fronts[blockIdx.x];
   const int m = f.m[s], k = f.k[s];
   const int w = min(P, k - j0);
@@ -116,29 +126,28 @@ __global__ void k_potrf(T* __restrict__ L, Fronts f, const int* __restrict__ fro
     A[i][j] = (i >= j) ? F[(j0 + i) + (int64_t)(j0 + j) * m] : (T)0;
   }
   __syncthreads();
+  const int i = threadIdx.x & (P - 1), g = threadIdx.x >> 6;
   for (int j = 0; j < w; ++j) {
-    if (threadIdx.x == 0) {
-      T d = A[j][j];
-      if (!(d > (T)0)) {
-        atomicCAS(err, 0, c0_of[s] + j0 + j + 1);
-        d = (T)1;
-      }
-      A[j][j] = tsqrt(d);
+    T d = A[j][j];
+    if (!(d > (T)0)) {
+      if (threadIdx.x == 0) atomicCAS(err, 0, c0_of[s] + j0 + j + 1);
+      d = (T)1;
     }
-    __syncthreads();
-    const T inv = (T)1 / A[j][j];
-    for (int i = j + 1 + threadIdx.x; i < w; i += blockDim.x) A[i][j] *= inv;
-    __syncthreads();
-    const int t = w - j - 1;
-    for (int idx = threadIdx.x; idx < t * t; idx += blockDim.x) {
-      const int i = j + 1 + idx / t, c = j + 1 + idx % t;
-      if (c <= i) A[i][c] -= A[i][j] * A[c][j];
+    const T sd = tsqrt(d);
+    const T inv = (T)1 / sd;
+    if (i > j && i < w) {
+      const T lij = A[i][j] * inv;
+      // first column of this thread's group after j
+      int c = j + 1 + ((g - (j + 1)) & 3);
+      for (; c <= i; c += 4) A[i][c] -= lij * (A[c][j] * inv);
+      if (g == 0) A[j][i] = lij;
     }
+    if (threadIdx.x == 0) diag[j] = sd;
     __syncthreads();
   }
   for (int idx = threadIdx.x; idx < w * w; idx += blockDim.x) {
-    const int i = idx % w, j = idx / w;
-    if (i >= j) F[(j0 + i) + (int64_t)(j0 + j) * m] = A[i][j];
+    const int r = idx % w, c = idx / w;
+    if (r >= c) F[(j0 + r) + (int64_t)(j0 + c) * m] = (r == c) ? diag[c] : A[c][r];
   }
 }
 
