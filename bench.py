@@ -486,7 +486,9 @@ def run_ours(args, world, rank, local):
                            "factor_slots": inf["factor_slots"],
                            "overlap": ("factorization k+1 runs beside the time steps of decade k (phase times "
                                        "overlap)") if inf["factor_slots"] > 1 else "none"},
-                "latency_ms": {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
+                "latency_ms": {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
+                               "what": "device time per forward solve with requests one at a time (the served "
+                                       "stream's latency is --config c4)"},
                 "phase_ms_per_solve": {"factor": factor_ms / units, "steps": solve_ms / units},
                 "wall_s": wall,
                 "gpu_launches": launches,
@@ -575,6 +577,18 @@ def batched_leg(args, pkg, base: str, form: str, scheme: int, device: int, singl
             "steps": inf["steps"], "factorizations": inf["factorizations"]}
 
 
+def write_request(job):
+    """Inputs of one served request (seed, cells lo, cells hi, directory); runs in a
+    worker process.  Returns (directory, formulation, scheme, edges)."""
+    seed, lo, hi, d = job
+    sys.path.insert(0, HERE)
+    mg = importlib.import_module(PKG + ".modelgen")
+    spec, form, scheme = mg.random_request_model(seed, lo, hi)
+    info = mg.write_model(d, spec)
+    mg.write_analytic_initial_field(d, spec)
+    return d, form, scheme, info["n_edges"]
+
+
 def run_serving(args, world, rank, local):
     """Config c4: a Poisson stream of random forward-modelling requests through
     the serving loop (tdem_server_*) on one GPU; prints solves/s and p50/p99 latency."""
@@ -587,13 +601,15 @@ def run_serving(args, world, rank, local):
     s0 = 20261203
     base = tempfile.mkdtemp(prefix="tdem_serve_r%d_" % rank)
     try:
-        reqs = []
-        for i in range(args.c4_requests):
-            spec, form, scheme = mg.random_request_model(s0 + i, lo, hi)
-            d = os.path.join(base, "req%03d" % i)
-            info = mg.write_model(d, spec)
-            mg.write_analytic_initial_field(d, spec)
-            reqs.append((d, form, scheme, info["n_edges"]))
+        # request inputs written by a spawned process pool (no CUDA state is shared)
+        import multiprocessing as mp
+        from concurrent.futures import ProcessPoolExecutor
+        jobs = [(s0 + i, lo, hi, os.path.join(base, "req%03d" % i)) for i in range(args.c4_requests)]
+        t_gen = time.perf_counter()
+        with ProcessPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1)),
+                                 mp_context=mp.get_context("spawn")) as ex:
+            reqs = list(ex.map(write_request, jobs))
+        t_gen = time.perf_counter() - t_gen
         # single-stream service rate from the first requests run alone
         t_alone = []
         for d, form, scheme, _ in reqs[:2]:
@@ -631,6 +647,7 @@ def run_serving(args, world, rank, local):
                 "makespan_s": st["makespan_s"], "completed": st["completed"], "failed": st["failed"],
                 "peak_device_gb": st["peak_device_bytes"] / 1e9, "peak_active": st["peak_active"],
                 "queue_wait_s_max": max(i["admit_s"] - i["submit_s"] for i in infos),
+                "inputs_written_s": t_gen,
                 "clocks": clocks}
         if rank == 0:
             print(json.dumps(line), flush=True)
