@@ -144,6 +144,7 @@ EXPORTED = [
     "tdem_correct_time_mesh",
     "tdem_sum_nonstat_3d_only",
     "tdem_summator_edmn",
+    "tdem_pipeline_directory",
     "tdem_solver_create",
     "tdem_solver_create_ex",
     "tdem_solver_plan",
@@ -184,6 +185,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.tdem_run_directory.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                        ctypes.c_char_p, ctypes.c_size_t]
     lib.tdem_run_directory.restype = ctypes.c_int
+    lib.tdem_pipeline_directory.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                            ctypes.c_char_p, ctypes.c_size_t]
+    lib.tdem_pipeline_directory.restype = ctypes.c_int
     lib.tdem_stationary_directory.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t]
     lib.tdem_stationary_directory.restype = ctypes.c_int
     for name in ("tdem_time_direct_solver", "tdem_correct_time_mesh"):
@@ -260,6 +264,21 @@ def run_directory(workdir: str, formulation="A", scheme: int = 2, device: int = 
                                 len(buf))
     if st != 0:
         raise TdemError(st, buf.value.decode(errors="replace"))
+
+
+PIPE_TIME_GRID, PIPE_STATIONARY, PIPE_SPLIT = 1, 2, 4
+
+
+def pipeline_directory(workdir: str, formulation="A", scheme: int = 2, device: int = 0,
+                       flags: int = PIPE_TIME_GRID | PIPE_STATIONARY | PIPE_SPLIT) -> None:
+    """The direct-mode 3D-only module sequence of GeoCalculatorSP in workdir: time
+    grid (when tcff exists), stationary initial field, transient, component split."""
+    lib = load_library()
+    err = ctypes.create_string_buffer(1024)
+    st = lib.tdem_pipeline_directory(os.fsencode(workdir), _form(formulation), int(scheme), int(device), int(flags),
+                                     err, len(err))
+    if st != 0:
+        raise TdemError(st, err.value.decode(errors="replace"))
 
 
 def stationary_directory(workdir: str, device: int = 0) -> None:

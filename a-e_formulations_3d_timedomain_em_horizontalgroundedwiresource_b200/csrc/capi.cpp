@@ -334,6 +334,53 @@ tdem_status tdem_run_directory(const char* workdir, int formulation, int scheme,
   }, errbuf, errlen);
 }
 
+tdem_status tdem_pipeline_directory(const char* workdir, int formulation, int scheme, int device, int flags,
+                                    char* errbuf, size_t errlen) {
+  return guard([&]() -> tdem_status {
+    if (!workdir) return TDEM_ERR_ARGUMENT;
+    if ((formulation != 0 && formulation != 1) || (scheme != 2 && scheme != 3)) return TDEM_ERR_ARGUMENT;
+    if (flags & ~(TDEM_PIPE_TIME_GRID | TDEM_PIPE_STATIONARY | TDEM_PIPE_SPLIT)) return TDEM_ERR_ARGUMENT;
+    const std::string dir(workdir);
+    auto exists = [&](const char* name) {
+      FILE* f = std::fopen((dir + "/" + name).c_str(), "rb");
+      if (f) std::fclose(f);
+      return f != nullptr;
+    };
+    char err[1024] = {0};
+    auto stage = [&](const char* module, tdem_status st) {
+      if (st != TDEM_OK) put_err(errbuf, errlen, std::string(module) + ": " + err);
+      return st;
+    };
+    if (exists("stop")) {
+      put_err(errbuf, errlen, "stop file present");
+      return TDEM_ERR_CANCELLED;
+    }
+    tdem_status st = TDEM_OK;
+    if ((flags & TDEM_PIPE_TIME_GRID) && exists("tcff")) {
+      if ((st = stage("TimeDirectSolver", tdem_time_direct_solver(workdir, err, sizeof err))) != TDEM_OK) return st;
+      if ((st = stage("CorrectTimeMesh", tdem_correct_time_mesh(workdir, err, sizeof err))) != TDEM_OK) return st;
+    }
+    if (flags & TDEM_PIPE_STATIONARY)
+      if ((st = stage("CalcStat3D_3T_A", tdem_stationary_directory(workdir, device, err, sizeof err))) != TDEM_OK)
+        return st;
+    if (!exists("xyzVectorE0")) {
+      FILE* f = std::fopen((dir + "/xyzVectorE0").c_str(), "w");
+      if (!f) {
+        put_err(errbuf, errlen, "cannot write xyzVectorE0");
+        return TDEM_ERR_INPUT;
+      }
+      std::fprintf(f, "0\n");
+      std::fclose(f);
+    }
+    if ((st = stage("CalcNonstat3DLine", tdem_run_directory(workdir, formulation, scheme, device, err, sizeof err))) !=
+        TDEM_OK)
+      return st;
+    if (flags & TDEM_PIPE_SPLIT)
+      if ((st = stage("SumNonstat3DOnly", tdem_sum_nonstat_3d_only(workdir, err, sizeof err))) != TDEM_OK) return st;
+    return TDEM_OK;
+  }, errbuf, errlen);
+}
+
 struct tdem_server {
   tdem::Server srv;
   std::mutex mu;

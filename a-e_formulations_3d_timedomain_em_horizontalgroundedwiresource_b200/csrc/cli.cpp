@@ -20,6 +20,10 @@
 // (SummatorEDMN/main.cpp:253-294) and writes the line voltages.  Under a name
 // containing TimeDirectSolver or CorrectTimeMesh (or with --time-direct-solver /
 // --correct-time-mesh [workdir]) it prepares the time grid as those modules do.
+// With --pipeline (or under a name containing GeoCalculatorSP) it runs the
+// direct-mode 3D-only module sequence in workdir (tdem_pipeline_directory): the
+// time grid, the stationary field (--no-stationary skips it), the transient and
+// the per-component split.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -95,10 +99,11 @@ int main(int argc, char** argv) {
     if (argc > 1 && !strcmp(argv[1], "--sum-nonstat-3d-only")) return post_main(false, argc, argv, 2);
   }
   int form = 0, scheme = 2, device = 0;
-  bool stationary = false;
+  bool stationary = false, pipeline = false, pipe_stat = true;
   std::string dir = ".";
   const std::string prog = argv[0];
   if (prog.find("CalcStat3D") != std::string::npos) stationary = true;
+  if (prog.find("GeoCalculatorSP") != std::string::npos) pipeline = true;
   if (prog.size() >= 3) {
     const std::string tail = prog.substr(prog.size() - 3);
     if (tail == "_A2") { form = 0; scheme = 2; }
@@ -116,14 +121,25 @@ int main(int argc, char** argv) {
       device = atoi(argv[++i]);
     } else if (!strcmp(argv[i], "--stationary")) {
       stationary = true;
+    } else if (!strcmp(argv[i], "--pipeline")) {
+      pipeline = true;
+    } else if (!strcmp(argv[i], "--no-stationary")) {
+      pipe_stat = false;
     } else if (argv[i][0] == '-') {
-      fprintf(stderr, "usage: %s [--form A|E] [--scheme 2|3] [--stationary] [--device N] [workdir]\n", argv[0]);
+      fprintf(stderr, "usage: %s [--form A|E] [--scheme 2|3] [--stationary | --pipeline [--no-stationary]] "
+              "[--device N] [workdir]\n", argv[0]);
       return (int)TDEM_ERR_ARGUMENT;
     } else {
       dir = argv[i];
     }
   }
   char err[1024] = {0};
+  if (pipeline) {
+    const int flags = TDEM_PIPE_TIME_GRID | TDEM_PIPE_SPLIT | (pipe_stat ? TDEM_PIPE_STATIONARY : 0);
+    const tdem_status st = tdem_pipeline_directory(dir.c_str(), form, scheme, device, flags, err, sizeof err);
+    if (st != TDEM_OK) fprintf(stderr, "pipeline (B200): %s\n", err);
+    return (int)st;
+  }
   if (stationary) {
     const tdem_status st = tdem_stationary_directory(dir.c_str(), device, err, sizeof err);
     if (st != TDEM_OK) fprintf(stderr, "CalcStat3D_3T_A (B200): %s\n", err);

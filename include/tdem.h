@@ -120,6 +120,29 @@ tdem_status tdem_sum_nonstat_3d_only(const char* workdir, char* errbuf, size_t e
 tdem_status tdem_summator_edmn(const char* workdir, int with_ddv, int profile, int place, char* errbuf,
                                size_t errlen);
 
+/* ---- The module sequence of a direct-mode 3D-only run --------------------------------
+ * Runs, in `workdir` and in one process, the modules GeoCalculatorSP starts one after
+ * another for a direct-mode (fdirect 1) run without the 2D chain, on a model directory
+ * whose mesh files are already there (GeoCalculatorSP.cpp:2111-2126 Calc1Loop, then
+ * CalcMainTask :1327-1709):
+ *   TDEM_PIPE_TIME_GRID  TimeDirectSolver then CorrectTimeMesh (when `tcff` exists);
+ *   TDEM_PIPE_STATIONARY CalcStat3D_3T_A (the grounded-wire initial field);
+ *   always               xyzVectorE0 with 0 points when absent (:1579-1583), then
+ *                        CalcNonstat3DLine (:1648-1655);
+ *   TDEM_PIPE_SPLIT      SumNonstat3DOnly (:1664-1673).
+ * Stops at the first module that fails and returns its status; errbuf then names the
+ * module.  Unlike GeoCalculatorSP it builds no mesh (RegularMeshBuilder / p.bat), starts
+ * no process and maps no shared memory; the line voltages (SummatorEDMN, per
+ * transmitter and profile) stay a separate call.  A `stop` file ends the run as in the
+ * modules themselves. */
+enum {
+  TDEM_PIPE_TIME_GRID = 1,
+  TDEM_PIPE_STATIONARY = 2,
+  TDEM_PIPE_SPLIT = 4
+};
+tdem_status tdem_pipeline_directory(const char* workdir, int formulation, int scheme, int device, int flags,
+                                    char* errbuf, size_t errlen);
+
 typedef struct tdem_solver tdem_solver;
 
 typedef struct tdem_info {
