@@ -201,6 +201,8 @@ tdem_status tdem_solver_plan(const char* workdir, int formulation, int scheme, c
     out->n_times = (int)m.time.size();
     out->plan_seconds = ts.times().setup_s;
     out->digest = tdem::plan_digest(*sy);
+    out->ozaki_flops = sy->oz_flops;
+    out->ozaki_rows = sy->oz_rows_max;
     return TDEM_OK;
   }, err, err_len);
 }

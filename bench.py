@@ -206,12 +206,13 @@ def cpu_baseline(cfg: str, spec, form: str, scheme: int, workdir: str, full_fact
                  full_steps: int, threads: int) -> dict:
     """Times the reference's own CalcNonstat3DLine (built from source, oracle/_ref)
     on a bounded sample of the same workload: the same variant, mesh and matrices
-    with the time grid cut to one factorization (the first 3 steps of the two-point
-    scheme; the first 2 of the three-point one, which takes them with the two-point
-    formula before its own).  The per-call wall times logged by the pardiso_64
-    stand-in split the run into set-up, factorization and per-step time; the full
-    solve's time is extrapolated from them (set-up + factorizations x factor time +
-    steps x step time) and labelled as such.  The sample's outputs stay in workdir."""
+    with the time grid cut to its first 3 steps (one factorization for the
+    two-point scheme; two for the three-point one, which takes its first two steps
+    with the two-point formula), so that 3 time layers are printed.  The per-call
+    wall times logged by the pardiso_64 stand-in split the run into set-up,
+    factorization and per-step time; the full solve's time is extrapolated from
+    them (set-up + factorizations x mean factor time + steps x step time) and
+    labelled as such.  The sample's outputs stay in workdir."""
     sys.path.insert(0, os.path.join(HERE, "oracle"))
     import run_ref  # noqa: E402  (oracle: baseline leg only)
     mg = importlib.import_module(PKG + ".modelgen")
@@ -221,7 +222,7 @@ def cpu_baseline(cfg: str, spec, form: str, scheme: int, workdir: str, full_fact
                 "sample": "unavailable: oracle/_ref not built"}
     import copy
     s2 = copy.deepcopy(spec)
-    cut = 4 if scheme == 2 else 3
+    cut = 4
     s2.times = spec.times[:cut]
     s2.print_interval = (float(s2.times[1]), float(s2.times[cut - 1]))
     mg.write_model(workdir, s2)
@@ -263,7 +264,7 @@ def cpu_baseline(cfg: str, spec, form: str, scheme: int, workdir: str, full_fact
             "sampled_factorizations": len(fac), "setup_s": t_setup, "factor_s": t_fact, "step_s": t_step,
             "extrapolated_solve_s": full, "full_factorizations": full_factorizations, "full_steps": full_steps,
             "sample": "reference CalcNonstat3DLine_%s (built from source, CPU FP64 Cholesky stand-in for "
-                      "MKL PARDISO) on the same mesh cut to %d steps: wall %.1f s = set-up %.1f s + "
+                      "MKL PARDISO) on the same mesh, time grid cut to %d steps: wall %.1f s = set-up %.1f s + "
                       "%d factorization(s) x %.2f s + %d steps x %.3f s; extrapolated to %d factorizations + "
                       "%d steps = %.1f s per forward solve" % (variant, steps, wall, t_setup, len(fac), t_fact,
                                                                steps, t_step, full_factorizations, full_steps,
@@ -296,7 +297,7 @@ def gpu_parity(pkg, outs, ref_dir: str, work: str, form: str, scheme: int, devic
 def run_reference_arm(args, world, rank, local):
     """The reference's own CalcNonstat3DLine on the host cores.  A full solve of the
     80^3 workload takes ~13 min on 16 cores, so each sample runs the workload cut to
-    one factorization and the full solve is extrapolated (labelled so in the line,
+    its first 3 steps and the full solve is extrapolated (labelled so in the line,
     with the measured phases); the extrapolation is checked once per run against a
     full reference solve of the 40^3 half-space (A-form, two-point, 120 steps),
     extrapolated and measured side by side."""
@@ -342,7 +343,7 @@ def run_reference_arm(args, world, rank, local):
             "steps": len(vals), "warmup": 0, "steps_requested": args.steps, "warmup_requested": args.warmup,
             "extrapolated": True,
             "ms_per_step": (1000.0 * sum(x["measured_wall_s"] for x in ok) / len(ok)) if ok else None,
-            "ms_per_step_is": "measured wall time of one sample (the workload cut to one factorization)",
+            "ms_per_step_is": "measured wall time of one sample (the workload cut to its first 3 steps)",
             "extrapolated_ms_per_solve": (1000.0 / v) if v else None,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": {"workload": desc, "parallelism": "host cores (%d threads)" % threads},
@@ -454,7 +455,7 @@ def run_ours(args, world, rank, local):
                     outs = importlib.import_module(PKG + ".outputs")
                     try:
                         pc = gpu_parity(pkg, outs, d, os.path.join(base, "gpu_on_cpu_sample"), form, scheme,
-                                        local, "%s mesh (%d edges), %s%d, time grid cut to one factorization" %
+                                        local, "%s mesh (%d edges), %s%d, time grid cut to its first 3 steps" %
                                         (args.config, winfo["n_edges"], form, scheme))
                         parity = {"max_rel_err": pc["max_rel_err"], "tol": 1e-9,
                                   "pass": pc["max_rel_err"] <= 1e-9, "cases": [pc],

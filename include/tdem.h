@@ -236,6 +236,9 @@ typedef struct tdem_plan_info {
   double plan_seconds;      /* host time of the planning (inputs, patterns, analysis) */
   uint64_t digest;          /* hash of the elimination order, the fronts, the entry map and the
                                solve units: equal digests mean identical launch plans */
+  double ozaki_flops;       /* flops of the trailing updates planned on the integer tensor
+                               pipe (FP64 products by digit splitting; FP64 solvers) */
+  int64_t ozaki_rows;       /* rows of the digit buffer those updates need */
 } tdem_plan_info;
 tdem_status tdem_solver_plan(const char* workdir, int formulation, int scheme, const tdem_options* opts,
                              tdem_plan_info* out, char* err, size_t err_len);
