@@ -381,6 +381,7 @@ std::string TransientSolve::setup_device(cudaStream_t stream) {
   std::string e;
   chol_.reset(new GpuCholesky());
   if (opt_.fp32_update != 0) chol_->set_tensor_core_update(opt_.fp32_update == 2);
+  if (const char* oz = std::getenv("TDEM_OZAKI")) chol_->set_ozaki(oz[0] != '0');
   int slots = opt_.factor_slots;
   if (slots == 0) {
     size_t free_b = 0, total_b = 0;

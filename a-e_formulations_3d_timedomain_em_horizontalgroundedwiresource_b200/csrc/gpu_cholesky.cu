@@ -2225,7 +2225,8 @@ std::string set_attributes() {
 template <class T>
 int launch_factor(const Symbolic& sy, T* L, T* U, const double* vals, const int64_t* entry, Fronts fr,
                   const int* parent, const int64_t* rel_off, const int* rel, const int* tasks,
-                  const int64_t* prefix, int* err, const int* c0, bool use_tc, cudaStream_t s) {
+                  const int64_t* prefix, int* err, const int* c0, bool use_tc, cudaStream_t s,
+                  const OzakiBuffers* oz = nullptr, const int64_t* aux = nullptr) {
   int launches = 0;
   cudaMemsetAsync(L, 0, sizeof(T) * sy.nnz_l, s);
   {
@@ -2268,8 +2269,18 @@ int launch_factor(const Symbolic& sy, T* L, T* U, const double* vals, const int6
       }
       if (ps.syrk_big.ctas > 0) {
         if constexpr (std::is_same<T, double>::value) {
-          k_syrk_big_dmma<<<grid_of(2 * ps.syrk_big.ctas), kBigThreads, dmma_smem(), s>>>(
-              L, U, fr, tasks + ps.syrk_big.off, prefix + ps.syrk_big.pre, ps.syrk_big.count, ps.j0);
+          if (oz && ps.ozaki) {
+            // digits of the panel rows, then the update on the integer tensor pipe
+            launch_ozaki_slice(L, fr.l_off, fr.m, fr.k, tasks + ps.oz_slice.off, prefix + ps.oz_slice.pre,
+                               aux + ps.oz_slice.off, ps.oz_slice.count, ps.oz_slice.ctas, ps.j0, *oz, s);
+            launch_ozaki_update(L, U, fr.l_off, fr.u_off, fr.m, fr.k, tasks + ps.syrk_big.off,
+                                prefix + ps.syrk_big.pre, aux + ps.syrk_big.off, ps.syrk_big.count,
+                                ps.syrk_big.ctas, ps.j0, *oz, err, s);
+            ++launches;
+          } else {
+            k_syrk_big_dmma<<<grid_of(2 * ps.syrk_big.ctas), kBigThreads, dmma_smem(), s>>>(
+                L, U, fr, tasks + ps.syrk_big.off, prefix + ps.syrk_big.pre, ps.syrk_big.count, ps.j0);
+          }
         } else if (use_tc) {
           launch_syrk_tc((float*)L, (float*)U, fr.l_off, fr.u_off, fr.m, fr.k, tasks + ps.syrk_big.off,
                          prefix + ps.syrk_big.pre, ps.syrk_big.count, ps.syrk_big.ctas, ps.j0, err, s);
@@ -2549,6 +2560,8 @@ int64_t GpuCholesky::bytes_needed(const Symbolic& sy, int nrhs_max, int precisio
   int64_t b = fel * sy.u_elems + el * (sy.wvec_elems * nr + sy.solve_partials * nr + sy.solve_slots * kPanel * nr);
   b += std::max(1, std::min(nslots, kMaxSlots)) * slot_bytes(sy, precision_bytes);
   if (fel != el) b += slot_bytes(sy, (int)fel);  // the FP64 work factor of a demoted setup
+  if (fel == 8) b += sy.oz_rows_max * ((int64_t)kOzSlices * kOzK + 4);  // digit slices + exponents
+  b += 8 * (int64_t)sy.task_aux.size();
   b += 8 * (int64_t)(sy.l_off.size() + sy.u_off.size() + sy.wvec_off.size() + sy.entry_dst.size() +
                      sy.rel_off.size() + sy.rows_off.size() + sy.task_prefix.size() + sy.dinv_off.size());
   b += 4 * (int64_t)(sy.front_m.size() + sy.front_k.size() + sy.rel.size() + sy.rows_all.size() + sy.tasks.size() +
@@ -2596,6 +2609,13 @@ std::string GpuCholesky::setup(Symbolic&& sy, const std::vector<int>& perm_to_ve
   }
   if (!(e = upload(&d_tasks_, sy_.tasks, s)).empty()) return e;
   if (!(e = upload(&d_prefix_, sy_.task_prefix, s)).empty()) return e;
+  if (!(e = upload(&d_task_aux_, sy_.task_aux, s)).empty()) return e;
+  if (fac_elem_ == 8 && ozaki_ && sy_.oz_rows_max > 0) {
+    oz_.rows = sy_.oz_rows_max;
+    if (!(e = alloc((void**)&oz_.slices, (size_t)kOzSlices * kOzK * oz_.rows)).empty()) return e;
+    if (!(e = alloc((void**)&oz_.exps, sizeof(int) * (size_t)oz_.rows)).empty()) return e;
+    if (!(e = ozaki_setup(oz_)).empty()) return e;
+  }
   if (!(e = upload(&d_parent_, sy_.front_parent, s)).empty()) return e;
   if (!(e = upload(&d_c0_, sy_.front_c0, s)).empty()) return e;
   if (!(e = upload(&d_items_, sy_.solve_items, s)).empty()) return e;
@@ -2628,7 +2648,8 @@ void GpuCholesky::factor(const double* d_vals, cudaStream_t s, int slot) {
   if (demoted()) {
     // FP64 factorization into the work factor, then both arrays rounded into the slot
     launches_factor_ = launch_factor<double>(sy_, (double*)d_Lw_, (double*)d_U_, d_vals, d_entry_, fr, d_parent_,
-                                             d_rel_off_, d_rel_, d_tasks_, d_prefix_, d_err_, d_c0_, false, s);
+                                             d_rel_off_, d_rel_, d_tasks_, d_prefix_, d_err_, d_c0_, false, s,
+                                             ozaki() ? &oz_ : nullptr, d_task_aux_);
     if (ni) {
       k_diag_inverse<double><<<ni, 256, ism, s>>>((const double*)d_Lw_, (double*)d_dinvw_, fr, d_dinv_off_,
                                                   d_items_ + 2 * sy_.inv_off);
@@ -2649,7 +2670,8 @@ void GpuCholesky::factor(const double* d_vals, cudaStream_t s, int slot) {
                                                        d_items_ + 2 * sy_.inv_off);
   } else {
     launches_factor_ = launch_factor<double>(sy_, (double*)Lp, (double*)d_U_, d_vals, d_entry_, fr, d_parent_,
-                                             d_rel_off_, d_rel_, d_tasks_, d_prefix_, d_err_, d_c0_, false, s);
+                                             d_rel_off_, d_rel_, d_tasks_, d_prefix_, d_err_, d_c0_, false, s,
+                                             ozaki() ? &oz_ : nullptr, d_task_aux_);
     if (ni) k_diag_inverse<double><<<ni, 256, ism, s>>>((const double*)Lp, (double*)Dp, fr, d_dinv_off_,
                                                         d_items_ + 2 * sy_.inv_off);
   }

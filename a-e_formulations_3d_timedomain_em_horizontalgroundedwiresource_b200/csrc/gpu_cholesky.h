@@ -12,6 +12,7 @@
 #include <string>
 #include <vector>
 
+#include "ozaki_update.h"
 #include "symbolic.h"
 
 namespace tdem {
@@ -87,6 +88,12 @@ class GpuCholesky {
   // FP32 factor: trailing updates on the tensor cores (3xTF32) or on the
   // CUDA cores (default).  Takes effect at setup().
   void set_tensor_core_update(bool on) { tc_update_ = on; }
+  // FP64 factorization: the trailing updates the analysis planned for it (large
+  // outer panels, kOzRowsCap rows per launch at most) run on the integer tensor
+  // pipe by digit splitting (ozaki_update.h) instead of the FP64 tensor pipe.  On
+  // by default; takes effect at setup().
+  void set_ozaki(bool on) { ozaki_ = on; }
+  bool ozaki() const { return oz_.slices != nullptr; }
   // Selects the per-panel solve (one launch per 64-column panel and level) instead
   // of the fused level solves; both compute the same triangular solves.  Turns the
   // autotuner off.
@@ -118,6 +125,9 @@ class GpuCholesky {
   int nrhs_max_ = 0;
   size_t bytes_ = 0;
   int launches_factor_ = 0, launches_solve_ = 0;
+  bool ozaki_ = true;
+  OzakiBuffers oz_;
+  int64_t* d_task_aux_ = nullptr;
   bool autotune_ = true;
   bool has_forced_ = false;
   SolveSchedule forced_;

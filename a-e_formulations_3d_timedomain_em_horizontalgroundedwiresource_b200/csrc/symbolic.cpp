@@ -1,6 +1,8 @@
 // Host symbolic analysis: nested-dissection ordering, assembly tree, and the
 // flattened maps / task lists consumed by the GPU factorization and solves.
 #include "symbolic.h"
+
+#include <cstdlib>
 #include "parallel.h"
 
 #include <algorithm>
@@ -270,6 +272,7 @@ void add_tasks(Symbolic& sy, TaskList& tl, const std::vector<int>& fr,
   sy.task_prefix.push_back(0);
   for (size_t i = 0; i < fr.size(); ++i) {
     sy.tasks.push_back(fr[i]);
+    sy.task_aux.push_back(0);
     acc += ctas[i];
     sy.task_prefix.push_back(acc);
   }
@@ -597,6 +600,10 @@ std::string analyse(int n, const int64_t* rowptr, const int* colind, const doubl
     }
     int kmax = 0;
     for (int s : lp.fronts) kmax = std::max(kmax, sy.front_k[s]);
+    // TDEM_OZAKI_ALL=1 plans every trailing update that fits the digit buffer on the
+    // integer tensor pipe (tests of small models)
+    const char* oz_all = std::getenv("TDEM_OZAKI_ALL");
+    const double oz_min_flops = (oz_all && oz_all[0] == '1') ? 0.0 : kOzMinFlops;
     for (int j0 = 0; j0 < kmax; j0 += kPanel) {
       PanelStep ps;
       ps.j0 = j0;
@@ -634,6 +641,28 @@ std::string analyse(int n, const int64_t* rowptr, const int* colind, const doubl
       add_tasks(sy, ps.syrk, fin, c3);
       add_tasks(sy, ps.syrk_wide, fin, c6);
       add_tasks(sy, ps.syrk_big, fbig, c5);
+      {
+        // the Ozaki path: slice-buffer rows of the fronts, in task order
+        int64_t rows = 0;
+        double fl = 0.0;
+        std::vector<int64_t> c7;
+        for (size_t q = 0; q < fbig.size(); ++q) {
+          const int s = fbig[q], k = sy.front_k[s], m = sy.front_m[s];
+          const int J1 = std::min(k, J0 + kOuter);
+          sy.task_aux[ps.syrk_big.off + q] = rows;
+          rows += m - J1;
+          fl += (double)(m - J1) * (m - J1) * (J1 - J0);
+          c7.push_back(cdiv(m - J1, 64));
+        }
+        if (!fbig.empty() && rows <= kOzRowsCap && fl >= oz_min_flops) {
+          ps.ozaki = true;
+          ps.oz_rows = rows;
+          sy.oz_rows_max = std::max(sy.oz_rows_max, rows);
+          sy.oz_flops += fl;
+          add_tasks(sy, ps.oz_slice, fbig, c7);
+          for (size_t q = 0; q < fbig.size(); ++q) sy.task_aux[ps.oz_slice.off + q] = sy.task_aux[ps.syrk_big.off + q];
+        }
+      }
       add_tasks(sy, ps.solve_upd, fr, c4);
       max_partials = std::max(max_partials, ps.solve_upd.ctas);
       lp.panels.push_back(ps);

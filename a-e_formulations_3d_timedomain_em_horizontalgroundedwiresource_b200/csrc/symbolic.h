@@ -30,6 +30,14 @@ constexpr int kSolveRows = 256;  // rows per CTA of the solve updates
 constexpr int kSolveChunk = 8;   // 64 x 64 blocks accumulated by one level-solve unit
 constexpr int kUnitInts = 16;    // ints per level-solve unit record (64 bytes)
 constexpr int kSolveLookahead = 8;  // extra blocks a chain unit takes ahead of its newest one
+// Trailing updates on the integer tensor pipe (FP64 by the Ozaki splitting): each
+// row of the outer panel is split into kOzSlices signed 7-bit digits after scaling
+// by a power of two; only launches whose panels total at most kOzRowsCap rows (the
+// slice buffer) and at least kOzMinFlops flops take that path.
+constexpr int kOzSlices = 8;
+constexpr int kOzK = kOuter;          // digits per row and slice (K of an outer panel, padded)
+constexpr int64_t kOzRowsCap = 1 << 19;
+constexpr double kOzMinFlops = 2e9;
 // most blocks one level-solve unit accumulates (a chain unit, or a short row)
 constexpr int kUnitBlocks = (kSolveLookahead + 1 > kSolveChunk + 1) ? kSolveLookahead + 1 : kSolveChunk + 1;
 
@@ -60,6 +68,12 @@ struct PanelStep {
   TaskList syrk;       // update of columns [j1, J1) (rows >= j1) by the inner panel, 64-tiles
   TaskList syrk_wide;  // the same update in 128-row x 64-column tiles (FP64 tensor-pipe kernel)
   TaskList syrk_big;   // at the end of an outer panel: trailing [J1, m) by [J0, J1), 128-tiles
+  // Ozaki path of syrk_big (ozaki true): the panel rows [J1, m) of every front of
+  // syrk_big are split into digits, front after front (task_aux of the syrk_big
+  // entries: the front's first row in the slice buffer), by oz_slice (64 rows per CTA)
+  bool ozaki = false;
+  int64_t oz_rows = 0;
+  TaskList oz_slice;
   TaskList solve_upd;  // ceil((m - j1) / kSolveRows) CTAs per front (fwd update / bwd partials)
 };
 
@@ -99,6 +113,7 @@ struct Symbolic {
   std::vector<int> rows_all;         // concatenated [c0..c1) U rows, permuted numbering
   std::vector<int64_t> wvec_off;     // per front: offset of its m-long solve vector
   std::vector<int> tasks;            // concatenated task front lists
+  std::vector<int64_t> task_aux;     // per task entry: launch-specific value (see PanelStep)
   std::vector<int64_t> task_prefix;  // concatenated CTA prefix sums
 
   std::vector<int> solve_items;      // (front, block) pairs of the diagonal-block inversions
@@ -120,6 +135,8 @@ struct Symbolic {
   int64_t wvec_elems = 0;     // sum of m
   int64_t nnz_l = 0;          // sum of m*k (stored factor entries incl. diagonal blocks)
   double flops = 0.0;         // factorization flops
+  double oz_flops = 0.0;      // flops of the trailing updates on the Ozaki path
+  int64_t oz_rows_max = 0;    // slice-buffer rows the Ozaki path needs
   int max_m = 0, max_k = 0;
   int64_t solve_partials = 0; // scratch entries per RHS column for backward partial sums
 };
