@@ -154,6 +154,68 @@ __global__ void k_history_rhs(const int64_t* __restrict__ rowptr, const int* __r
   }
 }
 
+// Several sources: one warp per row, the sources in groups of 8.  Lane l takes the
+// entries q = b + l, b + l + 32, ... of the row (the row's columns and values are
+// read once per group, not once per source) and sums its products for the 8
+// sources; the 32 lanes' sums are combined by recursive halving (each round a
+// lane keeps half of its values and adds its partner's other half), after which
+// lane l holds the row total of source 4 ((l >> 4) & 1) + 2 ((l >> 3) & 1) +
+// ((l >> 2) & 1) of the group.  The additions happen in an order fixed by the
+// lane pattern alone.
+__global__ void k_history_rhs_multi(const int64_t* __restrict__ rowptr, const int* __restrict__ col,
+                                    const double* __restrict__ C, const double* __restrict__ u1,
+                                    const double* __restrict__ u2, double m1c, double m2c,
+                                    const double* __restrict__ S, double coef, const uint8_t* __restrict__ bound,
+                                    int n, int npls, double* __restrict__ rhs) {
+  const int row = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (row >= n) return;
+  if (bound[row]) {
+    for (int p = lane; p < npls; p += 32) rhs[row + (int64_t)p * n] = 0.0;
+    return;
+  }
+  const int64_t b = rowptr[row], e = rowptr[row + 1];
+  for (int p0 = 0; p0 < npls; p0 += 8) {
+    double v[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) v[r] = 0.0;
+    for (int64_t q = b + lane; q < e; q += 32) {
+      const double c = C[q];
+      const int64_t j = col[q];
+#pragma unroll
+      for (int r = 0; r < 8; ++r) {
+        const int64_t off = j + (int64_t)(p0 + r) * n;
+        if (p0 + r < npls) v[r] = fma(c, m2c != 0.0 ? u1[off] * m1c + u2[off] * m2c : u1[off] * m1c, v[r]);
+      }
+    }
+    double a4[4], a2[2];
+    bool up = (lane & 16) != 0;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const double mine = up ? v[4 + r] : v[r], other = up ? v[r] : v[4 + r];
+      a4[r] = mine + __shfl_xor_sync(0xffffffffu, other, 16);
+    }
+    up = (lane & 8) != 0;
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      const double mine = up ? a4[2 + r] : a4[r], other = up ? a4[r] : a4[2 + r];
+      a2[r] = mine + __shfl_xor_sync(0xffffffffu, other, 8);
+    }
+    up = (lane & 4) != 0;
+    double a1 = (up ? a2[1] : a2[0]) + __shfl_xor_sync(0xffffffffu, up ? a2[0] : a2[1], 4);
+    a1 += __shfl_xor_sync(0xffffffffu, a1, 2);
+    a1 += __shfl_xor_sync(0xffffffffu, a1, 1);
+    if ((lane & 3) == 0) {
+      const int p = p0 + 4 * ((lane >> 4) & 1) + 2 * ((lane >> 3) & 1) + ((lane >> 2) & 1);
+      if (p < npls) {
+        double t = a1;
+        if (coef != 0.0) t += coef * S[row + (int64_t)p * n];
+        rhs[row + (int64_t)p * n] = t;
+      }
+    }
+  }
+}
+
 __global__ void k_receivers(const int64_t* __restrict__ rowptr, const int* __restrict__ col,
                             const double* __restrict__ val, const int* __restrict__ src, int nrows,
                             const double* __restrict__ u, int64_t ld, double* __restrict__ out) {
@@ -377,8 +439,12 @@ void launch_history_rhs(const int64_t* rowptr, const int* col, const double* Cva
                         const double* u2, double m1c, double m2c, const double* S, double coef,
                         const uint8_t* bound, int n, int npls, double* rhs, cudaStream_t s) {
   const int64_t threads = (int64_t)n * 32;
-  k_history_rhs<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(rowptr, col, Cval, u1, u2, m1c, m2c, S, coef,
-                                                                  bound, n, npls, rhs);
+  if (npls > 1)
+    k_history_rhs_multi<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(rowptr, col, Cval, u1, u2, m1c, m2c, S,
+                                                                          coef, bound, n, npls, rhs);
+  else
+    k_history_rhs<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(rowptr, col, Cval, u1, u2, m1c, m2c, S, coef,
+                                                                    bound, n, npls, rhs);
 }
 
 void launch_normal_field(const float* f, const int* idx, const double* len, int nanom, int n, int npls, double* En,
