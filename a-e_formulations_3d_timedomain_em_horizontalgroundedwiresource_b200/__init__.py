@@ -81,6 +81,8 @@ class TdemInfo(ctypes.Structure):
         ("solve_split", ctypes.c_int),
         ("solve_candidates", ctypes.c_int),
         ("solve_tuned_ms", ctypes.c_double),
+        ("ozaki_ms", ctypes.c_double),
+        ("ozaki_macs", ctypes.c_double),
     ]
 
     def as_dict(self) -> dict:

@@ -290,6 +290,8 @@ tdem_status tdem_solver_info(const tdem_solver* s, tdem_info* info) {
       info->solve_schedule = sc.kind;
       info->solve_split = sc.split;
       info->solve_tuned_ms = sc.ms;
+      info->ozaki_ms = pt.ozaki_ms;
+      info->ozaki_macs = c.ozaki() ? c.symbolic().oz_macs : 0.0;
       for (const auto& t : c.tune_log())
         if (t.first == m.npls) info->solve_candidates = (int)t.second.size();
     }

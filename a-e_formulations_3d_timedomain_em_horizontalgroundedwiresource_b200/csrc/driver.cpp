@@ -382,6 +382,7 @@ std::string TransientSolve::setup_device(cudaStream_t stream) {
   chol_.reset(new GpuCholesky());
   if (opt_.fp32_update != 0) chol_->set_tensor_core_update(opt_.fp32_update == 2);
   if (const char* oz = std::getenv("TDEM_OZAKI")) chol_->set_ozaki(oz[0] != '0');
+  chol_->set_ozaki_timing(true);
   int slots = opt_.factor_slots;
   if (slots == 0) {
     size_t free_b = 0, total_b = 0;
@@ -669,6 +670,8 @@ std::string TransientSolve::run() {
   pt_.refine_iters = pt_.refine_iters_max = 0;
   pt_.refine_worst = 0.0;
   pt_.factor_gpu_ms = pt_.solve_gpu_ms = pt_.run_gpu_ms = 0;
+  pt_.ozaki_ms = 0;
+  chol_->take_ozaki_ms();  // events of an earlier run that ended early
   launches_ = 0;
   for (PhaseMark& m : marks_)  // marks of a run that ended early are dropped
     if (m.ev) cudaEventDestroy(m.ev);
@@ -940,6 +943,7 @@ std::string TransientSolve::run() {
   if (const int ss = chol_->solve_status(s_))
     return ss == 1 ? "CUDA: a wait of the level triangular solves gave up"
                    : "CUDA: a wait of the tensor-core update gave up";
+  pt_.ozaki_ms = chol_->take_ozaki_ms();
   pt_.factor_s = pt_.factor_gpu_ms * 1e-3;
   pt_.steps_s = pt_.solve_gpu_ms * 1e-3;
   (void)tstart;

@@ -51,6 +51,7 @@ struct PhaseTimes {
   // (factor_gpu_ms sums the factorizations, solve_gpu_ms the time-step spans;
   // with two factor slots they overlap and may add up to more than run_gpu_ms)
   double run_gpu_ms = 0, factor_gpu_ms = 0, solve_gpu_ms = 0;
+  double ozaki_ms = 0;  // summed device time of the integer-pipe trailing updates
   int factorizations = 0, steps = 0, factor_slots = 1;
   int64_t h2d_bytes = 0, d2h_bytes = 0;   // host<->device traffic of prepare/run/results
   int refine_iters = 0, refine_iters_max = 0;  // CG iterations of the last run (mixed precision)

@@ -2226,7 +2226,8 @@ template <class T>
 int launch_factor(const Symbolic& sy, T* L, T* U, const double* vals, const int64_t* entry, Fronts fr,
                   const int* parent, const int64_t* rel_off, const int* rel, const int* tasks,
                   const int64_t* prefix, int* err, const int* c0, bool use_tc, cudaStream_t s,
-                  const OzakiBuffers* oz = nullptr, const int64_t* aux = nullptr) {
+                  const OzakiBuffers* oz = nullptr, const int64_t* aux = nullptr,
+                  std::vector<cudaEvent_t>* oz_ev = nullptr, size_t* oz_used = nullptr) {
   int launches = 0;
   cudaMemsetAsync(L, 0, sizeof(T) * sy.nnz_l, s);
   {
@@ -2273,9 +2274,24 @@ int launch_factor(const Symbolic& sy, T* L, T* U, const double* vals, const int6
             // digits of the panel rows, then the update on the integer tensor pipe
             launch_ozaki_slice(L, fr.l_off, fr.m, fr.k, tasks + ps.oz_slice.off, prefix + ps.oz_slice.pre,
                                aux + ps.oz_slice.off, ps.oz_slice.count, ps.oz_slice.ctas, ps.j0, *oz, s);
+            cudaEvent_t ev[2] = {nullptr, nullptr};
+            if (oz_ev) {
+              while (oz_ev->size() < 2 * (*oz_used + 1)) {
+                cudaEvent_t e;
+                if (cudaEventCreate(&e) != cudaSuccess) break;
+                oz_ev->push_back(e);
+              }
+              if (oz_ev->size() >= 2 * (*oz_used + 1)) {
+                ev[0] = (*oz_ev)[2 * *oz_used];
+                ev[1] = (*oz_ev)[2 * *oz_used + 1];
+                ++*oz_used;
+                cudaEventRecord(ev[0], s);
+              }
+            }
             launch_ozaki_update(L, U, fr.l_off, fr.u_off, fr.m, fr.k, tasks + ps.syrk_big.off,
                                 prefix + ps.syrk_big.pre, aux + ps.syrk_big.off, ps.syrk_big.count,
                                 ps.syrk_big.ctas, ps.j0, *oz, err, s);
+            if (ev[1]) cudaEventRecord(ev[1], s);
             ++launches;
           } else {
             k_syrk_big_dmma<<<grid_of(2 * ps.syrk_big.ctas), kBigThreads, dmma_smem(), s>>>(
@@ -2526,6 +2542,7 @@ std::string set_fused_attributes() {
 GpuCholesky::~GpuCholesky() {
   for (SolveGraph& g : graph_)
     if (g.exec) cudaGraphExecDestroy(g.exec);
+  for (cudaEvent_t e : oz_events_) cudaEventDestroy(e);
   for (void* p : allocs_) cudaFree(p);
 }
 
@@ -2649,7 +2666,8 @@ void GpuCholesky::factor(const double* d_vals, cudaStream_t s, int slot) {
     // FP64 factorization into the work factor, then both arrays rounded into the slot
     launches_factor_ = launch_factor<double>(sy_, (double*)d_Lw_, (double*)d_U_, d_vals, d_entry_, fr, d_parent_,
                                              d_rel_off_, d_rel_, d_tasks_, d_prefix_, d_err_, d_c0_, false, s,
-                                             ozaki() ? &oz_ : nullptr, d_task_aux_);
+                                             ozaki() ? &oz_ : nullptr, d_task_aux_,
+                                             oz_timing_ ? &oz_events_ : nullptr, &oz_used_);
     if (ni) {
       k_diag_inverse<double><<<ni, 256, ism, s>>>((const double*)d_Lw_, (double*)d_dinvw_, fr, d_dinv_off_,
                                                   d_items_ + 2 * sy_.inv_off);
@@ -2671,7 +2689,8 @@ void GpuCholesky::factor(const double* d_vals, cudaStream_t s, int slot) {
   } else {
     launches_factor_ = launch_factor<double>(sy_, (double*)Lp, (double*)d_U_, d_vals, d_entry_, fr, d_parent_,
                                              d_rel_off_, d_rel_, d_tasks_, d_prefix_, d_err_, d_c0_, false, s,
-                                             ozaki() ? &oz_ : nullptr, d_task_aux_);
+                                             ozaki() ? &oz_ : nullptr, d_task_aux_,
+                                             oz_timing_ ? &oz_events_ : nullptr, &oz_used_);
     if (ni) k_diag_inverse<double><<<ni, 256, ism, s>>>((const double*)Lp, (double*)Dp, fr, d_dinv_off_,
                                                         d_items_ + 2 * sy_.inv_off);
   }
@@ -2833,6 +2852,16 @@ std::string GpuCholesky::solve_graph(const double* d_b, double* d_x, int64_t ld,
   }
   TDEM_CUDA_TRY(cudaGraphLaunch(sg.exec, s));
   return "";
+}
+
+double GpuCholesky::take_ozaki_ms() {
+  double tot = 0.0;
+  for (size_t i = 0; i < oz_used_; ++i) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, oz_events_[2 * i], oz_events_[2 * i + 1]) == cudaSuccess) tot += ms;
+  }
+  oz_used_ = 0;
+  return tot;
 }
 
 int GpuCholesky::status(cudaStream_t s) {

@@ -94,6 +94,11 @@ class GpuCholesky {
   // by default; takes effect at setup().
   void set_ozaki(bool on) { ozaki_ = on; }
   bool ozaki() const { return oz_.slices != nullptr; }
+  // Records CUDA events around every integer-pipe update launch of the following
+  // factorizations; take_ozaki_ms() returns their summed device time (after the
+  // stream has completed them) and starts over.
+  void set_ozaki_timing(bool on) { oz_timing_ = on; }
+  double take_ozaki_ms();
   // Selects the per-panel solve (one launch per 64-column panel and level) instead
   // of the fused level solves; both compute the same triangular solves.  Turns the
   // autotuner off.
@@ -127,6 +132,9 @@ class GpuCholesky {
   int launches_factor_ = 0, launches_solve_ = 0;
   bool ozaki_ = true;
   OzakiBuffers oz_;
+  bool oz_timing_ = false;
+  std::vector<cudaEvent_t> oz_events_;  // start/stop pairs, the first 2 * oz_used_ recorded
+  size_t oz_used_ = 0;
   int64_t* d_task_aux_ = nullptr;
   bool autotune_ = true;
   bool has_forced_ = false;

@@ -657,6 +657,16 @@ std::string analyse(int n, const int64_t* rowptr, const int* colind, const doubl
         if (!fbig.empty() && rows <= kOzRowsCap && fl >= oz_min_flops) {
           ps.ozaki = true;
           ps.oz_rows = rows;
+          // 128 x 64 output tiles (the right half of a last 128-column tile past the
+          // front is skipped) x K blocks of 64 digits x the kept digit pairs
+          for (int s : fbig) {
+            const int k = sy.front_k[s], m = sy.front_m[s];
+            const int J1 = std::min(k, J0 + kOuter);
+            const int64_t r = m - J1, nt = cdiv(r, 128);
+            const int64_t ctas = nt * (nt + 1) - ((r - (nt - 1) * 128) <= 64 ? 1 : 0);
+            const int64_t kpad = cdiv(J1 - J0, 64) * 64;
+            sy.oz_macs += (double)ctas * 128.0 * 64.0 * (double)kpad * (kOzSlices * (kOzSlices + 1) / 2);
+          }
           sy.oz_rows_max = std::max(sy.oz_rows_max, rows);
           sy.oz_flops += fl;
           add_tasks(sy, ps.oz_slice, fbig, c7);

@@ -136,6 +136,7 @@ struct Symbolic {
   int64_t nnz_l = 0;          // sum of m*k (stored factor entries incl. diagonal blocks)
   double flops = 0.0;         // factorization flops
   double oz_flops = 0.0;      // flops of the trailing updates on the Ozaki path
+  double oz_macs = 0.0;       // 8-bit multiply-adds those updates issue on the tensor pipe
   int64_t oz_rows_max = 0;    // slice-buffer rows the Ozaki path needs
   int max_m = 0, max_k = 0;
   int64_t solve_partials = 0; // scratch entries per RHS column for backward partial sums

@@ -373,7 +373,7 @@ def run_ours(args, world, rank, local):
         barrier(world)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        gpu_ms = factor_ms = solve_ms = 0.0
+        gpu_ms = factor_ms = solve_ms = oz_ms = 0.0
         launches = 0
         lat = []
         for _ in range(units):
@@ -382,6 +382,7 @@ def run_ours(args, world, rank, local):
             gpu_ms += inf["run_gpu_ms"]
             factor_ms += inf["factor_gpu_ms"]
             solve_ms += inf["solve_gpu_ms"]
+            oz_ms += inf["ozaki_ms"]
             launches += inf["kernel_launches"]
             lat.append(inf["run_gpu_ms"])
         torch.cuda.synchronize()
@@ -438,6 +439,22 @@ def run_ours(args, world, rank, local):
                           "bytes_per_step": solve_bytes, "avg_step_ms": solve_ms_step,
                           "peak_source": ("MEASURED_PEAKS.json hbm_gbs (measured)" if hbm_measured
                                           else "fallback 6650 GB/s (MEASURED_PEAKS.json absent)")}
+            roof_oz = None
+            if inf["ozaki_macs"] > 0 and oz_ms > 0:
+                # the integer tensor pipe: 8-bit multiply-adds of the digit products per launch
+                # time; peak = twice the measured dense bf16 rate (B200's 8-bit dense rate is
+                # twice its bf16 rate)
+                bf16 = peaks.get("bf16_tflops")
+                ops = 2.0 * inf["ozaki_macs"] * n_fact * units
+                ach = ops / (oz_ms * 1e-3) / 1e12
+                pk = 2.0 * bf16 if bf16 else 2.0 * 1590.0
+                roof_oz = {"bound": "tensor", "kernel": "k_oz_update (tcgen05 kind::i8, FP64 trailing updates by "
+                                                        "digit splitting)",
+                           "achieved": ach, "peak": pk, "unit": "TOP/s (int8)", "frac": ach / pk,
+                           "ops_per_factorization": 2.0 * inf["ozaki_macs"],
+                           "ms_per_factorization": oz_ms / max(units * n_fact, 1),
+                           "peak_source": ("2 x MEASURED_PEAKS.json bf16_tflops (measured bf16 burst)" if bf16
+                                           else "2 x fallback 1590 TF/s bf16")}
             cpu = None
             parity = None
             if not args.no_cpu_baseline:
@@ -496,6 +513,7 @@ def run_ours(args, world, rank, local):
                 "clocks": clocks,
                 "roofline": roof,
                 "roofline_solve": roof_solve,
+                "roofline_ozaki": roof_oz,
                 "cpu_baseline": cpu,
                 "parity": parity,
                 "e2e": e2e,

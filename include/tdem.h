@@ -178,6 +178,9 @@ typedef struct tdem_info {
   int solve_split;          /* column groups that solve is split into */
   int solve_candidates;     /* schedules the autotuner measured (0: not tuned) */
   double solve_tuned_ms;    /* the chosen schedule's measured device time per solve */
+  double ozaki_ms;          /* device time of the last run's trailing updates on the integer
+                               tensor pipe (CUDA events around each launch) */
+  double ozaki_macs;        /* 8-bit multiply-adds one factorization issues there */
 } tdem_info;
 
 /* Options of tdem_solver_create_ex (zero-initialise, then set what differs). */
