@@ -24,8 +24,9 @@
 // TMA boxes (64 x 128 x 8 and 64 x 64 x 8 bytes) into one of two stages; warp 1
 // lane 0 issues the 2 x 36 MMAs of a stage and commits them to the stage's
 // "empty" mbarrier; warps 2-5 (tensor-memory lane groups 2, 3, 0, 1) wait for the
-// last commit, read the eight accumulators of their rows 16 columns at a time
-// (tcgen05.ld), add the groups in FP64 from the smallest weight up, scale by
+// last commit, read the eight accumulators of their rows 8 columns at a time (all
+// eight tcgen05.ld before one wait), add the groups in FP64 from the smallest
+// weight up, scale by
 // 2^(e_a + e_b) and subtract from F.  TMA boxes read only this GPU's slice buffer
 // (no multicast).  Every mbarrier wait is bounded; a CTA that gives up records
 // err[2], waits (bounded) for its own MMAs and frees its tensor memory.
@@ -300,38 +301,40 @@ k_oz_update(double* __restrict__ L, double* __restrict__ U, const int64_t* __res
     const int64_t lo = l_off[s], uo = u_off[s];
     const int ea = s_ea[rl];
 #pragma unroll 1
-    for (int cc = 0; cc < ON / 16; ++cc) {
-      double v[16];
+    for (int cc = 0; cc < ON / 8; ++cc) {
+      // the 8 columns of all eight group accumulators, then one wait
+      uint32_t a[OS][8];
 #pragma unroll
-      for (int q = 0; q < 16; ++q) v[q] = 0.0;
-#pragma unroll 1
+      for (int g = 0; g < OS; ++g)
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                     : "=r"(a[g][0]), "=r"(a[g][1]), "=r"(a[g][2]), "=r"(a[g][3]), "=r"(a[g][4]), "=r"(a[g][5]),
+                       "=r"(a[g][6]), "=r"(a[g][7])
+                     : "r"(tmem + ((uint32_t)(32 * sub) << 16) + (uint32_t)(ON * g + 8 * cc)));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      double v[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) v[q] = 0.0;
+#pragma unroll
       for (int g = OS - 1; g >= 0; --g) {
-        uint32_t a[16];
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-            : "=r"(a[0]), "=r"(a[1]), "=r"(a[2]), "=r"(a[3]), "=r"(a[4]), "=r"(a[5]), "=r"(a[6]), "=r"(a[7]),
-              "=r"(a[8]), "=r"(a[9]), "=r"(a[10]), "=r"(a[11]), "=r"(a[12]), "=r"(a[13]), "=r"(a[14]), "=r"(a[15])
-            : "r"(tmem + ((uint32_t)(32 * sub) << 16) + (uint32_t)(ON * g + 16 * cc)));
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
         const double w = ldexp(1.0, -7 * (g + 2));
 #pragma unroll
-        for (int q = 0; q < 16; ++q) v[q] = fma((double)(int)a[q], w, v[q]);
+        for (int q = 0; q < 8; ++q) v[q] = fma((double)(int)a[g][q], w, v[q]);
       }
       if (r < m) {
-        double old[16];
+        double old[8];
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
-          const int c = c0 + 16 * cc + q;
+        for (int q = 0; q < 8; ++q) {
+          const int c = c0 + 8 * cc + q;
           old[q] = 0.0;
           if (c < m && c <= r)
             old[q] = (c < k) ? L[lo + r + (int64_t)c * m] : U[uo + (r - k) + (int64_t)(c - k) * (m - k)];
         }
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
-          const int c = c0 + 16 * cc + q;
+        for (int q = 0; q < 8; ++q) {
+          const int c = c0 + 8 * cc + q;
           if (c < m && c <= r) {
             double* e = (c < k) ? L + lo + r + (int64_t)c * m : U + uo + (r - k) + (int64_t)(c - k) * (m - k);
-            *e = old[q] - ldexp(v[q], ea + s_eb[16 * cc + q]);
+            *e = old[q] - ldexp(v[q], ea + s_eb[8 * cc + q]);
           }
         }
       }
