@@ -32,6 +32,9 @@
 // err[2], waits (bounded) for its own MMAs and frees its tensor memory.
 #include "ozaki_update.h"
 
+#include <algorithm>
+#include <string>
+
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -78,6 +81,9 @@ __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
 }
 __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("{ .reg .b64 st; mbarrier.arrive.shared::cta.b64 st, [%0]; }" ::"r"(bar) : "memory");
 }
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
   for (unsigned it = 0; it < kWaitLimit; ++it) {
@@ -186,46 +192,72 @@ __global__ void __launch_bounds__(256) k_oz_slice(const double* __restrict__ L, 
   }
 }
 
-__global__ void __launch_bounds__(NTHR, 1)
-k_oz_update(double* __restrict__ L, double* __restrict__ U, const int64_t* __restrict__ l_off,
-            const int64_t* __restrict__ u_off, const int* __restrict__ fm, const int* __restrict__ fk,
-            const int* __restrict__ fronts, const int64_t* __restrict__ prefix, const int64_t* __restrict__ aux,
-            int count, int j0, const int* __restrict__ exps, int64_t nrows_buf, int* err,
-            const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB) {
-  extern __shared__ __align__(16) unsigned char sm_raw[];
-  // 1024-byte aligned operand area (swizzle atoms are 512 bytes)
-  unsigned char* ops =
-      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(sm_raw) + 1023) & ~uintptr_t(1023));
-  uint64_t* bars = reinterpret_cast<uint64_t*>(ops + NST * STAGE_BYTES);  // full[NST], empty[NST], done
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(ops + NST * STAGE_BYTES + 64);
-  int* s_fail = reinterpret_cast<int*>(ops + NST * STAGE_BYTES + 68);
-  int* s_issued = s_fail + 1;    // K blocks whose TMA loads were issued
-  int* s_consumed = s_fail + 2;  // K blocks whose loads the MMA thread saw complete
-  int* s_ea = reinterpret_cast<int*>(ops + NST * STAGE_BYTES + 256);
-  int* s_eb = s_ea + OM;
-  const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + NST), done_bar = smem_u32(bars + 2 * NST);
+// One output tile of the task list: the tile's front and coordinates.  skip: the
+// right half of a last 128-column tile past the front (no work).
+struct OzTile {
+  int s, m, k, J0, J1, nkb, r0, c0, arow, brow;
+  bool skip;
+};
 
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int64_t tile = blockIdx.x >> 1;
+__device__ __forceinline__ OzTile oz_tile(const int* __restrict__ fm, const int* __restrict__ fk,
+                                          const int* __restrict__ fronts, const int64_t* __restrict__ prefix,
+                                          const int64_t* __restrict__ aux, int count, int j0, int64_t id) {
+  OzTile z;
+  const int64_t tile = id >> 1;
   const int idx = find_task(prefix, count, tile);
-  const int s = fronts[idx];
-  const int m = fm[s], k = fk[s];
-  const int J0 = (j0 / kOuter) * kOuter, J1 = min(k, J0 + kOuter);
-  const int K = J1 - J0, nkb = (K + OKB - 1) / OKB;
+  z.s = fronts[idx];
+  z.m = fm[z.s];
+  z.k = fk[z.s];
+  z.J0 = (j0 / kOuter) * kOuter;
+  z.J1 = min(z.k, z.J0 + kOuter);
+  z.nkb = (z.J1 - z.J0 + OKB - 1) / OKB;
   const int64_t t = tile - prefix[idx];
   int bi = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
   while ((int64_t)(bi + 1) * (bi + 2) / 2 <= t) ++bi;
   while ((int64_t)bi * (bi + 1) / 2 > t) --bi;
   const int bj = (int)(t - (int64_t)bi * (bi + 1) / 2);
-  const int r0 = J1 + bi * 128, c0 = J1 + bj * 128 + (int)(blockIdx.x & 1) * ON;
-  if (c0 >= m) return;  // the right half of a tile past the front (whole CTA, before any barrier)
-  const int arow = (int)(aux[idx] + (r0 - J1)), brow = (int)(aux[idx] + (c0 - J1));
+  z.r0 = z.J1 + bi * 128;
+  z.c0 = z.J1 + bj * 128 + (int)(id & 1) * ON;
+  z.skip = z.c0 >= z.m;
+  z.arow = (int)(aux[idx] + (z.r0 - z.J1));
+  z.brow = (int)(aux[idx] + (z.c0 - z.J1));
+  return z;
+}
+
+// Persistent: every CTA takes the tiles blockIdx.x, blockIdx.x + gridDim.x, ... of
+// the 2 x ctas tile list (all roles walk the same sequence).  The producer and the
+// MMA thread run ahead across tiles through the two-stage ring; the MMAs of a tile
+// wait until the epilogue warps have read the previous tile's accumulators out of
+// tensor memory ("tmem_free"), and the epilogue's global read-modify-write of a tile
+// overlaps the next tile's loads and MMAs.
+__global__ void __launch_bounds__(NTHR, 1)
+k_oz_update(double* __restrict__ L, double* __restrict__ U, const int64_t* __restrict__ l_off,
+            const int64_t* __restrict__ u_off, const int* __restrict__ fm, const int* __restrict__ fk,
+            const int* __restrict__ fronts, const int64_t* __restrict__ prefix, const int64_t* __restrict__ aux,
+            int count, int64_t ntiles, int j0, const int* __restrict__ exps, int64_t nrows_buf, int* err,
+            const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB) {
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  // 1024-byte aligned operand area (swizzle atoms are 512 bytes)
+  unsigned char* ops =
+      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(sm_raw) + 1023) & ~uintptr_t(1023));
+  // full[NST], empty[NST], acc_full, tmem_free, done
+  uint64_t* bars = reinterpret_cast<uint64_t*>(ops + NST * STAGE_BYTES);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(ops + NST * STAGE_BYTES + 64);
+  int* s_fail = reinterpret_cast<int*>(ops + NST * STAGE_BYTES + 68);
+  int* s_issued = s_fail + 1;    // K blocks (over all tiles) whose TMA loads were issued
+  int* s_consumed = s_fail + 2;  // K blocks whose loads the MMA thread saw complete
+  const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + NST);
+  const uint32_t acc_full = smem_u32(bars + 2 * NST), tmem_free = smem_u32(bars + 2 * NST + 1),
+                 done_bar = smem_u32(bars + 2 * NST + 2);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
   if (tid == 0) {
     for (int q = 0; q < NST; ++q) {
       mbar_init(full0 + 8 * q, 1);   // the producer's expect_tx arrival (+ the TMA bytes)
       mbar_init(empty0 + 8 * q, 1);  // one tcgen05.commit frees the stage
     }
+    mbar_init(acc_full, 1);          // the commit after a tile's last MMAs
+    mbar_init(tmem_free, 128);       // every epilogue thread, after its tensor-memory reads
     mbar_init(done_bar, 1);
     *s_fail = 0;
     *s_issued = 0;
@@ -238,108 +270,148 @@ k_oz_update(double* __restrict__ L, double* __restrict__ U, const int64_t* __res
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
-  for (int q = tid; q < OM + ON; q += NTHR) {
-    const int64_t row = q < OM ? (int64_t)arow + q : (int64_t)brow + (q - OM);
-    const int e = row < nrows_buf ? exps[row] : 0;
-    if (q < OM) s_ea[q] = e;
-    else s_eb[q - OM] = e;
-  }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
 
   if (warp == 0 && lane == 0) {
-    // producer: K block kb of every slice of the tile's rows (A) and columns (B)
-    for (int kb = 0; kb < nkb; ++kb) {
-      const int st = kb % NST;
-      if (kb >= NST && !mbar_wait(empty0 + 8 * st, (uint32_t)(((kb - NST) / NST) & 1))) {
-        atomicExch(s_fail, 1);
-        break;
+    // producer: K block kb of every slice of each tile's rows (A) and columns (B)
+    int kbg = 0;
+    bool stop = false;
+    for (int64_t id = blockIdx.x; id < ntiles && !stop; id += gridDim.x) {
+      const OzTile z = oz_tile(fm, fk, fronts, prefix, aux, count, j0, id);
+      if (z.skip) continue;
+      for (int kb = 0; kb < z.nkb; ++kb, ++kbg) {
+        const int st = kbg % NST;
+        if (kbg >= NST && !mbar_wait(empty0 + 8 * st, (uint32_t)(((kbg - NST) / NST) & 1))) {
+          atomicExch(s_fail, 1);
+          stop = true;
+          break;
+        }
+        if (*(volatile int*)s_fail) {
+          stop = true;
+          break;
+        }
+        const uint32_t a = smem_u32(ops + st * STAGE_BYTES);
+        mbar_expect_tx(full0 + 8 * st, (uint32_t)STAGE_BYTES);
+        tma_load_3d(a, &tmA, full0 + 8 * st, kb * OKB, z.arow, 0);
+        tma_load_3d(a + A_BYTES, &tmB, full0 + 8 * st, kb * OKB, z.brow, 0);
+        *s_issued = kbg + 1;
       }
-      if (*(volatile int*)s_fail) break;
-      const uint32_t a = smem_u32(ops + st * STAGE_BYTES);
-      mbar_expect_tx(full0 + 8 * st, (uint32_t)STAGE_BYTES);
-      tma_load_3d(a, &tmA, full0 + 8 * st, kb * OKB, arow, 0);
-      tma_load_3d(a + A_BYTES, &tmB, full0 + 8 * st, kb * OKB, brow, 0);
-      *s_issued = kb + 1;
     }
   } else if (warp == 1 && lane == 0) {
     // MMA issuer: the kept digit pairs (i, j), i + j < OS, into accumulator i + j
-    for (int kb = 0; kb < nkb; ++kb) {
-      const int st = kb % NST;
-      if (!mbar_wait(full0 + 8 * st, (uint32_t)((kb / NST) & 1))) {
+    int kbg = 0, tc = 0;
+    bool stop = false;
+    for (int64_t id = blockIdx.x; id < ntiles && !stop; id += gridDim.x) {
+      const OzTile z = oz_tile(fm, fk, fronts, prefix, aux, count, j0, id);
+      if (z.skip) continue;
+      // the epilogue has read the previous tile's accumulators
+      if (tc > 0 && !mbar_wait(tmem_free, (uint32_t)((tc - 1) & 1))) {
         atomicExch(s_fail, 1);
         break;
       }
-      *s_consumed = kb + 1;
-      if (*(volatile int*)s_fail) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t a0 = smem_u32(ops + st * STAGE_BYTES), b0 = a0 + A_BYTES;
-#pragma unroll 1
-      for (int i = 0; i < OS; ++i) {
-#pragma unroll 1
-        for (int j = 0; i + j < OS; ++j) {
-          const uint32_t d = tmem + (uint32_t)(ON * (i + j));
-#pragma unroll
-          for (int ks = 0; ks < OKB / 32; ++ks)
-            mma_i8(d, sdesc(a0 + i * A_SLICE, ks), sdesc(b0 + j * B_SLICE, ks),
-                   (kb > 0 || ks > 0 || i > 0) ? 1u : 0u);
+      for (int kb = 0; kb < z.nkb; ++kb, ++kbg) {
+        const int st = kbg % NST;
+        if (!mbar_wait(full0 + 8 * st, (uint32_t)((kbg / NST) & 1))) {
+          atomicExch(s_fail, 1);
+          stop = true;
+          break;
         }
+        *s_consumed = kbg + 1;
+        if (*(volatile int*)s_fail) {
+          stop = true;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t a0 = smem_u32(ops + st * STAGE_BYTES), b0 = a0 + A_BYTES;
+#pragma unroll 1
+        for (int i = 0; i < OS; ++i) {
+#pragma unroll 1
+          for (int j = 0; i + j < OS; ++j) {
+            const uint32_t d = tmem + (uint32_t)(ON * (i + j));
+#pragma unroll
+            for (int ks = 0; ks < OKB / 32; ++ks)
+              mma_i8(d, sdesc(a0 + i * A_SLICE, ks), sdesc(b0 + j * B_SLICE, ks),
+                     (kb > 0 || ks > 0 || i > 0) ? 1u : 0u);
+          }
+        }
+        mma_commit(empty0 + 8 * st);
       }
-      mma_commit(empty0 + 8 * st);
+      if (stop) break;
+      mma_commit(acc_full);
+      ++tc;
     }
-    // every MMA issued so far: arrives once they have completed
+    // every MMA issued: arrives once they have completed
     mma_commit(done_bar);
-  }
-  __syncthreads();
-  bool ok = mbar_wait(done_bar, 0u) && *(volatile int*)s_fail == 0;
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  if (ok && warp >= 2) {
+  } else if (warp >= 2) {
+    // epilogue: rows 32 (warp % 4) + lane of each tile
     const int sub = warp & 3, rl = 32 * sub + lane;
-    const int r = r0 + rl;
-    const int64_t lo = l_off[s], uo = u_off[s];
-    const int ea = s_ea[rl];
-#pragma unroll 1
-    for (int cc = 0; cc < ON / 8; ++cc) {
-      // the 8 columns of all eight group accumulators, then one wait
-      uint32_t a[OS][8];
+    int tc = 0;
+    for (int64_t id = blockIdx.x; id < ntiles; id += gridDim.x) {
+      const OzTile z = oz_tile(fm, fk, fronts, prefix, aux, count, j0, id);
+      if (z.skip) continue;
+      const int r = z.r0 + rl;
+      const int ea = ((int64_t)z.arow + rl < nrows_buf) ? exps[z.arow + rl] : 0;
+      bool ok = mbar_wait(acc_full, (uint32_t)(tc & 1)) && *(volatile int*)s_fail == 0;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      double v[ON];
+      if (ok) {
 #pragma unroll
-      for (int g = 0; g < OS; ++g)
-        asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-                     : "=r"(a[g][0]), "=r"(a[g][1]), "=r"(a[g][2]), "=r"(a[g][3]), "=r"(a[g][4]), "=r"(a[g][5]),
-                       "=r"(a[g][6]), "=r"(a[g][7])
-                     : "r"(tmem + ((uint32_t)(32 * sub) << 16) + (uint32_t)(ON * g + 8 * cc)));
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      double v[8];
+        for (int cc = 0; cc < ON / 4; ++cc) {
+          // 4 columns of all eight group accumulators, then one wait
+          uint32_t a[OS][4];
 #pragma unroll
-      for (int q = 0; q < 8; ++q) v[q] = 0.0;
+          for (int g = 0; g < OS; ++g)
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];"
+                         : "=r"(a[g][0]), "=r"(a[g][1]), "=r"(a[g][2]), "=r"(a[g][3])
+                         : "r"(tmem + ((uint32_t)(32 * sub) << 16) + (uint32_t)(ON * g + 4 * cc)));
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-      for (int g = OS - 1; g >= 0; --g) {
-        const double w = ldexp(1.0, -7 * (g + 2));
+          for (int q = 0; q < 4; ++q) v[4 * cc + q] = 0.0;
 #pragma unroll
-        for (int q = 0; q < 8; ++q) v[q] = fma((double)(int)a[g][q], w, v[q]);
-      }
-      if (r < m) {
-        double old[8];
+          for (int g = OS - 1; g >= 0; --g) {
+            const double w = ldexp(1.0, -7 * (g + 2));
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          const int c = c0 + 8 * cc + q;
-          old[q] = 0.0;
-          if (c < m && c <= r)
-            old[q] = (c < k) ? L[lo + r + (int64_t)c * m] : U[uo + (r - k) + (int64_t)(c - k) * (m - k)];
+            for (int q = 0; q < 4; ++q) v[4 * cc + q] = fma((double)(int)a[g][q], w, v[4 * cc + q]);
+          }
         }
+      }
+      // the accumulators are free for the next tile's MMAs
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      mbar_arrive(tmem_free);
+      ++tc;
+      if (!ok) break;
+      if (r < z.m) {
+        const int64_t lo = l_off[z.s], uo = u_off[z.s];
+        const int m = z.m, k = z.k;
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          const int c = c0 + 8 * cc + q;
-          if (c < m && c <= r) {
-            double* e = (c < k) ? L + lo + r + (int64_t)c * m : U + uo + (r - k) + (int64_t)(c - k) * (m - k);
-            *e = old[q] - ldexp(v[q], ea + s_eb[8 * cc + q]);
+        for (int h = 0; h < ON / 8; ++h) {
+          double old[8];
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const int c = z.c0 + 8 * h + q;
+            old[q] = 0.0;
+            if (c < m && c <= r)
+              old[q] = (c < k) ? L[lo + r + (int64_t)c * m] : U[uo + (r - k) + (int64_t)(c - k) * (m - k)];
+          }
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const int c = z.c0 + 8 * h + q;
+            if (c < m && c <= r) {
+              const int eb = ((int64_t)z.brow + 8 * h + q < nrows_buf) ? exps[z.brow + 8 * h + q] : 0;
+              double* e = (c < k) ? L + lo + r + (int64_t)c * m : U + uo + (r - k) + (int64_t)(c - k) * (m - k);
+              *e = old[q] - ldexp(v[8 * h + q], ea + eb);
+            }
           }
         }
       }
     }
   }
+  __syncthreads();
+  const bool ok = mbar_wait(done_bar, 0u) && *(volatile int*)s_fail == 0;
   if (!ok && tid == 0) {
     atomicExch(err + 2, 1);
     // loads issued but never seen complete by the MMA thread: wait (bounded) for
@@ -378,6 +450,10 @@ std::string ozaki_setup(OzakiBuffers& ob) {
   if (r != CUDA_SUCCESS) return "cuTensorMapEncodeTiled (64-row digit boxes) failed: " + std::to_string((int)r);
   e = cudaFuncSetAttribute(k_oz_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES);
   if (e != cudaSuccess) return std::string("cudaFuncSetAttribute(k_oz_update): ") + cudaGetErrorString(e);
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&ob.sms, cudaDevAttrMultiProcessorCount, dev) !=
+                                                 cudaSuccess)
+    return "cannot read the SM count";
   return "";
 }
 
@@ -391,8 +467,10 @@ void launch_ozaki_slice(const double* L, const int64_t* l_off, const int* m, con
 void launch_ozaki_update(double* L, double* U, const int64_t* l_off, const int64_t* u_off, const int* m,
                          const int* k, const int* fronts, const int64_t* prefix, const int64_t* aux, int count,
                          int64_t ctas, int j0, const OzakiBuffers& ob, int* err, cudaStream_t s) {
-  k_oz_update<<<(unsigned)(2 * ctas), NTHR, SMEM_BYTES, s>>>(
-      L, U, l_off, u_off, m, k, fronts, prefix, aux, count, j0, ob.exps, ob.rows, err,
+  const int64_t ntiles = 2 * ctas;
+  const unsigned grid = (unsigned)std::min<int64_t>(ntiles, ob.sms > 0 ? ob.sms : 148);
+  k_oz_update<<<grid, NTHR, SMEM_BYTES, s>>>(
+      L, U, l_off, u_off, m, k, fronts, prefix, aux, count, ntiles, j0, ob.exps, ob.rows, err,
       *reinterpret_cast<const CUtensorMap*>(ob.map_a), *reinterpret_cast<const CUtensorMap*>(ob.map_b));
 }
 

@@ -17,6 +17,7 @@ struct OzakiBuffers {
   int8_t* slices = nullptr;  // [kOzSlices][rows][kOzK] digits
   int* exps = nullptr;       // [rows] row exponents
   int64_t rows = 0;
+  int sms = 0;               // SMs of the device: CTAs of the persistent update
   alignas(64) unsigned char map_a[128] = {};  // CUtensorMap of 128-row operand boxes
   alignas(64) unsigned char map_b[128] = {};  // CUtensorMap of 64-row operand boxes
 };
