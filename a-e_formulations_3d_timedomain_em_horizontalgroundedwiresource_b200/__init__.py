@@ -157,6 +157,7 @@ EXPORTED = [
     "tdem_solver_info",
     "tdem_solver_cancel",
     "tdem_solver_time_step",
+    "tdem_solver_tune_log",
     "tdem_solver_error",
     "tdem_solver_destroy",
     "tdem_pardiso_64",
@@ -215,6 +216,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         getattr(lib, name).restype = ctypes.c_int
     lib.tdem_solver_time_step.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     lib.tdem_solver_time_step.restype = ctypes.c_int
+    lib.tdem_solver_tune_log.argtypes = [P, P, P, P, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    lib.tdem_solver_tune_log.restype = ctypes.c_int
     lib.tdem_solver_results.argtypes = [P, P, P, P]
     lib.tdem_solver_results.restype = ctypes.c_int
     lib.tdem_solver_info.argtypes = [P, ctypes.POINTER(TdemInfo)]
@@ -392,6 +395,18 @@ class Solver:
         ms = ctypes.c_double(0.0)
         self._check(self._lib.tdem_solver_time_step(self._h, 1 if block else 0, int(reps), ctypes.byref(ms)))
         return ms.value
+
+    def tune_log(self) -> list:
+        """The solve autotuner's candidates for this solver's column count:
+        [(kind, column groups, device ms per solve), ...]."""
+        kinds = (ctypes.c_int * 16)()
+        splits = (ctypes.c_int * 16)()
+        ms = (ctypes.c_double * 16)()
+        n = ctypes.c_int(0)
+        self._check(self._lib.tdem_solver_tune_log(self._h, ctypes.cast(kinds, ctypes.c_void_p),
+                                                   ctypes.cast(splits, ctypes.c_void_p),
+                                                   ctypes.cast(ms, ctypes.c_void_p), 16, ctypes.byref(n)))
+        return [(kinds[i], splits[i], ms[i]) for i in range(min(n.value, 16))]
 
     def write_outputs(self) -> None:
         self._check(self._lib.tdem_solver_write_outputs(self._h))

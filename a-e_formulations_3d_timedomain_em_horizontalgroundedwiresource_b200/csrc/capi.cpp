@@ -309,6 +309,25 @@ tdem_status tdem_solver_time_step(tdem_solver* s, int block, int reps, double* m
   }, nullptr, 0, s ? &s->error : nullptr);
 }
 
+tdem_status tdem_solver_tune_log(const tdem_solver* s, int* kinds, int* splits, double* ms, int max, int* count) {
+  return guard([&]() -> tdem_status {
+    if (!s || !count || max < 0) return TDEM_ERR_ARGUMENT;
+    *count = 0;
+    if (s->solve.model().n_edges <= 0 || s->solve.n_interior() <= 0) return TDEM_OK;
+    for (const auto& t : s->solve.cholesky().tune_log()) {
+      if (t.first != s->solve.model().npls) continue;
+      const int n = (int)t.second.size();
+      for (int i = 0; i < n && i < max; ++i) {
+        if (kinds) kinds[i] = t.second[i].kind;
+        if (splits) splits[i] = t.second[i].split;
+        if (ms) ms[i] = t.second[i].ms;
+      }
+      *count = n;
+    }
+    return TDEM_OK;
+  });
+}
+
 tdem_status tdem_solver_cancel(tdem_solver* s) {
   return guard([&]() -> tdem_status {
     if (!s) return TDEM_ERR_ARGUMENT;

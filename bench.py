@@ -584,6 +584,7 @@ def batched_leg(args, pkg, base: str, form: str, scheme: int, device: int, singl
         inf = s.info()
         step_block = s.time_step(True, 5)
         step_seq = s.time_step(False, 2)
+        tune = s.tune_log()
     ms = sum(runs) / len(runs)
     npls = inf["n_sources"]
     return {"workload": "same model, %s-form, %s, %d wires as one n x %d block per step, FP64" %
@@ -593,7 +594,11 @@ def batched_leg(args, pkg, base: str, form: str, scheme: int, device: int, singl
             "step_ms": {"block_graph": step_block, "sequential_single_column": step_seq,
                         "sequential_over_block": step_seq / step_block},
             "factor_gpu_ms_per_run": inf["factor_gpu_ms"], "solve_gpu_ms_per_run": inf["solve_gpu_ms"],
-            "steps": inf["steps"], "factorizations": inf["factorizations"]}
+            "steps": inf["steps"], "factorizations": inf["factorizations"],
+            "autotuner": {"chosen": {"kind": inf["solve_schedule"], "split": inf["solve_split"],
+                                     "ms": inf["solve_tuned_ms"]},
+                          "kinds": "0 fused level solves, 1 panel solves, 2 persistent fused level solves",
+                          "candidates": [{"kind": a, "split": b, "ms": c} for a, b, c in tune]}}
 
 
 def write_request(job):

@@ -265,6 +265,11 @@ tdem_status tdem_solver_info(const tdem_solver* s, tdem_info* info);
  * No counterpart in the reference: it lets a caller compare the batched step with
  * sequential per-source solves (pardiso.cpp:113-120 solves npls columns per call). */
 tdem_status tdem_solver_time_step(tdem_solver* s, int block, int reps, double* ms_per_step);
+/* The solve autotuner's measurements for the solver's column count (n_sources):
+ * up to max entries of (schedule kind, column groups, device ms per solve), in the
+ * order measured; *count receives how many there are (0 before the first run, or
+ * when the count is not tuned).  No counterpart in the reference. */
+tdem_status tdem_solver_tune_log(const tdem_solver* s, int* kinds, int* splits, double* ms, int max, int* count);
 /* Requests cancellation of a running tdem_solver_run (checked between time steps;
  * the reference polls a file named "stop", GeoCalculatorSP.cpp:27-39). */
 tdem_status tdem_solver_cancel(tdem_solver* s);

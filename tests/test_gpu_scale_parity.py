@@ -67,7 +67,9 @@ def test_solve_autotuner_measures_every_schedule(pkg, outs, tmp_path, monkeypatc
         s.run()
         s.write_outputs()
         info = s.info()
+        log = s.tune_log()
     assert info["solve_candidates"] == 9 and info["solve_tuned_ms"] > 0
+    assert len(log) == 9 and min(ms for _, _, ms in log) == pytest.approx(info["solve_tuned_ms"])
     assert info["solve_schedule"] in (0, 1, 2) and info["solve_split"] in (1, 2, 4)
     _compare(outs, d, "wires32", "A3", 32)
     monkeypatch.setenv("TDEM_SOLVE_AUTOTUNE", "0")
