@@ -326,16 +326,20 @@ k_oz_update(double* __restrict__ L, double* __restrict__ U, const int64_t* __res
           break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t a0 = smem_u32(ops + st * STAGE_BYTES), b0 = a0 + A_BYTES;
-#pragma unroll 1
+        // descriptors of the stage's slice 0; the others differ only in the start
+        // address field (bits 0-13, in 16-byte units), so the fully unrolled issue
+        // below adds constants
+        const uint64_t da0 = sdesc(smem_u32(ops + st * STAGE_BYTES), 0);
+        const uint64_t db0 = sdesc(smem_u32(ops + st * STAGE_BYTES + A_BYTES), 0);
+        const uint32_t first = kb > 0 ? 1u : 0u;
+#pragma unroll
         for (int i = 0; i < OS; ++i) {
-#pragma unroll 1
-          for (int j = 0; i + j < OS; ++j) {
-            const uint32_t d = tmem + (uint32_t)(ON * (i + j));
+#pragma unroll
+          for (int j = 0; j < OS - i; ++j) {
 #pragma unroll
             for (int ks = 0; ks < OKB / 32; ++ks)
-              mma_i8(d, sdesc(a0 + i * A_SLICE, ks), sdesc(b0 + j * B_SLICE, ks),
-                     (kb > 0 || ks > 0 || i > 0) ? 1u : 0u);
+              mma_i8(tmem + (uint32_t)(ON * (i + j)), da0 + (uint64_t)((i * A_SLICE + 32 * ks) >> 4),
+                     db0 + (uint64_t)((j * B_SLICE + 32 * ks) >> 4), (ks > 0 || i > 0) ? 1u : first);
           }
         }
         mma_commit(empty0 + 8 * st);
