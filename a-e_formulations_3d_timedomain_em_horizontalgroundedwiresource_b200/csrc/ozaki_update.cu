@@ -23,10 +23,10 @@
 // 64-digit K block of all slices of the tile's 128 rows and 64 columns with two
 // TMA boxes (64 x 128 x 8 and 64 x 64 x 8 bytes) into one of two stages; warp 1
 // lane 0 issues the 2 x 36 MMAs of a stage and commits them to the stage's
-// "empty" mbarrier; warps 2-5 (tensor-memory lane groups 2, 3, 0, 1) wait for the
-// last commit, read the eight accumulators of their rows 8 columns at a time (all
-// eight tcgen05.ld before one wait), add the groups in FP64 from the smallest
-// weight up, scale by
+// "empty" mbarrier; warps 2-9 (tensor-memory lane groups 2, 3, 0, 1, twice: one
+// warp per 32 rows and 32 columns) wait for the tile's last commit, read the eight
+// accumulators of their columns 4 at a time (all eight tcgen05.ld before one wait),
+// add the groups in FP64 from the smallest weight up, scale by
 // 2^(e_a + e_b) and subtract from F.  TMA boxes read only this GPU's slice buffer
 // (no multicast).  Every mbarrier wait is bounded; a CTA that gives up records
 // err[2], waits (bounded) for its own MMAs and frees its tensor memory.
@@ -53,7 +53,9 @@ constexpr int A_BYTES = OS * A_SLICE;    // 64 KB
 constexpr int B_BYTES = OS * B_SLICE;    // 32 KB
 constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
 constexpr int NST = 2;                   // stages
-constexpr int NTHR = 192;                // producer warp, MMA warp, 4 epilogue warps
+constexpr int NTHR = 320;                // producer warp, MMA warp, 8 epilogue warps
+constexpr int NEPI = NTHR - 64;          // epilogue threads: two per tile row (32 columns each)
+constexpr int EC = ON / 2;               // columns per epilogue thread
 constexpr int TMEM_COLS = 512;           // OS accumulators of ON columns
 constexpr size_t SMEM_BYTES = 1024 /* alignment */ + (size_t)NST * STAGE_BYTES + 256 /* barriers */ +
                               (OM + ON) * sizeof(int) /* exponents */;
@@ -257,7 +259,7 @@ k_oz_update(double* __restrict__ L, double* __restrict__ U, const int64_t* __res
       mbar_init(empty0 + 8 * q, 1);  // one tcgen05.commit frees the stage
     }
     mbar_init(acc_full, 1);          // the commit after a tile's last MMAs
-    mbar_init(tmem_free, 128);       // every epilogue thread, after its tensor-memory reads
+    mbar_init(tmem_free, NEPI);      // every epilogue thread, after its tensor-memory reads
     mbar_init(done_bar, 1);
     *s_fail = 0;
     *s_issued = 0;
@@ -351,27 +353,31 @@ k_oz_update(double* __restrict__ L, double* __restrict__ U, const int64_t* __res
     // every MMA issued: arrives once they have completed
     mma_commit(done_bar);
   } else if (warp >= 2) {
-    // epilogue: rows 32 (warp % 4) + lane of each tile
-    const int sub = warp & 3, rl = 32 * sub + lane;
+    // epilogue: row 32 (warp % 4) + lane of each tile, columns [cb, cb + EC) (warps
+    // w and w + 4 share the tensor-memory lanes of their rows and split the columns)
+    const int sub = warp & 3, rl = 32 * sub + lane, cb = EC * ((warp - 2) >> 2);
     int tc = 0;
     for (int64_t id = blockIdx.x; id < ntiles; id += gridDim.x) {
       const OzTile z = oz_tile(fm, fk, fronts, prefix, aux, count, j0, id);
       if (z.skip) continue;
       const int r = z.r0 + rl;
       const int ea = ((int64_t)z.arow + rl < nrows_buf) ? exps[z.arow + rl] : 0;
+      // the exponents of this thread's 32 columns, one per lane (read before the
+      // wait, handed to the other lanes with shuffles)
+      const int ebl = ((int64_t)z.brow + cb + lane < nrows_buf) ? exps[z.brow + cb + lane] : 0;
       bool ok = mbar_wait(acc_full, (uint32_t)(tc & 1)) && *(volatile int*)s_fail == 0;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      double v[ON];
+      double v[EC];
       if (ok) {
 #pragma unroll
-        for (int cc = 0; cc < ON / 4; ++cc) {
+        for (int cc = 0; cc < EC / 4; ++cc) {
           // 4 columns of all eight group accumulators, then one wait
           uint32_t a[OS][4];
 #pragma unroll
           for (int g = 0; g < OS; ++g)
             asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];"
                          : "=r"(a[g][0]), "=r"(a[g][1]), "=r"(a[g][2]), "=r"(a[g][3])
-                         : "r"(tmem + ((uint32_t)(32 * sub) << 16) + (uint32_t)(ON * g + 4 * cc)));
+                         : "r"(tmem + ((uint32_t)(32 * sub) << 16) + (uint32_t)(ON * g + cb + 4 * cc)));
           asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
           for (int q = 0; q < 4; ++q) v[4 * cc + q] = 0.0;
@@ -388,26 +394,28 @@ k_oz_update(double* __restrict__ L, double* __restrict__ U, const int64_t* __res
       mbar_arrive(tmem_free);
       ++tc;
       if (!ok) break;
-      if (r < z.m) {
+      {
         const int64_t lo = l_off[z.s], uo = u_off[z.s];
         const int m = z.m, k = z.k;
+        const bool live = r < m;
 #pragma unroll
-        for (int h = 0; h < ON / 8; ++h) {
+        for (int h = 0; h < EC / 8; ++h) {
           double old[8];
 #pragma unroll
           for (int q = 0; q < 8; ++q) {
-            const int c = z.c0 + 8 * h + q;
+            const int c = z.c0 + cb + 8 * h + q;
             old[q] = 0.0;
-            if (c < m && c <= r)
+            if (live && c < m && c <= r)
               old[q] = (c < k) ? L[lo + r + (int64_t)c * m] : U[uo + (r - k) + (int64_t)(c - k) * (m - k)];
           }
 #pragma unroll
           for (int q = 0; q < 8; ++q) {
-            const int c = z.c0 + 8 * h + q;
-            if (c < m && c <= r) {
-              const int eb = ((int64_t)z.brow + 8 * h + q < nrows_buf) ? exps[z.brow + 8 * h + q] : 0;
+            const int cl = 8 * h + q, c = z.c0 + cb + cl;
+            // every lane takes part in the shuffle
+            const int eb = __shfl_sync(0xffffffffu, ebl, cl);
+            if (live && c < m && c <= r) {
               double* e = (c < k) ? L + lo + r + (int64_t)c * m : U + uo + (r - k) + (int64_t)(c - k) * (m - k);
-              *e = old[q] - ldexp(v[8 * h + q], ea + eb);
+              *e = old[q] - ldexp(v[cl], ea + eb);
             }
           }
         }
