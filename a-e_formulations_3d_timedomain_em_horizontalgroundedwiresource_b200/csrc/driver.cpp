@@ -384,6 +384,14 @@ std::string TransientSolve::setup_device(cudaStream_t stream) {
   if (const char* oz = std::getenv("TDEM_OZAKI")) chol_->set_ozaki(oz[0] != '0');
   chol_->set_ozaki_timing(true);
   int slots = opt_.factor_slots;
+  // The integer-pipe trailing update holds 199 KB of shared memory per CTA, so it
+  // cannot share an SM with a level-solve CTA: a factorization ahead of use then
+  // only interleaves with the steps instead of overlapping them (measured at 80^3:
+  // 0.151 forward solves/s with two slots, 0.155 with one).  Auto picks one slot
+  // when the analysis put trailing updates on that path.
+  const char* oz_env = std::getenv("TDEM_OZAKI");
+  const bool oz_planned = sy_->oz_rows_max > 0 && factor_bytes() == 8 && !(oz_env && oz_env[0] == '0');
+  if (slots == 0 && oz_planned) slots = 1;
   if (slots == 0) {
     size_t free_b = 0, total_b = 0;
     TRY_CUDA(cudaMemGetInfo(&free_b, &total_b));
