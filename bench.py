@@ -31,6 +31,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 PKG = "a-e_formulations_3d_timedomain_em_horizontalgroundedwiresource_b200"
 METRIC = "forward solves/s + p50/p99 latency, mixed vs FP64 GPU, ≤1e-5 rel. error"
+# k_oz_update, one launch of the 40^3 half-space (ncu --set full, profiles/k_oz_update_c1.md):
+# DRAM bytes read + written and 8-bit tensor ops of that launch
+OZ_CAPTURE_DRAM_BYTES = 342.647296e6 + 200.931328e6
+OZ_CAPTURE_OPS = 493753466880.0
 
 
 # ---------------------------------------------------------------------------
@@ -448,12 +452,22 @@ def run_ours(args, world, rank, local):
                 ops = 2.0 * inf["ozaki_macs"] * n_fact * units
                 ach = ops / (oz_ms * 1e-3) / 1e12
                 pk = 2.0 * bf16 if bf16 else 2.0 * 1590.0
+                # DRAM bytes per 8-bit op of one captured launch (ncu, 40^3 half-space:
+                # profiles/k_oz_update_c1.md), scaled to a factorization's ops: the traffic is
+                # the read-modify-write of the trailing tiles, which grows with the tiles as the
+                # ops do
+                traffic = OZ_CAPTURE_DRAM_BYTES / OZ_CAPTURE_OPS * 2.0 * inf["ozaki_macs"]
                 roof_oz = {"bound": "tensor", "kernel": "k_oz_update (tcgen05 kind::i8, FP64 trailing updates by "
-                                                        "digit splitting)",
+                                                        "digit splitting; the dominant kernel)",
                            "achieved": ach, "peak": pk, "unit": "TOP/s (int8)", "frac": ach / pk,
-                           "ops_per_factorization": 2.0 * inf["ozaki_macs"],
-                           "ms_per_factorization": oz_ms / max(units * n_fact, 1),
-                           "peak_source": ("2 x MEASURED_PEAKS.json bf16_tflops (measured bf16 burst)" if bf16
+                           "ops_per_launch": 2.0 * inf["ozaki_macs"],
+                           "launch": "all k_oz_update launches of one factorization",
+                           "avg_launch_ms": oz_ms / max(units * n_fact, 1),
+                           "traffic": traffic,
+                           "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 40^3 launch "
+                                             "(profiles/k_oz_update_c1.md), scaled by 8-bit ops",
+                           "peak_source": ("2 x MEASURED_PEAKS.json bf16_tflops (measured bf16 burst; B200's dense "
+                                           "8-bit rate is twice its bf16 rate)" if bf16
                                            else "2 x fallback 1590 TF/s bf16")}
             cpu = None
             parity = None
@@ -511,9 +525,11 @@ def run_ours(args, world, rank, local):
                 "wall_s": wall,
                 "gpu_launches": launches,
                 "clocks": clocks,
-                "roofline": roof,
+                # the dominant kernel: the integer-pipe trailing update when the factorization
+                # uses it, else the factorization as a whole on the FP64 pipes
+                "roofline": roof_oz if roof_oz else roof,
+                "roofline_factorization": roof,
                 "roofline_solve": roof_solve,
-                "roofline_ozaki": roof_oz,
                 "cpu_baseline": cpu,
                 "parity": parity,
                 "e2e": e2e,
