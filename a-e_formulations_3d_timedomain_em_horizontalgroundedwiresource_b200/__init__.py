@@ -106,7 +106,7 @@ class TdemPlanInfo(ctypes.Structure):
                 ("factor_slot_bytes", ctypes.c_int64), ("solve_units", ctypes.c_int64), ("n_fronts", ctypes.c_int),
                 ("tree_levels", ctypes.c_int), ("n_sources", ctypes.c_int), ("n_times", ctypes.c_int),
                 ("plan_seconds", ctypes.c_double), ("digest", ctypes.c_uint64), ("ozaki_flops", ctypes.c_double),
-                ("ozaki_rows", ctypes.c_int64)]
+                ("ozaki_rows", ctypes.c_int64), ("solve_chain", ctypes.c_int64)]
 
     def as_dict(self) -> dict:
         return {n: getattr(self, n) for n, _ in self._fields_}

@@ -203,6 +203,12 @@ tdem_status tdem_solver_plan(const char* workdir, int formulation, int scheme, c
     out->digest = tdem::plan_digest(*sy);
     out->ozaki_flops = sy->oz_flops;
     out->ozaki_rows = sy->oz_rows_max;
+    out->solve_chain = 0;
+    for (const tdem::LevelPlan& lp : sy->levels) {
+      int64_t mx = 0;
+      for (int f : lp.fronts) mx = std::max<int64_t>(mx, (sy->front_k[f] + tdem::kPanel - 1) / tdem::kPanel);
+      out->solve_chain += mx;
+    }
     return TDEM_OK;
   }, err, err_len);
 }

@@ -173,8 +173,9 @@ typedef struct tdem_info {
   int factor_slots;         /* numeric factors held (2: factorizations overlapped the steps;
                                factor_gpu_ms and solve_gpu_ms then overlap in run_gpu_ms) */
   int solve_schedule;       /* per-step solve of the n_sources columns: 0 fused level solves,
-                               1 panel solves (chosen by the solve autotuner for more than two
-                               columns, measured on the first step of the first run) */
+                               1 panel solves, 2 persistent fused level solves (chosen by the
+                               solve autotuner for more than two columns, measured on the first
+                               step of the first run) */
   int solve_split;          /* column groups that solve is split into */
   int solve_candidates;     /* schedules the autotuner measured (0: not tuned) */
   double solve_tuned_ms;    /* the chosen schedule's measured device time per solve */
@@ -242,6 +243,9 @@ typedef struct tdem_plan_info {
   double ozaki_flops;       /* flops of the trailing updates planned on the integer tensor
                                pipe (FP64 products by digit splitting; FP64 solvers) */
   int64_t ozaki_rows;       /* rows of the digit buffer those updates need */
+  int64_t solve_chain;      /* 64-wide pivot blocks on the critical path of one triangular
+                               solve direction: the sum over the tree levels of the largest
+                               front's pivot blocks (each is one dependent link) */
 } tdem_plan_info;
 tdem_status tdem_solver_plan(const char* workdir, int formulation, int scheme, const tdem_options* opts,
                              tdem_plan_info* out, char* err, size_t err_len);

@@ -15,6 +15,8 @@ def _counts_consistent(p):
     assert p["factor_slot_bytes"] >= 8 * p["nnz_factor"]
     assert p["factor_flops"] > 0 and p["solve_units"] > 0
     assert p["n_fronts"] > 0 and p["tree_levels"] >= 1
+    # one dependent 64-wide link per level at least, never more than all pivot blocks
+    assert p["tree_levels"] <= p["solve_chain"] <= p["n_interior"] // 64 + p["n_fronts"]
 
 
 @pytest.mark.parametrize("cells,form,scheme", [(8, "A", 2), (10, "E", 3), (14, "A", 3), (16, "E", 2)])
