@@ -122,33 +122,39 @@ __global__ void k_combine(const double* __restrict__ C, const double* __restrict
   }
 }
 
-// One warp per row.
+// Eight lanes per row, four rows per warp: a row holds about 33 entries, so each
+// lane takes four or five of them (a warp per row would leave most lanes idle on
+// the second pass and spend five shuffle steps per row), and three shuffle steps
+// within the group of eight combine the lanes.  Every lane reaches the shuffles.
+constexpr int kRhsLanes = 8;
 __global__ void k_history_rhs(const int64_t* __restrict__ rowptr, const int* __restrict__ col,
                               const double* __restrict__ C, const double* __restrict__ u1,
                               const double* __restrict__ u2, double m1c, double m2c,
                               const double* __restrict__ S, double coef, const uint8_t* __restrict__ bound,
                               int n, int npls, double* __restrict__ rhs) {
-  const int row = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
-  const int lane = threadIdx.x & 31;
-  if (row >= n) return;
-  if (bound[row]) {
-    for (int p = lane; p < npls; p += 32) rhs[row + (int64_t)p * n] = 0.0;
-    return;
+  const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int row = (int)(tid / kRhsLanes);
+  const int sub = threadIdx.x & (kRhsLanes - 1);
+  const bool live = row < n;
+  const bool zero = live && bound[row] != 0;
+  int64_t b = 0, e = 0;
+  if (live && !zero) {
+    b = __ldg(rowptr + row);
+    e = __ldg(rowptr + row + 1);
   }
-  const int64_t b = rowptr[row], e = rowptr[row + 1];
   for (int p = 0; p < npls; ++p) {
     const double* a1 = u1 + (int64_t)p * n;
     const double* a2 = u2 + (int64_t)p * n;
     double acc = 0.0;
-    for (int64_t q = b + lane; q < e; q += 32) {
-      const int j = col[q];
-      acc = fma(C[q], a1[j] * m1c + a2[j] * m2c, acc);
+    for (int64_t q = b + sub; q < e; q += kRhsLanes) {
+      const int j = __ldg(col + q);
+      acc = fma(__ldg(C + q), a1[j] * m1c + a2[j] * m2c, acc);
     }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-    if (lane == 0) {
-      double v = acc;
-      if (coef != 0.0) v += coef * S[row + (int64_t)p * n];
+    for (int o = kRhsLanes / 2; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o, kRhsLanes);
+    if (live && sub == 0) {
+      double v = zero ? 0.0 : acc;
+      if (!zero && coef != 0.0) v += coef * S[row + (int64_t)p * n];
       rhs[row + (int64_t)p * n] = v;
     }
   }
@@ -438,13 +444,15 @@ void launch_combine(const double* Cval, const double* Bval, const int64_t* src, 
 void launch_history_rhs(const int64_t* rowptr, const int* col, const double* Cval, const double* u1,
                         const double* u2, double m1c, double m2c, const double* S, double coef,
                         const uint8_t* bound, int n, int npls, double* rhs, cudaStream_t s) {
-  const int64_t threads = (int64_t)n * 32;
-  if (npls > 1)
+  if (npls > 1) {
+    const int64_t threads = (int64_t)n * 32;
     k_history_rhs_multi<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(rowptr, col, Cval, u1, u2, m1c, m2c, S,
                                                                           coef, bound, n, npls, rhs);
-  else
+  } else {
+    const int64_t threads = (int64_t)n * kRhsLanes;
     k_history_rhs<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(rowptr, col, Cval, u1, u2, m1c, m2c, S, coef,
                                                                     bound, n, npls, rhs);
+  }
 }
 
 void launch_normal_field(const float* f, const int* idx, const double* len, int nanom, int n, int npls, double* En,

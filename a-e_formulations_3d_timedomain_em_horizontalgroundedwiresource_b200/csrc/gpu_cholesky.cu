@@ -112,11 +112,18 @@ __global__ void k_extend_add(T* __restrict__ L, T* __restrict__ U, Fronts f, con
 // unchanged throughout its step.  Same operations in the same order per element
 // as a column-at-a-time factorization: the result does not depend on the thread
 // layout.
+// With dinv (FP64 factorization) the CTA also inverts the finished block into the
+// front's inverted diagonal blocks (dinv_off[s] + 64 * 64 * (j0 / 64), column-major,
+// leading dimension w): the operand of the panel solve k_trsm_dmma and of the
+// triangular solves, by the substitution and operation order of k_diag_inverse.
 template <class T>
 __global__ void __launch_bounds__(256) k_potrf(T* __restrict__ L, Fronts f, const int* __restrict__ fronts, int j0,
-                                               int* __restrict__ err, const int* __restrict__ c0_of) {
+                                               int* __restrict__ err, const int* __restrict__ c0_of,
+                                               T* __restrict__ dinv = nullptr,
+                                               const int64_t* __restrict__ dinv_off = nullptr) {
   __shared__ T A[P][P + 1];
   __shared__ T diag[P];
+  __shared__ T xd[P];
   const int s = fronts[blockIdx.x];
   const int m = f.m[s], k = f.k[s];
   const int w = min(P, k - j0);
@@ -148,6 +155,32 @@ __global__ void __launch_bounds__(256) k_potrf(T* __restrict__ L, Fronts f, cons
   for (int idx = threadIdx.x; idx < w * w; idx += blockDim.x) {
     const int r = idx % w, c = idx / w;
     if (r >= c) F[(j0 + r) + (int64_t)(j0 + c) * m] = (r == c) ? diag[c] : A[c][r];
+  }
+  if (dinv == nullptr) return;
+  // L(r, c) = A[c][r] (r > c) or diag[r]; the inverse X(r, c) (r > c) goes to the
+  // lower triangle, whose working values are dead, and its diagonal to xd.  Four
+  // threads per column c run X(r, c) = -(sum_{c <= l < r} L(r, l) X(l, c)) / L(r, r).
+  {
+    const int c = threadIdx.x >> 2, part = threadIdx.x & 3;
+    const unsigned mask = 0xFu << ((threadIdx.x & 31) & ~3);
+    if (c < w) {
+      if (part == 0) xd[c] = (T)1 / diag[c];
+      __syncwarp(mask);
+      for (int r = c + 1; r < w; ++r) {
+        T sum = (T)0;
+        for (int l = c + part; l < r; l += 4) sum = fma(A[l][r], l == c ? xd[c] : A[l][c], sum);
+        sum += __shfl_xor_sync(mask, sum, 1);
+        sum += __shfl_xor_sync(mask, sum, 2);
+        if (part == 0) A[r][c] = -sum / diag[r];
+        __syncwarp(mask);
+      }
+    }
+  }
+  __syncthreads();
+  T* D = dinv + dinv_off[s] + (int64_t)(j0 / P) * P * P;
+  for (int q = threadIdx.x; q < w * w; q += blockDim.x) {
+    const int r = q % w, c = q / w;
+    D[q] = (r > c) ? A[r][c] : (r == c ? xd[c] : (T)0);
   }
 }
 
@@ -402,6 +435,82 @@ __device__ __forceinline__ void dmma16816(double (&c)[4], const double (&a)[8], 
       : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
       : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]), "d"(b[0]),
         "d"(b[1]), "d"(b[2]), "d"(b[3]));
+}
+
+// Panel triangular solve on the FP64 tensor pipe: rows [j1, m) of the panel columns
+// times L_dd^-T, with L_dd^-1 the inverse k_potrf wrote (dinv_off[s] + 64 * 64 *
+// (j0 / 64), column-major, leading dimension w).  kTrsmRows = 128 rows per CTA
+// (the task list of k_trsm), 256 threads: warp v owns rows 16 v .. 16 v + 15 and
+// all 64 columns (8 MMA tiles of m16n8k16), K = the 64 panel columns.  The rows are
+// staged k-major (stride 4 mod 16 doubles: conflict-free fragment loads), the
+// product is staged back the same way and written column by column, coalesced.
+// A substitution would chain 64 dependent steps per row; the product has none.
+constexpr int kLdT = kTrsmRows + 4;  // 132
+constexpr int kLdI = P + 4;          // 68
+constexpr size_t trsm_dmma_smem() { return sizeof(double) * P * (kLdT + kLdI); }
+
+__global__ void __launch_bounds__(256) k_trsm_dmma(double* __restrict__ L, Fronts f, const int* __restrict__ fronts,
+                                                   const int64_t* __restrict__ prefix, int count, int j0,
+                                                   const double* __restrict__ dinv,
+                                                   const int64_t* __restrict__ dinv_off) {
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  double(*As)[kLdT] = reinterpret_cast<double(*)[kLdT]>(sm_raw);                          // As[l][row]
+  double(*Bs)[kLdI] = reinterpret_cast<double(*)[kLdI]>(sm_raw + sizeof(double) * P * kLdT);  // Bs[l][c]
+  const int idx = find_task(prefix, count, blockIdx.x);
+  const int s = fronts[idx];
+  const int m = f.m[s], k = f.k[s];
+  const int w = min(P, k - j0), j1 = j0 + w;
+  double* F = L + f.l_off[s];
+  const int row0 = j1 + (int)(blockIdx.x - prefix[idx]) * kTrsmRows;
+  const int t = threadIdx.x;
+  // rows: thread t reads row t % 128 of columns t / 128 + 2 e
+  {
+    const int r = t & (kTrsmRows - 1), l0 = t >> 7;
+    const bool live = row0 + r < m;
+#pragma unroll 8
+    for (int l = l0; l < P; l += 2) As[l][r] = (live && l < w) ? F[(row0 + r) + (int64_t)(j0 + l) * m] : 0.0;
+  }
+  // B(l, c) = L_dd^-1(c, l) = D[c + l w] (zero above the diagonal and outside w)
+  {
+    const double* D = dinv + dinv_off[s] + (int64_t)(j0 / P) * P * P;
+    for (int q = t; q < P * P; q += 256) {
+      const int c = q & (P - 1), l = q >> 6;
+      Bs[l][c] = (c < w && l < w) ? D[c + l * w] : 0.0;
+    }
+  }
+  __syncthreads();
+  const int lane = t & 31, warp = t >> 5, g = lane >> 2, q = lane & 3;
+  double acc[8][4];
+#pragma unroll
+  for (int j = 0; j < 8; ++j)
+#pragma unroll
+    for (int e = 0; e < 4; ++e) acc[j][e] = 0.0;
+#pragma unroll
+  for (int k16 = 0; k16 < P; k16 += 16) {
+    double af[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) af[i] = As[k16 + q + 4 * (i >> 1)][16 * warp + g + 8 * (i & 1)];
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) {
+      double bf[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) bf[i] = Bs[k16 + q + 4 * i][8 * nt + g];
+      dmma16816(acc[nt], af, bf);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int nt = 0; nt < 8; ++nt)
+#pragma unroll
+    for (int i = 0; i < 4; ++i) As[8 * nt + 2 * q + (i & 1)][16 * warp + g + 8 * (i >> 1)] = acc[nt][i];
+  __syncthreads();
+  {
+    const int r = t & (kTrsmRows - 1), l0 = t >> 7;
+    if (row0 + r < m) {
+#pragma unroll 8
+      for (int l = l0; l < w; l += 2) F[(row0 + r) + (int64_t)(j0 + l) * m] = As[l][r];
+    }
+  }
 }
 
 // One 128 x 64 tile of F -= X X^T on the FP64 tensor pipe: rows [r0, r0 + 128)
@@ -2216,6 +2325,8 @@ std::string set_attributes() {
   TDEM_CUDA_TRY(cudaFuncSetAttribute(k_syrk_big<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big_smem<T>()));
   TDEM_CUDA_TRY(cudaFuncSetAttribute(k_syrk_big_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dmma_smem()));
   TDEM_CUDA_TRY(cudaFuncSetAttribute(k_panel_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dmma_smem()));
+  TDEM_CUDA_TRY(
+      cudaFuncSetAttribute(k_trsm_dmma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_dmma_smem()));
   TDEM_CUDA_TRY(cudaFuncSetAttribute(k_fwd_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
   TDEM_CUDA_TRY(cudaFuncSetAttribute(k_bwd_diag<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
   TDEM_CUDA_TRY(cudaFuncSetAttribute(k_fwd_update<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
@@ -2227,7 +2338,10 @@ int launch_factor(const Symbolic& sy, T* L, T* U, const double* vals, const int6
                   const int* parent, const int64_t* rel_off, const int* rel, const int* tasks,
                   const int64_t* prefix, int* err, const int* c0, bool use_tc, cudaStream_t s,
                   const OzakiBuffers* oz = nullptr, const int64_t* aux = nullptr,
-                  std::vector<cudaEvent_t>* oz_ev = nullptr, size_t* oz_used = nullptr) {
+                  std::vector<cudaEvent_t>* oz_ev = nullptr, size_t* oz_used = nullptr, T* dinv = nullptr,
+                  const int64_t* dinv_off = nullptr) {
+  // dinv (FP64): k_potrf also writes the inverted diagonal blocks, and the panel
+  // solves run on the FP64 tensor pipe with them (k_trsm_dmma)
   int launches = 0;
   cudaMemsetAsync(L, 0, sizeof(T) * sy.nnz_l, s);
   {
@@ -2251,11 +2365,20 @@ int launch_factor(const Symbolic& sy, T* L, T* U, const double* vals, const int6
       ++launches;
     }
     for (const PanelStep& ps : lp.panels) {
-      k_potrf<T><<<ps.potrf.count, 256, 0, s>>>(L, fr, tasks + ps.potrf.off, ps.j0, err, c0);
+      k_potrf<T><<<ps.potrf.count, 256, 0, s>>>(L, fr, tasks + ps.potrf.off, ps.j0, err, c0, dinv, dinv_off);
       ++launches;
       if (ps.trsm.ctas > 0) {
-        k_trsm<T><<<grid_of(ps.trsm.ctas), kTrsmRows, 0, s>>>(L, fr, tasks + ps.trsm.off,
-                                                                           prefix + ps.trsm.pre, ps.trsm.count, ps.j0);
+        bool done = false;
+        if constexpr (std::is_same<T, double>::value) {
+          if (dinv) {
+            k_trsm_dmma<<<grid_of(ps.trsm.ctas), 256, trsm_dmma_smem(), s>>>(
+                L, fr, tasks + ps.trsm.off, prefix + ps.trsm.pre, ps.trsm.count, ps.j0, dinv, dinv_off);
+            done = true;
+          }
+        }
+        if (!done)
+          k_trsm<T><<<grid_of(ps.trsm.ctas), kTrsmRows, 0, s>>>(L, fr, tasks + ps.trsm.off, prefix + ps.trsm.pre,
+                                                                ps.trsm.count, ps.j0);
         ++launches;
       }
       if (ps.syrk.ctas > 0) {
@@ -2667,12 +2790,8 @@ void GpuCholesky::factor(const double* d_vals, cudaStream_t s, int slot) {
     launches_factor_ = launch_factor<double>(sy_, (double*)d_Lw_, (double*)d_U_, d_vals, d_entry_, fr, d_parent_,
                                              d_rel_off_, d_rel_, d_tasks_, d_prefix_, d_err_, d_c0_, false, s,
                                              ozaki() ? &oz_ : nullptr, d_task_aux_,
-                                             oz_timing_ ? &oz_events_ : nullptr, &oz_used_);
-    if (ni) {
-      k_diag_inverse<double><<<ni, 256, ism, s>>>((const double*)d_Lw_, (double*)d_dinvw_, fr, d_dinv_off_,
-                                                  d_items_ + 2 * sy_.inv_off);
-      ++launches_factor_;
-    }
+                                             oz_timing_ ? &oz_events_ : nullptr, &oz_used_, (double*)d_dinvw_,
+                                             d_dinv_off_);
     const int64_t nl = std::max<int64_t>(1, sy_.nnz_l), nd = std::max<int64_t>(1, sy_.dinv_elems);
     k_round_to_float<<<(unsigned)std::min<int64_t>((nl / 2 + 255) / 256, 148 * 16), 256, 0, s>>>(
         (const double*)d_Lw_, (float*)Lp, nl);
@@ -2690,9 +2809,9 @@ void GpuCholesky::factor(const double* d_vals, cudaStream_t s, int slot) {
     launches_factor_ = launch_factor<double>(sy_, (double*)Lp, (double*)d_U_, d_vals, d_entry_, fr, d_parent_,
                                              d_rel_off_, d_rel_, d_tasks_, d_prefix_, d_err_, d_c0_, false, s,
                                              ozaki() ? &oz_ : nullptr, d_task_aux_,
-                                             oz_timing_ ? &oz_events_ : nullptr, &oz_used_);
-    if (ni) k_diag_inverse<double><<<ni, 256, ism, s>>>((const double*)Lp, (double*)Dp, fr, d_dinv_off_,
-                                                        d_items_ + 2 * sy_.inv_off);
+                                             oz_timing_ ? &oz_events_ : nullptr, &oz_used_, (double*)Dp,
+                                             d_dinv_off_);
+    return;
   }
   if (ni) ++launches_factor_;
 }
