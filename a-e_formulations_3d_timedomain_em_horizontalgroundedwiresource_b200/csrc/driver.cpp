@@ -384,14 +384,14 @@ std::string TransientSolve::setup_device(cudaStream_t stream) {
   if (const char* oz = std::getenv("TDEM_OZAKI")) chol_->set_ozaki(oz[0] != '0');
   chol_->set_ozaki_timing(true);
   int slots = opt_.factor_slots;
-  // The integer-pipe trailing update holds 199 KB of shared memory per CTA, so it
-  // cannot share an SM with a level-solve CTA: a factorization ahead of use then
-  // only interleaves with the steps instead of overlapping them (measured at 80^3:
-  // 0.151 forward solves/s with two slots, 0.155 with one).  Auto picks one slot
-  // when the analysis put trailing updates on that path.
+  // The integer-pipe trailing update holds 199 KB of shared memory and 168 x 320
+  // registers per CTA, so it cannot share an SM with a level-solve CTA; a
+  // factorization ahead of use still fills the SMs its panel chain (one front's
+  // 64-column steps at a time) leaves idle.  Measured at 80^3 (E-form, BDF2, 160
+  // steps): one slot 0.161 forward solves/s; two slots with the level solves kept
+  // to one CTA per SM 0.157, with their full two CTAs per SM 0.169.
   const char* oz_env = std::getenv("TDEM_OZAKI");
   const bool oz_planned = sy_->oz_rows_max > 0 && factor_bytes() == 8 && !(oz_env && oz_env[0] == '0');
-  if (slots == 0 && oz_planned) slots = 1;
   if (slots == 0) {
     size_t free_b = 0, total_b = 0;
     TRY_CUDA(cudaMemGetInfo(&free_b, &total_b));
@@ -421,9 +421,10 @@ std::string TransientSolve::setup_device(cudaStream_t stream) {
     else
       return "TDEM_SOLVE_SCHEDULE must be \"kind,split\" with kind 0, 1 or 2";
   }
-  // with a factorization running beside the steps, the level solves keep one CTA
-  // per SM so the factor kernels can share every SM
-  if (slots > 1) chol_->set_solve_ctas_per_sm(1);
+  // with a factorization on the FP64 tensor pipe running beside the steps, the level
+  // solves keep one CTA per SM so its kernels can share every SM (with the
+  // integer-pipe update they keep their two, see above)
+  if (slots > 1 && !oz_planned) chol_->set_solve_ctas_per_sm(1);
   const RunOptions& opt = opt_;
 
   // device buffers

@@ -42,6 +42,47 @@ def test_dense_front_on_the_integer_pipe(pkg):
     pkg.pardiso_64(h, -1, a, ia, ja)
 
 
+def test_large_dense_front_on_the_integer_pipe(pkg):
+    """12,000 pivots in one front: the first trailing update (11,488 rows, K = 512,
+    8,190 output tiles of 128 x 64 for 148 persistent CTAs) has the shape of the
+    large 80^3 updates, so this is also the case the kernel is profiled on.  The
+    matrix is D (3 I + (B + B^T) / sqrt(2 n)) D with Gaussian B (eigenvalues of the
+    inner matrix within about [1, 5]) and row scales over six decades; the check is
+    the componentwise-scaled residual, which an FP64 backward-stable solve keeps
+    near n u."""
+    n = 12000
+    rng = np.random.default_rng(23)
+    A = rng.standard_normal((n, n))
+    A += A.T
+    A *= 1.0 / np.sqrt(2.0 * n)
+    A[np.diag_indices(n)] += 3.0
+    dsc = 10.0 ** rng.uniform(-3, 3, n)
+    A *= dsc[:, None]
+    A *= dsc[None, :]
+    # 1-based upper CSR, row by row (a dense 12,000^2 matrix through scipy.sparse
+    # would need several copies of it)
+    counts = np.arange(n, 0, -1, dtype=np.int64)
+    ia = np.empty(n + 1, dtype=np.int64)
+    ia[0] = 1
+    np.cumsum(counts, out=ia[1:])
+    ia[1:] += 1
+    a = np.empty(ia[-1] - 1)
+    ja = np.empty(ia[-1] - 1, dtype=np.int64)
+    cols = np.arange(1, n + 1, dtype=np.int64)
+    for i in range(n):
+        a[ia[i] - 1:ia[i + 1] - 1] = A[i, i:]
+        ja[ia[i] - 1:ia[i + 1] - 1] = cols[i:]
+    h = np.zeros(64, dtype=np.int64)
+    assert pkg.pardiso_64(h, 12, a, ia, ja, nrhs=1) == 0
+    b = rng.standard_normal((1, n))
+    x = np.zeros_like(b)
+    assert pkg.pardiso_64(h, 33, a, ia, ja, nrhs=1, b=b, x=x) == 0
+    pkg.pardiso_64(h, -1, a, ia, ja)
+    r = A @ x[0] - b[0]
+    scale = np.abs(A) @ np.abs(x[0]) + np.abs(b[0])
+    assert np.max(np.abs(r) / scale) <= 1e-11
+
+
 @pytest.mark.parametrize("variant", ["A2", "A3", "E2", "E3"])
 @pytest.mark.parametrize("case", ["cube8_block", "cube8_two_wires"])
 def test_every_trailing_update_on_the_integer_pipe(pkg, golden, outs, tmp_path, monkeypatch, case, variant):
