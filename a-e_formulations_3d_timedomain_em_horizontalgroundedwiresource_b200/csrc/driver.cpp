@@ -412,6 +412,7 @@ std::string TransientSolve::setup_device(cudaStream_t stream) {
   sy_.reset();
   if (!e.empty()) return e;
   if (const char* ps = std::getenv("TDEM_PANEL_SOLVE")) chol_->set_panel_solve(ps[0] == '1');
+  if (const char* la = std::getenv("TDEM_LOOKAHEAD")) chol_->set_lookahead(la[0] != '0');
   if (const char* at = std::getenv("TDEM_SOLVE_AUTOTUNE")) chol_->set_autotune(at[0] != '0');
   if (const char* fs = std::getenv("TDEM_SOLVE_SCHEDULE")) {  // "kind,split": a fixed schedule
     SolveSchedule sc;

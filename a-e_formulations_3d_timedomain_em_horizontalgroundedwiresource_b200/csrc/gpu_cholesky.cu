@@ -650,7 +650,7 @@ __global__ void __launch_bounds__(kBigThreads, 2) k_syrk_big_dmma(double* __rest
 __global__ void __launch_bounds__(kBigThreads, 2) k_panel_dmma(double* __restrict__ L, double* __restrict__ U,
                                                                 Fronts f, const int* __restrict__ fronts,
                                                                 const int64_t* __restrict__ prefix, int count,
-                                                                int j0) {
+                                                                int j0, int bj0 = 0) {
   extern __shared__ __align__(16) unsigned char sm_raw[];
   const int idx = find_task(prefix, count, blockIdx.x);
   const int s = fronts[idx];
@@ -658,7 +658,8 @@ __global__ void __launch_bounds__(kBigThreads, 2) k_panel_dmma(double* __restric
   const int w = min(kPanel, k - j0), j1 = j0 + w;
   const int J0 = (j0 / kOuter) * kOuter, J1 = min(k, J0 + kOuter);
   const int nr = (m - j1 + kTileBig - 1) / kTileBig;
-  int t = (int)(blockIdx.x - prefix[idx]), bj = 0;
+  // tiles from column tile bj0 on (the task list's counts say how many)
+  int t = (int)(blockIdx.x - prefix[idx]), bj = bj0;
   while (t >= nr - bj / 2) {
     t -= nr - bj / 2;
     ++bj;
@@ -2333,16 +2334,32 @@ std::string set_attributes() {
   return "";
 }
 
+// Look-ahead of the FP64 panel chain: the update of the outer panel's columns
+// right of the next inner panel (syrk_rest) runs on a side stream while the main
+// stream factors and solves the next panel.  Per inner panel j:
+//   main: potrf_j, trsm_j, wait(rest_{j-1}), record(solved), next_j
+//   side: wait(solved), rest_j, record(rest)
+// rest_{j-1} and next_j write the same columns (panel j + 1), hence the wait;
+// rest_j touches neither panel j + 1 nor the trailing columns of the outer panel
+// (the syrk_big input is final once every rest with work has been waited for by
+// the next next_; a rest of the outer panel's last two inner panels has none).
+// The side stream joins the main one at the end.
+struct LookAhead {
+  cudaStream_t side = nullptr;
+  cudaEvent_t solved = nullptr, rest = nullptr, join = nullptr;
+};
+
 template <class T>
 int launch_factor(const Symbolic& sy, T* L, T* U, const double* vals, const int64_t* entry, Fronts fr,
                   const int* parent, const int64_t* rel_off, const int* rel, const int* tasks,
                   const int64_t* prefix, int* err, const int* c0, bool use_tc, cudaStream_t s,
                   const OzakiBuffers* oz = nullptr, const int64_t* aux = nullptr,
                   std::vector<cudaEvent_t>* oz_ev = nullptr, size_t* oz_used = nullptr, T* dinv = nullptr,
-                  const int64_t* dinv_off = nullptr) {
+                  const int64_t* dinv_off = nullptr, const LookAhead* la = nullptr) {
   // dinv (FP64): k_potrf also writes the inverted diagonal blocks, and the panel
   // solves run on the FP64 tensor pipe with them (k_trsm_dmma)
   int launches = 0;
+  bool rest_pending = false, side_used = false;
   cudaMemsetAsync(L, 0, sizeof(T) * sy.nnz_l, s);
   {
     const int64_t nnz = sy.nnz_lower;
@@ -2382,10 +2399,26 @@ int launch_factor(const Symbolic& sy, T* L, T* U, const double* vals, const int6
         ++launches;
       }
       if (ps.syrk.ctas > 0) {
-        if constexpr (std::is_same<T, double>::value)
-          k_panel_dmma<<<grid_of(ps.syrk_wide.ctas), kBigThreads, dmma_smem(), s>>>(
-              L, U, fr, tasks + ps.syrk_wide.off, prefix + ps.syrk_wide.pre, ps.syrk_wide.count, ps.j0);
-        else
+        if constexpr (std::is_same<T, double>::value) {
+          if (la && la->side) {
+            if (rest_pending) cudaStreamWaitEvent(s, la->rest, 0);
+            rest_pending = false;
+            if (ps.syrk_rest.ctas > 0) {
+              cudaEventRecord(la->solved, s);
+              cudaStreamWaitEvent(la->side, la->solved, 0);
+              k_panel_dmma<<<grid_of(ps.syrk_rest.ctas), kBigThreads, dmma_smem(), la->side>>>(
+                  L, U, fr, tasks + ps.syrk_rest.off, prefix + ps.syrk_rest.pre, ps.syrk_rest.count, ps.j0, 1);
+              cudaEventRecord(la->rest, la->side);
+              rest_pending = side_used = true;
+              ++launches;
+            }
+            k_panel_dmma<<<grid_of(ps.syrk_next.ctas), kBigThreads, dmma_smem(), s>>>(
+                L, U, fr, tasks + ps.syrk_next.off, prefix + ps.syrk_next.pre, ps.syrk_next.count, ps.j0, 0);
+          } else {
+            k_panel_dmma<<<grid_of(ps.syrk_wide.ctas), kBigThreads, dmma_smem(), s>>>(
+                L, U, fr, tasks + ps.syrk_wide.off, prefix + ps.syrk_wide.pre, ps.syrk_wide.count, ps.j0, 0);
+          }
+        } else
           k_syrk_panel<T><<<grid_of(ps.syrk.ctas), 256, syrk_smem<T>(), s>>>(L, fr, tasks + ps.syrk.off,
                                                                              prefix + ps.syrk.pre, ps.syrk.count,
                                                                              ps.j0);
@@ -2430,6 +2463,10 @@ int launch_factor(const Symbolic& sy, T* L, T* U, const double* vals, const int6
         ++launches;
       }
     }
+  }
+  if (side_used) {
+    cudaEventRecord(la->join, la->side);
+    cudaStreamWaitEvent(s, la->join, 0);
   }
   return launches;
 }
@@ -2665,6 +2702,9 @@ std::string set_fused_attributes() {
 GpuCholesky::~GpuCholesky() {
   for (SolveGraph& g : graph_)
     if (g.exec) cudaGraphExecDestroy(g.exec);
+  for (cudaEvent_t e : la_ev_)
+    if (e) cudaEventDestroy(e);
+  if (la_side_) cudaStreamDestroy(la_side_);
   for (cudaEvent_t e : oz_events_) cudaEventDestroy(e);
   for (void* p : allocs_) cudaFree(p);
 }
@@ -2779,8 +2819,41 @@ std::string GpuCholesky::setup(Symbolic&& sy, const std::vector<int>& perm_to_ve
   return "";
 }
 
+bool GpuCholesky::lookahead_ready(cudaStream_t s) {
+  if (!lookahead_) return false;
+  int prio = 0;
+  if (cudaStreamGetPriority(s, &prio) != cudaSuccess) return false;
+  if (la_side_ && prio != la_prio_) {
+    cudaStreamSynchronize(la_side_);
+    cudaStreamDestroy(la_side_);
+    la_side_ = nullptr;
+  }
+  if (!la_side_) {
+    if (cudaStreamCreateWithPriority(&la_side_, cudaStreamNonBlocking, prio) != cudaSuccess) {
+      la_side_ = nullptr;
+      return false;
+    }
+    la_prio_ = prio;
+  }
+  for (cudaEvent_t& e : la_ev_)
+    if (!e && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+      e = nullptr;
+      return false;
+    }
+  return true;
+}
+
 void GpuCholesky::factor(const double* d_vals, cudaStream_t s, int slot) {
   Fronts fr{d_l_off_, d_u_off_, d_m_, d_k_};
+  LookAhead la;
+  if (elem_ == 8 || demoted()) {
+    if (lookahead_ready(s)) {
+      la.side = la_side_;
+      la.solved = la_ev_[0];
+      la.rest = la_ev_[1];
+      la.join = la_ev_[2];
+    }
+  }
   const unsigned ni = (unsigned)sy_.inv_count;
   const size_t ism = 2 * sizeof(double) * SB * (SB + 1);
   void* Lp = d_L_[slot];
@@ -2791,7 +2864,7 @@ void GpuCholesky::factor(const double* d_vals, cudaStream_t s, int slot) {
                                              d_rel_off_, d_rel_, d_tasks_, d_prefix_, d_err_, d_c0_, false, s,
                                              ozaki() ? &oz_ : nullptr, d_task_aux_,
                                              oz_timing_ ? &oz_events_ : nullptr, &oz_used_, (double*)d_dinvw_,
-                                             d_dinv_off_);
+                                             d_dinv_off_, &la);
     const int64_t nl = std::max<int64_t>(1, sy_.nnz_l), nd = std::max<int64_t>(1, sy_.dinv_elems);
     k_round_to_float<<<(unsigned)std::min<int64_t>((nl / 2 + 255) / 256, 148 * 16), 256, 0, s>>>(
         (const double*)d_Lw_, (float*)Lp, nl);
@@ -2810,7 +2883,7 @@ void GpuCholesky::factor(const double* d_vals, cudaStream_t s, int slot) {
                                              d_rel_off_, d_rel_, d_tasks_, d_prefix_, d_err_, d_c0_, false, s,
                                              ozaki() ? &oz_ : nullptr, d_task_aux_,
                                              oz_timing_ ? &oz_events_ : nullptr, &oz_used_, (double*)Dp,
-                                             d_dinv_off_);
+                                             d_dinv_off_, &la);
     return;
   }
   if (ni) ++launches_factor_;

@@ -98,6 +98,8 @@ class GpuCholesky {
   // factorizations; take_ozaki_ms() returns their summed device time (after the
   // stream has completed them) and starts over.
   void set_ozaki_timing(bool on) { oz_timing_ = on; }
+  // FP64 factorizations: the panel chain's look-ahead on a side stream (default on)
+  void set_lookahead(bool on) { lookahead_ = on; }
   double take_ozaki_ms();
   // Selects the per-panel solve (one launch per 64-column panel and level) instead
   // of the fused level solves; both compute the same triangular solves.  Turns the
@@ -136,6 +138,12 @@ class GpuCholesky {
   std::vector<cudaEvent_t> oz_events_;  // start/stop pairs, the first 2 * oz_used_ recorded
   size_t oz_used_ = 0;
   int64_t* d_task_aux_ = nullptr;
+  bool lookahead_ = true;
+  cudaStream_t la_side_ = nullptr;   // side stream of the look-ahead, priority la_prio_
+  int la_prio_ = 0;
+  cudaEvent_t la_ev_[3] = {nullptr, nullptr, nullptr};
+  // the side stream at the priority of s (created or re-created on first use)
+  bool lookahead_ready(cudaStream_t s);
   bool autotune_ = true;
   bool has_forced_ = false;
   SolveSchedule forced_;

@@ -12,7 +12,7 @@
 // for 8 slices).  Each inner product of digit rows is an exact integer sum
 // (|.| <= 127^2 K <= 8.3e6, a group of at most 8 of them < 2^31), so the only
 // roundings are the truncation of the digit expansion and the final FP64
-// additions: with 8 slices the transients of the solve agree with the FP64
+// addition and subtraction: with 8 slices the transients of the solve agree with the FP64
 // direct factorization to the level at which two FP64 orderings agree.
 //
 // k_oz_slice writes the digits of every row, k_oz_update multiplies them on the
@@ -26,8 +26,10 @@
 // "empty" mbarrier; warps 2-9 (tensor-memory lane groups 2, 3, 0, 1, twice: one
 // warp per 32 rows and 32 columns) wait for the tile's last commit, read the eight
 // accumulators of their columns 4 at a time (all eight tcgen05.ld before one wait),
-// add the groups in FP64 from the smallest weight up, scale by
-// 2^(e_a + e_b) and subtract from F.  TMA boxes read only this GPU's slice buffer
+// put groups 0-3 and 4-7 together exactly as 64-bit integers, convert both by
+// the magic-number method (no conversion-unit instructions: with a conversion per
+// group the epilogue kept that unit 73% busy and held the tensor pipe at 36%),
+// add them with one rounding, scale by 2^(e_a + e_b) and subtract from F.  TMA boxes read only this GPU's slice buffer
 // (no multicast).  Every mbarrier wait is bounded; a CTA that gives up records
 // err[2], waits (bounded) for its own MMAs and frees its tensor memory.
 #include "ozaki_update.h"
@@ -117,6 +119,19 @@ __device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t da, uint64_t db
 __device__ __forceinline__ void mma_commit(uint32_t bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
                : "memory");
+}
+
+// x (|x| < 2^51) as a double without the conversion unit: the bit pattern of
+// 2^52 + 2^51 plus x is the double 2^52 + 2^51 + x (unit spacing in [2^52, 2^53)),
+// from which the subtraction is exact (the "magic number" conversion).
+__device__ __forceinline__ double exact_double(long long x) {
+  return __longlong_as_double(0x4338000000000000LL + x) - 6755399441055744.0;
+}
+// v 2^n: a product with the power of two built from its exponent bits (exact, or
+// rounded once like ldexp when the result is subnormal); ldexp outside the range
+// of normal powers
+__device__ __forceinline__ double scale2(double v, int n) {
+  return (n >= -1022 && n <= 1023) ? v * __longlong_as_double((long long)(n + 1023) << 52) : ldexp(v, n);
 }
 
 __device__ __forceinline__ int find_task(const int64_t* __restrict__ prefix, int count, int64_t b) {
@@ -365,7 +380,12 @@ k_oz_update(double* __restrict__ L, double* __restrict__ U, const int64_t* __res
       // the exponents of this thread's 32 columns, one per lane (read before the
       // wait, handed to the other lanes with shuffles)
       const int ebl = ((int64_t)z.brow + cb + lane < nrows_buf) ? exps[z.brow + cb + lane] : 0;
-      bool ok = mbar_wait(acc_full, (uint32_t)(tc & 1)) && *(volatile int*)s_fail == 0;
+      // one lane per warp polls the barrier (256 threads polling through a tile's
+      // MMA phase kept a shared pipe busy and throttled the MMA and load threads);
+      // the shuffle is the warp's synchronisation point before its tensor-memory reads
+      int got = 1;
+      if (lane == 0) got = mbar_wait(acc_full, (uint32_t)(tc & 1)) ? 1 : 0;
+      bool ok = __shfl_sync(0xffffffffu, got, 0) != 0 && *(volatile int*)s_fail == 0;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       double v[EC];
       if (ok) {
@@ -380,12 +400,16 @@ k_oz_update(double* __restrict__ L, double* __restrict__ U, const int64_t* __res
                          : "r"(tmem + ((uint32_t)(32 * sub) << 16) + (uint32_t)(ON * g + cb + 4 * cc)));
           asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-          for (int q = 0; q < 4; ++q) v[4 * cc + q] = 0.0;
+          for (int q = 0; q < 4; ++q) {
+            // groups 0-3 and 4-7 put together exactly in 64-bit integers (|a_g| <=
+            // 8 * 127^2 * 512 < 2^26, so |hi|, |lo| < 2^47), then one rounding
+            long long hi = (int)a[0][q], lo = (int)a[4][q];
 #pragma unroll
-          for (int g = OS - 1; g >= 0; --g) {
-            const double w = ldexp(1.0, -7 * (g + 2));
-#pragma unroll
-            for (int q = 0; q < 4; ++q) v[4 * cc + q] = fma((double)(int)a[g][q], w, v[4 * cc + q]);
+            for (int g = 1; g < 4; ++g) {
+              hi = hi * 128 + (int)a[g][q];
+              lo = lo * 128 + (int)a[4 + g][q];
+            }
+            v[4 * cc + q] = fma(exact_double(hi), 0x1p-35, exact_double(lo) * 0x1p-63);
           }
         }
       }
@@ -415,7 +439,7 @@ k_oz_update(double* __restrict__ L, double* __restrict__ U, const int64_t* __res
             const int eb = __shfl_sync(0xffffffffu, ebl, cl);
             if (live && c < m && c <= r) {
               double* e = (c < k) ? L + lo + r + (int64_t)c * m : U + uo + (r - k) + (int64_t)(c - k) * (m - k);
-              *e = old[q] - ldexp(v[cl], ea + eb);
+              *e = old[q] - scale2(v[cl], ea + eb);
             }
           }
         }

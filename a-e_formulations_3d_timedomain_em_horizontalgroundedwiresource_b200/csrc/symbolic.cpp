@@ -607,8 +607,8 @@ std::string analyse(int n, const int64_t* rowptr, const int* colind, const doubl
     for (int j0 = 0; j0 < kmax; j0 += kPanel) {
       PanelStep ps;
       ps.j0 = j0;
-      std::vector<int> fr, fin, fbig;
-      std::vector<int64_t> c1, c2, c3, c4, c5, c6;
+      std::vector<int> fr, fin, fbig, frest;
+      std::vector<int64_t> c1, c2, c3, c4, c5, c6, c6a, c6b;
       const int J0 = (j0 / kOuter) * kOuter;
       for (int s : lp.fronts) {
         const int k = sy.front_k[s], m = sy.front_m[s];
@@ -630,6 +630,11 @@ std::string analyse(int n, const int64_t* rowptr, const int* colind, const doubl
           int64_t w6 = 0;
           for (int64_t bj = 0; bj < nc64; ++bj) w6 += nr128 - bj / 2;
           c6.push_back(w6);
+          c6a.push_back(nr128);
+          if (w6 > nr128) {
+            frest.push_back(s);
+            c6b.push_back(w6 - nr128);
+          }
         } else if (m > J1) {
           const int64_t nt = cdiv(m - J1, kTileBig);
           fbig.push_back(s);
@@ -640,6 +645,8 @@ std::string analyse(int n, const int64_t* rowptr, const int* colind, const doubl
       add_tasks(sy, ps.trsm, fr, c2);
       add_tasks(sy, ps.syrk, fin, c3);
       add_tasks(sy, ps.syrk_wide, fin, c6);
+      add_tasks(sy, ps.syrk_next, fin, c6a);
+      add_tasks(sy, ps.syrk_rest, frest, c6b);
       add_tasks(sy, ps.syrk_big, fbig, c5);
       {
         // the Ozaki path: slice-buffer rows of the fronts, in task order

@@ -67,6 +67,9 @@ struct PanelStep {
   TaskList trsm;       // ceil((m - j1) / kTrsmRows) CTAs per front
   TaskList syrk;       // update of columns [j1, J1) (rows >= j1) by the inner panel, 64-tiles
   TaskList syrk_wide;  // the same update in 128-row x 64-column tiles (FP64 tensor-pipe kernel)
+  // syrk_wide split for the look-ahead: the column tile of the next inner panel
+  // [j1, j1 + 64) (syrk_next) and the tiles right of it (syrk_rest)
+  TaskList syrk_next, syrk_rest;
   TaskList syrk_big;   // at the end of an outer panel: trailing [J1, m) by [J0, J1), 128-tiles
   // Ozaki path of syrk_big (ozaki true): the panel rows [J1, m) of every front of
   // syrk_big are split into digits, front after front (task_aux of the syrk_big
