@@ -114,7 +114,7 @@ class TdemPlanInfo(ctypes.Structure):
 
 class TdemServerOptions(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("max_active", ctypes.c_int), ("prep_threads", ctypes.c_int),
-                ("hbm_budget_bytes", ctypes.c_int64)]
+                ("hbm_budget_bytes", ctypes.c_int64), ("batch_max", ctypes.c_int)]
 
 
 class TdemRequestInfo(ctypes.Structure):
@@ -122,7 +122,7 @@ class TdemRequestInfo(ctypes.Structure):
                 ("n_rec_b", ctypes.c_int), ("n_rec_e", ctypes.c_int), ("n_sources", ctypes.c_int),
                 ("steps", ctypes.c_int), ("factorizations", ctypes.c_int), ("submit_s", ctypes.c_double),
                 ("admit_s", ctypes.c_double), ("done_s", ctypes.c_double), ("run_gpu_ms", ctypes.c_double),
-                ("device_bytes", ctypes.c_int64)]
+                ("device_bytes", ctypes.c_int64), ("batch_size", ctypes.c_int)]
 
     def as_dict(self) -> dict:
         return {n: getattr(self, n) for n, _ in self._fields_}
@@ -132,7 +132,8 @@ class TdemServerStats(ctypes.Structure):
     _fields_ = [("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("failed", ctypes.c_int64),
                 ("latency_p50_s", ctypes.c_double), ("latency_p99_s", ctypes.c_double),
                 ("makespan_s", ctypes.c_double), ("solves_per_s", ctypes.c_double),
-                ("peak_device_bytes", ctypes.c_int64), ("peak_active", ctypes.c_int)]
+                ("peak_device_bytes", ctypes.c_int64), ("peak_active", ctypes.c_int),
+                ("merged_runs", ctypes.c_int64), ("merged_requests", ctypes.c_int64)]
 
     def as_dict(self) -> dict:
         return {n: getattr(self, n) for n, _ in self._fields_}
@@ -167,6 +168,7 @@ EXPORTED = [
     "tdem_residual_norms",
     "tdem_server_create",
     "tdem_server_submit",
+    "tdem_server_submit_keyed",
     "tdem_server_wait",
     "tdem_server_results",
     "tdem_server_error",
@@ -242,6 +244,10 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.tdem_server_submit.argtypes = [P, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(TdemOptions),
                                        ctypes.c_int, ctypes.POINTER(ctypes.c_int64)]
     lib.tdem_server_submit.restype = ctypes.c_int
+    lib.tdem_server_submit_keyed.argtypes = [P, ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
+                                             ctypes.POINTER(TdemOptions), ctypes.c_int, ctypes.c_char_p,
+                                             ctypes.POINTER(ctypes.c_int64)]
+    lib.tdem_server_submit_keyed.restype = ctypes.c_int
     lib.tdem_server_wait.argtypes = [P, ctypes.c_int64, ctypes.POINTER(TdemRequestInfo)]
     lib.tdem_server_wait.restype = ctypes.c_int
     lib.tdem_server_results.argtypes = [P, ctypes.c_int64, P, P, P]
@@ -481,22 +487,26 @@ def residual_norms(device: int, n: int, rowptr: int, col: int, val: int, x: int,
 class Server:
     """Serving loop on one GPU (tdem_server_*): submit model directories, wait for
     their transients; requests are admitted by the device memory their analysis
-    needs and run concurrently on their own streams."""
+    needs and run concurrently on their own streams; with batch_max > 1, queued
+    requests submitted with the same batch key are merged into one run."""
 
-    def __init__(self, device: int = 0, max_active: int = 4, prep_threads: int = 2, hbm_budget_bytes: int = 0):
+    def __init__(self, device: int = 0, max_active: int = 4, prep_threads: int = 2, hbm_budget_bytes: int = 0,
+                 batch_max: int = 0):
         self._lib = load_library()
         self._h = ctypes.c_void_p()
-        o = TdemServerOptions(int(device), int(max_active), int(prep_threads), int(hbm_budget_bytes))
+        o = TdemServerOptions(int(device), int(max_active), int(prep_threads), int(hbm_budget_bytes),
+                              int(batch_max))
         st = self._lib.tdem_server_create(ctypes.byref(o), ctypes.byref(self._h))
         if st != 0:
             raise TdemError(st, "tdem_server_create failed")
 
     def submit(self, workdir: str, formulation="A", scheme: int = 2, precision: int = 64,
-               write_outputs: bool = False) -> int:
+               write_outputs: bool = False, batch_key: str = "") -> int:
         opts = TdemOptions(int(precision), 1e-10, 200, 128, 0, 0)
         rid = ctypes.c_int64(0)
-        st = self._lib.tdem_server_submit(self._h, os.fsencode(workdir), _form(formulation), int(scheme),
-                                          ctypes.byref(opts), int(bool(write_outputs)), ctypes.byref(rid))
+        st = self._lib.tdem_server_submit_keyed(self._h, os.fsencode(workdir), _form(formulation), int(scheme),
+                                                ctypes.byref(opts), int(bool(write_outputs)),
+                                                batch_key.encode() if batch_key else None, ctypes.byref(rid))
         if st != 0:
             raise TdemError(st, "tdem_server_submit failed")
         return int(rid.value)

@@ -444,6 +444,7 @@ tdem_status tdem_server_create(const tdem_server_options* opts, tdem_server** ou
       if (opts->max_active > 0) o.max_active = opts->max_active;
       if (opts->prep_threads > 0) o.prep_threads = opts->prep_threads;
       o.hbm_budget = opts->hbm_budget_bytes;
+      o.batch_max = opts->batch_max;
     }
     auto s = std::make_unique<tdem_server>();
     const std::string e = s->srv.start(o);
@@ -453,17 +454,24 @@ tdem_status tdem_server_create(const tdem_server_options* opts, tdem_server** ou
   });
 }
 
-tdem_status tdem_server_submit(tdem_server* srv, const char* workdir, int formulation, int scheme,
-                               const tdem_options* opts, int write_outputs, int64_t* request_id) {
+tdem_status tdem_server_submit_keyed(tdem_server* srv, const char* workdir, int formulation, int scheme,
+                                     const tdem_options* opts, int write_outputs, const char* batch_key,
+                                     int64_t* request_id) {
   return guard([&]() -> tdem_status {
     if (!srv || !workdir || !request_id) return TDEM_ERR_ARGUMENT;
     if ((formulation != 0 && formulation != 1) || (scheme != 2 && scheme != 3)) return TDEM_ERR_ARGUMENT;
     if (opts && (opts->precision != 0 && opts->precision != 32 && opts->precision != 64)) return TDEM_ERR_ARGUMENT;
     if (opts && (opts->fp32_update < 0 || opts->fp32_update > 2)) return TDEM_ERR_ARGUMENT;
     if (opts && (opts->factor_slots < 0 || opts->factor_slots > 2)) return TDEM_ERR_ARGUMENT;
-    *request_id = srv->srv.submit(workdir, run_options(formulation, scheme, opts), write_outputs != 0);
+    *request_id = srv->srv.submit(workdir, run_options(formulation, scheme, opts), write_outputs != 0,
+                                  batch_key ? batch_key : "");
     return TDEM_OK;
   });
+}
+
+tdem_status tdem_server_submit(tdem_server* srv, const char* workdir, int formulation, int scheme,
+                               const tdem_options* opts, int write_outputs, int64_t* request_id) {
+  return tdem_server_submit_keyed(srv, workdir, formulation, scheme, opts, write_outputs, nullptr, request_id);
 }
 
 tdem_status tdem_server_wait(tdem_server* srv, int64_t request_id, tdem_request_info* info) {
@@ -487,6 +495,7 @@ tdem_status tdem_server_wait(tdem_server* srv, int64_t request_id, tdem_request_
       info->done_s = r.done_s;
       info->run_gpu_ms = r.run_gpu_ms;
       info->device_bytes = r.device_bytes;
+      info->batch_size = r.batch_size;
     }
     std::lock_guard<std::mutex> lk(srv->mu);
     srv->done[request_id] = std::move(r);
@@ -529,6 +538,8 @@ tdem_status tdem_server_stats_get(tdem_server* srv, tdem_server_stats* st) {
     st->solves_per_s = s.solves_per_s;
     st->peak_device_bytes = s.peak_device_bytes;
     st->peak_active = s.peak_active;
+    st->merged_runs = s.merged_runs;
+    st->merged_requests = s.merged_requests;
     return TDEM_OK;
   });
 }

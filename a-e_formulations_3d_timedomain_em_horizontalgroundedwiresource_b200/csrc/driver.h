@@ -5,6 +5,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <array>
 #include <memory>
 #include <string>
 #include <vector>
@@ -69,6 +70,12 @@ class TransientSolve {
   // Host half: reads the inputs, builds the patterns, the analysis, the source
   // vectors and the receiver operators.  Touches no device.
   std::string plan(const std::string& dir, const RunOptions& opt);
+  // plan() for several direct-mode model directories that differ only in their
+  // sources and receivers (merge_models): one run solves all their sources as one
+  // n x npls block per step, each source with its own initial field and receivers.
+  // part_info receives each directory's (sources, B receivers, E receivers).
+  std::string plan_merged(const std::vector<std::string>& dirs, const RunOptions& opt,
+                          std::vector<std::array<int, 3>>* part_info = nullptr);
   // Device bytes setup_device() will allocate (valid after plan()).
   int64_t device_bytes_needed() const;
   // The analysis made by plan() (null before plan() and after setup_device()).
@@ -105,7 +112,16 @@ class TransientSolve {
   int kernel_launches() const { return launches_; }
 
  private:
+  // everything plan() does after the model is in m_
+  std::string plan_model(const RunOptions& opt, double t0);
   Model m_;
+  // merged plans: each directory with its source and receiver counts (its initial
+  // field is read there, and its receivers are evaluated on their own neighbourhood)
+  struct MergedPart {
+    std::string dir;
+    int npls = 0, nrec_b = 0, nrec_e = 0;
+  };
+  std::vector<MergedPart> parts_;
   RunOptions opt_;
   cudaStream_t s_ = nullptr;
   std::unique_ptr<GpuCholesky> chol_;

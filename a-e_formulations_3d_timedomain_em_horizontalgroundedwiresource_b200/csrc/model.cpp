@@ -341,7 +341,13 @@ std::string locate_dipoles(Model& m) {
 }
 
 std::string load_initial_field(const Model& m, bool eform, std::vector<double>& u0) {
-  const size_t n = (size_t)m.n_edges, np = (size_t)m.npls;
+  return load_initial_field(m, m.dir, m.npls, eform, u0);
+}
+
+std::string load_initial_field(const Model& m, const std::string& dir, int npls, bool eform,
+                               std::vector<double>& u0) {
+  const size_t n = (size_t)m.n_edges, np = (size_t)npls;
+  auto path = [&dir](const Model&, const char* name) { return dir + "/" + name; };
   u0.assign(n * np, 0.0);
   const std::string edge_file = path(m, eform ? "e0.edge" : "a0.edge");
   {
@@ -385,6 +391,47 @@ std::string load_initial_field(const Model& m, bool eform, std::vector<double>& 
         const double etan = -(va[v2 + p * nn] - va[v1 + p * nn]) / len;
         u0[e + p * n] = etan * len * 0.5;
       }
+  }
+  return "";
+}
+
+std::string merge_models(const std::vector<Model>& parts, Model& out) {
+  if (parts.empty()) return "no models to merge";
+  const Model& a = parts[0];
+  for (size_t i = 1; i < parts.size(); ++i) {
+    const Model& b = parts[i];
+    if (!a.fdirect || !b.fdirect) return "only direct-mode models are merged";
+    if (b.n_nodes != a.n_nodes || b.n_elem != a.n_elem || b.n_edges != a.n_edges ||
+        b.n_bound_nodes != a.n_bound_nodes || b.xyz != a.xyz || b.nver != a.nver || b.nvkat != a.nvkat ||
+        b.l13d != a.l13d || b.ed != a.ed || b.edge_nodes != a.edge_nodes || b.edge_bound != a.edge_bound)
+      return "the meshes differ";
+    if (b.sigma != a.sigma || b.sigma0 != a.sigma0 || b.mu != a.mu) return "the materials differ";
+    if (b.time != a.time || b.currentfunction != a.currentfunction || b.print_left != a.print_left ||
+        b.print_right != a.print_right)
+      return "the time grids differ";
+    if (b.n_srs_razb != a.n_srs_razb || b.n_neib != a.n_neib || b.eps_reg != a.eps_reg)
+      return "the source or receiver settings differ";
+  }
+  out = a;
+  out.npls = 0;
+  out.wires.clear();
+  out.dipoles.clear();
+  out.rec_b.clear();
+  out.rec_e.clear();
+  out.rec_b_ig.assign(1, 0);
+  out.rec_e_ig.assign(1, 0);
+  for (const Model& p : parts) {
+    if ((int)p.rec_b_ig.size() != p.npls + 1 || (int)p.rec_e_ig.size() != p.npls + 1)
+      return "receiver ranges missing";
+    const int ob = (int)out.rec_b.size(), oe = (int)out.rec_e.size();
+    out.wires.insert(out.wires.end(), p.wires.begin(), p.wires.end());
+    out.rec_b.insert(out.rec_b.end(), p.rec_b.begin(), p.rec_b.end());
+    out.rec_e.insert(out.rec_e.end(), p.rec_e.begin(), p.rec_e.end());
+    for (int s = 1; s <= p.npls; ++s) {
+      out.rec_b_ig.push_back(ob + p.rec_b_ig[s]);
+      out.rec_e_ig.push_back(oe + p.rec_e_ig[s]);
+    }
+    out.npls += p.npls;
   }
   return "";
 }

@@ -65,6 +65,16 @@ std::string load_model(const std::string& dir, Model& m);
 // when present, else the nodal a0.dat (A-form) / v3a.dat (E-form) projected onto
 // the edges (CalcNonstat3DLine time_approx.cpp:816-889, E-form time_approx.cpp:856-901).
 std::string load_initial_field(const Model& m, bool eform, std::vector<double>& u0);
+// The same for the npls sources whose files are in dir, on the mesh of m.
+std::string load_initial_field(const Model& m, const std::string& dir, int npls, bool eform,
+                               std::vector<double>& u0);
+
+// Several direct-mode models that differ only in their sources and receivers (the
+// same mesh, materials, time grid, current function and printed range) as one model
+// with all their sources, in order, each with its own receivers (the per-source
+// receiver ranges rec_*_ig index the concatenated receiver lists).  The result keeps
+// parts[0].dir.  Returns "" or why the parts cannot be merged.
+std::string merge_models(const std::vector<Model>& parts, Model& out);
 
 // Full symmetric CSR pattern over all edges (both triangles, sorted columns).
 void edge_pattern(const Model& m, std::vector<int64_t>& rowptr, std::vector<int>& col);

@@ -41,12 +41,20 @@ std::string Server::start(const ServerOptions& opt) {
   return "";
 }
 
-int64_t Server::submit(const std::string& dir, const RunOptions& opt, bool write_outputs) {
+bool Server::same_options(const RunOptions& a, const RunOptions& b) {
+  return a.formulation == b.formulation && a.scheme == b.scheme && a.precision == b.precision &&
+         a.refine_tol == b.refine_tol && a.refine_maxit == b.refine_maxit && a.leaf_size == b.leaf_size &&
+         a.fp32_update == b.fp32_update && a.factor_slots == b.factor_slots;
+}
+
+int64_t Server::submit(const std::string& dir, const RunOptions& opt, bool write_outputs,
+                       const std::string& batch_key) {
   auto r = std::make_unique<Request>();
   r->dir = dir;
   r->opt = opt;
   r->opt.cancel = nullptr;
   r->write_outputs = write_outputs;
+  r->key = batch_key;
   r->res.submit_s = now_s();
   int64_t id;
   {
@@ -63,6 +71,8 @@ void Server::plan_loop() {
   for (;;) {
     int64_t id;
     Request* r;
+    std::vector<int64_t> batch;
+    std::vector<std::string> dirs;
     {
       std::unique_lock<std::mutex> lk(mu_);
       cv_.wait(lk, [&] { return stop_ || !to_plan_.empty(); });
@@ -70,11 +80,45 @@ void Server::plan_loop() {
       id = to_plan_.front();
       to_plan_.pop_front();
       r = reqs_[id].get();
+      batch.push_back(id);
+      // queued requests with the same key and options join this one
+      if (opt_.batch_max > 1 && !r->key.empty() && !r->write_outputs) {
+        for (auto it = to_plan_.begin(); it != to_plan_.end() && (int)batch.size() < opt_.batch_max;) {
+          const Request* q = reqs_[*it].get();
+          if (q->key == r->key && !q->write_outputs && same_options(q->opt, r->opt)) {
+            batch.push_back(*it);
+            it = to_plan_.erase(it);
+          } else {
+            ++it;
+          }
+        }
+      }
+      for (int64_t b : batch) dirs.push_back(reqs_[b]->dir);
     }
     std::string e;
     try {
       r->solve.reset(new TransientSolve());
-      e = r->solve->plan(r->dir, r->opt);
+      if (batch.size() > 1) {
+        e = r->solve->plan_merged(dirs, r->opt, &r->part_info);
+        if (e.empty()) {
+          r->members = batch;
+        } else {
+          // not mergeable after all: this request alone, the others back at the head
+          // of the queue, never merged again
+          {
+            std::lock_guard<std::mutex> lk(mu_);
+            for (size_t k = batch.size(); k-- > 1;) {
+              reqs_[batch[k]]->key.clear();
+              to_plan_.push_front(batch[k]);
+            }
+          }
+          cv_.notify_all();
+          r->solve.reset(new TransientSolve());
+          e = r->solve->plan(r->dir, r->opt);
+        }
+      } else {
+        e = r->solve->plan(r->dir, r->opt);
+      }
     } catch (const std::exception& x) {  // host memory exhausted or another host failure
       e = std::string("host error: ") + x.what();
     }
@@ -85,12 +129,58 @@ void Server::plan_loop() {
         r->res.done_s = now_s();
         r->solve.reset();
         r->done = true;
+        for (size_t k = 1; k < r->members.size(); ++k) {
+          Request* q = reqs_[r->members[k]].get();
+          q->res.error = e;
+          q->res.done_s = r->res.done_s;
+          q->done = true;
+        }
       } else {
         r->bytes = r->solve->device_bytes_needed();
         planned_.push_back(id);
+        if (r->members.size() > 1) {
+          ++merged_runs_;
+          merged_requests_ += (int64_t)r->members.size();
+        }
       }
     }
     cv_.notify_all();
+  }
+}
+
+void Server::split_results(Request& lead) {
+  const int nl = lead.res.last_layer - lead.res.first_layer + 1;
+  const int NB = lead.res.n_rec_b, NE = lead.res.n_rec_e;
+  const RequestResult all = lead.res;
+  int ob = 0, oe = 0;
+  for (size_t k = 0; k < lead.members.size(); ++k) {
+    Request& q = *reqs_[lead.members[k]];
+    const int ns = lead.part_info[k][0], nb = lead.part_info[k][1], ne = lead.part_info[k][2];
+    RequestResult& rr = q.res;
+    const double submit = rr.submit_s;
+    rr = all;
+    rr.submit_s = submit;
+    rr.n_sources = ns;
+    rr.n_rec_b = nb;
+    rr.n_rec_e = ne;
+    rr.batch_size = (int)lead.members.size();
+    if (k > 0) rr.device_bytes = 0;  // counted with the first request of the run
+    auto slice = [nl](const std::vector<double>& src, int total, int off, int cnt, std::vector<double>& dst) {
+      dst.assign((size_t)nl * 3 * cnt, 0.0);
+      if (src.size() < (size_t)nl * 3 * total) return;
+      for (int l = 0; l < nl; ++l)
+        for (int c = 0; c < 3; ++c)
+          for (int j = 0; j < cnt; ++j)
+            dst[((size_t)l * 3 + c) * cnt + j] = src[((size_t)l * 3 + c) * total + off + j];
+    };
+    if (all.error.empty()) {
+      slice(all.eall, NE, oe, ne, rr.eall);
+      slice(all.emf, NB, ob, nb, rr.emf);
+      slice(all.ball, NB, ob, nb, rr.ball);
+    }
+    ob += nb;
+    oe += ne;
+    q.done = true;
   }
 }
 
@@ -158,6 +248,7 @@ void Server::run_loop() {
       std::lock_guard<std::mutex> lk(mu_);
       r->res.error = e;
       r->res.done_s = now_s();
+      if (r->members.size() > 1) split_results(*r);
       r->done = true;
       used_ -= r->bytes;
       --active_;
@@ -209,6 +300,8 @@ ServerStats Server::stats() {
   }
   st.peak_device_bytes = peak_used_;
   st.peak_active = peak_active_;
+  st.merged_runs = merged_runs_;
+  st.merged_requests = merged_requests_;
   return st;
 }
 

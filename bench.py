@@ -618,12 +618,21 @@ def batched_leg(args, pkg, base: str, form: str, scheme: int, device: int, singl
 
 
 def write_request(job):
-    """Inputs of one served request (seed, cells lo, cells hi, directory); runs in a
-    worker process.  Returns (directory, formulation, scheme, edges)."""
-    seed, lo, hi, d = job
+    """Inputs of one served request (seed, cells lo, cells hi, directory, transmitter
+    index); runs in a worker process.  Transmitter t > 0 moves the model's wires and
+    receivers 100 t m along y (the same earth model and mesh: a survey's next
+    transmitter position).  Returns (directory, formulation, scheme, edges)."""
+    import dataclasses
+    seed, lo, hi, d, tx = job
     sys.path.insert(0, HERE)
     mg = importlib.import_module(PKG + ".modelgen")
     spec, form, scheme = mg.random_request_model(seed, lo, hi)
+    if tx:
+        dy = 100.0 * tx
+        mv = lambda p: (p[0], p[1] + dy, p[2])
+        spec = dataclasses.replace(spec, sources=[(mv(a), mv(b)) for a, b in spec.sources],
+                                   receivers_b=[[mv(p) for p in r] for r in spec.receivers_b],
+                                   receivers_e=[[mv(p) for p in r] for r in spec.receivers_e])
     info = mg.write_model(d, spec)
     mg.write_analytic_initial_field(d, spec)
     return d, form, scheme, info["n_edges"]
@@ -644,7 +653,10 @@ def run_serving(args, world, rank, local):
         # request inputs written by a spawned process pool (no CUDA state is shared)
         import multiprocessing as mp
         from concurrent.futures import ProcessPoolExecutor
-        jobs = [(s0 + i, lo, hi, os.path.join(base, "req%03d" % i)) for i in range(args.c4_requests)]
+        # --c4-survey K: requests in groups of K transmitter positions over one model,
+        # submitted with the group's batch key (the server merges queued ones)
+        K = max(1, args.c4_survey)
+        jobs = [(s0 + i // K, lo, hi, os.path.join(base, "req%03d" % i), i % K) for i in range(args.c4_requests)]
         t_gen = time.perf_counter()
         with ProcessPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1)),
                                  mp_context=mp.get_context("spawn")) as ex:
@@ -663,14 +675,15 @@ def run_serving(args, world, rank, local):
         arrivals = np.cumsum(rng.exponential(1.0 / lam, len(reqs)))
         sampler = ClockSampler(local)
         sampler.start()
-        with pkg.Server(device=local, max_active=args.c4_active) as srv:
+        bmax = K if args.c4_batch_max < 0 else args.c4_batch_max
+        with pkg.Server(device=local, max_active=args.c4_active, batch_max=bmax) as srv:
             t0 = time.perf_counter()
             ids = []
-            for (d, form, scheme, _), ta in zip(reqs, arrivals):
+            for i, ((d, form, scheme, _), ta) in enumerate(zip(reqs, arrivals)):
                 delay = t0 + ta - time.perf_counter()
                 if delay > 0:
                     time.sleep(delay)
-                ids.append(srv.submit(d, form, scheme))
+                ids.append(srv.submit(d, form, scheme, batch_key="model%d" % (i // K) if K > 1 else ""))
             infos = [srv.wait(i) for i in ids]
             st = srv.stats()
         clocks = sampler.stop()
@@ -679,13 +692,16 @@ def run_serving(args, world, rank, local):
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic",
                 "config": {"workload": "served stream: %d requests, %d^3..%d^3 cells, random A/E x 2/3-point, "
-                                       "1-3 layers + 1-3 boxes, 60-200 steps, PCG64(%d + i)" % (len(reqs), lo, hi, s0),
+                                       "1-3 layers + 1-3 boxes, 60-200 steps, PCG64(%d + i)" % (len(reqs), lo, hi, s0)
+                                       + ("" if K == 1 else ", %d transmitter positions per model (batch key "
+                                          "per model, up to %d requests merged per run)" % (K, bmax)),
                            "arrival_rate_per_s": lam, "single_stream_service_s": t_alone,
                            "max_active": args.c4_active,
                            "edges_min_max": [min(r[3] for r in reqs), max(r[3] for r in reqs)]},
                 "latency_s": {"p50": st["latency_p50_s"], "p99": st["latency_p99_s"]},
                 "makespan_s": st["makespan_s"], "completed": st["completed"], "failed": st["failed"],
                 "peak_device_gb": st["peak_device_bytes"] / 1e9, "peak_active": st["peak_active"],
+                "merged_runs": st["merged_runs"], "merged_requests": st["merged_requests"],
                 "queue_wait_s_max": max(i["admit_s"] - i["submit_s"] for i in infos),
                 "inputs_written_s": t_gen,
                 "clocks": clocks}
@@ -879,6 +895,10 @@ def main():
     ap.add_argument("--c4-requests", type=int, default=16, help="served-stream length (config c4)")
     ap.add_argument("--c4-cells", default="30,60", help="mesh cells per side, lo,hi (config c4; 30,100 in full)")
     ap.add_argument("--c4-active", type=int, default=4, help="requests on the device at once (config c4)")
+    ap.add_argument("--c4-survey", type=int, default=1,
+                    help="transmitter positions per earth model (config c4; > 1 batches their time steps)")
+    ap.add_argument("--c4-batch-max", type=int, default=-1,
+                    help="requests merged per run (config c4; default: --c4-survey; 0 turns merging off)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the 32-wire block leg (config c2)")
     ap.add_argument("--no-mixed", action="store_true", help="skip the precision-32 leg (config c2)")

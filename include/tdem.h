@@ -294,13 +294,16 @@ typedef struct tdem_server_options {
   int max_active;           /* requests on the device at once (default 4 when 0) */
   int prep_threads;         /* host threads planning requests (default 2 when 0) */
   int64_t hbm_budget_bytes; /* admission budget (default: 85% of the free device memory) */
+  int batch_max;            /* requests of one batch key merged into one run (0 or 1: none);
+                               see tdem_server_submit_keyed */
 } tdem_server_options;
 typedef struct tdem_request_info {
   int status;               /* tdem_status of the request */
   int first_layer, last_layer, n_rec_b, n_rec_e, n_sources, steps, factorizations;
   double submit_s, admit_s, done_s;  /* steady-clock seconds */
   double run_gpu_ms;        /* device time of the request's time stepping */
-  int64_t device_bytes;     /* admission footprint */
+  int64_t device_bytes;     /* admission footprint (0 for the later requests of a merged run) */
+  int batch_size;           /* requests solved by the run that solved this one */
 } tdem_request_info;
 typedef struct tdem_server_stats {
   int64_t submitted, completed, failed;
@@ -308,12 +311,25 @@ typedef struct tdem_server_stats {
   double makespan_s, solves_per_s;     /* first submit -> last completion */
   int64_t peak_device_bytes;
   int peak_active;
+  int64_t merged_runs, merged_requests; /* runs that solved several requests, and those requests */
 } tdem_server_stats;
 tdem_status tdem_server_create(const tdem_server_options* opts, tdem_server** out);
 /* Queues one request (write_outputs != 0: also write the reference output files into
  * workdir); *request_id receives its id. */
 tdem_status tdem_server_submit(tdem_server* srv, const char* workdir, int formulation, int scheme,
                                const tdem_options* opts, int write_outputs, int64_t* request_id);
+/* tdem_server_submit with a batch key: queued requests with the same non-empty key,
+ * the same formulation, scheme and options, and no output files are merged (up to
+ * the server's batch_max) into one run that solves all their sources as one n x k
+ * block per time step on one factorization per step size; each request receives its
+ * own receivers' values.  The key states that the models differ only in their sources
+ * and receivers (sours, group, recvsb/recvse and the receiver files, the initial
+ * fields); the server checks it on the loaded models and runs them one by one when it
+ * does not hold.  No counterpart in the reference, which solves the sources of one
+ * model directory as npls right-hand sides (time_approx.cpp:1087). */
+tdem_status tdem_server_submit_keyed(tdem_server* srv, const char* workdir, int formulation, int scheme,
+                                     const tdem_options* opts, int write_outputs, const char* batch_key,
+                                     int64_t* request_id);
 /* Blocks until the request has finished; returns its status.  info may be NULL. */
 tdem_status tdem_server_wait(tdem_server* srv, int64_t request_id, tdem_request_info* info);
 /* Output tables of a finished request, as tdem_solver_results. */
