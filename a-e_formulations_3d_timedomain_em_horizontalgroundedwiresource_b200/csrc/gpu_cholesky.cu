@@ -76,8 +76,10 @@ __global__ void k_zero_u(T* __restrict__ U, Fronts f, const int* __restrict__ fr
   const int64_t t = blockIdx.x - prefix[idx];
   const int c0 = (int)t * kSolveRows, c1 = min(r, c0 + kSolveRows);
   T* u = U + f.u_off[s];
+  // the lower triangle only: the updates, the extend-add and the trailing update
+  // read and write rows i >= c of column c and nothing above
   for (int c = c0; c < c1; ++c)
-    for (int i = threadIdx.x; i < r; i += blockDim.x) u[i + (int64_t)c * r] = (T)0;
+    for (int i = c + threadIdx.x; i < r; i += blockDim.x) u[i + (int64_t)c * r] = (T)0;
 }
 
 // Extend-add of the children's update blocks into their parents (one child per

@@ -672,7 +672,13 @@ def run_serving(args, world, rank, local):
             t_alone.append(time.perf_counter() - t0)
         lam = 1.2 / (sum(t_alone) / len(t_alone))
         rng = np.random.Generator(np.random.PCG64(s0))
-        arrivals = np.cumsum(rng.exponential(1.0 / lam, len(reqs)))
+        if K > 1:
+            # a survey's transmitter positions arrive together (one client submits them),
+            # the surveys as a Poisson stream at the same request rate
+            ng = (len(reqs) + K - 1) // K
+            arrivals = np.repeat(np.cumsum(rng.exponential(K / lam, ng)), K)[:len(reqs)]
+        else:
+            arrivals = np.cumsum(rng.exponential(1.0 / lam, len(reqs)))
         sampler = ClockSampler(local)
         sampler.start()
         bmax = K if args.c4_batch_max < 0 else args.c4_batch_max
@@ -693,8 +699,9 @@ def run_serving(args, world, rank, local):
                 "data": "synthetic",
                 "config": {"workload": "served stream: %d requests, %d^3..%d^3 cells, random A/E x 2/3-point, "
                                        "1-3 layers + 1-3 boxes, 60-200 steps, PCG64(%d + i)" % (len(reqs), lo, hi, s0)
-                                       + ("" if K == 1 else ", %d transmitter positions per model (batch key "
-                                          "per model, up to %d requests merged per run)" % (K, bmax)),
+                                       + ("" if K == 1 else ", %d transmitter positions per model arriving "
+                                          "together (batch key per model, up to %d requests merged per run)"
+                                          % (K, bmax)),
                            "arrival_rate_per_s": lam, "single_stream_service_s": t_alone,
                            "max_active": args.c4_active,
                            "edges_min_max": [min(r[3] for r in reqs), max(r[3] for r in reqs)]},
