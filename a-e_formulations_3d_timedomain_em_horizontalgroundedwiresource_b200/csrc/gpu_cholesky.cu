@@ -117,7 +117,7 @@ __global__ void k_extend_add(T* __restrict__ L, T* __restrict__ U, Fronts f, con
 // With dinv (FP64 factorization) the CTA also inverts the finished block into the
 // front's inverted diagonal blocks (dinv_off[s] + 64 * 64 * (j0 / 64), column-major,
 // leading dimension w): the operand of the panel solve k_trsm_dmma and of the
-// triangular solves, by the substitution and operation order of k_diag_inverse.
+// triangular solves (by 16 x 16 blocks, see below).
 template <class T>
 __global__ void __launch_bounds__(256) k_potrf(T* __restrict__ L, Fronts f, const int* __restrict__ fronts, int j0,
                                                int* __restrict__ err, const int* __restrict__ c0_of,
@@ -126,6 +126,7 @@ __global__ void __launch_bounds__(256) k_potrf(T* __restrict__ L, Fronts f, cons
   __shared__ T A[P][P + 1];
   __shared__ T diag[P];
   __shared__ T xd[P];
+  __shared__ T tb[3][16][16];  // band products of the blocked inverse
   const int s = fronts[blockIdx.x];
   const int m = f.m[s], k = f.k[s];
   const int w = min(P, k - j0);
@@ -160,15 +161,22 @@ __global__ void __launch_bounds__(256) k_potrf(T* __restrict__ L, Fronts f, cons
   }
   if (dinv == nullptr) return;
   // L(r, c) = A[c][r] (r > c) or diag[r]; the inverse X(r, c) (r > c) goes to the
-  // lower triangle, whose working values are dead, and its diagonal to xd.  Four
-  // threads per column c run X(r, c) = -(sum_{c <= l < r} L(r, l) X(l, c)) / L(r, r).
+  // lower triangle, whose working values are dead, and its diagonal to xd.  By
+  // 16 x 16 blocks: the diagonal blocks by substitution, four threads per column
+  // running X(r, c) = -(sum_{c <= l < r} L(r, l) X(l, c)) / L(r, r) over at most 15
+  // rows; then the blocks below them band by band, X_ij = -X_ii sum_{j <= k < i}
+  // L_ik X_kj, every element of a band at once (a column-long substitution would
+  // chain 63 dependent steps).
+  constexpr int QB = 16;
+  auto Xv = [&](int l, int c) -> T { return l == c ? xd[c] : (l > c ? A[l][c] : (T)0); };
   {
     const int c = threadIdx.x >> 2, part = threadIdx.x & 3;
     const unsigned mask = 0xFu << ((threadIdx.x & 31) & ~3);
     if (c < w) {
+      const int bend = min(w, (c / QB + 1) * QB);
       if (part == 0) xd[c] = (T)1 / diag[c];
       __syncwarp(mask);
-      for (int r = c + 1; r < w; ++r) {
+      for (int r = c + 1; r < bend; ++r) {
         T sum = (T)0;
         for (int l = c + part; l < r; l += 4) sum = fma(A[l][r], l == c ? xd[c] : A[l][c], sum);
         sum += __shfl_xor_sync(mask, sum, 1);
@@ -179,6 +187,29 @@ __global__ void __launch_bounds__(256) k_potrf(T* __restrict__ L, Fronts f, cons
     }
   }
   __syncthreads();
+  const int nb = (w + QB - 1) / QB;
+  for (int d = 1; d < nb; ++d) {
+    const int np = nb - d;  // block pairs (j + d, j) of band d
+    for (int e = threadIdx.x; e < np * QB * QB; e += blockDim.x) {
+      const int j = e / (QB * QB), rr = (e / QB) % QB, cc = e % QB;
+      const int r = (j + d) * QB + rr, c = j * QB + cc;
+      T t = (T)0;
+      if (r < w && c < w)
+        for (int l = j * QB; l < (j + d) * QB; ++l) t = fma(A[l][r], Xv(l, c), t);
+      tb[j][rr][cc] = t;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < np * QB * QB; e += blockDim.x) {
+      const int j = e / (QB * QB), rr = (e / QB) % QB, cc = e % QB;
+      const int i0 = (j + d) * QB, r = i0 + rr, c = j * QB + cc;
+      if (r < w && c < w) {
+        T x = (T)0;
+        for (int l = i0; l <= r; ++l) x = fma(Xv(r, l), tb[j][l - i0][cc], x);
+        A[r][c] = -x;
+      }
+    }
+    __syncthreads();
+  }
   T* D = dinv + dinv_off[s] + (int64_t)(j0 / P) * P * P;
   for (int q = threadIdx.x; q < w * w; q += blockDim.x) {
     const int r = q % w, c = q / w;
