@@ -135,3 +135,41 @@ def test_element_colouring_is_valid_and_greedy(pkg, mg, tmp_path):
     mg.write_analytic_initial_field(d, spec)
     r = subprocess.run([exe, d], capture_output=True, text=True)
     assert r.returncode == 0 and r.stdout.startswith("ok"), r.stdout
+
+
+def test_models_of_one_mesh_merge_for_batched_serving(pkg, mg, tmp_path):
+    """merge_models / plan_merged (host): directories of one mesh with different wires
+    and receivers merge in order, each keeping its receivers' ranges and its initial
+    field; a directory with another mesh is refused (CPU driver compiled against the
+    library)."""
+    import dataclasses
+    import shutil
+    import subprocess
+    if shutil.which("g++") is None:
+        pytest.skip("no C++ compiler")
+    here = os.path.dirname(os.path.abspath(__file__))
+    lib_dir = os.path.dirname(pkg.LIB_PATH)
+    exe = str(tmp_path / "merge")
+    cuda_inc = "/usr/local/cuda/include"
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", os.path.join(os.path.dirname(pkg.__file__), "csrc"),
+                    "-I", os.path.join(os.path.dirname(here), "include"), "-I", cuda_inc,
+                    os.path.join(here, "native", "merge_models.cpp"), "-L" + lib_dir, "-ltdem_b200",
+                    "-Wl,-rpath," + lib_dir, "-o", exe], check=True)
+    base = mg.small_model(cells=8, n_dec=2, steps_per_dec=4)
+    dirs = []
+    for i, wires in enumerate([[((-30.0, 0.0, 0.0), (30.0, 0.0, 0.0))],
+                               [((-30.0, 20.0, 0.0), (30.0, 20.0, 0.0)), ((0.0, -40.0, 0.0), (0.0, 20.0, 0.0))],
+                               [((-20.0, -20.0, 0.0), (40.0, -20.0, 0.0))]]):
+        rec = [(0.0, 15.0 + 5.0 * i + 25.0 * k, 0.0) for k in range(3 + i)]
+        spec = dataclasses.replace(base, sources=wires, receivers_b=[rec] * len(wires),
+                                   receivers_e=[rec] * len(wires))
+        d = str(tmp_path / ("tx%d" % i))
+        mg.write_model(d, spec)
+        mg.write_analytic_initial_field(d, spec)
+        dirs.append(d)
+    other = str(tmp_path / "other")
+    spec = mg.small_model(cells=10, n_dec=2, steps_per_dec=4)
+    mg.write_model(other, spec)
+    mg.write_analytic_initial_field(other, spec)
+    r = subprocess.run([exe] + dirs + [other], capture_output=True, text=True)
+    assert r.returncode == 0 and r.stdout.startswith("ok 4 sources"), r.stdout + r.stderr
