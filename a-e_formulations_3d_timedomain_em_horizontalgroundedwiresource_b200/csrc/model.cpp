@@ -1,5 +1,6 @@
 // Readers for the reference's direct-mode input files (see model.h).
 #include "model.h"
+#include "boxgrid.h"
 #include "parallel.h"
 
 #include <algorithm>
@@ -284,8 +285,8 @@ std::string locate_dipoles(Model& m) {
       m.dipoles[i][j].dz = dz;
     }
   }
-  // every dipole goes to the first element (in element order) that holds it: each
-  // range of elements finds its first candidates, the lowest range wins
+  // every dipole goes to the first element (in element order) that holds it: the
+  // elements whose box (+-1e-3) holds the dipole are all in its grid cell's list
   const double lo = -1e-2, hi = 1.0 + 1e-2;
   const int nall = m.npls * nd;
   auto local = [&](int e, const P& p, double l[3]) {
@@ -296,44 +297,46 @@ std::string locate_dipoles(Model& m) {
     l[1] = (p.y - p0[1]) / (p7[1] - p0[1]);
     l[2] = (p.z - p0[2]) / (p7[2] - p0[2]);
   };
-  const int nt = chunk_count(m.n_elem, 16384);
-  std::vector<int> found((size_t)nt * nall, -1);
-  parallel_chunks(m.n_elem, nt, [&](int t, int64_t e0, int64_t e1) {
-    int* fnd = found.data() + (size_t)t * nall;
-    for (int e = (int)e0; e < (int)e1; ++e) {
+  std::vector<double> bmn(3 * (size_t)m.n_elem), bmx(3 * (size_t)m.n_elem);
+  parallel_ranges(m.n_elem, [&](int64_t e0, int64_t e1) {
+    for (int64_t e = e0; e < e1; ++e) {
       double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
       for (int k = 0; k < 8; ++k)
         for (int a = 0; a < 3; ++a) {
           mn[a] = std::min(mn[a], m.xyz[m.nver[e][k]][a]);
           mx[a] = std::max(mx[a], m.xyz[m.nver[e][k]][a]);
         }
-      for (int i = 0; i < m.npls; ++i)
-        for (int j = 0; j < nd; ++j) {
-          if (fnd[i * nd + j] != -1) continue;
-          const P& p = pos[i][j];
-          if (p.x < mn[0] - 1e-3 || p.x > mx[0] + 1e-3 || p.y < mn[1] - 1e-3 || p.y > mx[1] + 1e-3 ||
-              p.z < mn[2] - 1e-3 || p.z > mx[2] + 1e-3)
-            continue;
-          double l[3];
-          local(e, p, l);
-          if (l[0] > lo && l[0] < hi && l[1] > lo && l[1] < hi && l[2] > lo && l[2] < hi) fnd[i * nd + j] = e;
-        }
+      for (int a = 0; a < 3; ++a) {
+        bmn[3 * e + a] = mn[a] - 1e-3;
+        bmx[3 * e + a] = mx[a] + 1e-3;
+      }
     }
   });
-  for (int i = 0; i < m.npls; ++i)
-    for (int j = 0; j < nd; ++j)
-      for (int t = 0; t < nt; ++t) {
-        const int e = found[(size_t)t * nall + i * nd + j];
-        if (e < 0) continue;
-        Dipole& d = m.dipoles[i][j];
+  BoxGrid grid;
+  grid.build(bmn, bmx);
+  parallel_ranges(nall, [&](int64_t k0, int64_t k1) {
+    for (int64_t k = k0; k < k1; ++k) {
+      const int i = (int)(k / nd), j = (int)(k % nd);
+      const P& p = pos[i][j];
+      const double q[3] = {p.x, p.y, p.z};
+      const auto cand = grid.candidates(q);
+      for (const int* c = cand.first; c != cand.second; ++c) {
+        const int e = *c;
+        const double* mn = &bmn[3 * (size_t)e];
+        const double* mx = &bmx[3 * (size_t)e];
+        if (p.x < mn[0] || p.x > mx[0] || p.y < mn[1] || p.y > mx[1] || p.z < mn[2] || p.z > mx[2]) continue;
         double l[3];
-        local(e, pos[i][j], l);
+        local(e, p, l);
+        if (!(l[0] > lo && l[0] < hi && l[1] > lo && l[1] < hi && l[2] > lo && l[2] < hi)) continue;
+        Dipole& d = m.dipoles[i][j];
         d.elem = e;
         d.ksi = l[0];
         d.eta = l[1];
         d.zeta = l[2];
         break;
       }
+    }
+  }, 256);
   for (int i = 0; i < m.npls; ++i)
     for (int j = 0; j < nd; ++j)
       if (m.dipoles[i][j].elem < 0) return "source dipole outside the mesh";

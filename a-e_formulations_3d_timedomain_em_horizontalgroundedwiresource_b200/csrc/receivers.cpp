@@ -2,8 +2,11 @@
 #include "receivers.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
-#include <map>
+
+#include "boxgrid.h"
+#include "parallel.h"
 
 namespace tdem {
 namespace {
@@ -50,18 +53,21 @@ struct Sub {
   std::vector<std::array<int, 8>> lnode;  // local node numbers per subdomain element
   std::vector<std::array<double, 8>> g;   // mass row sums per element
   std::vector<std::array<double, 3>> h;
+  std::vector<std::array<double, 4>> mv;  // the element's nodal_mass values by popcount
   std::vector<double> diag;
 };
 
 void matvec(const Sub& s, const std::vector<double>& x, std::vector<double>& y) {
   std::fill(y.begin(), y.end(), 0.0);
   for (size_t e = 0; e < s.elems.size(); ++e) {
-    double b[8][8];
-    nodal_mass(s.h[e][0], s.h[e][1], s.h[e][2], b);
+    const std::array<int, 8>& ln = s.lnode[e];
+    const std::array<double, 4>& v = s.mv[e];
+    double xl[8];
+    for (int j = 0; j < 8; ++j) xl[j] = x[ln[j]];
     for (int i = 0; i < 8; ++i) {
       double acc = 0.0;
-      for (int j = 0; j < 8; ++j) acc += b[i][j] * x[s.lnode[e][j]];
-      y[s.lnode[e][i]] += acc;
+      for (int j = 0; j < 8; ++j) acc += v[__builtin_popcount(i ^ j)] * xl[j];
+      y[ln[i]] += acc;
     }
   }
 }
@@ -123,8 +129,12 @@ std::string build_receiver_operator(const Model& m, const std::vector<std::array
       mn[3 * e + a] = m.xyz[m.nver[e][0]][a] - 1e-6;
       mx[3 * e + a] = m.xyz[m.nver[e][7]][a] + 1e-6;
     }
+  BoxGrid grid;
+  grid.build(mn, mx);
   for (int i = 0; i < nrec; ++i) {
-    for (int e = 0; e < m.n_elem; ++e) {
+    const auto cand = grid.candidates(pts[i].data());
+    for (const int* c = cand.first; c != cand.second; ++c) {
+      const int e = *c;
       bool in = true;
       for (int a = 0; a < 3 && in; ++a) in = pts[i][a] >= mn[3 * e + a] && pts[i][a] <= mx[3 * e + a];
       if (in) {
@@ -159,7 +169,10 @@ std::string build_receiver_operator(const Model& m, const std::vector<std::array
   std::vector<char> has_rec(m.n_elem, 0);
   for (int i = 0; i < nrec; ++i) has_rec[out.elem[i]] = 1;
 
-  std::vector<std::map<int, double>> rows((size_t)3 * nrec);
+  // row comp*nrec+i: edge ids (increasing) and weights
+  std::vector<std::vector<int>> row_col((size_t)3 * nrec);
+  std::vector<std::vector<double>> row_val((size_t)3 * nrec);
+  std::vector<int> edge_local(m.n_edges, -1);
   for (int mat : mats) {
     // --- subdomain growth (Subdomain.cpp:165-242) -------------------------------
     std::vector<char> in_e(m.n_elem, 0), in_n(m.n_nodes, 0);
@@ -195,6 +208,7 @@ std::string build_receiver_operator(const Model& m, const std::vector<std::array
     s.lnode.resize(ne);
     s.g.resize(ne);
     s.h.resize(ne);
+    s.mv.resize(ne);
     s.diag.assign(nn, 0.0);
     for (size_t t = 0; t < ne; ++t) {
       const int e = s.elems[t];
@@ -202,6 +216,7 @@ std::string build_receiver_operator(const Model& m, const std::vector<std::array
       for (int a = 0; a < 3; ++a) s.h[t][a] = m.xyz[m.nver[e][7]][a] - m.xyz[m.nver[e][0]][a];
       double b[8][8];
       nodal_mass(s.h[t][0], s.h[t][1], s.h[t][2], b);
+      for (int d = 0; d < 4; ++d) s.mv[t][d] = b[0][(1 << d) - 1];
       for (int j = 0; j < 8; ++j) {
         double gsum = 0.0;
         for (int k = 0; k < 8; ++k) gsum += b[j][k];
@@ -209,37 +224,81 @@ std::string build_receiver_operator(const Model& m, const std::vector<std::array
         s.diag[s.lnode[t][j]] += b[j][j];
       }
     }
-    // --- one mass-matrix solve per receiver of this subdomain ----------------------
-    std::vector<double> c(nn), y;
-    for (int i = 0; i < nrec; ++i) {
-      const int e = out.elem[i];
-      if (!(mat == -1 || m.nvkat[e] == mat)) continue;
-      std::fill(c.begin(), c.end(), 0.0);
-      for (int k = 0; k < 8; ++k) c[renum[m.nver[e][k]]] += cfa[i][k];
-      std::string err = pcg(s, c, y);
-      if (!err.empty()) return err;
-      for (size_t t = 0; t < ne; ++t) {
-        double wt = 0.0;
-        for (int j = 0; j < 8; ++j) wt += s.g[t][j] * y[s.lnode[t][j]];
-        if (wt == 0.0) continue;
-        const int eg = s.elems[t];
+    // the subdomain's edges in increasing id order, and each element's edges by that order
+    std::vector<int> sub_edges;
+    for (size_t t = 0; t < ne; ++t)
+      for (int l = 0; l < 12; ++l) sub_edges.push_back(m.ed[s.elems[t]][l]);
+    std::sort(sub_edges.begin(), sub_edges.end());
+    sub_edges.erase(std::unique(sub_edges.begin(), sub_edges.end()), sub_edges.end());
+    const size_t nse = sub_edges.size();
+    for (size_t k = 0; k < nse; ++k) edge_local[sub_edges[k]] = (int)k;
+    std::vector<std::array<int, 12>> ledge(ne);
+    std::vector<std::array<double, 36>> cfe(ne);  // centre coefficients [comp][l]
+    for (size_t t = 0; t < ne; ++t)
+      for (int l = 0; l < 12; ++l) {
+        ledge[t][l] = edge_local[m.ed[s.elems[t]][l]];
         for (int comp = 0; comp < 3; ++comp)
-          for (int l = 0; l < 12; ++l) {
-            const double cf = centre_coef(curl, comp, l, s.h[t][0], s.h[t][1], s.h[t][2]);
-            if (cf != 0.0) rows[(size_t)comp * nrec + i][m.ed[eg][l]] += wt * cf;
-          }
+          cfe[t][comp * 12 + l] = centre_coef(curl, comp, l, s.h[t][0], s.h[t][1], s.h[t][2]);
       }
-    }
+    for (int ge : sub_edges) edge_local[ge] = -1;
+    // --- one mass-matrix solve per receiver of this subdomain; the receivers are
+    // taken by host threads one at a time, and receiver i writes rows comp*nrec+i only,
+    // so the rows do not depend on the thread count -------------------------------
+    std::vector<int> todo;
+    for (int i = 0; i < nrec; ++i)
+      if (mat == -1 || m.nvkat[out.elem[i]] == mat) todo.push_back(i);
+    const int nt = std::max(1, std::min(host_threads(), (int)todo.size()));
+    std::atomic<int64_t> next(0);
+    std::vector<std::string> errs(nt);
+    parallel_chunks(nt, nt, [&](int th, int64_t, int64_t) {
+      std::vector<double> c(nn), y, acc(3 * nse);
+      std::vector<char> hit(3 * nse);
+      for (int64_t k; (k = next++) < (int64_t)todo.size();) {
+        const int i = todo[k], e = out.elem[i];
+        std::fill(c.begin(), c.end(), 0.0);
+        for (int q = 0; q < 8; ++q) c[renum[m.nver[e][q]]] += cfa[i][q];
+        std::string err = pcg(s, c, y);
+        if (!err.empty()) {
+          errs[th] = err;
+          return;
+        }
+        // weights summed per edge in element order (dense over the subdomain's edges)
+        std::fill(acc.begin(), acc.end(), 0.0);
+        std::fill(hit.begin(), hit.end(), 0);
+        for (size_t t = 0; t < ne; ++t) {
+          double wt = 0.0;
+          for (int j = 0; j < 8; ++j) wt += s.g[t][j] * y[s.lnode[t][j]];
+          if (wt == 0.0) continue;
+          for (int comp = 0; comp < 3; ++comp)
+            for (int l = 0; l < 12; ++l) {
+              const double cf = cfe[t][comp * 12 + l];
+              if (cf == 0.0) continue;
+              const size_t q = comp * nse + ledge[t][l];
+              acc[q] += wt * cf;
+              hit[q] = 1;
+            }
+        }
+        for (int comp = 0; comp < 3; ++comp) {
+          std::vector<int>& rc = row_col[(size_t)comp * nrec + i];
+          std::vector<double>& rv = row_val[(size_t)comp * nrec + i];
+          for (size_t q = 0; q < nse; ++q)
+            if (hit[comp * nse + q]) {
+              rc.push_back(sub_edges[q]);
+              rv.push_back(acc[comp * nse + q]);
+            }
+        }
+      }
+    });
+    for (const std::string& err : errs)
+      if (!err.empty()) return err;
   }
   out.rowptr.assign(1, 0);
   out.src.resize((size_t)3 * nrec);
   for (int comp = 0; comp < 3; ++comp)
     for (int i = 0; i < nrec; ++i) {
-      const auto& r = rows[(size_t)comp * nrec + i];
-      for (const auto& kv : r) {
-        out.col.push_back(kv.first);
-        out.val.push_back(kv.second);
-      }
+      const size_t r = (size_t)comp * nrec + i;
+      out.col.insert(out.col.end(), row_col[r].begin(), row_col[r].end());
+      out.val.insert(out.val.end(), row_val[r].begin(), row_val[r].end());
       out.rowptr.push_back((int64_t)out.col.size());
       out.src[(size_t)comp * nrec + i] = owner[i];
     }
