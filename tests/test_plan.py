@@ -173,3 +173,31 @@ def test_models_of_one_mesh_merge_for_batched_serving(pkg, mg, tmp_path):
     mg.write_analytic_initial_field(other, spec)
     r = subprocess.run([exe] + dirs + [other], capture_output=True, text=True)
     assert r.returncode == 0 and r.stdout.startswith("ok 4 sources"), r.stdout + r.stderr
+
+
+def test_point_location_and_threaded_receiver_smoothing(pkg, mg, tmp_path):
+    """The element grid used to place dipoles and receivers finds the same element as a
+    scan over all elements (graded tensor mesh with points on nodes and faces, random
+    overlapping boxes, a model's dipoles), and the receiver operators built on 1 and on 3
+    host threads are byte-identical (CPU driver compiled against the library)."""
+    import dataclasses
+    import shutil
+    import subprocess
+    if shutil.which("g++") is None:
+        pytest.skip("no C++ compiler")
+    here = os.path.dirname(os.path.abspath(__file__))
+    lib_dir = os.path.dirname(pkg.LIB_PATH)
+    exe = str(tmp_path / "locate")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", os.path.join(os.path.dirname(pkg.__file__), "csrc"),
+                    "-I", os.path.join(os.path.dirname(here), "include"), "-I", "/usr/local/cuda/include",
+                    os.path.join(here, "native", "point_location.cpp"), "-L" + lib_dir, "-ltdem_b200",
+                    "-Wl,-rpath," + lib_dir, "-o", exe], check=True)
+    base = mg.small_model(cells=10, n_dec=2, steps_per_dec=4)
+    wires = [((-30.0, 0.0, 0.0), (30.0, 0.0, 0.0)), ((-30.0, 20.0, 0.0), (30.0, 20.0, 0.0)),
+             ((0.0, -40.0, 0.0), (0.0, 20.0, 0.0))]
+    rec = [(0.0, 10.0 + 12.5 * k, 0.0) for k in range(6)] + [(-20.0, -20.0, 0.0)]
+    spec = dataclasses.replace(base, sources=wires, receivers_b=[rec] * 3, receivers_e=[rec] * 3)
+    d = str(tmp_path / "m")
+    mg.write_model(d, spec)
+    r = subprocess.run([exe, d], capture_output=True, text=True)
+    assert r.returncode == 0 and r.stdout.startswith("ok "), r.stdout + r.stderr
