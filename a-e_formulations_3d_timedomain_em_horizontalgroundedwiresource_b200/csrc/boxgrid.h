@@ -24,13 +24,20 @@ namespace tdem {
 class BoxGrid {
  public:
   // lo, hi: 3 per box (x, y, z); a box with !(lo <= hi) on some axis (empty or NaN)
-  // is never listed
-  void build(const std::vector<double>& lo, const std::vector<double>& hi) {
+  // is never listed.  With qlo/qhi (the bounding box of the points that will be
+  // looked up), boxes that do not reach it are not listed either: none of them can
+  // hold such a point.
+  void build(const std::vector<double>& lo, const std::vector<double>& hi, const double* qlo = nullptr,
+             const double* qhi = nullptr) {
     const int64_t n = (int64_t)lo.size() / 3;
     std::vector<char> ok(n, 1);
     for (int64_t b = 0; b < n; ++b)
-      for (int a = 0; a < 3; ++a)
+      for (int a = 0; a < 3; ++a) {
         if (!(lo[3 * b + a] <= hi[3 * b + a])) ok[b] = 0;
+        if (qlo && (hi[3 * b + a] < qlo[a] || lo[3 * b + a] > qhi[a])) ok[b] = 0;
+      }
+    int64_t listed = 0;
+    for (int64_t b = 0; b < n; ++b) listed += ok[b];
     int64_t cells = 1;
     for (int a = 0; a < 3; ++a) {
       std::vector<double>& c = cut_[a];
@@ -43,8 +50,8 @@ class BoxGrid {
       std::sort(c.begin(), c.end());
       c.erase(std::unique(c.begin(), c.end()), c.end());
     }
-    // thin the cuts while the cell count is above twice the box count
-    const double target = 2.0 * (double)std::max<int64_t>(n, 32);
+    // thin the cuts while the cell count is above twice the listed box count
+    const double target = 2.0 * (double)std::max<int64_t>(listed, 32);
     double prod = 1.0;
     for (int a = 0; a < 3; ++a) prod *= (double)(cut_[a].size() + 1);
     if (prod > target) {

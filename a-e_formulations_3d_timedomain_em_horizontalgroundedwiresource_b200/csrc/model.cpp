@@ -312,8 +312,18 @@ std::string locate_dipoles(Model& m) {
       }
     }
   });
+  double qlo[3] = {INFINITY, INFINITY, INFINITY}, qhi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (const auto& w : pos)
+    for (const P& p : w) {
+      const double q[3] = {p.x, p.y, p.z};
+      for (int a = 0; a < 3; ++a)
+        if (!std::isnan(q[a])) {
+          qlo[a] = std::min(qlo[a], q[a]);
+          qhi[a] = std::max(qhi[a], q[a]);
+        }
+    }
   BoxGrid grid;
-  grid.build(bmn, bmx);
+  grid.build(bmn, bmx, qlo, qhi);
   parallel_ranges(nall, [&](int64_t k0, int64_t k1) {
     for (int64_t k = k0; k < k1; ++k) {
       const int i = (int)(k / nd), j = (int)(k % nd);

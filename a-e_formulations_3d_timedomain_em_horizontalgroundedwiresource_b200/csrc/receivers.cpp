@@ -129,8 +129,15 @@ std::string build_receiver_operator(const Model& m, const std::vector<std::array
       mn[3 * e + a] = m.xyz[m.nver[e][0]][a] - 1e-6;
       mx[3 * e + a] = m.xyz[m.nver[e][7]][a] + 1e-6;
     }
+  double qlo[3] = {INFINITY, INFINITY, INFINITY}, qhi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (const auto& p : pts)
+    for (int a = 0; a < 3; ++a)
+      if (!std::isnan(p[a])) {
+        qlo[a] = std::min(qlo[a], p[a]);
+        qhi[a] = std::max(qhi[a], p[a]);
+      }
   BoxGrid grid;
-  grid.build(mn, mx);
+  grid.build(mn, mx, qlo, qhi);
   for (int i = 0; i < nrec; ++i) {
     const auto cand = grid.candidates(pts[i].data());
     for (const int* c = cand.first; c != cand.second; ++c) {
