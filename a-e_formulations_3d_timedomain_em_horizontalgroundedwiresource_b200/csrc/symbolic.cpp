@@ -504,63 +504,47 @@ std::string analyse(int n, const int64_t* rowptr, const int* colind, const doubl
         return "internal error: root front with off-diagonal rows";
   }
 
-  // entry map: lower-CSR entry -> front element.  Entries are bucketed by front
-  // (counting sort, keeping each entry's row), then placed front by front.
+  // entry map: lower-CSR entry -> front element.  An entry (i, j) lands in the front
+  // of column min(perm i, perm j), at the local row of max(perm i, perm j): one of the
+  // front's own columns, or found by binary search in its sorted row list (rows_all).
+  // Every entry is placed on its own, so rows of the CSR run in parallel.
   {
     sy.entry_dst.assign(sy.nnz_lower, -1);
-    // per row range: count its entries of every front, then place them after the
-    // entries of the lower ranges (the order inside a front is the serial one)
     const int nt = chunk_count(n, 16384);
-    std::vector<int64_t> hist((size_t)nt * nf, 0), fstart(nf + 1, 0);
+    std::vector<char> bad(nt, 0);
     parallel_chunks(n, nt, [&](int t, int64_t i0, int64_t i1) {
-      int64_t* h = hist.data() + (size_t)t * nf;
-      for (int64_t i = i0; i < i1; ++i)
-        for (int64_t q = rowptr[i]; q < rowptr[i + 1]; ++q) ++h[colfront[std::min(sy.perm[i], sy.perm[colind[q]])]];
-    });
-    for (int s = 0; s < nf; ++s) {
-      int64_t acc = fstart[s];
-      for (int t = 0; t < nt; ++t) {
-        const int64_t c = hist[(size_t)t * nf + s];
-        hist[(size_t)t * nf + s] = acc;
-        acc += c;
-      }
-      fstart[s + 1] = acc;
-    }
-    std::vector<int64_t> eq(sy.nnz_lower);
-    std::vector<int> er(sy.nnz_lower);
-    parallel_chunks(n, nt, [&](int t, int64_t i0, int64_t i1) {
-      int64_t* fill = hist.data() + (size_t)t * nf;
-      for (int64_t i = i0; i < i1; ++i)
+      for (int64_t i = i0; i < i1; ++i) {
+        const int a = sy.perm[i];
         for (int64_t q = rowptr[i]; q < rowptr[i + 1]; ++q) {
-          const int64_t at = fill[colfront[std::min(sy.perm[i], sy.perm[colind[q]])]]++;
-          eq[at] = q;
-          er[at] = (int)i;
-        }
-    });
-    // fronts in parallel, each thread with its own row -> slot map
-    std::vector<char> bad(host_threads() + 1, 0);
-    parallel_ranges(nf, [&](int64_t s0, int64_t s1) {
-      std::vector<int> pos(n, -1);
-      for (int64_t s = s0; s < s1; ++s) {
-        const FrontInfo& f = sy.fronts[s];
-        for (int cc = f.c0; cc < f.c1; ++cc) pos[cc] = cc - f.c0;
-        for (size_t t = 0; t < f.rows.size(); ++t) pos[f.rows[t]] = f.k() + (int)t;
-        const int64_t m = f.m();
-        for (int64_t t = fstart[s]; t < fstart[s + 1]; ++t) {
-          const int64_t q = eq[t];
-          const int i = er[t];
-          const int a = sy.perm[i], b = sy.perm[colind[q]];
+          const int b = sy.perm[colind[q]];
           const int col = std::min(a, b), row = std::max(a, b);
-          const int lr = pos[row], lc = col - f.c0;
-          if (lr < 0 || lc < 0 || lc >= f.k() || lr < lc) {
-            bad[0] = 1;
+          const int f = colfront[col];
+          const int c0 = sy.front_c0[f], k = sy.front_k[f];
+          const int64_t m = sy.front_m[f];
+          const int lc = col - c0;
+          int64_t lr;
+          if (row < c0 + k) {
+            lr = row - c0;
+          } else {
+            const int* r0 = sy.rows_all.data() + sy.rows_off[f] + k;
+            const int* r1 = sy.rows_all.data() + sy.rows_off[f] + m;
+            const int* p = std::lower_bound(r0, r1, row);
+            if (p == r1 || *p != row) {
+              bad[t] = 1;
+              return;
+            }
+            lr = k + (p - r0);
+          }
+          if (lc < 0 || lc >= k || lr < lc) {
+            bad[t] = 1;
             return;
           }
-          sy.entry_dst[q] = sy.l_off[s] + lr + (int64_t)lc * m;
+          sy.entry_dst[q] = sy.l_off[f] + lr + (int64_t)lc * m;
         }
       }
-    }, 64);
-    if (bad[0]) return "internal error: entry outside its front";
+    });
+    for (char x : bad)
+      if (x) return "internal error: entry outside its front";
   }
 
   // level plans
