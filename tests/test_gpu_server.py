@@ -82,7 +82,7 @@ def test_failed_request_does_not_stop_the_others(pkg, mix_models, tmp_path):
 
 
 # transmitter positions of one survey over one earth model: (wires, receivers' y offset)
-SURVEY = [
+TX_POSITIONS = [
     ([((-30.0, 0.0, 0.0), (30.0, 0.0, 0.0))], 0.0),
     ([((-30.0, 20.0, 0.0), (30.0, 20.0, 0.0))], 5.0),
     ([((-20.0, -20.0, 0.0), (40.0, -20.0, 0.0)), ((-30.0, 40.0, 0.0), (30.0, 40.0, 0.0))], 10.0),
@@ -95,7 +95,7 @@ def survey_models(mg, tmp_path_factory):
     import dataclasses
     base = mg.small_model(cells=10, n_dec=2, steps_per_dec=5)
     dirs = []
-    for i, (wires, dy) in enumerate(SURVEY):
+    for i, (wires, dy) in enumerate(TX_POSITIONS):
         rec = [(0.0, 10.0 + dy + 25.0 * k, 0.0) for k in range(4 + i)]
         spec = dataclasses.replace(base, sources=wires, receivers_b=[rec] * len(wires),
                                    receivers_e=[rec] * len(wires))
@@ -122,14 +122,14 @@ def test_batched_requests_match_their_solo_runs(pkg, survey_models, form, scheme
         infos = [srv.wait(rid) for rid in ids]
         got = [srv.results(rid, info) for rid, info in zip(ids, infos)]
         st = srv.stats()
-    assert st["completed"] == len(SURVEY) and st["failed"] == 0
+    assert st["completed"] == len(TX_POSITIONS) and st["failed"] == 0
     # the plan thread takes a request as soon as it is queued, with whatever of the
     # others is queued by then: at least one run solves two or more of them
     assert st["merged_runs"] >= 1 and st["merged_requests"] >= 2
     assert max(i["batch_size"] for i in infos) >= 2
-    assert sum(1.0 / i["batch_size"] for i in infos) == pytest.approx(len(SURVEY) - st["merged_requests"]
+    assert sum(1.0 / i["batch_size"] for i in infos) == pytest.approx(len(TX_POSITIONS) - st["merged_requests"]
                                                                        + st["merged_runs"])
-    for info, (wires, _) in zip(infos, SURVEY):
+    for info, (wires, _) in zip(infos, TX_POSITIONS):
         assert info["n_sources"] == len(wires)
     for a, b in zip(alone, got):
         for x, y in zip(a, b):  # (the E-form has no B table: zeros both ways)
