@@ -405,18 +405,24 @@ def run_ours(args, world, rank, local):
         barrier(world)
         te = time.perf_counter()
         h2d = d2h = 0
+        create_s = plan_s = 0.0
         for _ in range(e2e_steps):
+            tc = time.perf_counter()
             with pkg.Solver(wdir, form, scheme, device=local, **sopts) as s:
+                create_s += time.perf_counter() - tc
                 s.run()
                 s.results()
                 ii = s.info()
                 h2d += ii["h2d_bytes"]
                 d2h += ii["d2h_bytes"]
+                plan_s += ii["t_setup_s"]
         torch.cuda.synchronize()
         t_e2e = max_over_ranks(world, time.perf_counter() - te)
         e2e = {"value": world * e2e_steps * per_run / t_e2e, "unit": "forward solves/s",
                "h2d_bytes_per_step": h2d // e2e_steps, "d2h_bytes_per_step": d2h // e2e_steps,
-               "path": "tdem_solver_create (reads the input files, analysis, H2D) + run + results (D2H)"}
+               "path": "tdem_solver_create (reads the input files, analysis, H2D) + run + results (D2H)",
+               "create_s_per_step": create_s / e2e_steps,
+               "setup_s_per_step": plan_s / e2e_steps}
 
         if rank == 0:
             peaks = measured_peaks()
