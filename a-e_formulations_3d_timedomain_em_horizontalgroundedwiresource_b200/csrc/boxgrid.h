@@ -1,7 +1,8 @@
 // Point location over the elements' axis-aligned boxes.  The reference walks all
 // elements for every point and takes the first (in element order) whose box holds
-// it (OutputResultant3d.cpp:572-712 for receivers, the dipole search of the
-// source setup); BoxGrid returns, for a point, a short list that holds every box
+// it (CalcNonstat3DLine/OutputResultant3d.cpp:572-712 for receivers,
+// Vec_Prep_Data::LoadAndInitCurrent, vec_prep_data.cpp:1080-1180, for the wire's
+// dipoles); BoxGrid returns, for a point, a short list that holds every box
 // containing it, in increasing box order, so scanning that list with the same test
 // gives the same element.
 //
