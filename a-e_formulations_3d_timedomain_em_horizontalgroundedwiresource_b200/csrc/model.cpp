@@ -347,6 +347,67 @@ std::string locate_dipoles(Model& m) {
       }
     }
   }, 256);
+  // A dipole that no element holds (outside the mesh) goes to the nearest element
+  // (Vec_Prep_Data::GetNearestElement, vec_prep_data.cpp:878-980, called from :1186-1250):
+  // of the 8 elements with the least L1 distance from the dipole to their node box
+  // (ties in element order), the first with the least L1 distance of the dipole's local
+  // coordinates from [0, 1]; the dipole keeps those local coordinates (outside [0, 1]).
+  std::vector<int64_t> lost;
+  for (int64_t k = 0; k < nall; ++k)
+    if (m.dipoles[k / nd][k % nd].elem < 0) lost.push_back(k);
+  if (!lost.empty() && m.n_elem == 0) return "source dipole outside the mesh";
+  parallel_ranges((int64_t)lost.size(), [&](int64_t k0, int64_t k1) {
+    for (int64_t k = k0; k < k1; ++k) {
+      const int i = (int)(lost[k] / nd), j = (int)(lost[k] % nd);
+      const P& p = pos[i][j];
+      const double q[3] = {p.x, p.y, p.z};
+      const int n_best = std::min(8, m.n_elem);
+      double sb[8];
+      int eb[8];
+      for (int b = 0; b < 8; ++b) {
+        sb[b] = 1e30;
+        eb[b] = -1;
+      }
+      double sbest = sb[7];
+      for (int e = 0; e < m.n_elem; ++e) {
+        double mn[3], mx[3];
+        for (int a = 0; a < 3; ++a) mn[a] = mx[a] = m.xyz[m.nver[e][0]][a];
+        for (int v = 1; v < 8; ++v)
+          for (int a = 0; a < 3; ++a) {
+            const double c = m.xyz[m.nver[e][v]][a];
+            if (c < mn[a]) mn[a] = c;
+            if (c > mx[a]) mx[a] = c;
+          }
+        double sc = 0.0;
+        for (int a = 0; a < 3; ++a) sc += (q[a] < mn[a]) ? (mn[a] - q[a]) : (q[a] > mx[a]) ? (q[a] - mx[a]) : 0.0;
+        if (!(sc < sbest)) continue;
+        int b = 0;
+        while (b < n_best && eb[b] != -1 && !(sc < sb[b])) ++b;
+        for (int c = n_best - 1; c > b; --c) {
+          eb[c] = eb[c - 1];
+          sb[c] = sb[c - 1];
+        }
+        eb[b] = e;
+        sb[b] = sc;
+        sbest = sb[n_best - 1];
+      }
+      double lbest = 1e30;
+      for (int b = 0; b < n_best && eb[b] != -1; ++b) {
+        double l[3];
+        local(eb[b], p, l);
+        double sc = 0.0;
+        for (int a = 0; a < 3; ++a) sc += (l[a] < 0.0) ? -l[a] : (l[a] > 1.0) ? (l[a] - 1.0) : 0.0;
+        if (sc < lbest) {
+          lbest = sc;
+          Dipole& d = m.dipoles[i][j];
+          d.elem = eb[b];
+          d.ksi = l[0];
+          d.eta = l[1];
+          d.zeta = l[2];
+        }
+      }
+    }
+  }, 1);
   for (int i = 0; i < m.npls; ++i)
     for (int j = 0; j < nd; ++j)
       if (m.dipoles[i][j].elem < 0) return "source dipole outside the mesh";

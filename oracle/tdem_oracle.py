@@ -266,9 +266,27 @@ def initial_field(m: Dict, eform: bool) -> np.ndarray:
     return u
 
 
+def _nearest_element(x: np.ndarray, mn: np.ndarray, mx: np.ndarray, p0: np.ndarray, p7: np.ndarray):
+    """Element of a dipole that no element holds (vec_prep_data.cpp:878-980, called at
+    :1186-1250): the 8 elements of least L1 distance from the point to their node box
+    (ties in element order), and of those the first with the least L1 distance of the
+    point's local coordinates from [0, 1]."""
+    d = np.where(x < mn, mn - x, np.where(x > mx, x - mx, 0.0))
+    s = (d[:, 0] + d[:, 1]) + d[:, 2]
+    best, e = 1e30, None
+    for c in np.lexsort((np.arange(len(s)), s))[:8]:
+        loc = (x - p0[c]) / (p7[c] - p0[c])
+        o = np.where(loc < 0.0, -loc, np.where(loc > 1.0, loc - 1.0, 0.0))
+        so = (o[0] + o[1]) + o[2]
+        if so < best:
+            best, e = so, int(c)
+    return e
+
+
 def source_vectors(m: Dict) -> np.ndarray:
     """Wire split into nSrsRazb dipoles located in the first element (file order)
-    holding them (vec_prep_data.cpp:1050-1183); RHS weights per edge."""
+    holding them (vec_prep_data.cpp:1050-1183), or the nearest one when none does;
+    RHS weights per edge."""
     n, npls = m["n"], m["npls"]
     S = np.zeros((n, npls))
     ns = m["nsrs"]
@@ -288,6 +306,8 @@ def source_vectors(m: Dict) -> np.ndarray:
                 if np.all((loc > -1e-2) & (loc < 1 + 1e-2)):
                     e = cand
                     break
+            if e is None:
+                e = _nearest_element(x, mn, mx, p0, p7)
             if e is None:
                 raise RuntimeError("dipole outside the mesh")
             loc = (x - p0[e]) / (p7[e] - p0[e])

@@ -3,9 +3,11 @@
 //     the point) on a graded tensor-product mesh (nodes, face centres, interior and
 //     outside points) and on random overlapping boxes (thinned cuts, empty and NaN
 //     boxes).
-//  2. argv[1], a model directory: the dipoles' elements against a linear scan over the
-//     elements, and the receiver operators built on 1 and on 3 host threads, which must
+//  2. argv[1], a model directory: the dipoles' elements and local coordinates against a
+//     linear scan over the elements (with the nearest-element rule for dipoles outside
+//     the mesh), and the receiver operators built on 1 and on 3 host threads, which must
 //     be byte-identical.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -137,6 +139,7 @@ int main(int argc, char** argv) {
     }
     // the dipole search: first element whose node box (+-1e-3) holds the dipole and whose
     // local coordinates on nodes 0/7 lie in (-1e-2, 1 + 1e-2)
+    int beyond = 0;
     for (int i = 0; i < m.npls; ++i)
       for (size_t j = 0; j < m.dipoles[i].size(); ++j) {
         const auto& w = m.wires[i];
@@ -158,8 +161,50 @@ int main(int argc, char** argv) {
           }
           if (in) want = el;
         }
-        if (want != m.dipoles[i][j].elem) {
-          printf("dipole %d/%zu: scan %d, located %d\n", i, j, want, m.dipoles[i][j].elem);
+        double lw[3] = {0, 0, 0};
+        if (want < 0) {
+          // none holds it: of the 8 nearest boxes (L1, ties in element order) the first
+          // whose local coordinates lie least far (L1) outside [0, 1]
+          std::vector<std::pair<double, int>> dist;
+          for (int el = 0; el < m.n_elem; ++el) {
+            double s = 0.0;
+            for (int a = 0; a < 3; ++a) {
+              double mn = 1e300, mx = -1e300;
+              for (int k = 0; k < 8; ++k) {
+                mn = std::min(mn, m.xyz[m.nver[el][k]][a]);
+                mx = std::max(mx, m.xyz[m.nver[el][k]][a]);
+              }
+              s += p[a] < mn ? mn - p[a] : p[a] > mx ? p[a] - mx : 0.0;
+            }
+            dist.push_back({s, el});
+          }
+          std::sort(dist.begin(), dist.end());
+          double best = 1e30;
+          for (size_t b = 0; b < 8 && b < dist.size(); ++b) {
+            const int el = dist[b].second;
+            double l[3], o = 0.0;
+            for (int a = 0; a < 3; ++a) {
+              const double x0 = m.xyz[m.nver[el][0]][a], x7 = m.xyz[m.nver[el][7]][a];
+              l[a] = (p[a] - x0) / (x7 - x0);
+              o += l[a] < 0.0 ? -l[a] : l[a] > 1.0 ? l[a] - 1.0 : 0.0;
+            }
+            if (o < best) {
+              best = o;
+              want = el;
+              std::copy(l, l + 3, lw);
+            }
+          }
+          ++beyond;
+        } else {
+          for (int a = 0; a < 3; ++a) {
+            const double x0 = m.xyz[m.nver[want][0]][a], x7 = m.xyz[m.nver[want][7]][a];
+            lw[a] = (p[a] - x0) / (x7 - x0);
+          }
+        }
+        const Dipole& dp = m.dipoles[i][j];
+        if (want != dp.elem || lw[0] != dp.ksi || lw[1] != dp.eta || lw[2] != dp.zeta) {
+          printf("dipole %d/%zu: scan %d (%g %g %g), located %d (%g %g %g)\n", i, j, want, lw[0], lw[1], lw[2],
+                 dp.elem, dp.ksi, dp.eta, dp.zeta);
           return 1;
         }
       }
@@ -183,8 +228,8 @@ int main(int argc, char** argv) {
         return 1;
       }
     }
-    printf("ok %d points, %d dipoles, %zu + %zu receiver weights\n", npts, m.npls * m.n_srs_razb,
-           op[0][0].val.size(), op[0][1].val.size());
+    printf("ok %d points, %d dipoles (%d outside the mesh), %zu + %zu receiver weights\n", npts,
+           m.npls * m.n_srs_razb, beyond, op[0][0].val.size(), op[0][1].val.size());
     return 0;
   }
   printf("ok %d points\n", npts);

@@ -33,6 +33,22 @@ def test_gpu_matches_reference_goldens(pkg, golden, outs, tmp_path, case, varian
             assert err <= FP64_TOL, (o, p, err)
 
 
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_gpu_wire_beyond_the_mesh_matches_reference(pkg, outs, tmp_path, variant):
+    """A wire half past the mesh edge: the dipoles outside go to the nearest element, with
+    local coordinates outside [0, 1], as in the reference (vec_prep_data.cpp:878-980)."""
+    sys.path.insert(0, GOLDEN)
+    import make_beyond_golden as bg
+    d = str(tmp_path / "gpu")
+    bg.write_case_inputs(d)
+    with pkg.Solver(d, variant[0], int(variant[1])) as s:
+        s.run()
+        s.write_outputs()
+    for o in bg.OUTPUTS:
+        err = outs.compare_files(os.path.join(d, o + ".1"), os.path.join(GOLDEN, bg.CASE, "%s_%s.1" % (variant, o)))
+        assert err <= FP64_TOL, (o, err)
+
+
 @pytest.mark.parametrize("variant", ["A3", "E2"])
 def test_gpu_matches_numpy_oracle(pkg, mg, outs, tmp_path, variant):
     spec = mg.small_model(cells=10, n_dec=3, steps_per_dec=5, block=True)

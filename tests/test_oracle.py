@@ -167,6 +167,32 @@ def test_numpy_oracle_primary_secondary_matches_reference(outs, tmp_path, case, 
         assert err <= FP64_TOL, (o, err)
 
 
+@pytest.mark.parametrize("variant", ["A2", "A3", "E2", "E3"])
+def test_numpy_oracle_wire_beyond_the_mesh_matches_reference(outs, tmp_path, variant):
+    """A wire that runs past the mesh edge: the dipoles no element holds go to the nearest
+    element with local coordinates outside [0, 1] (vec_prep_data.cpp:878-980); the
+    restatement against the reference's outputs, and (E-form, whose step-off source reads
+    every dipole) against a run that drops those dipoles."""
+    import sys
+    sys.path.insert(0, GOLDEN)
+    import make_beyond_golden as bg
+    d = str(tmp_path / "beyond")
+    bg.write_case_inputs(d)
+    tdem_oracle.run(d, variant[0], int(variant[1]))
+    for o in bg.OUTPUTS:
+        err = outs.compare_files(os.path.join(d, o + ".1"), os.path.join(GOLDEN, bg.CASE, "%s_%s.1" % (variant, o)))
+        assert err <= FP64_TOL, (o, err)
+    if variant == "E2":
+        # the wire cut at the mesh edge, x = 600 .. 1000 m with the same dipole length
+        with open(os.path.join(d, "sours"), "w") as f:
+            f.write("600.0 0.0 0.0\n1000.0 0.0 0.0\n")
+        with open(os.path.join(d, "nSrsRazb"), "w") as f:
+            f.write("50\n")
+        tdem_oracle.run(d, "E", 2)
+        assert outs.compare_files(os.path.join(d, "eall_anom.1"),
+                                  os.path.join(GOLDEN, bg.CASE, "E2_eall_anom.1")) > 1e-3
+
+
 def test_three_point_formulas_exact_for_quadratics():
     """Known answers of the time discretisation (reference math, no reference run):
     the BDF2 step coefficients (A3/time_approx.cpp:943-945) and the three-point

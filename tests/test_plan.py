@@ -178,7 +178,8 @@ def test_models_of_one_mesh_merge_for_batched_serving(pkg, mg, tmp_path):
 def test_point_location_and_threaded_receiver_smoothing(pkg, mg, tmp_path):
     """The element grid used to place dipoles and receivers finds the same element as a
     scan over all elements (graded tensor mesh with points on nodes and faces, random
-    overlapping boxes, a model's dipoles), and the receiver operators built on 1 and on 3
+    overlapping boxes, a model's dipoles, a wire half past the mesh edge whose outer
+    dipoles go to the nearest element), and the receiver operators built on 1 and on 3
     host threads are byte-identical (CPU driver compiled against the library)."""
     import dataclasses
     import shutil
@@ -193,11 +194,14 @@ def test_point_location_and_threaded_receiver_smoothing(pkg, mg, tmp_path):
                     os.path.join(here, "native", "point_location.cpp"), "-L" + lib_dir, "-ltdem_b200",
                     "-Wl,-rpath," + lib_dir, "-o", exe], check=True)
     base = mg.small_model(cells=10, n_dec=2, steps_per_dec=4)
+    x_max = float(base.x[-1])
     wires = [((-30.0, 0.0, 0.0), (30.0, 0.0, 0.0)), ((-30.0, 20.0, 0.0), (30.0, 20.0, 0.0)),
-             ((0.0, -40.0, 0.0), (0.0, 20.0, 0.0))]
+             ((0.0, -40.0, 0.0), (0.0, 20.0, 0.0)),
+             ((x_max - 400.0, 0.0, 0.0), (x_max + 400.0, 0.0, 0.0))]  # half of it past the mesh edge
     rec = [(0.0, 10.0 + 12.5 * k, 0.0) for k in range(6)] + [(-20.0, -20.0, 0.0)]
-    spec = dataclasses.replace(base, sources=wires, receivers_b=[rec] * 3, receivers_e=[rec] * 3)
+    spec = dataclasses.replace(base, sources=wires, receivers_b=[rec] * 4, receivers_e=[rec] * 4)
     d = str(tmp_path / "m")
     mg.write_model(d, spec)
     r = subprocess.run([exe, d], capture_output=True, text=True)
     assert r.returncode == 0 and r.stdout.startswith("ok "), r.stdout + r.stderr
+    assert "(0 outside" not in r.stdout, r.stdout
