@@ -524,27 +524,44 @@ void edge_pattern(const Model& m, std::vector<int64_t>& rowptr, std::vector<int>
     for (int e = 0; e < m.n_elem; ++e)
       for (int i = 0; i < 12; ++i) elems[fill[m.ed[e][i]]++] = e;
   }
-  // each range of rows is gathered, sorted and deduplicated into its own buffer;
-  // the buffers are then placed one after the other
+  // two passes over the rows, each range on its own thread with its own marks: the
+  // distinct edges of each row are counted, then written in place and sorted (a row
+  // holds at most 33 of its at most 48 gathered edges)
   const int nt = chunk_count(n, 4096);
-  std::vector<std::vector<int>> part(nt);
   rowptr.assign(n + 1, 0);
-  parallel_chunks(n, nt, [&](int t, int64_t r0, int64_t r1) {
-    std::vector<int>& out = part[t];
-    out.reserve((size_t)(r1 - r0) * 36);
+  parallel_chunks(n, nt, [&](int, int64_t r0, int64_t r1) {
+    std::vector<int> seen(n, -1);  // row that last listed each edge
     for (int64_t i = r0; i < r1; ++i) {
-      const size_t b = out.size();
+      int64_t c = 0;
       for (int64_t q = eptr[i]; q < eptr[i + 1]; ++q)
-        for (int j = 0; j < 12; ++j) out.push_back(m.ed[elems[q]][j]);
-      std::sort(out.begin() + b, out.end());
-      out.erase(std::unique(out.begin() + b, out.end()), out.end());
-      rowptr[i + 1] = (int64_t)(out.size() - b);
+        for (int j = 0; j < 12; ++j) {
+          const int e = m.ed[elems[q]][j];
+          if (seen[e] != (int)i) {
+            seen[e] = (int)i;
+            ++c;
+          }
+        }
+      rowptr[i + 1] = c;
     }
   });
   for (int i = 0; i < n; ++i) rowptr[i + 1] += rowptr[i];
   col.resize(rowptr[n]);
-  parallel_chunks(n, nt, [&](int t, int64_t r0, int64_t) {
-    std::copy(part[t].begin(), part[t].end(), col.begin() + rowptr[r0]);
+  parallel_chunks(n, nt, [&](int, int64_t r0, int64_t r1) {
+    std::vector<int> seen(n, -1);
+    for (int64_t i = r0; i < r1; ++i) {
+      int* out = col.data() + rowptr[i];
+      int c = 0;
+      for (int64_t q = eptr[i]; q < eptr[i + 1]; ++q)
+        for (int j = 0; j < 12; ++j) {
+          const int e = m.ed[elems[q]][j];
+          if (seen[e] != (int)i) {
+            seen[e] = (int)i;
+            int y = c++;
+            for (; y > 0 && out[y - 1] > e; --y) out[y] = out[y - 1];
+            out[y] = e;
+          }
+        }
+    }
   });
 }
 
