@@ -389,29 +389,34 @@ std::string TransientSolve::plan_model(const RunOptions& opt, double t0) {
   n_int_ = (int64_t)int_edge.size();
   if (n_int_ == 0) return main_error("no interior edges");
   // lower triangle of the interior system (rows independent: count, then fill)
-  std::vector<int64_t> lptr(n_int_ + 1, 0);
+  std::vector<int64_t> lptr(n_int_ + 1, 0), aptr(n_int_ + 1, 0);
   std::vector<double> xyz((size_t)n_int_ * 3);
   parallel_ranges(n_int_, [&](int64_t r0, int64_t r1) {
     for (int64_t r = r0; r < r1; ++r) {
       const int i = int_edge[r];
-      int64_t c = 0;
+      int64_t c = 0, a = 0;
       for (int64_t q = rowptr_[i]; q < rowptr_[i + 1]; ++q) {
         const int j = col_[q];
         c += (int_id[j] >= 0 && int_id[j] <= r);
+        a += (int_id[j] >= 0 && j != i);
       }
       lptr[r + 1] = c;
+      aptr[r + 1] = a;
       for (int a = 0; a < 3; ++a)
         xyz[3 * r + a] = 0.5 * (m_.xyz[m_.edge_nodes[i][0]][a] + m_.xyz[m_.edge_nodes[i][1]][a]);
     }
   });
-  for (int64_t r = 0; r < n_int_; ++r) lptr[r + 1] += lptr[r];
+  for (int64_t r = 0; r < n_int_; ++r) {
+    lptr[r + 1] += lptr[r];
+    aptr[r + 1] += aptr[r];
+  }
   std::vector<int64_t> src(lptr[n_int_]);
-  std::vector<int> lcol(lptr[n_int_]);
+  std::vector<int> lcol(lptr[n_int_]), adj(aptr[n_int_]);
   std::vector<uint8_t> diag(lptr[n_int_]);
   parallel_ranges(n_int_, [&](int64_t r0, int64_t r1) {
     for (int64_t r = r0; r < r1; ++r) {
       const int i = int_edge[r];
-      int64_t o = lptr[r];
+      int64_t o = lptr[r], oa = aptr[r];
       for (int64_t q = rowptr_[i]; q < rowptr_[i + 1]; ++q) {
         const int j = col_[q];
         if (int_id[j] >= 0 && int_id[j] <= r) {
@@ -420,12 +425,15 @@ std::string TransientSolve::plan_model(const RunOptions& opt, double t0) {
           diag[o] = int_id[j] == r;
           ++o;
         }
+        if (int_id[j] >= 0 && j != i) adj[oa++] = int_id[j];
       }
     }
   });
   if (opt.precision != 64 && opt.precision != 32) return main_error("precision must be 64 or 32");
   sy_.reset(new Symbolic());
-  e = analyse((int)n_int_, lptr.data(), lcol.data(), xyz.data(), *sy_, opt.leaf_size);
+  // the interior graph's adjacency comes from the full pattern's rows (ascending, the
+  // order the analysis would build from the lower triangle)
+  e = analyse((int)n_int_, lptr.data(), lcol.data(), xyz.data(), *sy_, opt.leaf_size, aptr.data(), adj.data());
   if (!e.empty()) return main_error("analysis: " + e);
   p2v_.resize(n_int_);
   for (int64_t p = 0; p < n_int_; ++p) p2v_[p] = int_edge[sy_->iperm[p]];

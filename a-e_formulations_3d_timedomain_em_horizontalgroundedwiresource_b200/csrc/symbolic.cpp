@@ -16,10 +16,13 @@
 namespace tdem {
 namespace {
 
+// symmetric adjacency without the diagonal: the caller's arrays or its own storage
 struct Graph {
   int n = 0;
-  std::vector<int64_t> xadj;
-  std::vector<int> adj;
+  const int64_t* xadj = nullptr;  // n + 1 row starts
+  const int* adj = nullptr;
+  std::vector<int64_t> xadj_store;
+  std::vector<int> adj_store;
 };
 
 // Recursive dissection producing fronts in postorder.
@@ -284,7 +287,7 @@ inline int64_t cdiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
 }  // namespace
 
 std::string analyse(int n, const int64_t* rowptr, const int* colind, const double* coords,
-                    Symbolic& sy, int leaf_size) {
+                    Symbolic& sy, int leaf_size, const int64_t* adj_ptr, const int* adj) {
   sy = Symbolic();
   sy.n = n;
   sy.nnz_lower = rowptr[n];
@@ -293,10 +296,24 @@ std::string analyse(int n, const int64_t* rowptr, const int* colind, const doubl
   // symmetric adjacency without the diagonal
   Graph g;
   g.n = n;
-  // Row v lists its own lower entries (CSR order) and then the rows i > v that hold
-  // an entry in column v, ascending.  The transposed part is placed per range of
-  // rows after the entries of the lower ranges, which keeps that order.
-  {
+  if (adj_ptr && adj) {
+    // the caller's (each row ascending, the order built below); the lower triangle is
+    // only checked
+    std::vector<char> bad(host_threads() + 1, 0);
+    parallel_ranges(n, [&](int64_t i0, int64_t i1) {
+      for (int64_t i = i0; i < i1; ++i)
+        for (int64_t q = rowptr[i]; q < rowptr[i + 1]; ++q)
+          if (colind[q] < 0 || colind[q] > i) bad[0] = 1;
+    });
+    if (bad[0]) return "lower-triangle pattern expected (column index out of range)";
+    g.xadj = adj_ptr;
+    g.adj = adj;
+  } else {
+    // Row v lists its own lower entries (CSR order) and then the rows i > v that hold
+    // an entry in column v, ascending.  The transposed part is placed per range of
+    // rows after the entries of the lower ranges, which keeps that order.
+    std::vector<int64_t>& xadj = g.xadj_store;
+    std::vector<int>& adjv = g.adj_store;
     const int nt = chunk_count(n, 16384);
     std::vector<int64_t> own(n, 0);
     std::vector<int> upper((size_t)nt * n, 0);  // per range: entries of each column
@@ -317,37 +334,39 @@ std::string analyse(int n, const int64_t* rowptr, const int* colind, const doubl
     });
     for (char b : bad)
       if (b) return "lower-triangle pattern expected (column index out of range)";
-    g.xadj.assign(n + 1, 0);
+    xadj.assign(n + 1, 0);
     for (int v = 0; v < n; ++v) {
       int64_t d = own[v];
       for (int t = 0; t < nt; ++t) d += upper[(size_t)t * n + v];
-      g.xadj[v + 1] = g.xadj[v] + d;
+      xadj[v + 1] = xadj[v] + d;
     }
     // turn the per-range counts into the first slot of each range in each column
     parallel_ranges(n, [&](int64_t v0, int64_t v1) {
       for (int64_t v = v0; v < v1; ++v) {
-        int64_t at = g.xadj[v] + own[v];
+        int64_t at = xadj[v] + own[v];
         for (int t = 0; t < nt; ++t) {
           int& c = upper[(size_t)t * n + v];
           const int k = c;
-          c = (int)(at - g.xadj[v]);
+          c = (int)(at - xadj[v]);
           at += k;
         }
       }
     });
-    g.adj.resize(g.xadj[n]);
+    adjv.resize(xadj[n]);
     parallel_chunks(n, nt, [&](int t, int64_t i0, int64_t i1) {
       int* up = upper.data() + (size_t)t * n;
       for (int64_t i = i0; i < i1; ++i) {
-        int64_t o = g.xadj[i];
+        int64_t o = xadj[i];
         for (int64_t q = rowptr[i]; q < rowptr[i + 1]; ++q) {
           const int j = colind[q];
           if (j == i) continue;
-          g.adj[o++] = j;
-          g.adj[g.xadj[j] + up[j]++] = (int)i;
+          adjv[o++] = j;
+          adjv[xadj[j] + up[j]++] = (int)i;
         }
       }
     });
+    g.xadj = xadj.data();
+    g.adj = adjv.data();
   }
 
   // ordering + tree

@@ -145,14 +145,18 @@ struct Symbolic {
   int64_t solve_partials = 0; // scratch entries per RHS column for backward partial sums
 };
 
-// Analyse the lower triangle (row i holds columns j <= i, diagonal included)
-// of a symmetric n x n matrix.  coords (n x 3) are optional unknown positions.
-// Returns an empty string on success, an error message otherwise.
 // FNV-1a hash of the ordering, the fronts' columns and rows, the entry map and the
 // level-solve units (equal hashes: identical factorization and solve launches)
 uint64_t plan_digest(const Symbolic& sy);
 
+// Analyse the lower triangle (row i holds columns j <= i, diagonal included)
+// of a symmetric n x n matrix.  coords (n x 3) are optional unknown positions.
+// Returns an empty string on success, an error message otherwise.
+// adj_ptr/adj (optional): the same matrix's symmetric adjacency without the diagonal,
+// each row ascending (n + 1 row starts); when given it is used instead of being built
+// from the lower triangle, and the result is the same.
 std::string analyse(int n, const int64_t* rowptr, const int* colind, const double* coords,
-                    Symbolic& out, int leaf_size = 128);
+                    Symbolic& out, int leaf_size = 128, const int64_t* adj_ptr = nullptr,
+                    const int* adj = nullptr);
 
 }  // namespace tdem
