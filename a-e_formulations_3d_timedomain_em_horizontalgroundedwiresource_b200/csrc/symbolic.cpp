@@ -38,16 +38,34 @@ class Dissector {
     // then count values instead of sorting them (same order, same cuts)
     if (xyz_) {
       own_rank_.resize(3 * (size_t)g.n);
-      parallel_ranges(3, [&](int64_t a0, int64_t a1) {
-        for (int a = (int)a0; a < (int)a1; ++a) {
-          std::vector<double> vals(g.n);
-          for (int v = 0; v < g.n; ++v) vals[v] = c(v, a);
-          std::sort(vals.begin(), vals.end());
-          vals.erase(std::unique(vals.begin(), vals.end()), vals.end());
-          for (int v = 0; v < g.n; ++v)
-            own_rank_[3 * (size_t)v + a] = (int)(std::lower_bound(vals.begin(), vals.end(), c(v, a)) - vals.begin());
+      // distinct values per axis: each range of vertices sorts and deduplicates its
+      // own, then the (short, on a tensor-product mesh) lists are merged
+      const int nt = chunk_count(g.n, 65536);
+      std::vector<double> vals[3];
+      std::vector<std::vector<double>> part((size_t)3 * nt);
+      parallel_chunks(g.n, nt, [&](int t, int64_t v0, int64_t v1) {
+        for (int a = 0; a < 3; ++a) {
+          std::vector<double>& p = part[(size_t)a * nt + t];
+          p.reserve((size_t)(v1 - v0));
+          for (int64_t v = v0; v < v1; ++v) p.push_back(c((int)v, a));
+          std::sort(p.begin(), p.end());
+          p.erase(std::unique(p.begin(), p.end()), p.end());
         }
-      }, 1);
+      });
+      for (int a = 0; a < 3; ++a) {
+        for (int t = 0; t < nt; ++t) {
+          const std::vector<double>& p = part[(size_t)a * nt + t];
+          vals[a].insert(vals[a].end(), p.begin(), p.end());
+        }
+        std::sort(vals[a].begin(), vals[a].end());
+        vals[a].erase(std::unique(vals[a].begin(), vals[a].end()), vals[a].end());
+      }
+      parallel_ranges(g.n, [&](int64_t v0, int64_t v1) {
+        for (int64_t v = v0; v < v1; ++v)
+          for (int a = 0; a < 3; ++a)
+            own_rank_[3 * (size_t)v + a] =
+                (int)(std::lower_bound(vals[a].begin(), vals[a].end(), c((int)v, a)) - vals[a].begin());
+      });
       grank_ = own_rank_.data();
     }
   }
