@@ -6,6 +6,7 @@
 #include "parallel.h"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 #include <climits>
@@ -79,7 +80,10 @@ class Dissector {
     if ((int)verts.size() <= leaf_) return emit(verts, {});
     std::vector<int> L, S, R;
     int kind = 0;
-    if (xyz_ && split_coords(verts, L, S, R)) kind = 1;
+    // threads for the passes of one large split: all at the top, fewer where the
+    // recursion already runs on several threads
+    const int split_threads = (int)verts.size() >= kParSplitMin ? std::max(1, host_threads() >> (3 - std::min(depth, 3))) : 1;
+    if (xyz_ && split_coords(verts, L, S, R, split_threads)) kind = 1;
     if (!kind) kind = split_levels(verts, L, S, R);
     if (!kind) return emit(verts, {});
     std::vector<int>().swap(verts);
@@ -113,6 +117,7 @@ class Dissector {
 
  private:
   static constexpr size_t kForkMin = 20000;
+  static constexpr int kParSplitMin = 100000;
   const Graph& g_;
   const double* xyz_;
   int leaf_;
@@ -155,23 +160,61 @@ class Dissector {
   // populated coordinate value inside the central 30 % (a node plane on a
   // tensor-product mesh).  The separator is the set of vertices at or above the
   // cut that touch a vertex below it.
+  // nt > 1: the histograms and the partition run on nt ranges of verts, each with its
+  // own counts and lists, summed and concatenated in range order (the same result)
   bool split_coords(const std::vector<int>& verts, std::vector<int>& L, std::vector<int>& S,
-                    std::vector<int>& R) {
+                    std::vector<int>& R, int nt = 1) {
     const size_t nv = verts.size();
     // per axis: histogram of the coordinate ranks over [lo, hi]
     int ndist[3], lo[3];
-    for (int a = 0; a < 3; ++a) {
-      int l = INT_MAX, h = -1;
-      for (int v : verts) {
-        const int r = rank(v, a);
-        l = std::min(l, r);
-        h = std::max(h, r);
+    {
+      std::vector<std::array<int, 6>> ext(nt);  // per range: min and max rank per axis
+      parallel_chunks((int64_t)nv, nt, [&](int t, int64_t b, int64_t e) {
+        std::array<int, 6>& x = ext[t];
+        for (int a = 0; a < 3; ++a) {
+          x[a] = INT_MAX;
+          x[3 + a] = -1;
+        }
+        for (int64_t i = b; i < e; ++i)
+          for (int a = 0; a < 3; ++a) {
+            const int r = rank(verts[i], a);
+            x[a] = std::min(x[a], r);
+            x[3 + a] = std::max(x[3 + a], r);
+          }
+      });
+      int hi[3];
+      for (int a = 0; a < 3; ++a) {
+        lo[a] = INT_MAX;
+        hi[a] = -1;
+        for (const std::array<int, 6>& x : ext) {
+          lo[a] = std::min(lo[a], x[a]);
+          hi[a] = std::max(hi[a], x[3 + a]);
+        }
       }
-      lo[a] = l;
-      std::vector<int>& cnt = cnt_[a];
-      cnt.assign((size_t)(h - l + 1), 0);
-      for (int v : verts) ++cnt[rank(v, a) - l];
-      ndist[a] = (int)(cnt.size() - std::count(cnt.begin(), cnt.end(), 0));
+      size_t span = 0;
+      for (int a = 0; a < 3; ++a) span += (size_t)(hi[a] - lo[a] + 1);
+      const int ht = span <= ((size_t)1 << 20) ? nt : 1;  // per-range histograms only when short
+      std::vector<std::vector<int>> part(ht);
+      parallel_chunks((int64_t)nv, ht, [&](int t, int64_t b, int64_t e) {
+        std::vector<int>& h = part[t];
+        h.assign(span, 0);
+        for (int64_t i = b; i < e; ++i) {
+          size_t off = 0;
+          for (int a = 0; a < 3; ++a) {
+            ++h[off + (size_t)(rank(verts[i], a) - lo[a])];
+            off += (size_t)(hi[a] - lo[a] + 1);
+          }
+        }
+      });
+      size_t off = 0;
+      for (int a = 0; a < 3; ++a) {
+        std::vector<int>& cnt = cnt_[a];
+        cnt.assign((size_t)(hi[a] - lo[a] + 1), 0);
+        for (const std::vector<int>& h : part)
+          for (size_t k = 0; k < cnt.size(); ++k) cnt[k] += h[off + k];
+        off += cnt.size();
+        ndist[a] = (int)(cnt.size() - std::count(cnt.begin(), cnt.end(), 0));
+      }
     }
     int axes[3] = {0, 1, 2};
     std::sort(axes, axes + 3, [&](int a, int b) { return ndist[a] > ndist[b]; });
@@ -200,22 +243,32 @@ class Dissector {
         }
       }
       if (cut <= lo[a]) continue;
-      ++stamp_;
-      for (int v : verts) mark_[v] = stamp_;
+      const int st = ++stamp_;
+      parallel_chunks((int64_t)nv, nt, [&](int, int64_t b, int64_t e) {
+        for (int64_t i = b; i < e; ++i) mark_[verts[i]] = st;
+      });
+      // 0: below the cut, 1: at or above it and touching a vertex below (separator), 2: the rest
+      auto side = [&](int v) {
+        if (rank(v, a) < cut) return 0;
+        for (int64_t p = g_.xadj[v]; p < g_.xadj[v + 1]; ++p) {
+          const int u = g_.adj[p];
+          if (mark_[u] == st && rank(u, a) < cut) return 1;
+        }
+        return 2;
+      };
       L.clear();
       S.clear();
       R.clear();
-      for (int v : verts) {
-        if (rank(v, a) < cut) {
-          L.push_back(v);
-          continue;
-        }
-        bool touch = false;
-        for (int64_t p = g_.xadj[v]; p < g_.xadj[v + 1] && !touch; ++p) {
-          const int u = g_.adj[p];
-          touch = (mark_[u] == stamp_ && rank(u, a) < cut);
-        }
-        (touch ? S : R).push_back(v);
+      std::vector<int>* out[3] = {&L, &S, &R};
+      if (nt == 1) {
+        for (int v : verts) out[side(v)]->push_back(v);
+      } else {
+        std::vector<std::array<std::vector<int>, 3>> piece(nt);
+        parallel_chunks((int64_t)nv, nt, [&](int t, int64_t b, int64_t e) {
+          for (int64_t i = b; i < e; ++i) piece[t][side(verts[i])].push_back(verts[i]);
+        });
+        for (int k = 0; k < 3; ++k)
+          for (int t = 0; t < nt; ++t) out[k]->insert(out[k]->end(), piece[t][k].begin(), piece[t][k].end());
       }
       if (!L.empty() && !S.empty()) return true;
     }
