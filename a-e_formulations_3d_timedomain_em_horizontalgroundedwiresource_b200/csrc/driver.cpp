@@ -347,10 +347,21 @@ std::string TransientSolve::plan_model(const RunOptions& opt, double t0) {
     if (!e.empty()) return e;
   }
 
-  // the initial field, the source vectors and the receiver operators read only the
-  // model: they are built on a second thread while the patterns and the analysis run
+  // the initial field, and the source vectors with the receiver operators, read only
+  // the model: they are built on two more threads while the patterns and the analysis
+  // run (the threads are joined on every way out of this scope)
   std::string e_init, e_rec;
-  std::thread side([this, &opt, &e_init, &e_rec] {
+  std::thread side_init, side_rec;
+  struct Join {
+    std::thread& a;
+    std::thread& b;
+    void operator()() {
+      if (a.joinable()) a.join();
+      if (b.joinable()) b.join();
+    }
+    ~Join() { (*this)(); }
+  } join_sides{side_init, side_rec};
+  side_init = std::thread([this, &opt, &e_init] {
     try {
       if (parts_.empty()) {
         e_init = load_initial_field(m_, opt.formulation == 1, u0_);
@@ -364,17 +375,19 @@ std::string TransientSolve::plan_model(const RunOptions& opt, double t0) {
           u0_.insert(u0_.end(), u.begin(), u.end());
         }
       }
-      if (e_init.empty()) e_rec = build_sources_and_receivers();
     } catch (const std::exception& x) {
       e_init = std::string("host error: ") + x.what();
     }
   });
-  struct Join {
-    std::thread& t;
-    ~Join() { if (t.joinable()) t.join(); }
-  } join{side};
+  side_rec = std::thread([this, &e_rec] {
+    try {
+      e_rec = build_sources_and_receivers();
+    } catch (const std::exception& x) {
+      e_rec = std::string("host error: ") + x.what();
+    }
+  });
   auto main_error = [&](const std::string& err) {
-    side.join();
+    join_sides();
     return e_init.empty() ? err : e_init;
   };
 
@@ -439,7 +452,7 @@ std::string TransientSolve::plan_model(const RunOptions& opt, double t0) {
   for (int64_t p = 0; p < n_int_; ++p) p2v_[p] = int_edge[sy_->iperm[p]];
   src_ = std::move(src);
   diag_ = std::move(diag);
-  side.join();
+  join_sides();
   if (!e_init.empty()) return e_init;
   if (!e_rec.empty()) return e_rec;
   pt_.setup_s = now_s() - t0;

@@ -437,8 +437,10 @@ std::string load_initial_field(const Model& m, const std::string& dir, int npls,
   if (!eform) {
     std::vector<double> a0(nn * 3 * np);
     if (!read_binary(path(m, "a0.dat"), a0.data(), a0.size() * 8)) return "cannot read a0.dat";
+    // every (source, edge) value on its own: ranges of edges on host threads
+    parallel_ranges((int64_t)n, [&](int64_t e0, int64_t e1) {
     for (size_t p = 0; p < np; ++p)
-      for (size_t e = 0; e < n; ++e) {
+      for (size_t e = (size_t)e0; e < (size_t)e1; ++e) {
         const int v1 = m.edge_nodes[e][0], v2 = m.edge_nodes[e][1];
         double axis[3], mid[3], len2 = 0.0, dot = 0.0;
         for (int j = 0; j < 3; ++j) {
@@ -450,11 +452,13 @@ std::string load_initial_field(const Model& m, const std::string& dir, int npls,
         const double len = std::sqrt(len2);
         u0[e + p * n] = dot / std::sqrt(len2) * len * 0.5;
       }
+    });
   } else {
     std::vector<double> va(nn * np);
     if (!read_binary(path(m, "v3a.dat"), va.data(), va.size() * 8)) return "cannot read v3a.dat";
+    parallel_ranges((int64_t)n, [&](int64_t e0, int64_t e1) {
     for (size_t p = 0; p < np; ++p)
-      for (size_t e = 0; e < n; ++e) {
+      for (size_t e = (size_t)e0; e < (size_t)e1; ++e) {
         const int v1 = m.edge_nodes[e][0], v2 = m.edge_nodes[e][1];
         double len2 = 0.0;
         for (int j = 0; j < 3; ++j) {
@@ -465,6 +469,7 @@ std::string load_initial_field(const Model& m, const std::string& dir, int npls,
         const double etan = -(va[v2 + p * nn] - va[v1 + p * nn]) / len;
         u0[e + p * n] = etan * len * 0.5;
       }
+    });
   }
   return "";
 }
