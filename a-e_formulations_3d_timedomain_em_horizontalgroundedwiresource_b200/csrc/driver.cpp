@@ -293,11 +293,15 @@ std::string TransientSolve::plan_merged(const std::vector<std::string>& dirs, co
   if (opt.formulation != 0 && opt.formulation != 1) return "formulation must be 0 (A) or 1 (E)";
   if (opt.scheme != 2 && opt.scheme != 3) return "scheme must be 2 or 3";
   if (dirs.empty()) return "no model directories";
+  // the directories are read side by side; the first failure in order is reported
   std::vector<Model> parts(dirs.size());
-  for (size_t i = 0; i < dirs.size(); ++i) {
-    std::string e = load_model(dirs[i], parts[i]);
-    if (!e.empty()) return dirs[i] + ": " + e;
-  }
+  std::vector<std::string> errs(dirs.size());
+  parallel_chunks((int64_t)dirs.size(), (int)std::min<size_t>(dirs.size(), (size_t)host_threads()),
+                  [&](int, int64_t b, int64_t e) {
+                    for (int64_t i = b; i < e; ++i) errs[i] = load_model(dirs[i], parts[i]);
+                  });
+  for (size_t i = 0; i < dirs.size(); ++i)
+    if (!errs[i].empty()) return dirs[i] + ": " + errs[i];
   std::string e = merge_models(parts, m_);
   if (!e.empty()) return e;
   parts_.clear();
