@@ -103,6 +103,12 @@ class TransientSolve {
   std::string flush_marks();
 
   const Model& model() const { return m_; }
+  // Host products of plan(), until setup_device() moves them to the device: the source
+  // vectors and the initial field (n x npls, column-major) and the receiver operators.
+  const std::vector<double>& planned_sources() const { return S_; }
+  const std::vector<double>& planned_initial_field() const { return u0_; }
+  const ReceiverOperator& planned_receivers_b() const { return rop_b_; }
+  const ReceiverOperator& planned_receivers_e() const { return rop_e_; }
   const PhaseTimes& times() const { return pt_; }
   int first_layer() const { return tlf_; }
   int last_layer() const { return tll_; }
