@@ -5,7 +5,8 @@
 //   <argv[3]>.u0   initial field, n x npls doubles
 //   <argv[3]>.rb / .re   receiver operators: int64 nrec, nrows, nnz; int64 rowptr[nrows + 1];
 //                        int32 col[nnz]; double val[nnz]; int32 src[nrows]
-// and prints "ok <n> <npls>".
+// and prints "ok <n> <npls>".  With argv[1] = "--merged": host_plan_dump --merged <0|1>
+// <out prefix> <dir>...  plans the directories as one merged run (plan_merged).
 #include <cstdio>
 #include <cstdlib>
 #include <string>
@@ -34,20 +35,23 @@ static bool dump_op(const std::string& fn, const ReceiverOperator& r) {
 }
 
 int main(int argc, char** argv) {
-  if (argc < 4) {
-    printf("usage: host_plan_dump <dir> <0|1> <out prefix>\n");
+  const bool merged = argc > 1 && std::string(argv[1]) == "--merged";
+  if (argc < (merged ? 5 : 4)) {
+    printf("usage: host_plan_dump <dir> <0|1> <out prefix> | --merged <0|1> <out prefix> <dir>...\n");
     return 2;
   }
+  // both forms hold <0|1> and <out prefix> in argv[2] and argv[3]
   TransientSolve ts;
   RunOptions opt;
-  opt.formulation = std::atoi(argv[2]);
   opt.scheme = 2;
-  const std::string e = ts.plan(argv[1], opt);
+  opt.formulation = std::atoi(argv[2]);
+  const std::string out = argv[3];
+  const std::string e = merged ? ts.plan_merged(std::vector<std::string>(argv + 4, argv + argc), opt)
+                               : ts.plan(argv[1], opt);
   if (!e.empty()) {
     printf("plan: %s\n", e.c_str());
     return 1;
   }
-  const std::string out = argv[3];
   if (!dump_vec(out + ".S", ts.planned_sources()) || !dump_vec(out + ".u0", ts.planned_initial_field()) ||
       !dump_op(out + ".rb", ts.planned_receivers_b()) || !dump_op(out + ".re", ts.planned_receivers_e())) {
     printf("write failed\n");

@@ -275,3 +275,64 @@ def test_host_plan_products_match_the_oracle(pkg, golden, tmp_path, case, form):
         want = tdem_oracle.ReceiverSet(m, np.asarray(pts), curl).evaluate(u, own)
         # CG to 1e-15 against a direct solve: measured up to 2.5e-15 of the peak
         assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max(), (key, np.abs(got - want).max())
+
+
+def test_merged_host_plan_is_the_parts_side_by_side(pkg, mg, tmp_path):
+    """plan_merged (the serving loop's batched time steps), host half: the source vectors
+    and initial fields of three directories over one mesh are their solo plans' columns
+    side by side, and every receiver row is its solo plan's row (each directory's receivers
+    smoothed on their own neighbourhood), placed component-major over all receivers and
+    sampling the directory's shifted source column."""
+    import dataclasses
+    import shutil
+    import subprocess
+    if shutil.which("g++") is None:
+        pytest.skip("no C++ compiler")
+    here = os.path.dirname(os.path.abspath(__file__))
+    lib_dir = os.path.dirname(pkg.LIB_PATH)
+    exe = str(tmp_path / "dump")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", os.path.join(os.path.dirname(pkg.__file__), "csrc"),
+                    "-I", os.path.join(os.path.dirname(here), "include"), "-I", "/usr/local/cuda/include",
+                    os.path.join(here, "native", "host_plan_dump.cpp"), "-L" + lib_dir, "-ltdem_b200",
+                    "-Wl,-rpath," + lib_dir, "-o", exe], check=True)
+    base = mg.small_model(cells=8, n_dec=2, steps_per_dec=4)
+    dirs = []
+    for i, wires in enumerate([[((-30.0, 0.0, 0.0), (30.0, 0.0, 0.0))],
+                               [((-30.0, 20.0, 0.0), (30.0, 20.0, 0.0)), ((0.0, -40.0, 0.0), (0.0, 20.0, 0.0))],
+                               [((-20.0, -20.0, 0.0), (40.0, -20.0, 0.0))]]):
+        rec = [(0.0, 15.0 + 5.0 * i + 25.0 * k, 0.0) for k in range(3 + i)]
+        spec = dataclasses.replace(base, sources=wires, receivers_b=[rec] * len(wires),
+                                   receivers_e=[rec] * len(wires))
+        d = str(tmp_path / ("tx%d" % i))
+        mg.write_model(d, spec)
+        mg.write_analytic_initial_field(d, spec)
+        dirs.append(d)
+    for form in ("0", "1"):
+        solo = []
+        for k, d in enumerate(dirs):
+            out = str(tmp_path / ("solo%d_%s" % (k, form)))
+            r = subprocess.run([exe, d, form, out], capture_output=True, text=True)
+            assert r.returncode == 0, r.stdout + r.stderr
+            solo.append((out, int(r.stdout.split()[2])))
+        out = str(tmp_path / ("merged_" + form))
+        r = subprocess.run([exe, "--merged", form, out] + dirs, capture_output=True, text=True)
+        assert r.returncode == 0, r.stdout + r.stderr
+        n, npls = (int(v) for v in r.stdout.split()[1:3])
+        assert npls == sum(p for _, p in solo)
+        for ext in (".S", ".u0"):
+            want = np.concatenate([np.fromfile(o + ext) for o, _ in solo])
+            assert np.array_equal(np.fromfile(out + ext), want), ext
+        for key in ("rb", "re"):
+            nrec, rp, col, val, src = _read_operator(out + "." + key)
+            parts = [_read_operator(o + "." + key) for o, _ in solo]
+            assert nrec == sum(p[0] for p in parts)
+            for c in range(3):
+                roff = coff = 0
+                for (nr, prp, pcol, pval, psrc), (_, pn) in zip(parts, solo):
+                    for i in range(nr):
+                        a, b = c * nrec + roff + i, c * nr + i
+                        assert np.array_equal(col[rp[a]:rp[a + 1]], pcol[prp[b]:prp[b + 1]])
+                        assert np.array_equal(val[rp[a]:rp[a + 1]], pval[prp[b]:prp[b + 1]])
+                        assert src[a] == psrc[b] + coff
+                    roff += nr
+                    coff += pn
