@@ -75,14 +75,24 @@ class Dissector {
   struct Node { int c0, c1; std::vector<int> kids; };
   std::vector<Node> nodes;
 
-  // depth: splits still allowed to fork a thread below this call
-  int build(std::vector<int>& verts, int depth = 3) {
+  // levels of splits that fork their second half onto a thread: enough for one
+  // subtree per host thread (the forked halves are appended in serial order, so the
+  // result does not depend on it)
+  static int fork_depth() {
+    int d = 0;
+    while ((1 << d) < host_threads() && d < 5) ++d;
+    return d;
+  }
+
+  // depth: splits still allowed to fork a thread below this call (fork_depth() at the top)
+  int build(std::vector<int>& verts, int depth) {
     if ((int)verts.size() <= leaf_) return emit(verts, {});
     std::vector<int> L, S, R;
     int kind = 0;
     // threads for the passes of one large split: all at the top, fewer where the
     // recursion already runs on several threads
-    const int split_threads = (int)verts.size() >= kParSplitMin ? std::max(1, host_threads() >> (3 - std::min(depth, 3))) : 1;
+    const int split_threads =
+        (int)verts.size() >= kParSplitMin ? std::max(1, host_threads() >> std::max(0, fork_depth() - depth)) : 1;
     if (xyz_ && split_coords(verts, L, S, R, split_threads)) kind = 1;
     if (!kind) kind = split_levels(verts, L, S, R);
     if (!kind) return emit(verts, {});
@@ -445,7 +455,7 @@ std::string analyse(int n, const int64_t* rowptr, const int* colind, const doubl
   {
     std::vector<int> all(n);
     std::iota(all.begin(), all.end(), 0);
-    d.build(all);
+    d.build(all, Dissector::fork_depth());
   }
   sy.iperm = d.order;
   if ((int)sy.iperm.size() != n) return "ordering lost vertices";
