@@ -56,6 +56,29 @@ def test_plan_missing_input_is_an_input_error(pkg, golden, tmp_path):
     assert ei.value.status == 2 and "edges.dat" in str(ei.value)
 
 
+def test_plan_receiver_outside_the_mesh_is_an_input_error(pkg, mg, tmp_path):
+    """A receiver that no element holds stops the run, as the reference does ("There are
+    no elements for receiver(s)", OutputResultant3d.cpp:724-749, which has no nearest-element
+    rule for receivers); a wire past the mesh edge does not (its outer dipoles go to the
+    nearest element)."""
+    import dataclasses
+    base = mg.small_model(cells=8, n_dec=2, steps_per_dec=4)
+    far = float(base.x[-1]) + 500.0
+    spec = dataclasses.replace(base, receivers_b=[[(0.0, 10.0, 0.0), (far, 0.0, 0.0)]],
+                               receivers_e=[[(0.0, 10.0, 0.0)]])
+    d = str(tmp_path / "rec")
+    mg.write_model(d, spec)
+    mg.write_analytic_initial_field(d, spec)
+    with pytest.raises(pkg.TdemError) as ei:
+        pkg.plan(d, "A", 2)
+    assert ei.value.status == 2 and "receiver outside the mesh" in str(ei.value)
+    spec = dataclasses.replace(base, sources=[((far - 900.0, 0.0, 0.0), (far, 0.0, 0.0))])
+    d = str(tmp_path / "wire")
+    mg.write_model(d, spec)
+    mg.write_analytic_initial_field(d, spec)
+    assert pkg.plan(d, "E", 2)["n_sources"] == 1
+
+
 def test_plan_bad_arguments(pkg, tmp_path):
     with pytest.raises(pkg.TdemError) as ei:
         pkg.plan(str(tmp_path), "A", 4)
