@@ -49,6 +49,22 @@ def test_gpu_wire_beyond_the_mesh_matches_reference(pkg, outs, tmp_path, variant
         assert err <= FP64_TOL, (o, err)
 
 
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_gpu_receivers_on_element_boundaries_match_reference(pkg, outs, tmp_path, variant):
+    """Receivers on mesh nodes, edges and faces (the first element in element order holds
+    each, its material picks the field's smoothing subdomain), against the reference."""
+    sys.path.insert(0, GOLDEN)
+    import make_nodes_golden as ng
+    d = str(tmp_path / "gpu")
+    ng.write_case_inputs(d)
+    with pkg.Solver(d, variant[0], int(variant[1])) as s:
+        s.run()
+        s.write_outputs()
+    for o in ng.OUTPUTS:
+        err = outs.compare_files(os.path.join(d, o + ".1"), os.path.join(GOLDEN, ng.CASE, "%s_%s.1" % (variant, o)))
+        assert err <= FP64_TOL, (o, err)
+
+
 @pytest.mark.parametrize("variant", ["A3", "E2"])
 def test_gpu_matches_numpy_oracle(pkg, mg, outs, tmp_path, variant):
     spec = mg.small_model(cells=10, n_dec=3, steps_per_dec=5, block=True)

@@ -193,6 +193,22 @@ def test_numpy_oracle_wire_beyond_the_mesh_matches_reference(outs, tmp_path, var
                                   os.path.join(GOLDEN, bg.CASE, "E2_eall_anom.1")) > 1e-3
 
 
+@pytest.mark.parametrize("variant", ["A2", "A3", "E2", "E3"])
+def test_numpy_oracle_receivers_on_element_boundaries_match_reference(outs, tmp_path, variant):
+    """Receivers on mesh nodes, edges and faces, some on the conductive block's surface:
+    the first element in element order holds each (and, for field values, its material
+    picks the smoothing subdomain), as in the reference (OutputResultant3d.cpp:572-712)."""
+    import sys
+    sys.path.insert(0, GOLDEN)
+    import make_nodes_golden as ng
+    d = str(tmp_path / "nodes")
+    ng.write_case_inputs(d)
+    tdem_oracle.run(d, variant[0], int(variant[1]))
+    for o in ng.OUTPUTS:
+        err = outs.compare_files(os.path.join(d, o + ".1"), os.path.join(GOLDEN, ng.CASE, "%s_%s.1" % (variant, o)))
+        assert err <= FP64_TOL, (o, err)
+
+
 def test_three_point_formulas_exact_for_quadratics():
     """Known answers of the time discretisation (reference math, no reference run):
     the BDF2 step coefficients (A3/time_approx.cpp:943-945) and the three-point
