@@ -47,23 +47,42 @@ def write_receivers(path: str) -> None:
             f.write("%d\n" % len(RECEIVERS))
 
 
-def write_case_inputs(path: str) -> None:
-    """cube8_block's inputs with the stored receiver files of this case."""
+# the second case: cube8_two_wires with ragged receiver lists per source (B: 2 and 5,
+# E: 3 and 1), the per-source ranges of recvsb / recvse (TaskSP.cpp:467-516)
+CASE_RAGGED = "cube8_two_wires_ragged"
+BASE_RAGGED = "cube8_two_wires"
+RAGGED_B = [[(0.0, 20.0, 0.0), (5.0, 45.0, 0.0)],
+            [(0.0, 10.0, 0.0), (0.0, 30.0, 0.0), (-15.0, 60.0, 0.0), (25.0, 85.0, 0.0), (0.0, 110.0, 0.0)]]
+RAGGED_E = [[(0.0, 10.0, 0.0), (10.0, 35.0, 0.0), (-5.0, 60.0, 0.0)], [(0.0, 40.0, 0.0)]]
+
+
+def write_ragged_receivers(path: str) -> None:
+    for xyz, cnt, lists in (("xyzVectorB", "recvsb", RAGGED_B), ("xyzVectorE", "recvse", RAGGED_E)):
+        pts = [p for lst in lists for p in lst]
+        with open(os.path.join(path, xyz), "w") as f:
+            f.write("%d\n" % len(pts))
+            f.write("".join("%f %f %f\n" % p for p in pts))
+        with open(os.path.join(path, cnt), "w") as f:
+            f.write("".join("%d\n" % len(lst) for lst in lists))
+
+
+def write_case_inputs(path: str, case: str = CASE) -> None:
+    """The base case's inputs with the stored receiver files of `case`."""
     import make_golden
-    make_golden.write_case_inputs(BASE, path)
+    make_golden.write_case_inputs(BASE if case == CASE else BASE_RAGGED, path)
     for name in FILES:
-        shutil.copy2(os.path.join(HERE, CASE, name), os.path.join(path, name))
+        shutil.copy2(os.path.join(HERE, case, name), os.path.join(path, name))
 
 
-def main() -> None:
+def make_case(case: str, base: str, write, npls: int) -> None:
     import make_golden
     import run_ref
-    out = os.path.join(HERE, CASE)
+    out = os.path.join(HERE, case)
     os.makedirs(out, exist_ok=True)
     work = tempfile.mkdtemp(prefix="golden_nodes_")
     try:
-        make_golden.write_case_inputs(BASE, work)
-        write_receivers(work)
+        make_golden.write_case_inputs(base, work)
+        write(work)
         for name in FILES:
             shutil.copy2(os.path.join(work, name), os.path.join(out, name))
         for v in VARIANTS:
@@ -71,9 +90,15 @@ def main() -> None:
             run_ref.copy_inputs(work, d)
             run_ref.run_transient(d, v)
             for o in OUTPUTS:
-                shutil.copy2(os.path.join(d, "%s.1" % o), os.path.join(out, "%s_%s.1" % (v, o)))
+                for p in range(1, npls + 1):
+                    shutil.copy2(os.path.join(d, "%s.%d" % (o, p)), os.path.join(out, "%s_%s.%d" % (v, o, p)))
     finally:
         shutil.rmtree(work, ignore_errors=True)
+
+
+def main() -> None:
+    make_case(CASE, BASE, write_receivers, 1)
+    make_case(CASE_RAGGED, BASE_RAGGED, write_ragged_receivers, 2)
 
 
 if __name__ == "__main__":

@@ -50,19 +50,22 @@ def test_gpu_wire_beyond_the_mesh_matches_reference(pkg, outs, tmp_path, variant
 
 
 @pytest.mark.parametrize("variant", VARIANTS)
-def test_gpu_receivers_on_element_boundaries_match_reference(pkg, outs, tmp_path, variant):
+@pytest.mark.parametrize("case,npls", [("cube8_receivers_on_nodes", 1), ("cube8_two_wires_ragged", 2)])
+def test_gpu_receivers_on_element_boundaries_match_reference(pkg, outs, tmp_path, case, npls, variant):
     """Receivers on mesh nodes, edges and faces (the first element in element order holds
     each, its material picks the field's smoothing subdomain), against the reference."""
     sys.path.insert(0, GOLDEN)
     import make_nodes_golden as ng
     d = str(tmp_path / "gpu")
-    ng.write_case_inputs(d)
+    ng.write_case_inputs(d, case)
     with pkg.Solver(d, variant[0], int(variant[1])) as s:
         s.run()
         s.write_outputs()
     for o in ng.OUTPUTS:
-        err = outs.compare_files(os.path.join(d, o + ".1"), os.path.join(GOLDEN, ng.CASE, "%s_%s.1" % (variant, o)))
-        assert err <= FP64_TOL, (o, err)
+        for p in range(1, npls + 1):
+            err = outs.compare_files(os.path.join(d, "%s.%d" % (o, p)),
+                                     os.path.join(GOLDEN, case, "%s_%s.%d" % (variant, o, p)))
+            assert err <= FP64_TOL, (o, p, err)
 
 
 @pytest.mark.parametrize("variant", ["A3", "E2"])

@@ -194,19 +194,23 @@ def test_numpy_oracle_wire_beyond_the_mesh_matches_reference(outs, tmp_path, var
 
 
 @pytest.mark.parametrize("variant", ["A2", "A3", "E2", "E3"])
-def test_numpy_oracle_receivers_on_element_boundaries_match_reference(outs, tmp_path, variant):
+@pytest.mark.parametrize("case,npls", [("cube8_receivers_on_nodes", 1), ("cube8_two_wires_ragged", 2)])
+def test_numpy_oracle_receivers_on_element_boundaries_match_reference(outs, tmp_path, case, npls, variant):
     """Receivers on mesh nodes, edges and faces, some on the conductive block's surface:
     the first element in element order holds each (and, for field values, its material
-    picks the smoothing subdomain), as in the reference (OutputResultant3d.cpp:572-712)."""
+    picks the smoothing subdomain), as in the reference (OutputResultant3d.cpp:572-712);
+    and two sources with ragged receiver lists (recvsb 2 and 5, recvse 3 and 1)."""
     import sys
     sys.path.insert(0, GOLDEN)
     import make_nodes_golden as ng
     d = str(tmp_path / "nodes")
-    ng.write_case_inputs(d)
+    ng.write_case_inputs(d, case)
     tdem_oracle.run(d, variant[0], int(variant[1]))
     for o in ng.OUTPUTS:
-        err = outs.compare_files(os.path.join(d, o + ".1"), os.path.join(GOLDEN, ng.CASE, "%s_%s.1" % (variant, o)))
-        assert err <= FP64_TOL, (o, err)
+        for p in range(1, npls + 1):
+            err = outs.compare_files(os.path.join(d, "%s.%d" % (o, p)),
+                                     os.path.join(GOLDEN, case, "%s_%s.%d" % (variant, o, p)))
+            assert err <= FP64_TOL, (o, p, err)
 
 
 def test_three_point_formulas_exact_for_quadratics():

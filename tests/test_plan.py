@@ -247,7 +247,8 @@ def _read_operator(path):
 
 
 @pytest.mark.parametrize("case,form", [("cube8_two_wires", "A"), ("cube8_two_wires", "E"),
-                                       ("cube6_wire_beyond", "E"), ("cube8_receivers_on_nodes", "E")])
+                                       ("cube6_wire_beyond", "E"), ("cube8_receivers_on_nodes", "E"),
+                                       ("cube8_two_wires_ragged", "A")])
 def test_host_plan_products_match_the_oracle(pkg, golden, tmp_path, case, form):
     """The host half of a solve (TransientSolve::plan, no device) against the numpy oracle,
     which the reference's goldens pin: the source vectors and the initial field that go to
@@ -267,11 +268,14 @@ def test_host_plan_products_match_the_oracle(pkg, golden, tmp_path, case, form):
                     os.path.join(here, "native", "host_plan_dump.cpp"), "-L" + lib_dir, "-ltdem_b200",
                     "-Wl,-rpath," + lib_dir, "-o", exe], check=True)
     d = str(tmp_path / case)
-    if case in ("cube6_wire_beyond", "cube8_receivers_on_nodes"):
+    if case in ("cube6_wire_beyond", "cube8_receivers_on_nodes", "cube8_two_wires_ragged"):
         sys.path.insert(0, os.path.join(here, "golden"))
         import make_beyond_golden as bg
         import make_nodes_golden as ng
-        (bg if case == "cube6_wire_beyond" else ng).write_case_inputs(d)
+        if case == "cube6_wire_beyond":
+            bg.write_case_inputs(d)
+        else:
+            ng.write_case_inputs(d, case)
     else:
         golden.write_case_inputs(case, d)
     out = str(tmp_path / "plan")
