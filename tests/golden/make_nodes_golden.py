@@ -66,10 +66,25 @@ def write_ragged_receivers(path: str) -> None:
             f.write("".join("%d\n" % len(lst) for lst in lists))
 
 
+# the third case: cube6 without B receivers (xyzVectorB and recvsb hold 0); the reference
+# then writes empty edsall_anom / ball_anom files
+CASE_NO_B = "cube6_no_b_receivers"
+BASE_NO_B = "cube6"
+
+
+def write_no_b_receivers(path: str) -> None:
+    for name in ("xyzVectorB", "recvsb"):
+        with open(os.path.join(path, name), "w") as f:
+            f.write("0\n")
+
+
+BASES = {CASE: BASE, CASE_RAGGED: BASE_RAGGED, CASE_NO_B: BASE_NO_B}
+
+
 def write_case_inputs(path: str, case: str = CASE) -> None:
     """The base case's inputs with the stored receiver files of `case`."""
     import make_golden
-    make_golden.write_case_inputs(BASE if case == CASE else BASE_RAGGED, path)
+    make_golden.write_case_inputs(BASES[case], path)
     for name in FILES:
         shutil.copy2(os.path.join(HERE, case, name), os.path.join(path, name))
 
@@ -99,6 +114,7 @@ def make_case(case: str, base: str, write, npls: int) -> None:
 def main() -> None:
     make_case(CASE, BASE, write_receivers, 1)
     make_case(CASE_RAGGED, BASE_RAGGED, write_ragged_receivers, 2)
+    make_case(CASE_NO_B, BASE_NO_B, write_no_b_receivers, 1)
 
 
 if __name__ == "__main__":
