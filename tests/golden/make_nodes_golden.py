@@ -1,4 +1,6 @@
-"""Golden fixtures of receivers on element boundaries: the reference's own
+"""Golden fixtures of receiver edge cases (the first case: receivers on element
+boundaries; the others below: ragged per-source lists, no B receivers, a one-level
+neighbourhood with a printed window inside the grid): the reference's own
 CalcNonstat3DLine_{A2,A3,E2,E3} built from source by oracle/build_ref.sh, run on the
 golden case cube8_block with its receivers replaced by points on mesh nodes, edges and
 faces, some on the surface of the conductive block (x, y in [-30, 30] m, z in [-50, -20] m;
@@ -78,14 +80,33 @@ def write_no_b_receivers(path: str) -> None:
             f.write("0\n")
 
 
-BASES = {CASE: BASE, CASE_RAGGED: BASE_RAGGED, CASE_NO_B: BASE_NO_B}
+# the fourth case: cube8_block with a one-level receiver neighbourhood (n_neib 1) and a
+# printed window inside the grid (timeintervalforprint 2e-4 .. 4.2857e-4 s: from between
+# two layers in the second step-size decade to that decade's last layer), so the output
+# starts mid-decade and ends before the run does (give_out_vec_loop.cpp:52-73).  A window
+# that ends inside a decade is not used: the reference then never projects that decade's
+# receivers (OutputResultant3d.cpp:432-474 solves at the decade's last layer, which
+# Work2 skips past the window, give_out_vec_loop.cpp:234) and prints zeros there.
+CASE_WINDOW = "cube8_neib1_window"
+BASE_WINDOW = "cube8_block"
+
+
+def write_window(path: str) -> None:
+    with open(os.path.join(path, "n_neib"), "w") as f:
+        f.write("1\n")
+    with open(os.path.join(path, "timeintervalforprint"), "w") as f:
+        f.write("2.0000000000000e-04 4.2857142857143e-04\n")
+
+
+BASES = {CASE: BASE, CASE_RAGGED: BASE_RAGGED, CASE_NO_B: BASE_NO_B, CASE_WINDOW: BASE_WINDOW}
+CASE_FILES = {CASE: FILES, CASE_RAGGED: FILES, CASE_NO_B: FILES, CASE_WINDOW: ("n_neib", "timeintervalforprint")}
 
 
 def write_case_inputs(path: str, case: str = CASE) -> None:
-    """The base case's inputs with the stored receiver files of `case`."""
+    """The base case's inputs with the stored files of `case`."""
     import make_golden
     make_golden.write_case_inputs(BASES[case], path)
-    for name in FILES:
+    for name in CASE_FILES[case]:
         shutil.copy2(os.path.join(HERE, case, name), os.path.join(path, name))
 
 
@@ -98,7 +119,7 @@ def make_case(case: str, base: str, write, npls: int) -> None:
     try:
         make_golden.write_case_inputs(base, work)
         write(work)
-        for name in FILES:
+        for name in CASE_FILES[case]:
             shutil.copy2(os.path.join(work, name), os.path.join(out, name))
         for v in VARIANTS:
             d = os.path.join(work, v)
@@ -115,6 +136,7 @@ def main() -> None:
     make_case(CASE, BASE, write_receivers, 1)
     make_case(CASE_RAGGED, BASE_RAGGED, write_ragged_receivers, 2)
     make_case(CASE_NO_B, BASE_NO_B, write_no_b_receivers, 1)
+    make_case(CASE_WINDOW, BASE_WINDOW, write_window, 1)
 
 
 if __name__ == "__main__":

@@ -195,13 +195,14 @@ def test_numpy_oracle_wire_beyond_the_mesh_matches_reference(outs, tmp_path, var
 
 @pytest.mark.parametrize("variant", ["A2", "A3", "E2", "E3"])
 @pytest.mark.parametrize("case,npls", [("cube8_receivers_on_nodes", 1), ("cube8_two_wires_ragged", 2),
-                                       ("cube6_no_b_receivers", 1)])
+                                       ("cube6_no_b_receivers", 1), ("cube8_neib1_window", 1)])
 def test_numpy_oracle_receivers_on_element_boundaries_match_reference(outs, tmp_path, case, npls, variant):
     """Receivers on mesh nodes, edges and faces, some on the conductive block's surface:
     the first element in element order holds each (and, for field values, its material
     picks the smoothing subdomain), as in the reference (OutputResultant3d.cpp:572-712);
-    two sources with ragged receiver lists (recvsb 2 and 5, recvse 3 and 1); and no B
-    receivers at all (empty emf and B files)."""
+    two sources with ragged receiver lists (recvsb 2 and 5, recvse 3 and 1); no B
+    receivers at all (empty emf and B files); and a one-level receiver neighbourhood with
+    a printed window inside the time grid."""
     import sys
     sys.path.insert(0, GOLDEN)
     import make_nodes_golden as ng
@@ -213,6 +214,33 @@ def test_numpy_oracle_receivers_on_element_boundaries_match_reference(outs, tmp_
             err = outs.compare_files(os.path.join(d, "%s.%d" % (o, p)),
                                      os.path.join(GOLDEN, case, "%s_%s.%d" % (variant, o, p)))
             assert err <= FP64_TOL, (o, p, err)
+
+
+def test_reference_zeroes_receivers_when_the_print_window_ends_inside_a_decade(golden, outs, tmp_path):
+    """The one known divergence from the reference's outputs, shown on the reference itself:
+    it projects a decade's receivers when that decade's last layer passes the receiver step
+    (OutputResultant3d.cpp:432-474), and that step skips layers past the printed window
+    (give_out_vec_loop.cpp:234). So with a window ending inside a decade, every printed
+    layer of that decade holds zeros in B (and a jump in E). The restatement, like the
+    drop-in, prints the computed values there; it agrees everywhere else."""
+    import run_ref
+    if not run_ref.available("CalcNonstat3DLine_A2"):
+        pytest.skip("oracle/_ref not built")
+    d = str(tmp_path / "w")
+    golden.write_case_inputs("cube8_block", d)
+    with open(os.path.join(d, "timeintervalforprint"), "w") as f:
+        f.write("1.5000000000000e-04 6.0000000000000e-04\n")  # ends inside the third decade
+    r, o = os.path.join(d, "ref"), os.path.join(d, "oracle")
+    run_ref.copy_inputs(d, r)
+    run_ref.copy_inputs(d, o)
+    run_ref.run_transient(r, "A2")
+    tdem_oracle.run(o, "A", 2)
+    for (_, ref), (_, ora) in zip(outs.read_transients(os.path.join(r, "ball_anom.1")),
+                                  outs.read_transients(os.path.join(o, "ball_anom.1"))):
+        late = ref[:, 0] > 0.5  # ms: layers 5.24e-4 and 6.19e-4 s, the third decade
+        assert late.sum() == 2 and np.all(ref[late, 1:] == 0.0) and np.any(ora[late, 1:] != 0.0)
+        scale = np.abs(ref[~late, 1:]).max()
+        assert np.abs(ref[~late, 1:] - ora[~late, 1:]).max() <= FP64_TOL * scale
 
 
 def test_three_point_formulas_exact_for_quadratics():
