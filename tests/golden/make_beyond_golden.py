@@ -36,23 +36,48 @@ def write_sours(path: str) -> None:
         f.write("%f %f %f\n%f %f %f\n" % WIRE)
 
 
-def write_case_inputs(path: str) -> None:
-    """cube6's inputs with the stored `sours` of this case."""
+# the second case: cube6's own wire with a current that ramps down over four layers with
+# an undershoot (1, 0.7, 0.3, -0.1, 0.05, then 0) instead of stepping off: the A-form
+# source J(t) acts on several layers and the E-form source -dJ/dt is a difference of
+# them (time_approx.cpp:1039-1076, E2/time_approx.cpp:1057-1105)
+CASE_RAMP = "cube6_ramp_current"
+RAMP = (1.0, 0.7, 0.3, -0.1, 0.05)
+
+
+def write_ramp(path: str) -> None:
+    rows = [line.split() for line in open(os.path.join(path, "currentfunction")) if line.strip()]
+    with open(os.path.join(path, "currentfunction"), "w") as f:
+        for i, r in enumerate(rows):
+            f.write("%s\t%.13e\n" % (r[0], RAMP[i] if i < len(RAMP) else 0.0))
+
+
+CASE_FILES = {CASE: ("sours",), CASE_RAMP: ("currentfunction",)}
+
+
+def write_case_inputs(path: str, case: str = CASE) -> None:
+    """cube6's inputs with the stored files of `case`."""
     import make_golden
     make_golden.write_case_inputs(BASE, path)
-    shutil.copy2(os.path.join(HERE, CASE, "sours"), os.path.join(path, "sours"))
+    for name in CASE_FILES[case]:
+        shutil.copy2(os.path.join(HERE, case, name), os.path.join(path, name))
 
 
 def main() -> None:
+    make_case(CASE, write_sours)
+    make_case(CASE_RAMP, write_ramp)
+
+
+def make_case(case: str, write) -> None:
     import make_golden
     import run_ref
-    out = os.path.join(HERE, CASE)
+    out = os.path.join(HERE, case)
     os.makedirs(out, exist_ok=True)
     work = tempfile.mkdtemp(prefix="golden_beyond_")
     try:
         make_golden.write_case_inputs(BASE, work)
-        write_sours(work)
-        shutil.copy2(os.path.join(work, "sours"), os.path.join(out, "sours"))
+        write(work)
+        for name in CASE_FILES[case]:
+            shutil.copy2(os.path.join(work, name), os.path.join(out, name))
         for v in VARIANTS:
             d = os.path.join(work, v)
             run_ref.copy_inputs(work, d)

@@ -34,18 +34,21 @@ def test_gpu_matches_reference_goldens(pkg, golden, outs, tmp_path, case, varian
 
 
 @pytest.mark.parametrize("variant", VARIANTS)
-def test_gpu_wire_beyond_the_mesh_matches_reference(pkg, outs, tmp_path, variant):
+@pytest.mark.parametrize("case", ["cube6_wire_beyond", "cube6_ramp_current"])
+def test_gpu_wire_beyond_the_mesh_matches_reference(pkg, outs, tmp_path, case, variant):
     """A wire half past the mesh edge: the dipoles outside go to the nearest element, with
-    local coordinates outside [0, 1], as in the reference (vec_prep_data.cpp:878-980)."""
+    local coordinates outside [0, 1], as in the reference (vec_prep_data.cpp:878-980); and a
+    current ramped down over four layers (the A-form source on several layers, the E-form
+    source from their differences)."""
     sys.path.insert(0, GOLDEN)
     import make_beyond_golden as bg
     d = str(tmp_path / "gpu")
-    bg.write_case_inputs(d)
+    bg.write_case_inputs(d, case)
     with pkg.Solver(d, variant[0], int(variant[1])) as s:
         s.run()
         s.write_outputs()
     for o in bg.OUTPUTS:
-        err = outs.compare_files(os.path.join(d, o + ".1"), os.path.join(GOLDEN, bg.CASE, "%s_%s.1" % (variant, o)))
+        err = outs.compare_files(os.path.join(d, o + ".1"), os.path.join(GOLDEN, case, "%s_%s.1" % (variant, o)))
         assert err <= FP64_TOL, (o, err)
 
 

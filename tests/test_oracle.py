@@ -216,6 +216,24 @@ def test_numpy_oracle_receivers_on_element_boundaries_match_reference(outs, tmp_
             assert err <= FP64_TOL, (o, p, err)
 
 
+@pytest.mark.parametrize("variant", ["A2", "A3", "E2", "E3"])
+def test_numpy_oracle_ramped_current_matches_reference(outs, tmp_path, variant):
+    """A current that ramps down over four layers with an undershoot: the A-form source
+    J(t) on every layer where it is non-zero, the E-form source -dJ/dt from the layers'
+    differences (time_approx.cpp:1039-1076, E2/time_approx.cpp:1057-1105); measured up to
+    2.5e-10 of the peak (A2), 7e-12 (E-form)."""
+    import sys
+    sys.path.insert(0, GOLDEN)
+    import make_beyond_golden as bg
+    d = str(tmp_path / "ramp")
+    bg.write_case_inputs(d, bg.CASE_RAMP)
+    tdem_oracle.run(d, variant[0], int(variant[1]))
+    for o in bg.OUTPUTS:
+        err = outs.compare_files(os.path.join(d, o + ".1"),
+                                 os.path.join(GOLDEN, bg.CASE_RAMP, "%s_%s.1" % (variant, o)))
+        assert err <= FP64_TOL, (o, err)
+
+
 def test_reference_zeroes_receivers_when_the_print_window_ends_inside_a_decade(golden, outs, tmp_path):
     """The one known divergence from the reference's outputs, shown on the reference itself:
     it projects a decade's receivers when that decade's last layer passes the receiver step
