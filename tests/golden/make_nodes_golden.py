@@ -1,6 +1,6 @@
-"""Golden fixtures of receiver edge cases (the first case: receivers on element
-boundaries; the others below: ragged per-source lists, no B receivers, a one-level
-neighbourhood with a printed window inside the grid): the reference's own
+"""Golden fixtures of receiver and material edge cases (the first case: receivers on
+element boundaries; the others below: ragged per-source lists, no B receivers, a one-level
+neighbourhood with a printed window inside the grid, a permeable block): the reference's own
 CalcNonstat3DLine_{A2,A3,E2,E3} built from source by oracle/build_ref.sh, run on the
 golden case cube8_block with its receivers replaced by points on mesh nodes, edges and
 faces, some on the surface of the conductive block (x, y in [-30, 30] m, z in [-50, -20] m;
@@ -98,8 +98,24 @@ def write_window(path: str) -> None:
         f.write("2.0000000000000e-04 4.2857142857143e-04\n")
 
 
-BASES = {CASE: BASE, CASE_RAGGED: BASE_RAGGED, CASE_NO_B: BASE_NO_B, CASE_WINDOW: BASE_WINDOW}
-CASE_FILES = {CASE: FILES, CASE_RAGGED: FILES, CASE_NO_B: FILES, CASE_WINDOW: ("n_neib", "timeintervalforprint")}
+# the fifth case: cube8_block with a permeable block (mu3d: relative permeability 20 for
+# the block's material 4), so the curl-curl term B/mu varies between elements
+# (T_Brick.cpp:142-310 with mu from mu3d, vec_prep_data.cpp:83-257)
+CASE_MU = "cube8_permeable_block"
+BASE_MU = "cube8_block"
+
+
+def write_permeable(path: str) -> None:
+    rows = [line.split() for line in open(os.path.join(path, "mu3d")) if line.strip()]
+    with open(os.path.join(path, "mu3d"), "w") as f:
+        for r in rows:
+            mu = 20.0 if r[0] == "4" else float(r[1])
+            f.write("%s\t%.7e\t%.7e\n" % (r[0], mu, mu))
+
+
+BASES = {CASE: BASE, CASE_RAGGED: BASE_RAGGED, CASE_NO_B: BASE_NO_B, CASE_WINDOW: BASE_WINDOW, CASE_MU: BASE_MU}
+CASE_FILES = {CASE: FILES, CASE_RAGGED: FILES, CASE_NO_B: FILES, CASE_WINDOW: ("n_neib", "timeintervalforprint"),
+              CASE_MU: ("mu3d",)}
 
 
 def write_case_inputs(path: str, case: str = CASE) -> None:
@@ -137,6 +153,7 @@ def main() -> None:
     make_case(CASE_RAGGED, BASE_RAGGED, write_ragged_receivers, 2)
     make_case(CASE_NO_B, BASE_NO_B, write_no_b_receivers, 1)
     make_case(CASE_WINDOW, BASE_WINDOW, write_window, 1)
+    make_case(CASE_MU, BASE_MU, write_permeable, 1)
 
 
 if __name__ == "__main__":

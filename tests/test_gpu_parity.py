@@ -54,7 +54,8 @@ def test_gpu_wire_beyond_the_mesh_matches_reference(pkg, outs, tmp_path, case, v
 
 @pytest.mark.parametrize("variant", VARIANTS)
 @pytest.mark.parametrize("case,npls", [("cube8_receivers_on_nodes", 1), ("cube8_two_wires_ragged", 2),
-                                       ("cube6_no_b_receivers", 1), ("cube8_neib1_window", 1)])
+                                       ("cube6_no_b_receivers", 1), ("cube8_neib1_window", 1),
+                                       ("cube8_permeable_block", 1)])
 def test_gpu_receivers_on_element_boundaries_match_reference(pkg, outs, tmp_path, case, npls, variant):
     """Receivers on mesh nodes, edges and faces (the first element in element order holds
     each, its material picks the field's smoothing subdomain), against the reference."""

@@ -195,14 +195,15 @@ def test_numpy_oracle_wire_beyond_the_mesh_matches_reference(outs, tmp_path, var
 
 @pytest.mark.parametrize("variant", ["A2", "A3", "E2", "E3"])
 @pytest.mark.parametrize("case,npls", [("cube8_receivers_on_nodes", 1), ("cube8_two_wires_ragged", 2),
-                                       ("cube6_no_b_receivers", 1), ("cube8_neib1_window", 1)])
+                                       ("cube6_no_b_receivers", 1), ("cube8_neib1_window", 1),
+                                       ("cube8_permeable_block", 1)])
 def test_numpy_oracle_receivers_on_element_boundaries_match_reference(outs, tmp_path, case, npls, variant):
     """Receivers on mesh nodes, edges and faces, some on the conductive block's surface:
     the first element in element order holds each (and, for field values, its material
     picks the smoothing subdomain), as in the reference (OutputResultant3d.cpp:572-712);
     two sources with ragged receiver lists (recvsb 2 and 5, recvse 3 and 1); no B
-    receivers at all (empty emf and B files); and a one-level receiver neighbourhood with
-    a printed window inside the time grid."""
+    receivers at all (empty emf and B files); a one-level receiver neighbourhood with a
+    printed window inside the time grid; and a permeable block (relative mu 20)."""
     import sys
     sys.path.insert(0, GOLDEN)
     import make_nodes_golden as ng

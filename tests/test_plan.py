@@ -249,7 +249,8 @@ def _read_operator(path):
 @pytest.mark.parametrize("case,form", [("cube8_two_wires", "A"), ("cube8_two_wires", "E"),
                                        ("cube6_wire_beyond", "E"), ("cube8_receivers_on_nodes", "E"),
                                        ("cube8_two_wires_ragged", "A"), ("cube6_no_b_receivers", "A"),
-                                       ("cube8_neib1_window", "E"), ("cube6_ramp_current", "A")])
+                                       ("cube8_neib1_window", "E"), ("cube6_ramp_current", "A"),
+                                       ("cube8_permeable_block", "E")])
 def test_host_plan_products_match_the_oracle(pkg, golden, tmp_path, case, form):
     """The host half of a solve (TransientSolve::plan, no device) against the numpy oracle,
     which the reference's goldens pin: the source vectors and the initial field that go to
@@ -270,7 +271,7 @@ def test_host_plan_products_match_the_oracle(pkg, golden, tmp_path, case, form):
                     "-Wl,-rpath," + lib_dir, "-o", exe], check=True)
     d = str(tmp_path / case)
     if case in ("cube6_wire_beyond", "cube8_receivers_on_nodes", "cube8_two_wires_ragged", "cube6_no_b_receivers",
-                "cube8_neib1_window", "cube6_ramp_current"):
+                "cube8_neib1_window", "cube6_ramp_current", "cube8_permeable_block"):
         sys.path.insert(0, os.path.join(here, "golden"))
         import make_beyond_golden as bg
         import make_nodes_golden as ng
