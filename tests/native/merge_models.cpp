@@ -3,7 +3,8 @@
 // one mesh; argv[n]: a directory with another mesh.  Checks the merged model
 // (sources and receivers in order, per-source receiver ranges shifted), the initial
 // field read per directory, the host plan of the merged directories (TransientSolve
-// ::plan_merged, no device) and the refusal of a different mesh.
+// ::plan_merged, no device) and the refusal of a different mesh; with --expect, the
+// refusal of two directories with the given message.
 #include <cstdio>
 #include <string>
 #include <vector>
@@ -12,7 +13,26 @@
 #include "model.h"
 using namespace tdem;
 
+// --expect <dir a> <dir b> <error>: merging a and b must fail with exactly <error>
+static int expect(const char* a, const char* b, const char* want) {
+  std::vector<Model> parts(2);
+  std::string e;
+  if (!(e = load_model(a, parts[0])).empty() || !(e = load_model(b, parts[1])).empty()) {
+    printf("load: %s\n", e.c_str());
+    return 1;
+  }
+  Model m;
+  e = merge_models(parts, m);
+  if (e != want) {
+    printf("expected '%s', got '%s'\n", want, e.c_str());
+    return 1;
+  }
+  printf("ok refused: %s\n", e.c_str());
+  return 0;
+}
+
 int main(int argc, char** argv) {
+  if (argc == 5 && std::string(argv[1]) == "--expect") return expect(argv[2], argv[3], argv[4]);
   if (argc < 4) { printf("usage\n"); return 2; }
   std::vector<std::string> dirs(argv + 1, argv + argc - 1);
   std::vector<Model> parts(dirs.size());

@@ -198,6 +198,36 @@ def test_models_of_one_mesh_merge_for_batched_serving(pkg, mg, tmp_path):
     mg.write_analytic_initial_field(other, spec)
     r = subprocess.run([exe] + dirs + [other], capture_output=True, text=True)
     assert r.returncode == 0 and r.stdout.startswith("ok 4 sources"), r.stdout + r.stderr
+    # the other checks: materials, time grid, current function, source settings
+    import shutil as sh
+    for name, edit, message in (
+            ("mat", _scale_sigma, "the materials differ"),
+            ("grid", _shift_time, "the time grids differ"),
+            ("srs", _set_dipole_count, "the source or receiver settings differ")):
+        d = str(tmp_path / ("bad_" + name))
+        sh.copytree(dirs[0], d)
+        edit(d)
+        r = subprocess.run([exe, "--expect", dirs[1], d, message], capture_output=True, text=True)
+        assert r.returncode == 0, (name, r.stdout + r.stderr)
+
+
+def _set_dipole_count(d):
+    with open(os.path.join(d, "nSrsRazb"), "w") as f:
+        f.write("7\n")
+
+
+def _scale_sigma(d):
+    rows = [line.split() for line in open(os.path.join(d, "sig3d")) if line.strip()]
+    with open(os.path.join(d, "sig3d"), "w") as f:
+        f.write("".join("%s\t%.7e\t%.7e\n" % (r[0], 2 * float(r[1]), 2 * float(r[2])) for r in rows))
+
+
+def _shift_time(d):
+    with open(os.path.join(d, "infite.0")) as f:
+        head, body = f.read().split("T I M E :", 1)
+    last = body.replace(";", " ").split()[-1]
+    with open(os.path.join(d, "infite.0"), "w") as f:
+        f.write(head + "T I M E :" + body.replace(last, "%.13e" % (1.5 * float(last))))
 
 
 def test_point_location_and_threaded_receiver_smoothing(pkg, mg, tmp_path):
