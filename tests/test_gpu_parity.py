@@ -47,9 +47,13 @@ def test_gpu_wire_beyond_the_mesh_matches_reference(pkg, outs, tmp_path, case, v
     with pkg.Solver(d, variant[0], int(variant[1])) as s:
         s.run()
         s.write_outputs()
+    # the A-form with the ramped current is rounding-sensitive: the elimination order alone
+    # moves it by up to 5.4e-10 (three CPU orderings against each other and against the
+    # reference), so it gets 2e-9; every other case keeps the FP64 tolerance
+    tol = 2e-9 if (case == "cube6_ramp_current" and variant[0] == "A") else FP64_TOL
     for o in bg.OUTPUTS:
         err = outs.compare_files(os.path.join(d, o + ".1"), os.path.join(GOLDEN, case, "%s_%s.1" % (variant, o)))
-        assert err <= FP64_TOL, (o, err)
+        assert err <= tol, (o, err)
 
 
 @pytest.mark.parametrize("variant", VARIANTS)
