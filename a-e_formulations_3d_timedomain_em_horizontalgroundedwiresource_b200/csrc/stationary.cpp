@@ -14,7 +14,9 @@
 #include <memory>
 #include <vector>
 
+#include "boxgrid.h"
 #include "gpu_cholesky.h"
+#include "parallel.h"
 #include "symbolic.h"
 
 namespace tdem {
@@ -162,26 +164,56 @@ void bbox(const StatModel& m, int e, double mn[3], double mx[3]) {
 
 // First earth element (file order) whose box (+-1e-3) holds the point with local
 // coordinates in (-0.01, 1.01) (TaskSP.cpp:1745-1942, CheckAndGet :1361-1377);
-// otherwise the nearest earth element (GetNearestElement, :1379-1474).
+// otherwise the nearest earth element (GetNearestElement, :1379-1474).  The first
+// search looks only at the earth elements listed in the point's cell of a grid of the
+// boxes (BoxGrid: every box holding the point is listed there, in element order), the
+// points on host threads.
 std::string locate(const StatModel& m, std::vector<PointSource*>& pts) {
   const double lo = -1e-2, hi = 1.0 + 1e-2;
-  for (int e = 0; e < m.krect; ++e) {
-    if (m.mtr[e] == 1) continue;
-    double mn[3], mx[3];
-    bbox(m, e, mn, mx);
-    for (PointSource* p : pts) {
-      if (p->elem != -1) continue;
-      if (p->x < mn[0] - 1e-3 || p->x > mx[0] + 1e-3 || p->y < mn[1] - 1e-3 || p->y > mx[1] + 1e-3 ||
-          p->z < mn[2] - 1e-3 || p->z > mx[2] + 1e-3)
-        continue;
-      double l[3];
-      local_coords(m, e, *p, l);
-      if (l[0] > lo && l[0] < hi && l[1] > lo && l[1] < hi && l[2] > lo && l[2] < hi) {
-        p->elem = e;
-        std::copy(l, l + 3, p->l);
+  std::vector<double> bmn(3 * (size_t)m.krect), bmx(3 * (size_t)m.krect);
+  parallel_ranges(m.krect, [&](int64_t e0, int64_t e1) {
+    for (int64_t e = e0; e < e1; ++e) {
+      double mn[3], mx[3];
+      bbox(m, (int)e, mn, mx);
+      for (int c = 0; c < 3; ++c) {
+        // air elements are never candidates: an empty box is not listed
+        bmn[3 * e + c] = m.mtr[e] == 1 ? 1.0 : mn[c] - 1e-3;
+        bmx[3 * e + c] = m.mtr[e] == 1 ? 0.0 : mx[c] + 1e-3;
       }
     }
+  });
+  double qlo[3] = {INFINITY, INFINITY, INFINITY}, qhi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (const PointSource* p : pts) {
+    const double q[3] = {p->x, p->y, p->z};
+    for (int c = 0; c < 3; ++c)
+      if (!std::isnan(q[c])) {
+        qlo[c] = std::min(qlo[c], q[c]);
+        qhi[c] = std::max(qhi[c], q[c]);
+      }
   }
+  BoxGrid grid;
+  grid.build(bmn, bmx, qlo, qhi);
+  parallel_ranges((int64_t)pts.size(), [&](int64_t k0, int64_t k1) {
+    for (int64_t k = k0; k < k1; ++k) {
+      PointSource* p = pts[k];
+      if (p->elem != -1) continue;
+      const double q[3] = {p->x, p->y, p->z};
+      const auto cand = grid.candidates(q);
+      for (const int* c = cand.first; c != cand.second; ++c) {
+        const int e = *c;
+        const double* mn = &bmn[3 * (size_t)e];
+        const double* mx = &bmx[3 * (size_t)e];
+        if (p->x < mn[0] || p->x > mx[0] || p->y < mn[1] || p->y > mx[1] || p->z < mn[2] || p->z > mx[2]) continue;
+        double l[3];
+        local_coords(m, e, *p, l);
+        if (l[0] > lo && l[0] < hi && l[1] > lo && l[1] < hi && l[2] > lo && l[2] < hi) {
+          p->elem = e;
+          std::copy(l, l + 3, p->l);
+          break;
+        }
+      }
+    }
+  }, 256);
   for (PointSource* p : pts) {
     if (p->elem != -1) continue;
     // 8 nearest earth elements by L1 distance to their boxes, then the one whose
@@ -315,19 +347,14 @@ bool write_file(const std::string& fn, const double* v, size_t count, bool appen
   return fclose(f) == 0 && ok;
 }
 
-}  // namespace
-
-std::string solve_stationary(const std::string& dir, int device, StationaryTimes* times) {
-  const double t0 = now_s();
-  StatModel m;
-  std::string e = read_model(dir, m);
-  if (!e.empty()) return e;
-  const int n = m.kpnt, npls = m.npls;
-
-  // sources: nSrsRazb dipoles per wire and the two electrodes
-  std::vector<std::vector<PointSource>> dip(npls, std::vector<PointSource>(m.nsrs));
-  std::vector<PointSource> elA(npls), elB(npls);
-  std::vector<PointSource*> pts;
+// per wire its nSrsRazb dipoles, then electrodes A and B (pts in that order)
+void source_points(const StatModel& m, std::vector<std::vector<PointSource>>& dip, std::vector<PointSource>& elA,
+                   std::vector<PointSource>& elB, std::vector<PointSource*>& pts) {
+  const int npls = m.npls;
+  dip.assign(npls, std::vector<PointSource>(m.nsrs));
+  elA.assign(npls, PointSource());
+  elB.assign(npls, PointSource());
+  pts.clear();
   for (int i = 0; i < npls; ++i) {
     const auto& w = m.wires[i];
     const double d[3] = {(w[3] - w[0]) / m.nsrs, (w[4] - w[1]) / m.nsrs, (w[5] - w[2]) / m.nsrs};
@@ -346,6 +373,36 @@ std::string solve_stationary(const std::string& dir, int device, StationaryTimes
     pts.push_back(&elA[i]);
     pts.push_back(&elB[i]);
   }
+}
+
+}  // namespace
+
+std::string stationary_source_points(const std::string& dir, std::vector<std::array<double, 4>>& out) {
+  StatModel m;
+  std::string e = read_model(dir, m);
+  if (!e.empty()) return e;
+  std::vector<std::vector<PointSource>> dip;
+  std::vector<PointSource> elA, elB;
+  std::vector<PointSource*> pts;
+  source_points(m, dip, elA, elB, pts);
+  if (!(e = locate(m, pts)).empty()) return e;
+  out.clear();
+  for (const PointSource* p : pts) out.push_back({(double)p->elem, p->l[0], p->l[1], p->l[2]});
+  return "";
+}
+
+std::string solve_stationary(const std::string& dir, int device, StationaryTimes* times) {
+  const double t0 = now_s();
+  StatModel m;
+  std::string e = read_model(dir, m);
+  if (!e.empty()) return e;
+  const int n = m.kpnt, npls = m.npls;
+
+  // sources: nSrsRazb dipoles per wire and the two electrodes
+  std::vector<std::vector<PointSource>> dip;
+  std::vector<PointSource> elA, elB;
+  std::vector<PointSource*> pts;
+  source_points(m, dip, elA, elB, pts);
   if (!(e = locate(m, pts)).empty()) return e;
 
   NodalPattern pat;

@@ -10,7 +10,9 @@
 // Writes v3n.dat (zeros), v3a.dat (V per source) and a0.dat (Ax, Ay, Az per node
 // per source) in the reference's binary layout.
 #pragma once
+#include <array>
 #include <string>
+#include <vector>
 
 namespace tdem {
 
@@ -21,5 +23,10 @@ struct StationaryTimes {
 };
 
 std::string solve_stationary(const std::string& dir, int device, StationaryTimes* times = nullptr);
+
+// Host only (no device): the element and local coordinates {elem, l0, l1, l2} of every
+// source point solve_stationary places, in its order (per wire its nSrsRazb dipoles,
+// then electrodes A and B).
+std::string stationary_source_points(const std::string& dir, std::vector<std::array<double, 4>>& out);
 
 }  // namespace tdem

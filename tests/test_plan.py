@@ -400,3 +400,29 @@ def test_merged_host_plan_is_the_parts_side_by_side(pkg, mg, tmp_path):
                         assert src[a] == psrc[b] + coff
                     roff += nr
                     coff += pn
+
+
+def test_stationary_source_points_match_a_scan(pkg, golden, tmp_path):
+    """The stationary module's electrodes and dipoles (stationary_source_points, host only)
+    against a scan over all earth elements with the nearest-element rule, restated in the
+    driver: bitwise equal elements and local coordinates, on cube8_two_wires and on the wire
+    half past the mesh edge (51 points outside the mesh)."""
+    import shutil
+    import subprocess
+    if shutil.which("g++") is None:
+        pytest.skip("no C++ compiler")
+    here = os.path.dirname(os.path.abspath(__file__))
+    lib_dir = os.path.dirname(pkg.LIB_PATH)
+    exe = str(tmp_path / "points")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", os.path.join(os.path.dirname(pkg.__file__), "csrc"),
+                    "-I", os.path.join(os.path.dirname(here), "include"), "-I", "/usr/local/cuda/include",
+                    os.path.join(here, "native", "stationary_points.cpp"), "-L" + lib_dir, "-ltdem_b200",
+                    "-Wl,-rpath," + lib_dir, "-o", exe], check=True)
+    sys.path.insert(0, os.path.join(here, "golden"))
+    import make_beyond_golden as bg
+    a, b = str(tmp_path / "two"), str(tmp_path / "beyond")
+    golden.write_case_inputs("cube8_two_wires", a)
+    bg.write_case_inputs(b)
+    for d, outside in ((a, 0), (b, 51)):
+        r = subprocess.run([exe, d], capture_output=True, text=True)
+        assert r.returncode == 0 and r.stdout.strip().endswith("(%d outside)" % outside), r.stdout + r.stderr
